@@ -1,0 +1,217 @@
+/*
+ * zf.h — C ABI of the B200-native Zebraflow coupled LBM–IB–RBC time step.
+ *
+ * The reference (SweSoe/Zebraflow) has no plugin or FFI boundary: its steps are
+ * inline blocks of main() in ZebraflowWT.c, named only by the unused prototypes
+ * at ZebraflowWT.c:163-169 and by section comments.  Every entry point below
+ * replaces one of those blocks and says which one (file:line, reference paths
+ * relative to the reference project root).  All state the reference keeps in
+ * global static arrays (ZebraflowWT.c:171-276) lives in a zf_ctx; host buffers
+ * are caller-owned and copied in or out; device memory is owned by the context.
+ *
+ * Conventions shared by every call:
+ *  - Lattice points are addressed (i,j,k), 0-based, i in [0,nx), k fastest in
+ *    dense host arrays (C order of a [nx][ny][nz] array), so B_index[i][j][k]
+ *    of the reference maps to b_index[(i*ny + j)*nz + k] with i,j,k shifted by 1.
+ *  - "Listed nodes" are the lattice points with B_index >= 0, enumerated in the
+ *    reference's DOMLIST order (LBM_DOM_SETUP, ZebraflowWT.c:1481-1502: i outer,
+ *    j, k inner).  Every per-node host array is indexed by that 0-based order.
+ *  - Populations use the reference's direction order (ZebraflowWT.c:2471-2497):
+ *    slot q=0..18 is the reference's c=q+1 (c=19, slot 18, is the rest
+ *    population).  Population host arrays are [19][n_listed] (c-major, as F[c][l]).
+ *  - Membrane, nucleus and wall-mesh coordinates are in micrometres and
+ *    membrane forces in newtons, exactly as in the reference.
+ *  - Every call returns ZF_OK or an error code; zf_last_error() gives a message.
+ *  - One zf_ctx per host thread.  Calls enqueue on the context's CUDA stream and
+ *    are ordered; zf_sync() waits for them.
+ */
+#ifndef ZF_H
+#define ZF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZF_Q 19
+
+enum zf_status_code {
+  ZF_OK = 0,
+  ZF_ERR_CUDA = 1,      /* a CUDA runtime call failed (message in zf_last_error) */
+  ZF_ERR_ARG = 2,       /* invalid argument or unsupported input code */
+  ZF_ERR_OVERFLOW = 3,  /* a fixed-capacity list overflowed (cell list, neighbour list) */
+  ZF_ERR_NONFINITE = 4, /* non-finite value detected in a checked buffer */
+  ZF_ERR_STATE = 5,     /* call made before the state it needs was set */
+  ZF_ERR_NOMEM = 6      /* device allocation failed */
+};
+
+/* Wall treatment of the LBM step. */
+enum zf_wall_mode {
+  ZF_WALL_HALFWAY_BB = 0, /* link bounce-back halfway between fluid and non-fluid points */
+  ZF_WALL_REF_EQ = 1      /* reference: wall points (B_index==0) hold feq(rho_neighbour, u=0),
+                             ZebraflowWT.c:6290-6315 and :6429-6432 */
+};
+
+/* Storage type of the populations in HBM. */
+enum zf_storage {
+  ZF_STORE_F32 = 0,  /* plain fp32 populations */
+  ZF_STORE_F16 = 1,  /* fp16 of S*(f_q/w_q - rho_ref), arithmetic in fp32 */
+  ZF_STORE_BF16 = 2  /* bf16 of the same deviation */
+};
+
+/* Run-time parameters.  zf_params_default() fills the reference's values
+ * (ZebraflowWT.c:34-161) so that a default-filled struct reproduces the
+ * reference constants; callers override lattice size and what they need. */
+typedef struct zf_params {
+  /* lattice */
+  int32_t nx, ny, nz;       /* lattice box (reference IM, JM, KM) */
+  double origin[3];         /* um, coordinates of lattice point (0,0,0) (reference X0,Y0,Z0) */
+  double dx;                /* um, lattice spacing (reference DX = 0.5) */
+  double dt;                /* us, time step (reference DT = 0.5); also the factor that
+                               multiplies BODYFORCE in the Guo step, ZebraflowWT.c:6133,6141 */
+  float tau;                /* BGK relaxation time of every fluid point */
+  int32_t tau_from_phase;   /* 1: tau = 0.5 + 0.72*B_index per point (ZebraflowWT.c:6110) */
+  float g[3];               /* uniform effective Guo body force, lattice units; added to
+                               dt*BODYFORCE (0 in the reference) */
+  int32_t wall_mode;        /* enum zf_wall_mode */
+  int32_t periodic[3];      /* 1: the axis wraps (the reference wraps none) */
+  int32_t storage;          /* enum zf_storage */
+  float rho_ref;            /* reference density of the deviation storage */
+  /* membrane / IB / coupling (SI units unless stated) */
+  int32_t stagger;          /* membrane + IB solver every `stagger` LBM steps (SOLVERSTAGGER=50) */
+  double Es;                /* membrane shear modulus, N/m (reference 3e-6) */
+  double Es_nucleus_ratio;  /* nucleus shear modulus / Es (reference 0.1, ZebraflowWT.c:2039) */
+  double kbend;             /* bending coefficient, J (reference 1.3856406e-19) */
+  double kd;                /* local area coefficient, N/m (reference 3.6e-5) */
+  double ka;                /* global area coefficient, N/m (reference 7.7e-5) */
+  double kv;                /* volume coefficient, N/m^2 (reference 55) */
+  double area0;             /* rest cell area, m^2; <= 0: from the rest mesh (reference RBC_SURF) */
+  double volume0;           /* rest cell volume, m^3; <= 0: from the rest mesh (reference MCV) */
+  double kT;                /* TEMPERATURE*BOLTZ, J */
+  double e_ratio_eq;        /* rest / maximum spectrin length (0.3154574132) */
+  int32_t calib_passes;     /* fixed-point passes of the spring calibration (51) */
+  double gamma_p;           /* repulsion-to-force coefficient of IB spreading (1e-7) */
+  double unit_mass;         /* kg, lattice mass unit (UNITMASS = 1.25e-15) */
+  double bforce_scale;      /* LBM_BFORCE_SCALE = (1/3)*dx/dt^2 in SI (6.6667e5) */
+  double vel_scale;         /* VEL_SCALE (1.0) */
+  double vmax_remove;       /* node speed that removes a cell (5e-3) */
+  int32_t remove_count;     /* screened-term count that removes a cell (500) */
+  int32_t nuc_list_period;  /* nucleus-membrane list rebuild period in iterations (1000) */
+  int32_t nuc_list_max;     /* capacity of each nucleus node's triangle list (NucMembMAX) */
+} zf_params;
+
+typedef struct zf_ctx zf_ctx;
+
+/* Counters returned by zf_get_status (reference: printf + simfailure, which
+ * is counted but never read, ZebraflowWT.c:5647, :7086-7345). */
+typedef struct zf_status {
+  int64_t screened_terms;   /* force terms dropped as NaN/inf/over 1e-10 N */
+  int64_t cells_removed;    /* cells removed (bad geometry or speed) */
+  int64_t list_overflows;   /* cell-list / nucleus-list entries that did not fit */
+  int64_t bc_no_neighbour;  /* wall points without a designated neighbour */
+  int64_t iter;             /* completed LBM iterations */
+} zf_status;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Reference constants (ZebraflowWT.c:34-161) into *p. */
+void zf_params_default(zf_params* p);
+
+/* sizeof(zf_params), so that bindings can check their struct layout. */
+size_t zf_params_size(void);
+
+/* Creates a context on CUDA device `device`; params are copied.  Replaces the
+ * global state of ZebraflowWT.c:171-276.  Returns NULL on failure
+ * (zf_last_error says why). */
+zf_ctx* zf_create(const zf_params* p, int device);
+void zf_destroy(zf_ctx* ctx);
+const char* zf_last_error(void);
+int zf_sync(zf_ctx* ctx);
+int zf_get_status(zf_ctx* ctx, zf_status* out);
+
+/* ---- lattice ------------------------------------------------------------- */
+
+/* Sets the lattice from reference B_index codes ([nx][ny][nz], k fastest):
+ * <0 solid, 0 wall point, 1..9 fluid of that phase.  Codes >= 10 (pressure
+ * inlets >= 1000, the deprecated 4998) are rejected with ZF_ERR_ARG.
+ * Builds the listed-node order (LBM_DOM_SETUP, ZebraflowWT.c:1481-1502), the
+ * designated neighbour of every wall point (LBM_BC_SETUP, ZebraflowWT.c:1506-1589)
+ * and the device tile index; initialises f = feq(rho_ref, 0) (ZebraflowWT.c:5253-5295). */
+int zf_set_lattice(zf_ctx* ctx, const int32_t* b_index);
+
+/* Number of listed nodes (reference DOMMAX) and of fluid nodes (1..9). */
+int zf_num_listed(zf_ctx* ctx, int64_t* n_listed, int64_t* n_fluid);
+
+/* Listed-node coordinates in DOMLIST order, [n_listed][3] (i,j,k), 0-based. */
+int zf_get_domlist(zf_ctx* ctx, int32_t* ijk);
+
+/* ---- fluid fields (reference F, D/U/V/W, BODYFORCE; ZebraflowWT.c:176-183) -- */
+
+/* f: [19][n_listed] populations; NULL keeps them. */
+int zf_upload_populations(zf_ctx* ctx, const float* f);
+int zf_download_populations(zf_ctx* ctx, float* f);
+/* bodyforce: [3][n_listed], reference BODYFORCE units (IB force density) */
+int zf_upload_bodyforce(zf_ctx* ctx, const float* bodyforce);
+int zf_download_bodyforce(zf_ctx* ctx, float* bodyforce);
+/* D,U,V,W [n_listed] written by the last LBM step that stored moments
+ * (post-collision moments without force shift, ZebraflowWT.c:6599-6616). */
+int zf_download_moments(zf_ctx* ctx, float* D, float* U, float* V, float* W);
+
+/* ---- LBM step ------------------------------------------------------------ */
+
+/* One LBM time step: pull stream + BGK/Guo collision (ZebraflowWT.c:6100-6145),
+ * wall treatment (:6290-6315, :6429-6432 in ZF_WALL_REF_EQ; bounce-back links
+ * in ZF_WALL_HALFWAY_BB) and the moments/copy pass (:6599-6626), fused into one
+ * kernel over the tile index with ping-pong buffers.  store_moments=1 writes
+ * D,U,V,W (post-collision, as :6611-6614); zero_bodyforce=1 clears BODYFORCE
+ * after it was used (:6622-6624). */
+int zf_lbm_step(zf_ctx* ctx, int store_moments, int zero_bodyforce);
+
+/* n LBM steps back to back (moments stored on the last one only). */
+int zf_lbm_steps(zf_ctx* ctx, int n);
+
+/* One LBM step that also returns the global mass: the FP64 sum of the
+ * pre-collision density over fluid points, reduced inside the step kernel
+ * (per-block partial sums, then a fixed-order sum), copied to *mass. */
+int zf_lbm_step_mass(zf_ctx* ctx, int store_moments, int zero_bodyforce, double* mass);
+
+/* Sets the uniform effective body force g (lattice units) used from the next step. */
+int zf_set_uniform_force(zf_ctx* ctx, const float* g3);
+
+/* Runs subsequent work of the context on `cuda_stream` (a cudaStream_t of the
+ * context's device, e.g. the current PyTorch stream); NULL restores the
+ * context's own stream.  Work already queued is not moved. */
+int zf_set_stream(zf_ctx* ctx, void* cuda_stream);
+
+/* Total mass sum_l sum_q f (FP64 reduction over fluid points, or all listed
+ * points when include_walls=1). */
+int zf_mass(zf_ctx* ctx, int include_walls, double* mass);
+
+/* Device time of the last `n` LBM steps run by zf_lbm_steps_timed, in ms,
+ * measured with CUDA events on the context stream. */
+int zf_lbm_steps_timed(zf_ctx* ctx, int n, float* ms);
+
+/* Bytes of device memory the context holds. */
+int zf_device_bytes(zf_ctx* ctx, int64_t* bytes);
+
+/* ---- input generators (synthetic stand-ins for the reference's input files,
+ *      FLUIDdomainBindex.csv read at ZebraflowWT.c:2574-2619) ---------------- */
+
+/* Straight tube along z in lattice units: B_index 1 for (i-cx)^2+(j-cy)^2 < R^2,
+ * 0 for non-fluid points linked to a fluid point, -1 elsewhere. */
+int zf_gen_tube(int nx, int ny, int nz, double cx, double cy, double R, int periodic_z,
+                int32_t* b_index);
+
+/* Z-periodic Y-bifurcation: parent radius Rp splits at +-half_angle_deg (in x)
+ * into two daughters of radius Rd that run straight and merge back.  layout
+ * (6 doubles, may be NULL) receives z_split, z_straight, z_converge, z_merge,
+ * daughter offset. */
+int zf_gen_bifurcation(int nx, int ny, int nz, double Rp, double Rd, double half_angle_deg,
+                       int32_t* b_index, double* layout);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZF_H */

@@ -1,0 +1,6 @@
+/* ORACLE — test infrastructure only: the CPU restatement compiled with fp64
+ * arithmetic (the FP64 oracle of the precision form).  See orc_lbm.inc. */
+#include <omp.h>
+#define REAL double
+#define SFX _f64
+#include "orc_lbm.inc"

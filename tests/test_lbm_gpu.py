@@ -1,0 +1,145 @@
+"""GPU parity of the fused LBM kernel (zebraflow_b200/csrc/zf_lbm.cu) against
+the CPU oracle (oracle/orc_lbm.inc) through the C ABI.
+
+Tolerances: the fp32 kernel and the fp32 oracle evaluate the same formulas in
+a different order (FMA contraction on the GPU), so populations agree to a few
+ulp per step: max |df| <= 2e-6 absolute (populations are O(0.03-0.3)) after
+20 steps, density to 1e-6 and velocity to 3e-7 absolute.  The fp16 / bf16 storage forms are
+checked against the fp64 oracle with the bounds stated per test.
+"""
+import numpy as np
+import pytest
+
+import zebraflow_b200 as zf
+from oracle.bind import OracleLBM
+
+pytestmark = pytest.mark.gpu
+
+
+def make_ctx(b, wall_mode, tau=0.8, g=(0, 0, 0), storage=zf.STORE_F32, tau_from_phase=0,
+             periodic=(0, 0, 1)):
+    nx, ny, nz = b.shape
+    p = zf.default_params(nx=nx, ny=ny, nz=nz, tau=tau, tau_from_phase=tau_from_phase,
+                          wall_mode=wall_mode, storage=storage, periodic=periodic, g=g)
+    ctx = zf.Context(p)
+    ctx.set_lattice(b)
+    return ctx
+
+
+def perturbed(n, rng, amp=0.01):
+    return (zf.W[:, None] * (1 + amp * rng.standard_normal((19, n)))).astype(np.float32)
+
+
+def listed_codes(b):
+    dom = np.argwhere(b >= 0)
+    return b[dom[:, 0], dom[:, 1], dom[:, 2]]
+
+
+@pytest.mark.parametrize("wall_mode", [zf.WALL_HALFWAY_BB, zf.WALL_REF_EQ])
+def test_lbm_parity_fp32(wall_mode):
+    rng = np.random.default_rng(10 + wall_mode)
+    b = zf.gen_tube(24, 22, 32, 11.3, 10.6, 9.0, True)
+    g = (1e-6, -2e-6, 5e-6)
+    ctx = make_ctx(b, wall_mode, tau=0.83, g=g)
+    o = OracleLBM(b, wall_mode=wall_mode, periodic=(0, 0, 1), tau=0.83, g=g, precision="f32")
+    assert ctx.n_listed == o.n
+    assert np.array_equal(ctx.domlist(), np.argwhere(b >= 0))
+    f0 = perturbed(o.n, rng)
+    bf = (1e-4 * rng.standard_normal((3, o.n))).astype(np.float32)
+    ctx.upload_populations(f0)
+    ctx.upload_bodyforce(bf)
+    o.set_f(f0)
+    o.set_bodyforce(bf)
+    for s in range(20):
+        ctx.lbm_step(store_moments=True, zero_bodyforce=(s == 10))
+        o.step(rbc_flag=(s == 10))
+    codes = listed_codes(b)
+    sel = codes > 0 if wall_mode == zf.WALL_HALFWAY_BB else codes >= 0
+    fg, fo = ctx.download_populations(), o.get_f()
+    assert np.max(np.abs(fg[:, sel] - fo[:, sel])) < 2e-6
+    Dg, *ug = ctx.download_moments()
+    Do, *uo = o.moments()
+    assert np.max(np.abs(Dg[sel] - Do[sel])) <= 1e-6
+    # velocities are differences of O(0.05) populations: fp32 absolute bound
+    for a, b_ in zip(ug, uo):
+        assert np.max(np.abs(a[sel] - b_[sel])) <= 3e-7
+    # BODYFORCE was cleared on step 10 at every point the step updates
+    assert np.all(ctx.download_bodyforce()[:, sel] == 0)
+
+
+def test_lbm_tau_from_phase():
+    rng = np.random.default_rng(3)
+    b = zf.gen_tube(20, 20, 16, 9.5, 9.5, 8.0, True)
+    fl = b > 0
+    b[fl] = rng.integers(1, 4, size=int(fl.sum()))  # phases 1..3: tau = 0.5 + 0.72*B
+    ctx = make_ctx(b, zf.WALL_REF_EQ, tau_from_phase=1)
+    o = OracleLBM(b, wall_mode=1, periodic=(0, 0, 1), tau_from_phase=True, precision="f32")
+    f0 = perturbed(o.n, rng)
+    ctx.upload_populations(f0)
+    o.set_f(f0)
+    for _ in range(10):
+        ctx.lbm_step()
+        o.step()
+    assert np.max(np.abs(ctx.download_populations() - o.get_f())) < 2e-6
+
+
+def test_lbm_mass_conservation_gpu():
+    rng = np.random.default_rng(4)
+    b = zf.gen_tube(32, 32, 64, 15.5, 15.5, 14.0, True)
+    ctx = make_ctx(b, zf.WALL_HALFWAY_BB, g=(0, 0, 1e-5))
+    ctx.upload_populations(perturbed(ctx.n_listed, rng))
+    m0 = ctx.mass()
+    ctx.lbm_steps(200)
+    m1 = ctx.mass()
+    assert abs(m1 - m0) < 2e-6 * m0
+
+
+def test_lbm_periodic_bifurcation_runs():
+    b, _ = zf.gen_bifurcation(64, 48, 128, 8, 6, 20.0)
+    ctx = make_ctx(b, zf.WALL_HALFWAY_BB, tau=0.9, g=(0, 0, 1e-5))
+    m0 = ctx.mass()
+    ctx.lbm_steps(100)
+    D, U, V, W = ctx.download_moments()
+    fl = listed_codes(b) > 0
+    assert np.isfinite(W[fl]).all() and W[fl].mean() > 0
+    assert abs(ctx.mass() - m0) < 2e-6 * m0
+
+
+def poiseuille_run(storage, steps=1500):
+    b = zf.gen_tube(20, 20, 8, 9.5, 9.5, 8.0, True)
+    g = (0, 0, 2e-6)
+    ctx = make_ctx(b, zf.WALL_HALFWAY_BB, tau=0.8, g=g, storage=storage)
+    o = OracleLBM(b, wall_mode=0, periodic=(0, 0, 1), tau=0.8, g=g, precision="f64")
+    ctx.lbm_steps(steps)
+    for _ in range(steps):
+        o.step()
+    fl = listed_codes(b) > 0
+    wg = ctx.download_moments()[3][fl].astype(np.float64)
+    wo = o.moments()[3][fl]
+    return np.linalg.norm(wg - wo) / np.linalg.norm(wo)
+
+
+def test_storage_forms_against_fp64_oracle():
+    """Relative L2 error of the axial velocity after 1500 steps of developing
+    Poiseuille flow: fp32 <= 1e-5, fp16 deviation storage <= 2e-3,
+    bf16 deviation storage <= 3e-2 (8-bit mantissa)."""
+    e32 = poiseuille_run(zf.STORE_F32)
+    e16 = poiseuille_run(zf.STORE_F16)
+    ebf = poiseuille_run(zf.STORE_BF16)
+    print(f"rel L2 velocity error: fp32 {e32:.2e} fp16 {e16:.2e} bf16 {ebf:.2e}")
+    assert e32 < 1e-5
+    assert e16 < 2e-3
+    assert ebf < 3e-2
+
+
+def test_storage_roundtrip_fp16():
+    """Upload/download through the deviation codec is exact to fp16 rounding."""
+    rng = np.random.default_rng(5)
+    b = zf.gen_tube(16, 16, 8, 7.5, 7.5, 6.0, True)
+    ctx = make_ctx(b, zf.WALL_HALFWAY_BB, storage=zf.STORE_F16)
+    f0 = perturbed(ctx.n_listed, rng, amp=0.001)
+    ctx.upload_populations(f0)
+    f1 = ctx.download_populations()
+    dev = f0 / zf.W[:, None].astype(np.float32) - 1
+    err = np.abs(f1 - f0) / zf.W[:, None]
+    assert np.all(err <= np.abs(dev) * 2 ** -11 + 1e-8)

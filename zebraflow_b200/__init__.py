@@ -1,0 +1,239 @@
+"""zebraflow_b200 — B200-native Zebraflow coupled LBM-IB-RBC time step.
+
+The product is the C ABI of ``include/zf.h`` implemented by ``libzf.so``
+(hand-written sm_100a CUDA kernels plus C++ host setup).  This module is a
+thin ctypes mirror of that ABI for Python callers (tests, benchmarks); it
+does no numerics of its own and raises if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libzf.so")
+
+ZF_OK, ZF_ERR_CUDA, ZF_ERR_ARG, ZF_ERR_OVERFLOW, ZF_ERR_NONFINITE, ZF_ERR_STATE, ZF_ERR_NOMEM = range(7)
+WALL_HALFWAY_BB, WALL_REF_EQ = 0, 1
+STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
+Q = 19
+
+# D3Q19 in the reference order (ZebraflowWT.c:2471-2497); slot q = reference c-1.
+E = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
+              [1, 1, 0], [-1, -1, 0], [-1, 1, 0], [1, -1, 0], [1, 0, 1], [-1, 0, -1],
+              [-1, 0, 1], [1, 0, -1], [0, 1, 1], [0, -1, -1], [0, -1, 1], [0, 1, -1],
+              [0, 0, 0]], dtype=np.int32)
+W = np.array([1 / 18] * 6 + [1 / 36] * 12 + [1 / 3])
+
+
+class ZfError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"zf error {code}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("origin", C.c_double * 3), ("dx", C.c_double), ("dt", C.c_double),
+        ("tau", C.c_float), ("tau_from_phase", C.c_int32), ("g", C.c_float * 3),
+        ("wall_mode", C.c_int32), ("periodic", C.c_int32 * 3), ("storage", C.c_int32),
+        ("rho_ref", C.c_float), ("stagger", C.c_int32),
+        ("Es", C.c_double), ("Es_nucleus_ratio", C.c_double), ("kbend", C.c_double),
+        ("kd", C.c_double), ("ka", C.c_double), ("kv", C.c_double),
+        ("area0", C.c_double), ("volume0", C.c_double), ("kT", C.c_double),
+        ("e_ratio_eq", C.c_double), ("calib_passes", C.c_int32), ("gamma_p", C.c_double),
+        ("unit_mass", C.c_double), ("bforce_scale", C.c_double), ("vel_scale", C.c_double),
+        ("vmax_remove", C.c_double), ("remove_count", C.c_int32),
+        ("nuc_list_period", C.c_int32), ("nuc_list_max", C.c_int32),
+    ]
+
+
+class Status(C.Structure):
+    _fields_ = [("screened_terms", C.c_int64), ("cells_removed", C.c_int64),
+                ("list_overflows", C.c_int64), ("bc_no_neighbour", C.c_int64),
+                ("iter", C.c_int64)]
+
+
+_P = C.c_void_p
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "zf_params_default": (None, [C.POINTER(Params)]),
+    "zf_params_size": (C.c_size_t, []),
+    "zf_create": (_P, [C.POINTER(Params), C.c_int]),
+    "zf_destroy": (None, [_P]),
+    "zf_last_error": (C.c_char_p, []),
+    "zf_sync": (C.c_int, [_P]),
+    "zf_get_status": (C.c_int, [_P, C.POINTER(Status)]),
+    "zf_set_lattice": (C.c_int, [_P, _i32p]),
+    "zf_num_listed": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "zf_get_domlist": (C.c_int, [_P, _i32p]),
+    "zf_upload_populations": (C.c_int, [_P, _f32p]),
+    "zf_download_populations": (C.c_int, [_P, _f32p]),
+    "zf_upload_bodyforce": (C.c_int, [_P, _f32p]),
+    "zf_download_bodyforce": (C.c_int, [_P, _f32p]),
+    "zf_download_moments": (C.c_int, [_P, _f32p, _f32p, _f32p, _f32p]),
+    "zf_lbm_step": (C.c_int, [_P, C.c_int, C.c_int]),
+    "zf_lbm_steps": (C.c_int, [_P, C.c_int]),
+    "zf_lbm_step_mass": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "zf_set_uniform_force": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "zf_set_stream": (C.c_int, [_P, C.c_void_p]),
+    "zf_mass": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double)]),
+    "zf_lbm_steps_timed": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
+    "zf_device_bytes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "zf_gen_tube": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                              C.c_int, _i32p]),
+    "zf_gen_bifurcation": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                     C.c_double, _i32p, C.c_void_p]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libzf.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C zebraflow_b200/csrc`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        if L.zf_params_size() != C.sizeof(Params):
+            raise RuntimeError("zf_params layout mismatch between zf.h and the ctypes mirror")
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != ZF_OK:
+        raise ZfError(rc, lib().zf_last_error().decode(errors="replace"))
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    lib().zf_params_default(C.byref(p))
+    for k, v in kw.items():
+        if k in ("origin", "g", "periodic"):
+            arr = getattr(p, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def gen_tube(nx, ny, nz, cx, cy, R, periodic_z=True) -> np.ndarray:
+    b = np.empty(nx * ny * nz, np.int32)
+    _check(lib().zf_gen_tube(nx, ny, nz, cx, cy, R, int(periodic_z), b))
+    return b.reshape(nx, ny, nz)
+
+
+def gen_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg=20.0):
+    b = np.empty(nx * ny * nz, np.int32)
+    layout = (C.c_double * 6)()
+    _check(lib().zf_gen_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg, b,
+                                    C.cast(layout, C.c_void_p)))
+    return b.reshape(nx, ny, nz), list(layout)
+
+
+class Context:
+    """Owns one zf_ctx (one CUDA stream on one device)."""
+
+    def __init__(self, params: Params, device: int = 0):
+        self.params = params
+        self._h = lib().zf_create(C.byref(params), device)
+        if not self._h:
+            raise ZfError(ZF_ERR_CUDA, lib().zf_last_error().decode(errors="replace"))
+        self.n_listed = 0
+        self.n_fluid = 0
+
+    def close(self):
+        if self._h:
+            lib().zf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # lattice ---------------------------------------------------------------
+    def set_lattice(self, b_index: np.ndarray):
+        b = np.ascontiguousarray(b_index, np.int32).ravel()
+        _check(lib().zf_set_lattice(self._h, b))
+        nl, nf = C.c_int64(), C.c_int64()
+        _check(lib().zf_num_listed(self._h, C.byref(nl), C.byref(nf)))
+        self.n_listed, self.n_fluid = nl.value, nf.value
+
+    def domlist(self) -> np.ndarray:
+        out = np.empty(self.n_listed * 3, np.int32)
+        _check(lib().zf_get_domlist(self._h, out))
+        return out.reshape(-1, 3)
+
+    # fields ----------------------------------------------------------------
+    def upload_populations(self, f: np.ndarray):
+        _check(lib().zf_upload_populations(self._h, np.ascontiguousarray(f, np.float32).ravel()))
+
+    def download_populations(self) -> np.ndarray:
+        out = np.empty(Q * self.n_listed, np.float32)
+        _check(lib().zf_download_populations(self._h, out))
+        return out.reshape(Q, self.n_listed)
+
+    def upload_bodyforce(self, bf: np.ndarray):
+        _check(lib().zf_upload_bodyforce(self._h, np.ascontiguousarray(bf, np.float32).ravel()))
+
+    def download_bodyforce(self) -> np.ndarray:
+        out = np.empty(3 * self.n_listed, np.float32)
+        _check(lib().zf_download_bodyforce(self._h, out))
+        return out.reshape(3, self.n_listed)
+
+    def download_moments(self):
+        outs = [np.empty(self.n_listed, np.float32) for _ in range(4)]
+        _check(lib().zf_download_moments(self._h, *outs))
+        return outs
+
+    # steps -----------------------------------------------------------------
+    def lbm_step(self, store_moments=True, zero_bodyforce=False):
+        _check(lib().zf_lbm_step(self._h, int(store_moments), int(zero_bodyforce)))
+
+    def lbm_steps(self, n: int):
+        _check(lib().zf_lbm_steps(self._h, n))
+
+    def lbm_steps_timed(self, n: int) -> float:
+        ms = C.c_float()
+        _check(lib().zf_lbm_steps_timed(self._h, n, C.byref(ms)))
+        return ms.value
+
+    def mass(self, include_walls=False) -> float:
+        m = C.c_double()
+        _check(lib().zf_mass(self._h, int(include_walls), C.byref(m)))
+        return m.value
+
+    def sync(self):
+        _check(lib().zf_sync(self._h))
+
+    def status(self) -> Status:
+        s = Status()
+        _check(lib().zf_get_status(self._h, C.byref(s)))
+        return s
+
+    def device_bytes(self) -> int:
+        b = C.c_int64()
+        _check(lib().zf_device_bytes(self._h, C.byref(b)))
+        return b.value

@@ -1,0 +1,533 @@
+// Host side of the C ABI: context lifetime, parameters and the sparse tiled
+// lattice built from reference B_index codes.
+//
+// Reference behaviour restated here:
+//  - listed-node order: LBM_DOM_SETUP, ZebraflowWT.c:1481-1502
+//  - designated neighbour of each wall point: LBM_BC_SETUP, ZebraflowWT.c:1506-1589
+//  - initial state f = feq(rho, 0): ZebraflowWT.c:2562-2572, :5253-5295
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+
+#include "zf_internal.h"
+
+namespace {
+thread_local std::string g_last_error;
+
+// Reference lattice vectors, ZebraflowWT.c:2471-2497 (slot q = reference c-1).
+const int kE[ZF_Q][3] = {{1, 0, 0},  {-1, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0, 0, 1},
+                         {0, 0, -1}, {1, 1, 0},  {-1, -1, 0}, {-1, 1, 0}, {1, -1, 0},
+                         {1, 0, 1},  {-1, 0, -1}, {-1, 0, 1}, {1, 0, -1}, {0, 1, 1},
+                         {0, -1, -1}, {0, -1, 1}, {0, 1, -1}, {0, 0, 0}};
+}  // namespace
+
+namespace zf {
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+
+int dev_alloc(zf_ctx* c, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    *p = nullptr;
+    return e == cudaErrorMemoryAllocation ? ZF_ERR_NOMEM : ZF_ERR_CUDA;
+  }
+  c->device_bytes += (int64_t)bytes;
+  return ZF_OK;
+}
+}  // namespace zf
+
+using namespace zf;
+
+extern "C" {
+
+const char* zf_last_error(void) { return g_last_error.c_str(); }
+
+size_t zf_params_size(void) { return sizeof(zf_params); }
+
+void zf_params_default(zf_params* p) {
+  std::memset(p, 0, sizeof *p);
+  // ZebraflowWT.c:81-87 (ROI box) and :40-41 (DX, DT)
+  p->nx = 249;
+  p->ny = 547;
+  p->nz = 723;
+  p->origin[0] = -1.0;
+  p->origin[1] = 29.0;
+  p->origin[2] = -27.0;
+  p->dx = 0.5;
+  p->dt = 0.5;
+  // TauPlasma = 0.5 + MU_SCALE*MU = 1.22 (ZebraflowWT.c:62); phase-dependent (ZebraflowWT.c:6110)
+  p->tau = 1.22f;
+  p->tau_from_phase = 1;
+  p->wall_mode = ZF_WALL_REF_EQ;
+  p->storage = ZF_STORE_F32;
+  p->rho_ref = 1.0f;
+  p->stagger = 50;                 // SOLVERSTAGGER, ZebraflowWT.c:151
+  p->Es = 3.e-06;                  // ZebraflowWT.c:130
+  p->Es_nucleus_ratio = 0.1;       // ZebraflowWT.c:2039
+  p->kbend = 1.3856406e-19;        // ZebraflowWT.c:129
+  p->kd = 3.6e-05;                 // ZebraflowWT.c:131
+  p->ka = 7.7e-05;                 // ZebraflowWT.c:132
+  p->kv = 55.;                     // ZebraflowWT.c:133
+  p->area0 = 144.916e-012;         // RBC_SURF, ZebraflowWT.c:127
+  p->volume0 = 97.5671e-018;       // MCV, ZebraflowWT.c:126
+  p->kT = 300 * 1.3806488e-023;    // TEMPERATURE*BOLTZ, ZebraflowWT.c:36-37
+  p->e_ratio_eq = 0.3154574132;    // ZebraflowWT.c:134
+  p->calib_passes = 51;            // iterrelax loop, ZebraflowWT.c:2339-2346
+  p->gamma_p = 1.e-07;             // ZebraflowWT.c:125
+  p->unit_mass = 0.5e-6 * 0.5e-6 * 0.5e-6 * 10. * 1000.;  // UNITMASS, ZebraflowWT.c:50-51
+  p->bforce_scale = 1. / 3. * 0.5e-6 / (0.5e-6 * 0.5e-6);  // LBM_BFORCE_SCALE, ZebraflowWT.c:65
+  p->vel_scale = 1.0;              // VEL_SCALE, ZebraflowWT.c:67
+  p->vmax_remove = 5.e-3;          // ZebraflowWT.c:11976
+  p->remove_count = 500;           // ZebraflowWT.c:7473
+  p->nuc_list_period = 1000;       // ZebraflowWT.c:9527
+  p->nuc_list_max = 1004;          // NucMembMAX, ZebraflowWT.c:158
+}
+
+zf_ctx* zf_create(const zf_params* p, int device) {
+  if (!p) {
+    set_error("zf_create: params is NULL");
+    return nullptr;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    set_error("zf_create: no CUDA device (%s)", cudaGetErrorString(e));
+    return nullptr;
+  }
+  if (device < 0 || device >= ndev) {
+    set_error("zf_create: device %d out of range (%d devices)", device, ndev);
+    return nullptr;
+  }
+  if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->tau <= 0.5f || p->dx <= 0 ||
+      p->storage < 0 || p->storage > 2 || p->wall_mode < 0 || p->wall_mode > 1 ||
+      p->stagger <= 0) {
+    set_error("zf_create: invalid parameters (lattice %dx%dx%d, tau %g, storage %d, wall %d)",
+              p->nx, p->ny, p->nz, (double)p->tau, p->storage, p->wall_mode);
+    return nullptr;
+  }
+  for (int a = 0; a < 3; ++a) {
+    int n = a == 0 ? p->nx : (a == 1 ? p->ny : p->nz);
+    if (p->periodic[a] && (n % ZF_TS) != 0) {
+      set_error("zf_create: a periodic axis needs a length divisible by %d (axis %d has %d)",
+                ZF_TS, a, n);
+      return nullptr;
+    }
+  }
+  zf_ctx* c = new zf_ctx();
+  c->p = *p;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    set_error("zf_create: CUDA stream/event creation failed");
+    delete c;
+    return nullptr;
+  }
+  c->stream = c->own_stream;
+  return c;
+}
+
+static void free_lattice(zf_ctx* c) {
+  void* ptrs[] = {c->d_tile_map, c->d_active, c->d_nbr,   c->d_src_mask, c->d_fluid_mask,
+                  c->d_code,     c->d_f[0],   c->d_f[1],  c->d_force,    c->d_mom,
+                  c->d_rho_pre,  c->d_dom_slot, c->d_stage, c->d_wall_slot, c->d_wall_nbr,
+                  c->d_red};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  c->d_tile_map = c->d_active = c->d_nbr = nullptr;
+  c->d_src_mask = c->d_fluid_mask = nullptr;
+  c->d_code = nullptr;
+  c->d_f[0] = c->d_f[1] = nullptr;
+  c->d_force = c->d_mom = c->d_rho_pre = c->d_stage = nullptr;
+  c->d_dom_slot = c->d_wall_slot = c->d_wall_nbr = nullptr;
+  c->d_red = nullptr;
+  c->red_cap = 0;
+  c->device_bytes = 0;
+  c->lattice_set = false;
+}
+
+void zf_destroy(zf_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_lattice(c);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+}
+
+int zf_sync(zf_ctx* c) {
+  if (!c) return ZF_ERR_ARG;
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  return ZF_OK;
+}
+
+int zf_get_status(zf_ctx* c, zf_status* out) {
+  if (!c || !out) return ZF_ERR_ARG;
+  *out = c->status;
+  return ZF_OK;
+}
+
+int zf_device_bytes(zf_ctx* c, int64_t* bytes) {
+  if (!c || !bytes) return ZF_ERR_ARG;
+  *bytes = c->device_bytes;
+  return ZF_OK;
+}
+
+int zf_set_lattice(zf_ctx* c, const int32_t* b) {
+  if (!c || !b) return ZF_ERR_ARG;
+  ZF_CUDA(cudaSetDevice(c->device));
+  const zf_params& P = c->p;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const int64_t npts = (int64_t)nx * ny * nz;
+  for (int64_t n = 0; n < npts; ++n) {
+    if (b[n] >= 10) {
+      set_error("zf_set_lattice: B_index %d at linear index %lld is not supported "
+                "(pressure inlets >= 1000 and the deprecated 4998 are out of scope)",
+                b[n], (long long)n);
+      return ZF_ERR_ARG;
+    }
+  }
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  free_lattice(c);
+  c->b_index.assign(b, b + npts);
+
+  // Listed nodes in reference DOMLIST order (i outer, k inner), ZebraflowWT.c:1485-1499.
+  c->domlist.clear();
+  c->n_fluid = 0;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j)
+      for (int k = 0; k < nz; ++k) {
+        int32_t v = b[((int64_t)i * ny + j) * nz + k];
+        if (v >= 0) {
+          c->domlist.push_back(i);
+          c->domlist.push_back(j);
+          c->domlist.push_back(k);
+          if (v > 0) c->n_fluid++;
+        }
+      }
+  c->n_listed = (int64_t)c->domlist.size() / 3;
+
+  // Tiles holding populations: every tile with at least one listed point.
+  const int ntx = (nx + ZF_TS - 1) / ZF_TS, nty = (ny + ZF_TS - 1) / ZF_TS,
+            ntz = (nz + ZF_TS - 1) / ZF_TS;
+  c->ntx = ntx;
+  c->nty = nty;
+  c->ntz = ntz;
+  const int64_t ntiles_box = (int64_t)ntx * nty * ntz;
+  std::vector<uint8_t> has_listed(ntiles_box, 0), has_fluid(ntiles_box, 0);
+  for (int64_t l = 0; l < c->n_listed; ++l) {
+    int i = c->domlist[3 * l], j = c->domlist[3 * l + 1], k = c->domlist[3 * l + 2];
+    int64_t t = ((int64_t)(k / ZF_TS) * nty + j / ZF_TS) * ntx + i / ZF_TS;
+    has_listed[t] = 1;
+    if (b[((int64_t)i * ny + j) * nz + k] > 0) has_fluid[t] = 1;
+  }
+  c->h_tile_map.assign(ntiles_box, -1);
+  c->h_tile_origin.clear();
+  int64_t nt = 0;
+  std::vector<int32_t> active;
+  // tile ids follow (tz, ty, tx) order so that consecutive blocks touch neighbouring tiles
+  for (int64_t t = 0; t < ntiles_box; ++t) {
+    if (!has_listed[t]) continue;
+    c->h_tile_map[t] = (int32_t)nt;
+    int tx = (int)(t % ntx), ty = (int)((t / ntx) % nty), tz = (int)(t / ((int64_t)ntx * nty));
+    c->h_tile_origin.push_back(tx * ZF_TS);
+    c->h_tile_origin.push_back(ty * ZF_TS);
+    c->h_tile_origin.push_back(tz * ZF_TS);
+    if (has_fluid[t]) active.push_back((int32_t)nt);
+    ++nt;
+  }
+  if (nt > (int64_t)INT32_MAX / ZF_TC) {
+    set_error("zf_set_lattice: %lld tiles exceed the 32-bit slot index", (long long)nt);
+    return ZF_ERR_ARG;
+  }
+  c->n_pop_tiles = nt;
+  c->n_all_tiles = nt;
+  c->n_active = (int)active.size();
+  c->ns = nt * ZF_TC;
+  const int64_t ns = c->ns;
+
+  auto slot_of = [&](int i, int j, int k) -> int64_t {
+    int64_t t = ((int64_t)(k / ZF_TS) * nty + j / ZF_TS) * ntx + i / ZF_TS;
+    int32_t id = c->h_tile_map[t];
+    if (id < 0) return -1;
+    return (int64_t)id * ZF_TC + (i % ZF_TS) + ZF_TS * (j % ZF_TS) + ZF_TS * ZF_TS * (k % ZF_TS);
+  };
+
+  // Codes, masks and slots of listed nodes.
+  std::vector<uint8_t> code(ns, ZF_CODE_SOLID);
+  std::vector<uint64_t> fluid_mask(nt, 0), listed_mask(nt, 0);
+  std::vector<int32_t> dom_slot(c->n_listed);
+  for (int64_t l = 0; l < c->n_listed; ++l) {
+    int i = c->domlist[3 * l], j = c->domlist[3 * l + 1], k = c->domlist[3 * l + 2];
+    int32_t v = b[((int64_t)i * ny + j) * nz + k];
+    int64_t s = slot_of(i, j, k);
+    dom_slot[l] = (int32_t)s;
+    code[s] = v > 0 ? (uint8_t)v : (uint8_t)ZF_CODE_WALL;
+    int64_t t = s / ZF_TC;
+    int cell = (int)(s % ZF_TC);
+    listed_mask[t] |= 1ull << cell;
+    if (v > 0) fluid_mask[t] |= 1ull << cell;
+  }
+  // A pull may read from fluid points (bounce-back mode) or from every listed
+  // point (reference wall-equilibrium mode: wall points carry feq).
+  const std::vector<uint64_t>& src_mask = P.wall_mode == ZF_WALL_REF_EQ ? listed_mask : fluid_mask;
+
+  // 27-neighbour tile table with periodic wrap.
+  std::vector<int32_t> nbr(nt * 27, -1);
+  for (int64_t t = 0; t < nt; ++t) {
+    int tx = c->h_tile_origin[3 * t] / ZF_TS, ty = c->h_tile_origin[3 * t + 1] / ZF_TS,
+        tz = c->h_tile_origin[3 * t + 2] / ZF_TS;
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          int x = tx + dx, y = ty + dy, z = tz + dz;
+          if (P.periodic[0]) x = (x + ntx) % ntx;
+          if (P.periodic[1]) y = (y + nty) % nty;
+          if (P.periodic[2]) z = (z + ntz) % ntz;
+          int32_t id = -1;
+          if (x >= 0 && x < ntx && y >= 0 && y < nty && z >= 0 && z < ntz)
+            id = c->h_tile_map[((int64_t)z * nty + y) * ntx + x];
+          nbr[t * 27 + (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)] = id;
+        }
+  }
+
+  // Designated neighbour of each wall point, reference search order
+  // (fluid first over c=1..18, then wall), ZebraflowWT.c:1534-1578.
+  std::vector<int32_t> wall_slot, wall_nbr;
+  c->status.bc_no_neighbour = 0;
+  if (P.wall_mode == ZF_WALL_REF_EQ) {
+    auto code_at = [&](int i, int j, int k, int* ii, int* jj, int* kk) -> int32_t {
+      int n3[3] = {i, j, k}, lim[3] = {nx, ny, nz};
+      for (int a = 0; a < 3; ++a) {
+        if (n3[a] < 0 || n3[a] >= lim[a]) {
+          if (!P.periodic[a]) return INT32_MIN;
+          n3[a] = (n3[a] + lim[a]) % lim[a];
+        }
+      }
+      *ii = n3[0];
+      *jj = n3[1];
+      *kk = n3[2];
+      return b[((int64_t)n3[0] * ny + n3[1]) * nz + n3[2]];
+    };
+    for (int64_t l = 0; l < c->n_listed; ++l) {
+      int i = c->domlist[3 * l], j = c->domlist[3 * l + 1], k = c->domlist[3 * l + 2];
+      if (b[((int64_t)i * ny + j) * nz + k] != 0) continue;
+      int64_t found = -1;
+      for (int pass = 0; pass < 2 && found < 0; ++pass) {
+        for (int q = 0; q < ZF_Q - 1; ++q) {
+          int ii, jj, kk;
+          int32_t v = code_at(i + kE[q][0], j + kE[q][1], k + kE[q][2], &ii, &jj, &kk);
+          if (v == INT32_MIN) continue;
+          bool ok = pass == 0 ? (v > 0 && v < 1000) : (v == 0);
+          if (ok) {
+            found = slot_of(ii, jj, kk);
+            break;
+          }
+        }
+      }
+      if (found < 0) c->status.bc_no_neighbour++;
+      wall_slot.push_back(dom_slot[l]);
+      wall_nbr.push_back((int32_t)found);
+    }
+  }
+  c->n_wall = (int)wall_slot.size();
+
+  // Device allocation.
+  const size_t esz = P.storage == ZF_STORE_F32 ? 4 : 2;
+  int rc;
+#define ALLOC(ptr, bytes)                                         \
+  if ((rc = dev_alloc(c, (void**)&(ptr), (bytes))) != ZF_OK) { \
+    free_lattice(c);                                              \
+    return rc;                                                    \
+  }
+  ALLOC(c->d_tile_map, ntiles_box * sizeof(int32_t));
+  ALLOC(c->d_active, std::max<size_t>(active.size(), 1) * sizeof(int32_t));
+  ALLOC(c->d_nbr, nt * 27 * sizeof(int32_t));
+  ALLOC(c->d_src_mask, nt * sizeof(uint64_t));
+  ALLOC(c->d_fluid_mask, nt * sizeof(uint64_t));
+  ALLOC(c->d_code, ns);
+  ALLOC(c->d_f[0], (size_t)ZF_Q * ns * esz);
+  ALLOC(c->d_f[1], (size_t)ZF_Q * ns * esz);
+  ALLOC(c->d_force, 3 * ns * sizeof(float));
+  ALLOC(c->d_mom, 4 * ns * sizeof(float));
+  if (P.wall_mode == ZF_WALL_REF_EQ) {
+    ALLOC(c->d_rho_pre, ns * sizeof(float));
+    ALLOC(c->d_wall_slot, std::max(c->n_wall, 1) * sizeof(int32_t));
+    ALLOC(c->d_wall_nbr, std::max(c->n_wall, 1) * sizeof(int32_t));
+  }
+  ALLOC(c->d_dom_slot, std::max<int64_t>(c->n_listed, 1) * sizeof(int32_t));
+  ALLOC(c->d_stage, (size_t)ZF_Q * std::max<int64_t>(c->n_listed, 1) * sizeof(float));
+#undef ALLOC
+
+  cudaStream_t s = c->stream;
+  ZF_CUDA(cudaMemcpyAsync(c->d_tile_map, c->h_tile_map.data(), ntiles_box * sizeof(int32_t),
+                          cudaMemcpyHostToDevice, s));
+  if (!active.empty())
+    ZF_CUDA(cudaMemcpyAsync(c->d_active, active.data(), active.size() * sizeof(int32_t),
+                            cudaMemcpyHostToDevice, s));
+  ZF_CUDA(cudaMemcpyAsync(c->d_nbr, nbr.data(), nbr.size() * sizeof(int32_t),
+                          cudaMemcpyHostToDevice, s));
+  ZF_CUDA(cudaMemcpyAsync(c->d_src_mask, src_mask.data(), nt * sizeof(uint64_t),
+                          cudaMemcpyHostToDevice, s));
+  ZF_CUDA(cudaMemcpyAsync(c->d_fluid_mask, fluid_mask.data(), nt * sizeof(uint64_t),
+                          cudaMemcpyHostToDevice, s));
+  ZF_CUDA(cudaMemcpyAsync(c->d_code, code.data(), ns, cudaMemcpyHostToDevice, s));
+  if (c->n_listed)
+    ZF_CUDA(cudaMemcpyAsync(c->d_dom_slot, dom_slot.data(), c->n_listed * sizeof(int32_t),
+                            cudaMemcpyHostToDevice, s));
+  if (c->n_wall) {
+    ZF_CUDA(cudaMemcpyAsync(c->d_wall_slot, wall_slot.data(), c->n_wall * sizeof(int32_t),
+                            cudaMemcpyHostToDevice, s));
+    ZF_CUDA(cudaMemcpyAsync(c->d_wall_nbr, wall_nbr.data(), c->n_wall * sizeof(int32_t),
+                            cudaMemcpyHostToDevice, s));
+  }
+  ZF_CUDA(cudaMemsetAsync(c->d_force, 0, 3 * ns * sizeof(float), s));
+  c->cur = 0;
+  if ((rc = lbm_init_equilibrium(c)) != ZF_OK) return rc;
+  ZF_CUDA(cudaStreamSynchronize(s));  // host vectors above go out of scope
+  c->status.iter = 0;
+  c->lattice_set = true;
+  return ZF_OK;
+}
+
+int zf_num_listed(zf_ctx* c, int64_t* n_listed, int64_t* n_fluid) {
+  if (!c) return ZF_ERR_ARG;
+  if (!c->lattice_set) {
+    set_error("zf_num_listed: lattice not set");
+    return ZF_ERR_STATE;
+  }
+  if (n_listed) *n_listed = c->n_listed;
+  if (n_fluid) *n_fluid = c->n_fluid;
+  return ZF_OK;
+}
+
+int zf_get_domlist(zf_ctx* c, int32_t* ijk) {
+  if (!c || !ijk) return ZF_ERR_ARG;
+  if (!c->lattice_set) {
+    set_error("zf_get_domlist: lattice not set");
+    return ZF_ERR_STATE;
+  }
+  std::memcpy(ijk, c->domlist.data(), c->domlist.size() * sizeof(int32_t));
+  return ZF_OK;
+}
+
+#define NEED_LATTICE(fn)                           \
+  if (!c) return ZF_ERR_ARG;                       \
+  if (!c->lattice_set) {                           \
+    set_error(fn ": lattice not set");             \
+    return ZF_ERR_STATE;                           \
+  }                                                \
+  ZF_CUDA(cudaSetDevice(c->device));
+
+int zf_upload_populations(zf_ctx* c, const float* f) {
+  NEED_LATTICE("zf_upload_populations");
+  if (!f) return ZF_OK;
+  return lbm_upload_populations(c, f);
+}
+
+int zf_download_populations(zf_ctx* c, float* f) {
+  NEED_LATTICE("zf_download_populations");
+  if (!f) return ZF_ERR_ARG;
+  return lbm_download_populations(c, f);
+}
+
+int zf_upload_bodyforce(zf_ctx* c, const float* bf) {
+  NEED_LATTICE("zf_upload_bodyforce");
+  if (!bf) return ZF_ERR_ARG;
+  return lbm_scatter_listed(c, bf, 3, c->d_force);
+}
+
+int zf_download_bodyforce(zf_ctx* c, float* bf) {
+  NEED_LATTICE("zf_download_bodyforce");
+  if (!bf) return ZF_ERR_ARG;
+  return lbm_gather_listed(c, c->d_force, 3, bf);
+}
+
+int zf_download_moments(zf_ctx* c, float* D, float* U, float* V, float* W) {
+  NEED_LATTICE("zf_download_moments");
+  float* outs[4] = {D, U, V, W};
+  for (int a = 0; a < 4; ++a) {
+    if (!outs[a]) continue;
+    int rc = lbm_gather_listed(c, c->d_mom + (size_t)a * c->ns, 1, outs[a]);
+    if (rc) return rc;
+  }
+  return ZF_OK;
+}
+
+int zf_lbm_step(zf_ctx* c, int store_moments, int zero_bodyforce) {
+  NEED_LATTICE("zf_lbm_step");
+  int rc = lbm_launch(c, store_moments, zero_bodyforce);
+  if (rc == ZF_OK) c->status.iter++;
+  return rc;
+}
+
+int zf_lbm_steps(zf_ctx* c, int n) {
+  NEED_LATTICE("zf_lbm_steps");
+  for (int s = 0; s < n; ++s) {
+    int rc = lbm_launch(c, s == n - 1, 0);
+    if (rc) return rc;
+    c->status.iter++;
+  }
+  return ZF_OK;
+}
+
+int zf_lbm_steps_timed(zf_ctx* c, int n, float* ms) {
+  NEED_LATTICE("zf_lbm_steps_timed");
+  if (!ms || n <= 0) return ZF_ERR_ARG;
+  ZF_CUDA(cudaEventRecord(c->ev0, c->stream));
+  for (int s = 0; s < n; ++s) {
+    int rc = lbm_launch(c, 0, 0);
+    if (rc) return rc;
+    c->status.iter++;
+  }
+  ZF_CUDA(cudaEventRecord(c->ev1, c->stream));
+  ZF_CUDA(cudaEventSynchronize(c->ev1));
+  ZF_CUDA(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+  return ZF_OK;
+}
+
+int zf_lbm_step_mass(zf_ctx* c, int store_moments, int zero_bodyforce, double* mass) {
+  NEED_LATTICE("zf_lbm_step_mass");
+  if (!mass) return ZF_ERR_ARG;
+  int rc = lbm_launch(c, store_moments, zero_bodyforce, mass);
+  if (rc == ZF_OK) c->status.iter++;
+  return rc;
+}
+
+int zf_set_uniform_force(zf_ctx* c, const float* g3) {
+  if (!c || !g3) return ZF_ERR_ARG;
+  for (int a = 0; a < 3; ++a) c->p.g[a] = g3[a];
+  return ZF_OK;
+}
+
+int zf_set_stream(zf_ctx* c, void* s) {
+  if (!c) return ZF_ERR_ARG;
+  ZF_CUDA(cudaSetDevice(c->device));
+  cudaStream_t ns = s ? (cudaStream_t)s : c->own_stream;
+  if (ns != c->stream) {
+    // order new work after what is already queued on the previous stream
+    ZF_CUDA(cudaEventRecord(c->ev0, c->stream));
+    ZF_CUDA(cudaStreamWaitEvent(ns, c->ev0, 0));
+  }
+  c->stream = ns;
+  return ZF_OK;
+}
+
+int zf_mass(zf_ctx* c, int include_walls, double* mass) {
+  NEED_LATTICE("zf_mass");
+  if (!mass) return ZF_ERR_ARG;
+  return lbm_mass(c, include_walls, mass);
+}
+
+}  // extern "C"

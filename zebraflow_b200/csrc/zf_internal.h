@@ -1,0 +1,123 @@
+// Internal declarations shared by the host setup (zf_host.cpp) and the CUDA
+// kernels (zf_lbm.cu, zf_cells.cu).  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/zf.h"
+
+// Tile geometry of the sparse lattice: 4x4x4 lattice points, x fastest.
+#define ZF_TS 4
+#define ZF_TC 64
+
+// Cell codes stored per tile slot (uint8).
+enum : uint8_t {
+  ZF_CODE_SOLID = 0,   // not listed (reference B_index < 0)
+  // 1..9: fluid of that phase (reference B_index 1..9)
+  ZF_CODE_WALL = 10    // listed wall point (reference B_index == 0)
+};
+
+namespace zf {
+
+void set_error(const char* fmt, ...);
+
+#define ZF_CUDA(call)                                                          \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      ::zf::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),  \
+                      __FILE__, __LINE__);                                     \
+      return ZF_ERR_CUDA;                                                      \
+    }                                                                          \
+  } while (0)
+
+// Device-side view of the tiled lattice, passed by value to kernels.
+struct LatticeView {
+  int ntx, nty, ntz;          // tile grid
+  int nx, ny, nz;             // lattice box
+  int per_x, per_y, per_z;    // periodic flags
+  int64_t ns;                 // slots per population plane (= n_pop_tiles*64)
+  const int32_t* tile_map;    // [ntx*nty*ntz] tile id or -1 (all tiles)
+  const uint8_t* code;        // [n_all_tiles*64]
+};
+
+struct LbmArgs {
+  const void* fin;
+  void* fout;
+  const int32_t* active;      // tiles with >= 1 fluid point
+  int n_active;
+  const int32_t* nbr;         // [n_pop_tiles][27] neighbour tile ids (-1 none)
+  const uint64_t* src_mask;   // [n_pop_tiles] points a pull may read from
+  const uint64_t* fluid_mask; // [n_pop_tiles] fluid points
+  const uint8_t* code;        // [n_pop_tiles*64]
+  float* force;               // [3][ns] BODYFORCE (reference units)
+  float* mom;                 // [4][ns] D,U,V,W
+  float* rho_pre;             // [ns] pre-collision density (wall-equilibrium mode)
+  int64_t ns;
+  float tau;
+  float force_dt;             // multiplier of BODYFORCE in the Guo step (reference DT)
+  float gx, gy, gz;           // uniform effective force
+  float rho_ref, scale, inv_scale;
+  double* mass_partial;       // per-block FP64 density sums, or nullptr
+  int store_moments, zero_force, tau_from_phase, write_rho_pre;
+};
+
+}  // namespace zf
+
+struct zf_ctx {
+  zf_params p;
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream the context's work is queued on
+  cudaStream_t own_stream = nullptr;  // created by zf_create
+  bool lattice_set = false;
+
+  // listed nodes (reference DOMLIST order)
+  int64_t n_listed = 0, n_fluid = 0;
+  std::vector<int32_t> domlist;   // [n_listed][3]
+  std::vector<int32_t> b_index;   // dense copy of the input codes
+
+  // tiles
+  int ntx = 0, nty = 0, ntz = 0;
+  int64_t n_pop_tiles = 0, n_all_tiles = 0;
+  int n_active = 0;
+  std::vector<int32_t> h_tile_map;     // host copy
+  std::vector<int32_t> h_tile_origin;  // [n_all_tiles][3] tile coords
+  int64_t ns = 0;
+
+  int32_t* d_tile_map = nullptr;
+  int32_t* d_active = nullptr;
+  int32_t* d_nbr = nullptr;
+  uint64_t* d_src_mask = nullptr;
+  uint64_t* d_fluid_mask = nullptr;
+  uint8_t* d_code = nullptr;
+  void* d_f[2] = {nullptr, nullptr};
+  int cur = 0;
+  float* d_force = nullptr;
+  float* d_mom = nullptr;
+  float* d_rho_pre = nullptr;
+  int32_t* d_dom_slot = nullptr;  // [n_listed] slot of listed node l
+  float* d_stage = nullptr;       // [19*n_listed] upload/download staging
+  int32_t* d_wall_slot = nullptr; // REF mode wall points
+  int32_t* d_wall_nbr = nullptr;  // designated neighbour slot (-1 none)
+  int n_wall = 0;
+  double* d_red = nullptr;        // reduction scratch
+  int red_cap = 0;
+
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  zf_status status{};
+  int64_t device_bytes = 0;
+};
+
+namespace zf {
+int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out = nullptr);
+int lbm_upload_populations(zf_ctx* c, const float* f);
+int lbm_download_populations(zf_ctx* c, float* f);
+int lbm_init_equilibrium(zf_ctx* c);
+int lbm_scatter_listed(zf_ctx* c, const float* h, int planes, float* d_dst);
+int lbm_gather_listed(zf_ctx* c, const float* d_src, int planes, float* h);
+int lbm_mass(zf_ctx* c, int include_walls, double* out);
+int dev_alloc(zf_ctx* c, void** p, size_t bytes);
+}  // namespace zf
