@@ -41,8 +41,9 @@ WORKLOADS = {
     "bifurcation_x2_256x256x1024": (256, 256, 1024, 60.0, 44.0, 20.0, 2e-6),
     "bifurcation_small_128x96x256": (128, 96, 256, 15.0, 11.0, 20.0, 2e-6),
 }
-BYTES_PER_LUP = {0: 152, 1: 76, 2: 76}  # 2*19*S, S = bytes per stored population
-DTYPE_NAME = {0: "f32", 1: "f16-storage/f32-math", 2: "bf16-storage/f32-math"}
+BYTES_PER_LUP = {0: 152, 1: 76, 2: 76, 3: 152}  # 2*19*S, S = bytes per stored population
+DTYPE_NAME = {0: "f32", 1: "f16-storage/f32-math", 2: "bf16-storage/f32-math",
+              3: "f32-deviation-storage/f32-math"}
 
 
 def read_peaks():
@@ -217,7 +218,8 @@ def run_ours(args):
 
     b, dims, layout = build_geometry(args.workload)
     nx, ny, nz, Rp, Rd, ang, g = dims
-    storage = {"f32": zf.STORE_F32, "f16": zf.STORE_F16, "bf16": zf.STORE_BF16}[args.storage]
+    storage = {"f32": zf.STORE_F32, "f16": zf.STORE_F16, "bf16": zf.STORE_BF16,
+               "f32dev": zf.STORE_F32_DEV}[args.storage]
     p = zf.default_params(nx=nx, ny=ny, nz=nz, tau=0.9, tau_from_phase=0,
                           wall_mode=zf.WALL_HALFWAY_BB, periodic=(0, 0, 1), storage=storage,
                           g=(0.0, 0.0, g))
@@ -337,7 +339,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="bifurcation_256x256x1024", choices=sorted(WORKLOADS))
-    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f32dev"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()

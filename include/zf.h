@@ -56,9 +56,10 @@ enum zf_wall_mode {
 
 /* Storage type of the populations in HBM. */
 enum zf_storage {
-  ZF_STORE_F32 = 0,  /* plain fp32 populations */
-  ZF_STORE_F16 = 1,  /* fp16 of S*(f_q/w_q - rho_ref), arithmetic in fp32 */
-  ZF_STORE_BF16 = 2  /* bf16 of the same deviation */
+  ZF_STORE_F32 = 0,     /* plain fp32 populations f_q, as the reference stores F */
+  ZF_STORE_F16 = 1,     /* fp16 of S*(f_q/w_q - rho_ref), arithmetic in fp32 */
+  ZF_STORE_BF16 = 2,    /* bf16 of the same deviation */
+  ZF_STORE_F32_DEV = 3  /* fp32 of the deviation f_q/w_q - rho_ref */
 };
 
 /* Run-time parameters.  zf_params_default() fills the reference's values
@@ -100,6 +101,10 @@ typedef struct zf_params {
   int32_t remove_count;     /* screened-term count that removes a cell (500) */
   int32_t nuc_list_period;  /* nucleus-membrane list rebuild period in iterations (1000) */
   int32_t nuc_list_max;     /* capacity of each nucleus node's triangle list (NucMembMAX) */
+  int32_t stochastic_round; /* 16-bit storage forms: 1 = hardware stochastic rounding
+                               (cvt.rs, hashed random bits per point, step and direction),
+                               0 = round to nearest */
+  int32_t wall_list_max;    /* capacity of a wall node's triangle list (reference 12) */
 } zf_params;
 
 typedef struct zf_ctx zf_ctx;
@@ -196,6 +201,66 @@ int zf_lbm_steps_timed(zf_ctx* ctx, int n, float* ms);
 /* Bytes of device memory the context holds. */
 int zf_device_bytes(zf_ctx* ctx, int64_t* bytes);
 
+/* ---- membrane mesh and cells ---------------------------------------------- */
+
+/* Sets the membrane mesh shared by every cell and its nucleus mesh, with the
+ * rest shapes the springs are calibrated on (the reference reads them from
+ * ZFISHRBCNODES.dat / ZFISHRBCTRIANGLES.dat / NucleusNodes.dat /
+ * NucleusEdges.dat, ZebraflowWT.c:1601-1922).  tri: [n_tri][3] 1-based,
+ * counter-clockwise seen from outside; rest: [n_node][3] um; edge_n:
+ * [n_edge_n][2] 1-based; rest_n: [n_node_n][3] um.  Builds the edge/rhombus
+ * list in the reference's order (CGSM_ZFISHRBC_DATA_GEN, ZebraflowWT.c:1640-1805),
+ * calibrates WLC/POW springs (CGSM_FILAMENT_PARAMETERS, :1930-2053, iterated
+ * as :2339-2346), rest metrics (CGSM_EQUILIBRIUM_METRICS, :2056-2223) and rest
+ * triangle areas (:2387-2460).  Cells set before are dropped. */
+int zf_set_mesh(zf_ctx* ctx, int n_node, int n_tri, const int32_t* tri, const double* rest,
+                int n_node_n, int n_edge_n, const int32_t* edge_n, const double* rest_n);
+
+/* Number of membrane edges and the rest cell area (m^2) / volume (m^3) used
+ * by the global-area and volume constraints. */
+int zf_mesh_info(zf_ctx* ctx, int32_t* n_edge, double* area0, double* volume0);
+
+/* Edge list [n_edge][6] (n1,n2,n3,n4,tri1,tri2, 1-based: EDGENODE_LIST[edge][1..6],
+ * ZebraflowWT.c:224) and per edge the first-visitor flags of the area/volume
+ * terms (bit 0: tri1, bit 1: tri2; AREA_UPDATE, :7127-7128).  NULL skips. */
+int zf_get_edges(zf_ctx* ctx, int32_t* edges, uint8_t* area_first);
+
+/* Spring and rest parameters: epar [5][n_edge] = LMAX, Plength, kp,
+ * SINETHETA0, COSINETHETA0 (ZebraflowWT.c:228); epar_n [3][n_edge_n] =
+ * LMAX_N, Plength_N, kp_N (:235); tri_area_eq [n_tri] (TRI_AREA_eq, :220). */
+int zf_get_edge_params(zf_ctx* ctx, float* epar, float* epar_n, float* tri_area_eq);
+
+/* Places n_cells cells: x [3][n_cells][n_node] and xn [3][n_cells][n_node_n]
+ * in um (NODECOORD / NODECOORD_N layout, ZebraflowWT.c:225, :238).  All cells
+ * start independent (reference CellStatus 1). */
+int zf_set_cells(zf_ctx* ctx, int n_cells, const double* x, const double* xn);
+
+/* Positions (layouts as zf_set_cells) and status per cell (1 active,
+ * -5000 removed).  NULL skips. */
+int zf_get_cells(zf_ctx* ctx, double* x, double* xn, int32_t* status);
+
+/* F_Total [3][n_cells][n_node] and F_Total_N [3][n_cells][n_node_n] in N. */
+int zf_get_cell_forces(zf_ctx* ctx, float* ftot, float* ftot_n);
+
+/* NODE_VEL / NODE_VEL_N (um/us, fp64) and NODE_WALLREPUL / NODE_WALLREPUL_N
+ * (velocity increments) of the last membrane step. */
+int zf_get_cell_kinematics(zf_ctx* ctx, double* vel, double* vel_n, float* wrep, float* wrep_n);
+
+/* Geometry of the last membrane step: TRI_AREA [n_cells][n_tri] (m^2),
+ * TRI_NORMAL and TRI_CENTROID [3][n_cells][n_tri], NODE_NORMAL
+ * [3][n_cells][n_node], and per cell [n_cells][8]: area (m^2), volume (m^3),
+ * centroid (um, 3), F_AREA_GLOBAL, F_VOLUME_SCALAR, unused. */
+int zf_get_cell_geometry(zf_ctx* ctx, float* tri_area, float* tri_normal, float* tri_centroid,
+                         float* node_normal, float* cell_f);
+
+/* Membrane and nucleus forces of every cell (one CTA per cell): force
+ * reset (ZebraflowWT.c:5704-5745), triangle geometry and sliver repulsion
+ * (CGSM_AREA, :5749-6096), cell area and centroid (:6717-6796),
+ * CGSM_LOCAL_FORCES (:6800-7386), nucleus springs (:7388-7471), bad-cell
+ * removal (:7473-7501) and CGSM_VOLUME_CALC (:7510-7535).  Writes F_Total,
+ * F_Total_N and the geometry; clears node velocities and repulsions. */
+int zf_cgsm_forces(zf_ctx* ctx);
+
 /* ---- input generators (synthetic stand-ins for the reference's input files,
  *      FLUIDdomainBindex.csv read at ZebraflowWT.c:2574-2619) ---------------- */
 
@@ -210,6 +275,10 @@ int zf_gen_tube(int nx, int ny, int nz, double cx, double cy, double R, int peri
  * daughter offset. */
 int zf_gen_bifurcation(int nx, int ny, int nz, double Rp, double Rd, double half_angle_deg,
                        int32_t* b_index, double* layout);
+
+/* Unit icosphere subdivided `level` times: 10*4^level+2 nodes into xyz
+ * [n][3], 20*4^level triangles into tri [n][3] (1-based, outward winding). */
+int zf_gen_icosphere(int level, double* xyz, int32_t* tri);
 
 #ifdef __cplusplus
 }

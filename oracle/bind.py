@@ -43,6 +43,8 @@ def lib() -> C.CDLL:
             g("orc_lbm_step").argtypes = [C.c_void_p, C.c_int]
             g("orc_lbm_mass").restype = C.c_double
             g("orc_lbm_mass").argtypes = [C.c_void_p, C.c_int]
+            g("orc_lbm_set_storage_emulation").argtypes = [C.c_void_p, C.c_int, C.c_double,
+                                                           C.c_double]
             g("orc_lbm_time_steps").restype = C.c_double
             g("orc_lbm_time_steps").argtypes = [C.c_void_p, C.c_int]
         _lib = L
@@ -98,6 +100,12 @@ class OracleLBM:
 
     def step(self, rbc_flag=False):
         self._fn("orc_lbm_step")(self._h, int(rbc_flag))
+
+    def set_storage_emulation(self, mode, scale=65536.0, rho_ref=1.0):
+        """Rounds the stored populations after every step as a storage form
+        would: 0 none, 1 raw fp32, 2 fp32 deviation, 3 fp16 deviation,
+        4 bf16 deviation (deviation d = f/w - rho_ref, stored as scale*d)."""
+        self._fn("orc_lbm_set_storage_emulation")(self._h, int(mode), float(scale), float(rho_ref))
 
     def mass(self, include_walls=False):
         return float(self._fn("orc_lbm_mass")(self._h, int(include_walls)))

@@ -4,3 +4,4 @@
 #define REAL float
 #define SFX _f32
 #include "orc_lbm.inc"
+#include "orc_cells.inc"

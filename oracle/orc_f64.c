@@ -4,3 +4,4 @@
 #define REAL double
 #define SFX _f64
 #include "orc_lbm.inc"
+#include "orc_cells.inc"

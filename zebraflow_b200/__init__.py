@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(_HERE, "libzf.so")
 
 ZF_OK, ZF_ERR_CUDA, ZF_ERR_ARG, ZF_ERR_OVERFLOW, ZF_ERR_NONFINITE, ZF_ERR_STATE, ZF_ERR_NOMEM = range(7)
 WALL_HALFWAY_BB, WALL_REF_EQ = 0, 1
-STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
+STORE_F32, STORE_F16, STORE_BF16, STORE_F32_DEV = 0, 1, 2, 3
 Q = 19
 
 # D3Q19 in the reference order (ZebraflowWT.c:2471-2497); slot q = reference c-1.
@@ -48,6 +48,7 @@ class Params(C.Structure):
         ("unit_mass", C.c_double), ("bforce_scale", C.c_double), ("vel_scale", C.c_double),
         ("vmax_remove", C.c_double), ("remove_count", C.c_int32),
         ("nuc_list_period", C.c_int32), ("nuc_list_max", C.c_int32),
+        ("stochastic_round", C.c_int32), ("wall_list_max", C.c_int32),
     ]
 
 

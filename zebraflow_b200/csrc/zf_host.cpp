@@ -90,6 +90,10 @@ void zf_params_default(zf_params* p) {
   p->remove_count = 500;           // ZebraflowWT.c:7473
   p->nuc_list_period = 1000;       // ZebraflowWT.c:9527
   p->nuc_list_max = 1004;          // NucMembMAX, ZebraflowWT.c:158
+  p->stochastic_round = 1;
+  // WALLNODETOCELLNEIGHBORLIST holds 12 entries but its overflow check fires
+  // above 24 (ZebraflowWT.c:221, :3911-3934); 24 is the capacity here
+  p->wall_list_max = 24;
 }
 
 zf_ctx* zf_create(const zf_params* p, int device) {
@@ -108,7 +112,7 @@ zf_ctx* zf_create(const zf_params* p, int device) {
     return nullptr;
   }
   if (p->nx <= 0 || p->ny <= 0 || p->nz <= 0 || p->tau <= 0.5f || p->dx <= 0 ||
-      p->storage < 0 || p->storage > 2 || p->wall_mode < 0 || p->wall_mode > 1 ||
+      p->storage < 0 || p->storage > 3 || p->wall_mode < 0 || p->wall_mode > 1 ||
       p->stagger <= 0) {
     set_error("zf_create: invalid parameters (lattice %dx%dx%d, tau %g, storage %d, wall %d)",
               p->nx, p->ny, p->nz, (double)p->tau, p->storage, p->wall_mode);
@@ -137,14 +141,14 @@ zf_ctx* zf_create(const zf_params* p, int device) {
 }
 
 static void free_lattice(zf_ctx* c) {
-  void* ptrs[] = {c->d_tile_map, c->d_active, c->d_nbr,   c->d_src_mask, c->d_fluid_mask,
+  void* ptrs[] = {c->d_tile_map, c->d_active, c->d_nbr, c->d_link,
                   c->d_code,     c->d_f[0],   c->d_f[1],  c->d_force,    c->d_mom,
                   c->d_rho_pre,  c->d_dom_slot, c->d_stage, c->d_wall_slot, c->d_wall_nbr,
                   c->d_red};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   c->d_tile_map = c->d_active = c->d_nbr = nullptr;
-  c->d_src_mask = c->d_fluid_mask = nullptr;
+  c->d_link = nullptr;
   c->d_code = nullptr;
   c->d_f[0] = c->d_f[1] = nullptr;
   c->d_force = c->d_mom = c->d_rho_pre = c->d_stage = nullptr;
@@ -160,6 +164,7 @@ void zf_destroy(zf_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_lattice(c);
+  cells_free(c);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -175,6 +180,14 @@ int zf_sync(zf_ctx* c) {
 int zf_get_status(zf_ctx* c, zf_status* out) {
   if (!c || !out) return ZF_ERR_ARG;
   *out = c->status;
+  if (c->cells_set) {
+    unsigned long long cnt[4];
+    ZF_CUDA(cudaMemcpyAsync(cnt, c->cells.counters, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
+    ZF_CUDA(cudaStreamSynchronize(c->stream));
+    out->screened_terms = (int64_t)cnt[0];
+    out->cells_removed = (int64_t)cnt[1];
+    out->list_overflows = (int64_t)cnt[2];
+  }
   return ZF_OK;
 }
 
@@ -264,9 +277,8 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
     return (int64_t)id * ZF_TC + (i % ZF_TS) + ZF_TS * (j % ZF_TS) + ZF_TS * ZF_TS * (k % ZF_TS);
   };
 
-  // Codes, masks and slots of listed nodes.
+  // Codes and slots of listed nodes.
   std::vector<uint8_t> code(ns, ZF_CODE_SOLID);
-  std::vector<uint64_t> fluid_mask(nt, 0), listed_mask(nt, 0);
   std::vector<int32_t> dom_slot(c->n_listed);
   for (int64_t l = 0; l < c->n_listed; ++l) {
     int i = c->domlist[3 * l], j = c->domlist[3 * l + 1], k = c->domlist[3 * l + 2];
@@ -274,14 +286,34 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
     int64_t s = slot_of(i, j, k);
     dom_slot[l] = (int32_t)s;
     code[s] = v > 0 ? (uint8_t)v : (uint8_t)ZF_CODE_WALL;
-    int64_t t = s / ZF_TC;
-    int cell = (int)(s % ZF_TC);
-    listed_mask[t] |= 1ull << cell;
-    if (v > 0) fluid_mask[t] |= 1ull << cell;
   }
-  // A pull may read from fluid points (bounce-back mode) or from every listed
-  // point (reference wall-equilibrium mode: wall points carry feq).
-  const std::vector<uint64_t>& src_mask = P.wall_mode == ZF_WALL_REF_EQ ? listed_mask : fluid_mask;
+  // Link word of every fluid point: bit 31 marks the point live, bit q that the
+  // pull along q bounces back because its upstream point x - e_q is not a
+  // source.  Sources are fluid points (bounce-back mode) or every listed point
+  // (reference wall-equilibrium mode: wall points carry feq).
+  std::vector<uint32_t> link(ns, 0u);
+  const bool ref_eq = P.wall_mode == ZF_WALL_REF_EQ;
+  for (int64_t l = 0; l < c->n_listed; ++l) {
+    int i = c->domlist[3 * l], j = c->domlist[3 * l + 1], k = c->domlist[3 * l + 2];
+    if (b[((int64_t)i * ny + j) * nz + k] <= 0) continue;
+    uint32_t w = 1u << 31;
+    for (int q = 0; q < ZF_Q - 1; ++q) {
+      int p3[3] = {i - kE[q][0], j - kE[q][1], k - kE[q][2]}, lim[3] = {nx, ny, nz};
+      bool src = true;
+      for (int a = 0; a < 3; ++a) {
+        if (p3[a] < 0 || p3[a] >= lim[a]) {
+          if (!P.periodic[a]) src = false;
+          p3[a] = (p3[a] + lim[a]) % lim[a];
+        }
+      }
+      if (src) {
+        int32_t v = b[((int64_t)p3[0] * ny + p3[1]) * nz + p3[2]];
+        src = ref_eq ? v >= 0 : v > 0;
+      }
+      if (!src) w |= 1u << q;
+    }
+    link[dom_slot[l]] = w;
+  }
 
   // 27-neighbour tile table with periodic wrap.
   std::vector<int32_t> nbr(nt * 27, -1);
@@ -344,7 +376,8 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
   c->n_wall = (int)wall_slot.size();
 
   // Device allocation.
-  const size_t esz = P.storage == ZF_STORE_F32 ? 4 : 2;
+  // bytes per stored population: fp32 forms 4, fp16/bf16 deviations 2
+  const size_t esz = (P.storage == ZF_STORE_F16 || P.storage == ZF_STORE_BF16) ? 2 : 4;
   int rc;
 #define ALLOC(ptr, bytes)                                         \
   if ((rc = dev_alloc(c, (void**)&(ptr), (bytes))) != ZF_OK) { \
@@ -354,8 +387,7 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
   ALLOC(c->d_tile_map, ntiles_box * sizeof(int32_t));
   ALLOC(c->d_active, std::max<size_t>(active.size(), 1) * sizeof(int32_t));
   ALLOC(c->d_nbr, nt * 27 * sizeof(int32_t));
-  ALLOC(c->d_src_mask, nt * sizeof(uint64_t));
-  ALLOC(c->d_fluid_mask, nt * sizeof(uint64_t));
+  ALLOC(c->d_link, ns * sizeof(uint32_t));
   ALLOC(c->d_code, ns);
   ALLOC(c->d_f[0], (size_t)ZF_Q * ns * esz);
   ALLOC(c->d_f[1], (size_t)ZF_Q * ns * esz);
@@ -378,10 +410,8 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
                             cudaMemcpyHostToDevice, s));
   ZF_CUDA(cudaMemcpyAsync(c->d_nbr, nbr.data(), nbr.size() * sizeof(int32_t),
                           cudaMemcpyHostToDevice, s));
-  ZF_CUDA(cudaMemcpyAsync(c->d_src_mask, src_mask.data(), nt * sizeof(uint64_t),
-                          cudaMemcpyHostToDevice, s));
-  ZF_CUDA(cudaMemcpyAsync(c->d_fluid_mask, fluid_mask.data(), nt * sizeof(uint64_t),
-                          cudaMemcpyHostToDevice, s));
+  ZF_CUDA(cudaMemcpyAsync(c->d_link, link.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                          s));
   ZF_CUDA(cudaMemcpyAsync(c->d_code, code.data(), ns, cudaMemcpyHostToDevice, s));
   if (c->n_listed)
     ZF_CUDA(cudaMemcpyAsync(c->d_dom_slot, dom_slot.data(), c->n_listed * sizeof(int32_t),

@@ -50,8 +50,7 @@ struct LbmArgs {
   const int32_t* active;      // tiles with >= 1 fluid point
   int n_active;
   const int32_t* nbr;         // [n_pop_tiles][27] neighbour tile ids (-1 none)
-  const uint64_t* src_mask;   // [n_pop_tiles] points a pull may read from
-  const uint64_t* fluid_mask; // [n_pop_tiles] fluid points
+  const uint32_t* link;       // [ns] bit q: pull along q bounces back; bit 31: fluid point
   const uint8_t* code;        // [n_pop_tiles*64]
   float* force;               // [3][ns] BODYFORCE (reference units)
   float* mom;                 // [4][ns] D,U,V,W
@@ -62,8 +61,45 @@ struct LbmArgs {
   float gx, gy, gz;           // uniform effective force
   float rho_ref, scale, inv_scale;
   double* mass_partial;       // per-block FP64 density sums, or nullptr
-  int store_moments, zero_force, tau_from_phase, write_rho_pre;
+  uint32_t step;              // step counter (seeds the stochastic rounding)
+  int store_moments, zero_force, tau_from_phase, write_rho_pre, stochastic;
 };
+
+// Device view of the cells (membrane + nucleus meshes shared by every cell).
+// Layouts follow the reference: [3][cells][nodes] for vectors, [cells][n]
+// for scalars; positions and node velocities are FP64, the rest FP32.
+struct CellArgs {
+  int n_cells, nn, nt, ne, nnn, nen;
+  const int32_t* tri;        // [nt][3]
+  const int32_t* edge;       // [ne][6] n1 n2 n3 n4 tri1 tri2
+  const uint8_t* area_first; // [ne]
+  const float* epar;         // [5][ne] LMAX, Plength, kp, sin(theta0), cos(theta0)
+  const float* tri_area_eq;  // [nt]
+  const int32_t* edge_n;     // [nen][2]
+  const float* epar_n;       // [3][nen] LMAX, Plength, kp
+  double* x;                 // [3][nc][nn] um
+  double* xn;                // [3][nc][nnn]
+  double* vel;               // [3][nc][nn] um/us
+  double* vel_n;             // [3][nc][nnn]
+  float* ftot;               // [3][nc][nn] N
+  float* ftot_n;             // [3][nc][nnn]
+  float* wrep;               // [3][nc][nn] velocity increments (NODE_WALLREPUL)
+  float* wrep_n;             // [3][nc][nnn]
+  float* node_normal;        // [3][nc][nn]
+  float* tri_c;              // [3][nc][nt] um
+  float* tri_nrm;            // [3][nc][nt]
+  float* tri_a;              // [nc][nt] m^2
+  float* cell_f;             // [nc][8] area, volume, centroid xyz, F_area_global, F_vol_scalar
+  int32_t* status;           // [nc] 1 active, -5000 removed
+  int32_t* caps_remove;      // [nc]
+  unsigned long long* counters;  // [4] screened terms, cells removed, list overflows, spare
+  float kT, kbend, kd, ka, kv;
+  float area0, volume0;
+  int remove_count;
+};
+
+int cells_membrane_launch(zf_ctx* c);
+void cells_free(zf_ctx* c);
 
 }  // namespace zf
 
@@ -90,8 +126,7 @@ struct zf_ctx {
   int32_t* d_tile_map = nullptr;
   int32_t* d_active = nullptr;
   int32_t* d_nbr = nullptr;
-  uint64_t* d_src_mask = nullptr;
-  uint64_t* d_fluid_mask = nullptr;
+  uint32_t* d_link = nullptr;
   uint8_t* d_code = nullptr;
   void* d_f[2] = {nullptr, nullptr};
   int cur = 0;
@@ -109,10 +144,18 @@ struct zf_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   zf_status status{};
   int64_t device_bytes = 0;
+
+  // membrane mesh and cells
+  bool mesh_set = false, cells_set = false;
+  void* mesh_host = nullptr;       // zf::MeshHost*
+  zf::CellArgs cells{};            // device pointers + sizes
+  std::vector<void*> cell_allocs;  // device buffers owned for the cells
+  std::vector<void*> mesh_allocs;  // device buffers owned for the mesh
 };
 
 namespace zf {
 int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out = nullptr);
+int ensure_red(zf_ctx* c, int n);
 int lbm_upload_populations(zf_ctx* c, const float* f);
 int lbm_download_populations(zf_ctx* c, float* f);
 int lbm_init_equilibrium(zf_ctx* c);

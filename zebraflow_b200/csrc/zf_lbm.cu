@@ -10,8 +10,17 @@
 //
 // Layout in HBM: populations are SoA planes [19][ns] with ns = tiles*64; a
 // tile holds 4x4x4 lattice points, x fastest.  One thread updates one fluid
-// point; a 256-thread block covers 4 tiles.  The 27-neighbour tile table and
-// the per-tile source masks of a block's tiles are staged in shared memory.
+// point; a 256-thread block covers 4 tiles.  Per point a 32-bit link word
+// (bit q: the pull along q bounces back; bit 31: fluid point) replaces any
+// neighbour-code lookup; the 27-neighbour tile table of a block's tiles is
+// staged in shared memory.
+//
+// Arithmetic is done on deviations d_q = f_q/w_q - rho_ref in fp32 whatever
+// the storage form, so that the small body-force increments are not lost in
+// the rounding of O(0.05) populations.  Storage forms: plain fp32 f (as the
+// reference), fp32 deviations, and fp16 / bf16 deviations scaled by 2^16,
+// written with Blackwell's stochastic-rounding conversion (cvt.rs) from
+// hashed random bits, or with round-to-nearest.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -19,95 +28,118 @@
 
 namespace zf {
 
-__constant__ int c_ex[ZF_Q] = {1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0, 0};
-__constant__ int c_ey[ZF_Q] = {0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 0};
-__constant__ int c_ez[ZF_Q] = {0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0};
-// Weights: 1/18 for c=1..6, 1/36 for c=7..18, 1/3 for the rest population
-// (ZebraflowWT.c:72-74, :2329-2333).
-__constant__ float c_w[ZF_Q] = {1.f / 18, 1.f / 18, 1.f / 18, 1.f / 18, 1.f / 18, 1.f / 18,
-                                1.f / 36, 1.f / 36, 1.f / 36, 1.f / 36, 1.f / 36, 1.f / 36,
-                                1.f / 36, 1.f / 36, 1.f / 36, 1.f / 36, 1.f / 36, 1.f / 36,
-                                1.f / 3};
-__constant__ float c_iw[ZF_Q] = {18.f, 18.f, 18.f, 18.f, 18.f, 18.f, 36.f, 36.f, 36.f, 36.f,
-                                 36.f, 36.f, 36.f, 36.f, 36.f, 36.f, 36.f, 36.f, 3.f};
-
-__host__ __device__ __forceinline__ int opp(int q) {
-  // reference: cc = c-1 for even c, c+1 for odd c (ZebraflowWT.c:6114-6115), rest to itself
-  return q == 18 ? 18 : (q ^ 1);
+// D3Q19 in the reference order (ZebraflowWT.c:2471-2497), as compile-time
+// constants so that zero components and signs fold away after unrolling.
+__host__ __device__ constexpr int EX(int q) {
+  return (q == 0 || q == 6 || q == 9 || q == 10 || q == 13) ? 1
+         : (q == 1 || q == 7 || q == 8 || q == 11 || q == 12) ? -1 : 0;
 }
+__host__ __device__ constexpr int EY(int q) {
+  return (q == 2 || q == 6 || q == 8 || q == 14 || q == 17) ? 1
+         : (q == 3 || q == 7 || q == 9 || q == 15 || q == 16) ? -1 : 0;
+}
+__host__ __device__ constexpr int EZ(int q) {
+  return (q == 4 || q == 10 || q == 12 || q == 14 || q == 16) ? 1
+         : (q == 5 || q == 11 || q == 13 || q == 15 || q == 17) ? -1 : 0;
+}
+// weights 1/18, 1/36, 1/3 (ZebraflowWT.c:72-74, :2329-2333)
+__host__ __device__ constexpr float WQ(int q) {
+  return q < 6 ? 1.f / 18.f : (q < 18 ? 1.f / 36.f : 1.f / 3.f);
+}
+__host__ __device__ constexpr float IWQ(int q) { return q < 6 ? 18.f : (q < 18 ? 36.f : 3.f); }
+__host__ __device__ constexpr int OPP(int q) { return q == 18 ? 18 : (q ^ 1); }
 
-// Storage codecs: fp32 stores f; fp16/bf16 store S*(f/w - rho_ref).
-template <typename T>
-struct Codec;
-template <>
-struct Codec<float> {
-  __device__ __forceinline__ static float dec(float v, int, const LbmArgs&) { return v; }
-  __device__ __forceinline__ static float enc(float f, int, const LbmArgs&) { return f; }
+// ---- storage codecs: decode to / encode from the deviation d = f/w - rho_ref
+struct RawF32 {  // plain populations, as the reference keeps F
+  using T = float;
+  __device__ static float dec(T v, int q, const LbmArgs& a) { return v * IWQ(q) - a.rho_ref; }
+  __device__ static T enc(float d, int q, const LbmArgs& a) { return WQ(q) * (a.rho_ref + d); }
 };
-template <>
-struct Codec<__half> {
-  __device__ __forceinline__ static float dec(__half v, int q, const LbmArgs& a) {
-    return c_w[q] * (a.rho_ref + __half2float(v) * a.inv_scale);
-  }
-  __device__ __forceinline__ static __half enc(float f, int q, const LbmArgs& a) {
-    return __float2half_rn((f * c_iw[q] - a.rho_ref) * a.scale);
-  }
+struct DevF32 {
+  using T = float;
+  __device__ static float dec(T v, int, const LbmArgs&) { return v; }
+  __device__ static T enc(float d, int, const LbmArgs&) { return d; }
 };
-template <>
-struct Codec<__nv_bfloat16> {
-  __device__ __forceinline__ static float dec(__nv_bfloat16 v, int q, const LbmArgs& a) {
-    return c_w[q] * (a.rho_ref + __bfloat162float(v) * a.inv_scale);
-  }
-  __device__ __forceinline__ static __nv_bfloat16 enc(float f, int q, const LbmArgs& a) {
-    return __float2bfloat16_rn((f * c_iw[q] - a.rho_ref) * a.scale);
+struct DevF16 {
+  using T = __half;
+  __device__ static float dec(T v, int, const LbmArgs& a) { return __half2float(v) * a.inv_scale; }
+  __device__ static T enc(float d, int, const LbmArgs& a) { return __float2half_rn(d * a.scale); }
+  __device__ static T from_bits(unsigned short u) { return __ushort_as_half(u); }
+  // two values with stochastic rounding; lo -> low half, hi -> high half
+  __device__ static uint32_t enc2_sr(float lo, float hi, uint32_t rbits, const LbmArgs& a) {
+    uint32_t r;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(hi * a.scale), "f"(lo * a.scale), "r"(rbits));
+    return r;
   }
 };
+struct DevBF16 {
+  using T = __nv_bfloat16;
+  __device__ static float dec(T v, int, const LbmArgs& a) { return __bfloat162float(v) * a.inv_scale; }
+  __device__ static T enc(float d, int, const LbmArgs& a) { return __float2bfloat16_rn(d * a.scale); }
+  __device__ static T from_bits(unsigned short u) { return __ushort_as_bfloat16(u); }
+  __device__ static uint32_t enc2_sr(float lo, float hi, uint32_t rbits, const LbmArgs& a) {
+    uint32_t r;
+    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(hi * a.scale), "f"(lo * a.scale), "r"(rbits));
+    return r;
+  }
+};
+template <class C>
+struct IsHalf {
+  static constexpr bool v = sizeof(typename C::T) == 2;
+};
+
+__device__ __forceinline__ uint32_t mix32(uint32_t h) {
+  h ^= h >> 16;
+  h *= 0x7feb352du;
+  h ^= h >> 15;
+  h *= 0x846ca68bu;
+  h ^= h >> 16;
+  return h;
+}
 
 constexpr int kTilesPerBlock = 4;
 
-template <typename T>
+template <class C, typename I>
 __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
-  __shared__ int s_nbr[kTilesPerBlock][27];
-  __shared__ unsigned long long s_mask[kTilesPerBlock][27];
+  using T = typename C::T;
+  __shared__ I s_base[kTilesPerBlock][27];  // neighbour tile id * 64
   const int lt = threadIdx.x >> 6, cell = threadIdx.x & 63;
   const int tb = blockIdx.x * kTilesPerBlock;
   for (int t = threadIdx.x; t < kTilesPerBlock * 27; t += blockDim.x) {
     const int l = t / 27, s = t - l * 27;
     int nb = -1;
-    unsigned long long m = 0;
-    if (tb + l < a.n_active) {
-      const int tile = a.active[tb + l];
-      nb = a.nbr[(int64_t)tile * 27 + s];
-      if (nb >= 0) m = a.src_mask[nb];
-    }
-    s_nbr[l][s] = nb;
-    s_mask[l][s] = m;
+    if (tb + l < a.n_active) nb = a.nbr[(int64_t)a.active[tb + l] * 27 + s];
+    s_base[l][s] = nb >= 0 ? (I)nb * ZF_TC : (I)0;
   }
   __syncthreads();
   bool live = tb + lt < a.n_active;
-  const int tile = live ? s_nbr[lt][13] : 0;
-  live = live && ((a.fluid_mask[tile] >> cell) & 1ull);
+  const I self = live ? s_base[lt][13] + (I)cell : (I)0;
+  const uint32_t link = live ? a.link[self] : 0u;
+  live = live && (link >> 31);
   float rho = 0.f;
 
   if (live) {
     const int x = cell & 3, y = (cell >> 2) & 3, z = cell >> 4;
-    const int64_t self = (int64_t)tile * ZF_TC + cell;
-    const int64_t ns = a.ns;
+    const I ns = (I)a.ns;
     const T* __restrict__ fin = static_cast<const T*>(a.fin);
     T* __restrict__ fout = static_cast<T*>(a.fout);
 
-    float f[ZF_Q];
+    // pull from the upstream point x - e_q; halfway bounce-back where flagged
+    float d[ZF_Q];
 #pragma unroll
     for (int q = 0; q < ZF_Q; ++q) {
-      const int sx = x - c_ex[q], sy = y - c_ey[q], sz = z - c_ez[q];
-      const int slot27 = ((sz >> 2) + 1) * 9 + ((sy >> 2) + 1) * 3 + ((sx >> 2) + 1);
-      const int scell = (sx & 3) | ((sy & 3) << 2) | ((sz & 3) << 4);
-      const int nb = s_nbr[lt][slot27];
-      const bool ok = (s_mask[lt][slot27] >> scell) & 1ull;
-      // pull from the upstream point; halfway bounce-back when it is not a source
-      const int64_t idx = ok ? (int64_t)q * ns + (int64_t)nb * ZF_TC + scell
-                             : (int64_t)opp(q) * ns + self;
-      f[q] = Codec<T>::dec(fin[idx], q, a);
+      I idx;
+      if (q == 18) {
+        idx = (I)18 * ns + self;
+      } else {
+        const int sx = x - EX(q), sy = y - EY(q), sz = z - EZ(q);
+        const int s27 = ((sz >> 2) + 1) * 9 + ((sy >> 2) + 1) * 3 + ((sx >> 2) + 1);
+        const int scell = (sx & 3) | ((sy & 3) << 2) | ((sz & 3) << 4);
+        const I src = (I)q * ns + s_base[lt][s27] + (I)scell;
+        const I bb = (I)OPP(q) * ns + self;
+        idx = ((link >> q) & 1u) ? bb : src;
+      }
+      d[q] = C::dec(fin[idx], q, a);
     }
 
     float tau = a.tau;
@@ -125,47 +157,80 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
       }
     }
 
-    // moments with the half-force shift, ZebraflowWT.c:6125-6135
-    float mx = 0.f, my = 0.f, mz = 0.f;
+    // moments with the half-force shift, ZebraflowWT.c:6125-6135:
+    // rho = rho_ref + sum w d,  m = sum w c d  (sum w c = 0)
+    float drho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
 #pragma unroll
     for (int q = 0; q < ZF_Q; ++q) {
-      rho += f[q];
-      mx += f[q] * c_ex[q];
-      my += f[q] * c_ey[q];
-      mz += f[q] * c_ez[q];
+      const float wd = WQ(q) * d[q];
+      drho += wd;
+      if (EX(q)) mx += EX(q) * wd;
+      if (EY(q)) my += EY(q) * wd;
+      if (EZ(q)) mz += EZ(q) * wd;
     }
+    rho = a.rho_ref + drho;
     const float irho = 1.f / rho;
     const float ux = (mx + 0.5f * Fx) * irho, uy = (my + 0.5f * Fy) * irho,
                 uz = (mz + 0.5f * Fz) * irho;
     const float omega = 1.f / tau;
-    const float usq = ux * ux + uy * uy + uz * uz;
+    const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
     const float uF = ux * Fx + uy * Fy + uz * Fz;
     const float sfac = 1.f - 0.5f * omega;
 
-    // BGK + Guo source, ZebraflowWT.c:6138-6142
+    // BGK + Guo source in deviation form, ZebraflowWT.c:6138-6142:
+    // d' = d + omega (deq - d) + src/w,  deq = drho + rho (3cu + 4.5cu^2 - 1.5u^2)
     float r2 = 0.f, m2x = 0.f, m2y = 0.f, m2z = 0.f;
+    uint32_t rseed = 0;
+    if (IsHalf<C>::v) rseed = mix32((uint32_t)self * 0x9E3779B1u + a.step * 0x85EBCA77u);
+    float dn_prev = 0.f;
 #pragma unroll
     for (int q = 0; q < ZF_Q; ++q) {
-      const float cu = ux * c_ex[q] + uy * c_ey[q] + uz * c_ez[q];
-      const float cF = Fx * c_ex[q] + Fy * c_ey[q] + Fz * c_ez[q];
-      const float feq = rho * c_w[q] * (1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * usq);
-      const float src = sfac * c_w[q] * (3.f * (cF - uF) + 9.f * cu * cF);
-      const float fp = f[q] * (1.f - omega) + feq * omega + src;
-      const T v = Codec<T>::enc(fp, q, a);
-      fout[(int64_t)q * ns + self] = v;
+      const float cu = EX(q) * ux + EY(q) * uy + EZ(q) * uz;
+      const float cF = EX(q) * Fx + EY(q) * Fy + EZ(q) * Fz;
+      const float deq = drho + rho * (3.f * cu + 4.5f * cu * cu - usq15);
+      const float src = sfac * (3.f * (cF - uF) + 9.f * cu * cF);
+      const float dn = d[q] + omega * (deq - d[q]) + src;
+      float ds;  // the value the storage keeps
+      if constexpr (IsHalf<C>::v) {
+        if (a.stochastic && q < 18) {
+          if (q & 1) {  // pairs (q-1, q): one stochastic-rounding conversion
+            const uint32_t r = C::enc2_sr(dn_prev, dn, mix32(rseed + (uint32_t)q), a);
+            const T lo = C::from_bits((unsigned short)(r & 0xffffu));
+            const T hi = C::from_bits((unsigned short)(r >> 16));
+            fout[(I)(q - 1) * ns + self] = lo;
+            fout[(I)q * ns + self] = hi;
+            if (a.store_moments) {
+              const float d0 = C::dec(lo, q - 1, a), d1 = C::dec(hi, q, a);
+              r2 += WQ(q - 1) * d0 + WQ(q) * d1;
+              if (EX(q - 1)) m2x += EX(q - 1) * WQ(q - 1) * d0;
+              if (EY(q - 1)) m2y += EY(q - 1) * WQ(q - 1) * d0;
+              if (EZ(q - 1)) m2z += EZ(q - 1) * WQ(q - 1) * d0;
+              if (EX(q)) m2x += EX(q) * WQ(q) * d1;
+              if (EY(q)) m2y += EY(q) * WQ(q) * d1;
+              if (EZ(q)) m2z += EZ(q) * WQ(q) * d1;
+            }
+          } else {
+            dn_prev = dn;
+          }
+          continue;
+        }
+      }
+      const T v = C::enc(dn, q, a);
+      fout[(I)q * ns + self] = v;
       if (a.store_moments) {
-        const float fs = Codec<T>::dec(v, q, a);
-        r2 += fs;
-        m2x += fs * c_ex[q];
-        m2y += fs * c_ey[q];
-        m2z += fs * c_ez[q];
+        ds = C::dec(v, q, a);
+        r2 += WQ(q) * ds;
+        if (EX(q)) m2x += EX(q) * WQ(q) * ds;
+        if (EY(q)) m2y += EY(q) * WQ(q) * ds;
+        if (EZ(q)) m2z += EZ(q) * WQ(q) * ds;
       }
     }
     if (a.store_moments) {  // post-collision moments without force shift, ZebraflowWT.c:6611-6614
-      a.mom[self] = r2;
-      a.mom[ns + self] = m2x / r2;
-      a.mom[2 * ns + self] = m2y / r2;
-      a.mom[3 * ns + self] = m2z / r2;
+      const float D = a.rho_ref + r2;
+      a.mom[self] = D;
+      a.mom[ns + self] = m2x / D;
+      a.mom[2 * ns + self] = m2y / D;
+      a.mom[3 * ns + self] = m2z / D;
     }
     if (a.write_rho_pre) a.rho_pre[self] = rho;
   }
@@ -188,9 +253,10 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
 // Reference wall points: F[c][n] = feq(D[m], u=0) with m the designated
 // neighbour (ZebraflowWT.c:6303-6315, :6429-6432), then the moments pass for
 // those points (ZebraflowWT.c:6603-6616).
-template <typename T>
+template <class C>
 __global__ void k_lbm_wall(LbmArgs a, const int32_t* __restrict__ wall_slot,
                            const int32_t* __restrict__ wall_nbr, int n_wall) {
+  using T = typename C::T;
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= n_wall) return;
   const int64_t slot = wall_slot[w];
@@ -200,19 +266,20 @@ __global__ void k_lbm_wall(LbmArgs a, const int32_t* __restrict__ wall_slot,
   float r2 = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
 #pragma unroll
   for (int q = 0; q < ZF_Q; ++q) {
-    const T v = Codec<T>::enc(rho_m * c_w[q], q, a);
+    const T v = C::enc(rho_m - a.rho_ref, q, a);  // feq(rho, 0)/w - rho_ref
     fout[(int64_t)q * a.ns + slot] = v;
-    const float fs = Codec<T>::dec(v, q, a);
-    r2 += fs;
-    mx += fs * c_ex[q];
-    my += fs * c_ey[q];
-    mz += fs * c_ez[q];
+    const float ds = C::dec(v, q, a);
+    r2 += WQ(q) * ds;
+    mx += EX(q) * WQ(q) * ds;
+    my += EY(q) * WQ(q) * ds;
+    mz += EZ(q) * WQ(q) * ds;
   }
   if (a.store_moments) {
-    a.mom[slot] = r2;
-    a.mom[a.ns + slot] = mx / r2;
-    a.mom[2 * a.ns + slot] = my / r2;
-    a.mom[3 * a.ns + slot] = mz / r2;
+    const float D = a.rho_ref + r2;
+    a.mom[slot] = D;
+    a.mom[a.ns + slot] = mx / D;
+    a.mom[2 * a.ns + slot] = my / D;
+    a.mom[3 * a.ns + slot] = mz / D;
   }
   if (a.zero_force) {
     a.force[slot] = 0.f;
@@ -221,32 +288,33 @@ __global__ void k_lbm_wall(LbmArgs a, const int32_t* __restrict__ wall_slot,
   }
 }
 
-template <typename T>
-__global__ void k_fill_equilibrium(T* f, int64_t ns, LbmArgs a) {
+template <class C>
+__global__ void k_fill_equilibrium(typename C::T* f, int64_t ns, LbmArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
 #pragma unroll
-  for (int q = 0; q < ZF_Q; ++q) f[q * ns + s] = Codec<T>::enc(a.rho_ref * c_w[q], q, a);
+  for (int q = 0; q < ZF_Q; ++q) f[q * ns + s] = C::enc(0.f, q, a);
 }
 
-template <typename T>
-__global__ void k_scatter_pop(T* f, int64_t ns, const float* __restrict__ stage,
+template <class C>
+__global__ void k_scatter_pop(typename C::T* f, int64_t ns, const float* __restrict__ stage,
                               const int32_t* __restrict__ dom_slot, int64_t n, LbmArgs a) {
   const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= n) return;
   const int64_t s = dom_slot[l];
 #pragma unroll
-  for (int q = 0; q < ZF_Q; ++q) f[q * ns + s] = Codec<T>::enc(stage[q * n + l], q, a);
+  for (int q = 0; q < ZF_Q; ++q)
+    f[q * ns + s] = C::enc(stage[q * n + l] * IWQ(q) - a.rho_ref, q, a);
 }
 
-template <typename T>
-__global__ void k_gather_pop(const T* f, int64_t ns, float* __restrict__ stage,
+template <class C>
+__global__ void k_gather_pop(const typename C::T* f, int64_t ns, float* __restrict__ stage,
                              const int32_t* __restrict__ dom_slot, int64_t n, LbmArgs a) {
   const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= n) return;
   const int64_t s = dom_slot[l];
 #pragma unroll
-  for (int q = 0; q < ZF_Q; ++q) stage[q * n + l] = Codec<T>::dec(f[q * ns + s], q, a);
+  for (int q = 0; q < ZF_Q; ++q) stage[q * n + l] = WQ(q) * (a.rho_ref + C::dec(f[q * ns + s], q, a));
 }
 
 __global__ void k_scatter_planes(float* dst, int64_t ns, const float* __restrict__ stage,
@@ -267,18 +335,19 @@ __global__ void k_gather_planes(const float* src, int64_t ns, float* __restrict_
 
 // Global mass: per-block FP64 partial sums into scratch, then one block sums
 // the partials in a fixed order (deterministic).
-template <typename T>
-__global__ void k_mass_partial(const T* __restrict__ f, int64_t ns, const uint8_t* __restrict__ code,
-                               int include_walls, double* __restrict__ partial, LbmArgs a) {
+template <class C>
+__global__ void k_mass_partial(const typename C::T* __restrict__ f, int64_t ns,
+                               const uint8_t* __restrict__ code, int include_walls,
+                               double* __restrict__ partial, LbmArgs a) {
   double acc = 0.0;
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < ns;
        s += (int64_t)gridDim.x * blockDim.x) {
     const uint8_t cd = code[s];
     const bool take = (cd >= 1 && cd <= 9) || (include_walls && cd == ZF_CODE_WALL);
     if (!take) continue;
-    double r = 0.0;
+    double r = a.rho_ref;
 #pragma unroll
-    for (int q = 0; q < ZF_Q; ++q) r += (double)Codec<T>::dec(f[q * ns + s], q, a);
+    for (int q = 0; q < ZF_Q; ++q) r += (double)WQ(q) * (double)C::dec(f[q * ns + s], q, a);
     acc += r;
   }
   __shared__ double sh[256];
@@ -312,8 +381,7 @@ static LbmArgs make_args(zf_ctx* c) {
   a.active = c->d_active;
   a.n_active = c->n_active;
   a.nbr = c->d_nbr;
-  a.src_mask = c->d_src_mask;
-  a.fluid_mask = c->d_fluid_mask;
+  a.link = c->d_link;
   a.code = c->d_code;
   a.force = c->d_force;
   a.mom = c->d_mom;
@@ -325,28 +393,43 @@ static LbmArgs make_args(zf_ctx* c) {
   a.gy = P.g[1];
   a.gz = P.g[2];
   a.rho_ref = P.rho_ref;
-  // deviations (f/w - rho_ref) are O(1e-6..1e-2); 2^16 keeps them normal in fp16
-  a.scale = P.storage == ZF_STORE_F32 ? 1.f : 65536.f;
+  // deviations d are O(1e-6..1e-2); 2^16 keeps them in the normal fp16 range
+  const bool half = P.storage == ZF_STORE_F16 || P.storage == ZF_STORE_BF16;
+  a.scale = half ? 65536.f : 1.f;
   a.inv_scale = 1.f / a.scale;
+  a.stochastic = half && P.stochastic_round;
+  a.step = (uint32_t)c->status.iter;
   a.tau_from_phase = P.tau_from_phase;
   a.write_rho_pre = P.wall_mode == ZF_WALL_REF_EQ;
   return a;
 }
 
-template <typename T>
-static int launch_typed(zf_ctx* c, LbmArgs a) {
-  if (c->n_active > 0) {
-    const int grid = (c->n_active + kTilesPerBlock - 1) / kTilesPerBlock;
-    k_lbm<T><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a);
-    ZF_CUDA(cudaGetLastError());
+// Dispatch on the storage form.
+template <template <class> class K, typename... Args>
+static void dispatch_storage(int storage, Args&&... args) {
+  switch (storage) {
+    case ZF_STORE_F16: K<DevF16>::run(args...); break;
+    case ZF_STORE_BF16: K<DevBF16>::run(args...); break;
+    case ZF_STORE_F32_DEV: K<DevF32>::run(args...); break;
+    default: K<RawF32>::run(args...); break;
   }
-  if (c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0) {
-    k_lbm_wall<T><<<(c->n_wall + 255) / 256, 256, 0, c->stream>>>(a, c->d_wall_slot,
-                                                                   c->d_wall_nbr, c->n_wall);
-    ZF_CUDA(cudaGetLastError());
-  }
-  return ZF_OK;
 }
+
+template <class C>
+struct LaunchStep {
+  static void run(zf_ctx* c, const LbmArgs& a) {
+    if (c->n_active > 0) {
+      const int grid = (c->n_active + kTilesPerBlock - 1) / kTilesPerBlock;
+      if ((int64_t)ZF_Q * c->ns < (int64_t)INT32_MAX)
+        k_lbm<C, uint32_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a);
+      else
+        k_lbm<C, int64_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a);
+    }
+    if (c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0)
+      k_lbm_wall<C><<<(c->n_wall + 255) / 256, 256, 0, c->stream>>>(a, c->d_wall_slot,
+                                                                    c->d_wall_nbr, c->n_wall);
+  }
+};
 
 int ensure_red(zf_ctx* c, int n) {
   if (c->red_cap >= n) return ZF_OK;
@@ -369,13 +452,8 @@ int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out) {
     if (rc0) return rc0;
     a.mass_partial = c->d_red;
   }
-  int rc;
-  switch (c->p.storage) {
-    case ZF_STORE_F16: rc = launch_typed<__half>(c, a); break;
-    case ZF_STORE_BF16: rc = launch_typed<__nv_bfloat16>(c, a); break;
-    default: rc = launch_typed<float>(c, a); break;
-  }
-  if (rc != ZF_OK) return rc;
+  dispatch_storage<LaunchStep>(c->p.storage, c, a);
+  ZF_CUDA(cudaGetLastError());
   c->cur ^= 1;
   if (mass_out) {
     k_sum_partials<<<1, 256, 0, c->stream>>>(c->d_red, grid, c->d_red + grid);
@@ -387,21 +465,18 @@ int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out) {
   return ZF_OK;
 }
 
+template <class C>
+struct Fill {
+  static void run(zf_ctx* c, const LbmArgs& a, int b) {
+    k_fill_equilibrium<C><<<(int)((c->ns + 255) / 256), 256, 0, c->stream>>>(
+        (typename C::T*)c->d_f[b], c->ns, a);
+  }
+};
+
 int lbm_init_equilibrium(zf_ctx* c) {
   LbmArgs a = make_args(c);
-  const int grid = (int)((c->ns + 255) / 256);
   for (int b = 0; b < 2; ++b) {
-    switch (c->p.storage) {
-      case ZF_STORE_F16:
-        k_fill_equilibrium<__half><<<grid, 256, 0, c->stream>>>((__half*)c->d_f[b], c->ns, a);
-        break;
-      case ZF_STORE_BF16:
-        k_fill_equilibrium<__nv_bfloat16>
-            <<<grid, 256, 0, c->stream>>>((__nv_bfloat16*)c->d_f[b], c->ns, a);
-        break;
-      default:
-        k_fill_equilibrium<float><<<grid, 256, 0, c->stream>>>((float*)c->d_f[b], c->ns, a);
-    }
+    dispatch_storage<Fill>(c->p.storage, c, a, b);
     ZF_CUDA(cudaGetLastError());
   }
   // moments of the rest state: D = rho_ref, U = V = W = 0
@@ -417,26 +492,27 @@ int lbm_init_equilibrium(zf_ctx* c) {
   return ZF_OK;
 }
 
+template <class C>
+struct Scatter {
+  static void run(zf_ctx* c, const LbmArgs& a, int64_t n) {
+    k_scatter_pop<C><<<(int)((n + 255) / 256), 256, 0, c->stream>>>(
+        (typename C::T*)c->d_f[c->cur], c->ns, c->d_stage, c->d_dom_slot, n, a);
+  }
+};
+template <class C>
+struct Gather {
+  static void run(zf_ctx* c, const LbmArgs& a, int64_t n) {
+    k_gather_pop<C><<<(int)((n + 255) / 256), 256, 0, c->stream>>>(
+        (const typename C::T*)c->d_f[c->cur], c->ns, c->d_stage, c->d_dom_slot, n, a);
+  }
+};
+
 int lbm_upload_populations(zf_ctx* c, const float* h) {
   const int64_t n = c->n_listed;
   if (n == 0) return ZF_OK;
   ZF_CUDA(cudaMemcpyAsync(c->d_stage, h, (size_t)ZF_Q * n * sizeof(float),
                           cudaMemcpyHostToDevice, c->stream));
-  LbmArgs a = make_args(c);
-  const int grid = (int)((n + 255) / 256);
-  switch (c->p.storage) {
-    case ZF_STORE_F16:
-      k_scatter_pop<__half><<<grid, 256, 0, c->stream>>>((__half*)c->d_f[c->cur], c->ns,
-                                                         c->d_stage, c->d_dom_slot, n, a);
-      break;
-    case ZF_STORE_BF16:
-      k_scatter_pop<__nv_bfloat16><<<grid, 256, 0, c->stream>>>(
-          (__nv_bfloat16*)c->d_f[c->cur], c->ns, c->d_stage, c->d_dom_slot, n, a);
-      break;
-    default:
-      k_scatter_pop<float><<<grid, 256, 0, c->stream>>>((float*)c->d_f[c->cur], c->ns,
-                                                        c->d_stage, c->d_dom_slot, n, a);
-  }
+  dispatch_storage<Scatter>(c->p.storage, c, make_args(c), n);
   ZF_CUDA(cudaGetLastError());
   ZF_CUDA(cudaStreamSynchronize(c->stream));
   return ZF_OK;
@@ -445,21 +521,7 @@ int lbm_upload_populations(zf_ctx* c, const float* h) {
 int lbm_download_populations(zf_ctx* c, float* h) {
   const int64_t n = c->n_listed;
   if (n == 0) return ZF_OK;
-  LbmArgs a = make_args(c);
-  const int grid = (int)((n + 255) / 256);
-  switch (c->p.storage) {
-    case ZF_STORE_F16:
-      k_gather_pop<__half><<<grid, 256, 0, c->stream>>>((const __half*)c->d_f[c->cur], c->ns,
-                                                        c->d_stage, c->d_dom_slot, n, a);
-      break;
-    case ZF_STORE_BF16:
-      k_gather_pop<__nv_bfloat16><<<grid, 256, 0, c->stream>>>(
-          (const __nv_bfloat16*)c->d_f[c->cur], c->ns, c->d_stage, c->d_dom_slot, n, a);
-      break;
-    default:
-      k_gather_pop<float><<<grid, 256, 0, c->stream>>>((const float*)c->d_f[c->cur], c->ns,
-                                                       c->d_stage, c->d_dom_slot, n, a);
-  }
+  dispatch_storage<Gather>(c->p.storage, c, make_args(c), n);
   ZF_CUDA(cudaGetLastError());
   ZF_CUDA(cudaMemcpyAsync(h, c->d_stage, (size_t)ZF_Q * n * sizeof(float),
                           cudaMemcpyDeviceToHost, c->stream));
@@ -491,24 +553,19 @@ int lbm_gather_listed(zf_ctx* c, const float* d_src, int planes, float* h) {
   return ZF_OK;
 }
 
+template <class C>
+struct Mass {
+  static void run(zf_ctx* c, const LbmArgs& a, int nblk, int include_walls) {
+    k_mass_partial<C><<<nblk, 256, 0, c->stream>>>((const typename C::T*)c->d_f[c->cur], c->ns,
+                                                   c->d_code, include_walls, c->d_red, a);
+  }
+};
+
 int lbm_mass(zf_ctx* c, int include_walls, double* out) {
   const int nblk = 148 * 8;
   int rc0 = ensure_red(c, nblk + 1);
   if (rc0) return rc0;
-  LbmArgs a = make_args(c);
-  switch (c->p.storage) {
-    case ZF_STORE_F16:
-      k_mass_partial<__half><<<nblk, 256, 0, c->stream>>>(
-          (const __half*)c->d_f[c->cur], c->ns, c->d_code, include_walls, c->d_red, a);
-      break;
-    case ZF_STORE_BF16:
-      k_mass_partial<__nv_bfloat16><<<nblk, 256, 0, c->stream>>>(
-          (const __nv_bfloat16*)c->d_f[c->cur], c->ns, c->d_code, include_walls, c->d_red, a);
-      break;
-    default:
-      k_mass_partial<float><<<nblk, 256, 0, c->stream>>>(
-          (const float*)c->d_f[c->cur], c->ns, c->d_code, include_walls, c->d_red, a);
-  }
+  dispatch_storage<Mass>(c->p.storage, c, make_args(c), nblk, include_walls);
   ZF_CUDA(cudaGetLastError());
   k_sum_partials<<<1, 256, 0, c->stream>>>(c->d_red, nblk, c->d_red + nblk);
   ZF_CUDA(cudaGetLastError());
