@@ -92,7 +92,25 @@ _SIGS = {
                               C.c_int, _i32p]),
     "zf_gen_bifurcation": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                      C.c_double, _i32p, C.c_void_p]),
+    "zf_gen_icosphere": (C.c_int, [C.c_int, _f64p, _i32p]),
+    "zf_set_mesh": (C.c_int, [_P, C.c_int, C.c_int, _i32p, _f64p, C.c_int, C.c_int, _i32p, _f64p]),
+    "zf_mesh_info": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                               C.POINTER(C.c_double)]),
+    "zf_get_edges": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "zf_get_edge_params": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "zf_set_cells": (C.c_int, [_P, C.c_int, _f64p, C.c_void_p]),
+    "zf_get_cells": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "zf_get_cell_forces": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "zf_get_cell_kinematics": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "zf_get_cell_geometry": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
+    "zf_cgsm_forces": (C.c_int, [_P]),
 }
+
+
+def _ptr(a):
+    """Data pointer of a numpy array (or None)."""
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 _lib = None
 
@@ -144,6 +162,24 @@ def gen_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg=20.0):
     _check(lib().zf_gen_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg, b,
                                     C.cast(layout, C.c_void_p)))
     return b.reshape(nx, ny, nz), list(layout)
+
+
+def gen_icosphere(level: int):
+    """Unit icosphere: (xyz [n][3] float64, tri [m][3] int32 1-based)."""
+    n, m = 10 * 4 ** level + 2, 20 * 4 ** level
+    xyz = np.empty(3 * n)
+    tri = np.empty(3 * m, np.int32)
+    _check(lib().zf_gen_icosphere(level, xyz, tri))
+    return xyz.reshape(n, 3), tri.reshape(m, 3)
+
+
+def mesh_edges(tri1: np.ndarray) -> np.ndarray:
+    """Unique edges of a triangle mesh, 1-based [n][2] (nucleus edge list)."""
+    t = np.asarray(tri1) - 1
+    e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
+    e = np.sort(e, axis=1)
+    e = np.unique(e, axis=0)
+    return (e + 1).astype(np.int32)
 
 
 class Context:
@@ -233,6 +269,76 @@ class Context:
         s = Status()
         _check(lib().zf_get_status(self._h, C.byref(s)))
         return s
+
+    # membrane mesh and cells ---------------------------------------------
+    def set_mesh(self, rest, tri1, rest_n=None, edge_n1=None):
+        rest = np.ascontiguousarray(rest, np.float64).ravel()
+        tri1 = np.ascontiguousarray(tri1, np.int32).ravel()
+        rest_n = np.zeros(3) if rest_n is None else np.ascontiguousarray(rest_n, np.float64).ravel()
+        edge_n1 = (np.zeros(2, np.int32) if edge_n1 is None
+                   else np.ascontiguousarray(edge_n1, np.int32).ravel())
+        self.nn, self.nt = rest.size // 3, tri1.size // 3
+        self.nnn = 0 if rest_n.size == 3 and edge_n1.size == 2 and not edge_n1.any() else rest_n.size // 3
+        nen = 0 if self.nnn == 0 else edge_n1.size // 2
+        _check(lib().zf_set_mesh(self._h, self.nn, self.nt, tri1, rest, self.nnn, nen, edge_n1,
+                                 rest_n))
+        ne, a0, v0 = C.c_int32(), C.c_double(), C.c_double()
+        _check(lib().zf_mesh_info(self._h, C.byref(ne), C.byref(a0), C.byref(v0)))
+        self.ne, self.nen, self.area0, self.volume0 = ne.value, nen, a0.value, v0.value
+
+    def edges(self):
+        e = np.empty(6 * self.ne, np.int32)
+        af = np.empty(self.ne, np.uint8)
+        _check(lib().zf_get_edges(self._h, _ptr(e), _ptr(af)))
+        return e.reshape(self.ne, 6), af
+
+    def edge_params(self):
+        ep = np.empty(5 * self.ne, np.float32)
+        epn = np.empty(max(3 * self.nen, 1), np.float32)
+        ae = np.empty(self.nt, np.float32)
+        _check(lib().zf_get_edge_params(self._h, _ptr(ep), _ptr(epn), _ptr(ae)))
+        return ep.reshape(5, self.ne), epn[:3 * self.nen].reshape(3, self.nen), ae
+
+    def set_cells(self, x, xn=None):
+        """x: [3][n_cells][n_node] um; xn: [3][n_cells][n_node_n]."""
+        x = np.ascontiguousarray(x, np.float64)
+        self.nc = x.shape[1]
+        xn_ = None if xn is None else np.ascontiguousarray(xn, np.float64)
+        _check(lib().zf_set_cells(self._h, self.nc, x.ravel(), _ptr(xn_)))
+
+    def cells(self):
+        x = np.empty((3, self.nc, self.nn))
+        xn = np.empty((3, self.nc, self.nnn)) if self.nnn else None
+        st = np.empty(self.nc, np.int32)
+        _check(lib().zf_get_cells(self._h, _ptr(x), _ptr(xn), _ptr(st)))
+        return x, xn, st
+
+    def cell_forces(self):
+        f = np.empty((3, self.nc, self.nn), np.float32)
+        fn = np.empty((3, self.nc, self.nnn), np.float32) if self.nnn else None
+        _check(lib().zf_get_cell_forces(self._h, _ptr(f), _ptr(fn)))
+        return f, fn
+
+    def cell_kinematics(self):
+        v = np.empty((3, self.nc, self.nn))
+        vn = np.empty((3, self.nc, self.nnn)) if self.nnn else None
+        w = np.empty((3, self.nc, self.nn), np.float32)
+        wn = np.empty((3, self.nc, self.nnn), np.float32) if self.nnn else None
+        _check(lib().zf_get_cell_kinematics(self._h, _ptr(v), _ptr(vn), _ptr(w), _ptr(wn)))
+        return v, vn, w, wn
+
+    def cell_geometry(self):
+        ta = np.empty((self.nc, self.nt), np.float32)
+        tn = np.empty((3, self.nc, self.nt), np.float32)
+        tc = np.empty((3, self.nc, self.nt), np.float32)
+        nn_ = np.empty((3, self.nc, self.nn), np.float32)
+        cf = np.empty((self.nc, 8), np.float32)
+        _check(lib().zf_get_cell_geometry(self._h, _ptr(ta), _ptr(tn), _ptr(tc), _ptr(nn_),
+                                          _ptr(cf)))
+        return ta, tn, tc, nn_, cf
+
+    def cgsm_forces(self):
+        _check(lib().zf_cgsm_forces(self._h))
 
     def device_bytes(self) -> int:
         b = C.c_int64()
