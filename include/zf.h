@@ -182,6 +182,20 @@ int zf_lbm_steps(zf_ctx* ctx, int n);
  * (per-block partial sums, then a fixed-order sum), copied to *mass. */
 int zf_lbm_step_mass(zf_ctx* ctx, int store_moments, int zero_bodyforce, double* mass);
 
+/* No counterpart in the reference.  zf_lbm_step_mass for callers that cannot
+ * call cudaMalloc once their run has started (device memory owned by another
+ * allocator that has already reserved the GPU; loops that must not take
+ * cudaMalloc's implicit device synchronisation or an out-of-memory failure
+ * mid-run): it allocates nothing.  Its reduction scratch is a file-scope
+ * device array of 65,536 + 1 doubles (512 KB, held on every GPU that loads the
+ * library until exit), so it serves lattices of at most 65,536 blocks of four
+ * 4x4x4 tiles with fluid (262,144 tiles); larger ones get ZF_ERR_ARG with a
+ * message.  The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call overwrites the scratch, so nothing carries over between calls;
+ * calls that overlap on the GPU share the scratch and race. */
+int zf_lbm_step_mass_noalloc(zf_ctx* ctx, int store_moments, int zero_bodyforce, double* mass);
+
 /* Sets the uniform effective body force g (lattice units) used from the next step. */
 int zf_set_uniform_force(zf_ctx* ctx, const float* g3);
 

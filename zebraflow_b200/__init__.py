@@ -83,6 +83,7 @@ _SIGS = {
     "zf_lbm_step": (C.c_int, [_P, C.c_int, C.c_int]),
     "zf_lbm_steps": (C.c_int, [_P, C.c_int]),
     "zf_lbm_step_mass": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "zf_lbm_step_mass_noalloc": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "zf_set_uniform_force": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "zf_set_stream": (C.c_int, [_P, C.c_void_p]),
     "zf_mass": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double)]),

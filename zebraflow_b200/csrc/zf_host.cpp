@@ -535,6 +535,14 @@ int zf_lbm_step_mass(zf_ctx* c, int store_moments, int zero_bodyforce, double* m
   return rc;
 }
 
+int zf_lbm_step_mass_noalloc(zf_ctx* c, int store_moments, int zero_bodyforce, double* mass) {
+  NEED_LATTICE("zf_lbm_step_mass_noalloc");
+  if (!mass) return ZF_ERR_ARG;
+  int rc = lbm_step_mass_noalloc(c, store_moments, zero_bodyforce, mass);
+  if (rc == ZF_OK) c->status.iter++;
+  return rc;
+}
+
 int zf_set_uniform_force(zf_ctx* c, const float* g3) {
   if (!c || !g3) return ZF_ERR_ARG;
   for (int a = 0; a < 3; ++a) c->p.g[a] = g3[a];

@@ -156,6 +156,7 @@ struct zf_ctx {
 namespace zf {
 int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out = nullptr);
 int ensure_red(zf_ctx* c, int n);
+int lbm_step_mass_noalloc(zf_ctx* c, int store_moments, int zero_force, double* mass_out);
 int lbm_upload_populations(zf_ctx* c, const float* f);
 int lbm_download_populations(zf_ctx* c, float* f);
 int lbm_init_equilibrium(zf_ctx* c);

@@ -24,6 +24,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <mutex>
+
 #include "zf_internal.h"
 
 namespace zf {
@@ -570,6 +572,74 @@ int lbm_mass(zf_ctx* c, int include_walls, double* out) {
   k_sum_partials<<<1, 256, 0, c->stream>>>(c->d_red, nblk, c->d_red + nblk);
   ZF_CUDA(cudaGetLastError());
   ZF_CUDA(cudaMemcpyAsync(out, c->d_red + nblk, sizeof(double), cudaMemcpyDeviceToHost,
+                          c->stream));
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  return ZF_OK;
+}
+
+}  // namespace zf
+
+// ---- allocation-free step with the fused FP64 mass sum ----------------------
+//
+// Some callers cannot call cudaMalloc once their run has started: code whose
+// device memory is owned by another allocator that has already reserved the
+// GPU (a framework's caching allocator, a fixed memory budget), and time loops
+// that must not take cudaMalloc's implicit device synchronisation or risk an
+// out-of-memory failure half-way through a run.  For them the per-block
+// partial sums of the mass reduction live in this file-scope device array
+// instead of scratch memory from cudaMalloc.  Every GPU that loads the
+// library holds the array (512 KB) until the process exits.
+namespace zf {
+
+constexpr int kNoAllocMaxBlocks = 65536;  // partial sums: one per block of 4 tiles
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxBlocks + 1];
+
+// Device address of g_noalloc_scratch on `device`, looked up once per device
+// with that device current.  In host code the array's name is only a host-side
+// stand-in; kernels must be given this address instead.
+static int noalloc_scratch(int device, double** out) {
+  static std::mutex mu;
+  static double* addr[256] = {};
+  if (device < 0 || device >= 256) {
+    set_error("zf_lbm_step_mass_noalloc: device %d out of range", device);
+    return ZF_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    void* p = nullptr;
+    ZF_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    addr[device] = static_cast<double*>(p);
+  }
+  *out = addr[device];
+  return ZF_OK;
+}
+
+int lbm_step_mass_noalloc(zf_ctx* c, int store_moments, int zero_force, double* mass_out) {
+  const int grid = (c->n_active + kTilesPerBlock - 1) / kTilesPerBlock;
+  if (grid > kNoAllocMaxBlocks) {
+    set_error("zf_lbm_step_mass_noalloc: the lattice needs %d partial sums but the "
+              "allocation-free scratch holds %d (at most %d tiles of 4x4x4 points with fluid); "
+              "use zf_lbm_step_mass",
+              grid, kNoAllocMaxBlocks, kNoAllocMaxBlocks * kTilesPerBlock);
+    return ZF_ERR_ARG;
+  }
+  double* scratch = nullptr;
+  int rc = noalloc_scratch(c->device, &scratch);
+  if (rc) return rc;
+  // Every block of the step writes its own partial sum and the final sum
+  // overwrites scratch[grid]: nothing accumulates across calls, so nothing
+  // needs clearing.  Calls that overlap on the GPU (other streams, other
+  // contexts on the same device) share the array and race.
+  LbmArgs a = make_args(c);
+  a.store_moments = store_moments;
+  a.zero_force = zero_force;
+  a.mass_partial = scratch;
+  dispatch_storage<LaunchStep>(c->p.storage, c, a);
+  ZF_CUDA(cudaGetLastError());
+  c->cur ^= 1;
+  k_sum_partials<<<1, 256, 0, c->stream>>>(scratch, grid, scratch + grid);
+  ZF_CUDA(cudaGetLastError());
+  ZF_CUDA(cudaMemcpyAsync(mass_out, scratch + grid, sizeof(double), cudaMemcpyDeviceToHost,
                           c->stream));
   ZF_CUDA(cudaStreamSynchronize(c->stream));
   return ZF_OK;
