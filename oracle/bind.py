@@ -45,10 +45,100 @@ def lib() -> C.CDLL:
             g("orc_lbm_mass").argtypes = [C.c_void_p, C.c_int]
             g("orc_lbm_set_storage_emulation").argtypes = [C.c_void_p, C.c_int, C.c_double,
                                                            C.c_double]
+            g("orc_lbm_get_dom").argtypes = [C.c_void_p, _i32p, _i32p]
             g("orc_lbm_time_steps").restype = C.c_double
             g("orc_lbm_time_steps").argtypes = [C.c_void_p, C.c_int]
+            g("orc_cells_create").restype = C.c_void_p
+            g("orc_cells_create").argtypes = [C.c_int, C.c_int, _i32p, _f64p, C.c_int, C.c_int,
+                                              _i32p, _f64p, _f64p]
+            g("orc_cells_num_edges").restype = C.c_int
+            g("orc_cells_num_edges").argtypes = [C.c_void_p]
+            g("orc_cells_topology").argtypes = [C.c_void_p, _i32p, _f64p, _f64p, _f64p, _f64p]
+            g("orc_cells_set").argtypes = [C.c_void_p, C.c_int, _f64p, _f64p]
+            g("orc_cells_forces").argtypes = [C.c_void_p]
+            g("orc_cells_get").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+            g("orc_cells_geometry").argtypes = [C.c_void_p, _f64p, _f64p, _f64p, _f64p]
+            g("orc_cells_destroy").argtypes = [C.c_void_p]
         _lib = L
     return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class OracleCells:
+    """Reference membrane set-up and membrane step (ZebraflowWT.c:1592-2460,
+    :5704-7535) restated in C; see oracle/orc_cells.inc."""
+
+    def __init__(self, rest, tri1, rest_n, edge_n1, params, precision="f64"):
+        """params: a zebraflow_b200 Params (moduli, kT, e_ratio_eq, area0/volume0,
+        calibration passes, removal count are read from it)."""
+        self.sfx = "_f32" if precision == "f32" else "_f64"
+        self._fn = lambda n: getattr(lib(), n + self.sfx)  # noqa: E731
+        rest = np.ascontiguousarray(rest, np.float64).ravel()
+        tri1 = np.ascontiguousarray(tri1, np.int32).ravel()
+        rest_n = np.ascontiguousarray(rest_n, np.float64).ravel()
+        edge_n1 = np.ascontiguousarray(edge_n1, np.int32).ravel()
+        self.nn, self.nt = rest.size // 3, tri1.size // 3
+        self.nnn, self.nen = rest_n.size // 3, edge_n1.size // 2
+        P = params
+        par = np.array([P.Es, P.Es_nucleus_ratio, P.kbend, P.kd, P.ka, P.kv, P.kT, P.e_ratio_eq,
+                        P.area0, P.volume0, P.calib_passes, P.remove_count], np.float64)
+        self._h = self._fn("orc_cells_create")(self.nn, self.nt, tri1, rest, self.nnn, self.nen,
+                                                edge_n1, rest_n, par)
+        self.ne = int(self._fn("orc_cells_num_edges")(self._h))
+        self.nc = 0
+
+    def topology(self):
+        e = np.empty(6 * self.ne, np.int32)
+        ep = np.empty(5 * self.ne)
+        epn = np.empty(max(3 * self.nen, 1))
+        ae = np.empty(self.nt)
+        av = np.empty(2)
+        self._fn("orc_cells_topology")(self._h, e, ep, epn, ae, av)
+        return (e.reshape(self.ne, 6), ep.reshape(5, self.ne),
+                epn[:3 * self.nen].reshape(3, self.nen), ae, av)
+
+    def set_cells(self, x, xn):
+        x = np.ascontiguousarray(x, np.float64)
+        self.nc = x.shape[1]
+        self._fn("orc_cells_set")(self._h, self.nc, x.ravel(),
+                                  np.ascontiguousarray(xn, np.float64).ravel())
+
+    def forces(self):
+        self._fn("orc_cells_forces")(self._h)
+
+    def get(self):
+        x = np.empty((3, self.nc, self.nn))
+        xn = np.empty((3, self.nc, self.nnn))
+        f = np.empty((3, self.nc, self.nn))
+        fn = np.empty((3, self.nc, self.nnn))
+        cf = np.empty((self.nc, 8))
+        st = np.empty(self.nc, np.int32)
+        cnt = np.zeros(2, np.int64)
+        self._fn("orc_cells_get")(self._h, _p(x), _p(xn), _p(f), _p(fn), _p(cf), _p(st), _p(cnt))
+        return dict(x=x, xn=xn, ftot=f, ftot_n=fn, cell=cf, status=st, counters=cnt)
+
+    def geometry(self):
+        ta = np.empty((self.nc, self.nt))
+        tn = np.empty((3, self.nc, self.nt))
+        tc = np.empty((3, self.nc, self.nt))
+        nn_ = np.empty((3, self.nc, self.nn))
+        self._fn("orc_cells_geometry")(self._h, ta, tn, tc, nn_)
+        return ta, tn, tc, nn_
+
+    def close(self):
+        if self._h:
+            self._fn("orc_cells_destroy")(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class OracleLBM:
@@ -100,6 +190,13 @@ class OracleLBM:
 
     def step(self, rbc_flag=False):
         self._fn("orc_lbm_step")(self._h, int(rbc_flag))
+
+    def dom(self):
+        """(listed points [n][3] 0-based, designated neighbour per point or -1)."""
+        d = np.empty(3 * self.n, np.int32)
+        nb = np.empty(self.n, np.int32)
+        self._fn("orc_lbm_get_dom")(self._h, d, nb)
+        return d.reshape(self.n, 3), nb
 
     def set_storage_emulation(self, mode, scale=65536.0, rho_ref=1.0):
         """Rounds the stored populations after every step as a storage form

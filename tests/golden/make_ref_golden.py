@@ -1,0 +1,59 @@
+"""Builds tests/golden/ref_setup.npz from the reference's own set-up code.
+
+Runs oracle/ref/Makefile, which compiles the reference's ZebraflowWT.c where
+it lies (main renamed) with oracle/ref/harness_setup.c and runs its
+CGSM_ZFISHRBC_DATA_GEN / CGSM_FILAMENT_PARAMETERS / CGSM_EQUILIBRIUM_METRICS
+on the shipped RBC and nucleus meshes, and LBM_DOM_SETUP / LBM_BC_SETUP on a
+small synthetic lattice.  The fixture keeps the mesh inputs and the
+reference's outputs so that the pin runs where the reference tree is absent.
+
+Usage: python tests/golden/make_ref_golden.py [reference_dir]
+"""
+import gzip
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+
+
+def read_mesh(ref):
+    def rd(name, conv):
+        lines = gzip.open(os.path.join(ref, name), "rt").read().split("\n")[1:]
+        return np.array([conv(v) for ln in lines for v in ln.split()])
+    X = rd("ZFISHRBCNODES.dat.gz", float).reshape(-1, 3)
+    T = rd("ZFISHRBCTRIANGLES.dat.gz", int).reshape(-1, 3).astype(np.int32)
+    XN = rd("NucleusNodes.dat.gz", float).reshape(-1, 3)
+    EN = rd("NucleusEdges.dat.gz", int).reshape(-1, 2).astype(np.int32)
+    return X, T, XN, EN
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), f"REF={ref}"], check=True)
+    raw = open(os.path.join(ROOT, "oracle", "_ref", "ref_setup.bin"), "rb").read()
+    a = np.frombuffer(raw, np.int32)
+    f = np.frombuffer(raw, np.float32)
+    p = 0
+    ne = int(a[p]); p += 1
+    edges = a[p:p + 6 * ne].reshape(ne, 6).copy(); p += 6 * ne
+    epar = f[p:p + 5 * ne].reshape(5, ne).copy(); p += 5 * ne
+    nen = int(a[p]); p += 1
+    epar_n = f[p:p + 3 * nen].reshape(3, nen).copy(); p += 3 * nen
+    dommax = int(a[p]); p += 1
+    domlist = a[p:p + 3 * dommax].reshape(dommax, 3).copy(); p += 3 * dommax
+    bcmax = int(a[p]); p += 1
+    bc = a[p:p + 7 * bcmax].reshape(bcmax, 7).copy(); p += 7 * bcmax
+    assert p == a.size
+    X, T, XN, EN = read_mesh(ref)
+    np.savez_compressed(os.path.join(HERE, "ref_setup.npz"), mesh_x=X, mesh_tri=T, nuc_x=XN,
+                        nuc_edges=EN, edges=edges, epar=epar, epar_n=epar_n, domlist=domlist,
+                        bclist=bc[:, :4], bcnlist=bc[:, 4:])
+    print(f"edges {ne}, nucleus edges {nen}, listed points {dommax}, boundary points {bcmax}")
+
+
+if __name__ == "__main__":
+    main()
