@@ -275,6 +275,58 @@ int zf_get_cell_geometry(zf_ctx* ctx, float* tri_area, float* tri_normal, float*
  * F_Total_N and the geometry; clears node velocities and repulsions. */
 int zf_cgsm_forces(zf_ctx* ctx);
 
+/* ---- vessel wall and the IB coupling ------------------------------------ */
+
+/* Sets the lumen wall mesh: xyz [3][n_node_w] (um, WALLNODECOORD), tri
+ * [3][n_tri_w] 1-based node ids (WALLCELLNODE after its +1, ZebraflowWT.c:3840-3852),
+ * normals [3][n_tri_w] pointing into the lumen (WALLCELLNORMALS).  Builds the
+ * nearest-wall-node index of every lattice point within +-4 points of a wall
+ * node (W_index, :3715-3822), the node-to-triangle lists (:3899-3935, capacity
+ * zf_params.wall_list_max), triangle centroids (:4648-4663) and the void
+ * velocity of non-fluid points near the wall (:4788-4852). */
+int zf_set_wall(zf_ctx* ctx, int n_node_w, const float* xyz, int n_tri_w, const int32_t* tri,
+                const float* normals);
+
+/* W_index (1-based wall node, 0 none) and void velocity [3] of every lattice
+ * point as dense [nx][ny][nz] arrays (NULL skips). */
+int zf_get_wall_index(zf_ctx* ctx, int32_t* windex, float* uvoid);
+
+/* IB velocity interpolation of every membrane and nucleus node from the
+ * moments of the last LBM step run with store_moments=1, plus the nearest
+ * wall triangle search and wall repulsion (ZebraflowWT.c:8690-9142,
+ * :9149-9430).  Adds to NODE_VEL / NODE_VEL_N and NODE_WALLREPUL. */
+int zf_ibm_interp(zf_ctx* ctx);
+
+/* Nucleus-membrane repulsion (ZebraflowWT.c:9516-9730); rebuild_lists=1
+ * rebuilds every nucleus node's triangle list (the reference does so every
+ * 1000 iterations, :9527).  Adds to NODE_WALLREPUL. */
+int zf_nuc_memb_repulsion(zf_ctx* ctx, int rebuild_lists);
+
+/* Builds the triangle cell list (EulNeigh, ZebraflowWT.c:5857-5902) and adds
+ * the membrane-membrane repulsion to NODE_WALLREPUL (:9911-10053). */
+int zf_rbc_rbc_repulsion(zf_ctx* ctx);
+
+/* IB spreading of F_Total + gamma_p*NODE_WALLREPUL into BODYFORCE, after
+ * NODE_VEL += NODE_WALLREPUL (ZebraflowWT.c:10737-10870, :10874-10990). */
+int zf_ibm_spread(zf_ctx* ctx);
+
+/* x += NODE_VEL*DT*SOLVERSTAGGER for membrane and nucleus nodes; a cell
+ * with a node faster than vmax_remove (or not finite) is removed
+ * (ZebraflowWT.c:11965-12031). */
+int zf_update_positions(zf_ctx* ctx);
+
+/* nsteps iterations of the reference time loop (ZebraflowWT.c:5646-12190):
+ * every iteration an LBM step; every `stagger`-th iteration also the
+ * membrane forces, IB interpolation, repulsions, spreading and position
+ * update, in the reference's order. */
+int zf_step(zf_ctx* ctx, int nsteps);
+
+/* zf_step timed with CUDA events on the context stream (ms). */
+int zf_step_timed(zf_ctx* ctx, int nsteps, float* ms);
+
+/* Completed iterations (the reference's iter). */
+int zf_iteration(zf_ctx* ctx, int64_t* iter);
+
 /* ---- input generators (synthetic stand-ins for the reference's input files,
  *      FLUIDdomainBindex.csv read at ZebraflowWT.c:2574-2619) ---------------- */
 
@@ -293,6 +345,32 @@ int zf_gen_bifurcation(int nx, int ny, int nz, double Rp, double Rd, double half
 /* Unit icosphere subdivided `level` times: 10*4^level+2 nodes into xyz
  * [n][3], 20*4^level triangles into tri [n][3] (1-based, outward winding). */
 int zf_gen_icosphere(int level, double* xyz, int32_t* tri);
+
+/* Wall meshes of the generated vessels in the zf_set_wall layouts (um):
+ * a cylinder of radius R (lattice units) around lattice axis (cx, cy), rings
+ * every h lattice units with nseg segments; and the zero set of the
+ * bifurcation's signed distance by marching tetrahedra.  Normals point into
+ * the lumen.  With NULL outputs only n_node/n_tri are returned; otherwise the
+ * outputs must hold cap_node / cap_tri entries per component. */
+int zf_gen_wall_tube(double cx, double cy, double R, int nz, double h, int nseg,
+                     const double* origin, double dx, int* n_node, int* n_tri, float* xyz,
+                     int32_t* tri, float* nrm, int cap_node, int cap_tri);
+int zf_gen_wall_bifurcation(int nx, int ny, int nz, double Rp, double Rd, double half_angle_deg,
+                            const double* origin, double dx, int* n_node, int* n_tri, float* xyz,
+                            int32_t* tri, float* nrm, int cap_node, int cap_tri);
+
+/* Seeded cell placement (stand-in for the reference's cell start files,
+ * ZebraflowWT.c:5297-5637): centres uniform over the fluid points of b
+ * ([nx][ny][nz] B_index codes), orientations uniform, candidates rejected
+ * when their ellipsoid (semi-axes `axes` um + margin) overlaps a placed one
+ * or a membrane node comes within one lattice unit of a non-fluid point.
+ * rest [n_node][3] / rest_n [n_node_n][3] are the shapes (um) around their
+ * centres; x [3][n_cells][n_node], xn [3][n_cells][n_node_n] receive um;
+ * *placed the number placed (the first *placed cells are valid). */
+int zf_gen_cells(const int32_t* b, int nx, int ny, int nz, const double* origin, double dx,
+                 int periodic_z, int n_cells, int n_node, const double* rest, int n_node_n,
+                 const double* rest_n, const double* axes, double margin, uint64_t seed,
+                 double* x, double* xn, int* placed);
 
 #ifdef __cplusplus
 }

@@ -15,6 +15,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboracle.so")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _lib = None
 
 
@@ -60,6 +61,18 @@ def lib() -> C.CDLL:
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
             g("orc_cells_geometry").argtypes = [C.c_void_p, _f64p, _f64p, _f64p, _f64p]
             g("orc_cells_destroy").argtypes = [C.c_void_p]
+            g("orc_world_create").restype = C.c_void_p
+            g("orc_world_create").argtypes = [C.c_void_p, C.c_void_p, _f64p, C.c_double, _f64p]
+            g("orc_world_set_wall").argtypes = [C.c_void_p, C.c_int, _f32p, C.c_int, _i32p, _f32p,
+                                                C.c_int]
+            g("orc_world_get_wall").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+            for n in ("orc_world_interp", "orc_world_rbc_rbc", "orc_world_spread",
+                      "orc_world_update", "orc_world_destroy"):
+                g(n).argtypes = [C.c_void_p]
+            g("orc_world_nuc_memb").argtypes = [C.c_void_p, C.c_int]
+            g("orc_world_step").argtypes = [C.c_void_p, C.c_int]
+            g("orc_world_kinematics").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p]
         _lib = L
     return _lib
 
@@ -209,3 +222,71 @@ class OracleLBM:
 
     def time_steps(self, n):
         return float(self._fn("orc_lbm_time_steps")(self._h, int(n)))
+
+
+class OracleWorld:
+    """The reference IB coupling and time loop (ZebraflowWT.c:5646-12190) over an
+    OracleLBM and an OracleCells of the same precision; see oracle/orc_ib.inc."""
+
+    def __init__(self, lbm: OracleLBM, cells: OracleCells, params):
+        assert lbm.sfx == cells.sfx
+        self.lbm, self.cells, self.sfx = lbm, cells, lbm.sfx
+        self._fn = lambda n: getattr(lib(), n + self.sfx)  # noqa: E731
+        P = params
+        par = np.array([P.gamma_p, P.unit_mass, P.bforce_scale, P.vel_scale, P.dt, P.vmax_remove,
+                        P.stagger, P.nuc_list_period, P.nuc_list_max], np.float64)
+        self._h = self._fn("orc_world_create")(lbm._h, cells._h, np.asarray(P.origin[:], np.float64),
+                                               float(P.dx), par)
+        self.wall_cap = P.wall_list_max
+
+    def set_wall(self, xyz, tri, nrm):
+        xyz = np.ascontiguousarray(xyz, np.float32)
+        tri = np.ascontiguousarray(tri, np.int32)
+        nrm = np.ascontiguousarray(nrm, np.float32)
+        self._fn("orc_world_set_wall")(self._h, xyz.shape[1], xyz.ravel(), tri.shape[1], tri.ravel(),
+                                       nrm.ravel(), int(self.wall_cap))
+
+    def wall_index(self, shape):
+        n = int(np.prod(shape))
+        wi = np.empty(n, np.int32)
+        uv = np.empty(3 * n, np.float32)
+        self._fn("orc_world_get_wall")(self._h, _p(wi), _p(uv))
+        return wi.reshape(shape), uv.reshape((3,) + tuple(shape))
+
+    def interp(self):
+        self._fn("orc_world_interp")(self._h)
+
+    def nuc_memb(self, rebuild=False):
+        self._fn("orc_world_nuc_memb")(self._h, int(rebuild))
+
+    def rbc_rbc(self):
+        self._fn("orc_world_rbc_rbc")(self._h)
+
+    def spread(self):
+        self._fn("orc_world_spread")(self._h)
+
+    def update(self):
+        self._fn("orc_world_update")(self._h)
+
+    def step(self, n=1):
+        self._fn("orc_world_step")(self._h, int(n))
+
+    def kinematics(self):
+        c = self.cells
+        v = np.empty((3, c.nc, c.nn))
+        vn = np.empty((3, c.nc, c.nnn))
+        w = np.empty((3, c.nc, c.nn))
+        wn = np.empty((3, c.nc, c.nnn))
+        self._fn("orc_world_kinematics")(self._h, _p(v), _p(vn), _p(w), _p(wn))
+        return v, vn, w, wn
+
+    def close(self):
+        if self._h:
+            self._fn("orc_world_destroy")(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

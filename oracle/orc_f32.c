@@ -5,3 +5,4 @@
 #define SFX _f32
 #include "orc_lbm.inc"
 #include "orc_cells.inc"
+#include "orc_ib.inc"

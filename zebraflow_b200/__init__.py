@@ -106,6 +106,26 @@ _SIGS = {
     "zf_get_cell_geometry": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_void_p]),
     "zf_cgsm_forces": (C.c_int, [_P]),
+    "zf_set_wall": (C.c_int, [_P, C.c_int, _f32p, C.c_int, _i32p, _f32p]),
+    "zf_get_wall_index": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "zf_ibm_interp": (C.c_int, [_P]),
+    "zf_nuc_memb_repulsion": (C.c_int, [_P, C.c_int]),
+    "zf_rbc_rbc_repulsion": (C.c_int, [_P]),
+    "zf_ibm_spread": (C.c_int, [_P]),
+    "zf_update_positions": (C.c_int, [_P]),
+    "zf_step": (C.c_int, [_P, C.c_int]),
+    "zf_step_timed": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
+    "zf_iteration": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "zf_gen_wall_tube": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
+                                   _f64p, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "zf_gen_wall_bifurcation": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                          C.c_double, _f64p, C.c_double, C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_int, C.c_int]),
+    "zf_gen_cells": (C.c_int, [_i32p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, C.c_int,
+                               C.c_int, C.c_int, _f64p, C.c_int, _f64p, _f64p, C.c_double,
+                               C.c_uint64, _f64p, _f64p, C.POINTER(C.c_int)]),
 }
 
 
@@ -172,6 +192,51 @@ def gen_icosphere(level: int):
     tri = np.empty(3 * m, np.int32)
     _check(lib().zf_gen_icosphere(level, xyz, tri))
     return xyz.reshape(n, 3), tri.reshape(m, 3)
+
+
+def _wall_out(fn, *args):
+    nn_, nt_ = C.c_int(), C.c_int()
+    _check(fn(*args, C.byref(nn_), C.byref(nt_), None, None, None, 0, 0))
+    xyz = np.empty(3 * nn_.value, np.float32)
+    tri = np.empty(3 * nt_.value, np.int32)
+    nrm = np.empty(3 * nt_.value, np.float32)
+    _check(fn(*args, C.byref(nn_), C.byref(nt_), _ptr(xyz), _ptr(tri), _ptr(nrm), nn_.value,
+              nt_.value))
+    return xyz.reshape(3, -1), tri.reshape(3, -1), nrm.reshape(3, -1)
+
+
+def gen_wall_tube(cx, cy, R, nz, origin=(0.0, 0.0, 0.0), dx=0.5, h=1.0, nseg=None):
+    """Cylinder wall mesh in um: (xyz [3][n], tri [3][m] 1-based, normals [3][m])."""
+    if nseg is None:
+        nseg = max(12, int(round(2 * np.pi * R / h)))
+    return _wall_out(lib().zf_gen_wall_tube, cx, cy, R, nz, h, nseg,
+                     np.asarray(origin, np.float64), dx)
+
+
+def gen_wall_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg=20.0, origin=(0.0, 0.0, 0.0), dx=0.5):
+    return _wall_out(lib().zf_gen_wall_bifurcation, nx, ny, nz, Rp, Rd, half_angle_deg,
+                     np.asarray(origin, np.float64), dx)
+
+
+def gen_cells(b, n_cells, rest, rest_n, axes, seed=1234, origin=(0.0, 0.0, 0.0), dx=0.5,
+              periodic_z=True, margin=0.25):
+    """Seeded placement; returns (x [3][placed][n_node], xn [3][placed][n_node_n])."""
+    b = np.ascontiguousarray(b, np.int32)
+    nx, ny, nz = b.shape
+    rest = np.ascontiguousarray(rest, np.float64)
+    rest_n = np.ascontiguousarray(rest_n, np.float64)
+    nn_, nnn = rest.shape[0], rest_n.shape[0]
+    x = np.zeros(3 * n_cells * nn_)
+    xn = np.zeros(max(3 * n_cells * nnn, 1))
+    placed = C.c_int()
+    _check(lib().zf_gen_cells(b.ravel(), nx, ny, nz, np.asarray(origin, np.float64), dx,
+                              int(periodic_z), n_cells, nn_, rest.ravel(), nnn, rest_n.ravel(),
+                              np.asarray(axes, np.float64), margin, seed, x, xn,
+                              C.byref(placed)))
+    k = placed.value
+    x = x.reshape(3, n_cells, nn_)[:, :k, :].copy()
+    xn = xn[:3 * n_cells * nnn].reshape(3, n_cells, nnn)[:, :k, :].copy()
+    return x, xn
 
 
 def mesh_edges(tri1: np.ndarray) -> np.ndarray:
@@ -340,6 +405,50 @@ class Context:
 
     def cgsm_forces(self):
         _check(lib().zf_cgsm_forces(self._h))
+
+    # wall and IB coupling ---------------------------------------------------
+    def set_wall(self, xyz, tri, nrm):
+        xyz = np.ascontiguousarray(xyz, np.float32)
+        tri = np.ascontiguousarray(tri, np.int32)
+        nrm = np.ascontiguousarray(nrm, np.float32)
+        _check(lib().zf_set_wall(self._h, xyz.shape[1], xyz.ravel(), tri.shape[1], tri.ravel(),
+                                 nrm.ravel()))
+
+    def wall_index(self):
+        p = self.params
+        n = p.nx * p.ny * p.nz
+        wi = np.empty(n, np.int32)
+        uv = np.empty(3 * n, np.float32)
+        _check(lib().zf_get_wall_index(self._h, _ptr(wi), _ptr(uv)))
+        return wi.reshape(p.nx, p.ny, p.nz), uv.reshape(3, p.nx, p.ny, p.nz)
+
+    def ibm_interp(self):
+        _check(lib().zf_ibm_interp(self._h))
+
+    def nuc_memb_repulsion(self, rebuild=False):
+        _check(lib().zf_nuc_memb_repulsion(self._h, int(rebuild)))
+
+    def rbc_rbc_repulsion(self):
+        _check(lib().zf_rbc_rbc_repulsion(self._h))
+
+    def ibm_spread(self):
+        _check(lib().zf_ibm_spread(self._h))
+
+    def update_positions(self):
+        _check(lib().zf_update_positions(self._h))
+
+    def step(self, n=1):
+        _check(lib().zf_step(self._h, n))
+
+    def step_timed(self, n):
+        ms = C.c_float()
+        _check(lib().zf_step_timed(self._h, n, C.byref(ms)))
+        return ms.value
+
+    def iteration(self):
+        it = C.c_int64()
+        _check(lib().zf_iteration(self._h, C.byref(it)))
+        return it.value
 
     def device_bytes(self) -> int:
         b = C.c_int64()

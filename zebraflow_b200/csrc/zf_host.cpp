@@ -163,6 +163,7 @@ void zf_destroy(zf_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  ib_free(c);
   free_lattice(c);
   cells_free(c);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -212,6 +213,7 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
     }
   }
   ZF_CUDA(cudaStreamSynchronize(c->stream));
+  ib_free(c);  // the wall and IB views belong to the previous lattice
   free_lattice(c);
   c->b_index.assign(b, b + npts);
 
@@ -428,7 +430,7 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
   ZF_CUDA(cudaStreamSynchronize(s));  // host vectors above go out of scope
   c->status.iter = 0;
   c->lattice_set = true;
-  return ZF_OK;
+  return ib_prepare(c);
 }
 
 int zf_num_listed(zf_ctx* c, int64_t* n_listed, int64_t* n_fluid) {

@@ -1,0 +1,688 @@
+// Immersed-boundary coupling and cell interactions, one membrane step.
+//
+//   k_ib_interp     velocity interpolation (Peskin cosine delta, spherical
+//                   support of 2 lattice units, not renormalised) of the fluid
+//                   velocity, or of the void velocity at non-fluid points near
+//                   the wall, plus nearest-wall-triangle search and wall
+//                   repulsion                       ZebraflowWT.c:8690-9142, :9149-9430
+//   k_bin_*         cell list: each triangle centroid binned to its nearest
+//                   listed lattice point within 1 um (the reference's Eulerian
+//                   lists EulNeigh, :5857-5902), as a CSR over lattice slots
+//   k_nuc_memb      nucleus-membrane repulsion over per-node triangle lists
+//                   rebuilt every nuc_list_period iterations  :9516-9730
+//   k_rbc_rbc       membrane node vs. facing triangles of any cell (16 sub-
+//                   triangle centroids)                :9911-10053
+//   k_ib_spread     force spreading with the same delta into BODYFORCE
+//                                                      :10737-10870, :10874-10990
+//   k_update        explicit Euler position update and the speed check that
+//                   removes a cell                     :11965-12031
+// Positions and node velocities are fp64 as in the reference; distances and
+// weights are fp32 on fp32 copies of the positions, as the reference's float
+// locals.  Sums of distances that pick a nearest triangle use non-contracted
+// fp32 operations so that ties resolve as on the CPU.
+#include "zf_internal.h"
+
+namespace zf {
+
+namespace {
+
+constexpr float kPI = 3.14159265358979f;
+
+__device__ __forceinline__ float dist3(float dx, float dy, float dz) {
+  return sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
+}
+__device__ __forceinline__ float wrapd(float d, float L) {
+  if (L > 0.f) {
+    if (d > 0.5f * L) d -= L;
+    else if (d < -0.5f * L) d += L;
+  }
+  return d;
+}
+
+// 0-based lattice index of a coordinate as the reference computes its 1-based
+// one: (int)((x - x0)/DX + 1.01) - 1, with floor for coordinates below x0.
+__device__ __forceinline__ int lat_index(float x, double x0, double dx) {
+  return (int)floor(((double)x - x0) / dx + 1.01) - 1;
+}
+__device__ __forceinline__ int wrapk(const IbArgs& a, int k) {
+  return a.per_z ? ((k % a.nz) + a.nz) % a.nz : k;
+}
+
+// slot of lattice point (i,j,k), k already wrapped; -1 when no tile holds it
+__device__ __forceinline__ int64_t slot_of(const IbArgs& a, int i, int j, int k) {
+  const int t = a.tile_map[((k >> 2) * a.nty + (j >> 2)) * a.ntx + (i >> 2)];
+  if (t < 0) return -1;
+  return (int64_t)t * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (k & 3);
+}
+
+// Peskin cosine weight of a lattice point at offsets (dx,dy,dz) from the node,
+// ZebraflowWT.c:8971-8973 (support radius 2 DX = StencilWidth*DX)
+__device__ __forceinline__ float peskin(float dx, float dy, float dz, float h2) {
+  const float cx = cosf((float)((double)kPI * fabsf(dx) / (double)h2));
+  const float cy = cosf((float)((double)kPI * fabsf(dy) / (double)h2));
+  const float cz = cosf((float)((double)kPI * fabsf(dz) / (double)h2));
+  return (1.f + cx) * (1.f + cy) * (1.f + cz) / 64.f;
+}
+
+struct NodeRef {
+  double* x;      // [3][nc][n] positions
+  int n;          // nodes per cell of this kind
+};
+
+__device__ __forceinline__ void node_pos(const double* x, int nc, int n, int cell, int node,
+                                         float LZ, double Z0, float& xp, float& yp, float& zp) {
+  xp = (float)x[((size_t)0 * nc + cell) * n + node];
+  yp = (float)x[((size_t)1 * nc + cell) * n + node];
+  double z = x[((size_t)2 * nc + cell) * n + node];
+  if (LZ > 0.f) z -= (double)LZ * floor((z - (double)Z0) / (double)LZ);
+  zp = (float)z;
+}
+
+}  // namespace
+
+// One thread per node: membrane nodes of all cells, then nucleus nodes.
+__global__ void k_ib_interp(IbArgs a, CellArgs c) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  const int64_t nmem = (int64_t)nc * c.nn;
+  const bool nuc = gid >= nmem;
+  if (gid >= nmem + (int64_t)nc * c.nnn) return;
+  const int n = nuc ? c.nnn : c.nn;
+  const int64_t lid = nuc ? gid - nmem : gid;
+  const int cell = (int)(lid / n), node = (int)(lid % n);
+  if (c.status[cell] <= 0) return;
+  const double* X = nuc ? c.xn : c.x;
+  float xp, yp, zp;
+  node_pos(X, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
+  const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
+            k0 = lat_index(zp, a.Z0, a.DX);
+  const float h2 = 2.f * a.DX;
+
+  // velocity interpolation over the points that can lie within 2 DX
+  double vx = 0.0, vy = 0.0, vz = 0.0;
+  {
+    // candidates: the 4 points per axis around the node (the others of the
+    // reference's +-4 window lie beyond 2 DX or weigh 0)
+    const int ib = (int)floor(((double)xp - a.X0) / a.DX) - 1;
+    const int jb = (int)floor(((double)yp - a.Y0) / a.DX) - 1;
+    const int kb = (int)floor(((double)zp - a.Z0) / a.DX) - 1;
+    for (int i = ib; i <= ib + 3; ++i) {
+      if (i < 0 || i >= a.nx || i < i0 - 4 || i > i0 + 4) continue;
+      for (int j = jb; j <= jb + 3; ++j) {
+        if (j < 0 || j >= a.ny || j < j0 - 4 || j > j0 + 4) continue;
+        for (int k = kb; k <= kb + 3; ++k) {
+          if (k < a.kmin || k > a.kmax || k < k0 - 4 || k > k0 + 4) continue;
+          const int kw = wrapk(a, k);
+          const float xc = (float)(a.X0 + i * a.DX);
+          const float yc = (float)(a.Y0 + j * a.DX);
+          const float zc = (float)(a.Z0 + k * a.DX);
+          const float dx = xc - xp, dy = yc - yp, dz = zc - zp;
+          const int64_t s = slot_of(a, i, j, kw);
+          if (s < 0) continue;
+          const uint8_t cd = a.code[s];
+          const bool fluid = cd >= 1 && cd <= 9;
+          if (!fluid && a.windex[s] <= 0) continue;
+          const float d = dist3(dx, dy, dz);
+          if (!(d <= h2)) continue;
+          const float w = peskin(dx, dy, dz, h2);
+          float u, v, ww;
+          if (fluid) {
+            u = a.mom[a.ns + s];
+            v = a.mom[2 * a.ns + s];
+            ww = a.mom[3 * a.ns + s];
+          } else {
+            u = a.uvoid[s];
+            v = a.uvoid[a.ns_all + s];
+            ww = a.uvoid[2 * a.ns_all + s];
+          }
+          vx += (double)w * (double)(a.vel_scale * u);
+          vy += (double)w * (double)(a.vel_scale * v);
+          vz += (double)w * (double)(a.vel_scale * ww);
+        }
+      }
+    }
+  }
+  double* V = nuc ? c.vel_n : c.vel;
+  V[((size_t)0 * nc + cell) * n + node] += vx;
+  V[((size_t)1 * nc + cell) * n + node] += vy;
+  V[((size_t)2 * nc + cell) * n + node] += vz;
+
+  // nearest wall triangle over the +-4 window, reference scan order
+  if (a.nw == 0) return;
+  const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
+  const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
+  const int k1 = max(k0 - 4, a.kmin), k2 = min(k0 + 4, a.kmax);
+  // skip the scan when no tile of the window holds a point with W_index > 0
+  bool any = false;
+  for (int ti = i1 >> 2; ti <= (i2 >> 2) && !any; ++ti)
+    for (int tj = j1 >> 2; tj <= (j2 >> 2) && !any; ++tj)
+      for (int k = k1; k <= k2 && !any; ++k) {
+        if (k != k1 && (k & 3) != 0) continue;  // first point of each z tile
+        const int kw = wrapk(a, k);
+        const int t = a.tile_map[((kw >> 2) * a.nty + tj) * a.ntx + ti];
+        if (t >= 0 && a.tile_wall[t]) any = true;
+      }
+  if (!any) return;
+  float mindis = 1.5f;
+  int triwall = -1;
+  for (int i = i1; i <= i2; ++i)
+    for (int j = j1; j <= j2; ++j)
+      for (int k = k1; k <= k2; ++k) {
+        const int kw = wrapk(a, k);
+        const int64_t s = slot_of(a, i, j, kw);
+        if (s < 0) continue;
+        const int nodewall = a.windex[s];
+        if (nodewall <= 0) continue;
+        const int32_t* L = a.wntri + (size_t)(nodewall - 1) * (a.wcap + 1);
+        const int nl = L[0];
+        for (int l = 1; l <= nl; ++l) {
+          const int tri = L[l];
+          for (int v = 0; v < 4; ++v) {
+            float px, py, pz;
+            if (v < 3) {
+              const int wn = a.wtri[3 * tri + v];
+              px = a.wxyz[wn];
+              py = a.wxyz[a.nw + wn];
+              pz = a.wxyz[2 * a.nw + wn];
+            } else {
+              px = a.wcen[tri];
+              py = a.wcen[a.mt + tri];
+              pz = a.wcen[2 * a.mt + tri];
+            }
+            const float d = dist3(xp - px, yp - py, wrapd(zp - pz, a.LZ));
+            if (d < mindis) {
+              mindis = d;
+              triwall = tri;
+            }
+          }
+        }
+      }
+  if (triwall < 0) return;
+  // signed distance to the plane of the wall triangle, repulsion, :9055-9077
+  const int w1 = a.wtri[3 * triwall];
+  const float n0 = a.wnrm[triwall], n1 = a.wnrm[a.mt + triwall], n2 = a.wnrm[2 * a.mt + triwall];
+  const float ddx = xp - a.wxyz[w1], ddy = yp - a.wxyz[a.nw + w1],
+              ddz = wrapd(zp - a.wxyz[2 * a.nw + w1], a.LZ);
+  const float dist = __fadd_rn(__fadd_rn(__fmul_rn(ddx, n0), __fmul_rn(ddy, n1)), __fmul_rn(ddz, n2));
+  if (dist < 0.25f && fabsf(dist) < 1.0f) {
+    float repulf = (float)((0.25 - (double)dist) / 1.0);
+    if (dist < -0.75f) repulf = 1.f;
+    // nucleus nodes add to the membrane array at their own index, as the
+    // reference does (ZebraflowWT.c:9415-9430 write NODE_WALLREPUL[v][caps][node])
+    float* R = c.wrep;
+    const int tn = node;
+    if (nuc && tn >= c.nn) return;
+    atomicAdd(&R[((size_t)0 * nc + cell) * c.nn + tn], (float)((double)repulf * 1.e-04 * n0));
+    atomicAdd(&R[((size_t)1 * nc + cell) * c.nn + tn], (float)((double)repulf * 1.e-04 * n1));
+    atomicAdd(&R[((size_t)2 * nc + cell) * c.nn + tn], (float)((double)repulf * 1.e-04 * n2));
+  }
+}
+
+// ---- cell list of triangle centroids ----------------------------------------
+
+// bin of each triangle: the nearest listed lattice point within 1 um of its
+// centroid inside the reference window (:5857-5902), or -1
+__global__ void k_bin_assign(IbArgs a, CellArgs c, int32_t* tri_bin, int32_t* counts) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  if (g >= (int64_t)nc * c.nt) return;
+  const int cell = (int)(g / c.nt), t = (int)(g % c.nt);
+  tri_bin[g] = -1;
+  if (c.status[cell] <= 0) return;
+  const float xp = c.tri_c[((size_t)0 * nc + cell) * c.nt + t];
+  const float yp = c.tri_c[((size_t)1 * nc + cell) * c.nt + t];
+  float zp = c.tri_c[((size_t)2 * nc + cell) * c.nt + t];
+  if (a.LZ > 0.f) zp = (float)((double)zp - (double)a.LZ * floor(((double)zp - a.Z0) / a.LZ));
+  else if (zp < a.Z0 || zp > a.Z0 + (a.nz - 1) * a.DX) return;
+  const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
+            k0 = lat_index(zp, a.Z0, a.DX);
+  const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
+  const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
+  const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
+  float mindis = 5000.f;
+  int64_t best = -1;
+  for (int i = i1; i <= i2; ++i)
+    for (int j = j1; j <= j2; ++j)
+      for (int k = k1; k <= k2; ++k) {
+        const int kw = a.per_z ? ((k % a.nz) + a.nz) % a.nz : k;
+        const int64_t s = slot_of(a, i, j, kw);
+        if (s < 0 || s >= a.ns) continue;
+        const uint8_t cd = a.code[s];
+        if (cd == 0) continue;  // listed points only
+        const float xc = (float)((double)a.X0 + i * (double)a.DX);
+        const float yc = (float)((double)a.Y0 + j * (double)a.DX);
+        const float zc = (float)((double)a.Z0 + k * (double)a.DX);
+        const float d = dist3(xc - xp, yc - yp, zc - zp);
+        if (d < mindis) {
+          mindis = d;
+          best = s;
+        }
+      }
+  if (best < 0 || !(mindis < 1.f)) return;
+  tri_bin[g] = (int32_t)best;
+  atomicAdd(&counts[best], 1);
+}
+
+// exclusive scan of counts[0..n) into off[0..n], three passes
+__global__ void k_scan_blocks(const int32_t* in, int64_t n, int32_t* out, int32_t* bsum) {
+  __shared__ int32_t sh[1024];
+  const int64_t i = (int64_t)blockIdx.x * 1024 + threadIdx.x;
+  int32_t v = i < n ? in[i] : 0;
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    int32_t t = threadIdx.x >= o ? sh[threadIdx.x - o] : 0;
+    __syncthreads();
+    sh[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < n) out[i] = sh[threadIdx.x] - v;
+  if (threadIdx.x == 1023) bsum[blockIdx.x] = sh[1023];
+}
+__global__ void k_scan_sums(int32_t* bsum, int nb, int32_t* total) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int32_t run = 0;
+    for (int b = 0; b < nb; ++b) {
+      const int32_t v = bsum[b];
+      bsum[b] = run;
+      run += v;
+    }
+    *total = run;
+  }
+}
+__global__ void k_scan_add(int32_t* out, int64_t n, const int32_t* bsum) {
+  const int64_t i = (int64_t)blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) out[i] += bsum[blockIdx.x];
+}
+
+__global__ void k_bin_fill(CellArgs c, const int32_t* tri_bin, const int32_t* off, int32_t* cursor,
+                           int32_t* bin_tri) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (int64_t)c.n_cells * c.nt) return;
+  const int32_t b = tri_bin[g];
+  if (b < 0) return;
+  const int pos = atomicAdd(&cursor[b], 1);
+  bin_tri[off[b] + pos] = (int32_t)g;
+}
+
+// deterministic order inside each bin (ascending global triangle id)
+__global__ void k_bin_sort(const int32_t* off, int64_t ns, int32_t* bin_tri) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const int b0 = off[s], b1 = off[s + 1];
+  for (int i = b0 + 1; i < b1; ++i) {
+    const int32_t v = bin_tri[i];
+    int j = i - 1;
+    while (j >= b0 && bin_tri[j] > v) {
+      bin_tri[j + 1] = bin_tri[j];
+      --j;
+    }
+    bin_tri[j + 1] = v;
+  }
+}
+
+// ---- nucleus-membrane repulsion --------------------------------------------
+
+__global__ void k_nuc_memb(IbArgs a, CellArgs c, int rebuild, unsigned long long* overflow) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  if (gid >= (int64_t)nc * c.nnn) return;
+  const int cell = (int)(gid / c.nnn), node = (int)(gid % c.nnn);
+  if (c.status[cell] <= 0) return;
+  const float xc = (float)c.xn[((size_t)0 * nc + cell) * c.nnn + node];
+  const float yc = (float)c.xn[((size_t)1 * nc + cell) * c.nnn + node];
+  const float zc = (float)c.xn[((size_t)2 * nc + cell) * c.nnn + node];
+  const float* TC = c.tri_c;
+  const size_t tb = (size_t)cell * c.nt;
+  uint16_t* list = a.nuc_list + (size_t)gid * a.nuc_cap;
+  if (rebuild) {  // own triangles with centroid within 0.5 um, :9530-9590
+    int l = 0;
+    for (int m = 0; m < c.nt; ++m) {
+      const float d = dist3(xc - TC[(size_t)0 * nc * c.nt + tb + m], yc - TC[(size_t)1 * nc * c.nt + tb + m],
+                            zc - TC[(size_t)2 * nc * c.nt + tb + m]);
+      if (d < 0.5f) {
+        if (l < a.nuc_cap) list[l++] = (uint16_t)m;
+        else atomicAdd(overflow, 1ull);
+      }
+    }
+    a.nuc_cnt[gid] = l;
+  }
+  const int cnt = a.nuc_cnt[gid];
+  for (int l = 0; l < cnt; ++l) {
+    const int tri = list[l];
+    const float px = TC[(size_t)0 * nc * c.nt + tb + tri], py = TC[(size_t)1 * nc * c.nt + tb + tri],
+                pz = TC[(size_t)2 * nc * c.nt + tb + tri];
+    if (!(dist3(xc - px, yc - py, zc - pz) < 1.f)) continue;
+    const int n1 = c.tri[3 * tri], n2 = c.tri[3 * tri + 1], n3 = c.tri[3 * tri + 2];
+    const float e1v[3] = {c.tri_nrm[((size_t)0 * nc + cell) * c.nt + tri],
+                          c.tri_nrm[((size_t)1 * nc + cell) * c.nt + tri],
+                          c.tri_nrm[((size_t)2 * nc + cell) * c.nt + tri]};
+    float p1[3], p2[3], p3[3];
+    for (int v = 0; v < 3; ++v) {
+      p1[v] = (float)c.x[((size_t)v * nc + cell) * c.nn + n1];
+      p2[v] = (float)c.x[((size_t)v * nc + cell) * c.nn + n2];
+      p3[v] = (float)c.x[((size_t)v * nc + cell) * c.nn + n3];
+    }
+    // 19 sample points of the triangle, :9638-9687
+    float tp[20][3];
+    for (int v = 0; v < 3; ++v) {
+      float ep[10];
+      ep[1] = (p1[v] + p2[v]) / 2.f;
+      ep[2] = (p2[v] + p3[v]) / 2.f;
+      ep[3] = (p3[v] + p1[v]) / 2.f;
+      ep[4] = (p1[v] + ep[1]) / 2.f;
+      ep[5] = (ep[1] + p2[v]) / 2.f;
+      ep[6] = (p2[v] + ep[2]) / 2.f;
+      ep[7] = (ep[2] + p3[v]) / 2.f;
+      ep[8] = (p3[v] + ep[3]) / 2.f;
+      ep[9] = (ep[3] + p1[v]) / 2.f;
+      tp[1][v] = (p1[v] + p2[v] + p3[v]) / 3.f;
+      tp[2][v] = (ep[3] + p1[v] + ep[1]) / 3.f;
+      tp[3][v] = (ep[1] + p2[v] + ep[2]) / 3.f;
+      tp[4][v] = (ep[2] + p3[v] + ep[3]) / 3.f;
+      tp[5][v] = (ep[1] + ep[3]) / 2.f;
+      tp[6][v] = (ep[1] + ep[2]) / 2.f;
+      tp[7][v] = (ep[2] + ep[3]) / 2.f;
+      tp[8][v] = (p1[v] + tp[2][v]) / 2.f;
+      tp[9][v] = (ep[1] + tp[2][v]) / 2.f;
+      tp[10][v] = (ep[3] + tp[2][v]) / 2.f;
+      tp[11][v] = (ep[1] + tp[3][v]) / 2.f;
+      tp[12][v] = (p2[v] + tp[3][v]) / 2.f;
+      tp[13][v] = (ep[2] + tp[3][v]) / 2.f;
+      tp[14][v] = (ep[3] + tp[4][v]) / 2.f;
+      tp[15][v] = (ep[2] + tp[4][v]) / 2.f;
+      tp[16][v] = (p3[v] + tp[4][v]) / 2.f;
+      tp[17][v] = (ep[1] + tp[1][v]) / 2.f;
+      tp[18][v] = (ep[2] + tp[1][v]) / 2.f;
+      tp[19][v] = (ep[3] + tp[1][v]) / 2.f;
+    }
+    for (int v = 1; v <= 19; ++v) {
+      const float d = dist3(tp[v][0] - xc, tp[v][1] - yc, tp[v][2] - zc);
+      if (d <= 0.2f) {
+        float repulf = (float)((0.2 - (double)d) / 0.2);
+        repulf = (float)((double)repulf * 4.1666667e-07);
+        for (int i = 0; i < 3; ++i) {
+          const float f = (float)((double)(repulf * e1v[i]) / 3.);
+          atomicAdd(&c.wrep[((size_t)i * nc + cell) * c.nn + n1], f);
+          atomicAdd(&c.wrep[((size_t)i * nc + cell) * c.nn + n2], f);
+          atomicAdd(&c.wrep[((size_t)i * nc + cell) * c.nn + n3], f);
+        }
+      }
+    }
+  }
+}
+
+// ---- cell-cell repulsion ------------------------------------------------------
+
+__global__ void k_rbc_rbc(IbArgs a, CellArgs c) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  if (gid >= (int64_t)nc * c.nn) return;
+  const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
+  if (c.status[cell] <= 0) return;
+  float xc, yc, zc;
+  node_pos(c.x, nc, c.nn, cell, node, a.LZ, a.Z0, xc, yc, zc);
+  const float e1v[3] = {c.node_normal[((size_t)0 * nc + cell) * c.nn + node],
+                        c.node_normal[((size_t)1 * nc + cell) * c.nn + node],
+                        c.node_normal[((size_t)2 * nc + cell) * c.nn + node]};
+  const int i0 = lat_index(xc, a.X0, a.DX), j0 = lat_index(yc, a.Y0, a.DX),
+            k0 = lat_index(zc, a.Z0, a.DX);
+  const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
+  const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
+  const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
+  float rx = 0.f, ry = 0.f, rz = 0.f;
+  for (int i = i1; i <= i2; ++i)
+    for (int j = j1; j <= j2; ++j)
+      for (int k = k1; k <= k2; ++k) {
+        const int kw = a.per_z ? ((k % a.nz) + a.nz) % a.nz : k;
+        const int64_t s = slot_of(a, i, j, kw);
+        if (s < 0 || s >= a.ns) continue;
+        const int b0 = a.bin_off[s], b1 = a.bin_off[s + 1];
+        for (int e = b0; e < b1; ++e) {
+          const int g = a.bin_tri[e];
+          const int m = g / c.nt, tri = g - m * c.nt;
+          const int n1 = c.tri[3 * tri], n2 = c.tri[3 * tri + 1], n3 = c.tri[3 * tri + 2];
+          if (m == cell && (n1 == node || n2 == node || n3 == node)) continue;
+          const float e2v[3] = {c.tri_nrm[((size_t)0 * nc + m) * c.nt + tri],
+                                c.tri_nrm[((size_t)1 * nc + m) * c.nt + tri],
+                                c.tri_nrm[((size_t)2 * nc + m) * c.nt + tri]};
+          const float dot = e1v[0] * e2v[0] + e1v[1] * e2v[1] + e1v[2] * e2v[2];
+          if (!(dot < 0.f)) continue;
+          const float px = c.tri_c[((size_t)0 * nc + m) * c.nt + tri];
+          const float py = c.tri_c[((size_t)1 * nc + m) * c.nt + tri];
+          const float pzr = c.tri_c[((size_t)2 * nc + m) * c.nt + tri];
+          const float dzc = wrapd(pzr - zc, a.LZ);
+          const float shift = (pzr - zc) - dzc;  // periodic image of the other cell
+          if (!(dist3(xc - px, yc - py, -dzc) < 2.f)) continue;
+          float tp[16][3], tc[17][3];
+          for (int v = 0; v < 3; ++v) {
+            const float off = v == 2 ? shift : 0.f;
+            tp[1][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n1] - off;
+            tp[2][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n2] - off;
+            tp[3][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n3] - off;
+            tp[4][v] = 0.5f * (tp[1][v] + tp[2][v]);
+            tp[5][v] = 0.5f * (tp[2][v] + tp[3][v]);
+            tp[6][v] = 0.5f * (tp[1][v] + tp[3][v]);
+            tp[7][v] = 0.5f * (tp[1][v] + tp[4][v]);
+            tp[8][v] = 0.5f * (tp[2][v] + tp[4][v]);
+            tp[9][v] = 0.5f * (tp[2][v] + tp[5][v]);
+            tp[10][v] = 0.5f * (tp[5][v] + tp[3][v]);
+            tp[11][v] = 0.5f * (tp[3][v] + tp[6][v]);
+            tp[12][v] = 0.5f * (tp[6][v] + tp[1][v]);
+            tp[13][v] = 0.5f * (tp[4][v] + tp[6][v]);
+            tp[14][v] = 0.5f * (tp[4][v] + tp[5][v]);
+            tp[15][v] = 0.5f * (tp[5][v] + tp[6][v]);
+            tc[1][v] = (tp[1][v] + tp[7][v] + tp[12][v]) / 3.f;
+            tc[2][v] = (tp[7][v] + tp[13][v] + tp[12][v]) / 3.f;
+            tc[3][v] = (tp[7][v] + tp[4][v] + tp[13][v]) / 3.f;
+            tc[4][v] = (tp[4][v] + tp[14][v] + tp[13][v]) / 3.f;
+            tc[5][v] = (tp[4][v] + tp[8][v] + tp[14][v]) / 3.f;
+            tc[6][v] = (tp[8][v] + tp[9][v] + tp[14][v]) / 3.f;
+            tc[7][v] = (tp[8][v] + tp[2][v] + tp[9][v]) / 3.f;
+            tc[8][v] = (tp[12][v] + tp[13][v] + tp[6][v]) / 3.f;
+            tc[9][v] = (tp[13][v] + tp[15][v] + tp[6][v]) / 3.f;
+            tc[10][v] = (tp[13][v] + tp[14][v] + tp[15][v]) / 3.f;
+            tc[11][v] = (tp[14][v] + tp[5][v] + tp[15][v]) / 3.f;
+            tc[12][v] = (tp[14][v] + tp[9][v] + tp[5][v]) / 3.f;
+            tc[13][v] = (tp[6][v] + tp[15][v] + tp[11][v]) / 3.f;
+            tc[14][v] = (tp[15][v] + tp[10][v] + tp[11][v]) / 3.f;
+            tc[15][v] = (tp[15][v] + tp[5][v] + tp[10][v]) / 3.f;
+            tc[16][v] = (tp[11][v] + tp[10][v] + tp[3][v]) / 3.f;
+          }
+          for (int v = 1; v <= 16; ++v) {
+            const float dx = tc[v][0] - xc, dy = tc[v][1] - yc, dz = tc[v][2] - zc;
+            const float d = dist3(dx, dy, dz);
+            if (d < 1.0f) {
+              const float repulf = (float)(-8.333e-07 * (1.0 - (double)d) / 1.0);
+              rx += repulf * (dx / d);
+              ry += repulf * (dy / d);
+              rz += repulf * (dz / d);
+            }
+          }
+        }
+      }
+  c.wrep[((size_t)0 * nc + cell) * c.nn + node] += rx;
+  c.wrep[((size_t)1 * nc + cell) * c.nn + node] += ry;
+  c.wrep[((size_t)2 * nc + cell) * c.nn + node] += rz;
+}
+
+// ---- spreading ----------------------------------------------------------------
+
+__global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  const int64_t nmem = (int64_t)nc * c.nn;
+  const bool nuc = gid >= nmem;
+  if (gid >= nmem + (int64_t)nc * c.nnn) return;
+  const int n = nuc ? c.nnn : c.nn;
+  const int64_t lid = nuc ? gid - nmem : gid;
+  const int cell = (int)(lid / n), node = (int)(lid % n);
+  if (c.status[cell] <= 0) return;
+  const double* X = nuc ? c.xn : c.x;
+  double* V = nuc ? c.vel_n : c.vel;
+  const float* R = nuc ? c.wrep_n : c.wrep;
+  const float* FT = nuc ? c.ftot_n : c.ftot;
+  float Ff[3];
+  for (int v = 0; v < 3; ++v) {  // :10749-10754
+    const size_t g = ((size_t)v * nc + cell) * n + node;
+    V[g] += (double)R[g];
+    Ff[v] = (float)((double)a.gamma_p * (double)R[g] + (double)FT[g]);
+  }
+  float xp, yp, zp;
+  node_pos(X, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
+  const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
+            k0 = lat_index(zp, a.Z0, a.DX);
+  const float h2 = 2.f * a.DX;
+  const int ib = (int)floor(((double)xp - a.X0) / a.DX) - 1;
+  const int jb = (int)floor(((double)yp - a.Y0) / a.DX) - 1;
+  const int kb = (int)floor(((double)zp - a.Z0) / a.DX) - 1;
+  for (int i = ib; i <= ib + 3; ++i) {
+    if (i < 0 || i >= a.nx || i < i0 - 4 || i > i0 + 4) continue;
+    for (int j = jb; j <= jb + 3; ++j) {
+      if (j < 0 || j >= a.ny || j < j0 - 4 || j > j0 + 4) continue;
+      for (int k = kb; k <= kb + 3; ++k) {
+        if (k < a.kmin || k > a.kmax || k < k0 - 4 || k > k0 + 4) continue;
+        const int kw = wrapk(a, k);
+        const int64_t s = slot_of(a, i, j, kw);
+        if (s < 0 || s >= a.ns) continue;
+        const uint8_t cd = a.code[s];
+        if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) continue;
+        const float xc = (float)((double)a.X0 + i * (double)a.DX);
+        const float yc = (float)((double)a.Y0 + j * (double)a.DX);
+        const float zc = (float)((double)a.Z0 + k * (double)a.DX);
+        const float dx = xc - xp, dy = yc - yp, dz = zc - zp;
+        if (!(dist3(dx, dy, dz) <= h2)) continue;
+        const float w = peskin(dx, dy, dz, h2);
+        for (int v = 0; v < 3; ++v)
+          atomicAdd(&a.force[v * a.ns + s], (float)((double)(w * Ff[v]) * (double)a.force_scale));
+      }
+    }
+  }
+}
+
+// ---- position update ------------------------------------------------------------
+
+__global__ void k_update(IbArgs a, CellArgs c) {
+  const int cell = blockIdx.x;
+  if (c.status[cell] <= 0) return;
+  const int nc = c.n_cells;
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < c.nnn; i += blockDim.x)  // nucleus first, :11969-11973
+    for (int v = 0; v < 3; ++v) {
+      const size_t g = ((size_t)v * nc + cell) * c.nnn + i;
+      c.xn[g] += c.vel_n[g] * a.dt_stagger;
+    }
+  for (int i = threadIdx.x; i < c.nn; i += blockDim.x) {  // speed check, :11975-11981
+    const double vx = c.vel[((size_t)0 * nc + cell) * c.nn + i];
+    const double vy = c.vel[((size_t)1 * nc + cell) * c.nn + i];
+    const double vz = c.vel[((size_t)2 * nc + cell) * c.nn + i];
+    const float sp = sqrtf((float)(vx * vx + vy * vy + vz * vz));
+    if (sp > a.vmax_remove || isnan(sp) || isinf(sp)) bad = 1;
+  }
+  __syncthreads();
+  if (!bad) {
+    for (int i = threadIdx.x; i < c.nn; i += blockDim.x)
+      for (int v = 0; v < 3; ++v) {
+        const size_t g = ((size_t)v * nc + cell) * c.nn + i;
+        c.x[g] += c.vel[g] * a.dt_stagger;
+      }
+    return;
+  }
+  // removal: every node to the null position, :12007-12030
+  for (int i = threadIdx.x; i < c.nn; i += blockDim.x)
+    for (int v = 0; v < 3; ++v) {
+      const size_t g = ((size_t)v * nc + cell) * c.nn + i;
+      c.x[g] = -5000.0;
+      c.vel[g] = 0.0;
+      c.ftot[g] = 0.f;
+      c.wrep[g] = 0.f;
+    }
+  for (int i = threadIdx.x; i < c.nnn; i += blockDim.x)
+    for (int v = 0; v < 3; ++v) {
+      const size_t g = ((size_t)v * nc + cell) * c.nnn + i;
+      c.xn[g] = -5000.0;
+      c.vel_n[g] = 0.0;
+      c.ftot_n[g] = 0.f;
+    }
+  if (threadIdx.x == 0) {
+    c.status[cell] = -5000;
+    atomicAdd(&c.counters[1], 1ull);
+  }
+}
+
+// ---- launchers --------------------------------------------------------------------
+
+int ib_interp_launch(zf_ctx* ctx) {
+  const CellArgs& c = ctx->cells;
+  const int64_t n = (int64_t)c.n_cells * (c.nn + c.nnn);
+  if (n == 0) return ZF_OK;
+  k_ib_interp<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c);
+  ZF_CUDA(cudaGetLastError());
+  return ZF_OK;
+}
+
+int ib_bins_launch(zf_ctx* ctx) {
+  const CellArgs& c = ctx->cells;
+  IbArgs& a = ctx->ib;
+  const int64_t ntri = (int64_t)c.n_cells * c.nt;
+  if (ntri == 0) return ZF_OK;
+  int32_t* counts = const_cast<int32_t*>(a.bin_off) + (a.ns + 1);  // scratch after off
+  int32_t* tri_bin = counts + (a.ns + 1);
+  int32_t* bsum = tri_bin + ntri;
+  int32_t* off = const_cast<int32_t*>(a.bin_off);
+  ZF_CUDA(cudaMemsetAsync(counts, 0, (a.ns + 1) * sizeof(int32_t), ctx->stream));
+  k_bin_assign<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(a, c, tri_bin, counts);
+  const int64_t nscan = a.ns + 1;
+  const int nb = (int)((nscan + 1023) / 1024);
+  k_scan_blocks<<<nb, 1024, 0, ctx->stream>>>(counts, nscan, off, bsum);
+  k_scan_sums<<<1, 32, 0, ctx->stream>>>(bsum, nb, bsum + nb);
+  k_scan_add<<<nb, 1024, 0, ctx->stream>>>(off, nscan, bsum);
+  ZF_CUDA(cudaMemsetAsync(counts, 0, (a.ns + 1) * sizeof(int32_t), ctx->stream));
+  k_bin_fill<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(c, tri_bin, off, counts,
+                                                                       const_cast<int32_t*>(a.bin_tri));
+  k_bin_sort<<<(unsigned)((a.ns + 255) / 256), 256, 0, ctx->stream>>>(off, a.ns,
+                                                                       const_cast<int32_t*>(a.bin_tri));
+  ZF_CUDA(cudaGetLastError());
+  return ZF_OK;
+}
+
+int ib_nuc_memb_launch(zf_ctx* ctx, int rebuild) {
+  const CellArgs& c = ctx->cells;
+  const int64_t n = (int64_t)c.n_cells * c.nnn;
+  if (n == 0) return ZF_OK;
+  k_nuc_memb<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c, rebuild,
+                                                                     c.counters + 2);
+  ZF_CUDA(cudaGetLastError());
+  return ZF_OK;
+}
+
+int ib_rbc_rbc_launch(zf_ctx* ctx) {
+  const CellArgs& c = ctx->cells;
+  const int64_t n = (int64_t)c.n_cells * c.nn;
+  if (n == 0) return ZF_OK;
+  k_rbc_rbc<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c);
+  ZF_CUDA(cudaGetLastError());
+  return ZF_OK;
+}
+
+int ib_spread_launch(zf_ctx* ctx) {
+  const CellArgs& c = ctx->cells;
+  const int64_t n = (int64_t)c.n_cells * (c.nn + c.nnn);
+  if (n == 0) return ZF_OK;
+  k_ib_spread<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
+      ctx->ib, c, ctx->p.wall_mode == ZF_WALL_REF_EQ);
+  ZF_CUDA(cudaGetLastError());
+  return ZF_OK;
+}
+
+int ib_update_launch(zf_ctx* ctx) {
+  const CellArgs& c = ctx->cells;
+  if (c.n_cells == 0) return ZF_OK;
+  k_update<<<c.n_cells, 256, 0, ctx->stream>>>(ctx->ib, c);
+  ZF_CUDA(cudaGetLastError());
+  return ZF_OK;
+}
+
+}  // namespace zf

@@ -101,6 +101,71 @@ struct CellArgs {
 int cells_membrane_launch(zf_ctx* c);
 void cells_free(zf_ctx* c);
 
+// Wall mesh on the host (reference WALLNODECOORD, WALLCELLNODE, WALLCELLNORMALS,
+// WALL_CENTROID, WALLNODETOCELLNEIGHBORLIST, W_index, Wdistance, Uvoid).
+struct VoidPoint {
+  int64_t p;   // lattice point (dense index)
+  float u[3];  // void velocity
+};
+struct WallHost {
+  int nw = 0, mt = 0, cap = 0;
+  std::vector<float> xyz;        // [3][nw]
+  std::vector<int32_t> tri;      // [mt][3] 0-based
+  std::vector<float> nrm, cen;   // [3][mt]
+  std::vector<int32_t> ntri;     // [nw][cap+1]: count, triangles (0-based)
+  std::vector<int32_t> windex;   // [npts] 1-based wall node, 0 none
+  std::vector<float> wdist;      // [npts]
+  std::vector<VoidPoint> uvoid;  // non-zero void velocities
+};
+int wall_build(zf_ctx* c, int nw, const float* xyz, int mt, const int32_t* tri1, const float* nrm,
+               WallHost& W);
+
+// Device view used by the IB kernels.
+struct IbArgs {
+  int nx, ny, nz, ntx, nty, ntz;
+  int per_z;
+  int kmin, kmax;               // z range of lattice points the coupling sees: the
+                                // reference keeps 3 <= k <= KM-3 (1-based) in its region
+                                // of interest; a periodic axis has no limit
+  double X0, Y0, Z0, DX;        // um
+  float LZ;                     // nz*DX when z is periodic, else 0
+  const int32_t* tile_map;      // all tiles
+  const uint8_t* code;          // [n_all*64]
+  const uint8_t* tile_wall;     // [n_all] tile holds a point with W_index > 0
+  const int32_t* windex;        // [n_all*64] 1-based wall node or 0
+  const float* uvoid;           // [3][n_all*64]
+  const float* mom;             // [4][ns] D,U,V,W of population tiles
+  float* force;                 // [3][ns] BODYFORCE
+  int64_t ns, ns_all;
+  // wall mesh
+  int nw, mt, wcap;
+  const float* wxyz;            // [3][nw]
+  const int32_t* wtri;          // [mt][3]
+  const float* wnrm;            // [3][mt]
+  const float* wcen;            // [3][mt]
+  const int32_t* wntri;         // [nw][wcap+1]
+  // cell list of triangle centroids over population slots (CSR)
+  const int32_t* bin_off;       // [ns+1]
+  const int32_t* bin_tri;       // [n_cells*nt] global triangle id = cell*nt + tri
+  // constants
+  float vel_scale, gamma_p;
+  double force_scale;           // 1/(UNITMASS*LBM_BFORCE_SCALE)
+  double dt_stagger;            // DT * SOLVERSTAGGER
+  float vmax_remove;
+  int nuc_cap;
+  uint16_t* nuc_list;           // [nc][nnn][nuc_cap]
+  int32_t* nuc_cnt;             // [nc][nnn]
+};
+
+int ib_prepare(zf_ctx* c);
+void ib_free(zf_ctx* c);
+int ib_interp_launch(zf_ctx* c);
+int ib_bins_launch(zf_ctx* c);
+int ib_nuc_memb_launch(zf_ctx* c, int rebuild);
+int ib_rbc_rbc_launch(zf_ctx* c);
+int ib_spread_launch(zf_ctx* c);
+int ib_update_launch(zf_ctx* c);
+
 }  // namespace zf
 
 struct zf_ctx {
@@ -151,6 +216,13 @@ struct zf_ctx {
   zf::CellArgs cells{};            // device pointers + sizes
   std::vector<void*> cell_allocs;  // device buffers owned for the cells
   std::vector<void*> mesh_allocs;  // device buffers owned for the mesh
+
+  // wall mesh and the IB view of the lattice
+  bool wall_set = false;
+  zf::IbArgs ib{};
+  std::vector<void*> wall_allocs;  // wall + aux-tile buffers
+  std::vector<void*> ib_allocs;    // cell list + nucleus lists (sized with the cells)
+  bool nuc_lists_valid = false;    // nucleus-membrane lists built since the cells were set
 };
 
 namespace zf {

@@ -437,7 +437,7 @@ int zf_set_cells(zf_ctx* c, int n_cells, const double* x, const double* xn) {
   if ((rc = upload<unsigned long long>(c, own, &a.counters, nullptr, 4))) return rc;
   ZF_CUDA(cudaStreamSynchronize(c->stream));
   c->cells_set = true;
-  return ZF_OK;
+  return ib_prepare(c);  // cell list and nucleus lists sized for these cells
 }
 
 int zf_get_cells(zf_ctx* c, double* x, double* xn, int32_t* status) {
@@ -505,6 +505,106 @@ int zf_cgsm_forces(zf_ctx* c) {
   NEED(c->cells_set, "zf_cgsm_forces", "cells not set");
   ZF_CUDA(cudaSetDevice(c->device));
   return cells_membrane_launch(c);
+}
+
+// Seeded placement of n_cells cells in a vessel (B_index codes, lattice
+// units): centres uniform over fluid points, orientations uniform (random
+// unit quaternion), rejecting a candidate whose ellipsoid (semi-axes
+// `axes` um plus `margin` um) overlaps an accepted one on the lattice, or
+// any of whose membrane nodes has a non-fluid lattice point among its 27
+// nearest.  Outputs x [3][n_cells][n_node], xn [3][n_cells][n_node_n] in um.
+// Returns the number placed in *placed (fewer than asked when the attempts
+// run out).
+int zf_gen_cells(const int32_t* b, int nx, int ny, int nz, const double* origin, double dx,
+                 int periodic_z, int n_cells, int n_node, const double* rest, int n_node_n,
+                 const double* rest_n, const double* axes, double margin, uint64_t seed,
+                 double* x, double* xn, int* placed) {
+  if (!b || !origin || !rest || !axes || !x || !placed || n_cells < 0 || dx <= 0) return ZF_ERR_ARG;
+  uint64_t st = seed;
+  auto next = [&]() {  // splitmix64
+    uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  auto uni = [&]() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); };
+  std::vector<int64_t> fluid;
+  for (int64_t p = 0; p < (int64_t)nx * ny * nz; ++p)
+    if (b[p] > 0) fluid.push_back(p);
+  if (fluid.empty()) return ZF_ERR_ARG;
+  std::vector<uint8_t> occ((size_t)nx * ny * nz, 0);
+  auto at = [&](int i, int j, int k) -> int64_t {
+    if (i < 0 || i >= nx || j < 0 || j >= ny) return -1;
+    if (k < 0 || k >= nz) {
+      if (!periodic_z) return -1;
+      k = ((k % nz) + nz) % nz;
+    }
+    return ((int64_t)i * ny + j) * nz + k;
+  };
+  const double A[3] = {axes[0] + margin, axes[1] + margin, axes[2] + margin};
+  const int reach = (int)std::ceil(std::max(A[0], std::max(A[1], A[2])) / dx) + 1;
+  int n_ok = 0;
+  const int64_t max_tries = 400LL * n_cells + 1000;
+  std::vector<int64_t> mark;
+  for (int64_t tries = 0; n_ok < n_cells && tries < max_tries; ++tries) {
+    const int64_t p = fluid[(size_t)(uni() * fluid.size()) % fluid.size()];
+    const double ci = (double)(p / ((int64_t)ny * nz)) + uni() - 0.5;
+    const double cj = (double)((p / nz) % ny) + uni() - 0.5;
+    const double ck = (double)(p % nz) + uni() - 0.5;
+    // uniform rotation (Shoemake)
+    const double u1 = uni(), u2 = uni(), u3 = uni();
+    const double qw = std::sqrt(1 - u1) * std::sin(2 * M_PI * u2), qx = std::sqrt(1 - u1) * std::cos(2 * M_PI * u2),
+                 qy = std::sqrt(u1) * std::sin(2 * M_PI * u3), qz = std::sqrt(u1) * std::cos(2 * M_PI * u3);
+    const double R[3][3] = {{1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qz * qw), 2 * (qx * qz + qy * qw)},
+                            {2 * (qx * qy + qz * qw), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qx * qw)},
+                            {2 * (qx * qz - qy * qw), 2 * (qy * qz + qx * qw), 1 - 2 * (qx * qx + qy * qy)}};
+    // lattice points inside the inflated ellipsoid: free?
+    mark.clear();
+    bool ok = true;
+    for (int di = -reach; di <= reach && ok; ++di)
+      for (int dj = -reach; dj <= reach && ok; ++dj)
+        for (int dk = -reach; dk <= reach && ok; ++dk) {
+          const int i = (int)std::floor(ci) + di, j = (int)std::floor(cj) + dj, k = (int)std::floor(ck) + dk;
+          const double v[3] = {(i - ci) * dx, (j - cj) * dx, (k - ck) * dx};
+          double q[3];
+          for (int a = 0; a < 3; ++a) q[a] = R[0][a] * v[0] + R[1][a] * v[1] + R[2][a] * v[2];
+          const double e = q[0] * q[0] / (A[0] * A[0]) + q[1] * q[1] / (A[1] * A[1]) + q[2] * q[2] / (A[2] * A[2]);
+          if (e > 1.0) continue;
+          const int64_t s = at(i, j, k);
+          if (s < 0 || occ[s]) ok = false;
+          else mark.push_back(s);
+        }
+    if (!ok) continue;
+    // every membrane node at least one lattice unit from the wall
+    for (int n = 0; n < n_node && ok; ++n) {
+      double pos[3];
+      for (int a = 0; a < 3; ++a)
+        pos[a] = R[a][0] * rest[3 * n] + R[a][1] * rest[3 * n + 1] + R[a][2] * rest[3 * n + 2];
+      const int i = (int)std::lround(ci + pos[0] / dx), j = (int)std::lround(cj + pos[1] / dx),
+                k = (int)std::lround(ck + pos[2] / dx);
+      for (int di = -1; di <= 1 && ok; ++di)
+        for (int dj = -1; dj <= 1 && ok; ++dj)
+          for (int dk = -1; dk <= 1 && ok; ++dk) {
+            const int64_t s = at(i + di, j + dj, k + dk);
+            if (s < 0 || b[s] <= 0) ok = false;
+          }
+    }
+    if (!ok) continue;
+    for (int64_t s : mark) occ[s] = 1;
+    const double c0[3] = {origin[0] + ci * dx, origin[1] + cj * dx, origin[2] + ck * dx};
+    for (int n = 0; n < n_node; ++n)
+      for (int a = 0; a < 3; ++a)
+        x[((size_t)a * n_cells + n_ok) * n_node + n] =
+            c0[a] + R[a][0] * rest[3 * n] + R[a][1] * rest[3 * n + 1] + R[a][2] * rest[3 * n + 2];
+    if (xn && rest_n)
+      for (int n = 0; n < n_node_n; ++n)
+        for (int a = 0; a < 3; ++a)
+          xn[((size_t)a * n_cells + n_ok) * n_node_n + n] =
+              c0[a] + R[a][0] * rest_n[3 * n] + R[a][1] * rest_n[3 * n + 1] + R[a][2] * rest_n[3 * n + 2];
+    ++n_ok;
+  }
+  *placed = n_ok;
+  return ZF_OK;
 }
 
 }  // extern "C"
