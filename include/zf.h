@@ -324,6 +324,20 @@ int zf_step(zf_ctx* ctx, int nsteps);
 /* zf_step timed with CUDA events on the context stream (ms). */
 int zf_step_timed(zf_ctx* ctx, int nsteps, float* ms);
 
+/* One iteration of zf_step that also returns the FP64 global mass reduced
+ * inside its LBM kernel (see zf_lbm_step_mass); waits for the result. */
+int zf_step_mass(zf_ctx* ctx, double* mass);
+
+/* Number of kernels the context has launched so far. */
+int zf_launch_count(zf_ctx* ctx, int64_t* n);
+
+/* Instrumentation of zf_step: with enable=1, CUDA events bracket the LBM
+ * kernel and the membrane/IB work of up to `capacity` iterations;
+ * zf_profile_read returns their summed device times (ms) and counts. */
+int zf_profile(zf_ctx* ctx, int enable, int capacity);
+int zf_profile_read(zf_ctx* ctx, float* lbm_ms, int* lbm_count, float* membrane_ms,
+                    int* membrane_count);
+
 /* Completed iterations (the reference's iter). */
 int zf_iteration(zf_ctx* ctx, int64_t* iter);
 

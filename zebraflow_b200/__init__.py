@@ -116,6 +116,11 @@ _SIGS = {
     "zf_step": (C.c_int, [_P, C.c_int]),
     "zf_step_timed": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
     "zf_iteration": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "zf_step_mass": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "zf_launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "zf_profile": (C.c_int, [_P, C.c_int, C.c_int]),
+    "zf_profile_read": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int),
+                                  C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "zf_gen_wall_tube": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                                    _f64p, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
@@ -449,6 +454,27 @@ class Context:
         it = C.c_int64()
         _check(lib().zf_iteration(self._h, C.byref(it)))
         return it.value
+
+    def step_mass(self) -> float:
+        m = C.c_double()
+        _check(lib().zf_step_mass(self._h, C.byref(m)))
+        return m.value
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        _check(lib().zf_launch_count(self._h, C.byref(n)))
+        return n.value
+
+    def profile(self, enable=True, capacity=4096):
+        _check(lib().zf_profile(self._h, int(enable), capacity))
+
+    def profile_read(self):
+        lm, lc, mm, mc = C.c_float(), C.c_int(), C.c_float(), C.c_int()
+        _check(lib().zf_profile_read(self._h, C.byref(lm), C.byref(lc), C.byref(mm), C.byref(mc)))
+        return lm.value, lc.value, mm.value, mc.value
+
+    def set_stream(self, stream_handle):
+        _check(lib().zf_set_stream(self._h, C.c_void_p(stream_handle) if stream_handle else None))
 
     def device_bytes(self) -> int:
         b = C.c_int64()

@@ -166,6 +166,7 @@ void zf_destroy(zf_ctx* c) {
   ib_free(c);
   free_lattice(c);
   cells_free(c);
+  for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);

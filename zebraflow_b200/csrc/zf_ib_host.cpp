@@ -263,7 +263,7 @@ int zf_update_positions(zf_ctx* c) {
 }
 
 // One or more iterations of the reference time loop, ZebraflowWT.c:5646-12190.
-int zf_step(zf_ctx* c, int nsteps) {
+static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
   if (!c) return ZF_ERR_ARG;
   if (!c->lattice_set) {
     set_error("zf_step: lattice not set");
@@ -278,10 +278,22 @@ int zf_step(zf_ctx* c, int nsteps) {
   for (int s = 0; s < nsteps; ++s) {
     const int64_t iter = c->status.iter + 1;
     const bool membrane = cells && (iter % c->p.stagger == 0);  // RBCSOLVERFLAG, :5650-5652
+    const bool last = s == nsteps - 1;
     int rc;
+    const bool pm = c->profiling && membrane && c->prof_mem < c->prof_cap;
+    if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (c->prof_cap + c->prof_mem)], c->stream));
     if (membrane && (rc = cells_membrane_launch(c))) return rc;
-    if ((rc = lbm_launch(c, membrane, membrane))) return rc;
+    if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (c->prof_cap + c->prof_mem) + 1], c->stream));
+    const bool pl = c->profiling && c->prof_lbm < c->prof_cap;
+    if (pl) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * c->prof_lbm], c->stream));
+    if ((rc = lbm_launch(c, membrane, membrane, (last && mass_last) ? mass_last : nullptr)))
+      return rc;
+    if (pl) {
+      ZF_CUDA(cudaEventRecord(c->prof_ev[2 * c->prof_lbm + 1], c->stream));
+      c->prof_lbm++;
+    }
     if (membrane) {
+      if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (2 * c->prof_cap + c->prof_mem)], c->stream));
       const bool rebuild = !c->nuc_lists_valid || (iter % c->p.nuc_list_period == 0);
       if ((rc = ib_interp_launch(c))) return rc;
       if ((rc = ib_nuc_memb_launch(c, rebuild))) return rc;
@@ -290,9 +302,68 @@ int zf_step(zf_ctx* c, int nsteps) {
       if ((rc = ib_rbc_rbc_launch(c))) return rc;
       if ((rc = ib_spread_launch(c))) return rc;
       if ((rc = ib_update_launch(c))) return rc;
+      if (pm) {
+        ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (2 * c->prof_cap + c->prof_mem) + 1], c->stream));
+        c->prof_mem++;
+      }
+      // k_membrane, k_ib_interp, k_nuc_memb, 7 cell-list kernels, k_rbc_rbc,
+      // k_ib_spread, k_update
+      c->launches += 13;
     }
     c->status.iter = iter;
   }
+  return ZF_OK;
+}
+
+int zf_step(zf_ctx* c, int nsteps) { return step_impl(c, nsteps, nullptr); }
+
+int zf_step_mass(zf_ctx* c, double* mass) {
+  if (!mass) return ZF_ERR_ARG;
+  return step_impl(c, 1, mass);
+}
+
+int zf_launch_count(zf_ctx* c, int64_t* n) {
+  if (!c || !n) return ZF_ERR_ARG;
+  *n = c->launches;
+  return ZF_OK;
+}
+
+int zf_profile(zf_ctx* c, int enable, int capacity) {
+  if (!c) return ZF_ERR_ARG;
+  ZF_CUDA(cudaSetDevice(c->device));
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+  c->prof_ev.clear();
+  c->prof_cap = c->prof_lbm = c->prof_mem = 0;
+  c->profiling = enable != 0;
+  if (!enable) return ZF_OK;
+  c->prof_cap = capacity > 0 ? capacity : 4096;
+  // [LBM pairs][membrane-force pairs][IB-block pairs]
+  c->prof_ev.resize(6 * (size_t)c->prof_cap);
+  for (auto& e : c->prof_ev) ZF_CUDA(cudaEventCreate(&e));
+  return ZF_OK;
+}
+
+int zf_profile_read(zf_ctx* c, float* lbm_ms, int* lbm_count, float* membrane_ms, int* membrane_count) {
+  if (!c) return ZF_ERR_ARG;
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  float tl = 0.f, tm = 0.f;
+  for (int i = 0; i < c->prof_lbm; ++i) {
+    float ms = 0.f;
+    ZF_CUDA(cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]));
+    tl += ms;
+  }
+  for (int i = 0; i < c->prof_mem; ++i) {
+    float a = 0.f, b = 0.f;
+    ZF_CUDA(cudaEventElapsedTime(&a, c->prof_ev[2 * (c->prof_cap + i)], c->prof_ev[2 * (c->prof_cap + i) + 1]));
+    ZF_CUDA(cudaEventElapsedTime(&b, c->prof_ev[2 * (2 * c->prof_cap + i)],
+                                 c->prof_ev[2 * (2 * c->prof_cap + i) + 1]));
+    tm += a + b;
+  }
+  if (lbm_ms) *lbm_ms = tl;
+  if (lbm_count) *lbm_count = c->prof_lbm;
+  if (membrane_ms) *membrane_ms = tm;
+  if (membrane_count) *membrane_count = c->prof_mem;
   return ZF_OK;
 }
 

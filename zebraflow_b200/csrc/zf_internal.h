@@ -223,6 +223,13 @@ struct zf_ctx {
   std::vector<void*> wall_allocs;  // wall + aux-tile buffers
   std::vector<void*> ib_allocs;    // cell list + nucleus lists (sized with the cells)
   bool nuc_lists_valid = false;    // nucleus-membrane lists built since the cells were set
+
+  // instrumentation: kernel launches, and optional event pairs around the LBM
+  // kernel and the membrane block of zf_step
+  int64_t launches = 0;
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_ev;  // [2*cap]: LBM pairs then membrane pairs
+  int prof_cap = 0, prof_lbm = 0, prof_mem = 0;
 };
 
 namespace zf {

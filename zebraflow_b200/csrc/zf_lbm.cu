@@ -456,6 +456,8 @@ int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out) {
   }
   dispatch_storage<LaunchStep>(c->p.storage, c, a);
   ZF_CUDA(cudaGetLastError());
+  c->launches += (c->n_active > 0) + (c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0) +
+                 (mass_out ? 1 : 0);
   c->cur ^= 1;
   if (mass_out) {
     k_sum_partials<<<1, 256, 0, c->stream>>>(c->d_red, grid, c->d_red + grid);
