@@ -1,27 +1,40 @@
 #!/usr/bin/env python3
-"""Benchmark of the B200-native Zebraflow hot path.
+"""Benchmark of the B200-native Zebraflow time step (LBM + IB + membranes).
 
-Default workload: the periodic Y-bifurcation of 256x256x1024 lattice points
-(parent radius 30 splitting at 40 degrees into daughters of radius 22, about
-3.1M fluid points), halfway bounce-back walls, uniform Guo force 2e-6 along
-the parent axis, fp32 populations.  A step is one LBM time step
-(pull stream + BGK/Guo collision + walls) over the whole vessel.
+Default workload ``c1_bifurcation_256x256x1024_2000rbc``: the periodic
+Y-bifurcation of 256x256x1024 lattice points (parent radius 30 splitting at
+40 degrees into daughters of radius 22, about 3.1M fluid points), halfway
+bounce-back walls, tau 0.9, uniform Guo force 2e-6 along the parent axis,
+2000 nucleated RBCs (icosphere membranes of 642 nodes / 1280 triangles scaled
+to semi-axes 7, 4.5, 2 lattice units, nuclei of 162 nodes scaled to 2.5, 1.8,
+1.2) placed from a seed, a marching-tetrahedra wall mesh of the vessel, the
+membrane/IB block every 50 steps.  A step is one iteration of the reference
+time loop: an LBM step, plus on every 50th step the membrane forces, IB
+velocity interpolation, nucleus-membrane and cell-cell/cell-wall repulsion,
+IB spreading and the position update.
 
 One JSON line on rank 0:
-  value  MLUPS with populations resident in HBM, device-timed with CUDA
-         events on the stream the kernels run on (max over ranks)
-  e2e    the same metric through the C ABI with host buffers: every step
-         sets the uniform force from pinned host memory and reads the FP64
-         global mass back to the host
-  roofline, cpu_baseline, clocks, gpu_launches as described in DESIGN.md.
+  value   MLUPS of the coupled step with the state resident in HBM,
+          device-timed with CUDA events on the stream the kernels run on
+          (max over ranks); ``membrane_node_updates_per_s`` beside it
+  e2e     the same metric through the C ABI with host buffers: every step
+          sets the driving force from pinned host memory and reads the FP64
+          global mass back to the host (zf_set_uniform_force + zf_step_mass)
+  roofline  k_lbm's algorithmic bytes over its average launch time, taken
+          from per-launch CUDA events (zf_profile) in a second timed pass of
+          the same steps
+  storage_variants  the same measurement with fp16 / bf16 deviation storage
+  cpu_baseline  the CPU restatement of the reference time loop (oracle,
+          OpenMP, reference pass structure) on the host cores, one bounded
+          block of 50 steps
 
-``--impl reference`` times the CPU restatement of the reference algorithm
-(two LBM passes, FEQ store, F_OLD copy; OpenMP) on the host cores instead.
-Input data are synthetic (seeded geometry); there is no dataset.
+``--impl reference`` times that CPU restatement alone, as the reference arm.
+Input data are synthetic (seeded geometry and cells); there is no dataset.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -36,32 +49,46 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 WORKLOADS = {
-    # name: (nx, ny, nz, Rp, Rd, half_angle, g)
-    "bifurcation_256x256x1024": (256, 256, 1024, 30.0, 22.0, 20.0, 2e-6),
-    "bifurcation_x2_256x256x1024": (256, 256, 1024, 60.0, 44.0, 20.0, 2e-6),
-    "bifurcation_small_128x96x256": (128, 96, 256, 15.0, 11.0, 20.0, 2e-6),
+    # name: (nx, ny, nz, Rp, Rd, half_angle_deg, g, cells)
+    "c1_bifurcation_256x256x1024_2000rbc": (256, 256, 1024, 30.0, 22.0, 20.0, 2e-6, 2000),
+    "bifurcation_small_128x96x256_60rbc": (128, 96, 256, 15.0, 11.0, 20.0, 2e-6, 60),
 }
-BYTES_PER_LUP = {0: 152, 1: 76, 2: 76, 3: 152}  # 2*19*S, S = bytes per stored population
+DX_UM = 0.5
+AXES_UM = (3.5, 2.25, 1.0)        # 7, 4.5, 2 lattice units
+AXES_N_UM = (1.25, 0.9, 0.6)      # 2.5, 1.8, 1.2 lattice units
+# placement margin (um) around each cell's ellipsoid: adjacent cells start
+# about 1 um apart, outside the reference's repulsion range, so that no cell
+# starts inside another's repulsion zone
+PLACEMENT_MARGIN_UM = 0.4
+STORAGES = {"f32": 0, "f16": 1, "bf16": 2, "f32dev": 3}
+BYTES_PER_POP = {0: 4, 1: 2, 2: 2, 3: 4}
 DTYPE_NAME = {0: "f32", 1: "f16-storage/f32-math", 2: "bf16-storage/f32-math",
               3: "f32-deviation-storage/f32-math"}
 
 
+def lbm_bytes_per_point(storage: int, membrane_step: bool) -> int:
+    """Algorithmic DRAM bytes of one k_lbm fluid-point update: 19 populations
+    read and written, the 3 body-force components read; on membrane steps the
+    4 moments written and the 3 force components cleared as well."""
+    b = 2 * 19 * BYTES_PER_POP[storage] + 12
+    if membrane_step:
+        b += 16 + 12
+    return b
+
+
 def read_peaks():
-    for path in (os.path.join(ROOT, "MEASURED_PEAKS.json"),):
-        try:
-            with open(path) as fh:
-                pk = json.load(fh)
-            return float(pk["hbm_gbs"]), "measured"
-        except Exception:
-            pass
-    return 6650.0, "fallback"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            pk = json.load(fh)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
 
 
 def read_traffic(workload, storage):
     """DRAM bytes per fluid-point update of k_lbm from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_lbm_traffic.json")
     try:
-        with open(path) as fh:
+        with open(os.path.join(ROOT, "profiles", "k_lbm_traffic.json")) as fh:
             d = json.load(fh)
         return float(d[DTYPE_NAME[storage]]["dram_bytes_per_fluid_point"])
     except Exception:
@@ -106,7 +133,7 @@ class ClockSampler:
             self.proc.kill()
         if self.t:
             self.t.join(timeout=2)
-        sm, smax, reasons = [], [], set()
+        sm, smax, power, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
@@ -115,6 +142,7 @@ class ClockSampler:
             try:
                 sm.append(float(parts[1]))
                 smax.append(float(parts[2]))
+                power.append(float(parts[3]))
             except ValueError:
                 continue
             for nm, v in zip(names, parts[5:9]):
@@ -122,6 +150,7 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
+                "power_w_median": statistics.median(power) if power else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
@@ -132,71 +161,124 @@ def dist_setup():
     return world, rank, local
 
 
-def build_geometry(name):
-    import zebraflow_b200 as zf
-    nx, ny, nz, Rp, Rd, ang, g = WORKLOADS[name]
-    b, layout = zf.gen_bifurcation(nx, ny, nz, Rp, Rd, ang)
-    return b, (nx, ny, nz, Rp, Rd, ang, g), layout
+class Case:
+    """Seeded geometry of one workload: lattice, wall mesh, cell meshes, cells."""
+
+    def __init__(self, name, n_cells=None, seed=2024):
+        import zebraflow_b200 as zf
+        nx, ny, nz, Rp, Rd, ang, g, nc = WORKLOADS[name]
+        if n_cells is None:
+            n_cells = nc
+        self.name, self.dims, self.g, self.seed = name, (nx, ny, nz), g, seed
+        self.b, _ = zf.gen_bifurcation(nx, ny, nz, Rp, Rd, ang)
+        self.n_fluid = int((self.b > 0).sum())
+        self.mesh = self.cells = self.wall = None
+        self.n_cells = 0
+        if n_cells > 0:
+            self.wall = zf.gen_wall_bifurcation(nx, ny, nz, Rp, Rd, ang, dx=DX_UM)
+            xyz, tri = zf.gen_icosphere(3)
+            xyzn, trin = zf.gen_icosphere(2)
+            rest = xyz * np.array(AXES_UM)
+            rest_n = xyzn * np.array(AXES_N_UM)
+            self.mesh = (rest, tri, rest_n, zf.mesh_edges(trin))
+            self.cells = zf.gen_cells(self.b, n_cells, rest, rest_n, AXES_UM, seed=seed, dx=DX_UM,
+                                      margin=PLACEMENT_MARGIN_UM)
+            self.n_requested = n_cells
+            self.n_cells = self.cells[0].shape[1]
+            self.nn, self.nnn = rest.shape[0], rest_n.shape[0]
+            vol_cell = 4.0 / 3.0 * np.pi * np.prod(np.array(AXES_UM) / DX_UM)
+            self.hematocrit = self.n_cells * vol_cell / self.n_fluid
+
+    def params(self, storage: int):
+        import zebraflow_b200 as zf
+        nx, ny, nz = self.dims
+        return zf.default_params(nx=nx, ny=ny, nz=nz, tau=0.9, tau_from_phase=0,
+                                 wall_mode=zf.WALL_HALFWAY_BB, periodic=(0, 0, 1), storage=storage,
+                                 g=(0.0, 0.0, self.g), origin=(0.0, 0.0, 0.0), dx=DX_UM,
+                                 area0=0.0, volume0=0.0)
+
+    def config(self, storage_name, world):
+        c = {"workload": self.name, "lattice": "x".join(map(str, self.dims)),
+             "fluid_points": self.n_fluid, "wall": "halfway bounce-back", "tau": 0.9,
+             "g": self.g, "storage": storage_name,
+             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+             "l2": "inputs larger than L2"}
+        if self.n_cells:
+            c.update({"cells": self.n_cells, "cells_requested": self.n_requested,
+                      "placement_margin_um": PLACEMENT_MARGIN_UM,
+                      "membrane_nodes": self.nn, "nucleus_nodes": self.nnn,
+                      "hematocrit": round(float(self.hematocrit), 3), "stagger": 50,
+                      "wall_mesh_triangles": int(self.wall[1].shape[1]), "seed": self.seed,
+                      "moduli": "reference SI constants"})
+        return c
+
+    def oracle_world(self, precision="f32"):
+        """The CPU restatement of the reference loop on the same inputs."""
+        from oracle.bind import OracleCells, OracleLBM, OracleWorld
+        p = self.params(0)
+        lbm = OracleLBM(self.b, wall_mode=0, periodic=(0, 0, 1), tau=0.9, g=(0.0, 0.0, self.g),
+                        precision=precision, faithful=True)
+        if not self.n_cells:
+            return lbm, None, None
+        oc = OracleCells(*self.mesh, p, precision=precision)
+        oc.set_cells(*self.cells)
+        w = OracleWorld(lbm, oc, p)
+        w.set_wall(*self.wall)
+        return lbm, oc, w
 
 
-def cpu_reference_time(b, dims, storage, max_seconds=15.0, threads=None):
-    """Times the reference-faithful CPU restatement (oracle port, fp32) on the
-    host cores: returns (MLUPS, cores, sample description)."""
-    if threads:
-        os.environ["OMP_NUM_THREADS"] = str(threads)
-    from oracle.bind import OracleLBM
-    nx, ny, nz, Rp, Rd, ang, g = dims
-    o = OracleLBM(b, wall_mode=0, periodic=(0, 0, 1), tau=0.9, g=(0, 0, g), precision="f32",
-                  faithful=True)
-    n_fluid = int((b > 0).sum())
-    o.time_steps(2)  # warm-up (first touch of the arrays)
-    steps, spent = 0, 0.0
-    per = max(1, int(o.time_steps(1) > 0))
-    t_budget = max_seconds
-    while spent < t_budget:
-        dt = o.time_steps(per)
-        steps += per
-        spent += dt
-        if dt < 0.5:
-            per *= 2
-    o.close()
-    mlups = n_fluid * steps / spent / 1e6
-    return mlups, steps, spent
+def oracle_threads():
+    from oracle.bind import lib as olib
+    try:
+        return int(olib().orc_max_threads())
+    except Exception:
+        return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+def time_oracle(case, max_seconds, max_steps, stagger=50):
+    """Times the CPU restatement: 3 LBM warm-up steps, then whole blocks of the
+    time loop (each ending in a membrane iteration) until max_seconds or
+    max_steps.  Returns (steps, membrane_steps, seconds)."""
+    lbm, oc, w = case.oracle_world()
+    run = (lambda n: w.step(n)) if w is not None else (lambda n: lbm.time_steps(n))
+    run(3)
+    it, steps, mem, spent = 3, 0, 0, 0.0
+    while True:
+        n = stagger - it % stagger
+        if steps > 0 and (spent >= max_seconds or steps + n > max_steps):
+            break
+        t0 = time.perf_counter()
+        run(n)
+        spent += time.perf_counter() - t0
+        it += n
+        steps += n
+        mem += 1 if w is not None else 0
+    for o in (w, oc, lbm):
+        if o is not None:
+            o.close()
+    return steps, mem, spent
 
 
 def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
         return 0
-    threads = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    b, dims, _ = build_geometry(args.workload)
-    n_fluid = int((b > 0).sum())
-    from oracle.bind import OracleLBM
-    nx, ny, nz, Rp, Rd, ang, g = dims
-    o = OracleLBM(b, wall_mode=0, periodic=(0, 0, 1), tau=0.9, g=(0, 0, g), precision="f32",
-                  faithful=True)
-    for _ in range(min(args.warmup, 5)):
-        o.time_steps(1)
-    # each step is the full workload; the number of timed steps is bounded so
-    # the run stays within about two minutes of host time
-    t1 = o.time_steps(1)
-    nsteps = max(1, min(args.steps, int(120.0 / max(t1, 1e-6))))
-    times = [o.time_steps(1) for _ in range(nsteps)]
-    o.close()
-    t = sum(times)
-    mlups = n_fluid * nsteps / t / 1e6
+    case = Case(args.workload, args.cells, args.seed)
+    steps, mem, t = time_oracle(case, args.reference_seconds, args.steps)
+    mlups = case.n_fluid * steps / t / 1e6
+    cores = oracle_threads()
+    nodes = case.n_cells * (case.nn + case.nnn) if case.n_cells else 0
     line = {
         "impl": "reference", "metric": "MLUPS", "value": round(mlups, 3), "unit": "MLUPS",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(1e3 * t / nsteps, 3), "higher_is_better": True,
+        "ms_per_step": round(1e3 * t / steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "fluid_points": n_fluid, "wall": "halfway bounce-back",
-                   "storage": "f32", "parallelism": "host OpenMP"},
-        "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": int(os.environ["OMP_NUM_THREADS"]),
-                         "kind": "port",
-                         "sample": f"{nsteps} full LBM steps of the workload (of {args.steps} asked; "
-                                   f"bounded to ~2 min of host time)"},
+        "membrane_node_updates_per_s": round(nodes * mem / t, 1),
+        "config": dict(case.config("f32", 1), parallelism=f"host OpenMP x{cores}"),
+        "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": cores, "kind": "port",
+                         "sample": f"{steps} steps ({mem} with the membrane/IB block) of the workload "
+                                   f"after 3 warm-up steps, of {args.steps} asked; bounded to "
+                                   f"~{args.reference_seconds:.0f} s of host time"},
         "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -204,147 +286,220 @@ def run_reference(args):
     return 0
 
 
+def membrane_steps_in(it0, n, stagger):
+    return (it0 + n) // stagger - it0 // stagger
+
+
+def measure_storage(case, storage, args, dev, stream, barrier, sample_clocks=False):
+    """Warm-up, timed pass, profiled pass (per-launch events) and the e2e pass
+    for one storage form.  Returns a dict of raw figures."""
+    import torch
+    import zebraflow_b200 as zf
+
+    ctx = zf.Context(case.params(storage), device=dev)
+    ctx.set_lattice(case.b)
+    if case.n_cells:
+        ctx.set_wall(*case.wall)
+        ctx.set_mesh(*case.mesh)
+        ctx.set_cells(*case.cells)
+    ctx.set_stream(stream.cuda_stream)
+    stagger = ctx.params.stagger
+
+    ctx.step(args.warmup)
+    barrier()
+    sampler = ClockSampler(dev) if sample_clocks else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    it0 = ctx.iteration()
+    l0 = ctx.launch_count()
+    barrier()
+    ev0.record(stream)
+    ctx.step(args.steps)
+    ev1.record(stream)
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launch_count() - l0
+    clocks = sampler.stop() if sampler else None
+    n_mem = membrane_steps_in(it0, args.steps, stagger) if case.n_cells else 0
+    st = ctx.status()
+    removed = int(st.cells_removed)
+
+    # second pass with per-launch events: k_lbm's device time
+    it1 = ctx.iteration()
+    ctx.profile(True, args.steps + 8)
+    barrier()
+    ev0.record(stream)
+    ctx.step(args.steps)
+    ev1.record(stream)
+    barrier()
+    ms_prof = ev0.elapsed_time(ev1)
+    lbm_ms, lbm_n, mem_ms, mem_n = ctx.profile_read()
+    ctx.profile(False)
+    n_mem_prof = membrane_steps_in(it1, args.steps, stagger) if case.n_cells else 0
+
+    # end to end through the C ABI with host buffers
+    gh = torch.tensor([0.0, 0.0, case.g], dtype=torch.float32).pin_memory()
+    gptr = ctypes.cast(gh.data_ptr(), ctypes.POINTER(ctypes.c_float))
+    mass = ctypes.c_double()
+    L = zf.lib()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        L.zf_set_uniform_force(ctx._h, gptr)
+        rc = L.zf_step_mass(ctx._h, ctypes.byref(mass))
+        if rc:
+            raise zf.ZfError(rc, L.zf_last_error().decode())
+    barrier()
+    ms_e2e = 1e3 * (time.perf_counter() - t0)
+    removed_end = int(ctx.status().cells_removed)
+    ctx.set_stream(None)
+    ctx.close()
+    return {"ms": ms, "launches": launches, "clocks": clocks, "n_mem": n_mem, "removed": removed,
+            "removed_end": removed_end, "ms_prof": ms_prof, "lbm_ms": lbm_ms, "lbm_n": lbm_n,
+            "mem_ms": mem_ms, "mem_n": mem_n, "n_mem_prof": n_mem_prof, "ms_e2e": ms_e2e,
+            "mass": mass.value}
+
+
+def summarize(case, storage, r, steps, world, peak):
+    n = case.n_fluid
+    out = {"mlups": world * n * steps / (r["ms"] * 1e-3) / 1e6,
+           "ms_per_step": r["ms"] / steps,
+           "mlups_e2e": world * n * steps / (r["ms_e2e"] * 1e-3) / 1e6}
+    nodes = case.n_cells * (case.nn + case.nnn) if case.n_cells else 0
+    out["membrane_node_updates_per_s"] = world * nodes * r["n_mem"] / (r["ms"] * 1e-3)
+    # k_lbm roofline from the profiled pass: algorithmic bytes of all launches
+    # over their summed device time
+    nm = r["mem_n"]
+    alg = n * (lbm_bytes_per_point(storage, False) * (r["lbm_n"] - nm)
+               + lbm_bytes_per_point(storage, True) * nm)
+    lbm_s = r["lbm_ms"] * 1e-3
+    out["k_lbm_ms"] = r["lbm_ms"] / max(r["lbm_n"], 1)
+    out["k_lbm_gbs"] = alg / lbm_s / 1e9 if lbm_s > 0 else None
+    out["k_lbm_frac"] = out["k_lbm_gbs"] / peak if out["k_lbm_gbs"] else None
+    out["membrane_block_ms"] = r["mem_ms"] / r["mem_n"] if r["mem_n"] else None
+    out["lbm_share"] = r["lbm_ms"] / r["ms_prof"] if r["ms_prof"] else None
+    return out
+
+
 def run_ours(args):
     world, rank, local = dist_setup()
     import torch
     import torch.distributed as dist
-    import zebraflow_b200 as zf
 
     if world > 1:
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
-
-    b, dims, layout = build_geometry(args.workload)
-    nx, ny, nz, Rp, Rd, ang, g = dims
-    storage = {"f32": zf.STORE_F32, "f16": zf.STORE_F16, "bf16": zf.STORE_BF16,
-               "f32dev": zf.STORE_F32_DEV}[args.storage]
-    p = zf.default_params(nx=nx, ny=ny, nz=nz, tau=0.9, tau_from_phase=0,
-                          wall_mode=zf.WALL_HALFWAY_BB, periodic=(0, 0, 1), storage=storage,
-                          g=(0.0, 0.0, g))
-    ctx = zf.Context(p, device=dev)
-    ctx.set_lattice(b)
-    n_fluid = ctx.n_fluid
     stream = torch.cuda.current_stream(dev)
-    zf.lib().zf_set_stream(ctx._h, C_void(stream.cuda_stream))
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    # warm-up (also develops the flow a little)
-    for _ in range(args.warmup):
-        ctx.lbm_step(store_moments=False)
-    barrier()
-
-    sampler = ClockSampler(dev) if rank == 0 else None
-    if sampler:
-        sampler.start()
-        time.sleep(0.3)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    barrier()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        ctx.lbm_step(store_moments=False)
-    ev1.record(stream)
-    barrier()
-    ms = ev0.elapsed_time(ev1)
-    clocks = sampler.stop() if sampler else None
-
-    # end-to-end through the C ABI with host buffers
-    gh = torch.tensor([0.0, 0.0, g], dtype=torch.float32).pin_memory()
-    import ctypes
-    mass = ctypes.c_double()
-    e2e_steps = max(1, min(args.steps, 50))
-    barrier()
-    t0 = time.perf_counter()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        zf.lib().zf_set_uniform_force(ctx._h, ctypes.cast(gh.data_ptr(), ctypes.POINTER(ctypes.c_float)))
-        rc = zf.lib().zf_lbm_step_mass(ctx._h, 0, 0, ctypes.byref(mass))
-        if rc:
-            raise zf.ZfError(rc, zf.lib().zf_last_error().decode())
-    e1.record(stream)
-    barrier()
-    wall_e2e = time.perf_counter() - t0
-    ms_e2e = max(e0.elapsed_time(e1), 1e3 * wall_e2e)
-    zf.lib().zf_set_stream(ctx._h, None)
-
-    # max over ranks
-    if world > 1:
-        t = torch.tensor([ms, ms_e2e], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e = float(t[0]), float(t[1])
-
-    mlups = world * n_fluid * args.steps / (ms * 1e-3) / 1e6
-    mlups_e2e = world * n_fluid * e2e_steps / (ms_e2e * 1e-3) / 1e6
+    case = Case(args.workload, args.cells, args.seed)
+    storage = STORAGES[args.storage]
     peak, peak_kind = read_peaks()
-    bytes_lup = BYTES_PER_LUP[storage]
-    achieved = n_fluid * bytes_lup / (ms * 1e-3 / args.steps) / 1e9
-    traffic = read_traffic(args.workload, storage)
 
-    result = None
+    main_r = measure_storage(case, storage, args, dev, stream, barrier, sample_clocks=(rank == 0))
+    variants = {}
+    for name in [v for v in args.variants.split(",") if v and v != args.storage]:
+        variants[name] = (STORAGES[name], measure_storage(case, STORAGES[name], args, dev, stream,
+                                                         barrier))
+
+    # max over ranks of every timed figure
+    def vmax(vals):
+        if world == 1:
+            return vals
+        t = torch.tensor(vals, dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return [float(x) for x in t]
+
+    for r in [main_r] + [v[1] for v in variants.values()]:
+        r["ms"], r["ms_e2e"], r["ms_prof"], r["lbm_ms"], r["mem_ms"] = vmax(
+            [r["ms"], r["ms_e2e"], r["ms_prof"], r["lbm_ms"], r["mem_ms"]])
+
     if rank == 0:
+        s = summarize(case, storage, main_r, args.steps, world, peak)
+        traffic = read_traffic(args.workload, storage)
         cpu = None
-        if not args.no_cpu_baseline:
-            threads = os.cpu_count() or 1
-            mlups_cpu, csteps, cspent = cpu_reference_time(b, dims, storage, max_seconds=args.cpu_seconds,
-                                                           threads=threads)
-            cpu = {"value": round(mlups_cpu, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
-                   "sample": f"{csteps} full LBM steps of the same workload (fp32, reference pass "
-                             f"structure) in {cspent:.1f} s"}
+        if not args.no_cpu_baseline and world == 1:
+            csteps, cmem, cspent = time_oracle(case, args.cpu_seconds, 10 ** 9)
+            cpu = {"value": round(case.n_fluid * csteps / cspent / 1e6, 3), "unit": "MLUPS",
+                   "cores": oracle_threads(), "kind": "port",
+                   "sample": f"{csteps} steps ({cmem} with the membrane/IB block) of the same "
+                             f"workload, fp32, reference pass structure, {cspent:.1f} s"}
+            if case.n_cells:
+                cpu["membrane_node_updates_per_s"] = round(
+                    case.n_cells * (case.nn + case.nnn) * cmem / cspent, 1)
+        vs = {}
+        for name, (sv, r) in variants.items():
+            v = summarize(case, sv, r, args.steps, world, peak)
+            vs[name] = {"dtype": DTYPE_NAME[sv], "value": round(v["mlups"], 1),
+                        "ms_per_step": round(v["ms_per_step"], 5),
+                        "ratio_to_" + args.storage: round(v["mlups"] / s["mlups"], 3),
+                        "membrane_node_updates_per_s": round(v["membrane_node_updates_per_s"], 1),
+                        "e2e": round(v["mlups_e2e"], 1),
+                        "k_lbm_ms": round(v["k_lbm_ms"], 5),
+                        "k_lbm_frac": round(v["k_lbm_frac"], 4) if v["k_lbm_frac"] else None,
+                        "cells_removed": r["removed_end"]}
+        alg_launch = case.n_fluid * lbm_bytes_per_point(storage, False)
         result = {
-            "metric": "MLUPS", "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": world,
+            "metric": "MLUPS", "value": round(s["mlups"], 1), "unit": "MLUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
+            "ms_per_step": round(s["ms_per_step"], 5), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": DTYPE_NAME[storage],
-            "data": "synthetic",
-            "config": {"workload": args.workload, "fluid_points": int(n_fluid),
-                       "wall": "halfway bounce-back", "tau": 0.9, "g": g,
-                       "storage": args.storage, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (populations %.0f MB per step)" % (n_fluid * bytes_lup / 1e6)},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                         "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": None if traffic is None else round(traffic * n_fluid),
+            "data": "synthetic (seeded vessel geometry, wall mesh and cell placement)",
+            "membrane_node_updates_per_s": round(s["membrane_node_updates_per_s"], 1),
+            "config": dict(case.config(args.storage, world),
+                           cells_removed=main_r["removed_end"]),
+            "roofline": {"bound": "hbm", "kernel": "k_lbm",
+                         "achieved": round(s["k_lbm_gbs"], 1) if s["k_lbm_gbs"] else None,
+                         "peak": peak, "unit": "GB/s",
+                         "frac": round(s["k_lbm_frac"], 4) if s["k_lbm_frac"] else None,
+                         "traffic": None if traffic is None else round(traffic * case.n_fluid),
                          "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": n_fluid * bytes_lup},
+                         "algorithmic_bytes_per_launch": alg_launch,
+                         "k_lbm_ms_per_launch": round(s["k_lbm_ms"], 5),
+                         "k_lbm_share_of_step": round(s["lbm_share"], 4) if s["lbm_share"] else None,
+                         "membrane_block_ms": round(s["membrane_block_ms"], 4)
+                         if s["membrane_block_ms"] else None},
+            "storage_variants": vs,
             "cpu_baseline": cpu,
-            "e2e": {"value": round(mlups_e2e, 1), "unit": "MLUPS", "h2d_bytes_per_step": 12,
+            "e2e": {"value": round(s["mlups_e2e"], 1), "unit": "MLUPS", "h2d_bytes_per_step": 12,
                     "d2h_bytes_per_step": 8},
-            "gpu_launches": args.steps,
-            "clocks": clocks,
+            "gpu_launches": main_r["launches"],
+            "clocks": main_r["clocks"],
         }
         print(json.dumps(result), flush=True)
-    ctx.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
 
 
-def C_void(ptr):
-    import ctypes
-    return ctypes.c_void_p(ptr)
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="bifurcation_256x256x1024", choices=sorted(WORKLOADS))
-    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f32dev"])
+    ap.add_argument("--workload", default="c1_bifurcation_256x256x1024_2000rbc",
+                    choices=sorted(WORKLOADS))
+    ap.add_argument("--cells", type=int, default=None, help="override the workload's cell count")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--storage", default="f32", choices=sorted(STORAGES))
+    ap.add_argument("--variants", default="f16,bf16",
+                    help="comma-separated storage forms measured beside --storage")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--reference-seconds", type=float, default=90.0)
     args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

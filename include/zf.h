@@ -377,14 +377,16 @@ int zf_gen_wall_bifurcation(int nx, int ny, int nz, double Rp, double Rd, double
  * ZebraflowWT.c:5297-5637): centres uniform over the fluid points of b
  * ([nx][ny][nz] B_index codes), orientations uniform, candidates rejected
  * when their ellipsoid (semi-axes `axes` um + margin) overlaps a placed one
- * or a membrane node comes within one lattice unit of a non-fluid point.
+ * or a membrane node has a non-fluid point in the lattice cube of half-width
+ * max(1, ceil(wall_clear / dx)) around it (wall_clear in um; 0 keeps one
+ * lattice unit of clearance).
  * rest [n_node][3] / rest_n [n_node_n][3] are the shapes (um) around their
  * centres; x [3][n_cells][n_node], xn [3][n_cells][n_node_n] receive um;
  * *placed the number placed (the first *placed cells are valid). */
 int zf_gen_cells(const int32_t* b, int nx, int ny, int nz, const double* origin, double dx,
                  int periodic_z, int n_cells, int n_node, const double* rest, int n_node_n,
-                 const double* rest_n, const double* axes, double margin, uint64_t seed,
-                 double* x, double* xn, int* placed);
+                 const double* rest_n, const double* axes, double margin, double wall_clear,
+                 uint64_t seed, double* x, double* xn, int* placed);
 
 #ifdef __cplusplus
 }

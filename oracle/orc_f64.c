@@ -6,3 +6,6 @@
 #include "orc_lbm.inc"
 #include "orc_cells.inc"
 #include "orc_ib.inc"
+
+/* threads the OpenMP loops of the oracle use */
+int orc_max_threads(void) { return omp_get_max_threads(); }

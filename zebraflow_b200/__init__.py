@@ -130,7 +130,7 @@ _SIGS = {
                                           C.c_int, C.c_int]),
     "zf_gen_cells": (C.c_int, [_i32p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, C.c_int,
                                C.c_int, C.c_int, _f64p, C.c_int, _f64p, _f64p, C.c_double,
-                               C.c_uint64, _f64p, _f64p, C.POINTER(C.c_int)]),
+                               C.c_double, C.c_uint64, _f64p, _f64p, C.POINTER(C.c_int)]),
 }
 
 
@@ -224,8 +224,11 @@ def gen_wall_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg=20.0, origin=(0.0, 0
 
 
 def gen_cells(b, n_cells, rest, rest_n, axes, seed=1234, origin=(0.0, 0.0, 0.0), dx=0.5,
-              periodic_z=True, margin=0.25):
-    """Seeded placement; returns (x [3][placed][n_node], xn [3][placed][n_node_n])."""
+              periodic_z=True, margin=0.25, wall_clear=0.0):
+    """Seeded placement; returns (x [3][placed][n_node], xn [3][placed][n_node_n]).
+    margin (um) inflates each cell's ellipsoid against the others; wall_clear
+    (um) is the least lattice (Chebyshev) distance of every membrane node
+    from a non-fluid point, at least one lattice unit."""
     b = np.ascontiguousarray(b, np.int32)
     nx, ny, nz = b.shape
     rest = np.ascontiguousarray(rest, np.float64)
@@ -236,7 +239,7 @@ def gen_cells(b, n_cells, rest, rest_n, axes, seed=1234, origin=(0.0, 0.0, 0.0),
     placed = C.c_int()
     _check(lib().zf_gen_cells(b.ravel(), nx, ny, nz, np.asarray(origin, np.float64), dx,
                               int(periodic_z), n_cells, nn_, rest.ravel(), nnn, rest_n.ravel(),
-                              np.asarray(axes, np.float64), margin, seed, x, xn,
+                              np.asarray(axes, np.float64), margin, wall_clear, seed, x, xn,
                               C.byref(placed)))
     k = placed.value
     x = x.reshape(3, n_cells, nn_)[:, :k, :].copy()

@@ -148,6 +148,12 @@ __global__ void k_ib_interp(IbArgs a, CellArgs c) {
   V[((size_t)2 * nc + cell) * n + node] += vz;
 
   // nearest wall triangle over the +-4 window, reference scan order
+  // (ZebraflowWT.c:8998-9053): the first candidate point (vertex or centroid of a triangle
+  // listed at a wall node) that reaches the window's minimum distance decides.
+  // Candidates that cannot reach it change nothing, so a wall node met again
+  // (its list repeats candidates already seen) is skipped, and so is a wall
+  // node whose candidates all lie farther than a distance some candidate of
+  // the window already reached: |node - m| - rad[m] > bound.
   if (a.nw == 0) return;
   const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
   const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
@@ -165,37 +171,63 @@ __global__ void k_ib_interp(IbArgs a, CellArgs c) {
   if (!any) return;
   float mindis = 1.5f;
   int triwall = -1;
+  // candidates of one wall node's list, in list order then v = 0..3
+  auto scan_list = [&](int nodewall, float& best, int& tbest) {
+    const int32_t* L = a.wntri + (size_t)(nodewall - 1) * (a.wcap + 1);
+    const int nl = L[0];
+    for (int l = 1; l <= nl; ++l) {
+      const int tri = L[l];
+      for (int v = 0; v < 4; ++v) {
+        float px, py, pz;
+        if (v < 3) {
+          const int wn = a.wtri[3 * tri + v];
+          px = a.wxyz[wn];
+          py = a.wxyz[a.nw + wn];
+          pz = a.wxyz[2 * a.nw + wn];
+        } else {
+          px = a.wcen[tri];
+          py = a.wcen[a.mt + tri];
+          pz = a.wcen[2 * a.mt + tri];
+        }
+        const float d = dist3(xp - px, yp - py, wrapd(zp - pz, a.LZ));
+        if (d < best) {
+          best = d;
+          tbest = tri;
+        }
+      }
+    }
+  };
+  // an upper bound of the window minimum: the node's own lattice point's list
+  float bound = 1.5f;
+  if (i0 >= i1 && i0 <= i2 && j0 >= j1 && j0 <= j2 && k0 >= k1 && k0 <= k2) {
+    const int64_t s = slot_of(a, i0, j0, wrapk(a, k0));
+    if (s >= 0 && a.windex[s] > 0) {
+      int unused = -1;
+      scan_list(a.windex[s], bound, unused);
+    }
+  }
+  int last = 0;
   for (int i = i1; i <= i2; ++i)
     for (int j = j1; j <= j2; ++j)
-      for (int k = k1; k <= k2; ++k) {
+      for (int k = k1; k <= k2;) {
+        // a run of points along z inside one tile
         const int kw = wrapk(a, k);
-        const int64_t s = slot_of(a, i, j, kw);
-        if (s < 0) continue;
-        const int nodewall = a.windex[s];
-        if (nodewall <= 0) continue;
-        const int32_t* L = a.wntri + (size_t)(nodewall - 1) * (a.wcap + 1);
-        const int nl = L[0];
-        for (int l = 1; l <= nl; ++l) {
-          const int tri = L[l];
-          for (int v = 0; v < 4; ++v) {
-            float px, py, pz;
-            if (v < 3) {
-              const int wn = a.wtri[3 * tri + v];
-              px = a.wxyz[wn];
-              py = a.wxyz[a.nw + wn];
-              pz = a.wxyz[2 * a.nw + wn];
-            } else {
-              px = a.wcen[tri];
-              py = a.wcen[a.mt + tri];
-              pz = a.wcen[2 * a.mt + tri];
-            }
-            const float d = dist3(xp - px, yp - py, wrapd(zp - pz, a.LZ));
-            if (d < mindis) {
-              mindis = d;
-              triwall = tri;
-            }
+        int run = min(k2 - k, 3 - (kw & 3));
+        if (a.per_z) run = min(run, a.nz - 1 - kw);
+        const int t = a.tile_map[((kw >> 2) * a.nty + (j >> 2)) * a.ntx + (i >> 2)];
+        if (t >= 0) {
+          const int64_t s0 = (int64_t)t * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (kw & 3);
+          for (int r = 0; r <= run; ++r) {
+            const int nodewall = a.windex[s0 + 16 * r];
+            if (nodewall <= 0 || nodewall == last) continue;
+            last = nodewall;
+            const int m = nodewall - 1;
+            const float dm = dist3(xp - a.wxyz[m], yp - a.wxyz[a.nw + m], wrapd(zp - a.wxyz[2 * a.nw + m], a.LZ));
+            if (dm - a.wrad[m] > fminf(bound, mindis) + 1e-4f) continue;
+            scan_list(nodewall, mindis, triwall);
           }
         }
+        k += run + 1;
       }
   if (triwall < 0) return;
   // signed distance to the plane of the wall triangle, repulsion, :9055-9077
@@ -220,8 +252,18 @@ __global__ void k_ib_interp(IbArgs a, CellArgs c) {
 
 // ---- cell list of triangle centroids ----------------------------------------
 
+// bin key of a population slot: the tile's 64 points with z fastest, so the
+// points of one (x, y) column of a tile have consecutive keys
+__device__ __forceinline__ int64_t bin_key(int64_t s) {
+  const int c = (int)(s & 63);
+  return (s & ~(int64_t)63) | (((c >> 4) & 3) + 4 * ((c >> 2) & 3) + 16 * (c & 3));
+}
+
 // bin of each triangle: the nearest listed lattice point within 1 um of its
-// centroid inside the reference window (:5857-5902), or -1
+// centroid inside the reference window (:5857-5902), or -1.  Only points
+// within 2 lattice units per axis can lie within 1 um (2 DX), and the first
+// minimum of the reference scan is the first minimum of any sub-scan in the
+// same order that holds every point within 1 um, so the scan covers +-2.
 __global__ void k_bin_assign(IbArgs a, CellArgs c, int32_t* tri_bin, int32_t* counts) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = c.n_cells;
@@ -236,9 +278,9 @@ __global__ void k_bin_assign(IbArgs a, CellArgs c, int32_t* tri_bin, int32_t* co
   else if (zp < a.Z0 || zp > a.Z0 + (a.nz - 1) * a.DX) return;
   const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
             k0 = lat_index(zp, a.Z0, a.DX);
-  const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
-  const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
-  const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
+  const int i1 = max(i0 - 2, 0), i2 = min(i0 + 2, a.nx - 1);
+  const int j1 = max(j0 - 2, 0), j2 = min(j0 + 2, a.ny - 1);
+  const int k1 = a.per_z ? k0 - 2 : max(k0 - 2, 2), k2 = a.per_z ? k0 + 2 : min(k0 + 2, a.nz - 4);
   float mindis = 5000.f;
   int64_t best = -1;
   for (int i = i1; i <= i2; ++i)
@@ -259,8 +301,9 @@ __global__ void k_bin_assign(IbArgs a, CellArgs c, int32_t* tri_bin, int32_t* co
         }
       }
   if (best < 0 || !(mindis < 1.f)) return;
-  tri_bin[g] = (int32_t)best;
-  atomicAdd(&counts[best], 1);
+  const int64_t key = bin_key(best);
+  tri_bin[g] = (int32_t)key;
+  atomicAdd(&counts[key], 1);
 }
 
 // exclusive scan of counts[0..n) into off[0..n], three passes
@@ -319,6 +362,33 @@ __global__ void k_bin_sort(const int32_t* off, int64_t ns, int32_t* bin_tri) {
     }
     bin_tri[j + 1] = v;
   }
+}
+
+// per bin entry: centroid and bounding radius, normal and triangle id, so the
+// repulsion search reads one contiguous range of 32-byte records per run of
+// bins.  The radius bounds the distance from the centroid to any point of the
+// triangle (the vertices, as float), with a margin for float rounding.
+__global__ void k_bin_records(IbArgs a, CellArgs c, const int32_t* total) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= *total) return;
+  const int nc = c.n_cells;
+  const int g = a.bin_tri[e];
+  const int m = g / c.nt, tri = g - m * c.nt;
+  const float cx = c.tri_c[((size_t)0 * nc + m) * c.nt + tri];
+  const float cy = c.tri_c[((size_t)1 * nc + m) * c.nt + tri];
+  const float cz = c.tri_c[((size_t)2 * nc + m) * c.nt + tri];
+  float r2 = 0.f;
+  for (int v = 0; v < 3; ++v) {
+    const int n = c.tri[3 * tri + v];
+    const float dx = (float)c.x[((size_t)0 * nc + m) * c.nn + n] - cx;
+    const float dy = (float)c.x[((size_t)1 * nc + m) * c.nn + n] - cy;
+    const float dz = (float)c.x[((size_t)2 * nc + m) * c.nn + n] - cz;
+    r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
+  }
+  a.bin_c[e] = make_float4(cx, cy, cz, sqrtf(r2) * 1.0001f + 1e-3f);
+  a.bin_n[e] = make_float4(c.tri_nrm[((size_t)0 * nc + m) * c.nt + tri],
+                           c.tri_nrm[((size_t)1 * nc + m) * c.nt + tri],
+                           c.tri_nrm[((size_t)2 * nc + m) * c.nt + tri], __int_as_float(g));
 }
 
 // ---- nucleus-membrane repulsion --------------------------------------------
@@ -430,31 +500,37 @@ __global__ void k_rbc_rbc(IbArgs a, CellArgs c) {
   const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
   const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
   const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
+  const int64_t n_pop_tiles = a.ns / ZF_TC;
   float rx = 0.f, ry = 0.f, rz = 0.f;
   for (int i = i1; i <= i2; ++i)
     for (int j = j1; j <= j2; ++j)
-      for (int k = k1; k <= k2; ++k) {
+      for (int k = k1; k <= k2;) {
+        // the bins of a run of points along z inside one tile: one range
         const int kw = a.per_z ? ((k % a.nz) + a.nz) % a.nz : k;
-        const int64_t s = slot_of(a, i, j, kw);
-        if (s < 0 || s >= a.ns) continue;
-        const int b0 = a.bin_off[s], b1 = a.bin_off[s + 1];
-        for (int e = b0; e < b1; ++e) {
-          const int g = a.bin_tri[e];
+        int run = min(k2 - k, 3 - (kw & 3));
+        if (a.per_z) run = min(run, a.nz - 1 - kw);
+        const int t = a.tile_map[((kw >> 2) * a.nty + (j >> 2)) * a.ntx + (i >> 2)];
+        k += run + 1;
+        if (t < 0 || t >= n_pop_tiles) continue;
+        const int64_t key = (int64_t)t * ZF_TC + 16 * (i & 3) + 4 * (j & 3) + (kw & 3);
+        const int e0 = a.bin_off[key], e1 = a.bin_off[key + run + 1];
+        for (int e = e0; e < e1; ++e) {
+          // centroid within 2 um (ZebraflowWT.c:9978), then only triangles one of whose
+          // sub-centroids can lie within 1 um contribute
+          const float4 cr = a.bin_c[e];
+          const float dzc = wrapd(cr.z - zc, a.LZ);
+          const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
+          if (!(dcen < 2.f) || dcen - cr.w > 1.f) continue;
+          const float4 nr = a.bin_n[e];
+          const float dot = e1v[0] * nr.x + e1v[1] * nr.y + e1v[2] * nr.z;
+          if (!(dot < 0.f)) continue;
+          const int g = __float_as_int(nr.w);
           const int m = g / c.nt, tri = g - m * c.nt;
           const int n1 = c.tri[3 * tri], n2 = c.tri[3 * tri + 1], n3 = c.tri[3 * tri + 2];
           if (m == cell && (n1 == node || n2 == node || n3 == node)) continue;
-          const float e2v[3] = {c.tri_nrm[((size_t)0 * nc + m) * c.nt + tri],
-                                c.tri_nrm[((size_t)1 * nc + m) * c.nt + tri],
-                                c.tri_nrm[((size_t)2 * nc + m) * c.nt + tri]};
-          const float dot = e1v[0] * e2v[0] + e1v[1] * e2v[1] + e1v[2] * e2v[2];
-          if (!(dot < 0.f)) continue;
-          const float px = c.tri_c[((size_t)0 * nc + m) * c.nt + tri];
-          const float py = c.tri_c[((size_t)1 * nc + m) * c.nt + tri];
-          const float pzr = c.tri_c[((size_t)2 * nc + m) * c.nt + tri];
-          const float dzc = wrapd(pzr - zc, a.LZ);
-          const float shift = (pzr - zc) - dzc;  // periodic image of the other cell
-          if (!(dist3(xc - px, yc - py, -dzc) < 2.f)) continue;
+          const float shift = (cr.z - zc) - dzc;  // periodic image of the other cell
           float tp[16][3], tc[17][3];
+#pragma unroll
           for (int v = 0; v < 3; ++v) {
             const float off = v == 2 ? shift : 0.f;
             tp[1][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n1] - off;
@@ -489,6 +565,7 @@ __global__ void k_rbc_rbc(IbArgs a, CellArgs c) {
             tc[15][v] = (tp[15][v] + tp[5][v] + tp[10][v]) / 3.f;
             tc[16][v] = (tp[11][v] + tp[10][v] + tp[3][v]) / 3.f;
           }
+#pragma unroll
           for (int v = 1; v <= 16; ++v) {
             const float dx = tc[v][0] - xc, dy = tc[v][1] - yc, dz = tc[v][2] - zc;
             const float d = dist3(dx, dy, dz);
@@ -644,6 +721,7 @@ int ib_bins_launch(zf_ctx* ctx) {
                                                                        const_cast<int32_t*>(a.bin_tri));
   k_bin_sort<<<(unsigned)((a.ns + 255) / 256), 256, 0, ctx->stream>>>(off, a.ns,
                                                                        const_cast<int32_t*>(a.bin_tri));
+  k_bin_records<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(a, c, off + a.ns);
   ZF_CUDA(cudaGetLastError());
   return ZF_OK;
 }

@@ -119,9 +119,10 @@ int build_view(zf_ctx* c, const WallHost* W) {
     if ((rc = dalloc<float>(c, own, const_cast<float**>(&a.wcen), W->cen.size(), W->cen.data()))) return rc;
     if ((rc = dalloc<int32_t>(c, own, const_cast<int32_t**>(&a.wntri), W->ntri.size(), W->ntri.data())))
       return rc;
+    if ((rc = dalloc<float>(c, own, const_cast<float**>(&a.wrad), W->rad.size(), W->rad.data()))) return rc;
   } else {
     a.nw = a.mt = a.wcap = 0;
-    a.wxyz = a.wnrm = a.wcen = nullptr;
+    a.wxyz = a.wnrm = a.wcen = a.wrad = nullptr;
     a.wtri = a.wntri = nullptr;
   }
   ZF_CUDA(cudaStreamSynchronize(c->stream));
@@ -142,6 +143,8 @@ int ib_buffers(zf_ctx* c) {
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &buf, 2 * nscan + ntri + nb + 1))) return rc;
   a.bin_off = buf;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, const_cast<int32_t**>(&a.bin_tri), ntri))) return rc;
+  if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_c, ntri))) return rc;
+  if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_n, ntri))) return rc;
   a.nuc_cap = std::max(1, c->p.nuc_list_max);
   const int64_t nnuc = (int64_t)cl.n_cells * cl.nnn;
   if ((rc = dalloc<uint16_t>(c, c->ib_allocs, &a.nuc_list, nnuc * a.nuc_cap))) return rc;
@@ -306,8 +309,8 @@ static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
         ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (2 * c->prof_cap + c->prof_mem) + 1], c->stream));
         c->prof_mem++;
       }
-      // k_membrane, k_ib_interp, k_nuc_memb, 7 cell-list kernels, k_rbc_rbc,
-      // k_ib_spread, k_update
+      // k_membrane, k_ib_interp, k_nuc_memb, 7 cell-list kernels (assign, 3
+      // scan passes, fill, sort, records), k_rbc_rbc, k_ib_spread, k_update
       c->launches += 13;
     }
     c->status.iter = iter;

@@ -113,6 +113,8 @@ struct WallHost {
   std::vector<int32_t> tri;      // [mt][3] 0-based
   std::vector<float> nrm, cen;   // [3][mt]
   std::vector<int32_t> ntri;     // [nw][cap+1]: count, triangles (0-based)
+  std::vector<float> rad;        // [nw] farthest vertex or centroid of the node's listed
+                                 // triangles from the node (um, rounded up)
   std::vector<int32_t> windex;   // [npts] 1-based wall node, 0 none
   std::vector<float> wdist;      // [npts]
   std::vector<VoidPoint> uvoid;  // non-zero void velocities
@@ -144,9 +146,14 @@ struct IbArgs {
   const float* wnrm;            // [3][mt]
   const float* wcen;            // [3][mt]
   const int32_t* wntri;         // [nw][wcap+1]
-  // cell list of triangle centroids over population slots (CSR)
+  const float* wrad;            // [nw] WallHost::rad
+  // cell list of triangle centroids over population slots (CSR).  Bin keys
+  // order the points of a tile with z fastest (bin_key), so the bins of a
+  // run of points along z are one contiguous range of entries.
   const int32_t* bin_off;       // [ns+1]
   const int32_t* bin_tri;       // [n_cells*nt] global triangle id = cell*nt + tri
+  float4* bin_c;                // [n_cells*nt] per entry: centroid xyz, bounding radius
+  float4* bin_n;                // [n_cells*nt] per entry: normal xyz, id (int bits)
   // constants
   float vel_scale, gamma_p;
   double force_scale;           // 1/(UNITMASS*LBM_BFORCE_SCALE)

@@ -11,6 +11,7 @@
 //    CGSM_FILAMENT_PARAMETERS :1930-2053, run `calib_passes` times (:2339-2346)
 //  - LMAX, rest dihedral angles: CGSM_EQUILIBRIUM_METRICS :2056-2223
 //  - rest triangle areas TRI_AREA_eq: :2387-2460
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -511,14 +512,15 @@ int zf_cgsm_forces(zf_ctx* c) {
 // units): centres uniform over fluid points, orientations uniform (random
 // unit quaternion), rejecting a candidate whose ellipsoid (semi-axes
 // `axes` um plus `margin` um) overlaps an accepted one on the lattice, or
-// any of whose membrane nodes has a non-fluid lattice point among its 27
-// nearest.  Outputs x [3][n_cells][n_node], xn [3][n_cells][n_node_n] in um.
+// any of whose membrane nodes has a non-fluid lattice point within the cube
+// of half-width r = max(1, ceil(wall_clear / dx)) around its nearest lattice
+// point.  Outputs x [3][n_cells][n_node], xn [3][n_cells][n_node_n] in um.
 // Returns the number placed in *placed (fewer than asked when the attempts
 // run out).
 int zf_gen_cells(const int32_t* b, int nx, int ny, int nz, const double* origin, double dx,
                  int periodic_z, int n_cells, int n_node, const double* rest, int n_node_n,
-                 const double* rest_n, const double* axes, double margin, uint64_t seed,
-                 double* x, double* xn, int* placed) {
+                 const double* rest_n, const double* axes, double margin, double wall_clear,
+                 uint64_t seed, double* x, double* xn, int* placed) {
   if (!b || !origin || !rest || !axes || !x || !placed || n_cells < 0 || dx <= 0) return ZF_ERR_ARG;
   uint64_t st = seed;
   auto next = [&]() {  // splitmix64
@@ -533,6 +535,50 @@ int zf_gen_cells(const int32_t* b, int nx, int ny, int nz, const double* origin,
     if (b[p] > 0) fluid.push_back(p);
   if (fluid.empty()) return ZF_ERR_ARG;
   std::vector<uint8_t> occ((size_t)nx * ny * nz, 0);
+  // clear[p] = 1 when every point of the cube of half-width r around p is
+  // fluid: the fluid mask eroded by a cube, one axis at a time (a point
+  // outside the box counts as non-fluid, except across a periodic z face)
+  const int r_clear = std::max(1, (int)std::ceil(wall_clear / dx - 1e-9));
+  std::vector<uint8_t> clear((size_t)nx * ny * nz);
+  for (int64_t p = 0; p < (int64_t)nx * ny * nz; ++p) clear[p] = b[p] > 0;
+  {
+    const int64_t stride[3] = {(int64_t)ny * nz, nz, 1};
+    const int len[3] = {nx, ny, nz};
+    for (int ax = 0; ax < 3; ++ax) {
+      const int L = len[ax];
+      const bool wrap = ax == 2 && periodic_z;
+      const int64_t nlines = (int64_t)nx * ny * nz / L;
+#pragma omp parallel
+      {
+        std::vector<int> bad((size_t)L + 1);
+        std::vector<uint8_t> line((size_t)L);
+#pragma omp for schedule(static)
+        for (int64_t l = 0; l < nlines; ++l) {
+          // base point of line l: the index with the axis coordinate zero
+          int64_t base;
+          if (ax == 0) base = l;                                    // l = j*nz + k
+          else if (ax == 1) base = (l / nz) * (int64_t)ny * nz + l % nz;  // l = i*nz + k
+          else base = l * nz;                                       // l = i*ny + j
+          for (int t = 0; t < L; ++t) line[t] = clear[base + t * stride[ax]];
+          bad[0] = 0;  // prefix counts of non-fluid points
+          for (int t = 0; t < L; ++t) bad[t + 1] = bad[t] + (line[t] ? 0 : 1);
+          const int total = bad[L];
+          for (int t = 0; t < L; ++t) {
+            int lo = t - r_clear, hi = t + r_clear, cnt;
+            if (wrap) {
+              if (2 * r_clear + 1 >= L) cnt = total;
+              else if (lo < 0) cnt = bad[hi + 1] + (total - bad[L + lo]);
+              else if (hi >= L) cnt = (total - bad[lo]) + bad[hi - L + 1];
+              else cnt = bad[hi + 1] - bad[lo];
+            } else {
+              cnt = (lo < 0 || hi >= L) ? 1 : bad[hi + 1] - bad[lo];
+            }
+            clear[base + t * stride[ax]] = cnt == 0;
+          }
+        }
+      }
+    }
+  }
   auto at = [&](int i, int j, int k) -> int64_t {
     if (i < 0 || i >= nx || j < 0 || j >= ny) return -1;
     if (k < 0 || k >= nz) {
@@ -543,65 +589,86 @@ int zf_gen_cells(const int32_t* b, int nx, int ny, int nz, const double* origin,
   };
   const double A[3] = {axes[0] + margin, axes[1] + margin, axes[2] + margin};
   const int reach = (int)std::ceil(std::max(A[0], std::max(A[1], A[2])) / dx) + 1;
-  int n_ok = 0;
-  const int64_t max_tries = 400LL * n_cells + 1000;
-  std::vector<int64_t> mark;
-  for (int64_t tries = 0; n_ok < n_cells && tries < max_tries; ++tries) {
-    const int64_t p = fluid[(size_t)(uni() * fluid.size()) % fluid.size()];
-    const double ci = (double)(p / ((int64_t)ny * nz)) + uni() - 0.5;
-    const double cj = (double)((p / nz) % ny) + uni() - 0.5;
-    const double ck = (double)(p % nz) + uni() - 0.5;
-    // uniform rotation (Shoemake)
-    const double u1 = uni(), u2 = uni(), u3 = uni();
-    const double qw = std::sqrt(1 - u1) * std::sin(2 * M_PI * u2), qx = std::sqrt(1 - u1) * std::cos(2 * M_PI * u2),
-                 qy = std::sqrt(u1) * std::sin(2 * M_PI * u3), qz = std::sqrt(u1) * std::cos(2 * M_PI * u3);
-    const double R[3][3] = {{1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qz * qw), 2 * (qx * qz + qy * qw)},
-                            {2 * (qx * qy + qz * qw), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qx * qw)},
-                            {2 * (qx * qz - qy * qw), 2 * (qy * qz + qx * qw), 1 - 2 * (qx * qx + qy * qy)}};
+  struct Cand {
+    double c[3];
+    double R[3][3];
+  };
+  // the whole candidate stream comes from the seed; a candidate is accepted
+  // when it fits against the cells accepted before it, so evaluating a batch
+  // in parallel against the occupancy at the start of the batch and then
+  // re-checking the survivors in order gives the sequential result
+  auto fits = [&](const Cand& cd, std::vector<int64_t>* mark) -> bool {
+    const double ci = cd.c[0], cj = cd.c[1], ck = cd.c[2];
+    const int64_t s0 = at((int)std::lround(ci), (int)std::lround(cj), (int)std::lround(ck));
+    if (s0 < 0 || occ[s0]) return false;
+    // every membrane node at least r lattice units (Chebyshev) from the wall
+    for (int n = 0; n < n_node; ++n) {
+      double pos[3];
+      for (int a = 0; a < 3; ++a)
+        pos[a] = cd.R[a][0] * rest[3 * n] + cd.R[a][1] * rest[3 * n + 1] + cd.R[a][2] * rest[3 * n + 2];
+      const int64_t s = at((int)std::lround(ci + pos[0] / dx), (int)std::lround(cj + pos[1] / dx),
+                           (int)std::lround(ck + pos[2] / dx));
+      if (s < 0 || !clear[s]) return false;
+    }
     // lattice points inside the inflated ellipsoid: free?
-    mark.clear();
-    bool ok = true;
-    for (int di = -reach; di <= reach && ok; ++di)
-      for (int dj = -reach; dj <= reach && ok; ++dj)
-        for (int dk = -reach; dk <= reach && ok; ++dk) {
+    for (int di = -reach; di <= reach; ++di)
+      for (int dj = -reach; dj <= reach; ++dj)
+        for (int dk = -reach; dk <= reach; ++dk) {
           const int i = (int)std::floor(ci) + di, j = (int)std::floor(cj) + dj, k = (int)std::floor(ck) + dk;
           const double v[3] = {(i - ci) * dx, (j - cj) * dx, (k - ck) * dx};
           double q[3];
-          for (int a = 0; a < 3; ++a) q[a] = R[0][a] * v[0] + R[1][a] * v[1] + R[2][a] * v[2];
+          for (int a = 0; a < 3; ++a) q[a] = cd.R[0][a] * v[0] + cd.R[1][a] * v[1] + cd.R[2][a] * v[2];
           const double e = q[0] * q[0] / (A[0] * A[0]) + q[1] * q[1] / (A[1] * A[1]) + q[2] * q[2] / (A[2] * A[2]);
           if (e > 1.0) continue;
           const int64_t s = at(i, j, k);
-          if (s < 0 || occ[s]) ok = false;
-          else mark.push_back(s);
+          if (s < 0 || occ[s]) return false;
+          if (mark) mark->push_back(s);
         }
-    if (!ok) continue;
-    // every membrane node at least one lattice unit from the wall
-    for (int n = 0; n < n_node && ok; ++n) {
-      double pos[3];
-      for (int a = 0; a < 3; ++a)
-        pos[a] = R[a][0] * rest[3 * n] + R[a][1] * rest[3 * n + 1] + R[a][2] * rest[3 * n + 2];
-      const int i = (int)std::lround(ci + pos[0] / dx), j = (int)std::lround(cj + pos[1] / dx),
-                k = (int)std::lround(ck + pos[2] / dx);
-      for (int di = -1; di <= 1 && ok; ++di)
-        for (int dj = -1; dj <= 1 && ok; ++dj)
-          for (int dk = -1; dk <= 1 && ok; ++dk) {
-            const int64_t s = at(i + di, j + dj, k + dk);
-            if (s < 0 || b[s] <= 0) ok = false;
-          }
+    return true;
+  };
+  int n_ok = 0;
+  const int64_t max_tries = 12000LL * n_cells + 1000;
+  const int64_t batch = 4096;
+  std::vector<Cand> cand((size_t)batch);
+  std::vector<uint8_t> pass((size_t)batch);
+  std::vector<int64_t> mark;
+  for (int64_t tries = 0; n_ok < n_cells && tries < max_tries; tries += batch) {
+    const int64_t nb = std::min(batch, max_tries - tries);
+    for (int64_t t = 0; t < nb; ++t) {
+      Cand& cd = cand[(size_t)t];
+      const int64_t p = fluid[(size_t)(uni() * fluid.size()) % fluid.size()];
+      cd.c[0] = (double)(p / ((int64_t)ny * nz)) + uni() - 0.5;
+      cd.c[1] = (double)((p / nz) % ny) + uni() - 0.5;
+      cd.c[2] = (double)(p % nz) + uni() - 0.5;
+      // uniform rotation (Shoemake)
+      const double u1 = uni(), u2 = uni(), u3 = uni();
+      const double qw = std::sqrt(1 - u1) * std::sin(2 * M_PI * u2), qx = std::sqrt(1 - u1) * std::cos(2 * M_PI * u2),
+                   qy = std::sqrt(u1) * std::sin(2 * M_PI * u3), qz = std::sqrt(u1) * std::cos(2 * M_PI * u3);
+      const double R[3][3] = {{1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qz * qw), 2 * (qx * qz + qy * qw)},
+                              {2 * (qx * qy + qz * qw), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qx * qw)},
+                              {2 * (qx * qz - qy * qw), 2 * (qy * qz + qx * qw), 1 - 2 * (qx * qx + qy * qy)}};
+      std::memcpy(cd.R, R, sizeof(R));
     }
-    if (!ok) continue;
-    for (int64_t s : mark) occ[s] = 1;
-    const double c0[3] = {origin[0] + ci * dx, origin[1] + cj * dx, origin[2] + ck * dx};
-    for (int n = 0; n < n_node; ++n)
-      for (int a = 0; a < 3; ++a)
-        x[((size_t)a * n_cells + n_ok) * n_node + n] =
-            c0[a] + R[a][0] * rest[3 * n] + R[a][1] * rest[3 * n + 1] + R[a][2] * rest[3 * n + 2];
-    if (xn && rest_n)
-      for (int n = 0; n < n_node_n; ++n)
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t t = 0; t < nb; ++t) pass[(size_t)t] = fits(cand[(size_t)t], nullptr);
+    for (int64_t t = 0; t < nb && n_ok < n_cells; ++t) {
+      if (!pass[(size_t)t]) continue;
+      const Cand& cd = cand[(size_t)t];
+      mark.clear();
+      if (!fits(cd, &mark)) continue;
+      for (int64_t s : mark) occ[s] = 1;
+      const double c0[3] = {origin[0] + cd.c[0] * dx, origin[1] + cd.c[1] * dx, origin[2] + cd.c[2] * dx};
+      for (int n = 0; n < n_node; ++n)
         for (int a = 0; a < 3; ++a)
-          xn[((size_t)a * n_cells + n_ok) * n_node_n + n] =
-              c0[a] + R[a][0] * rest_n[3 * n] + R[a][1] * rest_n[3 * n + 1] + R[a][2] * rest_n[3 * n + 2];
-    ++n_ok;
+          x[((size_t)a * n_cells + n_ok) * n_node + n] =
+              c0[a] + cd.R[a][0] * rest[3 * n] + cd.R[a][1] * rest[3 * n + 1] + cd.R[a][2] * rest[3 * n + 2];
+      if (xn && rest_n)
+        for (int n = 0; n < n_node_n; ++n)
+          for (int a = 0; a < 3; ++a)
+            xn[((size_t)a * n_cells + n_ok) * n_node_n + n] =
+                c0[a] + cd.R[a][0] * rest_n[3 * n] + cd.R[a][1] * rest_n[3 * n + 1] + cd.R[a][2] * rest_n[3 * n + 2];
+      ++n_ok;
+    }
   }
   *placed = n_ok;
   return ZF_OK;

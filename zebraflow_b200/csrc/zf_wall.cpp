@@ -73,6 +73,27 @@ int wall_build(zf_ctx* c, int nw, const float* xyz, int mt, const int32_t* tri1,
                       xyz[(size_t)a * nw + W.tri[3 * m + 2]];
       W.cen[(size_t)a * mt + m] = (float)(s / 3.);
     }
+  // bounding radius of each node's candidates (the vertices and centroids of
+  // its listed triangles): lets a search skip a node whose candidates are all
+  // farther than a distance already reached
+  W.rad.assign(nw, 0.f);
+  for (int n = 0; n < nw; ++n) {
+    const int32_t* L = &W.ntri[(size_t)n * (cap + 1)];
+    double r2 = 0.0;
+    for (int l = 1; l <= L[0]; ++l) {
+      const int t = L[l];
+      for (int v = 0; v < 4; ++v) {
+        double d2 = 0.0;
+        for (int a = 0; a < 3; ++a) {
+          const double q = v < 3 ? xyz[(size_t)a * nw + W.tri[3 * (size_t)t + v]] : W.cen[(size_t)a * mt + t];
+          const double e = q - xyz[(size_t)a * nw + n];
+          d2 += e * e;
+        }
+        r2 = std::max(r2, d2);
+      }
+    }
+    W.rad[n] = (float)(std::sqrt(r2) * (1.0 + 1e-6) + 1e-5);
+  }
   // W_index / Wdistance over the lattice box
   const int64_t npts = (int64_t)nx * ny * nz;
   W.windex.assign(npts, 0);
