@@ -27,6 +27,8 @@ namespace zf {
 namespace {
 
 constexpr float kPI = 3.14159265358979f;
+// warps per block of the queue-based search kernels
+constexpr int kRepWarps = 4;
 
 __device__ __forceinline__ float dist3(float dx, float dy, float dz) {
   return sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
@@ -146,89 +148,189 @@ __global__ void k_ib_interp(IbArgs a, CellArgs c) {
   V[((size_t)0 * nc + cell) * n + node] += vx;
   V[((size_t)1 * nc + cell) * n + node] += vy;
   V[((size_t)2 * nc + cell) * n + node] += vz;
+}
 
-  // nearest wall triangle over the +-4 window, reference scan order
-  // (ZebraflowWT.c:8998-9053): the first candidate point (vertex or centroid of a triangle
-  // listed at a wall node) that reaches the window's minimum distance decides.
-  // Candidates that cannot reach it change nothing, so a wall node met again
-  // (its list repeats candidates already seen) is skipped, and so is a wall
-  // node whose candidates all lie farther than a distance some candidate of
-  // the window already reached: |node - m| - rad[m] > bound.
-  if (a.nw == 0) return;
-  const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
-  const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
-  const int k1 = max(k0 - 4, a.kmin), k2 = min(k0 + 4, a.kmax);
-  // skip the scan when no tile of the window holds a point with W_index > 0
-  bool any = false;
-  for (int ti = i1 >> 2; ti <= (i2 >> 2) && !any; ++ti)
-    for (int tj = j1 >> 2; tj <= (j2 >> 2) && !any; ++tj)
-      for (int k = k1; k <= k2 && !any; ++k) {
-        if (k != k1 && (k & 3) != 0) continue;  // first point of each z tile
-        const int kw = wrapk(a, k);
-        const int t = a.tile_map[((kw >> 2) * a.nty + tj) * a.ntx + ti];
-        if (t >= 0 && a.tile_wall[t]) any = true;
+// Nearest wall triangle over the +-4 window in the reference scan order
+// (ZebraflowWT.c:8998-9053) and the wall repulsion (:9055-9077), one thread
+// per node as k_ib_interp.  The first candidate point (vertex or centroid of a
+// triangle listed at a wall node) that reaches the window's minimum decides,
+// so lists that cannot reach it change nothing: a wall node met again (same
+// candidates) is skipped, and so is one whose candidates all lie farther than
+// a distance some candidate of the window already reached
+// (|node - m| - rad[m] > bound).  Lanes walk their windows in lock-step and
+// queue the lists that remain; a batch scans 32 lists, one per lane, each
+// giving its first minimum, and the owner folds them in its scan order with a
+// strict <, which is the reference's running minimum taken list by list.
+__device__ __forceinline__ void wall_list_min(const IbArgs& a, int nodewall, float xp, float yp, float zp,
+                                              float& best, int& tbest) {
+  const int32_t* L = a.wntri + (size_t)(nodewall - 1) * (a.wcap + 1);
+  const int nl = L[0];
+  for (int l = 1; l <= nl; ++l) {
+    const int tri = L[l];
+    for (int v = 0; v < 4; ++v) {
+      float px, py, pz;
+      if (v < 3) {
+        const int wn = a.wtri[3 * tri + v];
+        px = a.wxyz[wn];
+        py = a.wxyz[a.nw + wn];
+        pz = a.wxyz[2 * a.nw + wn];
+      } else {
+        px = a.wcen[tri];
+        py = a.wcen[a.mt + tri];
+        pz = a.wcen[2 * a.mt + tri];
       }
-  if (!any) return;
-  float mindis = 1.5f;
-  int triwall = -1;
-  // candidates of one wall node's list, in list order then v = 0..3
-  auto scan_list = [&](int nodewall, float& best, int& tbest) {
-    const int32_t* L = a.wntri + (size_t)(nodewall - 1) * (a.wcap + 1);
-    const int nl = L[0];
-    for (int l = 1; l <= nl; ++l) {
-      const int tri = L[l];
-      for (int v = 0; v < 4; ++v) {
-        float px, py, pz;
-        if (v < 3) {
-          const int wn = a.wtri[3 * tri + v];
-          px = a.wxyz[wn];
-          py = a.wxyz[a.nw + wn];
-          pz = a.wxyz[2 * a.nw + wn];
-        } else {
-          px = a.wcen[tri];
-          py = a.wcen[a.mt + tri];
-          pz = a.wcen[2 * a.mt + tri];
-        }
-        const float d = dist3(xp - px, yp - py, wrapd(zp - pz, a.LZ));
-        if (d < best) {
-          best = d;
-          tbest = tri;
-        }
+      const float d = dist3(xp - px, yp - py, wrapd(zp - pz, a.LZ));
+      if (d < best) {
+        best = d;
+        tbest = tri;
       }
     }
-  };
+  }
+}
+
+__global__ void __launch_bounds__(kRepWarps * 32) k_ib_wall(IbArgs a, CellArgs c) {
+  __shared__ int sq_m[kRepWarps][64];
+  __shared__ unsigned char sq_l[kRepWarps][64];
+  __shared__ float sq_d[kRepWarps][32];
+  __shared__ int sq_t[kRepWarps][32];
+  const unsigned FULL = 0xffffffffu;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  const int64_t nmem = (int64_t)nc * c.nn;
+  const bool nuc = gid >= nmem;
+  bool active = gid < nmem + (int64_t)nc * c.nnn;
+  const int n = nuc ? c.nnn : c.nn;
+  const int64_t lid = nuc ? gid - nmem : gid;
+  int cell = 0, node = 0;
+  if (active) {
+    cell = (int)(lid / n);
+    node = (int)(lid % n);
+    active = c.status[cell] > 0;
+  }
+  float xp = 0.f, yp = 0.f, zp = 0.f;
+  int i0 = 0, j0 = 0, k0 = 0, i1 = 0, i2 = -1, j1 = 0, j2 = -1, k1 = 0, k2 = -1;
+  if (active) {
+    node_pos(nuc ? c.xn : c.x, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
+    i0 = lat_index(xp, a.X0, a.DX);
+    j0 = lat_index(yp, a.Y0, a.DX);
+    k0 = lat_index(zp, a.Z0, a.DX);
+    i1 = max(i0 - 4, 0);
+    i2 = min(i0 + 4, a.nx - 1);
+    j1 = max(j0 - 4, 0);
+    j2 = min(j0 + 4, a.ny - 1);
+    k1 = max(k0 - 4, a.kmin);
+    k2 = min(k0 + 4, a.kmax);
+    // skip the walk when no tile of the window holds a point with W_index > 0
+    bool any = false;
+    for (int ti = i1 >> 2; ti <= (i2 >> 2) && !any; ++ti)
+      for (int tj = j1 >> 2; tj <= (j2 >> 2) && !any; ++tj)
+        for (int k = k1; k <= k2 && !any; ++k) {
+          if (k != k1 && (k & 3) != 0) continue;  // first point of each z tile
+          const int kw = wrapk(a, k);
+          const int t = a.tile_map[((kw >> 2) * a.nty + tj) * a.ntx + ti];
+          if (t >= 0 && a.tile_wall[t]) any = true;
+        }
+    active = any;
+  }
   // an upper bound of the window minimum: the node's own lattice point's list
   float bound = 1.5f;
-  if (i0 >= i1 && i0 <= i2 && j0 >= j1 && j0 <= j2 && k0 >= k1 && k0 <= k2) {
+  if (active && i0 >= i1 && i0 <= i2 && j0 >= j1 && j0 <= j2 && k0 >= k1 && k0 <= k2) {
     const int64_t s = slot_of(a, i0, j0, wrapk(a, k0));
     if (s >= 0 && a.windex[s] > 0) {
       int unused = -1;
-      scan_list(a.windex[s], bound, unused);
+      wall_list_min(a, a.windex[s], xp, yp, zp, bound, unused);
     }
   }
-  int last = 0;
-  for (int i = i1; i <= i2; ++i)
-    for (int j = j1; j <= j2; ++j)
-      for (int k = k1; k <= k2;) {
-        // a run of points along z inside one tile
-        const int kw = wrapk(a, k);
-        int run = min(k2 - k, 3 - (kw & 3));
-        if (a.per_z) run = min(run, a.nz - 1 - kw);
-        const int t = a.tile_map[((kw >> 2) * a.nty + (j >> 2)) * a.ntx + (i >> 2)];
-        if (t >= 0) {
-          const int64_t s0 = (int64_t)t * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (kw & 3);
-          for (int r = 0; r <= run; ++r) {
-            const int nodewall = a.windex[s0 + 16 * r];
-            if (nodewall <= 0 || nodewall == last) continue;
+  // walk of the window: columns (i, j), runs of z points inside one tile
+  int ci = i1, cj = j1, ck = k1, r = 0, rn = -1;
+  int64_t s0 = 0;
+  auto next_run = [&]() -> bool {
+    while (true) {
+      if (ck > k2) {
+        ck = k1;
+        if (++cj > j2) {
+          cj = j1;
+          if (++ci > i2) return false;
+        }
+      }
+      const int kw = wrapk(a, ck);
+      int run = min(k2 - ck, 3 - (kw & 3));
+      if (a.per_z) run = min(run, a.nz - 1 - kw);
+      ck += run + 1;
+      const int t = a.tile_map[((kw >> 2) * a.nty + (cj >> 2)) * a.ntx + (ci >> 2)];
+      if (t < 0 || !a.tile_wall[t]) continue;
+      s0 = (int64_t)t * ZF_TC + (ci & 3) + 4 * (cj & 3) + 16 * (kw & 3);
+      r = 0;
+      rn = run;
+      return true;
+    }
+  };
+  bool done = !(active && i1 <= i2 && j1 <= j2 && k1 <= k2);
+  if (!done) done = !next_run();
+  float mindis = 1.5f;
+  int triwall = -1, last = 0, qn = 0;
+  const unsigned below = (1u << lane) - 1u;
+  auto batch = [&](int nb) {
+    __syncwarp();
+    const int my = lane < nb ? sq_m[w][lane] : 0;
+    const int owner = lane < nb ? (int)sq_l[w][lane] : 0;
+    const float ox = __shfl_sync(FULL, xp, owner), oy = __shfl_sync(FULL, yp, owner),
+                oz = __shfl_sync(FULL, zp, owner);
+    float d = 3.0e38f;
+    int t = -1;
+    if (my > 0) wall_list_min(a, my, ox, oy, oz, d, t);
+    sq_d[w][lane] = d;
+    sq_t[w][lane] = t;
+    __syncwarp();
+    for (int q = 0; q < nb; ++q)
+      if (sq_l[w][q] == lane && sq_d[w][q] < mindis) {
+        mindis = sq_d[w][q];
+        triwall = sq_t[w][q];
+      }
+    __syncwarp();
+  };
+  while (__any_sync(FULL, !done)) {
+    int item = 0;
+    if (!done) {
+      const float4 wn = a.wnode[s0 + 16 * r];
+      if (wn.w >= 0.f) {
+        const float dm = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
+        if (!(dm - wn.w > fminf(bound, mindis) + 1e-4f)) {
+          const int nodewall = a.windex[s0 + 16 * r];
+          if (nodewall != last) {
             last = nodewall;
-            const int m = nodewall - 1;
-            const float dm = dist3(xp - a.wxyz[m], yp - a.wxyz[a.nw + m], wrapd(zp - a.wxyz[2 * a.nw + m], a.LZ));
-            if (dm - a.wrad[m] > fminf(bound, mindis) + 1e-4f) continue;
-            scan_list(nodewall, mindis, triwall);
+            item = nodewall;
           }
         }
-        k += run + 1;
       }
+      if (++r > rn) done = !next_run();
+    }
+    const unsigned bal = __ballot_sync(FULL, item > 0);
+    if (item > 0) {
+      const int pos = qn + __popc(bal & below);
+      sq_m[w][pos] = item;
+      sq_l[w][pos] = (unsigned char)lane;
+    }
+    qn += __popc(bal);
+    if (qn >= 32) {
+      batch(32);
+      const int rem = qn - 32;
+      int tm = 0, tl = 0;
+      if (lane < rem) {
+        tm = sq_m[w][32 + lane];
+        tl = sq_l[w][32 + lane];
+      }
+      __syncwarp();
+      if (lane < rem) {
+        sq_m[w][lane] = tm;
+        sq_l[w][lane] = (unsigned char)tl;
+      }
+      qn = rem;
+    }
+  }
+  if (qn > 0) batch(qn);
+  if (!active) return;
   if (triwall < 0) return;
   // signed distance to the plane of the wall triangle, repulsion, :9055-9077
   const int w1 = a.wtri[3 * triwall];
@@ -484,100 +586,199 @@ __global__ void k_nuc_memb(IbArgs a, CellArgs c, int rebuild, unsigned long long
 
 // ---- cell-cell repulsion ------------------------------------------------------
 
-__global__ void k_rbc_rbc(IbArgs a, CellArgs c) {
+// Warps work on a queue: every lane walks its node's bins in the reference
+// scan order and tests each entry with the cheap filters (centroid within
+// 2 um, ZebraflowWT.c:9978; a sub-centroid possibly within 1 um; facing
+// normals; not a triangle of the node itself).  Entries that pass go to a
+// per-warp queue in shared memory; each full batch of 32 is evaluated one
+// entry per lane (the 16 sub-centroids), and each owner adds its entries'
+// results in its own scan order, so the sums are deterministic.
+
+__device__ __forceinline__ void rbc_entry(const IbArgs& a, const CellArgs& c, int e, float xc, float yc,
+                                          float zc, float& tx, float& ty, float& tz) {
+  const int nc = c.n_cells;
+  const float4 cr = a.bin_c[e];
+  const int g = __float_as_int(a.bin_n[e].w);
+  const int m = g / c.nt, tri = g - m * c.nt;
+  const int n1 = c.tri[3 * tri], n2 = c.tri[3 * tri + 1], n3 = c.tri[3 * tri + 2];
+  const float dzc = wrapd(cr.z - zc, a.LZ);
+  const float shift = (cr.z - zc) - dzc;  // periodic image of the other cell
+  float tp[16][3], tc[17][3];
+#pragma unroll
+  for (int v = 0; v < 3; ++v) {
+    const float off = v == 2 ? shift : 0.f;
+    tp[1][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n1] - off;
+    tp[2][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n2] - off;
+    tp[3][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n3] - off;
+    tp[4][v] = 0.5f * (tp[1][v] + tp[2][v]);
+    tp[5][v] = 0.5f * (tp[2][v] + tp[3][v]);
+    tp[6][v] = 0.5f * (tp[1][v] + tp[3][v]);
+    tp[7][v] = 0.5f * (tp[1][v] + tp[4][v]);
+    tp[8][v] = 0.5f * (tp[2][v] + tp[4][v]);
+    tp[9][v] = 0.5f * (tp[2][v] + tp[5][v]);
+    tp[10][v] = 0.5f * (tp[5][v] + tp[3][v]);
+    tp[11][v] = 0.5f * (tp[3][v] + tp[6][v]);
+    tp[12][v] = 0.5f * (tp[6][v] + tp[1][v]);
+    tp[13][v] = 0.5f * (tp[4][v] + tp[6][v]);
+    tp[14][v] = 0.5f * (tp[4][v] + tp[5][v]);
+    tp[15][v] = 0.5f * (tp[5][v] + tp[6][v]);
+    tc[1][v] = (tp[1][v] + tp[7][v] + tp[12][v]) / 3.f;
+    tc[2][v] = (tp[7][v] + tp[13][v] + tp[12][v]) / 3.f;
+    tc[3][v] = (tp[7][v] + tp[4][v] + tp[13][v]) / 3.f;
+    tc[4][v] = (tp[4][v] + tp[14][v] + tp[13][v]) / 3.f;
+    tc[5][v] = (tp[4][v] + tp[8][v] + tp[14][v]) / 3.f;
+    tc[6][v] = (tp[8][v] + tp[9][v] + tp[14][v]) / 3.f;
+    tc[7][v] = (tp[8][v] + tp[2][v] + tp[9][v]) / 3.f;
+    tc[8][v] = (tp[12][v] + tp[13][v] + tp[6][v]) / 3.f;
+    tc[9][v] = (tp[13][v] + tp[15][v] + tp[6][v]) / 3.f;
+    tc[10][v] = (tp[13][v] + tp[14][v] + tp[15][v]) / 3.f;
+    tc[11][v] = (tp[14][v] + tp[5][v] + tp[15][v]) / 3.f;
+    tc[12][v] = (tp[14][v] + tp[9][v] + tp[5][v]) / 3.f;
+    tc[13][v] = (tp[6][v] + tp[15][v] + tp[11][v]) / 3.f;
+    tc[14][v] = (tp[15][v] + tp[10][v] + tp[11][v]) / 3.f;
+    tc[15][v] = (tp[15][v] + tp[5][v] + tp[10][v]) / 3.f;
+    tc[16][v] = (tp[11][v] + tp[10][v] + tp[3][v]) / 3.f;
+  }
+  tx = ty = tz = 0.f;
+#pragma unroll
+  for (int v = 1; v <= 16; ++v) {  // ZebraflowWT.c:10028-10042
+    const float dx = tc[v][0] - xc, dy = tc[v][1] - yc, dz = tc[v][2] - zc;
+    const float d = dist3(dx, dy, dz);
+    if (d < 1.0f) {
+      const float repulf = (float)(-8.333e-07 * (1.0 - (double)d) / 1.0);
+      tx += repulf * (dx / d);
+      ty += repulf * (dy / d);
+      tz += repulf * (dz / d);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kRepWarps * 32) k_rbc_rbc(IbArgs a, CellArgs c) {
+  __shared__ int sq_e[kRepWarps][64];
+  __shared__ unsigned char sq_l[kRepWarps][64];
+  __shared__ float sq_r[kRepWarps][32][3];
+  const unsigned FULL = 0xffffffffu;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = c.n_cells;
-  if (gid >= (int64_t)nc * c.nn) return;
-  const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
-  if (c.status[cell] <= 0) return;
-  float xc, yc, zc;
-  node_pos(c.x, nc, c.nn, cell, node, a.LZ, a.Z0, xc, yc, zc);
-  const float e1v[3] = {c.node_normal[((size_t)0 * nc + cell) * c.nn + node],
-                        c.node_normal[((size_t)1 * nc + cell) * c.nn + node],
-                        c.node_normal[((size_t)2 * nc + cell) * c.nn + node]};
-  const int i0 = lat_index(xc, a.X0, a.DX), j0 = lat_index(yc, a.Y0, a.DX),
-            k0 = lat_index(zc, a.Z0, a.DX);
-  const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
-  const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
-  const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
+  bool active = gid < (int64_t)nc * c.nn;
+  int cell = 0, node = 0;
+  if (active) {
+    cell = (int)(gid / c.nn);
+    node = (int)(gid % c.nn);
+    active = c.status[cell] > 0;
+  }
+  float xc = 0.f, yc = 0.f, zc = 0.f, e1x = 0.f, e1y = 0.f, e1z = 0.f;
+  int i1 = 0, i2 = -1, j1 = 0, j2 = -1, k1 = 0, k2 = -1;
+  if (active) {
+    node_pos(c.x, nc, c.nn, cell, node, a.LZ, a.Z0, xc, yc, zc);
+    e1x = c.node_normal[((size_t)0 * nc + cell) * c.nn + node];
+    e1y = c.node_normal[((size_t)1 * nc + cell) * c.nn + node];
+    e1z = c.node_normal[((size_t)2 * nc + cell) * c.nn + node];
+    const int i0 = lat_index(xc, a.X0, a.DX), j0 = lat_index(yc, a.Y0, a.DX),
+              k0 = lat_index(zc, a.Z0, a.DX);
+    i1 = max(i0 - 4, 0);
+    i2 = min(i0 + 4, a.nx - 1);
+    j1 = max(j0 - 4, 0);
+    j2 = min(j0 + 4, a.ny - 1);
+    k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2);
+    k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
+  }
   const int64_t n_pop_tiles = a.ns / ZF_TC;
-  float rx = 0.f, ry = 0.f, rz = 0.f;
-  for (int i = i1; i <= i2; ++i)
-    for (int j = j1; j <= j2; ++j)
-      for (int k = k1; k <= k2;) {
-        // the bins of a run of points along z inside one tile: one range
-        const int kw = a.per_z ? ((k % a.nz) + a.nz) % a.nz : k;
-        int run = min(k2 - k, 3 - (kw & 3));
-        if (a.per_z) run = min(run, a.nz - 1 - kw);
-        const int t = a.tile_map[((kw >> 2) * a.nty + (j >> 2)) * a.ntx + (i >> 2)];
-        k += run + 1;
-        if (t < 0 || t >= n_pop_tiles) continue;
-        const int64_t key = (int64_t)t * ZF_TC + 16 * (i & 3) + 4 * (j & 3) + (kw & 3);
-        const int e0 = a.bin_off[key], e1 = a.bin_off[key + run + 1];
-        for (int e = e0; e < e1; ++e) {
-          // centroid within 2 um (ZebraflowWT.c:9978), then only triangles one of whose
-          // sub-centroids can lie within 1 um contribute
-          const float4 cr = a.bin_c[e];
-          const float dzc = wrapd(cr.z - zc, a.LZ);
-          const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
-          if (!(dcen < 2.f) || dcen - cr.w > 1.f) continue;
-          const float4 nr = a.bin_n[e];
-          const float dot = e1v[0] * nr.x + e1v[1] * nr.y + e1v[2] * nr.z;
-          if (!(dot < 0.f)) continue;
-          const int g = __float_as_int(nr.w);
-          const int m = g / c.nt, tri = g - m * c.nt;
-          const int n1 = c.tri[3 * tri], n2 = c.tri[3 * tri + 1], n3 = c.tri[3 * tri + 2];
-          if (m == cell && (n1 == node || n2 == node || n3 == node)) continue;
-          const float shift = (cr.z - zc) - dzc;  // periodic image of the other cell
-          float tp[16][3], tc[17][3];
-#pragma unroll
-          for (int v = 0; v < 3; ++v) {
-            const float off = v == 2 ? shift : 0.f;
-            tp[1][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n1] - off;
-            tp[2][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n2] - off;
-            tp[3][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n3] - off;
-            tp[4][v] = 0.5f * (tp[1][v] + tp[2][v]);
-            tp[5][v] = 0.5f * (tp[2][v] + tp[3][v]);
-            tp[6][v] = 0.5f * (tp[1][v] + tp[3][v]);
-            tp[7][v] = 0.5f * (tp[1][v] + tp[4][v]);
-            tp[8][v] = 0.5f * (tp[2][v] + tp[4][v]);
-            tp[9][v] = 0.5f * (tp[2][v] + tp[5][v]);
-            tp[10][v] = 0.5f * (tp[5][v] + tp[3][v]);
-            tp[11][v] = 0.5f * (tp[3][v] + tp[6][v]);
-            tp[12][v] = 0.5f * (tp[6][v] + tp[1][v]);
-            tp[13][v] = 0.5f * (tp[4][v] + tp[6][v]);
-            tp[14][v] = 0.5f * (tp[4][v] + tp[5][v]);
-            tp[15][v] = 0.5f * (tp[5][v] + tp[6][v]);
-            tc[1][v] = (tp[1][v] + tp[7][v] + tp[12][v]) / 3.f;
-            tc[2][v] = (tp[7][v] + tp[13][v] + tp[12][v]) / 3.f;
-            tc[3][v] = (tp[7][v] + tp[4][v] + tp[13][v]) / 3.f;
-            tc[4][v] = (tp[4][v] + tp[14][v] + tp[13][v]) / 3.f;
-            tc[5][v] = (tp[4][v] + tp[8][v] + tp[14][v]) / 3.f;
-            tc[6][v] = (tp[8][v] + tp[9][v] + tp[14][v]) / 3.f;
-            tc[7][v] = (tp[8][v] + tp[2][v] + tp[9][v]) / 3.f;
-            tc[8][v] = (tp[12][v] + tp[13][v] + tp[6][v]) / 3.f;
-            tc[9][v] = (tp[13][v] + tp[15][v] + tp[6][v]) / 3.f;
-            tc[10][v] = (tp[13][v] + tp[14][v] + tp[15][v]) / 3.f;
-            tc[11][v] = (tp[14][v] + tp[5][v] + tp[15][v]) / 3.f;
-            tc[12][v] = (tp[14][v] + tp[9][v] + tp[5][v]) / 3.f;
-            tc[13][v] = (tp[6][v] + tp[15][v] + tp[11][v]) / 3.f;
-            tc[14][v] = (tp[15][v] + tp[10][v] + tp[11][v]) / 3.f;
-            tc[15][v] = (tp[15][v] + tp[5][v] + tp[10][v]) / 3.f;
-            tc[16][v] = (tp[11][v] + tp[10][v] + tp[3][v]) / 3.f;
-          }
-#pragma unroll
-          for (int v = 1; v <= 16; ++v) {
-            const float dx = tc[v][0] - xc, dy = tc[v][1] - yc, dz = tc[v][2] - zc;
-            const float d = dist3(dx, dy, dz);
-            if (d < 1.0f) {
-              const float repulf = (float)(-8.333e-07 * (1.0 - (double)d) / 1.0);
-              rx += repulf * (dx / d);
-              ry += repulf * (dy / d);
-              rz += repulf * (dz / d);
-            }
-          }
+  // walk of the +-4 window: columns (i, j), runs of z points inside one tile
+  int ci = i1, cj = j1, ck = k1, e = 0, e_end = 0;
+  auto next_run = [&]() -> bool {
+    while (true) {
+      if (ck > k2) {
+        ck = k1;
+        if (++cj > j2) {
+          cj = j1;
+          if (++ci > i2) return false;
         }
       }
+      const int kw = a.per_z ? ((ck % a.nz) + a.nz) % a.nz : ck;
+      int run = min(k2 - ck, 3 - (kw & 3));
+      if (a.per_z) run = min(run, a.nz - 1 - kw);
+      ck += run + 1;
+      const int t = a.tile_map[((kw >> 2) * a.nty + (cj >> 2)) * a.ntx + (ci >> 2)];
+      if (t < 0 || t >= n_pop_tiles) continue;
+      const int64_t key = (int64_t)t * ZF_TC + 16 * (ci & 3) + 4 * (cj & 3) + (kw & 3);
+      e = a.bin_off[key];
+      e_end = a.bin_off[key + run + 1];
+      if (e < e_end) return true;
+    }
+  };
+  bool done = !(active && i1 <= i2 && j1 <= j2 && k1 <= k2);
+  if (!done) done = !next_run();
+  float rx = 0.f, ry = 0.f, rz = 0.f;
+  int qn = 0;
+  const unsigned below = (1u << lane) - 1u;
+  auto batch = [&](int n) {
+    __syncwarp();
+    const int my = lane < n ? sq_e[w][lane] : -1;
+    const int owner = lane < n ? (int)sq_l[w][lane] : 0;
+    const float ox = __shfl_sync(FULL, xc, owner), oy = __shfl_sync(FULL, yc, owner),
+                oz = __shfl_sync(FULL, zc, owner);
+    float tx = 0.f, ty = 0.f, tz = 0.f;
+    if (my >= 0) rbc_entry(a, c, my, ox, oy, oz, tx, ty, tz);
+    sq_r[w][lane][0] = tx;
+    sq_r[w][lane][1] = ty;
+    sq_r[w][lane][2] = tz;
+    __syncwarp();
+    for (int q = 0; q < n; ++q)
+      if (sq_l[w][q] == lane) {
+        rx += sq_r[w][q][0];
+        ry += sq_r[w][q][1];
+        rz += sq_r[w][q][2];
+      }
+    __syncwarp();
+  };
+  while (__any_sync(FULL, !done)) {
+    int item = -1;
+    if (!done) {
+      const float4 cr = a.bin_c[e];
+      const float dzc = wrapd(cr.z - zc, a.LZ);
+      const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
+      if (dcen < 2.f && !(dcen - cr.w > 1.f)) {
+        const float4 nr = a.bin_n[e];
+        if (e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
+          const int g = __float_as_int(nr.w);
+          const int m = g / c.nt;
+          bool own = false;
+          if (m == cell) {
+            const int tri = g - m * c.nt;
+            own = c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node;
+          }
+          if (!own) item = e;
+        }
+      }
+      if (++e >= e_end) done = !next_run();
+    }
+    const unsigned bal = __ballot_sync(FULL, item >= 0);
+    if (item >= 0) {
+      const int pos = qn + __popc(bal & below);
+      sq_e[w][pos] = item;
+      sq_l[w][pos] = (unsigned char)lane;
+    }
+    qn += __popc(bal);
+    if (qn >= 32) {
+      batch(32);
+      const int rem = qn - 32;
+      int te = 0, tl = 0;
+      if (lane < rem) {
+        te = sq_e[w][32 + lane];
+        tl = sq_l[w][32 + lane];
+      }
+      __syncwarp();
+      if (lane < rem) {
+        sq_e[w][lane] = te;
+        sq_l[w][lane] = (unsigned char)tl;
+      }
+      qn = rem;
+    }
+  }
+  if (qn > 0) batch(qn);
+  if (!active) return;
   c.wrep[((size_t)0 * nc + cell) * c.nn + node] += rx;
   c.wrep[((size_t)1 * nc + cell) * c.nn + node] += ry;
   c.wrep[((size_t)2 * nc + cell) * c.nn + node] += rz;
@@ -696,6 +897,9 @@ int ib_interp_launch(zf_ctx* ctx) {
   const int64_t n = (int64_t)c.n_cells * (c.nn + c.nnn);
   if (n == 0) return ZF_OK;
   k_ib_interp<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c);
+  if (ctx->ib.nw > 0)
+    k_ib_wall<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
+        ctx->ib, c);
   ZF_CUDA(cudaGetLastError());
   return ZF_OK;
 }
@@ -740,7 +944,8 @@ int ib_rbc_rbc_launch(zf_ctx* ctx) {
   const CellArgs& c = ctx->cells;
   const int64_t n = (int64_t)c.n_cells * c.nn;
   if (n == 0) return ZF_OK;
-  k_rbc_rbc<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c);
+  k_rbc_rbc<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
+      ctx->ib, c);
   ZF_CUDA(cudaGetLastError());
   return ZF_OK;
 }

@@ -78,6 +78,7 @@ int build_view(zf_ctx* c, const WallHost* W) {
   std::vector<uint8_t> code(ns_all, ZF_CODE_SOLID);
   ZF_CUDA(cudaMemcpy(code.data(), c->d_code, c->ns, cudaMemcpyDeviceToHost));
   std::vector<int32_t> windex(ns_all, 0);
+  std::vector<float4> wnode(ns_all, make_float4(0.f, 0.f, 0.f, -1.f));
   std::vector<float> uvoid(3 * ns_all, 0.f);
   std::vector<uint8_t> twall(n_all, 0);
   if (W) {
@@ -90,6 +91,8 @@ int build_view(zf_ctx* c, const WallHost* W) {
       if (W->windex[p] <= 0) continue;
       const int64_t s = slot(p);
       windex[s] = W->windex[p];
+      const int m = W->windex[p] - 1;
+      wnode[s] = make_float4(W->xyz[m], W->xyz[(size_t)W->nw + m], W->xyz[2 * (size_t)W->nw + m], W->rad[m]);
       twall[s / ZF_TC] = 1;
     }
     for (const VoidPoint& v : W->uvoid) {
@@ -106,6 +109,7 @@ int build_view(zf_ctx* c, const WallHost* W) {
   if ((rc = dalloc<uint8_t>(c, own, const_cast<uint8_t**>(&a.code), code.size(), code.data()))) return rc;
   if ((rc = dalloc<int32_t>(c, own, const_cast<int32_t**>(&a.windex), windex.size(), windex.data())))
     return rc;
+  if ((rc = dalloc<float4>(c, own, const_cast<float4**>(&a.wnode), wnode.size(), wnode.data()))) return rc;
   if ((rc = dalloc<float>(c, own, const_cast<float**>(&a.uvoid), uvoid.size(), uvoid.data()))) return rc;
   if ((rc = dalloc<uint8_t>(c, own, const_cast<uint8_t**>(&a.tile_wall), twall.size(), twall.data())))
     return rc;
@@ -311,7 +315,7 @@ static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
       }
       // k_membrane, k_ib_interp, k_nuc_memb, 7 cell-list kernels (assign, 3
       // scan passes, fill, sort, records), k_rbc_rbc, k_ib_spread, k_update
-      c->launches += 13;
+      c->launches += 13 + (c->ib.nw > 0 ? 1 : 0);  // + k_ib_wall
     }
     c->status.iter = iter;
   }

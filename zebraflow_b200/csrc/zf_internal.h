@@ -135,6 +135,8 @@ struct IbArgs {
   const uint8_t* code;          // [n_all*64]
   const uint8_t* tile_wall;     // [n_all] tile holds a point with W_index > 0
   const int32_t* windex;        // [n_all*64] 1-based wall node or 0
+  const float4* wnode;          // [n_all*64] that wall node's position and bounding
+                                // radius (WallHost::rad); w < 0 where W_index is 0
   const float* uvoid;           // [3][n_all*64]
   const float* mom;             // [4][ns] D,U,V,W of population tiles
   float* force;                 // [3][ns] BODYFORCE
