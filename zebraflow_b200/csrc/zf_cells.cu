@@ -377,6 +377,7 @@ int cells_membrane_launch(zf_ctx* c) {
   ZF_CUDA(cudaFuncSetAttribute(k_membrane, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_membrane<<<a.n_cells, 256, smem, c->stream>>>(a);
   ZF_CUDA(cudaGetLastError());
+  c->launches += 1;
   return ZF_OK;
 }
 

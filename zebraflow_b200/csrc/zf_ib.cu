@@ -441,13 +441,14 @@ __global__ void k_scan_add(int32_t* out, int64_t n, const int32_t* bsum) {
 }
 
 __global__ void k_bin_fill(CellArgs c, const int32_t* tri_bin, const int32_t* off, int32_t* cursor,
-                           int32_t* bin_tri) {
+                           int32_t* bin_tri, uint8_t* bin_kk) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= (int64_t)c.n_cells * c.nt) return;
   const int32_t b = tri_bin[g];
   if (b < 0) return;
   const int pos = atomicAdd(&cursor[b], 1);
   bin_tri[off[b] + pos] = (int32_t)g;
+  bin_kk[off[b] + pos] = (uint8_t)(b & 63);
 }
 
 // deterministic order inside each bin (ascending global triangle id)
@@ -594,11 +595,9 @@ __global__ void k_nuc_memb(IbArgs a, CellArgs c, int rebuild, unsigned long long
 // entry per lane (the 16 sub-centroids), and each owner adds its entries'
 // results in its own scan order, so the sums are deterministic.
 
-__device__ __forceinline__ void rbc_entry(const IbArgs& a, const CellArgs& c, int e, float xc, float yc,
-                                          float zc, float& tx, float& ty, float& tz) {
+__device__ __forceinline__ void rbc_entry(const IbArgs& a, const CellArgs& c, const float4 cr, int g,
+                                          float xc, float yc, float zc, float& tx, float& ty, float& tz) {
   const int nc = c.n_cells;
-  const float4 cr = a.bin_c[e];
-  const int g = __float_as_int(a.bin_n[e].w);
   const int m = g / c.nt, tri = g - m * c.nt;
   const int n1 = c.tri[3 * tri], n2 = c.tri[3 * tri + 1], n3 = c.tri[3 * tri + 2];
   const float dzc = wrapd(cr.z - zc, a.LZ);
@@ -720,7 +719,7 @@ __global__ void __launch_bounds__(kRepWarps * 32) k_rbc_rbc(IbArgs a, CellArgs c
     const float ox = __shfl_sync(FULL, xc, owner), oy = __shfl_sync(FULL, yc, owner),
                 oz = __shfl_sync(FULL, zc, owner);
     float tx = 0.f, ty = 0.f, tz = 0.f;
-    if (my >= 0) rbc_entry(a, c, my, ox, oy, oz, tx, ty, tz);
+    if (my >= 0) rbc_entry(a, c, a.bin_c[my], __float_as_int(a.bin_n[my].w), ox, oy, oz, tx, ty, tz);
     sq_r[w][lane][0] = tx;
     sq_r[w][lane][1] = ty;
     sq_r[w][lane][2] = tz;
@@ -782,6 +781,438 @@ __global__ void __launch_bounds__(kRepWarps * 32) k_rbc_rbc(IbArgs a, CellArgs c
   c.wrep[((size_t)0 * nc + cell) * c.nn + node] += rx;
   c.wrep[((size_t)1 * nc + cell) * c.nn + node] += ry;
   c.wrep[((size_t)2 * nc + cell) * c.nn + node] += rz;
+}
+
+// ---- tile-cooperative searches ------------------------------------------------
+//
+// Nodes are grouped by the lattice tile of their nearest lattice point
+// (lat_index, clamped into the box; z wrapped when periodic).  The +-4 window
+// of every node of a tile then lies inside the 3x3x3 tiles around it, so one
+// CTA stages what those 27 tiles hold into shared memory once (bin records of
+// the cell list; wall-node records of the lattice points) and its warps test
+// the tile's nodes against the staged copy.  Each test applies the node's own
+// window exactly, so the candidates are the reference's.  Needs three distinct
+// z tiles when z is periodic (nz >= 9); smaller periodic boxes use k_rbc_rbc
+// and k_ib_wall.
+
+constexpr int kTileThreads = 256;
+constexpr int kTileWarps = kTileThreads / 32;
+constexpr int kStage = 1024;  // bin records staged per pass
+
+__device__ __forceinline__ int node_grid_tile(const IbArgs& a, float xp, float yp, float zp) {
+  const int i0 = min(max(lat_index(xp, a.X0, a.DX), 0), a.nx - 1);
+  const int j0 = min(max(lat_index(yp, a.Y0, a.DX), 0), a.ny - 1);
+  const int k0 = lat_index(zp, a.Z0, a.DX);
+  const int kw = a.per_z ? ((k0 % a.nz) + a.nz) % a.nz : min(max(k0, 0), a.nz - 1);
+  return ((kw >> 2) * a.nty + (j0 >> 2)) * a.ntx + (i0 >> 2);
+}
+
+// node gid: membrane nodes of all cells, then nucleus nodes (as k_ib_interp)
+__device__ __forceinline__ bool node_of(const CellArgs& c, int64_t gid, bool& nuc, int& cell, int& node) {
+  const int64_t nmem = (int64_t)c.n_cells * c.nn;
+  nuc = gid >= nmem;
+  const int n = nuc ? c.nnn : c.nn;
+  const int64_t lid = nuc ? gid - nmem : gid;
+  cell = (int)(lid / n);
+  node = (int)(lid % n);
+  return c.status[cell] > 0;
+}
+
+__global__ void k_node_tiles(IbArgs a, CellArgs c) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  if (gid >= (int64_t)nc * (c.nn + c.nnn)) return;
+  bool nuc;
+  int cell, node;
+  if (!node_of(c, gid, nuc, cell, node)) {
+    a.node_gt[gid] = -1;
+    return;
+  }
+  float xp, yp, zp;
+  node_pos(nuc ? c.xn : c.x, nc, nuc ? c.nnn : c.nn, cell, node, a.LZ, a.Z0, xp, yp, zp);
+  const int gt = node_grid_tile(a, xp, yp, zp);
+  a.node_gt[gid] = gt;
+  atomicAdd(&a.node_cnt[gt], 1);
+}
+
+__global__ void k_node_fill(IbArgs a, CellArgs c) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (int64_t)c.n_cells * (c.nn + c.nnn)) return;
+  const int gt = a.node_gt[gid];
+  if (gt < 0) return;
+  const int pos = atomicAdd(&a.node_cnt[gt], 1);
+  a.node_sorted[a.node_off[gt] + pos] = (int32_t)gid;
+  if (pos == 0) a.tile_list[atomicAdd(&a.tile_ctr[0], 1)] = gt;
+}
+
+// RBC-RBC repulsion (ZebraflowWT.c:9911-10053) over the staged bin records.
+// Lanes split a node's records; each lane sums its contributions, and a fixed
+// butterfly adds the lanes, so the result is deterministic.
+__global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c) {
+  __shared__ float4 s_c[kStage];
+  __shared__ float4 s_n[kStage];
+  __shared__ int2 s_p[kStage];
+  __shared__ int s_r0[28], s_e0[27], s_tx[27], s_ty[27], s_tz[27];
+  __shared__ float s_acc[kTileThreads][3];
+  __shared__ int s_q[kTileWarps][64];
+  __shared__ int s_li;
+  const unsigned FULL = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nc = c.n_cells;
+  const int64_t nmem = (int64_t)nc * c.nn;
+  const int64_t n_pop_tiles = a.ns / ZF_TC;
+  const int nlist = a.tile_ctr[0];
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_li = atomicAdd(&a.tile_ctr[1], 1);
+    __syncthreads();
+    const int li = s_li;
+    if (li >= nlist) break;
+    const int gt = a.tile_list[li];
+    const int tx = gt % a.ntx, ty = (gt / a.ntx) % a.nty, tz = gt / (a.ntx * a.nty);
+    if (threadIdx.x < 27) {  // record range of each of the 27 tiles
+      const int r = threadIdx.x;
+      int X = tx + r % 3 - 1, Y = ty + (r / 3) % 3 - 1, Z = tz + r / 9 - 1;
+      bool ok = X >= 0 && X < a.ntx && Y >= 0 && Y < a.nty;
+      if (a.per_z) Z = (Z + a.ntz) % a.ntz;
+      else ok = ok && Z >= 0 && Z < a.ntz;
+      int e0 = 0, len = 0;
+      if (ok) {
+        const int t = a.tile_map[((int64_t)Z * a.nty + Y) * a.ntx + X];
+        if (t >= 0 && t < n_pop_tiles) {
+          e0 = a.bin_off[(int64_t)t * ZF_TC];
+          len = a.bin_off[(int64_t)t * ZF_TC + ZF_TC] - e0;
+        }
+      }
+      s_e0[r] = e0;
+      s_r0[r + 1] = len;
+      s_tx[r] = X;
+      s_ty[r] = Y;
+      s_tz[r] = Z;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_r0[0] = 0;
+      for (int r = 0; r < 27; ++r) s_r0[r + 1] += s_r0[r];
+    }
+    __syncthreads();
+    const int R = s_r0[27];
+    const int n0 = a.node_off[gt], n1 = a.node_off[gt + 1];
+    if (R == 0) continue;
+    for (int g0 = n0; g0 < n1; g0 += kTileThreads) {
+      const int gn = min(kTileThreads, n1 - g0);
+      s_acc[threadIdx.x][0] = s_acc[threadIdx.x][1] = s_acc[threadIdx.x][2] = 0.f;
+      for (int f0 = 0; f0 < R; f0 += kStage) {
+        const int fn = min(kStage, R - f0);
+        __syncthreads();
+        for (int f = threadIdx.x; f < fn; f += kTileThreads) {
+          const int gf = f0 + f;
+          int r = 0;
+          while (gf >= s_r0[r + 1]) ++r;
+          const int64_t e = s_e0[r] + (gf - s_r0[r]);
+          const int kk = a.bin_kk[e];
+          s_c[f] = a.bin_c[e];
+          s_n[f] = a.bin_n[e];
+          s_p[f] = make_int2((s_tx[r] * 4 + ((kk >> 4) & 3)) | ((s_ty[r] * 4 + ((kk >> 2) & 3)) << 16),
+                             s_tz[r] * 4 + (kk & 3));
+        }
+        __syncthreads();
+        for (int q = warp; q < gn; q += kTileWarps) {
+          const int64_t gid = a.node_sorted[g0 + q];
+          if (gid >= nmem) continue;  // nucleus node: no RBC-RBC term
+          const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
+          if (c.status[cell] <= 0) continue;
+          float xc, yc, zc;
+          node_pos(c.x, nc, c.nn, cell, node, a.LZ, a.Z0, xc, yc, zc);
+          const float e1x = c.node_normal[((size_t)0 * nc + cell) * c.nn + node];
+          const float e1y = c.node_normal[((size_t)1 * nc + cell) * c.nn + node];
+          const float e1z = c.node_normal[((size_t)2 * nc + cell) * c.nn + node];
+          const int i0 = lat_index(xc, a.X0, a.DX), j0 = lat_index(yc, a.Y0, a.DX),
+                    k0 = lat_index(zc, a.Z0, a.DX);
+          const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
+          const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
+          const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
+          // lanes filter 32 records at a time; the records that pass queue up
+          // and are evaluated 32 at a time, one per lane
+          float rx = 0.f, ry = 0.f, rz = 0.f;
+          int qn = 0;
+          int* queue = s_q[warp];
+          for (int f0 = 0; f0 < fn; f0 += 32) {
+            const int f = f0 + lane;
+            bool pass = false;
+            if (f < fn) {
+              const int2 pp = s_p[f];
+              const int bi = pp.x & 0xffff, bj = pp.x >> 16, bk = pp.y;
+              bool in = bi >= i1 && bi <= i2 && bj >= j1 && bj <= j2;
+              if (a.per_z) {
+                int dk = (bk - k1) % a.nz;
+                if (dk < 0) dk += a.nz;
+                in = in && dk <= k2 - k1;
+              } else {
+                in = in && bk >= k1 && bk <= k2;
+              }
+              if (in) {
+                const float4 cr = s_c[f];
+                const float dzc = wrapd(cr.z - zc, a.LZ);
+                const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
+                if (dcen < 2.f && !(dcen - cr.w > 1.f)) {
+                  const float4 nr = s_n[f];
+                  if (e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
+                    const int g = __float_as_int(nr.w);
+                    const int m = g / c.nt;
+                    pass = true;
+                    if (m == cell) {
+                      const int tri = g - m * c.nt;
+                      pass = !(c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node);
+                    }
+                  }
+                }
+              }
+            }
+            const unsigned bal = __ballot_sync(FULL, pass);
+            if (pass) queue[qn + __popc(bal & ((1u << lane) - 1u))] = f;
+            qn += __popc(bal);
+            while (qn >= 32 || (f0 + 32 >= fn && qn > 0)) {
+              __syncwarp();
+              const int nb = min(qn, 32);
+              if (lane < nb) {
+                const int fq = queue[lane];
+                float tx2, ty2, tz2;
+                rbc_entry(a, c, s_c[fq], __float_as_int(s_n[fq].w), xc, yc, zc, tx2, ty2, tz2);
+                rx += tx2;
+                ry += ty2;
+                rz += tz2;
+              }
+              __syncwarp();
+              const int rem = qn - nb;
+              const int tq = lane < rem ? queue[nb + lane] : 0;
+              __syncwarp();
+              if (lane < rem) queue[lane] = tq;
+              __syncwarp();
+              qn = rem;
+            }
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            rx += __shfl_xor_sync(FULL, rx, o);
+            ry += __shfl_xor_sync(FULL, ry, o);
+            rz += __shfl_xor_sync(FULL, rz, o);
+          }
+          if (lane == 0) {
+            s_acc[q][0] += rx;
+            s_acc[q][1] += ry;
+            s_acc[q][2] += rz;
+          }
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x < gn) {
+        const int64_t gid = a.node_sorted[g0 + threadIdx.x];
+        if (gid < nmem) {
+          const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
+          if (c.status[cell] > 0) {
+            c.wrep[((size_t)0 * nc + cell) * c.nn + node] += s_acc[threadIdx.x][0];
+            c.wrep[((size_t)1 * nc + cell) * c.nn + node] += s_acc[threadIdx.x][1];
+            c.wrep[((size_t)2 * nc + cell) * c.nn + node] += s_acc[threadIdx.x][2];
+          }
+        }
+      }
+    }
+  }
+}
+
+// Nearest wall triangle and wall repulsion (as k_ib_wall) over the staged
+// W_index and wall-node records of the 27 tiles.  A warp takes one node and
+// walks its window 32 points at a time in the reference scan order; each lane
+// gives the first minimum of its point's list (skipped when the point repeats
+// the previous point's wall node or cannot reach the running bound); the
+// lowest lane holding the chunk minimum is the first candidate in scan order,
+// and it replaces the running minimum only when strictly smaller.
+__global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs c) {
+  __shared__ float4 s_wn[27 * ZF_TC];
+  __shared__ int s_wi[27 * ZF_TC];
+  __shared__ int s_q[kTileWarps][64];
+  __shared__ int s_li, s_any;
+  const unsigned FULL = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nc = c.n_cells;
+  const int nlist = a.tile_ctr[0];
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_li = atomicAdd(&a.tile_ctr[2], 1);
+      s_any = 0;
+    }
+    __syncthreads();
+    const int li = s_li;
+    if (li >= nlist) break;
+    const int gt = a.tile_list[li];
+    const int tx = gt % a.ntx, ty = (gt / a.ntx) % a.nty, tz = gt / (a.ntx * a.nty);
+    for (int idx = threadIdx.x; idx < 27 * ZF_TC; idx += kTileThreads) {
+      const int r = idx >> 6, o = idx & 63;
+      int X = tx + r % 3 - 1, Y = ty + (r / 3) % 3 - 1, Z = tz + r / 9 - 1;
+      bool ok = X >= 0 && X < a.ntx && Y >= 0 && Y < a.nty;
+      if (a.per_z) Z = (Z + a.ntz) % a.ntz;
+      else ok = ok && Z >= 0 && Z < a.ntz;
+      int wi = 0;
+      float4 wn = make_float4(0.f, 0.f, 0.f, -1.f);
+      if (ok) {
+        const int t = a.tile_map[((int64_t)Z * a.nty + Y) * a.ntx + X];
+        if (t >= 0 && a.tile_wall[t]) {
+          wi = a.windex[(int64_t)t * ZF_TC + o];
+          wn = a.wnode[(int64_t)t * ZF_TC + o];
+          if (o == 0) s_any = 1;
+        }
+      }
+      s_wi[idx] = wi;
+      s_wn[idx] = wn;
+    }
+    __syncthreads();
+    if (!s_any) continue;
+    const int n0 = a.node_off[gt], n1 = a.node_off[gt + 1];
+    for (int q = n0 + warp; q < n1; q += kTileWarps) {
+      const int64_t gid = a.node_sorted[q];
+      bool nuc;
+      int cell, node;
+      if (!node_of(c, gid, nuc, cell, node)) continue;
+      const int n = nuc ? c.nnn : c.nn;
+      float xp, yp, zp;
+      node_pos(nuc ? c.xn : c.x, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
+      const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
+                k0 = lat_index(zp, a.Z0, a.DX);
+      const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
+      const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
+      const int k1 = max(k0 - 4, a.kmin), k2 = min(k0 + 4, a.kmax);
+      if (i1 > i2 || j1 > j2 || k1 > k2) continue;
+      const int ni = i2 - i1 + 1, nj = j2 - j1 + 1, nk = k2 - k1 + 1;
+      // staged index of lattice point (i, j, k) of the window
+      auto sidx = [&](int i, int j, int k) {
+        const int kw = wrapk(a, k);
+        const int lx = (i >> 2) - tx + 1, ly = (j >> 2) - ty + 1;
+        int lz = (kw >> 2) - tz + 1;
+        if (a.per_z) lz = ((lz % a.ntz) + a.ntz) % a.ntz;
+        return ((lz * 3 + ly) * 3 + lx) * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (kw & 3);
+      };
+      // lane l starts at window point l (scan order i, j, k) and steps 32
+      // points at a time in mixed radix
+      const int npts = ni * nj * nk;
+      const int sk = 32 % nk, sj = (32 / nk) % nj, si = 32 / (nk * nj);
+      const int pi0 = i1 + lane / (nj * nk), pj0 = j1 + (lane / nk) % nj, pk0 = k1 + lane % nk;
+      auto step = [&](int& i, int& j, int& k) {
+        k += sk;
+        int cy = 0;
+        if (k > k2) {
+          k -= nk;
+          cy = 1;
+        }
+        j += sj + cy;
+        cy = 0;
+        if (j > j2) {
+          j -= nj;
+          cy = 1;
+        }
+        i += si + cy;
+      };
+      // bound: the first minimum of the list of the window's nearest wall
+      // node (any list of the window bounds the window minimum from above;
+      // 1.5 is the reference's starting value)
+      float bound = 1.5f;
+      {
+        float dbest = 3.0e38f;
+        int mbest = 0;
+        int i = pi0, j = pj0, k = pk0;
+        for (int p = lane; p < npts; p += 32) {
+          const int si2 = sidx(i, j, k);
+          const int wi = s_wi[si2];
+          if (wi > 0) {
+            const float4 wn = s_wn[si2];
+            const float dm = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
+            if (dm < dbest) {
+              dbest = dm;
+              mbest = wi;
+            }
+          }
+          step(i, j, k);
+        }
+        float dmin = dbest;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
+        const unsigned at = __ballot_sync(FULL, dbest == dmin && mbest > 0);
+        if (at) {
+          const int m = __shfl_sync(FULL, mbest, __ffs(at) - 1);
+          int unused = -1;
+          wall_list_min(a, m, xp, yp, zp, bound, unused);
+        }
+      }
+      // walk in scan order; lists that can still reach the minimum queue up
+      // (in scan order) and are scanned 32 at a time, one per lane
+      float mindis = 1.5f;
+      int triwall = -1, last = 0, qn = 0;
+      int* queue = s_q[warp];
+      auto flush = [&](int nb) {
+        __syncwarp();
+        float d = 3.0e38f;
+        int t = -1;
+        if (lane < nb) wall_list_min(a, queue[lane], xp, yp, zp, d, t);
+        float dmin = d;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
+        const unsigned at = __ballot_sync(FULL, d == dmin && t >= 0);
+        if (at && dmin < mindis) {
+          mindis = dmin;
+          triwall = __shfl_sync(FULL, t, __ffs(at) - 1);
+        }
+        const int rem = qn - nb;
+        const int tq = lane < rem ? queue[nb + lane] : 0;
+        __syncwarp();
+        if (lane < rem) queue[lane] = tq;
+        __syncwarp();
+        qn = rem;
+      };
+      {
+        int i = pi0, j = pj0, k = pk0;
+        for (int p0 = 0; p0 < npts; p0 += 32) {
+          int wi = 0;
+          float4 wn = make_float4(0.f, 0.f, 0.f, -1.f);
+          if (p0 + lane < npts) {
+            const int si2 = sidx(i, j, k);
+            wi = s_wi[si2];
+            if (wi > 0) wn = s_wn[si2];
+          }
+          step(i, j, k);
+          int prev = __shfl_up_sync(FULL, wi, 1);
+          if (lane == 0) prev = last;
+          last = __shfl_sync(FULL, wi, 31);
+          bool want = false;
+          if (wi > 0 && wi != prev) {
+            const float dm = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
+            want = !(dm - wn.w > fminf(bound, mindis) + 1e-4f);
+          }
+          const unsigned bal = __ballot_sync(FULL, want);
+          if (want) queue[qn + __popc(bal & ((1u << lane) - 1u))] = wi;
+          qn += __popc(bal);
+          while (qn >= 32) flush(32);
+        }
+        while (qn > 0) flush(min(qn, 32));
+      }
+      if (triwall < 0 || lane != 0) continue;
+      // signed distance to the plane of the wall triangle, repulsion, :9055-9077
+      const int w1 = a.wtri[3 * triwall];
+      const float n0 = a.wnrm[triwall], n1 = a.wnrm[a.mt + triwall], n2 = a.wnrm[2 * a.mt + triwall];
+      const float ddx = xp - a.wxyz[w1], ddy = yp - a.wxyz[a.nw + w1],
+                  ddz = wrapd(zp - a.wxyz[2 * a.nw + w1], a.LZ);
+      const float dist = __fadd_rn(__fadd_rn(__fmul_rn(ddx, n0), __fmul_rn(ddy, n1)), __fmul_rn(ddz, n2));
+      if (dist < 0.25f && fabsf(dist) < 1.0f && node < c.nn) {
+        float repulf = (float)((0.25 - (double)dist) / 1.0);
+        if (dist < -0.75f) repulf = 1.f;
+        // nucleus nodes add to the membrane array at their own index, as the
+        // reference does (ZebraflowWT.c:9415-9430 write NODE_WALLREPUL[v][caps][node])
+        atomicAdd(&c.wrep[((size_t)0 * nc + cell) * c.nn + node], (float)((double)repulf * 1.e-04 * n0));
+        atomicAdd(&c.wrep[((size_t)1 * nc + cell) * c.nn + node], (float)((double)repulf * 1.e-04 * n1));
+        atomicAdd(&c.wrep[((size_t)2 * nc + cell) * c.nn + node], (float)((double)repulf * 1.e-04 * n2));
+      }
+    }
+  }
 }
 
 // ---- spreading ----------------------------------------------------------------
@@ -892,14 +1323,71 @@ __global__ void k_update(IbArgs a, CellArgs c) {
 
 // ---- launchers --------------------------------------------------------------------
 
-int ib_interp_launch(zf_ctx* ctx) {
+namespace {
+
+// the tile kernels need the 3x3x3 tile neighbourhood of a tile to hold every
+// window point: along a periodic z axis the tiles must wrap with the lattice
+// (nz a multiple of the tile edge) and be at least three
+bool tiles_ok(const IbArgs& a) { return !a.per_z || (a.nz % ZF_TS == 0 && a.ntz >= 3); }
+
+template <typename K>
+int persistent_blocks(K kernel, int threads) {
+  int dev = 0, sms = 0, per_sm = 0;
+  ZF_CUDA(cudaGetDevice(&dev));
+  ZF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  ZF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
+  return sms * (per_sm > 0 ? per_sm : 1);
+}
+
+// exclusive scan of in[0..n) into out[0..n]; bsum holds (n+1023)/1024 + 1 ints
+void scan_launch(const int32_t* in, int64_t n, int32_t* out, int32_t* bsum, cudaStream_t st) {
+  const int nb = (int)((n + 1023) / 1024);
+  k_scan_blocks<<<nb, 1024, 0, st>>>(in, n, out, bsum);
+  k_scan_sums<<<1, 32, 0, st>>>(bsum, nb, bsum + nb);
+  k_scan_add<<<nb, 1024, 0, st>>>(out, n, bsum);
+}
+
+}  // namespace
+
+int ib_node_tiles_launch(zf_ctx* ctx) {
   const CellArgs& c = ctx->cells;
+  IbArgs& a = ctx->ib;
   const int64_t n = (int64_t)c.n_cells * (c.nn + c.nnn);
   if (n == 0) return ZF_OK;
-  k_ib_interp<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c);
-  if (ctx->ib.nw > 0)
-    k_ib_wall<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
-        ctx->ib, c);
+  const int64_t ng1 = a.ngrid + 1;
+  ZF_CUDA(cudaMemsetAsync(a.node_cnt, 0, ng1 * sizeof(int32_t), ctx->stream));
+  ZF_CUDA(cudaMemsetAsync(a.tile_ctr, 0, 4 * sizeof(int32_t), ctx->stream));
+  k_node_tiles<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(a, c);
+  scan_launch(a.node_cnt, ng1, a.node_off, a.node_bsum, ctx->stream);
+  ZF_CUDA(cudaMemsetAsync(a.node_cnt, 0, ng1 * sizeof(int32_t), ctx->stream));
+  k_node_fill<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(a, c);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 5;
+  ctx->node_tiles_valid = true;
+  return ZF_OK;
+}
+
+int ib_interp_launch(zf_ctx* ctx) {
+  const CellArgs& c = ctx->cells;
+  IbArgs& a = ctx->ib;
+  const int64_t n = (int64_t)c.n_cells * (c.nn + c.nnn);
+  if (n == 0) return ZF_OK;
+  k_ib_interp<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(a, c);
+  ctx->launches += 1;
+  if (a.nw > 0) {
+    if (tiles_ok(a)) {
+      if (!ctx->node_tiles_valid) {
+        const int rc = ib_node_tiles_launch(ctx);
+        if (rc) return rc;
+      }
+      ZF_CUDA(cudaMemsetAsync(a.tile_ctr + 2, 0, sizeof(int32_t), ctx->stream));
+      k_wall_tiles<<<persistent_blocks(k_wall_tiles, kTileThreads), kTileThreads, 0, ctx->stream>>>(a, c);
+    } else {
+      k_ib_wall<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
+          a, c);
+    }
+    ctx->launches += 1;
+  }
   ZF_CUDA(cudaGetLastError());
   return ZF_OK;
 }
@@ -915,18 +1403,15 @@ int ib_bins_launch(zf_ctx* ctx) {
   int32_t* off = const_cast<int32_t*>(a.bin_off);
   ZF_CUDA(cudaMemsetAsync(counts, 0, (a.ns + 1) * sizeof(int32_t), ctx->stream));
   k_bin_assign<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(a, c, tri_bin, counts);
-  const int64_t nscan = a.ns + 1;
-  const int nb = (int)((nscan + 1023) / 1024);
-  k_scan_blocks<<<nb, 1024, 0, ctx->stream>>>(counts, nscan, off, bsum);
-  k_scan_sums<<<1, 32, 0, ctx->stream>>>(bsum, nb, bsum + nb);
-  k_scan_add<<<nb, 1024, 0, ctx->stream>>>(off, nscan, bsum);
+  scan_launch(counts, a.ns + 1, off, bsum, ctx->stream);
   ZF_CUDA(cudaMemsetAsync(counts, 0, (a.ns + 1) * sizeof(int32_t), ctx->stream));
   k_bin_fill<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(c, tri_bin, off, counts,
-                                                                       const_cast<int32_t*>(a.bin_tri));
+                                                                       const_cast<int32_t*>(a.bin_tri), a.bin_kk);
   k_bin_sort<<<(unsigned)((a.ns + 255) / 256), 256, 0, ctx->stream>>>(off, a.ns,
                                                                        const_cast<int32_t*>(a.bin_tri));
   k_bin_records<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(a, c, off + a.ns);
   ZF_CUDA(cudaGetLastError());
+  ctx->launches += 7;
   return ZF_OK;
 }
 
@@ -937,16 +1422,28 @@ int ib_nuc_memb_launch(zf_ctx* ctx, int rebuild) {
   k_nuc_memb<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c, rebuild,
                                                                      c.counters + 2);
   ZF_CUDA(cudaGetLastError());
+  ctx->launches += 1;
   return ZF_OK;
 }
 
 int ib_rbc_rbc_launch(zf_ctx* ctx) {
   const CellArgs& c = ctx->cells;
+  IbArgs& a = ctx->ib;
   const int64_t n = (int64_t)c.n_cells * c.nn;
   if (n == 0) return ZF_OK;
-  k_rbc_rbc<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
-      ctx->ib, c);
+  if (tiles_ok(a)) {
+    if (!ctx->node_tiles_valid) {
+      const int rc = ib_node_tiles_launch(ctx);
+      if (rc) return rc;
+    }
+    ZF_CUDA(cudaMemsetAsync(a.tile_ctr + 1, 0, sizeof(int32_t), ctx->stream));
+    k_rbc_tiles<<<persistent_blocks(k_rbc_tiles, kTileThreads), kTileThreads, 0, ctx->stream>>>(a, c);
+  } else {
+    k_rbc_rbc<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
+        a, c);
+  }
   ZF_CUDA(cudaGetLastError());
+  ctx->launches += 1;
   return ZF_OK;
 }
 
@@ -957,6 +1454,7 @@ int ib_spread_launch(zf_ctx* ctx) {
   k_ib_spread<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
       ctx->ib, c, ctx->p.wall_mode == ZF_WALL_REF_EQ);
   ZF_CUDA(cudaGetLastError());
+  ctx->launches += 1;
   return ZF_OK;
 }
 
@@ -965,6 +1463,8 @@ int ib_update_launch(zf_ctx* ctx) {
   if (c.n_cells == 0) return ZF_OK;
   k_update<<<c.n_cells, 256, 0, ctx->stream>>>(ctx->ib, c);
   ZF_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  ctx->node_tiles_valid = false;  // positions moved
   return ZF_OK;
 }
 

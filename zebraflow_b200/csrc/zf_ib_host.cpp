@@ -149,6 +149,18 @@ int ib_buffers(zf_ctx* c) {
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, const_cast<int32_t**>(&a.bin_tri), ntri))) return rc;
   if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_c, ntri))) return rc;
   if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_n, ntri))) return rc;
+  if ((rc = dalloc<uint8_t>(c, c->ib_allocs, &a.bin_kk, ntri))) return rc;
+  // node-tile lists
+  const int64_t nnodes = (int64_t)cl.n_cells * (cl.nn + cl.nnn);
+  a.ngrid = (int64_t)c->ntx * c->nty * c->ntz;
+  const int64_t ng1 = a.ngrid + 1;
+  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.node_gt, nnodes))) return rc;
+  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.node_cnt, ng1))) return rc;
+  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.node_off, ng1))) return rc;
+  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.node_sorted, nnodes))) return rc;
+  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.tile_list, std::min(a.ngrid, nnodes)))) return rc;
+  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.tile_ctr, 4))) return rc;
+  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.node_bsum, (ng1 + 1023) / 1024 + 1))) return rc;
   a.nuc_cap = std::max(1, c->p.nuc_list_max);
   const int64_t nnuc = (int64_t)cl.n_cells * cl.nnn;
   if ((rc = dalloc<uint16_t>(c, c->ib_allocs, &a.nuc_list, nnuc * a.nuc_cap))) return rc;
@@ -170,6 +182,7 @@ int ib_prepare(zf_ctx* c) {
   if (c->cells_set)
     if ((rc = ib_buffers(c))) return rc;
   c->nuc_lists_valid = false;
+  c->node_tiles_valid = false;
   return ZF_OK;
 }
 
@@ -313,9 +326,7 @@ static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
         ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (2 * c->prof_cap + c->prof_mem) + 1], c->stream));
         c->prof_mem++;
       }
-      // k_membrane, k_ib_interp, k_nuc_memb, 7 cell-list kernels (assign, 3
-      // scan passes, fill, sort, records), k_rbc_rbc, k_ib_spread, k_update
-      c->launches += 13 + (c->ib.nw > 0 ? 1 : 0);  // + k_ib_wall
+
     }
     c->status.iter = iter;
   }

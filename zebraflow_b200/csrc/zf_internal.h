@@ -156,6 +156,17 @@ struct IbArgs {
   const int32_t* bin_tri;       // [n_cells*nt] global triangle id = cell*nt + tri
   float4* bin_c;                // [n_cells*nt] per entry: centroid xyz, bounding radius
   float4* bin_n;                // [n_cells*nt] per entry: normal xyz, id (int bits)
+  uint8_t* bin_kk;              // [n_cells*nt] per entry: its key inside the tile (0..63)
+  // membrane and nucleus nodes grouped by the lattice tile of their nearest
+  // point (tile grid index over all ntx*nty*ntz tiles), rebuilt after positions change
+  int64_t ngrid;                // ntx*nty*ntz
+  int32_t* node_gt;             // [n_nodes] grid tile of node gid, -1 for removed cells
+  int32_t* node_cnt;            // [ngrid+1] counts, then fill cursors
+  int32_t* node_off;            // [ngrid+1] first sorted position of each grid tile
+  int32_t* node_sorted;         // [n_nodes] node gids grouped by grid tile
+  int32_t* tile_list;           // [min(ngrid, n_nodes)] grid tiles that hold nodes
+  int32_t* tile_ctr;            // [4] listed tiles, work counters of the tile kernels
+  int32_t* node_bsum;           // scan block sums
   // constants
   float vel_scale, gamma_p;
   double force_scale;           // 1/(UNITMASS*LBM_BFORCE_SCALE)
@@ -172,6 +183,7 @@ int ib_interp_launch(zf_ctx* c);
 int ib_bins_launch(zf_ctx* c);
 int ib_nuc_memb_launch(zf_ctx* c, int rebuild);
 int ib_rbc_rbc_launch(zf_ctx* c);
+int ib_node_tiles_launch(zf_ctx* c);
 int ib_spread_launch(zf_ctx* c);
 int ib_update_launch(zf_ctx* c);
 
@@ -232,6 +244,8 @@ struct zf_ctx {
   std::vector<void*> wall_allocs;  // wall + aux-tile buffers
   std::vector<void*> ib_allocs;    // cell list + nucleus lists (sized with the cells)
   bool nuc_lists_valid = false;    // nucleus-membrane lists built since the cells were set
+  bool node_tiles_valid = false;   // node-tile lists match the current positions
+  int tile_blocks = 0;             // persistent grid of the tile kernels
 
   // instrumentation: kernel launches, and optional event pairs around the LBM
   // kernel and the membrane block of zf_step
