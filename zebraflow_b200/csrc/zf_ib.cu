@@ -787,17 +787,16 @@ __global__ void __launch_bounds__(kRepWarps * 32) k_rbc_rbc(IbArgs a, CellArgs c
 //
 // Nodes are grouped by the lattice tile of their nearest lattice point
 // (lat_index, clamped into the box; z wrapped when periodic).  The +-4 window
-// of every node of a tile then lies inside the 3x3x3 tiles around it, so one
-// CTA stages what those 27 tiles hold into shared memory once (bin records of
-// the cell list; wall-node records of the lattice points) and its warps test
-// the tile's nodes against the staged copy.  Each test applies the node's own
-// window exactly, so the candidates are the reference's.  Needs three distinct
-// z tiles when z is periodic (nz >= 9); smaller periodic boxes use k_rbc_rbc
-// and k_ib_wall.
+// of every node of a tile then lies inside the 3x3x3 tiles around it, so a
+// warp that takes a tile finds all its nodes' candidates (bin records of the
+// cell list, W_index points) in those 27 tiles, which stay in L1 while it
+// walks the tile's nodes.  Each test applies the node's own window exactly,
+// so the candidates are the reference's.  Needs the z tiles to wrap with the
+// lattice when z is periodic (nz a multiple of 4, at least three tiles);
+// other periodic boxes use k_rbc_rbc and k_ib_wall.
 
 constexpr int kTileThreads = 256;
 constexpr int kTileWarps = kTileThreads / 32;
-constexpr int kStage = 1024;  // bin records staged per pass
 
 __device__ __forceinline__ int node_grid_tile(const IbArgs& a, float xp, float yp, float zp) {
   const int i0 = min(max(lat_index(xp, a.X0, a.DX), 0), a.nx - 1);
@@ -845,232 +844,184 @@ __global__ void k_node_fill(IbArgs a, CellArgs c) {
   if (pos == 0) a.tile_list[atomicAdd(&a.tile_ctr[0], 1)] = gt;
 }
 
-// RBC-RBC repulsion (ZebraflowWT.c:9911-10053) over the staged bin records.
-// Lanes split a node's records; each lane sums its contributions, and a fixed
-// butterfly adds the lanes, so the result is deterministic.
+// One warp per tile (taken from a work counter), no block-level barriers: the
+// tile's nodes are handled one after another by the warp, and what the 27
+// neighbour tiles hold is read from global memory, where it stays in L1 while
+// the warp walks the tile's nodes.
+__device__ __forceinline__ int warp_next_tile(int32_t* ctr, int lane) {
+  int li = 0;
+  if (lane == 0) li = atomicAdd(ctr, 1);
+  return __shfl_sync(0xffffffffu, li, 0);
+}
+
+// neighbour r = (dz+1)*9 + (dy+1)*3 + (dx+1) of grid tile (tx, ty, tz): its
+// tile id in the lattice view, -1 when outside the box or absent
+__device__ __forceinline__ int neighbour_tile(const IbArgs& a, int tx, int ty, int tz, int r, int& X, int& Y,
+                                              int& Z) {
+  X = tx + r % 3 - 1;
+  Y = ty + (r / 3) % 3 - 1;
+  Z = tz + r / 9 - 1;
+  if (X < 0 || X >= a.ntx || Y < 0 || Y >= a.nty) return -1;
+  if (a.per_z) {
+    if (Z < 0) Z += a.ntz;
+    else if (Z >= a.ntz) Z -= a.ntz;
+  } else if (Z < 0 || Z >= a.ntz) {
+    return -1;
+  }
+  return a.tile_map[((int64_t)Z * a.nty + Y) * a.ntx + X];
+}
+
+// RBC-RBC repulsion (ZebraflowWT.c:9911-10053).  For each node the warp reads
+// the bin records of the 27 tiles 32 at a time and keeps those in the node's
+// +-4 window that pass the cheap filters; they queue up and are evaluated 32
+// at a time, one per lane.  Lane sums meet in a fixed butterfly, so the result
+// is deterministic.
 __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c) {
-  __shared__ float4 s_c[kStage];
-  __shared__ float4 s_n[kStage];
-  __shared__ int2 s_p[kStage];
-  __shared__ int s_r0[28], s_e0[27], s_tx[27], s_ty[27], s_tz[27];
-  __shared__ float s_acc[kTileThreads][3];
   __shared__ int s_q[kTileWarps][64];
-  __shared__ int s_li;
   const unsigned FULL = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nc = c.n_cells;
   const int64_t nmem = (int64_t)nc * c.nn;
   const int64_t n_pop_tiles = a.ns / ZF_TC;
   const int nlist = a.tile_ctr[0];
-  while (true) {
-    __syncthreads();
-    if (threadIdx.x == 0) s_li = atomicAdd(&a.tile_ctr[1], 1);
-    __syncthreads();
-    const int li = s_li;
-    if (li >= nlist) break;
+  int* queue = s_q[warp];
+  for (int li = warp_next_tile(&a.tile_ctr[1], lane); li < nlist; li = warp_next_tile(&a.tile_ctr[1], lane)) {
     const int gt = a.tile_list[li];
     const int tx = gt % a.ntx, ty = (gt / a.ntx) % a.nty, tz = gt / (a.ntx * a.nty);
-    if (threadIdx.x < 27) {  // record range of each of the 27 tiles
-      const int r = threadIdx.x;
-      int X = tx + r % 3 - 1, Y = ty + (r / 3) % 3 - 1, Z = tz + r / 9 - 1;
-      bool ok = X >= 0 && X < a.ntx && Y >= 0 && Y < a.nty;
-      if (a.per_z) Z = (Z + a.ntz) % a.ntz;
-      else ok = ok && Z >= 0 && Z < a.ntz;
-      int e0 = 0, len = 0;
-      if (ok) {
-        const int t = a.tile_map[((int64_t)Z * a.nty + Y) * a.ntx + X];
-        if (t >= 0 && t < n_pop_tiles) {
-          e0 = a.bin_off[(int64_t)t * ZF_TC];
-          len = a.bin_off[(int64_t)t * ZF_TC + ZF_TC] - e0;
-        }
+    // lane r < 27: record range and tile coordinates of neighbour r
+    int re0 = 0, rlen = 0, rx4 = 0, ry4 = 0, rz4 = 0;
+    if (lane < 27) {
+      int X, Y, Z;
+      const int t = neighbour_tile(a, tx, ty, tz, lane, X, Y, Z);
+      if (t >= 0 && t < n_pop_tiles) {
+        re0 = a.bin_off[(int64_t)t * ZF_TC];
+        rlen = a.bin_off[(int64_t)t * ZF_TC + ZF_TC] - re0;
       }
-      s_e0[r] = e0;
-      s_r0[r + 1] = len;
-      s_tx[r] = X;
-      s_ty[r] = Y;
-      s_tz[r] = Z;
+      rx4 = 4 * X;
+      ry4 = 4 * Y;
+      rz4 = 4 * Z;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_r0[0] = 0;
-      for (int r = 0; r < 27; ++r) s_r0[r + 1] += s_r0[r];
-    }
-    __syncthreads();
-    const int R = s_r0[27];
     const int n0 = a.node_off[gt], n1 = a.node_off[gt + 1];
-    if (R == 0) continue;
-    for (int g0 = n0; g0 < n1; g0 += kTileThreads) {
-      const int gn = min(kTileThreads, n1 - g0);
-      s_acc[threadIdx.x][0] = s_acc[threadIdx.x][1] = s_acc[threadIdx.x][2] = 0.f;
-      for (int f0 = 0; f0 < R; f0 += kStage) {
-        const int fn = min(kStage, R - f0);
-        __syncthreads();
-        for (int f = threadIdx.x; f < fn; f += kTileThreads) {
-          const int gf = f0 + f;
-          int r = 0;
-          while (gf >= s_r0[r + 1]) ++r;
-          const int64_t e = s_e0[r] + (gf - s_r0[r]);
-          const int kk = a.bin_kk[e];
-          s_c[f] = a.bin_c[e];
-          s_n[f] = a.bin_n[e];
-          s_p[f] = make_int2((s_tx[r] * 4 + ((kk >> 4) & 3)) | ((s_ty[r] * 4 + ((kk >> 2) & 3)) << 16),
-                             s_tz[r] * 4 + (kk & 3));
+    for (int q = n0; q < n1; ++q) {
+      const int64_t gid = a.node_sorted[q];
+      if (gid >= nmem) continue;  // nucleus node: no RBC-RBC term
+      const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
+      if (c.status[cell] <= 0) continue;
+      float xc, yc, zc;
+      node_pos(c.x, nc, c.nn, cell, node, a.LZ, a.Z0, xc, yc, zc);
+      const float e1x = c.node_normal[((size_t)0 * nc + cell) * c.nn + node];
+      const float e1y = c.node_normal[((size_t)1 * nc + cell) * c.nn + node];
+      const float e1z = c.node_normal[((size_t)2 * nc + cell) * c.nn + node];
+      const int i0 = lat_index(xc, a.X0, a.DX), j0 = lat_index(yc, a.Y0, a.DX),
+                k0 = lat_index(zc, a.Z0, a.DX);
+      const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
+      const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
+      const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
+      const int k1w = a.per_z ? ((k1 % a.nz) + a.nz) % a.nz : k1;  // window start, wrapped
+      const int g_own = cell * c.nt;
+      float rx = 0.f, ry = 0.f, rz = 0.f;
+      int qn = 0;
+      auto flush = [&](int nb) {
+        __syncwarp();
+        if (lane < nb) {
+          const int e = queue[lane];
+          float tx2, ty2, tz2;
+          rbc_entry(a, c, a.bin_c[e], __float_as_int(a.bin_n[e].w), xc, yc, zc, tx2, ty2, tz2);
+          rx += tx2;
+          ry += ty2;
+          rz += tz2;
         }
-        __syncthreads();
-        for (int q = warp; q < gn; q += kTileWarps) {
-          const int64_t gid = a.node_sorted[g0 + q];
-          if (gid >= nmem) continue;  // nucleus node: no RBC-RBC term
-          const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
-          if (c.status[cell] <= 0) continue;
-          float xc, yc, zc;
-          node_pos(c.x, nc, c.nn, cell, node, a.LZ, a.Z0, xc, yc, zc);
-          const float e1x = c.node_normal[((size_t)0 * nc + cell) * c.nn + node];
-          const float e1y = c.node_normal[((size_t)1 * nc + cell) * c.nn + node];
-          const float e1z = c.node_normal[((size_t)2 * nc + cell) * c.nn + node];
-          const int i0 = lat_index(xc, a.X0, a.DX), j0 = lat_index(yc, a.Y0, a.DX),
-                    k0 = lat_index(zc, a.Z0, a.DX);
-          const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
-          const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
-          const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
-          // lanes filter 32 records at a time; the records that pass queue up
-          // and are evaluated 32 at a time, one per lane
-          float rx = 0.f, ry = 0.f, rz = 0.f;
-          int qn = 0;
-          int* queue = s_q[warp];
-          for (int f0 = 0; f0 < fn; f0 += 32) {
-            const int f = f0 + lane;
-            bool pass = false;
-            if (f < fn) {
-              const int2 pp = s_p[f];
-              const int bi = pp.x & 0xffff, bj = pp.x >> 16, bk = pp.y;
-              bool in = bi >= i1 && bi <= i2 && bj >= j1 && bj <= j2;
-              if (a.per_z) {
-                int dk = (bk - k1) % a.nz;
-                if (dk < 0) dk += a.nz;
-                in = in && dk <= k2 - k1;
-              } else {
-                in = in && bk >= k1 && bk <= k2;
-              }
-              if (in) {
-                const float4 cr = s_c[f];
-                const float dzc = wrapd(cr.z - zc, a.LZ);
-                const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
+        const int rem = qn - nb;
+        const int tq = lane < rem ? queue[nb + lane] : 0;
+        __syncwarp();
+        if (lane < rem) queue[lane] = tq;
+        __syncwarp();
+        qn = rem;
+      };
+      for (int r = 0; r < 27; ++r) {
+        const int e0 = __shfl_sync(FULL, re0, r), len = __shfl_sync(FULL, rlen, r);
+        const int bx = __shfl_sync(FULL, rx4, r), by = __shfl_sync(FULL, ry4, r), bz = __shfl_sync(FULL, rz4, r);
+        for (int o = 0; o < len; o += 32) {
+          bool pass = false;
+          const int e = e0 + o + lane;
+          if (o + lane < len) {
+            const int kk = a.bin_kk[e];
+            const int bi = bx + ((kk >> 4) & 3), bj = by + ((kk >> 2) & 3), bk = bz + (kk & 3);
+            int dk = bk - k1w;
+            if (a.per_z && dk < 0) dk += a.nz;
+            if (bi >= i1 && bi <= i2 && bj >= j1 && bj <= j2 && dk >= 0 && dk <= k2 - k1) {
+              const float4 cr = a.bin_c[e];
+              const float dzc = wrapd(cr.z - zc, a.LZ);
+              const float ddx = xc - cr.x, ddy = yc - cr.y;
+              // squared distance well beyond 2 um: fails the exact test below
+              if (ddx * ddx + ddy * ddy + dzc * dzc < 4.01f) {
+                const float dcen = dist3(ddx, ddy, -dzc);
                 if (dcen < 2.f && !(dcen - cr.w > 1.f)) {
-                  const float4 nr = s_n[f];
+                  const float4 nr = a.bin_n[e];
                   if (e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
                     const int g = __float_as_int(nr.w);
-                    const int m = g / c.nt;
                     pass = true;
-                    if (m == cell) {
-                      const int tri = g - m * c.nt;
+                    if (g >= g_own && g < g_own + c.nt) {
+                      const int tri = g - g_own;
                       pass = !(c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node);
                     }
                   }
                 }
               }
             }
-            const unsigned bal = __ballot_sync(FULL, pass);
-            if (pass) queue[qn + __popc(bal & ((1u << lane) - 1u))] = f;
-            qn += __popc(bal);
-            while (qn >= 32 || (f0 + 32 >= fn && qn > 0)) {
-              __syncwarp();
-              const int nb = min(qn, 32);
-              if (lane < nb) {
-                const int fq = queue[lane];
-                float tx2, ty2, tz2;
-                rbc_entry(a, c, s_c[fq], __float_as_int(s_n[fq].w), xc, yc, zc, tx2, ty2, tz2);
-                rx += tx2;
-                ry += ty2;
-                rz += tz2;
-              }
-              __syncwarp();
-              const int rem = qn - nb;
-              const int tq = lane < rem ? queue[nb + lane] : 0;
-              __syncwarp();
-              if (lane < rem) queue[lane] = tq;
-              __syncwarp();
-              qn = rem;
-            }
           }
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            rx += __shfl_xor_sync(FULL, rx, o);
-            ry += __shfl_xor_sync(FULL, ry, o);
-            rz += __shfl_xor_sync(FULL, rz, o);
-          }
-          if (lane == 0) {
-            s_acc[q][0] += rx;
-            s_acc[q][1] += ry;
-            s_acc[q][2] += rz;
-          }
+          const unsigned bal = __ballot_sync(FULL, pass);
+          if (pass) queue[qn + __popc(bal & ((1u << lane) - 1u))] = e;
+          qn += __popc(bal);
+          if (qn >= 32) flush(32);
         }
       }
-      __syncthreads();
-      if (threadIdx.x < gn) {
-        const int64_t gid = a.node_sorted[g0 + threadIdx.x];
-        if (gid < nmem) {
-          const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
-          if (c.status[cell] > 0) {
-            c.wrep[((size_t)0 * nc + cell) * c.nn + node] += s_acc[threadIdx.x][0];
-            c.wrep[((size_t)1 * nc + cell) * c.nn + node] += s_acc[threadIdx.x][1];
-            c.wrep[((size_t)2 * nc + cell) * c.nn + node] += s_acc[threadIdx.x][2];
-          }
-        }
+      while (qn > 0) flush(min(qn, 32));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        rx += __shfl_xor_sync(FULL, rx, o);
+        ry += __shfl_xor_sync(FULL, ry, o);
+        rz += __shfl_xor_sync(FULL, rz, o);
+      }
+      if (lane == 0) {
+        c.wrep[((size_t)0 * nc + cell) * c.nn + node] += rx;
+        c.wrep[((size_t)1 * nc + cell) * c.nn + node] += ry;
+        c.wrep[((size_t)2 * nc + cell) * c.nn + node] += rz;
       }
     }
   }
 }
 
-// Nearest wall triangle and wall repulsion (as k_ib_wall) over the staged
-// W_index and wall-node records of the 27 tiles.  A warp takes one node and
-// walks its window 32 points at a time in the reference scan order; each lane
-// gives the first minimum of its point's list (skipped when the point repeats
-// the previous point's wall node or cannot reach the running bound); the
-// lowest lane holding the chunk minimum is the first candidate in scan order,
-// and it replaces the running minimum only when strictly smaller.
+// Nearest wall triangle and wall repulsion (as k_ib_wall).  A warp takes a
+// tile and then its nodes one by one, walking each node's window 32 points
+// at a time in the reference scan order (i, j, k).  A first pass finds the
+// window's nearest wall node; the first minimum of its list bounds the window
+// minimum from above.  The second pass skips a point that repeats the
+// previous point's wall node or whose wall node cannot reach the bound, and
+// queues the other lists in scan order; they are scanned 32 at a time, one
+// per lane, and folded in queue order: the lowest lane holding the batch
+// minimum is the first candidate in scan order, and it replaces the running
+// minimum only when strictly smaller.
 __global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs c) {
-  __shared__ float4 s_wn[27 * ZF_TC];
-  __shared__ int s_wi[27 * ZF_TC];
   __shared__ int s_q[kTileWarps][64];
-  __shared__ int s_li, s_any;
   const unsigned FULL = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nc = c.n_cells;
   const int nlist = a.tile_ctr[0];
-  while (true) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_li = atomicAdd(&a.tile_ctr[2], 1);
-      s_any = 0;
-    }
-    __syncthreads();
-    const int li = s_li;
-    if (li >= nlist) break;
+  int* queue = s_q[warp];
+  for (int li = warp_next_tile(&a.tile_ctr[2], lane); li < nlist; li = warp_next_tile(&a.tile_ctr[2], lane)) {
     const int gt = a.tile_list[li];
     const int tx = gt % a.ntx, ty = (gt / a.ntx) % a.nty, tz = gt / (a.ntx * a.nty);
-    for (int idx = threadIdx.x; idx < 27 * ZF_TC; idx += kTileThreads) {
-      const int r = idx >> 6, o = idx & 63;
-      int X = tx + r % 3 - 1, Y = ty + (r / 3) % 3 - 1, Z = tz + r / 9 - 1;
-      bool ok = X >= 0 && X < a.ntx && Y >= 0 && Y < a.nty;
-      if (a.per_z) Z = (Z + a.ntz) % a.ntz;
-      else ok = ok && Z >= 0 && Z < a.ntz;
-      int wi = 0;
-      float4 wn = make_float4(0.f, 0.f, 0.f, -1.f);
-      if (ok) {
-        const int t = a.tile_map[((int64_t)Z * a.nty + Y) * a.ntx + X];
-        if (t >= 0 && a.tile_wall[t]) {
-          wi = a.windex[(int64_t)t * ZF_TC + o];
-          wn = a.wnode[(int64_t)t * ZF_TC + o];
-          if (o == 0) s_any = 1;
-        }
-      }
-      s_wi[idx] = wi;
-      s_wn[idx] = wn;
+    // lane r < 27: tile id of neighbour r when it holds W_index points
+    int rt = -1;
+    if (lane < 27) {
+      int X, Y, Z;
+      const int t = neighbour_tile(a, tx, ty, tz, lane, X, Y, Z);
+      if (t >= 0 && a.tile_wall[t]) rt = t;
     }
-    __syncthreads();
-    if (!s_any) continue;
+    if (!__any_sync(FULL, rt >= 0)) continue;
     const int n0 = a.node_off[gt], n1 = a.node_off[gt + 1];
-    for (int q = n0 + warp; q < n1; q += kTileWarps) {
+    for (int q = n0; q < n1; ++q) {
       const int64_t gid = a.node_sorted[q];
       bool nuc;
       int cell, node;
@@ -1085,24 +1036,17 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs 
       const int k1 = max(k0 - 4, a.kmin), k2 = min(k0 + 4, a.kmax);
       if (i1 > i2 || j1 > j2 || k1 > k2) continue;
       const int ni = i2 - i1 + 1, nj = j2 - j1 + 1, nk = k2 - k1 + 1;
-      // staged index of lattice point (i, j, k) of the window
-      auto sidx = [&](int i, int j, int k) {
-        const int kw = wrapk(a, k);
-        const int lx = (i >> 2) - tx + 1, ly = (j >> 2) - ty + 1;
-        int lz = (kw >> 2) - tz + 1;
-        if (a.per_z) lz = ((lz % a.ntz) + a.ntz) % a.ntz;
-        return ((lz * 3 + ly) * 3 + lx) * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (kw & 3);
-      };
-      // lane l starts at window point l (scan order i, j, k) and steps 32
-      // points at a time in mixed radix
+      const int k1w = wrapk(a, k1);
       const int npts = ni * nj * nk;
+      // lane l starts at window point l and steps 32 points in mixed radix;
+      // (i, j, dk) with the wrapped z index kw = k1w + dk (minus nz past the end)
       const int sk = 32 % nk, sj = (32 / nk) % nj, si = 32 / (nk * nj);
-      const int pi0 = i1 + lane / (nj * nk), pj0 = j1 + (lane / nk) % nj, pk0 = k1 + lane % nk;
-      auto step = [&](int& i, int& j, int& k) {
-        k += sk;
+      const int pi0 = i1 + lane / (nj * nk), pj0 = j1 + (lane / nk) % nj, pk0 = lane % nk;
+      auto step = [&](int& i, int& j, int& dk) {
+        dk += sk;
         int cy = 0;
-        if (k > k2) {
-          k -= nk;
+        if (dk >= nk) {
+          dk -= nk;
           cy = 1;
         }
         j += sj + cy;
@@ -1113,26 +1057,36 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs 
         }
         i += si + cy;
       };
-      // bound: the first minimum of the list of the window's nearest wall
-      // node (any list of the window bounds the window minimum from above;
-      // 1.5 is the reference's starting value)
+      // slot of window point (i, j, dk) in the IB view, -1 outside the wall tiles
+      auto slot = [&](int i, int j, int dk) -> int64_t {
+        int kw = k1w + dk;
+        if (kw >= a.nz) kw -= a.nz;
+        int lz = (kw >> 2) - tz + 1;
+        if (lz < 0) lz += a.ntz;
+        else if (lz > 2) lz -= a.ntz;
+        const int r = (lz * 3 + ((j >> 2) - ty + 1)) * 3 + ((i >> 2) - tx + 1);
+        const int t = __shfl_sync(FULL, rt, r);  // every lane calls slot()
+        return t < 0 ? (int64_t)-1 : (int64_t)t * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (kw & 3);
+      };
       float bound = 1.5f;
       {
         float dbest = 3.0e38f;
         int mbest = 0;
-        int i = pi0, j = pj0, k = pk0;
-        for (int p = lane; p < npts; p += 32) {
-          const int si2 = sidx(i, j, k);
-          const int wi = s_wi[si2];
-          if (wi > 0) {
-            const float4 wn = s_wn[si2];
-            const float dm = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
-            if (dm < dbest) {
-              dbest = dm;
-              mbest = wi;
+        int i = pi0, j = pj0, dk = pk0;
+        for (int p0 = 0; p0 < npts; p0 += 32) {
+          const int64_t s = slot(i, j, dk);
+          if (p0 + lane < npts && s >= 0) {
+            const int wi = a.windex[s];
+            if (wi > 0) {
+              const float4 wn = a.wnode[s];
+              const float dm = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
+              if (dm < dbest) {
+                dbest = dm;
+                mbest = wi;
+              }
             }
           }
-          step(i, j, k);
+          step(i, j, dk);
         }
         float dmin = dbest;
 #pragma unroll
@@ -1144,11 +1098,8 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs 
           wall_list_min(a, m, xp, yp, zp, bound, unused);
         }
       }
-      // walk in scan order; lists that can still reach the minimum queue up
-      // (in scan order) and are scanned 32 at a time, one per lane
       float mindis = 1.5f;
       int triwall = -1, last = 0, qn = 0;
-      int* queue = s_q[warp];
       auto flush = [&](int nb) {
         __syncwarp();
         float d = 3.0e38f;
@@ -1170,16 +1121,16 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs 
         qn = rem;
       };
       {
-        int i = pi0, j = pj0, k = pk0;
+        int i = pi0, j = pj0, dk = pk0;
         for (int p0 = 0; p0 < npts; p0 += 32) {
           int wi = 0;
           float4 wn = make_float4(0.f, 0.f, 0.f, -1.f);
-          if (p0 + lane < npts) {
-            const int si2 = sidx(i, j, k);
-            wi = s_wi[si2];
-            if (wi > 0) wn = s_wn[si2];
+          const int64_t s = slot(i, j, dk);
+          if (p0 + lane < npts && s >= 0) {
+            wi = a.windex[s];
+            if (wi > 0) wn = a.wnode[s];
           }
-          step(i, j, k);
+          step(i, j, dk);
           int prev = __shfl_up_sync(FULL, wi, 1);
           if (lane == 0) prev = last;
           last = __shfl_sync(FULL, wi, 31);
