@@ -467,6 +467,15 @@ __global__ void k_bin_sort(const int32_t* off, int64_t ns, int32_t* bin_tri) {
   }
 }
 
+// The w word of a bin record holds the entry's key inside its tile (low 8
+// bits) and the bounding radius rounded up to 2^-20 um (high 24 bits).
+__device__ __forceinline__ float rec_pack(int kk, float rb) {
+  const unsigned q = min((unsigned)ceilf(rb * 1048576.f), 0xffffffu);
+  return __uint_as_float((q << 8) | (unsigned)kk);
+}
+__device__ __forceinline__ int rec_kk(float w) { return (int)(__float_as_uint(w) & 0xffu); }
+__device__ __forceinline__ float rec_rb(float w) { return (float)(__float_as_uint(w) >> 8) * (1.f / 1048576.f); }
+
 // per bin entry: centroid and bounding radius, normal and triangle id, so the
 // repulsion search reads one contiguous range of 32-byte records per run of
 // bins.  The radius bounds the distance from the centroid to any point of the
@@ -488,7 +497,7 @@ __global__ void k_bin_records(IbArgs a, CellArgs c, const int32_t* total) {
     const float dz = (float)c.x[((size_t)2 * nc + m) * c.nn + n] - cz;
     r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
   }
-  a.bin_c[e] = make_float4(cx, cy, cz, sqrtf(r2) * 1.0001f + 1e-3f);
+  a.bin_c[e] = make_float4(cx, cy, cz, rec_pack(a.bin_kk[e], sqrtf(r2) * 1.0001f + 1e-3f));
   a.bin_n[e] = make_float4(c.tri_nrm[((size_t)0 * nc + m) * c.nt + tri],
                            c.tri_nrm[((size_t)1 * nc + m) * c.nt + tri],
                            c.tri_nrm[((size_t)2 * nc + m) * c.nt + tri], __int_as_float(g));
@@ -602,7 +611,9 @@ __device__ __forceinline__ void rbc_entry(const IbArgs& a, const CellArgs& c, co
   const int n1 = c.tri[3 * tri], n2 = c.tri[3 * tri + 1], n3 = c.tri[3 * tri + 2];
   const float dzc = wrapd(cr.z - zc, a.LZ);
   const float shift = (cr.z - zc) - dzc;  // periodic image of the other cell
-  float tp[16][3], tc[17][3];
+  // the 15 points of the subdivided triangle, then the 16 sub-triangle
+  // centroids one at a time (ZebraflowWT.c:9981-10027)
+  float tp[16][3];
 #pragma unroll
   for (int v = 0; v < 3; ++v) {
     const float off = v == 2 ? shift : 0.f;
@@ -621,27 +632,18 @@ __device__ __forceinline__ void rbc_entry(const IbArgs& a, const CellArgs& c, co
     tp[13][v] = 0.5f * (tp[4][v] + tp[6][v]);
     tp[14][v] = 0.5f * (tp[4][v] + tp[5][v]);
     tp[15][v] = 0.5f * (tp[5][v] + tp[6][v]);
-    tc[1][v] = (tp[1][v] + tp[7][v] + tp[12][v]) / 3.f;
-    tc[2][v] = (tp[7][v] + tp[13][v] + tp[12][v]) / 3.f;
-    tc[3][v] = (tp[7][v] + tp[4][v] + tp[13][v]) / 3.f;
-    tc[4][v] = (tp[4][v] + tp[14][v] + tp[13][v]) / 3.f;
-    tc[5][v] = (tp[4][v] + tp[8][v] + tp[14][v]) / 3.f;
-    tc[6][v] = (tp[8][v] + tp[9][v] + tp[14][v]) / 3.f;
-    tc[7][v] = (tp[8][v] + tp[2][v] + tp[9][v]) / 3.f;
-    tc[8][v] = (tp[12][v] + tp[13][v] + tp[6][v]) / 3.f;
-    tc[9][v] = (tp[13][v] + tp[15][v] + tp[6][v]) / 3.f;
-    tc[10][v] = (tp[13][v] + tp[14][v] + tp[15][v]) / 3.f;
-    tc[11][v] = (tp[14][v] + tp[5][v] + tp[15][v]) / 3.f;
-    tc[12][v] = (tp[14][v] + tp[9][v] + tp[5][v]) / 3.f;
-    tc[13][v] = (tp[6][v] + tp[15][v] + tp[11][v]) / 3.f;
-    tc[14][v] = (tp[15][v] + tp[10][v] + tp[11][v]) / 3.f;
-    tc[15][v] = (tp[15][v] + tp[5][v] + tp[10][v]) / 3.f;
-    tc[16][v] = (tp[11][v] + tp[10][v] + tp[3][v]) / 3.f;
   }
+  // sub-triangle v = 1..16: corners (kSubA, kSubB, kSubC)[v-1]
+  constexpr int kSubA[16] = {1, 7, 7, 4, 4, 8, 8, 12, 13, 13, 14, 14, 6, 15, 15, 11};
+  constexpr int kSubB[16] = {7, 13, 4, 14, 8, 9, 2, 13, 15, 14, 5, 9, 15, 10, 5, 10};
+  constexpr int kSubC[16] = {12, 12, 13, 13, 14, 14, 9, 6, 6, 15, 15, 5, 11, 11, 10, 3};
   tx = ty = tz = 0.f;
 #pragma unroll
-  for (int v = 1; v <= 16; ++v) {  // ZebraflowWT.c:10028-10042
-    const float dx = tc[v][0] - xc, dy = tc[v][1] - yc, dz = tc[v][2] - zc;
+  for (int v = 0; v < 16; ++v) {  // ZebraflowWT.c:10028-10042
+    const float cx = (tp[kSubA[v]][0] + tp[kSubB[v]][0] + tp[kSubC[v]][0]) / 3.f;
+    const float cy = (tp[kSubA[v]][1] + tp[kSubB[v]][1] + tp[kSubC[v]][1]) / 3.f;
+    const float cz = (tp[kSubA[v]][2] + tp[kSubB[v]][2] + tp[kSubC[v]][2]) / 3.f;
+    const float dx = cx - xc, dy = cy - yc, dz = cz - zc;
     const float d = dist3(dx, dy, dz);
     if (d < 1.0f) {
       const float repulf = (float)(-8.333e-07 * (1.0 - (double)d) / 1.0);
@@ -738,7 +740,7 @@ __global__ void __launch_bounds__(kRepWarps * 32) k_rbc_rbc(IbArgs a, CellArgs c
       const float4 cr = a.bin_c[e];
       const float dzc = wrapd(cr.z - zc, a.LZ);
       const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
-      if (dcen < 2.f && !(dcen - cr.w > 1.f)) {
+      if (dcen < 2.f && !(dcen - rec_rb(cr.w) > 1.f)) {
         const float4 nr = a.bin_n[e];
         if (e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
           const int g = __float_as_int(nr.w);
@@ -878,6 +880,8 @@ __device__ __forceinline__ int neighbour_tile(const IbArgs& a, int tx, int ty, i
 // is deterministic.
 __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c) {
   __shared__ int s_q[kTileWarps][64];
+  __shared__ int s_re0[kTileWarps][27], s_rcum[kTileWarps][28];
+  __shared__ int s_rxyz[kTileWarps][27][3];
   const unsigned FULL = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nc = c.n_cells;
@@ -885,24 +889,39 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
   const int64_t n_pop_tiles = a.ns / ZF_TC;
   const int nlist = a.tile_ctr[0];
   int* queue = s_q[warp];
+  int* re0 = s_re0[warp];
+  int* rcum = s_rcum[warp];
   for (int li = warp_next_tile(&a.tile_ctr[1], lane); li < nlist; li = warp_next_tile(&a.tile_ctr[1], lane)) {
     const int gt = a.tile_list[li];
     const int tx = gt % a.ntx, ty = (gt / a.ntx) % a.nty, tz = gt / (a.ntx * a.nty);
-    // lane r < 27: record range and tile coordinates of neighbour r
-    int re0 = 0, rlen = 0, rx4 = 0, ry4 = 0, rz4 = 0;
+    // record range and lattice origin of each of the 27 tiles; the ranges
+    // are walked as one sequence (rcum: starts of the ranges in it)
+    int len = 0;
     if (lane < 27) {
       int X, Y, Z;
       const int t = neighbour_tile(a, tx, ty, tz, lane, X, Y, Z);
+      int e0 = 0;
       if (t >= 0 && t < n_pop_tiles) {
-        re0 = a.bin_off[(int64_t)t * ZF_TC];
-        rlen = a.bin_off[(int64_t)t * ZF_TC + ZF_TC] - re0;
+        e0 = a.bin_off[(int64_t)t * ZF_TC];
+        len = a.bin_off[(int64_t)t * ZF_TC + ZF_TC] - e0;
       }
-      rx4 = 4 * X;
-      ry4 = 4 * Y;
-      rz4 = 4 * Z;
+      re0[lane] = e0;
+      s_rxyz[warp][lane][0] = 4 * X;
+      s_rxyz[warp][lane][1] = 4 * Y;
+      s_rxyz[warp][lane][2] = 4 * Z;
     }
+    int cum = len;  // inclusive warp scan of the lengths
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(FULL, cum, o);
+      if (lane >= o) cum += v;
+    }
+    if (lane < 27) rcum[lane + 1] = cum;
+    if (lane == 0) rcum[0] = 0;
+    __syncwarp();
+    const int rtot = rcum[27];
     const int n0 = a.node_off[gt], n1 = a.node_off[gt + 1];
-    for (int q = n0; q < n1; ++q) {
+    for (int q = n0; q < n1 && rtot > 0; ++q) {
       const int64_t gid = a.node_sorted[q];
       if (gid >= nmem) continue;  // nucleus node: no RBC-RBC term
       const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
@@ -938,43 +957,60 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
         __syncwarp();
         qn = rem;
       };
-      for (int r = 0; r < 27; ++r) {
-        const int e0 = __shfl_sync(FULL, re0, r), len = __shfl_sync(FULL, rlen, r);
-        const int bx = __shfl_sync(FULL, rx4, r), by = __shfl_sync(FULL, ry4, r), bz = __shfl_sync(FULL, rz4, r);
-        for (int o = 0; o < len; o += 32) {
-          bool pass = false;
-          const int e = e0 + o + lane;
-          if (o + lane < len) {
-            const int kk = a.bin_kk[e];
-            const int bi = bx + ((kk >> 4) & 3), bj = by + ((kk >> 2) & 3), bk = bz + (kk & 3);
-            int dk = bk - k1w;
-            if (a.per_z && dk < 0) dk += a.nz;
-            if (bi >= i1 && bi <= i2 && bj >= j1 && bj <= j2 && dk >= 0 && dk <= k2 - k1) {
-              const float4 cr = a.bin_c[e];
-              const float dzc = wrapd(cr.z - zc, a.LZ);
-              const float ddx = xc - cr.x, ddy = yc - cr.y;
-              // squared distance well beyond 2 um: fails the exact test below
-              if (ddx * ddx + ddy * ddy + dzc * dzc < 4.01f) {
-                const float dcen = dist3(ddx, ddy, -dzc);
-                if (dcen < 2.f && !(dcen - cr.w > 1.f)) {
-                  const float4 nr = a.bin_n[e];
-                  if (e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
-                    const int g = __float_as_int(nr.w);
-                    pass = true;
-                    if (g >= g_own && g < g_own + c.nt) {
-                      const int tri = g - g_own;
-                      pass = !(c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node);
-                    }
+      // lane l takes positions l, l+32, ... of the sequence; the record of the
+      // next position is loaded before the current one is tested
+      int r = 0;
+      auto entry = [&](int f) {
+        while (f >= rcum[r + 1]) ++r;
+        return re0[r] + (f - rcum[r]);
+      };
+      int e_n = 0, r_n = 0;
+      float4 c_n = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (lane < rtot) {
+        e_n = entry(lane);
+        r_n = r;
+        c_n = a.bin_c[e_n];
+      }
+      for (int f0 = 0; f0 < rtot; f0 += 32) {
+        const int f = f0 + lane;
+        const int e = e_n, rr = r_n;
+        const float4 cr = c_n;
+        if (f + 32 < rtot) {
+          e_n = entry(f + 32);
+          r_n = r;
+          c_n = a.bin_c[e_n];
+        }
+        bool pass = false;
+        if (f < rtot) {
+          const int kk = rec_kk(cr.w);
+          const int bi = s_rxyz[warp][rr][0] + ((kk >> 4) & 3), bj = s_rxyz[warp][rr][1] + ((kk >> 2) & 3),
+                    bk = s_rxyz[warp][rr][2] + (kk & 3);
+          int dk = bk - k1w;
+          if (a.per_z && dk < 0) dk += a.nz;
+          if (bi >= i1 && bi <= i2 && bj >= j1 && bj <= j2 && dk >= 0 && dk <= k2 - k1) {
+            const float dzc = wrapd(cr.z - zc, a.LZ);
+            const float ddx = xc - cr.x, ddy = yc - cr.y;
+            // a squared distance well beyond 2 um fails the exact test below
+            if (ddx * ddx + ddy * ddy + dzc * dzc < 4.01f) {
+              const float dcen = dist3(ddx, ddy, -dzc);
+              if (dcen < 2.f && !(dcen - rec_rb(cr.w) > 1.f)) {
+                const float4 nr = a.bin_n[e];
+                if (e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
+                  const int g = __float_as_int(nr.w);
+                  pass = true;
+                  if (g >= g_own && g < g_own + c.nt) {
+                    const int tri = g - g_own;
+                    pass = !(c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node);
                   }
                 }
               }
             }
           }
-          const unsigned bal = __ballot_sync(FULL, pass);
-          if (pass) queue[qn + __popc(bal & ((1u << lane) - 1u))] = e;
-          qn += __popc(bal);
-          if (qn >= 32) flush(32);
         }
+        const unsigned bal = __ballot_sync(FULL, pass);
+        if (pass) queue[qn + __popc(bal & ((1u << lane) - 1u))] = e;
+        qn += __popc(bal);
+        if (qn >= 32) flush(32);
       }
       while (qn > 0) flush(min(qn, 32));
 #pragma unroll
@@ -989,6 +1025,7 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
         c.wrep[((size_t)2 * nc + cell) * c.nn + node] += rz;
       }
     }
+    __syncwarp();  // ranges of the next tile overwrite this one's
   }
 }
 
@@ -1068,25 +1105,26 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs 
         const int t = __shfl_sync(FULL, rt, r);  // every lane calls slot()
         return t < 0 ? (int64_t)-1 : (int64_t)t * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (kw & 3);
       };
+      // bound: the first minimum of one list of the window bounds the window
+      // minimum from above (1.5 is the reference's starting value); take the
+      // nearest wall node among those of the 8 lattice points around the node
       float bound = 1.5f;
       {
         float dbest = 3.0e38f;
         int mbest = 0;
-        int i = pi0, j = pj0, dk = pk0;
-        for (int p0 = 0; p0 < npts; p0 += 32) {
-          const int64_t s = slot(i, j, dk);
-          if (p0 + lane < npts && s >= 0) {
-            const int wi = a.windex[s];
-            if (wi > 0) {
-              const float4 wn = a.wnode[s];
-              const float dm = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
-              if (dm < dbest) {
-                dbest = dm;
-                mbest = wi;
-              }
-            }
+        const int ci = (int)floor(((double)xp - a.X0) / a.DX) + (lane & 1);
+        const int cj = (int)floor(((double)yp - a.Y0) / a.DX) + ((lane >> 1) & 1);
+        const int ck = (int)floor(((double)zp - a.Z0) / a.DX) + ((lane >> 2) & 1);
+        const bool in = lane < 8 && ci >= i1 && ci <= i2 && cj >= j1 && cj <= j2 && ck >= k1 && ck <= k2;
+        // every lane calls slot(); lanes outside pass a window point
+        const int64_t sc = slot(in ? ci : i1, in ? cj : j1, in ? ck - k1 : 0);
+        if (in && sc >= 0) {
+          const int wi = a.windex[sc];
+          const float4 wn = a.wnode[sc];
+          if (wi > 0) {
+            dbest = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
+            mbest = wi;
           }
-          step(i, j, dk);
         }
         float dmin = dbest;
 #pragma unroll
@@ -1128,7 +1166,7 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs 
           const int64_t s = slot(i, j, dk);
           if (p0 + lane < npts && s >= 0) {
             wi = a.windex[s];
-            if (wi > 0) wn = a.wnode[s];
+            wn = a.wnode[s];
           }
           step(i, j, dk);
           int prev = __shfl_up_sync(FULL, wi, 1);
