@@ -366,46 +366,73 @@ __device__ __forceinline__ int64_t bin_key(int64_t s) {
 // within 2 lattice units per axis can lie within 1 um (2 DX), and the first
 // minimum of the reference scan is the first minimum of any sub-scan in the
 // same order that holds every point within 1 um, so the scan covers +-2.
+//
+// Each bin also records its reach: the largest, over its triangles, of the
+// centroid's distance from the bin point plus the triangle's bounding radius
+// (as in k_bin_records), rounded up; reach[ns] holds the largest of all.  No
+// point of a triangle in a bin lies farther than the reach from the bin point.
 __global__ void k_bin_assign(IbArgs a, CellArgs c, int32_t* tri_bin, int32_t* counts) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = c.n_cells;
+  const unsigned live = __ballot_sync(0xffffffffu, g < (int64_t)nc * c.nt);
   if (g >= (int64_t)nc * c.nt) return;
   const int cell = (int)(g / c.nt), t = (int)(g % c.nt);
   tri_bin[g] = -1;
-  if (c.status[cell] <= 0) return;
-  const float xp = c.tri_c[((size_t)0 * nc + cell) * c.nt + t];
-  const float yp = c.tri_c[((size_t)1 * nc + cell) * c.nt + t];
-  float zp = c.tri_c[((size_t)2 * nc + cell) * c.nt + t];
-  if (a.LZ > 0.f) zp = (float)((double)zp - (double)a.LZ * floor(((double)zp - a.Z0) / a.LZ));
-  else if (zp < a.Z0 || zp > a.Z0 + (a.nz - 1) * a.DX) return;
-  const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
-            k0 = lat_index(zp, a.Z0, a.DX);
-  const int i1 = max(i0 - 2, 0), i2 = min(i0 + 2, a.nx - 1);
-  const int j1 = max(j0 - 2, 0), j2 = min(j0 + 2, a.ny - 1);
-  const int k1 = a.per_z ? k0 - 2 : max(k0 - 2, 2), k2 = a.per_z ? k0 + 2 : min(k0 + 2, a.nz - 4);
-  float mindis = 5000.f;
-  int64_t best = -1;
-  for (int i = i1; i <= i2; ++i)
-    for (int j = j1; j <= j2; ++j)
-      for (int k = k1; k <= k2; ++k) {
-        const int kw = a.per_z ? ((k % a.nz) + a.nz) % a.nz : k;
-        const int64_t s = slot_of(a, i, j, kw);
-        if (s < 0 || s >= a.ns) continue;
-        const uint8_t cd = a.code[s];
-        if (cd == 0) continue;  // listed points only
-        const float xc = (float)((double)a.X0 + i * (double)a.DX);
-        const float yc = (float)((double)a.Y0 + j * (double)a.DX);
-        const float zc = (float)((double)a.Z0 + k * (double)a.DX);
-        const float d = dist3(xc - xp, yc - yp, zc - zp);
-        if (d < mindis) {
-          mindis = d;
-          best = s;
-        }
+  unsigned reach_bits = 0;
+  if (c.status[cell] > 0) {
+    const float xp = c.tri_c[((size_t)0 * nc + cell) * c.nt + t];
+    const float yp = c.tri_c[((size_t)1 * nc + cell) * c.nt + t];
+    const float zraw = c.tri_c[((size_t)2 * nc + cell) * c.nt + t];
+    float zp = zraw;
+    bool in = true;
+    if (a.LZ > 0.f) zp = (float)((double)zp - (double)a.LZ * floor(((double)zp - a.Z0) / a.LZ));
+    else in = !(zp < a.Z0 || zp > a.Z0 + (a.nz - 1) * a.DX);
+    float mindis = 5000.f;
+    int64_t best = -1;
+    if (in) {
+      const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
+                k0 = lat_index(zp, a.Z0, a.DX);
+      const int i1 = max(i0 - 2, 0), i2 = min(i0 + 2, a.nx - 1);
+      const int j1 = max(j0 - 2, 0), j2 = min(j0 + 2, a.ny - 1);
+      const int k1 = a.per_z ? k0 - 2 : max(k0 - 2, 2), k2 = a.per_z ? k0 + 2 : min(k0 + 2, a.nz - 4);
+      for (int i = i1; i <= i2; ++i)
+        for (int j = j1; j <= j2; ++j)
+          for (int k = k1; k <= k2; ++k) {
+            const int kw = a.per_z ? ((k % a.nz) + a.nz) % a.nz : k;
+            const int64_t s = slot_of(a, i, j, kw);
+            if (s < 0 || s >= a.ns) continue;
+            const uint8_t cd = a.code[s];
+            if (cd == 0) continue;  // listed points only
+            const float xc = (float)((double)a.X0 + i * (double)a.DX);
+            const float yc = (float)((double)a.Y0 + j * (double)a.DX);
+            const float zc = (float)((double)a.Z0 + k * (double)a.DX);
+            const float d = dist3(xc - xp, yc - yp, zc - zp);
+            if (d < mindis) {
+              mindis = d;
+              best = s;
+            }
+          }
+    }
+    if (best >= 0 && mindis < 1.f) {
+      const int64_t key = bin_key(best);
+      tri_bin[g] = (int32_t)key;
+      atomicAdd(&counts[key], 1);
+      float r2 = 0.f;
+      for (int v = 0; v < 3; ++v) {
+        const int n = c.tri[3 * t + v];
+        const float dx = (float)c.x[((size_t)0 * nc + cell) * c.nn + n] - xp;
+        const float dy = (float)c.x[((size_t)1 * nc + cell) * c.nn + n] - yp;
+        const float dz = (float)c.x[((size_t)2 * nc + cell) * c.nn + n] - zraw;
+        r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
       }
-  if (best < 0 || !(mindis < 1.f)) return;
-  const int64_t key = bin_key(best);
-  tri_bin[g] = (int32_t)key;
-  atomicAdd(&counts[key], 1);
+      const float reach = (mindis + sqrtf(r2) * 1.0001f + 1e-3f) * 1.0001f + 1e-3f;
+      reach_bits = __float_as_uint(reach);
+      atomicMax(reinterpret_cast<unsigned*>(&a.bin_reach[key]), reach_bits);
+    }
+  }
+  const unsigned wmax = __reduce_max_sync(live, reach_bits);
+  if ((threadIdx.x & 31) == __ffs(live) - 1 && wmax)
+    atomicMax(reinterpret_cast<unsigned*>(&a.bin_reach[a.ns]), wmax);
 }
 
 // exclusive scan of counts[0..n) into off[0..n], three passes
@@ -873,55 +900,40 @@ __device__ __forceinline__ int neighbour_tile(const IbArgs& a, int tx, int ty, i
   return a.tile_map[((int64_t)Z * a.nty + Y) * a.ntx + X];
 }
 
-// RBC-RBC repulsion (ZebraflowWT.c:9911-10053).  For each node the warp reads
-// the bin records of the 27 tiles 32 at a time and keeps those in the node's
-// +-4 window that pass the cheap filters; they queue up and are evaluated 32
-// at a time, one per lane.  Lane sums meet in a fixed butterfly, so the result
-// is deterministic.
+// RBC-RBC repulsion (ZebraflowWT.c:9911-10053).  For each node the warp walks
+// the window's lattice points 32 at a time.  Only triangles with a
+// sub-centroid within 1 um of the node contribute, so a bin point farther
+// than 1 um plus its reach (plus a rounding margin) holds none: such points
+// are skipped, first against the largest reach with arithmetic alone, then
+// against the point's own reach.  The triangles of the remaining bins pass
+// the reference's tests (centroid within 2 um, facing normals, not the node's
+// own triangle) and one whose sub-centroids can reach 1 um queues up; queued
+// triangles are evaluated 32 at a time, one per lane.  Lane sums meet in a
+// fixed butterfly, so the result is deterministic.
 __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c) {
   __shared__ int s_q[kTileWarps][64];
-  __shared__ int s_re0[kTileWarps][27], s_rcum[kTileWarps][28];
-  __shared__ int s_rxyz[kTileWarps][27][3];
   const unsigned FULL = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nc = c.n_cells;
   const int64_t nmem = (int64_t)nc * c.nn;
   const int64_t n_pop_tiles = a.ns / ZF_TC;
   const int nlist = a.tile_ctr[0];
+  const float reach_all = __int_as_float(a.bin_reach[a.ns]);
+  const float lim = 1.f + reach_all + 1e-3f;
   int* queue = s_q[warp];
-  int* re0 = s_re0[warp];
-  int* rcum = s_rcum[warp];
   for (int li = warp_next_tile(&a.tile_ctr[1], lane); li < nlist; li = warp_next_tile(&a.tile_ctr[1], lane)) {
     const int gt = a.tile_list[li];
     const int tx = gt % a.ntx, ty = (gt / a.ntx) % a.nty, tz = gt / (a.ntx * a.nty);
-    // record range and lattice origin of each of the 27 tiles; the ranges
-    // are walked as one sequence (rcum: starts of the ranges in it)
-    int len = 0;
+    // lane r < 27: population tile of neighbour r, or -1
+    int rt = -1;
     if (lane < 27) {
       int X, Y, Z;
       const int t = neighbour_tile(a, tx, ty, tz, lane, X, Y, Z);
-      int e0 = 0;
-      if (t >= 0 && t < n_pop_tiles) {
-        e0 = a.bin_off[(int64_t)t * ZF_TC];
-        len = a.bin_off[(int64_t)t * ZF_TC + ZF_TC] - e0;
-      }
-      re0[lane] = e0;
-      s_rxyz[warp][lane][0] = 4 * X;
-      s_rxyz[warp][lane][1] = 4 * Y;
-      s_rxyz[warp][lane][2] = 4 * Z;
+      if (t >= 0 && t < n_pop_tiles) rt = t;
     }
-    int cum = len;  // inclusive warp scan of the lengths
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(FULL, cum, o);
-      if (lane >= o) cum += v;
-    }
-    if (lane < 27) rcum[lane + 1] = cum;
-    if (lane == 0) rcum[0] = 0;
-    __syncwarp();
-    const int rtot = rcum[27];
+    if (!__any_sync(FULL, rt >= 0)) continue;
     const int n0 = a.node_off[gt], n1 = a.node_off[gt + 1];
-    for (int q = n0; q < n1 && rtot > 0; ++q) {
+    for (int q = n0; q < n1; ++q) {
       const int64_t gid = a.node_sorted[q];
       if (gid >= nmem) continue;  // nucleus node: no RBC-RBC term
       const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
@@ -936,8 +948,15 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
       const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
       const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
       const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
-      const int k1w = a.per_z ? ((k1 % a.nz) + a.nz) % a.nz : k1;  // window start, wrapped
+      if (i1 > i2 || j1 > j2 || k1 > k2) continue;
+      const int ni = i2 - i1 + 1, nj = j2 - j1 + 1, nk = k2 - k1 + 1;
+      const int k1w = a.per_z ? ((k1 % a.nz) + a.nz) % a.nz : k1;
+      const int npts = ni * nj * nk;
       const int g_own = cell * c.nt;
+      // lane l starts at window point l (scan order i, j, k) and steps 32
+      // points at a time in mixed radix
+      const int sk = 32 % nk, sj = (32 / nk) % nj, si = 32 / (nk * nj);
+      int i = i1 + lane / (nj * nk), j = j1 + (lane / nk) % nj, dk = lane % nk;
       float rx = 0.f, ry = 0.f, rz = 0.f;
       int qn = 0;
       auto flush = [&](int nb) {
@@ -957,60 +976,68 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
         __syncwarp();
         qn = rem;
       };
-      // lane l takes positions l, l+32, ... of the sequence; the record of the
-      // next position is loaded before the current one is tested
-      int r = 0;
-      auto entry = [&](int f) {
-        while (f >= rcum[r + 1]) ++r;
-        return re0[r] + (f - rcum[r]);
-      };
-      int e_n = 0, r_n = 0;
-      float4 c_n = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (lane < rtot) {
-        e_n = entry(lane);
-        r_n = r;
-        c_n = a.bin_c[e_n];
-      }
-      for (int f0 = 0; f0 < rtot; f0 += 32) {
-        const int f = f0 + lane;
-        const int e = e_n, rr = r_n;
-        const float4 cr = c_n;
-        if (f + 32 < rtot) {
-          e_n = entry(f + 32);
-          r_n = r;
-          c_n = a.bin_c[e_n];
+      for (int p0 = 0; p0 < npts; p0 += 32) {
+        // the bin of this lane's window point: key and tile
+        int kw = k1w + dk;
+        if (kw >= a.nz) kw -= a.nz;
+        int lz = (kw >> 2) - tz + 1;
+        if (lz < 0) lz += a.ntz;
+        else if (lz > 2) lz -= a.ntz;
+        const int r = (lz * 3 + ((j >> 2) - ty + 1)) * 3 + ((i >> 2) - tx + 1);
+        const int t = __shfl_sync(FULL, rt, r);  // every lane takes part
+        int e0 = 0, len = 0;
+        if (p0 + lane < npts && t >= 0) {
+          const float ddx = (float)(a.X0 + i * a.DX) - xc, ddy = (float)(a.Y0 + j * a.DX) - yc,
+                      ddz = (float)(a.Z0 + (k1 + dk) * a.DX) - zc;
+          const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+          if (d2 < lim * lim) {
+            const int64_t key = (int64_t)t * ZF_TC + 16 * (i & 3) + 4 * (j & 3) + (kw & 3);
+            const float rch = __int_as_float(a.bin_reach[key]);
+            if (!(sqrtf(d2) - rch > 1.f + 1e-3f)) {
+              e0 = a.bin_off[key];
+              len = a.bin_off[key + 1] - e0;
+            }
+          }
         }
-        bool pass = false;
-        if (f < rtot) {
-          const int kk = rec_kk(cr.w);
-          const int bi = s_rxyz[warp][rr][0] + ((kk >> 4) & 3), bj = s_rxyz[warp][rr][1] + ((kk >> 2) & 3),
-                    bk = s_rxyz[warp][rr][2] + (kk & 3);
-          int dk = bk - k1w;
-          if (a.per_z && dk < 0) dk += a.nz;
-          if (bi >= i1 && bi <= i2 && bj >= j1 && bj <= j2 && dk >= 0 && dk <= k2 - k1) {
+        // advance to the point 32 further on
+        dk += sk;
+        int cy = 0;
+        if (dk >= nk) {
+          dk -= nk;
+          cy = 1;
+        }
+        j += sj + cy;
+        cy = 0;
+        if (j > j2) {
+          j -= nj;
+          cy = 1;
+        }
+        i += si + cy;
+        // the triangles of the bins that remain
+        for (int u = 0; __any_sync(FULL, u < len); ++u) {
+          bool pass = false;
+          const int e = e0 + u;
+          if (u < len) {
+            const float4 cr = a.bin_c[e];
             const float dzc = wrapd(cr.z - zc, a.LZ);
-            const float ddx = xc - cr.x, ddy = yc - cr.y;
-            // a squared distance well beyond 2 um fails the exact test below
-            if (ddx * ddx + ddy * ddy + dzc * dzc < 4.01f) {
-              const float dcen = dist3(ddx, ddy, -dzc);
-              if (dcen < 2.f && !(dcen - rec_rb(cr.w) > 1.f)) {
-                const float4 nr = a.bin_n[e];
-                if (e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
-                  const int g = __float_as_int(nr.w);
-                  pass = true;
-                  if (g >= g_own && g < g_own + c.nt) {
-                    const int tri = g - g_own;
-                    pass = !(c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node);
-                  }
+            const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
+            if (dcen < 2.f && !(dcen - rec_rb(cr.w) > 1.f)) {
+              const float4 nr = a.bin_n[e];
+              if (e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
+                const int g = __float_as_int(nr.w);
+                pass = true;
+                if (g >= g_own && g < g_own + c.nt) {
+                  const int tri = g - g_own;
+                  pass = !(c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node);
                 }
               }
             }
           }
+          const unsigned bal = __ballot_sync(FULL, pass);
+          if (pass) queue[qn + __popc(bal & ((1u << lane) - 1u))] = e;
+          qn += __popc(bal);
+          if (qn >= 32) flush(32);
         }
-        const unsigned bal = __ballot_sync(FULL, pass);
-        if (pass) queue[qn + __popc(bal & ((1u << lane) - 1u))] = e;
-        qn += __popc(bal);
-        if (qn >= 32) flush(32);
       }
       while (qn > 0) flush(min(qn, 32));
 #pragma unroll
@@ -1025,7 +1052,6 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
         c.wrep[((size_t)2 * nc + cell) * c.nn + node] += rz;
       }
     }
-    __syncwarp();  // ranges of the next tile overwrite this one's
   }
 }
 
@@ -1391,6 +1417,7 @@ int ib_bins_launch(zf_ctx* ctx) {
   int32_t* bsum = tri_bin + ntri;
   int32_t* off = const_cast<int32_t*>(a.bin_off);
   ZF_CUDA(cudaMemsetAsync(counts, 0, (a.ns + 1) * sizeof(int32_t), ctx->stream));
+  ZF_CUDA(cudaMemsetAsync(a.bin_reach, 0, (a.ns + 1) * sizeof(int32_t), ctx->stream));
   k_bin_assign<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(a, c, tri_bin, counts);
   scan_launch(counts, a.ns + 1, off, bsum, ctx->stream);
   ZF_CUDA(cudaMemsetAsync(counts, 0, (a.ns + 1) * sizeof(int32_t), ctx->stream));

@@ -150,6 +150,7 @@ int ib_buffers(zf_ctx* c) {
   if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_c, ntri))) return rc;
   if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_n, ntri))) return rc;
   if ((rc = dalloc<uint8_t>(c, c->ib_allocs, &a.bin_kk, ntri))) return rc;
+  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.bin_reach, nscan))) return rc;
   // node-tile lists
   const int64_t nnodes = (int64_t)cl.n_cells * (cl.nn + cl.nnn);
   a.ngrid = (int64_t)c->ntx * c->nty * c->ntz;

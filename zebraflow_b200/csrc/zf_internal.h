@@ -157,6 +157,8 @@ struct IbArgs {
   float4* bin_c;                // [n_cells*nt] per entry: centroid xyz, bounding radius
   float4* bin_n;                // [n_cells*nt] per entry: normal xyz, id (int bits)
   uint8_t* bin_kk;              // [n_cells*nt] per entry: its key inside the tile (0..63)
+  int32_t* bin_reach;           // [ns+1] float bits: farthest point of a bin's triangles
+                                // from the bin point (um, rounded up); [ns] the largest
   // membrane and nucleus nodes grouped by the lattice tile of their nearest
   // point (tile grid index over all ntx*nty*ntz tiles), rebuilt after positions change
   int64_t ngrid;                // ntx*nty*ntz
