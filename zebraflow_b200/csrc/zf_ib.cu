@@ -976,6 +976,10 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
         __syncwarp();
         qn = rem;
       };
+      // window point coordinates relative to the node, in float (the bound
+      // carries a margin far above their rounding)
+      const float X0f = (float)a.X0, Y0f = (float)a.Y0, Z0f = (float)a.Z0, DXf = (float)a.DX;
+      const float lim2 = lim * lim;
       for (int p0 = 0; p0 < npts; p0 += 32) {
         // the bin of this lane's window point: key and tile
         int kw = k1w + dk;
@@ -987,13 +991,12 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
         const int t = __shfl_sync(FULL, rt, r);  // every lane takes part
         int e0 = 0, len = 0;
         if (p0 + lane < npts && t >= 0) {
-          const float ddx = (float)(a.X0 + i * a.DX) - xc, ddy = (float)(a.Y0 + j * a.DX) - yc,
-                      ddz = (float)(a.Z0 + (k1 + dk) * a.DX) - zc;
+          const float ddx = (X0f + i * DXf) - xc, ddy = (Y0f + j * DXf) - yc, ddz = (Z0f + (k1 + dk) * DXf) - zc;
           const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-          if (d2 < lim * lim) {
+          if (d2 < lim2) {
             const int64_t key = (int64_t)t * ZF_TC + 16 * (i & 3) + 4 * (j & 3) + (kw & 3);
-            const float rch = __int_as_float(a.bin_reach[key]);
-            if (!(sqrtf(d2) - rch > 1.f + 1e-3f)) {
+            const float rr = __int_as_float(a.bin_reach[key]) + 1.f + 1e-3f;
+            if (d2 <= rr * rr) {
               e0 = a.bin_off[key];
               len = a.bin_off[key + 1] - e0;
             }
@@ -1013,11 +1016,27 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
           cy = 1;
         }
         i += si + cy;
-        // the triangles of the bins that remain
-        for (int u = 0; __any_sync(FULL, u < len); ++u) {
+        // the triangles of the remaining bins as one sequence over the lanes
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(FULL, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        const int base = incl - len;  // this lane's first position
+        for (int g0 = 0; g0 < total; g0 += 32) {
+          const int gpos = g0 + lane;
+          // source lane: the last lane whose first position is <= gpos
+          int src = 0;
+#pragma unroll
+          for (int stp = 16; stp > 0; stp >>= 1) {
+            const int v = __shfl_sync(FULL, base, src + stp);
+            if (src + stp < 32 && gpos >= v && v < total) src += stp;
+          }
+          const int e = __shfl_sync(FULL, e0, src) + (gpos - __shfl_sync(FULL, base, src));
           bool pass = false;
-          const int e = e0 + u;
-          if (u < len) {
+          if (gpos < total) {
             const float4 cr = a.bin_c[e];
             const float dzc = wrapd(cr.z - zc, a.LZ);
             const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
