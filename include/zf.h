@@ -315,6 +315,22 @@ int zf_ibm_spread(zf_ctx* ctx);
  * (ZebraflowWT.c:11965-12031). */
 int zf_update_positions(zf_ctx* ctx);
 
+/* Wall shear stress and wall pressure at the wall-mesh nodes, as the
+ * reference's post-processor computes them (PostProWSSandPressure.c:275-369)
+ * from the current populations (post-collision moments, :6603-6616):
+ *   probe x_m + DX n_m, velocity interpolated there with the Peskin cosine
+ *   weights inside 2 DX over fluid points (B_index 1..9) of the +-3 window,
+ *   WSS = -0.0012 Pa.s * (u - (u.n) n) / (DX 1e-6 m)   [wss: [3][nw], Pa];
+ *   pressure (D-1)/3*1e4 - pgauge at the nearest listed point within
+ *   1.42 DX of x_m                                    [pressure: [nw], Pa];
+ *   valid = 0 where no such point exists or the pressure is below 1 Pa.
+ * node_normals [3][nw] are unit normals into the lumen; NULL takes the
+ * area-weighted mean of the wall triangles' normals at each node.  With a
+ * periodic z axis the windows wrap (the reference has no periodic axis).
+ * pressure and valid may be NULL.  Waits for the result. */
+int zf_wss(zf_ctx* ctx, const float* node_normals, double pgauge, float* wss, float* pressure,
+           int32_t* valid);
+
 /* nsteps iterations of the reference time loop (ZebraflowWT.c:5646-12190):
  * every iteration an LBM step; every `stagger`-th iteration also the
  * membrane forces, IB interpolation, repulsions, spreading and position

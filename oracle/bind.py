@@ -73,6 +73,9 @@ def lib() -> C.CDLL:
             g("orc_world_step").argtypes = [C.c_void_p, C.c_int]
             g("orc_world_kinematics").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                   C.c_void_p]
+            g("orc_world_wss").argtypes = [C.c_void_p, _f32p, C.c_double, _f32p, C.c_void_p,
+                                           C.c_void_p]
+            g("orc_lbm_moments_from_f").argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -196,6 +199,10 @@ class OracleLBM:
         self._fn("orc_lbm_get_bodyforce")(self._h, out)
         return out.reshape(3, self.n)
 
+    def moments_from_f(self):
+        """Recomputes D, U, V, W from the current populations."""
+        self._fn("orc_lbm_moments_from_f")(self._h)
+
     def moments(self):
         outs = [np.empty(self.n) for _ in range(4)]
         self._fn("orc_lbm_get_moments")(self._h, *outs)
@@ -228,15 +235,16 @@ class OracleWorld:
     """The reference IB coupling and time loop (ZebraflowWT.c:5646-12190) over an
     OracleLBM and an OracleCells of the same precision; see oracle/orc_ib.inc."""
 
-    def __init__(self, lbm: OracleLBM, cells: OracleCells, params):
-        assert lbm.sfx == cells.sfx
+    def __init__(self, lbm: OracleLBM, cells, params):
+        """cells may be None for wall-only use (set_wall, wss)."""
+        assert cells is None or lbm.sfx == cells.sfx
         self.lbm, self.cells, self.sfx = lbm, cells, lbm.sfx
         self._fn = lambda n: getattr(lib(), n + self.sfx)  # noqa: E731
         P = params
         par = np.array([P.gamma_p, P.unit_mass, P.bforce_scale, P.vel_scale, P.dt, P.vmax_remove,
                         P.stagger, P.nuc_list_period, P.nuc_list_max], np.float64)
-        self._h = self._fn("orc_world_create")(lbm._h, cells._h, np.asarray(P.origin[:], np.float64),
-                                               float(P.dx), par)
+        self._h = self._fn("orc_world_create")(lbm._h, cells._h if cells is not None else None,
+                                               np.asarray(P.origin[:], np.float64), float(P.dx), par)
         self.wall_cap = P.wall_list_max
 
     def set_wall(self, xyz, tri, nrm):
@@ -270,6 +278,17 @@ class OracleWorld:
 
     def step(self, n=1):
         self._fn("orc_world_step")(self._h, int(n))
+
+    def wss(self, node_normals, pgauge=120.0):
+        """WSS [3][nw] (Pa), pressure [nw] (Pa) and valid flags [nw] from the
+        LBM's current moments (PostProWSSandPressure.c:275-369)."""
+        nrm = np.ascontiguousarray(node_normals, np.float32)
+        nw = nrm.shape[1]
+        wss = np.empty(3 * nw, np.float32)
+        press = np.empty(nw, np.float32)
+        valid = np.empty(nw, np.int32)
+        self._fn("orc_world_wss")(self._h, nrm.ravel(), float(pgauge), wss, _p(press), _p(valid))
+        return wss.reshape(3, nw), press, valid
 
     def kinematics(self):
         c = self.cells

@@ -108,3 +108,34 @@ def test_poiseuille_profile():
     core = r2 < (R - 2) ** 2                # staircase-wall error stays near the wall
     assert np.max(np.abs(pred - w)[core]) < 0.03 * w.max()
     assert np.all(np.abs(U[fl]) < 1e-3 * w.max())
+
+
+def test_oracle_wss_poiseuille():
+    """The oracle's WSS (PostProWSSandPressure.c:275-369) on developed flow in a
+    small periodic tube: mean axial WSS within 10 % of 0.0012 u(R-1)/0.5 um."""
+    import zebraflow_b200 as zf
+    from oracle.bind import OracleLBM, OracleWorld
+    nx = ny = 22
+    nz, R, c, g, tau = 8, 8.0, 10.5, 1e-4, 0.9
+    b = zf.gen_tube(nx, ny, nz, c, c, R, True)
+    lbm = OracleLBM(b, wall_mode=0, periodic=(0, 0, 1), tau=tau, g=(0, 0, g), precision="f64")
+    lbm.time_steps(4000)
+    lbm.moments_from_f()
+    p = zf.default_params(nx=nx, ny=ny, nz=nz, origin=(0.0, 0.0, 0.0), periodic=(0, 0, 1))
+    w = OracleWorld(lbm, None, p)
+    xyz, tri, nrm = zf.gen_wall_tube(c, c, R, nz)
+    w.set_wall(xyz, tri, nrm)
+    t = tri - 1
+    pts = xyz.T.astype(np.float64)
+    area = 0.5 * np.linalg.norm(np.cross((pts[t[1]] - pts[t[0]]), (pts[t[2]] - pts[t[0]])), axis=1)
+    acc = np.zeros((xyz.shape[1], 3))
+    for v in range(3):
+        np.add.at(acc, t[v], area[:, None] * nrm.T)
+    acc /= np.linalg.norm(acc, axis=1, keepdims=True)
+    wss, _, _ = w.wss(np.ascontiguousarray(acc.T, np.float32))
+    nu = (tau - 0.5) / 3.0
+    expected = 0.0012 * g * (R ** 2 - (R - 1) ** 2) / (4 * nu) / 0.5e-6
+    assert wss[2].mean() < 0
+    assert abs(-wss[2].mean() - expected) <= 0.1 * expected
+    w.close()
+    lbm.close()

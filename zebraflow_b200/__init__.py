@@ -128,6 +128,7 @@ _SIGS = {
                                           C.c_double, _f64p, C.c_double, C.POINTER(C.c_int),
                                           C.POINTER(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_int, C.c_int]),
+    "zf_wss": (C.c_int, [_P, C.c_void_p, C.c_double, _f32p, C.c_void_p, C.c_void_p]),
     "zf_gen_cells": (C.c_int, [_i32p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, C.c_int,
                                C.c_int, C.c_int, _f64p, C.c_int, _f64p, _f64p, C.c_double,
                                C.c_double, C.c_uint64, _f64p, _f64p, C.POINTER(C.c_int)]),
@@ -421,6 +422,7 @@ class Context:
         nrm = np.ascontiguousarray(nrm, np.float32)
         _check(lib().zf_set_wall(self._h, xyz.shape[1], xyz.ravel(), tri.shape[1], tri.ravel(),
                                  nrm.ravel()))
+        self._nw = xyz.shape[1]
 
     def wall_index(self):
         p = self.params
@@ -447,6 +449,19 @@ class Context:
 
     def step(self, n=1):
         _check(lib().zf_step(self._h, n))
+
+    def wss(self, node_normals=None, pgauge=120.0):
+        """WSS [3][nw] (Pa), wall pressure [nw] (Pa), valid [nw] from the current
+        populations (zf_wss); node_normals [3][nw] or None for the mesh's own."""
+        nw = self._nw
+        wss = np.empty(3 * nw, np.float32)
+        press = np.empty(nw, np.float32)
+        valid = np.empty(nw, np.int32)
+        nrm = None if node_normals is None else np.ascontiguousarray(node_normals, np.float32)
+        _check(lib().zf_wss(self._h, None if nrm is None else nrm.ctypes.data_as(C.c_void_p),
+                            float(pgauge), wss, press.ctypes.data_as(C.c_void_p),
+                            valid.ctypes.data_as(C.c_void_p)))
+        return wss.reshape(3, nw), press, valid
 
     def step_timed(self, n):
         ms = C.c_float()

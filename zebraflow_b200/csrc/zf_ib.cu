@@ -1357,6 +1357,117 @@ __global__ void k_update(IbArgs a, CellArgs c) {
 
 // ---- launchers --------------------------------------------------------------------
 
+// ---- wall shear stress ----------------------------------------------------------
+
+// One thread per wall-mesh node: the reference's post-processor
+// (PostProWSSandPressure.c:275-369).  Lattice coordinates X0 + i DX and the
+// 1-based index (int)((x - X0)/DX + 1.01) are kept; windows are +-3 with the
+// reference's one-sided clamps (i from 3, j and k from 1, 1-based).  Moments
+// (a.mom) must hold the current populations' D, U, V, W.
+__device__ __forceinline__ void wss_window(int ii, int n, int lo, bool wrap, int& i1, int& i2) {
+  // ii, lo 0-based; n points along the axis
+  i1 = ii - 3;
+  i2 = ii + 3;
+  if (wrap) return;
+  if (i2 > n - 1) i2 = n - 1;
+  else if (i1 < lo) i1 = lo;
+}
+
+__global__ void k_wss(IbArgs a, const float* __restrict__ nrm, float pgauge, float* __restrict__ wss,
+                      float* __restrict__ press, int32_t* __restrict__ valid) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.nw) return;
+  const float xm = a.wxyz[m], ym = a.wxyz[a.nw + m], zm = a.wxyz[2 * a.nw + m];
+  const float n0 = nrm[m], n1 = nrm[a.nw + m], n2 = nrm[2 * a.nw + m];
+  const bool wz = a.per_z;
+  auto lat1 = [&](float x, double x0) { return (int)(((double)x - x0) / a.DX + 1.01) - 1; };
+  auto point_slot = [&](int i, int j, int k) -> int64_t {  // k may lie outside when wrapping
+    if (i < 0 || i >= a.nx || j < 0 || j >= a.ny) return -1;
+    if (k < 0 || k >= a.nz) {
+      if (!wz) return -1;
+      k = ((k % a.nz) + a.nz) % a.nz;
+    }
+    return slot_of(a, i, j, k);
+  };
+  // wall pressure at the nearest listed point within 1.42 DX (:276-318)
+  {
+    int i1, i2, j1, j2, k1, k2;
+    wss_window(lat1(xm, a.X0), a.nx, 2, false, i1, i2);
+    wss_window(lat1(ym, a.Y0), a.ny, 0, false, j1, j2);
+    wss_window(lat1(zm, a.Z0), a.nz, 0, wz, k1, k2);
+    float mindis = (float)(1.42 * a.DX);
+    int64_t best = -1;
+    for (int i = i1; i <= i2; ++i)
+      for (int j = j1; j <= j2; ++j)
+        for (int k = k1; k <= k2; ++k) {
+          const int64_t s = point_slot(i, j, k);
+          if (s < 0 || s >= a.ns || a.code[s] == ZF_CODE_SOLID) continue;  // B_index >= 0
+          const float dx = xm - (float)(a.X0 + i * a.DX), dy = ym - (float)(a.Y0 + j * a.DX);
+          const float dz = wrapd(zm - (float)(a.Z0 + k * a.DX), a.LZ);
+          const float d = dist3(dx, dy, dz);
+          if (d < mindis) {
+            mindis = d;
+            best = s;
+          }
+        }
+    int ok = !((double)mindis > 1.419999 * a.DX) && best >= 0;
+    float pw = 0.f;
+    if (ok) {
+      const float pp = (float)(((double)a.mom[best] - 1.) / 3. * 10000.);
+      pw = pp - pgauge;
+    }
+    if (pw < 1.f) ok = 0;
+    if (press) press[m] = pw;
+    if (valid) valid[m] = ok;
+  }
+  // wall shear stress from the velocity one DX into the lumen (:320-369)
+  const float xp = (float)((double)xm + a.DX * (double)n0);
+  const float yp = (float)((double)ym + a.DX * (double)n1);
+  const float zp = (float)((double)zm + a.DX * (double)n2);
+  int i1, i2, j1, j2, k1, k2;
+  wss_window(lat1(xp, a.X0), a.nx, 2, false, i1, i2);
+  wss_window(lat1(yp, a.Y0), a.ny, 0, false, j1, j2);
+  wss_window(lat1(zp, a.Z0), a.nz, 0, wz, k1, k2);
+  float UU = 0.f, VV = 0.f, WW = 0.f;
+  for (int i = i1; i <= i2; ++i)
+    for (int j = j1; j <= j2; ++j)
+      for (int k = k1; k <= k2; ++k) {
+        const float dx = xp - (float)(a.X0 + i * a.DX), dy = yp - (float)(a.Y0 + j * a.DX);
+        const float dz = wrapd(zp - (float)(a.Z0 + k * a.DX), a.LZ);
+        const float d = dist3(dx, dy, dz);
+        if (!((double)d <= 2 * a.DX)) continue;
+        const int64_t s = point_slot(i, j, k);
+        if (s < 0 || s >= a.ns) continue;
+        const uint8_t cd = a.code[s];
+        if (!(cd >= 1 && cd <= 9)) continue;  // 0.11 < B_index < 4997
+        const float w =
+            (float)((1. + cosf((float)((double)kPI * fabsf(dx) / 2 / a.DX))) *
+                    (1. + cosf((float)((double)kPI * fabsf(dy) / 2 / a.DX))) *
+                    (1. + cosf((float)((double)kPI * fabsf(dz) / 2 / a.DX))) / 64.);
+        UU += w * a.mom[a.ns + s];
+        VV += w * a.mom[2 * a.ns + s];
+        WW += w * a.mom[3 * a.ns + s];
+      }
+  const float vn = UU * n0 + VV * n1 + WW * n2;
+  const float vt0 = UU - vn * n0, vt1 = VV - vn * n1, vt2 = WW - vn * n2;
+  wss[m] = (float)(-0.0012 * (double)vt0 / a.DX / 1.e-06);
+  wss[a.nw + m] = (float)(-0.0012 * (double)vt1 / a.DX / 1.e-06);
+  wss[2 * a.nw + m] = (float)(-0.0012 * (double)vt2 / a.DX / 1.e-06);
+}
+
+int wss_launch(zf_ctx* ctx, const float* d_normals, double pgauge, float* d_wss, float* d_press,
+               int32_t* d_valid) {
+  const IbArgs& a = ctx->ib;
+  if (a.nw == 0) return ZF_OK;
+  int rc = lbm_moments_launch(ctx);
+  if (rc) return rc;
+  k_wss<<<(a.nw + 127) / 128, 128, 0, ctx->stream>>>(a, d_normals ? d_normals : a.wnnrm, (float)pgauge,
+                                                     d_wss, d_press, d_valid);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  return ZF_OK;
+}
+
 namespace {
 
 // the tile kernels need the 3x3x3 tile neighbourhood of a tile to hold every

@@ -124,9 +124,11 @@ int build_view(zf_ctx* c, const WallHost* W) {
     if ((rc = dalloc<int32_t>(c, own, const_cast<int32_t**>(&a.wntri), W->ntri.size(), W->ntri.data())))
       return rc;
     if ((rc = dalloc<float>(c, own, const_cast<float**>(&a.wrad), W->rad.size(), W->rad.data()))) return rc;
+    if ((rc = dalloc<float>(c, own, const_cast<float**>(&a.wnnrm), W->nnrm.size(), W->nnrm.data())))
+      return rc;
   } else {
     a.nw = a.mt = a.wcap = 0;
-    a.wxyz = a.wnrm = a.wcen = a.wrad = nullptr;
+    a.wxyz = a.wnrm = a.wcen = a.wrad = a.wnnrm = nullptr;
     a.wtri = a.wntri = nullptr;
   }
   ZF_CUDA(cudaStreamSynchronize(c->stream));
@@ -251,6 +253,40 @@ int zf_get_wall_index(zf_ctx* c, int32_t* windex, float* uvoid) {
           for (int d = 0; d < 3; ++d) uvoid[(size_t)d * nx * ny * nz + p] = s < 0 ? 0.f : uv[(size_t)d * a.ns_all + s];
       }
   return ZF_OK;
+}
+
+int zf_wss(zf_ctx* c, const float* node_normals, double pgauge, float* wss, float* pressure,
+           int32_t* valid) {
+  if (!c || !wss) return ZF_ERR_ARG;
+  if (!c->lattice_set || c->wall_allocs.empty() || c->ib.nw == 0) {
+    set_error("zf_wss: lattice and wall must be set");
+    return ZF_ERR_STATE;
+  }
+  ZF_CUDA(cudaSetDevice(c->device));
+  const size_t nw = (size_t)c->ib.nw;
+  // [normals 3 nw][wss 3 nw][pressure nw][valid nw]
+  void* buf = nullptr;
+  int rc = dev_alloc(c, &buf, 8 * nw * sizeof(float));
+  if (rc) return rc;
+  float* d_nrm = (float*)buf;
+  float* d_wss = d_nrm + 3 * nw;
+  float* d_press = d_wss + 3 * nw;
+  int32_t* d_valid = (int32_t*)(d_press + nw);
+  cudaError_t e = cudaSuccess;
+  if (node_normals)
+    e = cudaMemcpyAsync(d_nrm, node_normals, 3 * nw * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) rc = wss_launch(c, node_normals ? d_nrm : nullptr, pgauge, d_wss, d_press, d_valid);
+  if (e == cudaSuccess && rc == ZF_OK)
+    e = cudaMemcpyAsync(wss, d_wss, 3 * nw * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && rc == ZF_OK && pressure)
+    e = cudaMemcpyAsync(pressure, d_press, nw * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && rc == ZF_OK && valid)
+    e = cudaMemcpyAsync(valid, d_valid, nw * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(buf);
+  c->device_bytes -= (int64_t)(8 * nw * sizeof(float));
+  ZF_CUDA(e);
+  return rc;
 }
 
 int zf_ibm_interp(zf_ctx* c) {

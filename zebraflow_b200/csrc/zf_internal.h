@@ -112,6 +112,7 @@ struct WallHost {
   std::vector<float> xyz;        // [3][nw]
   std::vector<int32_t> tri;      // [mt][3] 0-based
   std::vector<float> nrm, cen;   // [3][mt]
+  std::vector<float> nnrm;       // [3][nw] area-weighted node normals (unit, into the lumen)
   std::vector<int32_t> ntri;     // [nw][cap+1]: count, triangles (0-based)
   std::vector<float> rad;        // [nw] farthest vertex or centroid of the node's listed
                                  // triangles from the node (um, rounded up)
@@ -146,6 +147,7 @@ struct IbArgs {
   const float* wxyz;            // [3][nw]
   const int32_t* wtri;          // [mt][3]
   const float* wnrm;            // [3][mt]
+  const float* wnnrm;           // [3][nw] WallHost::nnrm
   const float* wcen;            // [3][mt]
   const int32_t* wntri;         // [nw][wcap+1]
   const float* wrad;            // [nw] WallHost::rad
@@ -186,6 +188,9 @@ int ib_bins_launch(zf_ctx* c);
 int ib_nuc_memb_launch(zf_ctx* c, int rebuild);
 int ib_rbc_rbc_launch(zf_ctx* c);
 int ib_node_tiles_launch(zf_ctx* c);
+int lbm_moments_launch(zf_ctx* c);
+int wss_launch(zf_ctx* c, const float* d_normals, double pgauge, float* d_wss, float* d_press,
+               int32_t* d_valid);
 int ib_spread_launch(zf_ctx* c);
 int ib_update_launch(zf_ctx* c);
 

@@ -469,6 +469,45 @@ int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out) {
   return ZF_OK;
 }
 
+// Moments D, U, V, W of the current populations at every listed point:
+// post-collision values without force shift, as the reference's LBM_FLUID
+// pass stores them (ZebraflowWT.c:6603-6616).
+template <class C>
+__global__ void k_moments(LbmArgs a) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.ns || a.code[s] == ZF_CODE_SOLID) return;
+  const typename C::T* __restrict__ f = static_cast<const typename C::T*>(a.fin);
+  float r2 = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+#pragma unroll
+  for (int q = 0; q < ZF_Q; ++q) {
+    const float d = C::dec(f[(int64_t)q * a.ns + s], q, a);
+    r2 += WQ(q) * d;
+    if (EX(q)) mx += EX(q) * WQ(q) * d;
+    if (EY(q)) my += EY(q) * WQ(q) * d;
+    if (EZ(q)) mz += EZ(q) * WQ(q) * d;
+  }
+  const float D = a.rho_ref + r2;
+  a.mom[s] = D;
+  a.mom[a.ns + s] = mx / D;
+  a.mom[2 * a.ns + s] = my / D;
+  a.mom[3 * a.ns + s] = mz / D;
+}
+
+template <class C>
+struct Moments {
+  static void run(zf_ctx* c, const LbmArgs& a) {
+    k_moments<C><<<(unsigned)((c->ns + 255) / 256), 256, 0, c->stream>>>(a);
+  }
+};
+
+int lbm_moments_launch(zf_ctx* c) {
+  const LbmArgs a = make_args(c);  // a.fin: the current populations
+  dispatch_storage<Moments>(c->p.storage, c, a);
+  ZF_CUDA(cudaGetLastError());
+  c->launches += 1;
+  return ZF_OK;
+}
+
 template <class C>
 struct Fill {
   static void run(zf_ctx* c, const LbmArgs& a, int b) {

@@ -73,6 +73,29 @@ int wall_build(zf_ctx* c, int nw, const float* xyz, int mt, const int32_t* tri1,
                       xyz[(size_t)a * nw + W.tri[3 * m + 2]];
       W.cen[(size_t)a * mt + m] = (float)(s / 3.);
     }
+  // node normals: triangle normals weighted by triangle area, normalised
+  W.nnrm.assign(3 * (size_t)nw, 0.f);
+  {
+    std::vector<double> acc(3 * (size_t)nw, 0.0);
+    for (int m = 0; m < mt; ++m) {
+      double e1[3], e2[3];
+      for (int a = 0; a < 3; ++a) {
+        e1[a] = (double)xyz[(size_t)a * nw + W.tri[3 * m + 1]] - xyz[(size_t)a * nw + W.tri[3 * m]];
+        e2[a] = (double)xyz[(size_t)a * nw + W.tri[3 * m + 2]] - xyz[(size_t)a * nw + W.tri[3 * m]];
+      }
+      const double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2],
+                   cz = e1[0] * e2[1] - e1[1] * e2[0];
+      const double area = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+      for (int v = 0; v < 3; ++v)
+        for (int a = 0; a < 3; ++a) acc[(size_t)a * nw + W.tri[3 * m + v]] += area * nrm[(size_t)a * mt + m];
+    }
+    for (int n = 0; n < nw; ++n) {
+      const double x = acc[n], y = acc[(size_t)nw + n], z = acc[2 * (size_t)nw + n];
+      const double l = std::sqrt(x * x + y * y + z * z);
+      if (l > 0)
+        for (int a = 0; a < 3; ++a) W.nnrm[(size_t)a * nw + n] = (float)(acc[(size_t)a * nw + n] / l);
+    }
+  }
   // bounding radius of each node's candidates (the vertices and centroids of
   // its listed triangles): lets a search skip a node whose candidates are all
   // farther than a distance already reached
