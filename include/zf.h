@@ -331,6 +331,30 @@ int zf_update_positions(zf_ctx* ctx);
 int zf_wss(zf_ctx* ctx, const float* node_normals, double pgauge, float* wss, float* pressure,
            int32_t* valid);
 
+/* Wall-shear-stress objective and its hand-written adjoint (no counterpart
+ * in the reference, which has no adjoint; the objective uses its WSS,
+ * PostProWSSandPressure.c:319-369).  The forward that is differentiated
+ * starts from the context's current populations, with the cells held at their
+ * current positions:
+ *   BODYFORCE = S(x) F_total(x; Es, kb) + fb       (spread membrane forces,
+ *                                                   ZebraflowWT.c:10737-10990)
+ *   nsteps LBM steps (:6100-6145) with that BODYFORCE, tau and g;
+ *   J = mean over steps t0..t1 (1 <= t0 <= t1 <= nsteps) of the mean over the
+ *       patch's wall nodes of |WSS| (Pa) of the state after step t.
+ * fb: [3][n_listed] per-node body-force field (DOMLIST order) or NULL (zero).
+ * node_normals as in zf_wss.  Needs fp32 storage, halfway bounce-back and a
+ * uniform tau.  Both calls leave the populations and BODYFORCE as they were.
+ * zf_wss_adjoint keeps the populations of every checkpoint_interval-th step,
+ * recomputes each interval backwards from them, and returns J and
+ * dJ/dfb ([3][n_listed], the same as dJ/dBODYFORCE), dJ/dtau, dJ/dEs and
+ * dJ/dkb (membrane shear and bending moduli, through the spread forces at
+ * the held positions; 0 without cells).  Any output may be NULL. */
+int zf_wss_objective(zf_ctx* ctx, int nsteps, int t0, int t1, const int32_t* patch, int n_patch,
+                     const float* node_normals, const float* fb, double* J);
+int zf_wss_adjoint(zf_ctx* ctx, int nsteps, int t0, int t1, const int32_t* patch, int n_patch,
+                   const float* node_normals, const float* fb, int checkpoint_interval, double* J,
+                   float* dJ_dfb, double* dJ_dtau, double* dJ_dEs, double* dJ_dkb);
+
 /* nsteps iterations of the reference time loop (ZebraflowWT.c:5646-12190):
  * every iteration an LBM step; every `stagger`-th iteration also the
  * membrane forces, IB interpolation, repulsions, spreading and position

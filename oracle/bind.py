@@ -73,7 +73,7 @@ def lib() -> C.CDLL:
             g("orc_world_step").argtypes = [C.c_void_p, C.c_int]
             g("orc_world_kinematics").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                   C.c_void_p]
-            g("orc_world_wss").argtypes = [C.c_void_p, _f32p, C.c_double, _f32p, C.c_void_p,
+            g("orc_world_wss").argtypes = [C.c_void_p, _f32p, C.c_double, _f64p, C.c_void_p,
                                            C.c_void_p]
             g("orc_lbm_moments_from_f").argtypes = [C.c_void_p]
         _lib = L
@@ -284,8 +284,8 @@ class OracleWorld:
         LBM's current moments (PostProWSSandPressure.c:275-369)."""
         nrm = np.ascontiguousarray(node_normals, np.float32)
         nw = nrm.shape[1]
-        wss = np.empty(3 * nw, np.float32)
-        press = np.empty(nw, np.float32)
+        wss = np.empty(3 * nw, np.float64)
+        press = np.empty(nw, np.float64)
         valid = np.empty(nw, np.int32)
         self._fn("orc_world_wss")(self._h, nrm.ravel(), float(pgauge), wss, _p(press), _p(valid))
         return wss.reshape(3, nw), press, valid

@@ -129,6 +129,12 @@ _SIGS = {
                                           C.POINTER(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_int, C.c_int]),
     "zf_wss": (C.c_int, [_P, C.c_void_p, C.c_double, _f32p, C.c_void_p, C.c_void_p]),
+    "zf_wss_objective": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, C.c_void_p,
+                                   C.c_void_p, C.POINTER(C.c_double)]),
+    "zf_wss_adjoint": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, C.c_void_p,
+                                 C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p,
+                                 C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double)]),
     "zf_gen_cells": (C.c_int, [_i32p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, C.c_int,
                                C.c_int, C.c_int, _f64p, C.c_int, _f64p, _f64p, C.c_double,
                                C.c_double, C.c_uint64, _f64p, _f64p, C.POINTER(C.c_int)]),
@@ -449,6 +455,34 @@ class Context:
 
     def step(self, n=1):
         _check(lib().zf_step(self._h, n))
+
+    @staticmethod
+    def _opt(a, dtype):
+        if a is None:
+            return None, None
+        a = np.ascontiguousarray(a, dtype)
+        return a, a.ctypes.data_as(C.c_void_p)
+
+    def wss_objective(self, nsteps, t0, t1, patch, fb=None, node_normals=None) -> float:
+        """J of zf_wss_objective (mean |WSS| over patch and steps t0..t1)."""
+        patch = np.ascontiguousarray(patch, np.int32)
+        _, pn = self._opt(node_normals, np.float32)
+        _fb, pf = self._opt(fb, np.float32)
+        J = C.c_double()
+        _check(lib().zf_wss_objective(self._h, nsteps, t0, t1, patch, patch.size, pn, pf, C.byref(J)))
+        return J.value
+
+    def wss_adjoint(self, nsteps, t0, t1, patch, fb=None, node_normals=None, checkpoint=50):
+        """(J, dJ/dfb [3][n_listed], dJ/dtau, dJ/dEs, dJ/dkb) of zf_wss_adjoint."""
+        patch = np.ascontiguousarray(patch, np.int32)
+        _, pn = self._opt(node_normals, np.float32)
+        _fb, pf = self._opt(fb, np.float32)
+        g = np.zeros((3, self.n_listed), np.float32)
+        J, gt, ge, gk = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        _check(lib().zf_wss_adjoint(self._h, nsteps, t0, t1, patch, patch.size, pn, pf, checkpoint,
+                                    C.byref(J), g.ctypes.data_as(C.c_void_p), C.byref(gt),
+                                    C.byref(ge), C.byref(gk)))
+        return J.value, g, gt.value, ge.value, gk.value
 
     def wss(self, node_normals=None, pgauge=120.0):
         """WSS [3][nw] (Pa), wall pressure [nw] (Pa), valid [nw] from the current

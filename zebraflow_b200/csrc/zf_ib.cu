@@ -1373,6 +1373,54 @@ __device__ __forceinline__ void wss_window(int ii, int n, int lo, bool wrap, int
   else if (i1 < lo) i1 = lo;
 }
 
+// probe one DX along the node normal and the Peskin stencil around it, in the
+// reference's order (:320-356); fn(slot, weight) for every fluid point in 2 DX
+template <class Fn>
+__device__ __forceinline__ void wss_stencil(const IbArgs& a, float xm, float ym, float zm, float n0, float n1,
+                                            float n2, Fn&& fn) {
+  const float xp = (float)((double)xm + a.DX * (double)n0);
+  const float yp = (float)((double)ym + a.DX * (double)n1);
+  const float zp = (float)((double)zm + a.DX * (double)n2);
+  auto lat1 = [&](float x, double x0) { return (int)(((double)x - x0) / a.DX + 1.01) - 1; };
+  int i1, i2, j1, j2, k1, k2;
+  wss_window(lat1(xp, a.X0), a.nx, 2, false, i1, i2);
+  wss_window(lat1(yp, a.Y0), a.ny, 0, false, j1, j2);
+  wss_window(lat1(zp, a.Z0), a.nz, 0, a.per_z, k1, k2);
+  for (int i = i1; i <= i2; ++i)
+    for (int j = j1; j <= j2; ++j)
+      for (int k = k1; k <= k2; ++k) {
+        const float dx = xp - (float)(a.X0 + i * a.DX), dy = yp - (float)(a.Y0 + j * a.DX);
+        const float dz = wrapd(zp - (float)(a.Z0 + k * a.DX), a.LZ);
+        const float d = dist3(dx, dy, dz);
+        if (!((double)d <= 2 * a.DX)) continue;
+        if (i < 0 || i >= a.nx || j < 0 || j >= a.ny) continue;
+        int kk = k;
+        if (kk < 0 || kk >= a.nz) {
+          if (!a.per_z) continue;
+          kk = ((kk % a.nz) + a.nz) % a.nz;
+        }
+        const int64_t s = slot_of(a, i, j, kk);
+        if (s < 0 || s >= a.ns) continue;
+        const uint8_t cd = a.code[s];
+        if (!(cd >= 1 && cd <= 9)) continue;  // 0.11 < B_index < 4997
+        const float w =
+            (float)((1. + cosf((float)((double)kPI * fabsf(dx) / 2 / a.DX))) *
+                    (1. + cosf((float)((double)kPI * fabsf(dy) / 2 / a.DX))) *
+                    (1. + cosf((float)((double)kPI * fabsf(dz) / 2 / a.DX))) / 64.);
+        fn(s, w);
+      }
+}
+
+// WSS = -0.0012 Pa.s (u - (u.n) n) / (DX 1e-6 m)   (:358-368)
+__device__ __forceinline__ void wss_of(const IbArgs& a, float UU, float VV, float WW, float n0, float n1,
+                                       float n2, float& W0, float& W1, float& W2) {
+  const float vn = UU * n0 + VV * n1 + WW * n2;
+  const float vt0 = UU - vn * n0, vt1 = VV - vn * n1, vt2 = WW - vn * n2;
+  W0 = (float)(-0.0012 * (double)vt0 / a.DX / 1.e-06);
+  W1 = (float)(-0.0012 * (double)vt1 / a.DX / 1.e-06);
+  W2 = (float)(-0.0012 * (double)vt2 / a.DX / 1.e-06);
+}
+
 __global__ void k_wss(IbArgs a, const float* __restrict__ nrm, float pgauge, float* __restrict__ wss,
                       float* __restrict__ press, int32_t* __restrict__ valid) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1421,38 +1469,138 @@ __global__ void k_wss(IbArgs a, const float* __restrict__ nrm, float pgauge, flo
     if (valid) valid[m] = ok;
   }
   // wall shear stress from the velocity one DX into the lumen (:320-369)
-  const float xp = (float)((double)xm + a.DX * (double)n0);
-  const float yp = (float)((double)ym + a.DX * (double)n1);
-  const float zp = (float)((double)zm + a.DX * (double)n2);
-  int i1, i2, j1, j2, k1, k2;
-  wss_window(lat1(xp, a.X0), a.nx, 2, false, i1, i2);
-  wss_window(lat1(yp, a.Y0), a.ny, 0, false, j1, j2);
-  wss_window(lat1(zp, a.Z0), a.nz, 0, wz, k1, k2);
   float UU = 0.f, VV = 0.f, WW = 0.f;
-  for (int i = i1; i <= i2; ++i)
-    for (int j = j1; j <= j2; ++j)
-      for (int k = k1; k <= k2; ++k) {
-        const float dx = xp - (float)(a.X0 + i * a.DX), dy = yp - (float)(a.Y0 + j * a.DX);
-        const float dz = wrapd(zp - (float)(a.Z0 + k * a.DX), a.LZ);
-        const float d = dist3(dx, dy, dz);
-        if (!((double)d <= 2 * a.DX)) continue;
-        const int64_t s = point_slot(i, j, k);
-        if (s < 0 || s >= a.ns) continue;
-        const uint8_t cd = a.code[s];
-        if (!(cd >= 1 && cd <= 9)) continue;  // 0.11 < B_index < 4997
-        const float w =
-            (float)((1. + cosf((float)((double)kPI * fabsf(dx) / 2 / a.DX))) *
-                    (1. + cosf((float)((double)kPI * fabsf(dy) / 2 / a.DX))) *
-                    (1. + cosf((float)((double)kPI * fabsf(dz) / 2 / a.DX))) / 64.);
-        UU += w * a.mom[a.ns + s];
-        VV += w * a.mom[2 * a.ns + s];
-        WW += w * a.mom[3 * a.ns + s];
+  wss_stencil(a, xm, ym, zm, n0, n1, n2, [&](int64_t s, float w) {
+    UU += w * a.mom[a.ns + s];
+    VV += w * a.mom[2 * a.ns + s];
+    WW += w * a.mom[3 * a.ns + s];
+  });
+  float W0, W1, W2;
+  wss_of(a, UU, VV, WW, n0, n1, n2, W0, W1, W2);
+  wss[m] = W0;
+  wss[a.nw + m] = W1;
+  wss[2 * a.nw + m] = W2;
+}
+
+// ---- adjoint pieces of a WSS objective -------------------------------------------
+//
+// J = c sum_{m in patch} |WSS_m| for one state (c = 1 / (window length x patch
+// size)); k_wss_patch adds J to *acc (FP64), k_wss_patch_adj scatters dJ/dU
+// (U the moments interpolated at the probes) into gU[3][ns]:
+//   WSS = k (v - (v.n) n), k = -0.0012 / (DX 1e-6)  =>  dJ/dv = c k P_n WSS/|WSS|.
+__global__ void k_wss_patch(IbArgs a, const float* __restrict__ nrm, const int32_t* __restrict__ patch,
+                            int np, double c, double* acc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < np) {
+    const int m = patch[i];
+    const float n0 = nrm[m], n1 = nrm[a.nw + m], n2 = nrm[2 * a.nw + m];
+    float UU = 0.f, VV = 0.f, WW = 0.f;
+    wss_stencil(a, a.wxyz[m], a.wxyz[a.nw + m], a.wxyz[2 * a.nw + m], n0, n1, n2, [&](int64_t s, float w) {
+      UU += w * a.mom[a.ns + s];
+      VV += w * a.mom[2 * a.ns + s];
+      WW += w * a.mom[3 * a.ns + s];
+    });
+    float W0, W1, W2;
+    wss_of(a, UU, VV, WW, n0, n1, n2, W0, W1, W2);
+    v = c * sqrt((double)W0 * W0 + (double)W1 * W1 + (double)W2 * W2);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(acc, v);
+}
+
+__global__ void k_wss_patch_adj(IbArgs a, const float* __restrict__ nrm, const int32_t* __restrict__ patch,
+                                int np, double c, float* __restrict__ gU) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int m = patch[i];
+  const float n0 = nrm[m], n1 = nrm[a.nw + m], n2 = nrm[2 * a.nw + m];
+  const float xm = a.wxyz[m], ym = a.wxyz[a.nw + m], zm = a.wxyz[2 * a.nw + m];
+  float UU = 0.f, VV = 0.f, WW = 0.f;
+  wss_stencil(a, xm, ym, zm, n0, n1, n2, [&](int64_t s, float w) {
+    UU += w * a.mom[a.ns + s];
+    VV += w * a.mom[2 * a.ns + s];
+    WW += w * a.mom[3 * a.ns + s];
+  });
+  float W0, W1, W2;
+  wss_of(a, UU, VV, WW, n0, n1, n2, W0, W1, W2);
+  const double mag = sqrt((double)W0 * W0 + (double)W1 * W1 + (double)W2 * W2);
+  if (!(mag > 0.0)) return;
+  const double k = -0.0012 / a.DX / 1.e-06;
+  const double h0 = W0 / mag, h1 = W1 / mag, h2 = W2 / mag;
+  const double hn = h0 * n0 + h1 * n1 + h2 * n2;
+  const float g0 = (float)(c * k * (h0 - hn * n0)), g1 = (float)(c * k * (h1 - hn * n1)),
+              g2 = (float)(c * k * (h2 - hn * n2));
+  wss_stencil(a, xm, ym, zm, n0, n1, n2, [&](int64_t s, float w) {
+    atomicAdd(&gU[s], w * g0);
+    atomicAdd(&gU[a.ns + s], w * g1);
+    atomicAdd(&gU[2 * a.ns + s], w * g2);
+  });
+}
+
+// transpose of the spreading (k_ib_spread without the repulsion term): for
+// every node, g_v = force_scale sum_s w(s) G_v(s) over the spreading stencil
+__global__ void k_spread_adj(IbArgs a, CellArgs c, int spread_walls, const float* __restrict__ G,
+                             float* __restrict__ g_mem, float* __restrict__ g_nuc) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  const int64_t nmem = (int64_t)nc * c.nn;
+  const bool nuc = gid >= nmem;
+  if (gid >= nmem + (int64_t)nc * c.nnn) return;
+  const int n = nuc ? c.nnn : c.nn;
+  const int64_t lid = nuc ? gid - nmem : gid;
+  const int cell = (int)(lid / n), node = (int)(lid % n);
+  float* out = nuc ? g_nuc : g_mem;
+  double acc[3] = {0.0, 0.0, 0.0};
+  if (c.status[cell] > 0) {
+    float xp, yp, zp;
+    node_pos(nuc ? c.xn : c.x, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
+    const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
+              k0 = lat_index(zp, a.Z0, a.DX);
+    const float h2 = 2.f * a.DX;
+    const int ib = (int)floor(((double)xp - a.X0) / a.DX) - 1;
+    const int jb = (int)floor(((double)yp - a.Y0) / a.DX) - 1;
+    const int kb = (int)floor(((double)zp - a.Z0) / a.DX) - 1;
+    for (int i = ib; i <= ib + 3; ++i) {
+      if (i < 0 || i >= a.nx || i < i0 - 4 || i > i0 + 4) continue;
+      for (int j = jb; j <= jb + 3; ++j) {
+        if (j < 0 || j >= a.ny || j < j0 - 4 || j > j0 + 4) continue;
+        for (int k = kb; k <= kb + 3; ++k) {
+          if (k < a.kmin || k > a.kmax || k < k0 - 4 || k > k0 + 4) continue;
+          const int64_t s = slot_of(a, i, j, wrapk(a, k));
+          if (s < 0 || s >= a.ns) continue;
+          const uint8_t cd = a.code[s];
+          if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) continue;
+          const float dx = (float)((double)a.X0 + i * (double)a.DX) - xp;
+          const float dy = (float)((double)a.Y0 + j * (double)a.DX) - yp;
+          const float dz = (float)((double)a.Z0 + k * (double)a.DX) - zp;
+          if (!(dist3(dx, dy, dz) <= h2)) continue;
+          const float w = peskin(dx, dy, dz, h2);
+          for (int v = 0; v < 3; ++v) acc[v] += (double)w * G[v * a.ns + s];
+        }
       }
-  const float vn = UU * n0 + VV * n1 + WW * n2;
-  const float vt0 = UU - vn * n0, vt1 = VV - vn * n1, vt2 = WW - vn * n2;
-  wss[m] = (float)(-0.0012 * (double)vt0 / a.DX / 1.e-06);
-  wss[a.nw + m] = (float)(-0.0012 * (double)vt1 / a.DX / 1.e-06);
-  wss[2 * a.nw + m] = (float)(-0.0012 * (double)vt2 / a.DX / 1.e-06);
+    }
+  }
+  for (int v = 0; v < 3; ++v) out[((size_t)v * nc + cell) * n + node] = (float)(acc[v] * a.force_scale);
+}
+
+// Es enters the membrane forces through the calibrated springs only, and at
+// the calibration's fixed point kT/Plength and kp are both proportional to Es
+// (ZebraflowWT.c:1989-1990, :6906-6907); scaling them by s = 2 or 1/2 (exact in
+// binary) gives the forces at s Es.
+__global__ void k_scale_springs(CellArgs c, float s) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  float* ep = const_cast<float*>(c.epar);
+  float* epn = const_cast<float*>(c.epar_n);
+  if (e < c.ne) {
+    ep[c.ne + e] /= s;     // Plength
+    ep[2 * c.ne + e] *= s; // kp
+  }
+  if (e < c.nen) {
+    epn[c.nen + e] /= s;
+    epn[2 * c.nen + e] *= s;
+  }
 }
 
 int wss_launch(zf_ctx* ctx, const float* d_normals, double pgauge, float* d_wss, float* d_press,
@@ -1463,6 +1611,44 @@ int wss_launch(zf_ctx* ctx, const float* d_normals, double pgauge, float* d_wss,
   if (rc) return rc;
   k_wss<<<(a.nw + 127) / 128, 128, 0, ctx->stream>>>(a, d_normals ? d_normals : a.wnnrm, (float)pgauge,
                                                      d_wss, d_press, d_valid);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  return ZF_OK;
+}
+
+int wss_patch_launch(zf_ctx* ctx, const float* d_nrm, const int32_t* d_patch, int np, double c, double* d_acc) {
+  if (np <= 0) return ZF_OK;
+  k_wss_patch<<<(np + 127) / 128, 128, 0, ctx->stream>>>(ctx->ib, d_nrm, d_patch, np, c, d_acc);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  return ZF_OK;
+}
+
+int wss_patch_adj_launch(zf_ctx* ctx, const float* d_nrm, const int32_t* d_patch, int np, double c,
+                         float* d_gU) {
+  if (np <= 0) return ZF_OK;
+  k_wss_patch_adj<<<(np + 127) / 128, 128, 0, ctx->stream>>>(ctx->ib, d_nrm, d_patch, np, c, d_gU);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  return ZF_OK;
+}
+
+int spread_adj_launch(zf_ctx* ctx, const float* d_G, float* d_gmem, float* d_gnuc) {
+  const CellArgs& c = ctx->cells;
+  const int64_t n = (int64_t)c.n_cells * (c.nn + c.nnn);
+  if (n == 0) return ZF_OK;
+  k_spread_adj<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
+      ctx->ib, c, ctx->p.wall_mode == ZF_WALL_REF_EQ, d_G, d_gmem, d_gnuc);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  return ZF_OK;
+}
+
+int scale_springs_launch(zf_ctx* ctx, float s) {
+  const CellArgs& c = ctx->cells;
+  const int n = c.ne > c.nen ? c.ne : c.nen;
+  if (n == 0) return ZF_OK;
+  k_scale_springs<<<(n + 255) / 256, 256, 0, ctx->stream>>>(c, s);
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 1;
   return ZF_OK;

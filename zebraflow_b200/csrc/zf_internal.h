@@ -189,6 +189,18 @@ int ib_nuc_memb_launch(zf_ctx* c, int rebuild);
 int ib_rbc_rbc_launch(zf_ctx* c);
 int ib_node_tiles_launch(zf_ctx* c);
 int lbm_moments_launch(zf_ctx* c);
+// adjoint building blocks
+int lbm_adj_blocks(zf_ctx* c);
+int lbm_adj_launch(zf_ctx* c, const void* f_pre, const float* lam, float* lam_prev, float* gF,
+                   double* gw_partial);
+int lbm_seed_launch(zf_ctx* c, const void* f, const float* gU, float* lam);
+int lbm_step_buffers(zf_ctx* c, const void* fin, void* fout);
+int lbm_moments_of(zf_ctx* c, const void* f);
+int wss_patch_launch(zf_ctx* c, const float* d_nrm, const int32_t* d_patch, int np, double w, double* d_acc);
+int wss_patch_adj_launch(zf_ctx* c, const float* d_nrm, const int32_t* d_patch, int np, double w,
+                         float* d_gU);
+int spread_adj_launch(zf_ctx* c, const float* d_G, float* d_gmem, float* d_gnuc);
+int scale_springs_launch(zf_ctx* c, float s);
 int wss_launch(zf_ctx* c, const float* d_normals, double pgauge, float* d_wss, float* d_press,
                int32_t* d_valid);
 int ib_spread_launch(zf_ctx* c);

@@ -508,6 +508,231 @@ int lbm_moments_launch(zf_ctx* c) {
   return ZF_OK;
 }
 
+// ---- adjoint of the LBM step ----------------------------------------------------
+//
+// Forward step at a fluid point x (halfway bounce-back walls): pull
+// f_q = f_old[q](x - e_q), or f_old[opp q](x) where the link bounces back; then
+//   rho = sum f, m = sum c f, u = (m + F/2)/rho, F = g + dt BODYFORCE(x),
+//   f'_q = f_q + w (feq_q - f_q) + S_q,   w = 1/tau,
+//   feq_q = w_q rho (1 + 3 c.u + 4.5 (c.u)^2 - 1.5 u.u),
+//   S_q   = (1 - w/2) w_q (3 (c - u).F + 9 (c.u)(c.F))      (ZebraflowWT.c:6125-6142).
+// Every f_old value of a fluid point is pulled by exactly one fluid point, so
+// the transpose of the pull is a permutation: the adjoint of f_q at x is stored
+// at the slot the forward pulled it from, with no atomics.  With lam the
+// adjoint of f'(x), the transposed collision is
+//   lam_in_p = (1 - w) lam_p + A + sum_a B_a (c_pa - u_a)/rho,
+//   A   = w sum_q lam_q w_q (1 + 3 c.u + 4.5 (c.u)^2 - 1.5 u.u),
+//   B_a = sum_q lam_q [w w_q rho (3 c_qa + 9 (c.u) c_qa - 3 u_a)
+//                      + (1 - w/2) w_q (9 c_qa (c.F) - 3 F_a)],
+// and the parameter sensitivities of the step are
+//   dJ/dF_a = B_a/(2 rho) + sum_q lam_q (1 - w/2) w_q (3 (c_qa - u_a) + 9 (c.u) c_qa),
+//   dJ/dw   = sum_q lam_q (feq_q - f_q - S_q / (2 - w)).
+// gF accumulates dt dJ/dF (the sensitivity to BODYFORCE), gw per block dJ/dw.
+template <class C, typename I>
+__global__ void __launch_bounds__(kTilesPerBlock * ZF_TC)
+    k_lbm_adj(LbmArgs a, const float* __restrict__ lam, float* __restrict__ lam_prev,
+              float* __restrict__ gF, double* __restrict__ gw_partial) {
+  __shared__ I s_base[kTilesPerBlock][27];
+  __shared__ double s_gw[kTilesPerBlock * ZF_TC / 32];
+  const int lt = threadIdx.x >> 6, cell = threadIdx.x & 63;
+  const int tb = blockIdx.x * kTilesPerBlock;
+  for (int t = threadIdx.x; t < kTilesPerBlock * 27; t += blockDim.x) {
+    const int l = t / 27, s = t - l * 27;
+    int nb = -1;
+    if (tb + l < a.n_active) nb = a.nbr[(int64_t)a.active[tb + l] * 27 + s];
+    s_base[l][s] = nb >= 0 ? (I)nb * ZF_TC : (I)0;
+  }
+  __syncthreads();
+  bool live = tb + lt < a.n_active;
+  const I self = live ? s_base[lt][13] + (I)cell : (I)0;
+  const uint32_t link = live ? a.link[self] : 0u;
+  live = live && (link >> 31);
+  double gw = 0.0;
+  if (live) {
+    const int x = cell & 3, y = (cell >> 2) & 3, z = cell >> 4;
+    const I ns = (I)a.ns;
+    const typename C::T* __restrict__ fin = static_cast<const typename C::T*>(a.fin);
+    float f[ZF_Q];
+    I src[ZF_Q];
+#pragma unroll
+    for (int q = 0; q < ZF_Q; ++q) {
+      I idx;
+      if (q == 18) {
+        idx = (I)18 * ns + self;
+      } else {
+        const int sx = x - EX(q), sy = y - EY(q), sz = z - EZ(q);
+        const int s27 = ((sz >> 2) + 1) * 9 + ((sy >> 2) + 1) * 3 + ((sx >> 2) + 1);
+        const int scell = (sx & 3) | ((sy & 3) << 2) | ((sz & 3) << 4);
+        const I pull = (I)q * ns + s_base[lt][s27] + (I)scell;
+        const I bb = (I)OPP(q) * ns + self;
+        idx = ((link >> q) & 1u) ? bb : pull;
+      }
+      src[q] = idx;
+      f[q] = WQ(q) * (a.rho_ref + C::dec(fin[idx], q, a));
+    }
+    const float Fx = a.gx + a.force_dt * a.force[self], Fy = a.gy + a.force_dt * a.force[ns + self],
+                Fz = a.gz + a.force_dt * a.force[2 * ns + self];
+    float rho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+#pragma unroll
+    for (int q = 0; q < ZF_Q; ++q) {
+      rho += f[q];
+      if (EX(q)) mx += EX(q) * f[q];
+      if (EY(q)) my += EY(q) * f[q];
+      if (EZ(q)) mz += EZ(q) * f[q];
+    }
+    const float irho = 1.f / rho;
+    const float ux = (mx + 0.5f * Fx) * irho, uy = (my + 0.5f * Fy) * irho, uz = (mz + 0.5f * Fz) * irho;
+    const float om = 1.f / a.tau, sfac = 1.f - 0.5f * om;
+    const float usq = ux * ux + uy * uy + uz * uz, uF = ux * Fx + uy * Fy + uz * Fz;
+    float A = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f, gFx = 0.f, gFy = 0.f, gFz = 0.f;
+    float lq[ZF_Q];
+#pragma unroll
+    for (int q = 0; q < ZF_Q; ++q) {
+      const float l = lam[(I)q * ns + self];
+      lq[q] = l;
+      const float cu = EX(q) * ux + EY(q) * uy + EZ(q) * uz;
+      const float cF = EX(q) * Fx + EY(q) * Fy + EZ(q) * Fz;
+      const float poly = 1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * usq;
+      const float feq = WQ(q) * rho * poly;
+      const float S = sfac * WQ(q) * (3.f * (cF - uF) + 9.f * cu * cF);
+      A += l * WQ(q) * poly;
+      const float e = om * WQ(q) * rho, sw = sfac * WQ(q);
+      // d feq/d u_a = w_q rho (3 c_a + 9 cu c_a - 3 u_a); d S/d u_a = sw (9 c_a cF - 3 F_a)
+      Bx += l * (e * (3.f * EX(q) + 9.f * cu * EX(q) - 3.f * ux) + sw * (9.f * EX(q) * cF - 3.f * Fx));
+      By += l * (e * (3.f * EY(q) + 9.f * cu * EY(q) - 3.f * uy) + sw * (9.f * EY(q) * cF - 3.f * Fy));
+      Bz += l * (e * (3.f * EZ(q) + 9.f * cu * EZ(q) - 3.f * uz) + sw * (9.f * EZ(q) * cF - 3.f * Fz));
+      // d S/d F_a at fixed u
+      gFx += l * sw * (3.f * (EX(q) - ux) + 9.f * cu * EX(q));
+      gFy += l * sw * (3.f * (EY(q) - uy) + 9.f * cu * EY(q));
+      gFz += l * sw * (3.f * (EZ(q) - uz) + 9.f * cu * EZ(q));
+      // d f'/d w = feq - f - S/(2 - w) ... written through sfac: dS/dw = -S/(2 sfac)
+      gw += (double)(l * (feq - f[q] - 0.5f * WQ(q) * (3.f * (cF - uF) + 9.f * cu * cF)));
+    }
+    A *= om;
+    gFx += 0.5f * Bx * irho;
+    gFy += 0.5f * By * irho;
+    gFz += 0.5f * Bz * irho;
+    gF[self] += a.force_dt * gFx;
+    gF[ns + self] += a.force_dt * gFy;
+    gF[2 * ns + self] += a.force_dt * gFz;
+    const float om1 = 1.f - om;
+#pragma unroll
+    for (int q = 0; q < ZF_Q; ++q) {
+      const float li = om1 * lq[q] + A + (Bx * (EX(q) - ux) + By * (EY(q) - uy) + Bz * (EZ(q) - uz)) * irho;
+      lam_prev[src[q]] = li;
+    }
+  }
+  // per-block sum of dJ/dw (uniform branch)
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) gw += __shfl_down_sync(0xffffffffu, gw, o);
+  if ((threadIdx.x & 31) == 0) s_gw[threadIdx.x >> 5] = gw;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kTilesPerBlock * ZF_TC / 32; ++w) t += s_gw[w];
+    gw_partial[blockIdx.x] += t;
+  }
+}
+
+// The objective's seed: lam[q](x) += sum_a gU_a(x) (c_qa - U_a)/rho at fluid
+// points, U and rho being the moments (no force shift) of the populations f.
+template <class C>
+__global__ void k_seed_moments(LbmArgs a, const float* __restrict__ gU, float* __restrict__ lam) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.ns) return;
+  const uint8_t cd = a.code[s];
+  if (!(cd >= 1 && cd <= 9)) return;
+  const float gx = gU[s], gy = gU[a.ns + s], gz = gU[2 * a.ns + s];
+  if (gx == 0.f && gy == 0.f && gz == 0.f) return;
+  const typename C::T* __restrict__ f = static_cast<const typename C::T*>(a.fin);
+  float fq[ZF_Q], rho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+#pragma unroll
+  for (int q = 0; q < ZF_Q; ++q) {
+    fq[q] = WQ(q) * (a.rho_ref + C::dec(f[(int64_t)q * a.ns + s], q, a));
+    rho += fq[q];
+    mx += EX(q) * fq[q];
+    my += EY(q) * fq[q];
+    mz += EZ(q) * fq[q];
+  }
+  const float ir = 1.f / rho, Ux = mx * ir, Uy = my * ir, Uz = mz * ir;
+#pragma unroll
+  for (int q = 0; q < ZF_Q; ++q)
+    lam[(int64_t)q * a.ns + s] += (gx * (EX(q) - Ux) + gy * (EY(q) - Uy) + gz * (EZ(q) - Uz)) * ir;
+}
+
+template <class C>
+struct AdjStep {
+  static void run(zf_ctx* c, const LbmArgs& a, const float* lam, float* lam_prev, float* gF, double* gw) {
+    if (c->n_active == 0) return;
+    const int grid = (c->n_active + kTilesPerBlock - 1) / kTilesPerBlock;
+    if ((int64_t)ZF_Q * c->ns < (int64_t)INT32_MAX)
+      k_lbm_adj<C, uint32_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a, lam, lam_prev, gF, gw);
+    else
+      k_lbm_adj<C, int64_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a, lam, lam_prev, gF, gw);
+  }
+};
+template <class C>
+struct SeedMoments {
+  static void run(zf_ctx* c, const LbmArgs& a, const float* gU, float* lam) {
+    k_seed_moments<C><<<(unsigned)((c->ns + 255) / 256), 256, 0, c->stream>>>(a, gU, lam);
+  }
+};
+template <class C>
+struct StepBuffers {
+  static void run(zf_ctx* c, const LbmArgs& a) { LaunchStep<C>::run(c, a); }
+};
+template <class C>
+struct MomentsOf {
+  static void run(zf_ctx* c, const LbmArgs& a) {
+    k_moments<C><<<(unsigned)((c->ns + 255) / 256), 256, 0, c->stream>>>(a);
+  }
+};
+
+// number of per-block partial sums k_lbm_adj writes
+int lbm_adj_blocks(zf_ctx* c) { return (c->n_active + kTilesPerBlock - 1) / kTilesPerBlock; }
+
+// one adjoint step: f_pre are the populations before the forward step
+int lbm_adj_launch(zf_ctx* c, const void* f_pre, const float* lam, float* lam_prev, float* gF,
+                   double* gw_partial) {
+  LbmArgs a = make_args(c);
+  a.fin = f_pre;
+  dispatch_storage<AdjStep>(c->p.storage, c, a, lam, lam_prev, gF, gw_partial);
+  ZF_CUDA(cudaGetLastError());
+  c->launches += c->n_active > 0;
+  return ZF_OK;
+}
+
+int lbm_seed_launch(zf_ctx* c, const void* f, const float* gU, float* lam) {
+  LbmArgs a = make_args(c);
+  a.fin = f;
+  dispatch_storage<SeedMoments>(c->p.storage, c, a, gU, lam);
+  ZF_CUDA(cudaGetLastError());
+  c->launches += 1;
+  return ZF_OK;
+}
+
+// forward step from explicit population buffers (the body force and
+// parameters of the context; no moments, no force clearing)
+int lbm_step_buffers(zf_ctx* c, const void* fin, void* fout) {
+  LbmArgs a = make_args(c);
+  a.fin = fin;
+  a.fout = fout;
+  dispatch_storage<StepBuffers>(c->p.storage, c, a);
+  ZF_CUDA(cudaGetLastError());
+  c->launches += (c->n_active > 0) + (c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0);
+  return ZF_OK;
+}
+
+// moments of explicit populations into the context's moment planes
+int lbm_moments_of(zf_ctx* c, const void* f) {
+  LbmArgs a = make_args(c);
+  a.fin = f;
+  dispatch_storage<MomentsOf>(c->p.storage, c, a);
+  ZF_CUDA(cudaGetLastError());
+  c->launches += 1;
+  return ZF_OK;
+}
+
 template <class C>
 struct Fill {
   static void run(zf_ctx* c, const LbmArgs& a, int b) {
