@@ -355,11 +355,13 @@ def measure_storage(case, storage, args, dev, stream, barrier, sample_clocks=Fal
     barrier()
     ms_e2e = 1e3 * (time.perf_counter() - t0)
     removed_end = int(ctx.status().cells_removed)
+    # wall shear stress of the final state (compared across storage forms)
+    wss = ctx.wss()[0] if case.wall is not None else None
     ctx.set_stream(None)
     ctx.close()
     return {"ms": ms, "launches": launches, "clocks": clocks, "n_mem": n_mem, "removed": removed,
             "removed_end": removed_end, "ms_prof": ms_prof, "lbm_ms": lbm_ms, "lbm_n": lbm_n,
-            "mem_ms": mem_ms, "mem_n": mem_n, "n_mem_prof": n_mem_prof, "ms_e2e": ms_e2e,
+            "mem_ms": mem_ms, "mem_n": mem_n, "n_mem_prof": n_mem_prof, "ms_e2e": ms_e2e, "wss": wss,
             "mass": mass.value}
 
 
@@ -384,6 +386,57 @@ def summarize(case, storage, r, steps, world, peak):
     return out
 
 
+def measure_adjoint(dev, stream, barrier, seed=2024):
+    """Cost of the hand-written adjoint on the C3 tube (96x96x512, R = 40,
+    200 RBCs held at slightly deformed positions): J = mean |WSS| over a
+    64-lattice-unit wall patch across steps 300..500, gradients for the
+    body-force field, tau, Es and kb, checkpoint every 50 steps."""
+    import torch
+    import zebraflow_b200 as zf
+    nx, ny, nz, R = 96, 96, 512, 40.0
+    c = (nx - 1) / 2.0
+    b = zf.gen_tube(nx, ny, nz, c, c, R, True)
+    xyz, tri = zf.gen_icosphere(3)
+    xyzn, trin = zf.gen_icosphere(2)
+    rest = xyz * np.array(AXES_UM)
+    rest_n = xyzn * np.array(AXES_N_UM)
+    x, xn = zf.gen_cells(b, 200, rest, rest_n, AXES_UM, seed=seed, dx=DX_UM, margin=PLACEMENT_MARGIN_UM)
+    rng = np.random.default_rng(seed)
+    x = x + 0.02 * rng.standard_normal(x.shape)
+    wall = zf.gen_wall_tube(c, c, R, nz)
+    z = wall[0][2] / DX_UM
+    patch = np.nonzero((z >= 224) & (z < 288))[0].astype(np.int32)
+    p = zf.default_params(nx=nx, ny=ny, nz=nz, tau=0.9, tau_from_phase=0, wall_mode=zf.WALL_HALFWAY_BB,
+                          periodic=(0, 0, 1), g=(0.0, 0.0, 2e-6), origin=(0.0, 0.0, 0.0), dx=DX_UM,
+                          area0=0.0, volume0=0.0, storage=zf.STORE_F32_DEV)
+    ctx = zf.Context(p, device=dev)
+    ctx.set_lattice(b)
+    ctx.set_wall(*wall)
+    ctx.set_mesh(rest, tri, rest_n, zf.mesh_edges(trin))
+    ctx.set_cells(x, xn)
+    ctx.set_stream(stream.cuda_stream)
+    nsteps, t0, t1, K = 500, 300, 500, 50
+    ctx.wss_objective(nsteps, t0, t1, patch)  # warm-up
+    barrier()
+    t = time.perf_counter()
+    J = ctx.wss_objective(nsteps, t0, t1, patch)
+    t_fwd = time.perf_counter() - t
+    barrier()
+    t = time.perf_counter()
+    Ja, gfb, gtau, gEs, gkb = ctx.wss_adjoint(nsteps, t0, t1, patch, checkpoint=K)
+    t_adj = time.perf_counter() - t
+    ctx.set_stream(None)
+    ctx.close()
+    return {"workload": "c3_tube_96x96x512_200rbc", "fluid_points": int((b > 0).sum()),
+            "steps": nsteps, "objective_window": [t0, t1], "patch_wall_nodes": int(patch.size),
+            "checkpoint_interval": K, "storage": "f32dev",
+            "forward_ms": round(1e3 * t_fwd, 2), "forward_and_adjoint_ms": round(1e3 * t_adj, 2),
+            "gradient_cost_over_forward": round((t_adj - t_fwd) / t_fwd, 3),
+            "J_pa": J, "dJ_dtau": gtau, "dJ_dEs": gEs, "dJ_dkb": gkb,
+            "dJ_dfb_max": float(np.abs(gfb).max()),
+            "timing": "host wall clock around each call (one synchronisation at its end)"}
+
+
 def run_ours(args):
     world, rank, local = dist_setup()
     import torch
@@ -406,6 +459,7 @@ def run_ours(args):
     peak, peak_kind = read_peaks()
 
     main_r = measure_storage(case, storage, args, dev, stream, barrier, sample_clocks=(rank == 0))
+    adjoint = measure_adjoint(dev, stream, barrier) if args.adjoint else None
     variants = {}
     for name in [v for v in args.variants.split(",") if v and v != args.storage]:
         variants[name] = (STORAGES[name], measure_storage(case, STORAGES[name], args, dev, stream,
@@ -447,6 +501,9 @@ def run_ours(args):
                         "k_lbm_ms": round(v["k_lbm_ms"], 5),
                         "k_lbm_frac": round(v["k_lbm_frac"], 4) if v["k_lbm_frac"] else None,
                         "cells_removed": r["removed_end"]}
+            if r["wss"] is not None and main_r["wss"] is not None:
+                vs[name]["wss_rel_l2_vs_" + args.storage] = float(
+                    np.linalg.norm(r["wss"] - main_r["wss"]) / np.linalg.norm(main_r["wss"]))
         alg_launch = case.n_fluid * lbm_bytes_per_point(storage, False)
         result = {
             "metric": "MLUPS", "value": round(s["mlups"], 1), "unit": "MLUPS", "n_gpus": world,
@@ -472,6 +529,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "e2e": {"value": round(s["mlups_e2e"], 1), "unit": "MLUPS", "h2d_bytes_per_step": 12,
                     "d2h_bytes_per_step": 8},
+            "adjoint": adjoint,
             "gpu_launches": main_r["launches"],
             "clocks": main_r["clocks"],
         }
@@ -498,6 +556,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--reference-seconds", type=float, default=90.0)
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
+                    help="skip the adjoint cost measurement on the C3 tube")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
