@@ -163,27 +163,15 @@ __global__ void k_ib_interp(IbArgs a, CellArgs c) {
 // strict <, which is the reference's running minimum taken list by list.
 __device__ __forceinline__ void wall_list_min(const IbArgs& a, int nodewall, float xp, float yp, float zp,
                                               float& best, int& tbest) {
-  const int32_t* L = a.wntri + (size_t)(nodewall - 1) * (a.wcap + 1);
-  const int nl = L[0];
-  for (int l = 1; l <= nl; ++l) {
-    const int tri = L[l];
-    for (int v = 0; v < 4; ++v) {
-      float px, py, pz;
-      if (v < 3) {
-        const int wn = a.wtri[3 * tri + v];
-        px = a.wxyz[wn];
-        py = a.wxyz[a.nw + wn];
-        pz = a.wxyz[2 * a.nw + wn];
-      } else {
-        px = a.wcen[tri];
-        py = a.wcen[a.mt + tri];
-        pz = a.wcen[2 * a.mt + tri];
-      }
-      const float d = dist3(xp - px, yp - py, wrapd(zp - pz, a.LZ));
-      if (d < best) {
-        best = d;
-        tbest = tri;
-      }
+  // the node's candidates, stored contiguously in list order: for each listed
+  // triangle its 3 vertices and its centroid (x, y, z, triangle id)
+  const int32_t c0 = a.wcand_off[nodewall - 1], c1 = a.wcand_off[nodewall];
+  for (int i = c0; i < c1; ++i) {
+    const float4 p = a.wcand[i];
+    const float d = dist3(xp - p.x, yp - p.y, wrapd(zp - p.z, a.LZ));
+    if (d < best) {
+      best = d;
+      tbest = __float_as_int(p.w);
     }
   }
 }
@@ -503,9 +491,10 @@ __device__ __forceinline__ float rec_pack(int kk, float rb) {
 __device__ __forceinline__ int rec_kk(float w) { return (int)(__float_as_uint(w) & 0xffu); }
 __device__ __forceinline__ float rec_rb(float w) { return (float)(__float_as_uint(w) >> 8) * (1.f / 1048576.f); }
 
-// per bin entry: centroid and bounding radius, normal and triangle id, so the
-// repulsion search reads one contiguous range of 32-byte records per run of
-// bins.  The radius bounds the distance from the centroid to any point of the
+// per bin entry: centroid and bounding radius, normal and triangle id, and the
+// three vertices (fp32 of the fp64 positions, with their node ids), so the
+// repulsion search reads one contiguous range of records per run of bins and
+// evaluates a triangle from its own record.  The radius bounds the distance from the centroid to any point of the
 // triangle (the vertices, as float), with a margin for float rounding.
 __global__ void k_bin_records(IbArgs a, CellArgs c, const int32_t* total) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -525,6 +514,13 @@ __global__ void k_bin_records(IbArgs a, CellArgs c, const int32_t* total) {
     r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
   }
   a.bin_c[e] = make_float4(cx, cy, cz, rec_pack(a.bin_kk[e], sqrtf(r2) * 1.0001f + 1e-3f));
+  const int64_t stride = (int64_t)nc * c.nt;
+  for (int v = 0; v < 3; ++v) {
+    const int n = c.tri[3 * tri + v];
+    a.bin_v[v * stride + e] = make_float4((float)c.x[((size_t)0 * nc + m) * c.nn + n],
+                                          (float)c.x[((size_t)1 * nc + m) * c.nn + n],
+                                          (float)c.x[((size_t)2 * nc + m) * c.nn + n], __int_as_float(n));
+  }
   a.bin_n[e] = make_float4(c.tri_nrm[((size_t)0 * nc + m) * c.nt + tri],
                            c.tri_nrm[((size_t)1 * nc + m) * c.nt + tri],
                            c.tri_nrm[((size_t)2 * nc + m) * c.nt + tri], __int_as_float(g));
@@ -631,11 +627,10 @@ __global__ void k_nuc_memb(IbArgs a, CellArgs c, int rebuild, unsigned long long
 // entry per lane (the 16 sub-centroids), and each owner adds its entries'
 // results in its own scan order, so the sums are deterministic.
 
-__device__ __forceinline__ void rbc_entry(const IbArgs& a, const CellArgs& c, const float4 cr, int g,
+__device__ __forceinline__ void rbc_entry(const IbArgs& a, const CellArgs& c, int e, const float4 cr,
                                           float xc, float yc, float zc, float& tx, float& ty, float& tz) {
-  const int nc = c.n_cells;
-  const int m = g / c.nt, tri = g - m * c.nt;
-  const int n1 = c.tri[3 * tri], n2 = c.tri[3 * tri + 1], n3 = c.tri[3 * tri + 2];
+  const int64_t stride = (int64_t)c.n_cells * c.nt;
+  const float4 v1 = a.bin_v[e], v2 = a.bin_v[stride + e], v3 = a.bin_v[2 * stride + e];
   const float dzc = wrapd(cr.z - zc, a.LZ);
   const float shift = (cr.z - zc) - dzc;  // periodic image of the other cell
   // the 15 points of the subdivided triangle, then the 16 sub-triangle
@@ -644,9 +639,9 @@ __device__ __forceinline__ void rbc_entry(const IbArgs& a, const CellArgs& c, co
 #pragma unroll
   for (int v = 0; v < 3; ++v) {
     const float off = v == 2 ? shift : 0.f;
-    tp[1][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n1] - off;
-    tp[2][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n2] - off;
-    tp[3][v] = (float)c.x[((size_t)v * nc + m) * c.nn + n3] - off;
+    tp[1][v] = (v == 0 ? v1.x : v == 1 ? v1.y : v1.z) - off;
+    tp[2][v] = (v == 0 ? v2.x : v == 1 ? v2.y : v2.z) - off;
+    tp[3][v] = (v == 0 ? v3.x : v == 1 ? v3.y : v3.z) - off;
     tp[4][v] = 0.5f * (tp[1][v] + tp[2][v]);
     tp[5][v] = 0.5f * (tp[2][v] + tp[3][v]);
     tp[6][v] = 0.5f * (tp[1][v] + tp[3][v]);
@@ -664,19 +659,22 @@ __device__ __forceinline__ void rbc_entry(const IbArgs& a, const CellArgs& c, co
   constexpr int kSubA[16] = {1, 7, 7, 4, 4, 8, 8, 12, 13, 13, 14, 14, 6, 15, 15, 11};
   constexpr int kSubB[16] = {7, 13, 4, 14, 8, 9, 2, 13, 15, 14, 5, 9, 15, 10, 5, 10};
   constexpr int kSubC[16] = {12, 12, 13, 13, 14, 14, 9, 6, 6, 15, 15, 5, 11, 11, 10, 3};
+  // (the reference divides by 3 and by d; multiplying by 1/3 and by 1/d
+  // differs in the last bit only, far below the forces' fp32 resolution)
   tx = ty = tz = 0.f;
 #pragma unroll
   for (int v = 0; v < 16; ++v) {  // ZebraflowWT.c:10028-10042
-    const float cx = (tp[kSubA[v]][0] + tp[kSubB[v]][0] + tp[kSubC[v]][0]) / 3.f;
-    const float cy = (tp[kSubA[v]][1] + tp[kSubB[v]][1] + tp[kSubC[v]][1]) / 3.f;
-    const float cz = (tp[kSubA[v]][2] + tp[kSubB[v]][2] + tp[kSubC[v]][2]) / 3.f;
+    const float third = 1.f / 3.f;
+    const float cx = (tp[kSubA[v]][0] + tp[kSubB[v]][0] + tp[kSubC[v]][0]) * third;
+    const float cy = (tp[kSubA[v]][1] + tp[kSubB[v]][1] + tp[kSubC[v]][1]) * third;
+    const float cz = (tp[kSubA[v]][2] + tp[kSubB[v]][2] + tp[kSubC[v]][2]) * third;
     const float dx = cx - xc, dy = cy - yc, dz = cz - zc;
     const float d = dist3(dx, dy, dz);
     if (d < 1.0f) {
-      const float repulf = (float)(-8.333e-07 * (1.0 - (double)d) / 1.0);
-      tx += repulf * (dx / d);
-      ty += repulf * (dy / d);
-      tz += repulf * (dz / d);
+      const float s = -8.333e-07f * (1.f - d) / d;
+      tx += s * dx;
+      ty += s * dy;
+      tz += s * dz;
     }
   }
 }
@@ -748,7 +746,7 @@ __global__ void __launch_bounds__(kRepWarps * 32) k_rbc_rbc(IbArgs a, CellArgs c
     const float ox = __shfl_sync(FULL, xc, owner), oy = __shfl_sync(FULL, yc, owner),
                 oz = __shfl_sync(FULL, zc, owner);
     float tx = 0.f, ty = 0.f, tz = 0.f;
-    if (my >= 0) rbc_entry(a, c, a.bin_c[my], __float_as_int(a.bin_n[my].w), ox, oy, oz, tx, ty, tz);
+    if (my >= 0) rbc_entry(a, c, my, a.bin_c[my], ox, oy, oz, tx, ty, tz);
     sq_r[w][lane][0] = tx;
     sq_r[w][lane][1] = ty;
     sq_r[w][lane][2] = tz;
@@ -964,7 +962,7 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
         if (lane < nb) {
           const int e = queue[lane];
           float tx2, ty2, tz2;
-          rbc_entry(a, c, a.bin_c[e], __float_as_int(a.bin_n[e].w), xc, yc, zc, tx2, ty2, tz2);
+          rbc_entry(a, c, e, a.bin_c[e], xc, yc, zc, tx2, ty2, tz2);
           rx += tx2;
           ry += ty2;
           rz += tz2;
@@ -1046,8 +1044,9 @@ __global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c
                 const int g = __float_as_int(nr.w);
                 pass = true;
                 if (g >= g_own && g < g_own + c.nt) {
-                  const int tri = g - g_own;
-                  pass = !(c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node);
+                  const int64_t stride = (int64_t)nc * c.nt;
+                  pass = !(__float_as_int(a.bin_v[e].w) == node || __float_as_int(a.bin_v[stride + e].w) == node ||
+                           __float_as_int(a.bin_v[2 * stride + e].w) == node);
                 }
               }
             }

@@ -124,11 +124,17 @@ int build_view(zf_ctx* c, const WallHost* W) {
     if ((rc = dalloc<int32_t>(c, own, const_cast<int32_t**>(&a.wntri), W->ntri.size(), W->ntri.data())))
       return rc;
     if ((rc = dalloc<float>(c, own, const_cast<float**>(&a.wrad), W->rad.size(), W->rad.data()))) return rc;
+    if ((rc = dalloc<int32_t>(c, own, const_cast<int32_t**>(&a.wcand_off), W->cand_off.size(),
+                              W->cand_off.data())))
+      return rc;
+    if ((rc = dalloc<float4>(c, own, const_cast<float4**>(&a.wcand), W->cand.size(), W->cand.data()))) return rc;
     if ((rc = dalloc<float>(c, own, const_cast<float**>(&a.wnnrm), W->nnrm.size(), W->nnrm.data())))
       return rc;
   } else {
     a.nw = a.mt = a.wcap = 0;
     a.wxyz = a.wnrm = a.wcen = a.wrad = a.wnnrm = nullptr;
+    a.wcand_off = nullptr;
+    a.wcand = nullptr;
     a.wtri = a.wntri = nullptr;
   }
   ZF_CUDA(cudaStreamSynchronize(c->stream));
@@ -151,6 +157,7 @@ int ib_buffers(zf_ctx* c) {
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, const_cast<int32_t**>(&a.bin_tri), ntri))) return rc;
   if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_c, ntri))) return rc;
   if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_n, ntri))) return rc;
+  if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_v, 3 * ntri))) return rc;
   if ((rc = dalloc<uint8_t>(c, c->ib_allocs, &a.bin_kk, ntri))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.bin_reach, nscan))) return rc;
   // node-tile lists

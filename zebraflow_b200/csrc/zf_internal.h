@@ -114,6 +114,9 @@ struct WallHost {
   std::vector<float> nrm, cen;   // [3][mt]
   std::vector<float> nnrm;       // [3][nw] area-weighted node normals (unit, into the lumen)
   std::vector<int32_t> ntri;     // [nw][cap+1]: count, triangles (0-based)
+  std::vector<int32_t> cand_off; // [nw+1] candidates of each node's list ...
+  std::vector<float4> cand;      // ... in list order: 3 vertices and the centroid of each
+                                 // listed triangle (x, y, z, triangle id as int bits)
   std::vector<float> rad;        // [nw] farthest vertex or centroid of the node's listed
                                  // triangles from the node (um, rounded up)
   std::vector<int32_t> windex;   // [npts] 1-based wall node, 0 none
@@ -151,6 +154,8 @@ struct IbArgs {
   const float* wcen;            // [3][mt]
   const int32_t* wntri;         // [nw][wcap+1]
   const float* wrad;            // [nw] WallHost::rad
+  const int32_t* wcand_off;     // [nw+1] WallHost::cand_off
+  const float4* wcand;          // WallHost::cand
   // cell list of triangle centroids over population slots (CSR).  Bin keys
   // order the points of a tile with z fastest (bin_key), so the bins of a
   // run of points along z are one contiguous range of entries.
@@ -158,6 +163,7 @@ struct IbArgs {
   const int32_t* bin_tri;       // [n_cells*nt] global triangle id = cell*nt + tri
   float4* bin_c;                // [n_cells*nt] per entry: centroid xyz, bounding radius
   float4* bin_n;                // [n_cells*nt] per entry: normal xyz, id (int bits)
+  float4* bin_v;                // [3][n_cells*nt] per entry: vertex xyz (fp32), node id (int bits)
   uint8_t* bin_kk;              // [n_cells*nt] per entry: its key inside the tile (0..63)
   int32_t* bin_reach;           // [ns+1] float bits: farthest point of a bin's triangles
                                 // from the bin point (um, rounded up); [ns] the largest

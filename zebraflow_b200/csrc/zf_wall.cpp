@@ -73,6 +73,24 @@ int wall_build(zf_ctx* c, int nw, const float* xyz, int mt, const int32_t* tri1,
                       xyz[(size_t)a * nw + W.tri[3 * m + 2]];
       W.cen[(size_t)a * mt + m] = (float)(s / 3.);
     }
+  // candidate points of each node's list, contiguous, in the order searched
+  W.cand_off.assign((size_t)nw + 1, 0);
+  for (int n = 0; n < nw; ++n) W.cand_off[n + 1] = W.cand_off[n] + 4 * W.ntri[(size_t)n * (cap + 1)];
+  W.cand.resize((size_t)W.cand_off[nw]);
+  for (int n = 0; n < nw; ++n) {
+    const int32_t* L = &W.ntri[(size_t)n * (cap + 1)];
+    float4* out = W.cand.data() + W.cand_off[n];
+    for (int l = 1; l <= L[0]; ++l) {
+      const int t = L[l];
+      float tid;
+      std::memcpy(&tid, &t, sizeof tid);
+      for (int v = 0; v < 3; ++v) {
+        const int q = W.tri[3 * (size_t)t + v];
+        *out++ = make_float4(xyz[q], xyz[(size_t)nw + q], xyz[2 * (size_t)nw + q], tid);
+      }
+      *out++ = make_float4(W.cen[t], W.cen[(size_t)mt + t], W.cen[2 * (size_t)mt + t], tid);
+    }
+  }
   // node normals: triangle normals weighted by triangle area, normalised
   W.nnrm.assign(3 * (size_t)nw, 0.f);
   {
