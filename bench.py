@@ -21,8 +21,8 @@ One JSON line on rank 0:
           sets the driving force from pinned host memory and reads the FP64
           global mass back to the host (zf_set_uniform_force + zf_step_mass)
   roofline  k_lbm's algorithmic bytes over its average launch time, taken
-          from per-launch CUDA events (zf_profile) in a second timed pass of
-          the same steps
+          from CUDA events around the runs of plain LBM steps between
+          membrane blocks (zf_profile) in a second timed pass of the same steps
   storage_variants  the same measurement with fp16 / bf16 deviation storage
   cpu_baseline  the CPU restatement of the reference time loop (oracle,
           OpenMP, reference pass structure) on the host cores, one bounded
@@ -372,11 +372,9 @@ def summarize(case, storage, r, steps, world, peak):
            "mlups_e2e": world * n * steps / (r["ms_e2e"] * 1e-3) / 1e6}
     nodes = case.n_cells * (case.nn + case.nnn) if case.n_cells else 0
     out["membrane_node_updates_per_s"] = world * nodes * r["n_mem"] / (r["ms"] * 1e-3)
-    # k_lbm roofline from the profiled pass: algorithmic bytes of all launches
-    # over their summed device time
-    nm = r["mem_n"]
-    alg = n * (lbm_bytes_per_point(storage, False) * (r["lbm_n"] - nm)
-               + lbm_bytes_per_point(storage, True) * nm)
+    # k_lbm roofline from the profiled pass: algorithmic bytes of the plain LBM
+    # launches (timed as runs of consecutive launches) over their device time
+    alg = n * lbm_bytes_per_point(storage, False) * r["lbm_n"]
     lbm_s = r["lbm_ms"] * 1e-3
     out["k_lbm_ms"] = r["lbm_ms"] / max(r["lbm_n"], 1)
     out["k_lbm_gbs"] = alg / lbm_s / 1e9 if lbm_s > 0 else None

@@ -371,9 +371,11 @@ int zf_step_mass(zf_ctx* ctx, double* mass);
 /* Number of kernels the context has launched so far. */
 int zf_launch_count(zf_ctx* ctx, int64_t* n);
 
-/* Instrumentation of zf_step: with enable=1, CUDA events bracket the LBM
- * kernel and the membrane/IB work of up to `capacity` iterations;
- * zf_profile_read returns their summed device times (ms) and counts. */
+/* Instrumentation of zf_step: with enable=1, CUDA events bracket each run of
+ * consecutive plain LBM steps (the steps between membrane blocks) and each
+ * membrane/IB block, up to `capacity` of each; zf_profile_read returns the
+ * summed device times (ms), the number of LBM launches in the timed runs and
+ * the number of membrane blocks. */
 int zf_profile(zf_ctx* ctx, int enable, int capacity);
 int zf_profile_read(zf_ctx* ctx, float* lbm_ms, int* lbm_count, float* membrane_ms,
                     int* membrane_count);

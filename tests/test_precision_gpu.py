@@ -1,22 +1,27 @@
-"""Precision forms against the FP64 oracle on a coupled run (config C2 at test
-scale): a bounce-back tube 40x40x48 (R = 16), 4 nucleated RBCs, its wall mesh,
-1000 steps of the reference loop with the membrane/IB block every 10 steps,
-force 5e-6 (centre-line speed below the reference's 5e-3 removal speed).
-The same run on the FP64 CPU oracle (oracle/orc_*.inc) is the reference; the
-relative L2 errors of velocity, density (deviation from 1), wall shear stress
-and membrane-node displacement after the run are bounded per storage form at
-about 10x what was measured on a B200 (float atomics in the spreading make
-runs differ slightly; over 1000 coupled steps this moves the errors by up to
-a few times):
+"""Config C0 and the precision forms against the FP64 oracle: a bounce-back
+tube of radius 20 in a 48x48x128 box (periodic in z), tau 0.9, Guo force 1e-6
+along z, 8 nucleated RBCs (icosphere 642/1280 scaled to 7, 4.5, 2 lattice
+units; nucleus 162 nodes scaled to 2.5, 1.8, 1.2) placed from seed 1234, the
+tube's wall mesh, 1000 steps of the reference loop from rest (membrane/IB
+block every 50 steps).  The FP64 CPU oracle (oracle/orc_*.inc) runs the same
+loop; the relative L2 errors of velocity, density (deviation from 1), wall
+shear stress and membrane-node displacement are bounded per storage form.
+BOUNDS holds about 10x what was measured on a B200 (float atomics in the
+spreading make runs differ slightly):
 
   storage            u        rho-1    WSS      displacement   (measured)
-  fp32 (plain)       5.1e-5   5.5e-1   6.9e-5   2.7e-5
-  fp32 deviation     3.2e-5   1.4e-3   2.8e-5   2.2e-5
-  fp16 dev. + SR     2.5e-4   9.0e-3   2.6e-4   4.3e-5
-  bf16 dev. + SR     1.5e-3   6.0e-2   6.4e-4   1.5e-4
+  fp32 (plain)       3.2e-4   1.6      4.0e-4   3.5e-4
+  fp32 deviation     8.1e-4   1.1e-2   4.1e-4   5.4e-4
+  fp16 dev. + SR     5.0e-4   9.9e-3   3.6e-4   5.9e-4
+  bf16 dev. + SR     2.1e-3   5.1e-2   1.1e-3   1.1e-3
+
+At this force the flow is slow (u_max ~ 7.5e-4) and the cells' forcing is a
+comparable signal, so the fp32 arithmetic of the membrane and IB path, not
+the population storage, sets the error of every form; the storage effect
+alone is measured on Poiseuille flow in test_lbm_gpu.py.
 
 Plain fp32 populations cannot resolve the density deviation of this flow
-(1 - rho ~ 1e-6, near the fp32 spacing of populations ~0.05); the deviation
+(rho - 1 is close to the fp32 spacing of populations of ~0.05); the deviation
 forms store f/w - rho_ref and keep it.
 """
 import numpy as np
@@ -27,11 +32,11 @@ from oracle.bind import OracleCells, OracleLBM, OracleWorld
 
 pytestmark = pytest.mark.gpu
 
-NX, NY, NZ, R = 40, 40, 48, 16.0
-CX = CY = 19.5
-NSTEPS, STAGGER = 1000, 10
-BOUNDS = {zf.STORE_F32: (5e-4, 1.0, 7e-4, 3e-4), zf.STORE_F32_DEV: (4e-4, 1.5e-2, 4e-4, 3e-4),
-          zf.STORE_F16: (2.5e-3, 9e-2, 2.5e-3, 5e-4), zf.STORE_BF16: (1.5e-2, 0.6, 6e-3, 1.5e-3)}
+NX, NY, NZ, R = 48, 48, 128, 20.0
+CX = CY = 23.5
+NSTEPS, STAGGER = 1000, 50
+BOUNDS = {zf.STORE_F32: (3e-3, 5.0, 4e-3, 3.5e-3), zf.STORE_F32_DEV: (8e-3, 0.11, 4e-3, 5e-3),
+          zf.STORE_F16: (5e-3, 0.1, 3.6e-3, 6e-3), zf.STORE_BF16: (2e-2, 0.5, 1.1e-2, 1.1e-2)}
 
 
 def case():
@@ -41,14 +46,14 @@ def case():
     rest = xyz * np.array([3.5, 2.25, 1.0])
     rest_n = xyzn * np.array([1.25, 0.9, 0.6])
     mesh = (rest, tri, rest_n, zf.mesh_edges(trin))
-    cells = zf.gen_cells(b, 4, rest, rest_n, (3.5, 2.25, 1.0), seed=21, margin=0.4)
+    cells = zf.gen_cells(b, 8, rest, rest_n, (3.5, 2.25, 1.0), seed=1234, margin=0.4)
     wall = zf.gen_wall_tube(CX, CY, R, NZ)
     return b, mesh, cells, wall
 
 
 def params(storage):
     return zf.default_params(nx=NX, ny=NY, nz=NZ, tau=0.9, tau_from_phase=0,
-                             wall_mode=zf.WALL_HALFWAY_BB, periodic=(0, 0, 1), g=(0, 0, 5e-6),
+                             wall_mode=zf.WALL_HALFWAY_BB, periodic=(0, 0, 1), g=(0, 0, 1e-6),
                              origin=(0.0, 0.0, 0.0), area0=0.0, volume0=0.0, stagger=STAGGER,
                              storage=storage)
 

@@ -339,23 +339,34 @@ static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
     int rc = ib_prepare(c);
     if (rc) return rc;
   }
+  // LBM profiling: one event pair around each run of consecutive plain LBM
+  // steps (events around single launches would also time the host's enqueue)
+  auto close_run = [&]() -> int {
+    if (!c->prof_open) return ZF_OK;
+    ZF_CUDA(cudaEventRecord(c->prof_ev[2 * c->prof_lbm + 1], c->stream));
+    c->prof_run_n.push_back(c->prof_open_n);
+    c->prof_lbm++;
+    c->prof_open = false;
+    return ZF_OK;
+  };
   for (int s = 0; s < nsteps; ++s) {
     const int64_t iter = c->status.iter + 1;
     const bool membrane = cells && (iter % c->p.stagger == 0);  // RBCSOLVERFLAG, :5650-5652
     const bool last = s == nsteps - 1;
     int rc;
+    if (membrane && (rc = close_run())) return rc;
     const bool pm = c->profiling && membrane && c->prof_mem < c->prof_cap;
     if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (c->prof_cap + c->prof_mem)], c->stream));
     if (membrane && (rc = cells_membrane_launch(c))) return rc;
     if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (c->prof_cap + c->prof_mem) + 1], c->stream));
-    const bool pl = c->profiling && c->prof_lbm < c->prof_cap;
-    if (pl) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * c->prof_lbm], c->stream));
+    if (!membrane && c->profiling && !c->prof_open && c->prof_lbm < c->prof_cap) {
+      ZF_CUDA(cudaEventRecord(c->prof_ev[2 * c->prof_lbm], c->stream));
+      c->prof_open = true;
+      c->prof_open_n = 0;
+    }
     if ((rc = lbm_launch(c, membrane, membrane, (last && mass_last) ? mass_last : nullptr)))
       return rc;
-    if (pl) {
-      ZF_CUDA(cudaEventRecord(c->prof_ev[2 * c->prof_lbm + 1], c->stream));
-      c->prof_lbm++;
-    }
+    if (c->prof_open) c->prof_open_n++;
     if (membrane) {
       if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (2 * c->prof_cap + c->prof_mem)], c->stream));
       const bool rebuild = !c->nuc_lists_valid || (iter % c->p.nuc_list_period == 0);
@@ -370,11 +381,10 @@ static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
         ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (2 * c->prof_cap + c->prof_mem) + 1], c->stream));
         c->prof_mem++;
       }
-
     }
     c->status.iter = iter;
   }
-  return ZF_OK;
+  return close_run();
 }
 
 int zf_step(zf_ctx* c, int nsteps) { return step_impl(c, nsteps, nullptr); }
@@ -397,6 +407,8 @@ int zf_profile(zf_ctx* c, int enable, int capacity) {
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   c->prof_ev.clear();
   c->prof_cap = c->prof_lbm = c->prof_mem = 0;
+  c->prof_open = false;
+  c->prof_run_n.clear();
   c->profiling = enable != 0;
   if (!enable) return ZF_OK;
   c->prof_cap = capacity > 0 ? capacity : 4096;
@@ -410,7 +422,9 @@ int zf_profile_read(zf_ctx* c, float* lbm_ms, int* lbm_count, float* membrane_ms
   if (!c) return ZF_ERR_ARG;
   ZF_CUDA(cudaStreamSynchronize(c->stream));
   float tl = 0.f, tm = 0.f;
+  int runs_n = 0;
   for (int i = 0; i < c->prof_lbm; ++i) {
+    runs_n += c->prof_run_n[i];
     float ms = 0.f;
     ZF_CUDA(cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]));
     tl += ms;
@@ -423,7 +437,7 @@ int zf_profile_read(zf_ctx* c, float* lbm_ms, int* lbm_count, float* membrane_ms
     tm += a + b;
   }
   if (lbm_ms) *lbm_ms = tl;
-  if (lbm_count) *lbm_count = c->prof_lbm;
+  if (lbm_count) *lbm_count = runs_n;
   if (membrane_ms) *membrane_ms = tm;
   if (membrane_count) *membrane_count = c->prof_mem;
   return ZF_OK;

@@ -277,7 +277,10 @@ struct zf_ctx {
   int64_t launches = 0;
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;  // [2*cap]: LBM pairs then membrane pairs
-  int prof_cap = 0, prof_lbm = 0, prof_mem = 0;
+  int prof_cap = 0, prof_lbm = 0, prof_mem = 0;  // event pairs: LBM runs, membrane blocks
+  bool prof_open = false;                          // an LBM run is being timed
+  int prof_open_n = 0;                             // its launches so far
+  std::vector<int> prof_run_n;                     // launches of each timed LBM run
 };
 
 namespace zf {
