@@ -445,7 +445,11 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
-    stream = torch.cuda.current_stream(dev)
+    # a stream of our own: the context's kernels and the timing events must be
+    # on the same stream (torch's default stream has handle 0, which the C ABI
+    # reads as "the context's own stream")
+    stream = torch.cuda.Stream(device=dev)
+    assert stream.cuda_stream != 0
 
     def barrier():
         if world > 1:

@@ -526,6 +526,9 @@ class Context:
         return lm.value, lc.value, mm.value, mc.value
 
     def set_stream(self, stream_handle):
+        """Queue the context's work on a CUDA stream (a cudaStream_t as int);
+        None or 0 selects the context's own stream (so the legacy default
+        stream cannot be chosen: pass a created stream)."""
         _check(lib().zf_set_stream(self._h, C.c_void_p(stream_handle) if stream_handle else None))
 
     def device_bytes(self) -> int:

@@ -908,7 +908,7 @@ __device__ __forceinline__ int neighbour_tile(const IbArgs& a, int tx, int ty, i
 // own triangle) and one whose sub-centroids can reach 1 um queues up; queued
 // triangles are evaluated 32 at a time, one per lane.  Lane sums meet in a
 // fixed butterfly, so the result is deterministic.
-__global__ void __launch_bounds__(kTileThreads) k_rbc_tiles(IbArgs a, CellArgs c) {
+__global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArgs c) {
   __shared__ int s_q[kTileWarps][64];
   const unsigned FULL = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

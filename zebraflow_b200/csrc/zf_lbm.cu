@@ -25,6 +25,7 @@
 #include <cuda_fp16.h>
 
 #include <mutex>
+#include <type_traits>
 
 #include "zf_internal.h"
 
@@ -50,6 +51,19 @@ __host__ __device__ constexpr float WQ(int q) {
 }
 __host__ __device__ constexpr float IWQ(int q) { return q < 6 ? 18.f : (q < 18 ? 36.f : 3.f); }
 __host__ __device__ constexpr int OPP(int q) { return q == 18 ? 18 : (q ^ 1); }
+
+// c_q . (x, y, z) from the nonzero components of c_q only (q is a constant
+// after unrolling, so this folds to at most one add; 0*x would not fold)
+__device__ __forceinline__ float cdot(int q, float x, float y, float z) {
+  const float tx = EX(q) > 0 ? x : -x, ty = EY(q) > 0 ? y : -y, tz = EZ(q) > 0 ? z : -z;
+  if (EX(q)) {
+    if (EY(q)) return tx + ty;
+    if (EZ(q)) return tx + tz;
+    return tx;
+  }
+  if (EY(q)) return EZ(q) ? ty + tz : ty;
+  return EZ(q) ? tz : 0.f;
+}
 
 // ---- storage codecs: decode to / encode from the deviation d = f/w - rho_ref
 struct RawF32 {  // plain populations, as the reference keeps F
@@ -104,18 +118,16 @@ constexpr int kTilesPerBlock = 4;
 template <class C, typename I>
 __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
   using T = typename C::T;
-  __shared__ I s_base[kTilesPerBlock][27];  // neighbour tile id * 64
+  // each thread reads the pull bases it needs from its tile's row of the
+  // 27-neighbour table (L1-resident, shared by the tile's 64 threads): no
+  // block-wide staging and no barrier before the populations are loaded
   const int lt = threadIdx.x >> 6, cell = threadIdx.x & 63;
-  const int tb = blockIdx.x * kTilesPerBlock;
-  for (int t = threadIdx.x; t < kTilesPerBlock * 27; t += blockDim.x) {
-    const int l = t / 27, s = t - l * 27;
-    int nb = -1;
-    if (tb + l < a.n_active) nb = a.nbr[(int64_t)a.active[tb + l] * 27 + s];
-    s_base[l][s] = nb >= 0 ? (I)nb * ZF_TC : (I)0;
-  }
-  __syncthreads();
-  bool live = tb + lt < a.n_active;
-  const I self = live ? s_base[lt][13] + (I)cell : (I)0;
+  const int ti = blockIdx.x * kTilesPerBlock + lt;
+  bool live = ti < a.n_active;
+  const int tile = live ? a.active[ti] : 0;
+  const int32_t* __restrict__ nbt = a.nbr + (int64_t)tile * 27;
+  const I tbase = (I)tile * ZF_TC;
+  const I self = tbase + (I)cell;
   const uint32_t link = live ? a.link[self] : 0u;
   live = live && (link >> 31);
   float rho = 0.f;
@@ -137,7 +149,9 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
         const int sx = x - EX(q), sy = y - EY(q), sz = z - EZ(q);
         const int s27 = ((sz >> 2) + 1) * 9 + ((sy >> 2) + 1) * 3 + ((sx >> 2) + 1);
         const int scell = (sx & 3) | ((sy & 3) << 2) | ((sz & 3) << 4);
-        const I src = (I)q * ns + s_base[lt][s27] + (I)scell;
+        // a missing neighbour only occurs on a bounce-back link (pull unused)
+        const I nbase = s27 == 13 ? tbase : (I)max(__ldg(nbt + s27), 0) * ZF_TC;
+        const I src = (I)q * ns + nbase + (I)scell;
         const I bb = (I)OPP(q) * ns + self;
         idx = ((link >> q) & 1u) ? bb : src;
       }
@@ -180,18 +194,33 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
     const float sfac = 1.f - 0.5f * omega;
 
     // BGK + Guo source in deviation form, ZebraflowWT.c:6138-6142:
-    // d' = d + omega (deq - d) + src/w,  deq = drho + rho (3cu + 4.5cu^2 - 1.5u^2)
+    // d' = d + omega (deq - d) + src/w,  deq = drho + rho (3cu + 4.5cu^2 - 1.5u^2),
+    // src/w = sfac (3 (cF - uF) + 9 cu cF); per point constants A, K1..K5 turn
+    // deq into two FMAs and the source into two, and d' keeps its form
+    // d + omega (deq - d) + src, which rounds only the non-equilibrium part
+    const float A = drho - rho * usq15;
+    const float K1 = 3.f * rho, K2 = 4.5f * rho, K3 = 9.f * sfac, K4 = 3.f * sfac, K5 = 3.f * sfac * uF;
     float r2 = 0.f, m2x = 0.f, m2y = 0.f, m2z = 0.f;
     uint32_t rseed = 0;
     if (IsHalf<C>::v) rseed = mix32((uint32_t)self * 0x9E3779B1u + a.step * 0x85EBCA77u);
     float dn_prev = 0.f;
 #pragma unroll
     for (int q = 0; q < ZF_Q; ++q) {
-      const float cu = EX(q) * ux + EY(q) * uy + EZ(q) * uz;
-      const float cF = EX(q) * Fx + EY(q) * Fy + EZ(q) * Fz;
-      const float deq = drho + rho * (3.f * cu + 4.5f * cu * cu - usq15);
-      const float src = sfac * (3.f * (cF - uF) + 9.f * cu * cF);
-      const float dn = d[q] + omega * (deq - d[q]) + src;
+      float dn;
+      if constexpr (std::is_same<C, RawF32>::value) {
+        // plain populations: the reference's expression as written
+        const float cu = cdot(q, ux, uy, uz), cF = cdot(q, Fx, Fy, Fz);
+        const float deq = drho + rho * (3.f * cu + 4.5f * cu * cu - usq15);
+        const float src = sfac * (3.f * (cF - uF) + 9.f * cu * cF);
+        dn = d[q] + omega * (deq - d[q]) + src;
+      } else if (q == 18) {
+        dn = fmaf(omega, A - d[q], d[q]) - K5;
+      } else {
+        const float cu = cdot(q, ux, uy, uz), cF = cdot(q, Fx, Fy, Fz);
+        const float deq = fmaf(cu, fmaf(K2, cu, K1), A);
+        const float src = fmaf(K3 * cu, cF, fmaf(K4, cF, -K5));
+        dn = fmaf(omega, deq - d[q], d[q]) + src;
+      }
       float ds;  // the value the storage keeps
       if constexpr (IsHalf<C>::v) {
         if (a.stochastic && q < 18) {
