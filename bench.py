@@ -154,6 +154,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(vals, device):
+    """Element-wise maximum of a list of floats over all ranks (timings are
+    reported as the slowest rank's)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(vals, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -469,11 +479,7 @@ def run_ours(args):
 
     # max over ranks of every timed figure
     def vmax(vals):
-        if world == 1:
-            return vals
-        t = torch.tensor(vals, dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return [float(x) for x in t]
+        return max_over_ranks(vals, f"cuda:{dev}") if world > 1 else vals
 
     for r in [main_r] + [v[1] for v in variants.values()]:
         r["ms"], r["ms_e2e"], r["ms_prof"], r["lbm_ms"], r["mem_ms"] = vmax(
