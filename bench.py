@@ -394,7 +394,7 @@ def summarize(case, storage, r, steps, world, peak):
     return out
 
 
-def measure_adjoint(dev, stream, barrier, seed=2024):
+def measure_adjoint(dev, stream, barrier, seed=2024, nsteps=500, t0=300, t1=500, K=50):
     """Cost of the hand-written adjoint on the C3 tube (96x96x512, R = 40,
     200 RBCs held at slightly deformed positions): J = mean |WSS| over a
     64-lattice-unit wall patch across steps 300..500, gradients for the
@@ -423,7 +423,6 @@ def measure_adjoint(dev, stream, barrier, seed=2024):
     ctx.set_mesh(rest, tri, rest_n, zf.mesh_edges(trin))
     ctx.set_cells(x, xn)
     ctx.set_stream(stream.cuda_stream)
-    nsteps, t0, t1, K = 500, 300, 500, 50
     ctx.wss_objective(nsteps, t0, t1, patch)  # warm-up
     barrier()
     t = time.perf_counter()

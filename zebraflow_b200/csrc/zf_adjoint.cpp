@@ -46,10 +46,20 @@ struct DevBuf {
 };
 
 struct Setup {
+  zf_ctx* c = nullptr;
   size_t pop_bytes = 0;        // one population state
   double weight = 0.0;         // 1 / (window length x patch size)
   DevBuf nrm, patch, acc;      // normals [3][nw], patch ids, FP64 accumulator
+  DevBuf U;                    // velocities at the stencils' compact points [3][nu]
+  PatchStencil ps;             // the patch's WSS stencils
+  std::vector<std::pair<void*, size_t>> ps_bufs;
   std::vector<float> bf_save;  // BODYFORCE at entry (listed order)
+  ~Setup() {
+    for (auto& b : ps_bufs) {
+      cudaFree(b.first);
+      c->device_bytes -= (int64_t)b.second;
+    }
+  }
 };
 
 int check_args(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, int n_patch) {
@@ -78,6 +88,7 @@ int check_args(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, int 
 int setup(zf_ctx* c, int t0, int t1, const int32_t* patch, int n_patch, const float* normals,
           const float* fb, Setup& S) {
   const size_t esz = c->p.storage == ZF_STORE_F32 || c->p.storage == ZF_STORE_F32_DEV ? 4 : 2;
+  S.c = c;
   S.pop_bytes = (size_t)ZF_Q * c->ns * esz;
   S.weight = 1.0 / ((double)(t1 - t0 + 1) * n_patch);
   const size_t nw = (size_t)c->ib.nw, nl = (size_t)c->n_listed;
@@ -89,6 +100,9 @@ int setup(zf_ctx* c, int t0, int t1, const int32_t* patch, int n_patch, const fl
                           normals ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c->stream));
   ZF_CUDA(cudaMemcpyAsync(S.patch.p, patch, (size_t)n_patch * sizeof(int32_t), cudaMemcpyHostToDevice,
                           c->stream));
+  if ((rc = wss_patch_stencil(c, (const float*)S.nrm.p, (const int32_t*)S.patch.p, n_patch, S.ps, S.ps_bufs)))
+    return rc;
+  if ((rc = S.U.alloc(c, 3 * (size_t)std::max(S.ps.nu, 1) * sizeof(float)))) return rc;
   S.bf_save.resize(3 * nl);
   if ((rc = lbm_gather_listed(c, c->d_force, 3, S.bf_save.data()))) return rc;
   ZF_CUDA(cudaMemsetAsync(c->d_force, 0, 3 * c->ns * sizeof(float), c->stream));
@@ -106,19 +120,20 @@ int setup(zf_ctx* c, int t0, int t1, const int32_t* patch, int n_patch, const fl
   return ZF_OK;
 }
 
+// BODYFORCE back as it was, and the moment planes of the context's populations
 int restore(zf_ctx* c, Setup& S) {
   int rc = lbm_scatter_listed(c, S.bf_save.data(), 3, c->d_force);
   if (rc) return rc;
+  if ((rc = lbm_moments_launch(c))) return rc;
   ZF_CUDA(cudaStreamSynchronize(c->stream));
   return ZF_OK;
 }
 
 // J of the state f (adds into S.acc)
-int objective_of(zf_ctx* c, const void* f, int n_patch, Setup& S) {
-  int rc = lbm_moments_of(c, f);
+int objective_of(zf_ctx* c, const void* f, Setup& S) {
+  int rc = lbm_moments_at(c, f, S.ps, (float*)S.U.p);
   if (rc) return rc;
-  return wss_patch_launch(c, (const float*)S.nrm.p, (const int32_t*)S.patch.p, n_patch, S.weight,
-                          (double*)S.acc.p);
+  return wss_patch_launch(c, S.ps, (const float*)S.nrm.p, (const float*)S.U.p, S.weight, (double*)S.acc.p);
 }
 
 }  // namespace
@@ -142,7 +157,7 @@ int zf_wss_objective(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch
   for (int t = 1; t <= nsteps; ++t) {
     if ((rc = lbm_step_buffers(c, fin, fout))) return rc;
     std::swap(fin, fout);
-    if (t >= t0 && t <= t1 && (rc = objective_of(c, fin, n_patch, S))) return rc;
+    if (t >= t0 && t <= t1 && (rc = objective_of(c, fin, S))) return rc;
   }
   ZF_CUDA(cudaMemcpyAsync(J, S.acc.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   return restore(c, S);
@@ -166,7 +181,8 @@ int zf_wss_adjoint(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, 
   if ((rc = seg.alloc(c, (size_t)(K + 1) * PB))) return rc;
   const size_t fl = (size_t)ZF_Q * c->ns * sizeof(float);
   if ((rc = lam.alloc(c, fl)) || (rc = lam2.alloc(c, fl))) return rc;
-  if ((rc = gF.alloc(c, 3 * c->ns * sizeof(float))) || (rc = gU.alloc(c, 3 * c->ns * sizeof(float))))
+  if ((rc = gF.alloc(c, 3 * c->ns * sizeof(float))) ||
+      (rc = gU.alloc(c, 3 * (size_t)std::max(S.ps.nu, 1) * sizeof(float))))
     return rc;
   const int nb = lbm_adj_blocks(c);
   if ((rc = gw.alloc(c, (size_t)std::max(nb, 1) * sizeof(double)))) return rc;
@@ -182,7 +198,7 @@ int zf_wss_adjoint(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, 
     for (int t = 1; t <= nsteps; ++t) {
       if ((rc = lbm_step_buffers(c, fin, fout))) return rc;
       std::swap(fin, fout);
-      if (t >= t0 && t <= t1 && (rc = objective_of(c, fin, n_patch, S))) return rc;
+      if (t >= t0 && t <= t1 && (rc = objective_of(c, fin, S))) return rc;
       if (t % K == 0 && t / K < nseg)
         ZF_CUDA(cudaMemcpyAsync(CK + (size_t)(t / K) * PB, fin, PB, cudaMemcpyDeviceToDevice, c->stream));
     }
@@ -192,6 +208,7 @@ int zf_wss_adjoint(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, 
   ZF_CUDA(cudaMemsetAsync(lam.p, 0, fl, c->stream));
   ZF_CUDA(cudaMemsetAsync(lam2.p, 0, fl, c->stream));
   ZF_CUDA(cudaMemsetAsync(gF.p, 0, 3 * c->ns * sizeof(float), c->stream));
+  ZF_CUDA(cudaMemsetAsync(gU.p, 0, gU.bytes, c->stream));  // k_seed_at clears it after each use
   ZF_CUDA(cudaMemsetAsync(gw.p, 0, (size_t)std::max(nb, 1) * sizeof(double), c->stream));
   float* L = (float*)lam.p;
   float* Lp = (float*)lam2.p;
@@ -205,12 +222,11 @@ int zf_wss_adjoint(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, 
       const int t = base + i;
       const char* ft = SG + (size_t)i * PB;
       if (t >= t0 && t <= t1) {  // dJ_t/df_t
-        if ((rc = lbm_moments_of(c, ft))) return rc;
-        ZF_CUDA(cudaMemsetAsync(gU.p, 0, 3 * c->ns * sizeof(float), c->stream));
-        if ((rc = wss_patch_adj_launch(c, (const float*)S.nrm.p, (const int32_t*)S.patch.p, n_patch,
-                                       S.weight, (float*)gU.p)))
+        if ((rc = lbm_moments_at(c, ft, S.ps, (float*)S.U.p))) return rc;
+        if ((rc = wss_patch_adj_launch(c, S.ps, (const float*)S.nrm.p, (const float*)S.U.p, S.weight,
+                                       (float*)gU.p)))
           return rc;
-        if ((rc = lbm_seed_launch(c, ft, (const float*)gU.p, L))) return rc;
+        if ((rc = lbm_seed_at(c, ft, S.ps, (float*)gU.p, L))) return rc;
       }
       if ((rc = lbm_adj_launch(c, SG + (size_t)(i - 1) * PB, L, Lp, (float*)gF.p, (double*)gw.p)))
         return rc;

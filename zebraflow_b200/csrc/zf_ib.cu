@@ -20,6 +20,8 @@
 // weights are fp32 on fp32 copies of the positions, as the reference's float
 // locals.  Sums of distances that pick a nearest triangle use non-contracted
 // fp32 operations so that ties resolve as on the CPU.
+#include <algorithm>
+
 #include "zf_internal.h"
 
 namespace zf {
@@ -1484,22 +1486,62 @@ __global__ void k_wss(IbArgs a, const float* __restrict__ nrm, float pgauge, flo
 // ---- adjoint pieces of a WSS objective -------------------------------------------
 //
 // J = c sum_{m in patch} |WSS_m| for one state (c = 1 / (window length x patch
-// size)); k_wss_patch adds J to *acc (FP64), k_wss_patch_adj scatters dJ/dU
-// (U the moments interpolated at the probes) into gU[3][ns]:
+// size)).  The patch's stencils (slot, Peskin weight, in the order of
+// wss_stencil) depend on the geometry only, so they are listed once per call:
+// entry e of node i (off[i] <= e < off[i+1]) has weight w[e] and reads the
+// velocity of compact point idx[e]; the compact points are the distinct slots
+// of all stencils, whose velocities each step computes from the populations
+// (k_moments_at).  Per step the objective is then a short sparse sum per node,
+// and its adjoint the transposed sum:
 //   WSS = k (v - (v.n) n), k = -0.0012 / (DX 1e-6)  =>  dJ/dv = c k P_n WSS/|WSS|.
-__global__ void k_wss_patch(IbArgs a, const float* __restrict__ nrm, const int32_t* __restrict__ patch,
-                            int np, double c, double* acc) {
+__global__ void k_wss_stencil_count(IbArgs a, const float* __restrict__ nrm, const int32_t* __restrict__ patch,
+                                    int np, int32_t* __restrict__ cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int m = patch[i];
+  int n = 0;
+  wss_stencil(a, a.wxyz[m], a.wxyz[a.nw + m], a.wxyz[2 * a.nw + m], nrm[m], nrm[a.nw + m], nrm[2 * a.nw + m],
+              [&](int64_t, float) { ++n; });
+  cnt[i] = n;
+}
+
+__global__ void k_wss_stencil_fill(IbArgs a, const float* __restrict__ nrm, const int32_t* __restrict__ patch,
+                                   int np, const int32_t* __restrict__ off, int32_t* __restrict__ slot,
+                                   float* __restrict__ w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const int m = patch[i];
+  int e = off[i];
+  wss_stencil(a, a.wxyz[m], a.wxyz[a.nw + m], a.wxyz[2 * a.nw + m], nrm[m], nrm[a.nw + m], nrm[2 * a.nw + m],
+              [&](int64_t s, float wt) {
+                slot[e] = (int32_t)s;
+                w[e] = wt;
+                ++e;
+              });
+}
+
+// the probe velocity of patch node i from the compact velocities U[3][nu]
+__device__ __forceinline__ void patch_probe(const PatchStencil& ps, const float* __restrict__ U, int i,
+                                            float& UU, float& VV, float& WW) {
+  UU = VV = WW = 0.f;
+  for (int e = ps.off[i]; e < ps.off[i + 1]; ++e) {
+    const int u = ps.idx[e];
+    const float w = ps.w[e];
+    UU += w * U[u];
+    VV += w * U[ps.nu + u];
+    WW += w * U[2 * ps.nu + u];
+  }
+}
+
+__global__ void k_wss_patch(IbArgs a, PatchStencil ps, const float* __restrict__ nrm,
+                            const float* __restrict__ U, double c, double* acc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v = 0.0;
-  if (i < np) {
-    const int m = patch[i];
+  if (i < ps.np) {
+    const int m = ps.patch[i];
     const float n0 = nrm[m], n1 = nrm[a.nw + m], n2 = nrm[2 * a.nw + m];
-    float UU = 0.f, VV = 0.f, WW = 0.f;
-    wss_stencil(a, a.wxyz[m], a.wxyz[a.nw + m], a.wxyz[2 * a.nw + m], n0, n1, n2, [&](int64_t s, float w) {
-      UU += w * a.mom[a.ns + s];
-      VV += w * a.mom[2 * a.ns + s];
-      WW += w * a.mom[3 * a.ns + s];
-    });
+    float UU, VV, WW;
+    patch_probe(ps, U, i, UU, VV, WW);
     float W0, W1, W2;
     wss_of(a, UU, VV, WW, n0, n1, n2, W0, W1, W2);
     v = c * sqrt((double)W0 * W0 + (double)W1 * W1 + (double)W2 * W2);
@@ -1509,19 +1551,15 @@ __global__ void k_wss_patch(IbArgs a, const float* __restrict__ nrm, const int32
   if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(acc, v);
 }
 
-__global__ void k_wss_patch_adj(IbArgs a, const float* __restrict__ nrm, const int32_t* __restrict__ patch,
-                                int np, double c, float* __restrict__ gU) {
+// gU[3][nu] += dJ/dU at the compact points
+__global__ void k_wss_patch_adj(IbArgs a, PatchStencil ps, const float* __restrict__ nrm,
+                                const float* __restrict__ U, double c, float* __restrict__ gU) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= np) return;
-  const int m = patch[i];
+  if (i >= ps.np) return;
+  const int m = ps.patch[i];
   const float n0 = nrm[m], n1 = nrm[a.nw + m], n2 = nrm[2 * a.nw + m];
-  const float xm = a.wxyz[m], ym = a.wxyz[a.nw + m], zm = a.wxyz[2 * a.nw + m];
-  float UU = 0.f, VV = 0.f, WW = 0.f;
-  wss_stencil(a, xm, ym, zm, n0, n1, n2, [&](int64_t s, float w) {
-    UU += w * a.mom[a.ns + s];
-    VV += w * a.mom[2 * a.ns + s];
-    WW += w * a.mom[3 * a.ns + s];
-  });
+  float UU, VV, WW;
+  patch_probe(ps, U, i, UU, VV, WW);
   float W0, W1, W2;
   wss_of(a, UU, VV, WW, n0, n1, n2, W0, W1, W2);
   const double mag = sqrt((double)W0 * W0 + (double)W1 * W1 + (double)W2 * W2);
@@ -1531,11 +1569,13 @@ __global__ void k_wss_patch_adj(IbArgs a, const float* __restrict__ nrm, const i
   const double hn = h0 * n0 + h1 * n1 + h2 * n2;
   const float g0 = (float)(c * k * (h0 - hn * n0)), g1 = (float)(c * k * (h1 - hn * n1)),
               g2 = (float)(c * k * (h2 - hn * n2));
-  wss_stencil(a, xm, ym, zm, n0, n1, n2, [&](int64_t s, float w) {
-    atomicAdd(&gU[s], w * g0);
-    atomicAdd(&gU[a.ns + s], w * g1);
-    atomicAdd(&gU[2 * a.ns + s], w * g2);
-  });
+  for (int e = ps.off[i]; e < ps.off[i + 1]; ++e) {
+    const int u = ps.idx[e];
+    const float w = ps.w[e];
+    atomicAdd(&gU[u], w * g0);
+    atomicAdd(&gU[ps.nu + u], w * g1);
+    atomicAdd(&gU[2 * ps.nu + u], w * g2);
+  }
 }
 
 // transpose of the spreading (k_ib_spread without the repulsion term): for
@@ -1615,18 +1655,79 @@ int wss_launch(zf_ctx* ctx, const float* d_normals, double pgauge, float* d_wss,
   return ZF_OK;
 }
 
-int wss_patch_launch(zf_ctx* ctx, const float* d_nrm, const int32_t* d_patch, int np, double c, double* d_acc) {
+// Lists the patch's stencils (see k_wss_stencil_count); device buffers and
+// their sizes are appended to `bufs` (the caller frees them).
+int wss_patch_stencil(zf_ctx* ctx, const float* d_nrm, const int32_t* d_patch, int np, PatchStencil& ps,
+                      std::vector<std::pair<void*, size_t>>& bufs) {
+  ps = PatchStencil{};
+  ps.np = np;
+  ps.patch = d_patch;
   if (np <= 0) return ZF_OK;
-  k_wss_patch<<<(np + 127) / 128, 128, 0, ctx->stream>>>(ctx->ib, d_nrm, d_patch, np, c, d_acc);
+  auto grab = [&](void** p, size_t b) -> int {
+    b = b < 4 ? 4 : b;
+    int r = dev_alloc(ctx, p, b);
+    if (!r) bufs.emplace_back(*p, b);
+    return r;
+  };
+  int32_t* d_cnt = nullptr;
+  int rc = grab((void**)&d_cnt, (size_t)np * sizeof(int32_t));
+  if (rc) return rc;
+  k_wss_stencil_count<<<(np + 127) / 128, 128, 0, ctx->stream>>>(ctx->ib, d_nrm, d_patch, np, d_cnt);
+  ZF_CUDA(cudaGetLastError());
+  std::vector<int32_t> off(np + 1, 0);
+  ZF_CUDA(cudaMemcpyAsync(off.data() + 1, d_cnt, (size_t)np * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  ZF_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < np; ++i) off[i + 1] += off[i];
+  const int ne = off[np];
+  int32_t *d_off = nullptr, *d_slot = nullptr, *d_idx = nullptr, *d_us = nullptr;
+  float* d_w = nullptr;
+  if ((rc = grab((void**)&d_off, (size_t)(np + 1) * sizeof(int32_t))) ||
+      (rc = grab((void**)&d_slot, (size_t)ne * sizeof(int32_t))) ||
+      (rc = grab((void**)&d_w, (size_t)ne * sizeof(float))))
+    return rc;
+  ZF_CUDA(cudaMemcpyAsync(d_off, off.data(), (size_t)(np + 1) * sizeof(int32_t), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  k_wss_stencil_fill<<<(np + 127) / 128, 128, 0, ctx->stream>>>(ctx->ib, d_nrm, d_patch, np, d_off, d_slot, d_w);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 2;
+  // distinct slots, and each entry's index among them
+  std::vector<int32_t> slot(ne), us, idx(ne);
+  ZF_CUDA(cudaMemcpyAsync(slot.data(), d_slot, (size_t)ne * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  ZF_CUDA(cudaStreamSynchronize(ctx->stream));
+  us = slot;
+  std::sort(us.begin(), us.end());
+  us.erase(std::unique(us.begin(), us.end()), us.end());
+  for (int e = 0; e < ne; ++e) idx[e] = (int32_t)(std::lower_bound(us.begin(), us.end(), slot[e]) - us.begin());
+  const int nu = (int)us.size();
+  if ((rc = grab((void**)&d_idx, (size_t)ne * sizeof(int32_t))) ||
+      (rc = grab((void**)&d_us, (size_t)nu * sizeof(int32_t))))
+    return rc;
+  ZF_CUDA(cudaMemcpyAsync(d_idx, idx.data(), (size_t)ne * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+  ZF_CUDA(cudaMemcpyAsync(d_us, us.data(), (size_t)nu * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream));
+  ZF_CUDA(cudaStreamSynchronize(ctx->stream));
+  ps.off = d_off;
+  ps.idx = d_idx;
+  ps.w = d_w;
+  ps.uslot = d_us;
+  ps.nu = nu;
+  return ZF_OK;
+}
+
+int wss_patch_launch(zf_ctx* ctx, const PatchStencil& ps, const float* d_nrm, const float* d_U, double c,
+                     double* d_acc) {
+  if (ps.np <= 0) return ZF_OK;
+  k_wss_patch<<<(ps.np + 127) / 128, 128, 0, ctx->stream>>>(ctx->ib, ps, d_nrm, d_U, c, d_acc);
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 1;
   return ZF_OK;
 }
 
-int wss_patch_adj_launch(zf_ctx* ctx, const float* d_nrm, const int32_t* d_patch, int np, double c,
+int wss_patch_adj_launch(zf_ctx* ctx, const PatchStencil& ps, const float* d_nrm, const float* d_U, double c,
                          float* d_gU) {
-  if (np <= 0) return ZF_OK;
-  k_wss_patch_adj<<<(np + 127) / 128, 128, 0, ctx->stream>>>(ctx->ib, d_nrm, d_patch, np, c, d_gU);
+  if (ps.np <= 0) return ZF_OK;
+  k_wss_patch_adj<<<(ps.np + 127) / 128, 128, 0, ctx->stream>>>(ctx->ib, ps, d_nrm, d_U, c, d_gU);
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 1;
   return ZF_OK;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/zf.h"
@@ -12,6 +13,13 @@
 // Tile geometry of the sparse lattice: 4x4x4 lattice points, x fastest.
 #define ZF_TS 4
 #define ZF_TC 64
+// Populations are stored tile-major, [tile][19][64]: the 19 planes of one
+// tile are contiguous (ZF_PT elements), so the offset of population q inside
+// a tile is the constant q*64.  Point slot s = tile*64 + cell.
+#define ZF_PT (19 * ZF_TC)
+__host__ __device__ __forceinline__ int64_t pop_at(int q, int64_t s) {
+  return (s >> 6) * ZF_PT + (int64_t)q * ZF_TC + (s & 63);
+}
 
 // Cell codes stored per tile slot (uint8).
 enum : uint8_t {
@@ -199,12 +207,28 @@ int lbm_moments_launch(zf_ctx* c);
 int lbm_adj_blocks(zf_ctx* c);
 int lbm_adj_launch(zf_ctx* c, const void* f_pre, const float* lam, float* lam_prev, float* gF,
                    double* gw_partial);
-int lbm_seed_launch(zf_ctx* c, const void* f, const float* gU, float* lam);
-int lbm_step_buffers(zf_ctx* c, const void* fin, void* fout);
-int lbm_moments_of(zf_ctx* c, const void* f);
-int wss_patch_launch(zf_ctx* c, const float* d_nrm, const int32_t* d_patch, int np, double w, double* d_acc);
-int wss_patch_adj_launch(zf_ctx* c, const float* d_nrm, const int32_t* d_patch, int np, double w,
+// Stencils of a WSS objective's patch nodes over compact points (the distinct
+// lattice slots the stencils read): node i owns entries off[i]..off[i+1]-1.
+struct PatchStencil {
+  int np = 0, nu = 0;
+  const int32_t* patch = nullptr;  // [np] wall-node ids
+  const int32_t* off = nullptr;    // [np+1]
+  const int32_t* idx = nullptr;    // [entries] compact point of each entry
+  const float* w = nullptr;        // [entries] Peskin weight
+  const int32_t* uslot = nullptr;  // [nu] slot of each compact point
+};
+int wss_patch_stencil(zf_ctx* c, const float* d_nrm, const int32_t* d_patch, int np, PatchStencil& ps,
+                      std::vector<std::pair<void*, size_t>>& bufs);
+int wss_patch_launch(zf_ctx* c, const PatchStencil& ps, const float* d_nrm, const float* d_U, double w,
+                     double* d_acc);
+int wss_patch_adj_launch(zf_ctx* c, const PatchStencil& ps, const float* d_nrm, const float* d_U, double w,
                          float* d_gU);
+// velocities U[3][nu] of the populations f at the compact points
+int lbm_moments_at(zf_ctx* c, const void* f, const PatchStencil& ps, float* d_U);
+// lam += seed of gU[3][nu] at the compact points (f: the state the objective
+// read); clears gU
+int lbm_seed_at(zf_ctx* c, const void* f, const PatchStencil& ps, float* d_gU, float* lam);
+int lbm_step_buffers(zf_ctx* c, const void* fin, void* fout);
 int spread_adj_launch(zf_ctx* c, const float* d_G, float* d_gmem, float* d_gnuc);
 int scale_springs_launch(zf_ctx* c, float s);
 int wss_launch(zf_ctx* c, const float* d_normals, double pgauge, float* d_wss, float* d_press,

@@ -81,11 +81,11 @@ struct DevF16 {
   __device__ static float dec(T v, int, const LbmArgs& a) { return __half2float(v) * a.inv_scale; }
   __device__ static T enc(float d, int, const LbmArgs& a) { return __float2half_rn(d * a.scale); }
   __device__ static T from_bits(unsigned short u) { return __ushort_as_half(u); }
-  // two values with stochastic rounding; lo -> low half, hi -> high half
-  __device__ static uint32_t enc2_sr(float lo, float hi, uint32_t rbits, const LbmArgs& a) {
-    uint32_t r;
-    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(hi * a.scale), "f"(lo * a.scale), "r"(rbits));
-    return r;
+  // values already in storage units (x 2^16): round to nearest, or a pair
+  // with stochastic rounding (lo -> low half, hi -> high half)
+  __device__ static T cvt_rn(float v) { return __float2half_rn(v); }
+  __device__ static void cvt2_sr(uint32_t& r, float lo, float hi, uint32_t rbits) {
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(hi), "f"(lo), "r"(rbits));
   }
 };
 struct DevBF16 {
@@ -93,10 +93,9 @@ struct DevBF16 {
   __device__ static float dec(T v, int, const LbmArgs& a) { return __bfloat162float(v) * a.inv_scale; }
   __device__ static T enc(float d, int, const LbmArgs& a) { return __float2bfloat16_rn(d * a.scale); }
   __device__ static T from_bits(unsigned short u) { return __ushort_as_bfloat16(u); }
-  __device__ static uint32_t enc2_sr(float lo, float hi, uint32_t rbits, const LbmArgs& a) {
-    uint32_t r;
-    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(hi * a.scale), "f"(lo * a.scale), "r"(rbits));
-    return r;
+  __device__ static T cvt_rn(float v) { return __float2bfloat16_rn(v); }
+  __device__ static void cvt2_sr(uint32_t& r, float lo, float hi, uint32_t rbits) {
+    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(r) : "f"(hi), "f"(lo), "r"(rbits));
   }
 };
 template <class C>
@@ -115,47 +114,89 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h) {
 
 constexpr int kTilesPerBlock = 4;
 
+// Pull sources of one point.  A pull along q reads x - e_q; it leaves the
+// point's tile only across the faces the point lies on, so a point needs at
+// most 7 tiles (its own, three across faces, three across edges: D3Q19 has no
+// corner directions).  The offsets below are those tiles' population bases,
+// each already shifted by the wrap of the cell coordinate (x - e_x wraps by
+// 4 across an x face, y by 16 cells, z by 64), so that the source of q is
+// base(crossing pattern) + q*64 - (e_x + 4 e_y + 16 e_z): a selection and a
+// constant per direction.  A missing neighbour tile (id -1) maps to tile 0;
+// it is only reached by links that bounce back.
+template <typename I>
+struct PullBases {
+  I b0, bx, by, bz, bxy, bxz, byz;
+  bool xlo, xhi, ylo, yhi, zlo, zhi;
+  __device__ __forceinline__ PullBases(const int32_t* __restrict__ nbr, int tile, int cell) {
+    const int x = cell & 3, y = (cell >> 2) & 3, z = cell >> 4;
+    xlo = x == 0; xhi = x == 3; ylo = y == 0; yhi = y == 3; zlo = z == 0; zhi = z == 3;
+    const int sx = xlo ? -1 : (int)xhi, sy = ylo ? -1 : (int)yhi, sz = zlo ? -1 : (int)zhi;
+    const int32_t* __restrict__ row = nbr + (int64_t)tile * 27 + 13;
+    auto nb = [&](int o) -> I { return (I)max(__ldg(row + o), 0) * (I)ZF_PT; };
+    b0 = (I)tile * (I)ZF_PT + (I)cell;
+    bx = nb(sx) + (I)(cell - 4 * sx);
+    by = nb(3 * sy) + (I)(cell - 16 * sy);
+    bz = nb(9 * sz) + (I)(cell - 64 * sz);
+    bxy = nb(sx + 3 * sy) + (I)(cell - 4 * sx - 16 * sy);
+    bxz = nb(sx + 9 * sz) + (I)(cell - 4 * sx - 64 * sz);
+    byz = nb(3 * sy + 9 * sz) + (I)(cell - 16 * sy - 64 * sz);
+  }
+  // source of the pull along q (q < 18; a constant after unrolling)
+  __device__ __forceinline__ I src(int q) const {
+    const bool cx = EX(q) > 0 ? xlo : (EX(q) < 0 ? xhi : false);
+    const bool cy = EY(q) > 0 ? ylo : (EY(q) < 0 ? yhi : false);
+    const bool cz = EZ(q) > 0 ? zlo : (EZ(q) < 0 ? zhi : false);
+    I b;
+    if (EX(q) && EY(q)) b = cx ? (cy ? bxy : bx) : (cy ? by : b0);
+    else if (EX(q) && EZ(q)) b = cx ? (cz ? bxz : bx) : (cz ? bz : b0);
+    else if (EY(q) && EZ(q)) b = cy ? (cz ? byz : by) : (cz ? bz : b0);
+    else if (EX(q)) b = cx ? bx : b0;
+    else if (EY(q)) b = cy ? by : b0;
+    else b = cz ? bz : b0;
+    return b + (I)(q * ZF_TC - EX(q) - 4 * EY(q) - 16 * EZ(q));
+  }
+  // where the pull along q comes from, given the point's link word
+  __device__ __forceinline__ I pull(int q, uint32_t link) const {
+    if (q == 18) return b0 + (I)(18 * ZF_TC);
+    return (link & (1u << q)) ? b0 + (I)(OPP(q) * ZF_TC) : src(q);
+  }
+};
+
+// 32 random bits for the pair of directions (q-1, q) from the point's seed:
+// an odd multiply and an xor-shift of a Weyl step (the seed itself is a full
+// avalanche hash of point and step)
+__device__ __forceinline__ uint32_t pair_bits(uint32_t seed, int q) {
+  uint32_t h = (seed + (uint32_t)q * 0x9E3779B9u) * 0x85EBCA6Bu;
+  return h ^ (h >> 16);
+}
+
 template <class C, typename I>
 __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
   using T = typename C::T;
-  // each thread reads the pull bases it needs from its tile's row of the
-  // 27-neighbour table (L1-resident, shared by the tile's 64 threads): no
-  // block-wide staging and no barrier before the populations are loaded
+  constexpr bool kHalf = IsHalf<C>::v;
   const int lt = threadIdx.x >> 6, cell = threadIdx.x & 63;
   const int ti = blockIdx.x * kTilesPerBlock + lt;
   bool live = ti < a.n_active;
-  const int tile = live ? a.active[ti] : 0;
-  const int32_t* __restrict__ nbt = a.nbr + (int64_t)tile * 27;
-  const I tbase = (I)tile * ZF_TC;
-  const I self = tbase + (I)cell;
-  const uint32_t link = live ? a.link[self] : 0u;
+  const int tile = live ? __ldg(a.active + ti) : 0;
+  const I self = (I)tile * ZF_TC + (I)cell;  // point slot
+  const uint32_t link = live ? __ldg(a.link + self) : 0u;
   live = live && (link >> 31);
   float rho = 0.f;
 
   if (live) {
-    const int x = cell & 3, y = (cell >> 2) & 3, z = cell >> 4;
     const I ns = (I)a.ns;
     const T* __restrict__ fin = static_cast<const T*>(a.fin);
     T* __restrict__ fout = static_cast<T*>(a.fout);
+    const PullBases<I> pb(a.nbr, tile, cell);
 
-    // pull from the upstream point x - e_q; halfway bounce-back where flagged
+    // pull from the upstream point x - e_q; halfway bounce-back where flagged.
+    // 16-bit forms stay in storage units (deviation x 2^16) until the moments.
     float d[ZF_Q];
 #pragma unroll
     for (int q = 0; q < ZF_Q; ++q) {
-      I idx;
-      if (q == 18) {
-        idx = (I)18 * ns + self;
-      } else {
-        const int sx = x - EX(q), sy = y - EY(q), sz = z - EZ(q);
-        const int s27 = ((sz >> 2) + 1) * 9 + ((sy >> 2) + 1) * 3 + ((sx >> 2) + 1);
-        const int scell = (sx & 3) | ((sy & 3) << 2) | ((sz & 3) << 4);
-        // a missing neighbour only occurs on a bounce-back link (pull unused)
-        const I nbase = s27 == 13 ? tbase : (I)max(__ldg(nbt + s27), 0) * ZF_TC;
-        const I src = (I)q * ns + nbase + (I)scell;
-        const I bb = (I)OPP(q) * ns + self;
-        idx = ((link >> q) & 1u) ? bb : src;
-      }
-      d[q] = C::dec(fin[idx], q, a);
+      const T v = fin[pb.pull(q, link)];
+      if constexpr (kHalf) d[q] = (float)v;
+      else d[q] = C::dec(v, q, a);
     }
 
     float tau = a.tau;
@@ -184,6 +225,12 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
       if (EY(q)) my += EY(q) * wd;
       if (EZ(q)) mz += EZ(q) * wd;
     }
+    if constexpr (kHalf) {
+      drho *= a.inv_scale;
+      mx *= a.inv_scale;
+      my *= a.inv_scale;
+      mz *= a.inv_scale;
+    }
     rho = a.rho_ref + drho;
     const float irho = 1.f / rho;
     const float ux = (mx + 0.5f * Fx) * irho, uy = (my + 0.5f * Fy) * irho,
@@ -196,14 +243,22 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
     // BGK + Guo source in deviation form, ZebraflowWT.c:6138-6142:
     // d' = d + omega (deq - d) + src/w,  deq = drho + rho (3cu + 4.5cu^2 - 1.5u^2),
     // src/w = sfac (3 (cF - uF) + 9 cu cF); per point constants A, K1..K5 turn
-    // deq into two FMAs and the source into two, and d' keeps its form
-    // d + omega (deq - d) + src, which rounds only the non-equilibrium part
+    // deq into two FMAs and the source into two.  fp32 deviations keep the
+    // form d + omega (deq - d) + src, which rounds only the non-equilibrium
+    // part (exact mass to fp32 round-off); 16-bit forms, whose storage rounds
+    // at 2^-11, use d' = (1 - omega) d + E with E = omega deq + src folded
+    // into per-point constants in storage units.
     const float A = drho - rho * usq15;
     const float K1 = 3.f * rho, K2 = 4.5f * rho, K3 = 9.f * sfac, K4 = 3.f * sfac, K5 = 3.f * sfac * uF;
+    const float sc = kHalf ? a.scale : 1.f;
+    const float omc = 1.f - omega;
+    const float Aw = sc * (omega * A - K5), K1w = sc * omega * K1, K2w = sc * omega * K2,
+                K3s = sc * K3, K4s = sc * K4;
     float r2 = 0.f, m2x = 0.f, m2y = 0.f, m2z = 0.f;
     uint32_t rseed = 0;
-    if (IsHalf<C>::v) rseed = mix32((uint32_t)self * 0x9E3779B1u + a.step * 0x85EBCA77u);
+    if (kHalf) rseed = mix32((uint32_t)self * 0x9E3779B1u + a.step * 0x85EBCA77u);
     float dn_prev = 0.f;
+    T* __restrict__ fo = fout + pb.b0;
 #pragma unroll
     for (int q = 0; q < ZF_Q; ++q) {
       float dn;
@@ -213,6 +268,14 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
         const float deq = drho + rho * (3.f * cu + 4.5f * cu * cu - usq15);
         const float src = sfac * (3.f * (cF - uF) + 9.f * cu * cF);
         dn = d[q] + omega * (deq - d[q]) + src;
+      } else if constexpr (kHalf) {
+        if (q == 18) {
+          dn = fmaf(omc, d[q], Aw);
+        } else {
+          const float cu = cdot(q, ux, uy, uz), cF = cdot(q, Fx, Fy, Fz);
+          const float E = fmaf(cF, fmaf(K3s, cu, K4s), fmaf(cu, fmaf(K2w, cu, K1w), Aw));
+          dn = fmaf(omc, d[q], E);
+        }
       } else if (q == 18) {
         dn = fmaf(omega, A - d[q], d[q]) - K5;
       } else {
@@ -221,17 +284,17 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
         const float src = fmaf(K3 * cu, cF, fmaf(K4, cF, -K5));
         dn = fmaf(omega, deq - d[q], d[q]) + src;
       }
-      float ds;  // the value the storage keeps
-      if constexpr (IsHalf<C>::v) {
+      if constexpr (kHalf) {
         if (a.stochastic && q < 18) {
           if (q & 1) {  // pairs (q-1, q): one stochastic-rounding conversion
-            const uint32_t r = C::enc2_sr(dn_prev, dn, mix32(rseed + (uint32_t)q), a);
+            uint32_t r;
+            C::cvt2_sr(r, dn_prev, dn, pair_bits(rseed, q));
             const T lo = C::from_bits((unsigned short)(r & 0xffffu));
             const T hi = C::from_bits((unsigned short)(r >> 16));
-            fout[(I)(q - 1) * ns + self] = lo;
-            fout[(I)q * ns + self] = hi;
+            fo[(q - 1) * ZF_TC] = lo;
+            fo[q * ZF_TC] = hi;
             if (a.store_moments) {
-              const float d0 = C::dec(lo, q - 1, a), d1 = C::dec(hi, q, a);
+              const float d0 = (float)lo, d1 = (float)hi;
               r2 += WQ(q - 1) * d0 + WQ(q) * d1;
               if (EX(q - 1)) m2x += EX(q - 1) * WQ(q - 1) * d0;
               if (EY(q - 1)) m2y += EY(q - 1) * WQ(q - 1) * d0;
@@ -245,18 +308,34 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
           }
           continue;
         }
-      }
-      const T v = C::enc(dn, q, a);
-      fout[(I)q * ns + self] = v;
-      if (a.store_moments) {
-        ds = C::dec(v, q, a);
-        r2 += WQ(q) * ds;
-        if (EX(q)) m2x += EX(q) * WQ(q) * ds;
-        if (EY(q)) m2y += EY(q) * WQ(q) * ds;
-        if (EZ(q)) m2z += EZ(q) * WQ(q) * ds;
+        const T v = C::cvt_rn(dn);
+        fo[q * ZF_TC] = v;
+        if (a.store_moments) {
+          const float ds = (float)v;
+          r2 += WQ(q) * ds;
+          if (EX(q)) m2x += EX(q) * WQ(q) * ds;
+          if (EY(q)) m2y += EY(q) * WQ(q) * ds;
+          if (EZ(q)) m2z += EZ(q) * WQ(q) * ds;
+        }
+      } else {
+        const T v = C::enc(dn, q, a);
+        fo[q * ZF_TC] = v;
+        if (a.store_moments) {
+          const float ds = C::dec(v, q, a);
+          r2 += WQ(q) * ds;
+          if (EX(q)) m2x += EX(q) * WQ(q) * ds;
+          if (EY(q)) m2y += EY(q) * WQ(q) * ds;
+          if (EZ(q)) m2z += EZ(q) * WQ(q) * ds;
+        }
       }
     }
     if (a.store_moments) {  // post-collision moments without force shift, ZebraflowWT.c:6611-6614
+      if constexpr (kHalf) {
+        r2 *= a.inv_scale;
+        m2x *= a.inv_scale;
+        m2y *= a.inv_scale;
+        m2z *= a.inv_scale;
+      }
       const float D = a.rho_ref + r2;
       a.mom[self] = D;
       a.mom[ns + self] = m2x / D;
@@ -298,7 +377,7 @@ __global__ void k_lbm_wall(LbmArgs a, const int32_t* __restrict__ wall_slot,
 #pragma unroll
   for (int q = 0; q < ZF_Q; ++q) {
     const T v = C::enc(rho_m - a.rho_ref, q, a);  // feq(rho, 0)/w - rho_ref
-    fout[(int64_t)q * a.ns + slot] = v;
+    fout[pop_at(q, slot)] = v;
     const float ds = C::dec(v, q, a);
     r2 += WQ(q) * ds;
     mx += EX(q) * WQ(q) * ds;
@@ -324,7 +403,7 @@ __global__ void k_fill_equilibrium(typename C::T* f, int64_t ns, LbmArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
 #pragma unroll
-  for (int q = 0; q < ZF_Q; ++q) f[q * ns + s] = C::enc(0.f, q, a);
+  for (int q = 0; q < ZF_Q; ++q) f[pop_at(q, s)] = C::enc(0.f, q, a);
 }
 
 template <class C>
@@ -335,7 +414,7 @@ __global__ void k_scatter_pop(typename C::T* f, int64_t ns, const float* __restr
   const int64_t s = dom_slot[l];
 #pragma unroll
   for (int q = 0; q < ZF_Q; ++q)
-    f[q * ns + s] = C::enc(stage[q * n + l] * IWQ(q) - a.rho_ref, q, a);
+    f[pop_at(q, s)] = C::enc(stage[q * n + l] * IWQ(q) - a.rho_ref, q, a);
 }
 
 template <class C>
@@ -345,7 +424,7 @@ __global__ void k_gather_pop(const typename C::T* f, int64_t ns, float* __restri
   if (l >= n) return;
   const int64_t s = dom_slot[l];
 #pragma unroll
-  for (int q = 0; q < ZF_Q; ++q) stage[q * n + l] = WQ(q) * (a.rho_ref + C::dec(f[q * ns + s], q, a));
+  for (int q = 0; q < ZF_Q; ++q) stage[q * n + l] = WQ(q) * (a.rho_ref + C::dec(f[pop_at(q, s)], q, a));
 }
 
 __global__ void k_scatter_planes(float* dst, int64_t ns, const float* __restrict__ stage,
@@ -378,7 +457,7 @@ __global__ void k_mass_partial(const typename C::T* __restrict__ f, int64_t ns,
     if (!take) continue;
     double r = a.rho_ref;
 #pragma unroll
-    for (int q = 0; q < ZF_Q; ++q) r += (double)WQ(q) * (double)C::dec(f[q * ns + s], q, a);
+    for (int q = 0; q < ZF_Q; ++q) r += (double)WQ(q) * (double)C::dec(f[pop_at(q, s)], q, a);
     acc += r;
   }
   __shared__ double sh[256];
@@ -452,7 +531,7 @@ struct LaunchStep {
     if (c->n_active > 0) {
       const int grid = (c->n_active + kTilesPerBlock - 1) / kTilesPerBlock;
       if ((int64_t)ZF_Q * c->ns < (int64_t)INT32_MAX)
-        k_lbm<C, uint32_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a);
+        k_lbm<C, int32_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a);
       else
         k_lbm<C, int64_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a);
     }
@@ -509,7 +588,7 @@ __global__ void k_moments(LbmArgs a) {
   float r2 = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
 #pragma unroll
   for (int q = 0; q < ZF_Q; ++q) {
-    const float d = C::dec(f[(int64_t)q * a.ns + s], q, a);
+    const float d = C::dec(f[pop_at(q, s)], q, a);
     r2 += WQ(q) * d;
     if (EX(q)) mx += EX(q) * WQ(q) * d;
     if (EY(q)) my += EY(q) * WQ(q) * d;
@@ -558,47 +637,25 @@ int lbm_moments_launch(zf_ctx* c) {
 //   dJ/dw   = sum_q lam_q (feq_q - f_q - S_q / (2 - w)).
 // gF accumulates dt dJ/dF (the sensitivity to BODYFORCE), gw per block dJ/dw.
 template <class C, typename I>
-__global__ void __launch_bounds__(kTilesPerBlock * ZF_TC)
+__global__ void __launch_bounds__(kTilesPerBlock * ZF_TC, 3)
     k_lbm_adj(LbmArgs a, const float* __restrict__ lam, float* __restrict__ lam_prev,
               float* __restrict__ gF, double* __restrict__ gw_partial) {
-  __shared__ I s_base[kTilesPerBlock][27];
   __shared__ double s_gw[kTilesPerBlock * ZF_TC / 32];
   const int lt = threadIdx.x >> 6, cell = threadIdx.x & 63;
-  const int tb = blockIdx.x * kTilesPerBlock;
-  for (int t = threadIdx.x; t < kTilesPerBlock * 27; t += blockDim.x) {
-    const int l = t / 27, s = t - l * 27;
-    int nb = -1;
-    if (tb + l < a.n_active) nb = a.nbr[(int64_t)a.active[tb + l] * 27 + s];
-    s_base[l][s] = nb >= 0 ? (I)nb * ZF_TC : (I)0;
-  }
-  __syncthreads();
-  bool live = tb + lt < a.n_active;
-  const I self = live ? s_base[lt][13] + (I)cell : (I)0;
+  const int ti = blockIdx.x * kTilesPerBlock + lt;
+  bool live = ti < a.n_active;
+  const int tile = live ? __ldg(a.active + ti) : 0;
+  const I self = (I)tile * ZF_TC + (I)cell;
   const uint32_t link = live ? a.link[self] : 0u;
   live = live && (link >> 31);
   double gw = 0.0;
   if (live) {
-    const int x = cell & 3, y = (cell >> 2) & 3, z = cell >> 4;
     const I ns = (I)a.ns;
     const typename C::T* __restrict__ fin = static_cast<const typename C::T*>(a.fin);
+    const PullBases<I> pb(a.nbr, tile, cell);
     float f[ZF_Q];
-    I src[ZF_Q];
 #pragma unroll
-    for (int q = 0; q < ZF_Q; ++q) {
-      I idx;
-      if (q == 18) {
-        idx = (I)18 * ns + self;
-      } else {
-        const int sx = x - EX(q), sy = y - EY(q), sz = z - EZ(q);
-        const int s27 = ((sz >> 2) + 1) * 9 + ((sy >> 2) + 1) * 3 + ((sx >> 2) + 1);
-        const int scell = (sx & 3) | ((sy & 3) << 2) | ((sz & 3) << 4);
-        const I pull = (I)q * ns + s_base[lt][s27] + (I)scell;
-        const I bb = (I)OPP(q) * ns + self;
-        idx = ((link >> q) & 1u) ? bb : pull;
-      }
-      src[q] = idx;
-      f[q] = WQ(q) * (a.rho_ref + C::dec(fin[idx], q, a));
-    }
+    for (int q = 0; q < ZF_Q; ++q) f[q] = WQ(q) * (a.rho_ref + C::dec(fin[pb.pull(q, link)], q, a));
     const float Fx = a.gx + a.force_dt * a.force[self], Fy = a.gy + a.force_dt * a.force[ns + self],
                 Fz = a.gz + a.force_dt * a.force[2 * ns + self];
     float rho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
@@ -613,12 +670,11 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC)
     const float ux = (mx + 0.5f * Fx) * irho, uy = (my + 0.5f * Fy) * irho, uz = (mz + 0.5f * Fz) * irho;
     const float om = 1.f / a.tau, sfac = 1.f - 0.5f * om;
     const float usq = ux * ux + uy * uy + uz * uz, uF = ux * Fx + uy * Fy + uz * Fz;
-    float A = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f, gFx = 0.f, gFy = 0.f, gFz = 0.f;
-    float lq[ZF_Q];
+    float A = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f, gFx = 0.f, gFy = 0.f, gFz = 0.f, gwp = 0.f;
+    const float* __restrict__ lp = lam + pb.b0;
 #pragma unroll
     for (int q = 0; q < ZF_Q; ++q) {
-      const float l = lam[(I)q * ns + self];
-      lq[q] = l;
+      const float l = lp[q * ZF_TC];
       const float cu = EX(q) * ux + EY(q) * uy + EZ(q) * uz;
       const float cF = EX(q) * Fx + EY(q) * Fy + EZ(q) * Fz;
       const float poly = 1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * usq;
@@ -635,8 +691,9 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC)
       gFy += l * sw * (3.f * (EY(q) - uy) + 9.f * cu * EY(q));
       gFz += l * sw * (3.f * (EZ(q) - uz) + 9.f * cu * EZ(q));
       // d f'/d w = feq - f - S/(2 - w) ... written through sfac: dS/dw = -S/(2 sfac)
-      gw += (double)(l * (feq - f[q] - 0.5f * WQ(q) * (3.f * (cF - uF) + 9.f * cu * cF)));
+      gwp += l * (feq - f[q] - 0.5f * WQ(q) * (3.f * (cF - uF) + 9.f * cu * cF));
     }
+    gw = (double)gwp;
     A *= om;
     gFx += 0.5f * Bx * irho;
     gFy += 0.5f * By * irho;
@@ -645,10 +702,13 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC)
     gF[ns + self] += a.force_dt * gFy;
     gF[2 * ns + self] += a.force_dt * gFz;
     const float om1 = 1.f - om;
+    // lam is read again (an L1/L2 hit) and the pull sources recomputed, rather
+    // than both held in registers across the accumulation
 #pragma unroll
     for (int q = 0; q < ZF_Q; ++q) {
-      const float li = om1 * lq[q] + A + (Bx * (EX(q) - ux) + By * (EY(q) - uy) + Bz * (EZ(q) - uz)) * irho;
-      lam_prev[src[q]] = li;
+      const float li =
+          om1 * lp[q * ZF_TC] + A + (Bx * (EX(q) - ux) + By * (EY(q) - uy) + Bz * (EZ(q) - uz)) * irho;
+      lam_prev[pb.pull(q, link)] = li;
     }
   }
   // per-block sum of dJ/dw (uniform branch)
@@ -663,21 +723,46 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC)
   }
 }
 
-// The objective's seed: lam[q](x) += sum_a gU_a(x) (c_qa - U_a)/rho at fluid
-// points, U and rho being the moments (no force shift) of the populations f.
+// Velocities of the populations f at listed slots (the compact points of a
+// WSS objective's stencils): the arithmetic of k_moments, U[3][nu].
 template <class C>
-__global__ void k_seed_moments(LbmArgs a, const float* __restrict__ gU, float* __restrict__ lam) {
-  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.ns) return;
-  const uint8_t cd = a.code[s];
-  if (!(cd >= 1 && cd <= 9)) return;
-  const float gx = gU[s], gy = gU[a.ns + s], gz = gU[2 * a.ns + s];
+__global__ void k_moments_at(LbmArgs a, const int32_t* __restrict__ uslot, int nu, float* __restrict__ U) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nu) return;
+  const int64_t s = uslot[u];
+  const typename C::T* __restrict__ f = static_cast<const typename C::T*>(a.fin);
+  float r2 = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+#pragma unroll
+  for (int q = 0; q < ZF_Q; ++q) {
+    const float d = C::dec(f[pop_at(q, s)], q, a);
+    r2 += WQ(q) * d;
+    if (EX(q)) mx += EX(q) * WQ(q) * d;
+    if (EY(q)) my += EY(q) * WQ(q) * d;
+    if (EZ(q)) mz += EZ(q) * WQ(q) * d;
+  }
+  const float D = a.rho_ref + r2;
+  U[u] = mx / D;
+  U[nu + u] = my / D;
+  U[2 * nu + u] = mz / D;
+}
+
+// The objective's seed at the compact points: lam[q](x) += sum_a gU_a(x)
+// (c_qa - U_a)/rho, U and rho the moments (no force shift) of the populations
+// f; gU is cleared for the next seed.
+template <class C>
+__global__ void k_seed_at(LbmArgs a, const int32_t* __restrict__ uslot, int nu, float* __restrict__ gU,
+                          float* __restrict__ lam) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nu) return;
+  const float gx = gU[u], gy = gU[nu + u], gz = gU[2 * nu + u];
   if (gx == 0.f && gy == 0.f && gz == 0.f) return;
+  gU[u] = gU[nu + u] = gU[2 * nu + u] = 0.f;
+  const int64_t s = uslot[u];
   const typename C::T* __restrict__ f = static_cast<const typename C::T*>(a.fin);
   float fq[ZF_Q], rho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
 #pragma unroll
   for (int q = 0; q < ZF_Q; ++q) {
-    fq[q] = WQ(q) * (a.rho_ref + C::dec(f[(int64_t)q * a.ns + s], q, a));
+    fq[q] = WQ(q) * (a.rho_ref + C::dec(f[pop_at(q, s)], q, a));
     rho += fq[q];
     mx += EX(q) * fq[q];
     my += EY(q) * fq[q];
@@ -686,7 +771,7 @@ __global__ void k_seed_moments(LbmArgs a, const float* __restrict__ gU, float* _
   const float ir = 1.f / rho, Ux = mx * ir, Uy = my * ir, Uz = mz * ir;
 #pragma unroll
   for (int q = 0; q < ZF_Q; ++q)
-    lam[(int64_t)q * a.ns + s] += (gx * (EX(q) - Ux) + gy * (EY(q) - Uy) + gz * (EZ(q) - Uz)) * ir;
+    lam[pop_at(q, s)] += (gx * (EX(q) - Ux) + gy * (EY(q) - Uy) + gz * (EZ(q) - Uz)) * ir;
 }
 
 template <class C>
@@ -695,28 +780,27 @@ struct AdjStep {
     if (c->n_active == 0) return;
     const int grid = (c->n_active + kTilesPerBlock - 1) / kTilesPerBlock;
     if ((int64_t)ZF_Q * c->ns < (int64_t)INT32_MAX)
-      k_lbm_adj<C, uint32_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a, lam, lam_prev, gF, gw);
+      k_lbm_adj<C, int32_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a, lam, lam_prev, gF, gw);
     else
       k_lbm_adj<C, int64_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a, lam, lam_prev, gF, gw);
   }
 };
 template <class C>
-struct SeedMoments {
-  static void run(zf_ctx* c, const LbmArgs& a, const float* gU, float* lam) {
-    k_seed_moments<C><<<(unsigned)((c->ns + 255) / 256), 256, 0, c->stream>>>(a, gU, lam);
+struct MomentsAt {
+  static void run(zf_ctx* c, const LbmArgs& a, const PatchStencil& ps, float* U) {
+    k_moments_at<C><<<(ps.nu + 255) / 256, 256, 0, c->stream>>>(a, ps.uslot, ps.nu, U);
+  }
+};
+template <class C>
+struct SeedAt {
+  static void run(zf_ctx* c, const LbmArgs& a, const PatchStencil& ps, float* gU, float* lam) {
+    k_seed_at<C><<<(ps.nu + 255) / 256, 256, 0, c->stream>>>(a, ps.uslot, ps.nu, gU, lam);
   }
 };
 template <class C>
 struct StepBuffers {
   static void run(zf_ctx* c, const LbmArgs& a) { LaunchStep<C>::run(c, a); }
 };
-template <class C>
-struct MomentsOf {
-  static void run(zf_ctx* c, const LbmArgs& a) {
-    k_moments<C><<<(unsigned)((c->ns + 255) / 256), 256, 0, c->stream>>>(a);
-  }
-};
-
 // number of per-block partial sums k_lbm_adj writes
 int lbm_adj_blocks(zf_ctx* c) { return (c->n_active + kTilesPerBlock - 1) / kTilesPerBlock; }
 
@@ -731,10 +815,21 @@ int lbm_adj_launch(zf_ctx* c, const void* f_pre, const float* lam, float* lam_pr
   return ZF_OK;
 }
 
-int lbm_seed_launch(zf_ctx* c, const void* f, const float* gU, float* lam) {
+int lbm_moments_at(zf_ctx* c, const void* f, const PatchStencil& ps, float* d_U) {
+  if (ps.nu <= 0) return ZF_OK;
   LbmArgs a = make_args(c);
   a.fin = f;
-  dispatch_storage<SeedMoments>(c->p.storage, c, a, gU, lam);
+  dispatch_storage<MomentsAt>(c->p.storage, c, a, ps, d_U);
+  ZF_CUDA(cudaGetLastError());
+  c->launches += 1;
+  return ZF_OK;
+}
+
+int lbm_seed_at(zf_ctx* c, const void* f, const PatchStencil& ps, float* d_gU, float* lam) {
+  if (ps.nu <= 0) return ZF_OK;
+  LbmArgs a = make_args(c);
+  a.fin = f;
+  dispatch_storage<SeedAt>(c->p.storage, c, a, ps, d_gU, lam);
   ZF_CUDA(cudaGetLastError());
   c->launches += 1;
   return ZF_OK;
@@ -749,16 +844,6 @@ int lbm_step_buffers(zf_ctx* c, const void* fin, void* fout) {
   dispatch_storage<StepBuffers>(c->p.storage, c, a);
   ZF_CUDA(cudaGetLastError());
   c->launches += (c->n_active > 0) + (c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0);
-  return ZF_OK;
-}
-
-// moments of explicit populations into the context's moment planes
-int lbm_moments_of(zf_ctx* c, const void* f) {
-  LbmArgs a = make_args(c);
-  a.fin = f;
-  dispatch_storage<MomentsOf>(c->p.storage, c, a);
-  ZF_CUDA(cudaGetLastError());
-  c->launches += 1;
   return ZF_OK;
 }
 
