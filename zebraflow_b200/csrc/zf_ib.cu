@@ -528,6 +528,35 @@ __global__ void k_bin_records(IbArgs a, CellArgs c, const int32_t* total) {
                            c.tri_nrm[((size_t)2 * nc + m) * c.nt + tri], __int_as_float(g));
 }
 
+// Normal cone of each non-empty bin: c = mean of its triangles' normals and
+// r = the largest |n - c| (rounded up).  A node with normal e1 for which
+// e1.c > r |e1| sees e1.n > 0 for every triangle of the bin, so none passes
+// the reference's facing test (e1.n < 0, ZebraflowWT.c:9911-10053).
+__global__ void k_bin_cones(IbArgs a) {
+  const int64_t key = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (key >= a.ns) return;
+  const int e0 = a.bin_off[key], e1 = a.bin_off[key + 1];
+  if (e0 == e1) return;
+  float cx = 0.f, cy = 0.f, cz = 0.f;
+  for (int e = e0; e < e1; ++e) {
+    const float4 n = a.bin_n[e];
+    cx += n.x;
+    cy += n.y;
+    cz += n.z;
+  }
+  const float inv = 1.f / (float)(e1 - e0);
+  cx *= inv;
+  cy *= inv;
+  cz *= inv;
+  float r2 = 0.f;
+  for (int e = e0; e < e1; ++e) {
+    const float4 n = a.bin_n[e];
+    const float dx = n.x - cx, dy = n.y - cy, dz = n.z - cz;
+    r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
+  }
+  a.bin_cone[key] = make_float4(cx, cy, cz, sqrtf(r2) * 1.0001f + 1e-6f);
+}
+
 // ---- nucleus-membrane repulsion --------------------------------------------
 
 __global__ void k_nuc_memb(IbArgs a, CellArgs c, int rebuild, unsigned long long* overflow) {
@@ -943,6 +972,9 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
       const float e1x = c.node_normal[((size_t)0 * nc + cell) * c.nn + node];
       const float e1y = c.node_normal[((size_t)1 * nc + cell) * c.nn + node];
       const float e1z = c.node_normal[((size_t)2 * nc + cell) * c.nn + node];
+      // a bin whose normal cone lies in the node normal's half-space holds no
+      // facing triangle (margin for the rounding of the dot products)
+      const float e1n = sqrtf(e1x * e1x + e1y * e1y + e1z * e1z), cone_tol = 1e-4f * e1n;
       const int i0 = lat_index(xc, a.X0, a.DX), j0 = lat_index(yc, a.Y0, a.DX),
                 k0 = lat_index(zc, a.Z0, a.DX);
       const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
@@ -999,6 +1031,10 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
             if (d2 <= rr * rr) {
               e0 = a.bin_off[key];
               len = a.bin_off[key + 1] - e0;
+              if (len > 0) {
+                const float4 cn = a.bin_cone[key];
+                if (e1x * cn.x + e1y * cn.y + e1z * cn.z > cn.w * e1n + cone_tol) len = 0;
+              }
             }
           }
         }
@@ -1075,6 +1111,66 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
   }
 }
 
+// Lower bound, for every lattice point p of a tile near the wall, on the
+// distance from any position whose lattice index is p (the box
+// [p - 0.01, p + 0.99] DX per axis, as lat_index rounds; 0.51 DX half-width
+// here for rounding) to the candidates of the wall nodes in p's search window.
+// A node whose bound exceeds 1.5 um, the reference's starting minimum, finds
+// no wall triangle (ZebraflowWT.c:8998-9077), so k_wall_tiles skips it.  Wall
+// nodes farther than 1.51 um plus their radius are not scanned; the bound is
+// capped at 1.51 um.  One thread per point, one block of 64 per grid tile.
+__global__ void k_wall_lb(IbArgs a, float* __restrict__ lb) {
+  const int64_t gt = blockIdx.x;
+  const int t = a.tile_map[gt];
+  if (t < 0) return;
+  const int tx = (int)(gt % a.ntx), ty = (int)((gt / a.ntx) % a.nty), tz = (int)(gt / ((int64_t)a.ntx * a.nty));
+  const int cl = threadIdx.x;
+  const int i = tx * 4 + (cl & 3), j = ty * 4 + ((cl >> 2) & 3), k = tz * 4 + (cl >> 4);
+  const int64_t s = (int64_t)t * ZF_TC + cl;
+  float best = 3.0e38f;
+  const float cap = 1.51f;
+  // windows of this tile reach the 27 tiles around it only
+  int near = 0;
+  if (cl < 27) {
+    int X, Y, Z;
+    const int tn = neighbour_tile(a, tx, ty, tz, cl, X, Y, Z);
+    near = tn >= 0 && a.tile_wall[tn];
+  }
+  if (!__syncthreads_or(near)) {
+    lb[s] = cap;
+    return;
+  }
+  const int i1 = max(i - 4, 0), i2 = min(i + 4, a.nx - 1);
+  const int j1 = max(j - 4, 0), j2 = min(j + 4, a.ny - 1);
+  const int k1 = max(k - 4, a.kmin), k2 = min(k + 4, a.kmax);
+  const float DXf = (float)a.DX;
+  const float cx = (float)(a.X0 + (i + 0.49) * a.DX), cy = (float)(a.Y0 + (j + 0.49) * a.DX),
+              cz = (float)(a.Z0 + (k + 0.49) * a.DX);
+  const float h = 0.51f * DXf;
+  auto box = [&](float x, float y, float z) {
+    const float dx = fmaxf(fabsf(x - cx) - h, 0.f), dy = fmaxf(fabsf(y - cy) - h, 0.f),
+                dz = fmaxf(fabsf(wrapd(z - cz, a.LZ)) - h, 0.f);
+    return sqrtf(dx * dx + dy * dy + dz * dz);
+  };
+  int last = 0;
+  for (int ii = i1; ii <= i2; ++ii)
+    for (int jj = j1; jj <= j2; ++jj)
+      for (int kk = k1; kk <= k2; ++kk) {
+        const int64_t sw = slot_of(a, ii, jj, wrapk(a, kk));
+        if (sw < 0) continue;
+        const int m = a.windex[sw];
+        if (m <= 0 || m == last) continue;
+        last = m;
+        const float4 wn = a.wnode[sw];
+        if (box(wn.x, wn.y, wn.z) - wn.w > cap) continue;  // every candidate beyond the cap
+        for (int e = a.wcand_off[m - 1]; e < a.wcand_off[m]; ++e) {
+          const float4 p = a.wcand[e];
+          best = fminf(best, box(p.x, p.y, p.z));
+        }
+      }
+  lb[s] = fminf(best, cap);
+}
+
 // Nearest wall triangle and wall repulsion (as k_ib_wall).  A warp takes a
 // tile and then its nodes one by one, walking each node's window 32 points
 // at a time in the reference scan order (i, j, k).  A first pass finds the
@@ -1118,6 +1214,14 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs 
       const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
       const int k1 = max(k0 - 4, a.kmin), k2 = min(k0 + 4, a.kmax);
       if (i1 > i2 || j1 > j2 || k1 > k2) continue;
+      if (a.wlb && i0 >= 0 && i0 < a.nx && j0 >= 0 && j0 < a.ny) {
+        // no candidate of the window within the starting minimum: no triangle
+        const int kw0 = wrapk(a, k0);
+        if (kw0 >= 0 && kw0 < a.nz) {
+          const int64_t s0 = slot_of(a, i0, j0, kw0);
+          if (s0 >= 0 && a.wlb[s0] > 1.5f + 1e-3f) continue;
+        }
+      }
       const int ni = i2 - i1 + 1, nj = j2 - j1 + 1, nk = k2 - k1 + 1;
       const int k1w = wrapk(a, k1);
       const int npts = ni * nj * nk;
@@ -1655,6 +1759,18 @@ int wss_launch(zf_ctx* ctx, const float* d_normals, double pgauge, float* d_wss,
   return ZF_OK;
 }
 
+int wall_lb_launch(zf_ctx* ctx, float* d_wlb) {
+  const IbArgs& a = ctx->ib;
+  const int64_t ng = (int64_t)a.ntx * a.nty * a.ntz;
+  ZF_CUDA(cudaMemsetAsync(d_wlb, 0, (size_t)a.ns_all * sizeof(float), ctx->stream));  // 0: no skip
+  if (ng > 0 && a.nw > 0) {
+    k_wall_lb<<<(unsigned)ng, ZF_TC, 0, ctx->stream>>>(a, d_wlb);
+    ZF_CUDA(cudaGetLastError());
+    ctx->launches += 1;
+  }
+  return ZF_OK;
+}
+
 // Lists the patch's stencils (see k_wss_stencil_count); device buffers and
 // their sizes are appended to `bufs` (the caller frees them).
 int wss_patch_stencil(zf_ctx* ctx, const float* d_nrm, const int32_t* d_patch, int np, PatchStencil& ps,
@@ -1842,8 +1958,9 @@ int ib_bins_launch(zf_ctx* ctx) {
   k_bin_sort<<<(unsigned)((a.ns + 255) / 256), 256, 0, ctx->stream>>>(off, a.ns,
                                                                        const_cast<int32_t*>(a.bin_tri));
   k_bin_records<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(a, c, off + a.ns);
+  k_bin_cones<<<(unsigned)((a.ns + 255) / 256), 256, 0, ctx->stream>>>(a);
   ZF_CUDA(cudaGetLastError());
-  ctx->launches += 7;
+  ctx->launches += 8;
   return ZF_OK;
 }
 

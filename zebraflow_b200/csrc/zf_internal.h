@@ -162,6 +162,9 @@ struct IbArgs {
   const float* wcen;            // [3][mt]
   const int32_t* wntri;         // [nw][wcap+1]
   const float* wrad;            // [nw] WallHost::rad
+  const float* wlb;             // [n_all*64] lower bound on the distance from a position whose
+                                // lattice index is this point to the wall candidates its
+                                // window lists (capped at 1.51 um), or nullptr
   const int32_t* wcand_off;     // [nw+1] WallHost::cand_off
   const float4* wcand;          // WallHost::cand
   // cell list of triangle centroids over population slots (CSR).  Bin keys
@@ -174,6 +177,8 @@ struct IbArgs {
   float4* bin_v;                // [3][n_cells*nt] per entry: vertex xyz (fp32), node id (int bits)
   uint8_t* bin_kk;              // [n_cells*nt] per entry: its key inside the tile (0..63)
   int32_t* bin_reach;           // [ns+1] float bits: farthest point of a bin's triangles
+  float4* bin_cone;             // [ns+1] normal cone of a non-empty bin: (c, r) with every
+                                // triangle normal n of the bin within |n - c| <= r
                                 // from the bin point (um, rounded up); [ns] the largest
   // membrane and nucleus nodes grouped by the lattice tile of their nearest
   // point (tile grid index over all ntx*nty*ntz tiles), rebuilt after positions change
@@ -217,6 +222,7 @@ struct PatchStencil {
   const float* w = nullptr;        // [entries] Peskin weight
   const int32_t* uslot = nullptr;  // [nu] slot of each compact point
 };
+int wall_lb_launch(zf_ctx* c, float* d_wlb);
 int wss_patch_stencil(zf_ctx* c, const float* d_nrm, const int32_t* d_patch, int np, PatchStencil& ps,
                       std::vector<std::pair<void*, size_t>>& bufs);
 int wss_patch_launch(zf_ctx* c, const PatchStencil& ps, const float* d_nrm, const float* d_U, double w,
