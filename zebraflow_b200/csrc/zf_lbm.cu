@@ -170,8 +170,12 @@ __device__ __forceinline__ uint32_t pair_bits(uint32_t seed, int q) {
   return h ^ (h >> 16);
 }
 
-template <class C, typename I>
-__global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
+// kMom: write the post-collision moments (the step before a membrane/IB
+// block); kSR: stochastic rounding of the 16-bit forms.  Both are launch
+// constants made template parameters so that the unrolled direction loop
+// carries no branch on them.
+template <class C, typename I, bool kMom, bool kSR>
+__global__ void __launch_bounds__(kTilesPerBlock * ZF_TC, 6) k_lbm(LbmArgs a) {
   using T = typename C::T;
   constexpr bool kHalf = IsHalf<C>::v;
   const int lt = threadIdx.x >> 6, cell = threadIdx.x & 63;
@@ -285,7 +289,7 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
         dn = fmaf(omega, deq - d[q], d[q]) + src;
       }
       if constexpr (kHalf) {
-        if (a.stochastic && q < 18) {
+        if (kSR && q < 18) {
           if (q & 1) {  // pairs (q-1, q): one stochastic-rounding conversion
             uint32_t r;
             C::cvt2_sr(r, dn_prev, dn, pair_bits(rseed, q));
@@ -293,7 +297,7 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
             const T hi = C::from_bits((unsigned short)(r >> 16));
             fo[(q - 1) * ZF_TC] = lo;
             fo[q * ZF_TC] = hi;
-            if (a.store_moments) {
+            if (kMom) {
               const float d0 = (float)lo, d1 = (float)hi;
               r2 += WQ(q - 1) * d0 + WQ(q) * d1;
               if (EX(q - 1)) m2x += EX(q - 1) * WQ(q - 1) * d0;
@@ -310,7 +314,7 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
         }
         const T v = C::cvt_rn(dn);
         fo[q * ZF_TC] = v;
-        if (a.store_moments) {
+        if (kMom) {
           const float ds = (float)v;
           r2 += WQ(q) * ds;
           if (EX(q)) m2x += EX(q) * WQ(q) * ds;
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
       } else {
         const T v = C::enc(dn, q, a);
         fo[q * ZF_TC] = v;
-        if (a.store_moments) {
+        if (kMom) {
           const float ds = C::dec(v, q, a);
           r2 += WQ(q) * ds;
           if (EX(q)) m2x += EX(q) * WQ(q) * ds;
@@ -329,7 +333,7 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC) k_lbm(LbmArgs a) {
         }
       }
     }
-    if (a.store_moments) {  // post-collision moments without force shift, ZebraflowWT.c:6611-6614
+    if (kMom) {  // post-collision moments without force shift, ZebraflowWT.c:6611-6614
       if constexpr (kHalf) {
         r2 *= a.inv_scale;
         m2x *= a.inv_scale;
@@ -527,13 +531,26 @@ static void dispatch_storage(int storage, Args&&... args) {
 
 template <class C>
 struct LaunchStep {
+  template <typename I>
+  static void launch_lbm(zf_ctx* c, const LbmArgs& a, int grid) {
+    const int nt = kTilesPerBlock * ZF_TC;
+    if constexpr (IsHalf<C>::v) {
+      if (a.stochastic) {
+        if (a.store_moments) k_lbm<C, I, true, true><<<grid, nt, 0, c->stream>>>(a);
+        else k_lbm<C, I, false, true><<<grid, nt, 0, c->stream>>>(a);
+        return;
+      }
+    }
+    if (a.store_moments) k_lbm<C, I, true, false><<<grid, nt, 0, c->stream>>>(a);
+    else k_lbm<C, I, false, false><<<grid, nt, 0, c->stream>>>(a);
+  }
   static void run(zf_ctx* c, const LbmArgs& a) {
     if (c->n_active > 0) {
       const int grid = (c->n_active + kTilesPerBlock - 1) / kTilesPerBlock;
       if ((int64_t)ZF_Q * c->ns < (int64_t)INT32_MAX)
-        k_lbm<C, int32_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a);
+        launch_lbm<int32_t>(c, a, grid);
       else
-        k_lbm<C, int64_t><<<grid, kTilesPerBlock * ZF_TC, 0, c->stream>>>(a);
+        launch_lbm<int64_t>(c, a, grid);
     }
     if (c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0)
       k_lbm_wall<C><<<(c->n_wall + 255) / 256, 256, 0, c->stream>>>(a, c->d_wall_slot,
