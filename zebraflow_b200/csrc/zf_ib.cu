@@ -385,23 +385,36 @@ __global__ void k_bin_assign(IbArgs a, CellArgs c, int32_t* tri_bin, int32_t* co
       const int i1 = max(i0 - 2, 0), i2 = min(i0 + 2, a.nx - 1);
       const int j1 = max(j0 - 2, 0), j2 = min(j0 + 2, a.ny - 1);
       const int k1 = a.per_z ? k0 - 2 : max(k0 - 2, 2), k2 = a.per_z ? k0 + 2 : min(k0 + 2, a.nz - 4);
-      for (int i = i1; i <= i2; ++i)
-        for (int j = j1; j <= j2; ++j)
-          for (int k = k1; k <= k2; ++k) {
-            const int kw = a.per_z ? ((k % a.nz) + a.nz) % a.nz : k;
-            const int64_t s = slot_of(a, i, j, kw);
-            if (s < 0 || s >= a.ns) continue;
-            const uint8_t cd = a.code[s];
-            if (cd == 0) continue;  // listed points only
-            const float xc = (float)((double)a.X0 + i * (double)a.DX);
-            const float yc = (float)((double)a.Y0 + j * (double)a.DX);
-            const float zc = (float)((double)a.Z0 + k * (double)a.DX);
-            const float d = dist3(xc - xp, yc - yp, zc - zp);
-            if (d < mindis) {
-              mindis = d;
-              best = s;
+      auto listed = [&](int i, int j, int k) -> int64_t {
+        const int kw = a.per_z ? ((k % a.nz) + a.nz) % a.nz : k;
+        const int64_t s = slot_of(a, i, j, kw);
+        return (s < 0 || s >= a.ns || a.code[s] == 0) ? (int64_t)-1 : s;
+      };
+      auto scan = [&](int ia, int ib, int ja, int jb, int ka, int kb) {
+        for (int i = ia; i <= ib; ++i)
+          for (int j = ja; j <= jb; ++j)
+            for (int k = ka; k <= kb; ++k) {
+              const int64_t s = listed(i, j, k);  // listed points only
+              if (s < 0) continue;
+              const float xc = (float)((double)a.X0 + i * (double)a.DX);
+              const float yc = (float)((double)a.Y0 + j * (double)a.DX);
+              const float zc = (float)((double)a.Z0 + k * (double)a.DX);
+              const float d = dist3(xc - xp, yc - yp, zc - zp);
+              if (d < mindis) {
+                mindis = d;
+                best = s;
+              }
             }
-          }
+      };
+      // the lattice point nearest the centroid: when it is listed, every
+      // point as near or nearer (ties included) is one of its 27 neighbours,
+      // so the first minimum of the window scan lies among them
+      const int ic = (int)floor(((double)xp - a.X0) / a.DX + 0.5), jc = (int)floor(((double)yp - a.Y0) / a.DX + 0.5),
+                kc = (int)floor(((double)zp - a.Z0) / a.DX + 0.5);
+      if (ic >= i1 && ic <= i2 && jc >= j1 && jc <= j2 && kc >= k1 && kc <= k2 && listed(ic, jc, kc) >= 0)
+        scan(max(ic - 1, i1), min(ic + 1, i2), max(jc - 1, j1), min(jc + 1, j2), max(kc - 1, k1), min(kc + 1, k2));
+      else
+        scan(i1, i2, j1, j2, k1, k2);
     }
     if (best >= 0 && mindis < 1.f) {
       const int64_t key = bin_key(best);
@@ -493,8 +506,8 @@ __device__ __forceinline__ float rec_pack(int kk, float rb) {
 __device__ __forceinline__ int rec_kk(float w) { return (int)(__float_as_uint(w) & 0xffu); }
 __device__ __forceinline__ float rec_rb(float w) { return (float)(__float_as_uint(w) >> 8) * (1.f / 1048576.f); }
 
-// per bin entry: centroid and bounding radius, normal and triangle id, and the
-// three vertices (fp32 of the fp64 positions, with their node ids), so the
+// per bin entry: centroid and bounding radius, normal and triangle id (one
+// 32-byte record), and the three vertices (fp32 of the fp64 positions, with their node ids), so the
 // repulsion search reads one contiguous range of records per run of bins and
 // evaluates a triangle from its own record.  The radius bounds the distance from the centroid to any point of the
 // triangle (the vertices, as float), with a margin for float rounding.
@@ -515,7 +528,7 @@ __global__ void k_bin_records(IbArgs a, CellArgs c, const int32_t* total) {
     const float dz = (float)c.x[((size_t)2 * nc + m) * c.nn + n] - cz;
     r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
   }
-  a.bin_c[e] = make_float4(cx, cy, cz, rec_pack(a.bin_kk[e], sqrtf(r2) * 1.0001f + 1e-3f));
+  a.bin_rec[2 * e] = make_float4(cx, cy, cz, rec_pack(a.bin_kk[e], sqrtf(r2) * 1.0001f + 1e-3f));
   const int64_t stride = (int64_t)nc * c.nt;
   for (int v = 0; v < 3; ++v) {
     const int n = c.tri[3 * tri + v];
@@ -523,38 +536,72 @@ __global__ void k_bin_records(IbArgs a, CellArgs c, const int32_t* total) {
                                           (float)c.x[((size_t)1 * nc + m) * c.nn + n],
                                           (float)c.x[((size_t)2 * nc + m) * c.nn + n], __int_as_float(n));
   }
-  a.bin_n[e] = make_float4(c.tri_nrm[((size_t)0 * nc + m) * c.nt + tri],
+  a.bin_rec[2 * e + 1] = make_float4(c.tri_nrm[((size_t)0 * nc + m) * c.nt + tri],
                            c.tri_nrm[((size_t)1 * nc + m) * c.nt + tri],
                            c.tri_nrm[((size_t)2 * nc + m) * c.nt + tri], __int_as_float(g));
 }
 
-// Normal cone of each non-empty bin: c = mean of its triangles' normals and
-// r = the largest |n - c| (rounded up).  A node with normal e1 for which
-// e1.c > r |e1| sees e1.n > 0 for every triangle of the bin, so none passes
-// the reference's facing test (e1.n < 0, ZebraflowWT.c:9911-10053).
-__global__ void k_bin_cones(IbArgs a) {
+// Normal cone of a bin packed in 32 bits: c = the mean of its triangles'
+// normals quantised to 8 signed bits per component (c' = q/127), and r' >= the
+// largest |n - c'| in units of 1/127 (8 bits, rounded up, the quantisation
+// error of c' included).  A node with normal e1 for which e1.c' > r' |e1| sees
+// e1.n > 0 for every triangle of the bin, so none passes the reference's
+// facing test (e1.n < 0, ZebraflowWT.c:9911-10053).
+__device__ __forceinline__ int cone_pack(float cx, float cy, float cz, float r) {
+  const int qx = __float2int_rn(fminf(fmaxf(cx, -1.f), 1.f) * 127.f);
+  const int qy = __float2int_rn(fminf(fmaxf(cy, -1.f), 1.f) * 127.f);
+  const int qz = __float2int_rn(fminf(fmaxf(cz, -1.f), 1.f) * 127.f);
+  // |c - c'| <= |c - clamp(c)| + sqrt(3) 0.5/127 (clamping moves c towards c')
+  const float dq = sqrtf((cx - qx / 127.f) * (cx - qx / 127.f) + (cy - qy / 127.f) * (cy - qy / 127.f) +
+                         (cz - qz / 127.f) * (cz - qz / 127.f));
+  const int qr = min((int)ceilf((r + dq) * 1.0001f * 127.f + 1e-3f), 255);
+  return (int)((unsigned)(qx & 0xff) | ((unsigned)(qy & 0xff) << 8) | ((unsigned)(qz & 0xff) << 16) |
+               ((unsigned)qr << 24));
+}
+// true when no triangle of the bin can face a node of normal e (|e| = en)
+__device__ __forceinline__ bool cone_excludes(int w, float ex, float ey, float ez, float en) {
+  const float cx = (float)(signed char)(w & 0xff), cy = (float)(signed char)((w >> 8) & 0xff),
+              cz = (float)(signed char)((w >> 16) & 0xff);
+  const float r = (float)((unsigned)w >> 24);
+  // in units of 1/127; the margin covers the rounding of the dot products
+  return ex * cx + ey * cy + ez * cz > (r + 0.0127f) * en;
+}
+
+// One header per bin: first entry, entry count, reach, and the normal cone of
+// its triangles (mean normal c and r = the largest |n - c|, rounded up).
+__global__ void k_bin_headers(IbArgs a) {
   const int64_t key = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (key >= a.ns) return;
   const int e0 = a.bin_off[key], e1 = a.bin_off[key + 1];
-  if (e0 == e1) return;
-  float cx = 0.f, cy = 0.f, cz = 0.f;
-  for (int e = e0; e < e1; ++e) {
-    const float4 n = a.bin_n[e];
-    cx += n.x;
-    cy += n.y;
-    cz += n.z;
+  int cone = 0;
+  if (e1 > e0) {
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    for (int e = e0; e < e1; ++e) {
+      const float4 n = a.bin_rec[2 * e + 1];
+      cx += n.x;
+      cy += n.y;
+      cz += n.z;
+    }
+    const float inv = 1.f / (float)(e1 - e0);
+    cx *= inv;
+    cy *= inv;
+    cz *= inv;
+    float r2 = 0.f;
+    for (int e = e0; e < e1; ++e) {
+      const float4 n = a.bin_rec[2 * e + 1];
+      const float dx = n.x - cx, dy = n.y - cy, dz = n.z - cz;
+      r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
+    }
+    cone = cone_pack(cx, cy, cz, sqrtf(r2) * 1.0001f + 1e-6f);
   }
-  const float inv = 1.f / (float)(e1 - e0);
-  cx *= inv;
-  cy *= inv;
-  cz *= inv;
-  float r2 = 0.f;
-  for (int e = e0; e < e1; ++e) {
-    const float4 n = a.bin_n[e];
-    const float dx = n.x - cx, dy = n.y - cy, dz = n.z - cz;
-    r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
+  a.bin_hdr[key] = make_int4(e0, e1 - e0, a.bin_reach[key], cone);
+  // occupancy of the tile's 64 bins, bit = key within the tile (ns is a
+  // multiple of 64, so a warp is either wholly inside or wholly past the end)
+  const unsigned occ = __ballot_sync(0xffffffffu, e1 > e0);
+  if ((threadIdx.x & 31) == 0) {
+    unsigned* o = reinterpret_cast<unsigned*>(a.bin_occ);
+    o[key >> 5] = occ;
   }
-  a.bin_cone[key] = make_float4(cx, cy, cz, sqrtf(r2) * 1.0001f + 1e-6f);
 }
 
 // ---- nucleus-membrane repulsion --------------------------------------------
@@ -777,7 +824,7 @@ __global__ void __launch_bounds__(kRepWarps * 32) k_rbc_rbc(IbArgs a, CellArgs c
     const float ox = __shfl_sync(FULL, xc, owner), oy = __shfl_sync(FULL, yc, owner),
                 oz = __shfl_sync(FULL, zc, owner);
     float tx = 0.f, ty = 0.f, tz = 0.f;
-    if (my >= 0) rbc_entry(a, c, my, a.bin_c[my], ox, oy, oz, tx, ty, tz);
+    if (my >= 0) rbc_entry(a, c, my, a.bin_rec[2 * my], ox, oy, oz, tx, ty, tz);
     sq_r[w][lane][0] = tx;
     sq_r[w][lane][1] = ty;
     sq_r[w][lane][2] = tz;
@@ -793,11 +840,11 @@ __global__ void __launch_bounds__(kRepWarps * 32) k_rbc_rbc(IbArgs a, CellArgs c
   while (__any_sync(FULL, !done)) {
     int item = -1;
     if (!done) {
-      const float4 cr = a.bin_c[e];
+      const float4 cr = a.bin_rec[2 * e];
       const float dzc = wrapd(cr.z - zc, a.LZ);
       const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
       if (dcen < 2.f && !(dcen - rec_rb(cr.w) > 1.f)) {
-        const float4 nr = a.bin_n[e];
+        const float4 nr = a.bin_rec[2 * e + 1];
         if (e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
           const int g = __float_as_int(nr.w);
           const int m = g / c.nt;
@@ -929,16 +976,42 @@ __device__ __forceinline__ int neighbour_tile(const IbArgs& a, int tx, int ty, i
   return a.tile_map[((int64_t)Z * a.nty + Y) * a.ntx + X];
 }
 
-// RBC-RBC repulsion (ZebraflowWT.c:9911-10053).  For each node the warp walks
-// the window's lattice points 32 at a time.  Only triangles with a
+// bits lo..hi (clamped to 0..3) of a 4-bit mask
+__device__ __forceinline__ unsigned axis_mask4(int lo, int hi) {
+  lo = max(lo, 0);
+  hi = min(hi, 3);
+  return lo > hi ? 0u : ((2u << hi) - 1u) & ~((1u << lo) - 1u);
+}
+// position of the n-th (0-based) set bit of m (n < popc(m))
+__device__ __forceinline__ int select_bit(unsigned m, int n) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w >= 1; w >>= 1) {
+    const unsigned low = m & ((1u << w) - 1u);
+    const int cnt = __popc(low);
+    if (n >= cnt) {
+      n -= cnt;
+      m >>= w;
+      pos += w;
+    } else {
+      m = low;
+    }
+  }
+  return pos;
+}
+
+// RBC-RBC repulsion (ZebraflowWT.c:9911-10053).  For each node the warp lists
+// the bins of its window that hold triangles (the tiles' occupancy masks cut
+// to the window) and takes them 32 at a time.  Only triangles with a
 // sub-centroid within 1 um of the node contribute, so a bin point farther
-// than 1 um plus its reach (plus a rounding margin) holds none: such points
-// are skipped, first against the largest reach with arithmetic alone, then
-// against the point's own reach.  The triangles of the remaining bins pass
-// the reference's tests (centroid within 2 um, facing normals, not the node's
-// own triangle) and one whose sub-centroids can reach 1 um queues up; queued
-// triangles are evaluated 32 at a time, one per lane.  Lane sums meet in a
-// fixed butterfly, so the result is deterministic.
+// than 1 um plus its reach (plus a rounding margin) holds none, and a bin
+// whose normal cone lies in the node normal's half-space holds no facing
+// triangle: both are skipped.  The triangles of the remaining bins pass the
+// reference's tests (centroid within 2 um, facing normals, not the node's own
+// triangle) and one whose plane is within 1 um queues up; queued triangles
+// are evaluated 32 at a time, one per lane.  The sum over a node's triangles
+// does not depend on the order they are met in (up to rounding); lane sums
+// meet in a fixed butterfly, so the result is deterministic.
 __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArgs c) {
   __shared__ int s_q[kTileWarps][64];
   const unsigned FULL = 0xffffffffu;
@@ -947,8 +1020,6 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
   const int64_t nmem = (int64_t)nc * c.nn;
   const int64_t n_pop_tiles = a.ns / ZF_TC;
   const int nlist = a.tile_ctr[0];
-  const float reach_all = __int_as_float(a.bin_reach[a.ns]);
-  const float lim = 1.f + reach_all + 1e-3f;
   int* queue = s_q[warp];
   for (int li = warp_next_tile(&a.tile_ctr[1], lane); li < nlist; li = warp_next_tile(&a.tile_ctr[1], lane)) {
     const int gt = a.tile_list[li];
@@ -974,21 +1045,42 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
       const float e1z = c.node_normal[((size_t)2 * nc + cell) * c.nn + node];
       // a bin whose normal cone lies in the node normal's half-space holds no
       // facing triangle (margin for the rounding of the dot products)
-      const float e1n = sqrtf(e1x * e1x + e1y * e1y + e1z * e1z), cone_tol = 1e-4f * e1n;
+      const float e1n = sqrtf(e1x * e1x + e1y * e1y + e1z * e1z);
       const int i0 = lat_index(xc, a.X0, a.DX), j0 = lat_index(yc, a.Y0, a.DX),
                 k0 = lat_index(zc, a.Z0, a.DX);
       const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
       const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
       const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
       if (i1 > i2 || j1 > j2 || k1 > k2) continue;
-      const int ni = i2 - i1 + 1, nj = j2 - j1 + 1, nk = k2 - k1 + 1;
-      const int k1w = a.per_z ? ((k1 % a.nz) + a.nz) % a.nz : k1;
-      const int npts = ni * nj * nk;
       const int g_own = cell * c.nt;
-      // lane l starts at window point l (scan order i, j, k) and steps 32
-      // points at a time in mixed radix
-      const int sk = 32 % nk, sj = (32 / nk) % nj, si = 32 / (nk * nj);
-      int i = i1 + lane / (nj * nk), j = j1 + (lane / nk) % nj, dk = lane % nk;
+      // the window's bins that hold triangles: lane r < 27 intersects the
+      // window with tile r and its occupancy mask (bit 16 x + 4 y + z).  z is
+      // unwrapped around the node: window k and tile origins share one frame.
+      const int kshift = a.per_z ? (((k0 % a.nz) + a.nz) % a.nz) - k0 : 0;
+      unsigned mlo = 0, mhi = 0;
+      if (rt >= 0) {
+        const int ox = (tx + lane % 3 - 1) * 4, oy = (ty + (lane / 3) % 3 - 1) * 4, oz = (tz + lane / 9 - 1) * 4;
+        const unsigned xm = axis_mask4(i1 - ox, i2 - ox), ym = axis_mask4(j1 - oy, j2 - oy),
+                       zm = axis_mask4(k1 + kshift - oz, k2 + kshift - oz);
+        unsigned long long w = 0ull;
+#pragma unroll
+        for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj)
+            if (((xm >> ii) & 1u) && ((ym >> jj) & 1u)) w |= (unsigned long long)zm << (16 * ii + 4 * jj);
+        const uint2 occ = a.bin_occ[rt];
+        mlo = occ.x & (unsigned)w;
+        mhi = occ.y & (unsigned)(w >> 32);
+      }
+      const int nbin = __popc(mlo) + __popc(mhi);
+      int bincl = nbin;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, bincl, o);
+        if (lane >= o) bincl += v;
+      }
+      const int nbins = __shfl_sync(FULL, bincl, 31);
+      const int bbase = bincl - nbin;  // this tile lane's first candidate
       float rx = 0.f, ry = 0.f, rz = 0.f;
       int qn = 0;
       auto flush = [&](int nb) {
@@ -996,7 +1088,7 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
         if (lane < nb) {
           const int e = queue[lane];
           float tx2, ty2, tz2;
-          rbc_entry(a, c, e, a.bin_c[e], xc, yc, zc, tx2, ty2, tz2);
+          rbc_entry(a, c, e, a.bin_rec[2 * e], xc, yc, zc, tx2, ty2, tz2);
           rx += tx2;
           ry += ty2;
           rz += tz2;
@@ -1008,50 +1100,35 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
         __syncwarp();
         qn = rem;
       };
-      // window point coordinates relative to the node, in float (the bound
-      // carries a margin far above their rounding)
       const float X0f = (float)a.X0, Y0f = (float)a.Y0, Z0f = (float)a.Z0, DXf = (float)a.DX;
-      const float lim2 = lim * lim;
-      for (int p0 = 0; p0 < npts; p0 += 32) {
-        // the bin of this lane's window point: key and tile
-        int kw = k1w + dk;
-        if (kw >= a.nz) kw -= a.nz;
-        int lz = (kw >> 2) - tz + 1;
-        if (lz < 0) lz += a.ntz;
-        else if (lz > 2) lz -= a.ntz;
-        const int r = (lz * 3 + ((j >> 2) - ty + 1)) * 3 + ((i >> 2) - tx + 1);
-        const int t = __shfl_sync(FULL, rt, r);  // every lane takes part
+      for (int p0 = 0; p0 < nbins; p0 += 32) {
+        // candidate p0 + lane: its tile lane r and the bin's bit in that tile
+        const int gb = p0 + lane;
+        int r = 0;
+#pragma unroll
+        for (int stp = 16; stp > 0; stp >>= 1) {
+          const int v = __shfl_sync(FULL, bbase, r + stp);
+          if (r + stp < 27 && gb >= v) r += stp;
+        }
+        const unsigned lo = __shfl_sync(FULL, mlo, r), hi = __shfl_sync(FULL, mhi, r);
+        const int t = __shfl_sync(FULL, rt, r);
+        const int nth = gb - __shfl_sync(FULL, bbase, r);
         int e0 = 0, len = 0;
-        if (p0 + lane < npts && t >= 0) {
-          const float ddx = (X0f + i * DXf) - xc, ddy = (Y0f + j * DXf) - yc, ddz = (Z0f + (k1 + dk) * DXf) - zc;
+        if (gb < nbins) {
+          const int nlo = __popc(lo);
+          const int b = nth < nlo ? select_bit(lo, nth) : 32 + select_bit(hi, nth - nlo);
+          const int ii = b >> 4, jj = (b >> 2) & 3, kk = b & 3;
+          const int i = (tx + r % 3 - 1) * 4 + ii, j = (ty + (r / 3) % 3 - 1) * 4 + jj,
+                    k = (tz + r / 9 - 1) * 4 + kk - kshift;  // unwrapped around the node
+          const float ddx = (X0f + i * DXf) - xc, ddy = (Y0f + j * DXf) - yc, ddz = (Z0f + k * DXf) - zc;
           const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-          if (d2 < lim2) {
-            const int64_t key = (int64_t)t * ZF_TC + 16 * (i & 3) + 4 * (j & 3) + (kw & 3);
-            const float rr = __int_as_float(a.bin_reach[key]) + 1.f + 1e-3f;
-            if (d2 <= rr * rr) {
-              e0 = a.bin_off[key];
-              len = a.bin_off[key + 1] - e0;
-              if (len > 0) {
-                const float4 cn = a.bin_cone[key];
-                if (e1x * cn.x + e1y * cn.y + e1z * cn.z > cn.w * e1n + cone_tol) len = 0;
-              }
-            }
+          const int4 h = a.bin_hdr[(int64_t)t * ZF_TC + b];
+          const float rr = __int_as_float(h.z) + 1.f + 1e-3f;
+          if (d2 <= rr * rr && !cone_excludes(h.w, e1x, e1y, e1z, e1n)) {
+            e0 = h.x;
+            len = h.y;
           }
         }
-        // advance to the point 32 further on
-        dk += sk;
-        int cy = 0;
-        if (dk >= nk) {
-          dk -= nk;
-          cy = 1;
-        }
-        j += sj + cy;
-        cy = 0;
-        if (j > j2) {
-          j -= nj;
-          cy = 1;
-        }
-        i += si + cy;
         // the triangles of the remaining bins as one sequence over the lanes
         int incl = len;
 #pragma unroll
@@ -1073,20 +1150,21 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
           const int e = __shfl_sync(FULL, e0, src) + (gpos - __shfl_sync(FULL, base, src));
           bool pass = false;
           if (gpos < total) {
-            const float4 cr = a.bin_c[e];
+            const float4 cr = a.bin_rec[2 * e], nr = a.bin_rec[2 * e + 1];
             const float dzc = wrapd(cr.z - zc, a.LZ);
             const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
-            if (dcen < 2.f && !(dcen - rec_rb(cr.w) > 1.f)) {
-              const float4 nr = a.bin_n[e];
-              if (e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
-                const int g = __float_as_int(nr.w);
-                pass = true;
-                if (g >= g_own && g < g_own + c.nt) {
-                  const int64_t stride = (int64_t)nc * c.nt;
-                  pass = !(__float_as_int(a.bin_v[e].w) == node || __float_as_int(a.bin_v[stride + e].w) == node ||
-                           __float_as_int(a.bin_v[2 * stride + e].w) == node);
-                }
-              }
+            if (dcen < 2.f && !(dcen - rec_rb(cr.w) > 1.f) && e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
+              // the 16 sub-centroids lie in the triangle's plane, within 3/4 of
+              // the bounding radius of the centroid (the farthest, at
+              // barycentric (10,1,1)/12, is half a median away): none is within
+              // 1 um unless the node's distance to that disk is (margin for the
+              // float rounding of the sub-centroids)
+              const float pd = (cr.x - xc) * nr.x + (cr.y - yc) * nr.y + dzc * nr.z;
+              const float qd = fmaxf(sqrtf(fmaxf(dcen * dcen - pd * pd, 0.f)) - 0.75f * rec_rb(cr.w), 0.f);
+              const int tri = __float_as_int(nr.w) - g_own;  // not the node's own triangle
+              pass = pd * pd + qd * qd <= 1.004f &&
+                     !((unsigned)tri < (unsigned)c.nt &&
+                       (c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node));
             }
           }
           const unsigned bal = __ballot_sync(FULL, pass);
@@ -1111,15 +1189,24 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
   }
 }
 
-// Lower bound, for every lattice point p of a tile near the wall, on the
-// distance from any position whose lattice index is p (the box
-// [p - 0.01, p + 0.99] DX per axis, as lat_index rounds; 0.51 DX half-width
-// here for rounding) to the candidates of the wall nodes in p's search window.
-// A node whose bound exceeds 1.5 um, the reference's starting minimum, finds
-// no wall triangle (ZebraflowWT.c:8998-9077), so k_wall_tiles skips it.  Wall
-// nodes farther than 1.51 um plus their radius are not scanned; the bound is
-// capped at 1.51 um.  One thread per point, one block of 64 per grid tile.
-__global__ void k_wall_lb(IbArgs a, float* __restrict__ lb) {
+// Wall nodes that can hold a node's nearest wall triangle, per lattice point
+// p of a tile near the wall (ZebraflowWT.c:8998-9077).  A node whose lattice
+// index is p lies in the box B = [p - 0.01, p + 0.99] DX per axis (as
+// lat_index rounds; 0.51 DX half-width here for rounding).  Its search scans
+// the lists of the wall nodes in p's window in scan order and keeps the first
+// candidate (triangle vertex or centroid) strictly nearer than the running
+// minimum, which starts at 1.5 um.  With U = min over the window's candidates
+// c of max over B of |x - c|, the minimum is at most min(U, 1.5), so a list
+// whose candidates are all farther from B than that holds neither the winner
+// nor a tie with it; a list met again adds nothing.  What remains is the
+// distinct wall nodes, in order of first appearance, whose lists come within
+// min(U, 1.5) + 1e-3 of B: at most kWallRel of them (more: -1, and the node
+// walks its window instead).  One thread per point, one block of 64 per grid
+// tile; the count pass writes counts, the fill pass the lists.
+constexpr int kWallRel = 96;
+template <bool kFill>
+__global__ void k_wall_rel(IbArgs a, int32_t* __restrict__ cnt, int32_t* __restrict__ clipped,
+                           const int32_t* __restrict__ off, int32_t* __restrict__ out) {
   const int64_t gt = blockIdx.x;
   const int t = a.tile_map[gt];
   if (t < 0) return;
@@ -1127,8 +1214,6 @@ __global__ void k_wall_lb(IbArgs a, float* __restrict__ lb) {
   const int cl = threadIdx.x;
   const int i = tx * 4 + (cl & 3), j = ty * 4 + ((cl >> 2) & 3), k = tz * 4 + (cl >> 4);
   const int64_t s = (int64_t)t * ZF_TC + cl;
-  float best = 3.0e38f;
-  const float cap = 1.51f;
   // windows of this tile reach the 27 tiles around it only
   int near = 0;
   if (cl < 27) {
@@ -1137,9 +1222,12 @@ __global__ void k_wall_lb(IbArgs a, float* __restrict__ lb) {
     near = tn >= 0 && a.tile_wall[tn];
   }
   if (!__syncthreads_or(near)) {
-    lb[s] = cap;
+    if (!kFill) cnt[s] = clipped[s] = 0;
     return;
   }
+  // the fill pass writes exactly the count pass's entries, and only there
+  const int nfill = kFill ? cnt[s] : 0;
+  if (kFill && nfill <= 0) return;
   const int i1 = max(i - 4, 0), i2 = min(i + 4, a.nx - 1);
   const int j1 = max(j - 4, 0), j2 = min(j + 4, a.ny - 1);
   const int k1 = max(k - 4, a.kmin), k2 = min(k + 4, a.kmax);
@@ -1147,11 +1235,17 @@ __global__ void k_wall_lb(IbArgs a, float* __restrict__ lb) {
   const float cx = (float)(a.X0 + (i + 0.49) * a.DX), cy = (float)(a.Y0 + (j + 0.49) * a.DX),
               cz = (float)(a.Z0 + (k + 0.49) * a.DX);
   const float h = 0.51f * DXf;
-  auto box = [&](float x, float y, float z) {
+  auto box_min = [&](float x, float y, float z) {
     const float dx = fmaxf(fabsf(x - cx) - h, 0.f), dy = fmaxf(fabsf(y - cy) - h, 0.f),
                 dz = fmaxf(fabsf(wrapd(z - cz, a.LZ)) - h, 0.f);
     return sqrtf(dx * dx + dy * dy + dz * dz);
   };
+  auto box_max = [&](float x, float y, float z) {
+    const float dx = fabsf(x - cx) + h, dy = fabsf(y - cy) + h, dz = fabsf(wrapd(z - cz, a.LZ)) + h;
+    return sqrtf(dx * dx + dy * dy + dz * dz);
+  };
+  const float cap = 1.51f;
+  float U = 3.0e38f;
   int last = 0;
   for (int ii = i1; ii <= i2; ++ii)
     for (int jj = j1; jj <= j2; ++jj)
@@ -1162,18 +1256,54 @@ __global__ void k_wall_lb(IbArgs a, float* __restrict__ lb) {
         if (m <= 0 || m == last) continue;
         last = m;
         const float4 wn = a.wnode[sw];
-        if (box(wn.x, wn.y, wn.z) - wn.w > cap) continue;  // every candidate beyond the cap
+        if (box_min(wn.x, wn.y, wn.z) - wn.w > cap) continue;  // cannot bring U below 1.5
         for (int e = a.wcand_off[m - 1]; e < a.wcand_off[m]; ++e) {
           const float4 p = a.wcand[e];
-          best = fminf(best, box(p.x, p.y, p.z));
+          U = fminf(U, box_max(p.x, p.y, p.z));
         }
       }
-  lb[s] = fminf(best, cap);
+  const float thr = fminf(U, 1.5f) + 1e-3f;
+  int seen[kWallRel];
+  int n = 0;
+  const int base = kFill ? off[s] : 0;
+  last = 0;
+  for (int ii = i1; ii <= i2; ++ii)
+    for (int jj = j1; jj <= j2; ++jj)
+      for (int kk = k1; kk <= k2; ++kk) {
+        const int64_t sw = slot_of(a, ii, jj, wrapk(a, kk));
+        if (sw < 0) continue;
+        const int m = a.windex[sw];
+        if (m <= 0 || m == last) continue;
+        last = m;
+        const float4 wn = a.wnode[sw];
+        if (box_min(wn.x, wn.y, wn.z) - wn.w > thr) continue;
+        float lbm = 3.0e38f;
+        for (int e = a.wcand_off[m - 1]; e < a.wcand_off[m]; ++e) {
+          const float4 p = a.wcand[e];
+          lbm = fminf(lbm, box_min(p.x, p.y, p.z));
+        }
+        if (lbm > thr) continue;
+        bool dup = false;
+        for (int q = 0; q < min(n, kWallRel); ++q) dup |= seen[q] == m;
+        if (dup) continue;
+        if (n < kWallRel) {
+          seen[n] = m;
+          if (kFill && n < nfill) out[base + n] = m;
+        }
+        ++n;
+      }
+  if (!kFill) {
+    cnt[s] = n > kWallRel ? -1 : n;
+    clipped[s] = n > kWallRel ? 0 : n;
+  }
 }
 
 // Nearest wall triangle and wall repulsion (as k_ib_wall).  A warp takes a
-// tile and then its nodes one by one, walking each node's window 32 points
-// at a time in the reference scan order (i, j, k).  A first pass finds the
+// tile and then its nodes one by one.  Where the node's lattice point has its
+// wall-node lists (k_wall_rel), lane l scans the l-th of them and the lanes
+// fold as below; no list means no triangle.  Otherwise the warp walks the
+// node's window 32 points at a time in the reference scan order (i, j, k).
+// A first pass finds the
 // window's nearest wall node; the first minimum of its list bounds the window
 // minimum from above.  The second pass skips a point that repeats the
 // previous point's wall node or whose wall node cannot reach the bound, and
@@ -1214,126 +1344,145 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs 
       const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
       const int k1 = max(k0 - 4, a.kmin), k2 = min(k0 + 4, a.kmax);
       if (i1 > i2 || j1 > j2 || k1 > k2) continue;
-      if (a.wlb && i0 >= 0 && i0 < a.nx && j0 >= 0 && j0 < a.ny) {
-        // no candidate of the window within the starting minimum: no triangle
+      float mindis = 1.5f;
+      int triwall = -1;
+      // the wall nodes listed for the node's lattice point (k_wall_rel): lane l
+      // scans the l-th list, and the ordered fold below keeps the first minimum
+      int rel = -1;  // -1: no lists here, walk the window
+      if (a.wrel_cnt && i0 >= 0 && i0 < a.nx && j0 >= 0 && j0 < a.ny) {
         const int kw0 = wrapk(a, k0);
         if (kw0 >= 0 && kw0 < a.nz) {
           const int64_t s0 = slot_of(a, i0, j0, kw0);
-          if (s0 >= 0 && a.wlb[s0] > 1.5f + 1e-3f) continue;
-        }
-      }
-      const int ni = i2 - i1 + 1, nj = j2 - j1 + 1, nk = k2 - k1 + 1;
-      const int k1w = wrapk(a, k1);
-      const int npts = ni * nj * nk;
-      // lane l starts at window point l and steps 32 points in mixed radix;
-      // (i, j, dk) with the wrapped z index kw = k1w + dk (minus nz past the end)
-      const int sk = 32 % nk, sj = (32 / nk) % nj, si = 32 / (nk * nj);
-      const int pi0 = i1 + lane / (nj * nk), pj0 = j1 + (lane / nk) % nj, pk0 = lane % nk;
-      auto step = [&](int& i, int& j, int& dk) {
-        dk += sk;
-        int cy = 0;
-        if (dk >= nk) {
-          dk -= nk;
-          cy = 1;
-        }
-        j += sj + cy;
-        cy = 0;
-        if (j > j2) {
-          j -= nj;
-          cy = 1;
-        }
-        i += si + cy;
-      };
-      // slot of window point (i, j, dk) in the IB view, -1 outside the wall tiles
-      auto slot = [&](int i, int j, int dk) -> int64_t {
-        int kw = k1w + dk;
-        if (kw >= a.nz) kw -= a.nz;
-        int lz = (kw >> 2) - tz + 1;
-        if (lz < 0) lz += a.ntz;
-        else if (lz > 2) lz -= a.ntz;
-        const int r = (lz * 3 + ((j >> 2) - ty + 1)) * 3 + ((i >> 2) - tx + 1);
-        const int t = __shfl_sync(FULL, rt, r);  // every lane calls slot()
-        return t < 0 ? (int64_t)-1 : (int64_t)t * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (kw & 3);
-      };
-      // bound: the first minimum of one list of the window bounds the window
-      // minimum from above (1.5 is the reference's starting value); take the
-      // nearest wall node among those of the 8 lattice points around the node
-      float bound = 1.5f;
-      {
-        float dbest = 3.0e38f;
-        int mbest = 0;
-        const int ci = (int)floor(((double)xp - a.X0) / a.DX) + (lane & 1);
-        const int cj = (int)floor(((double)yp - a.Y0) / a.DX) + ((lane >> 1) & 1);
-        const int ck = (int)floor(((double)zp - a.Z0) / a.DX) + ((lane >> 2) & 1);
-        const bool in = lane < 8 && ci >= i1 && ci <= i2 && cj >= j1 && cj <= j2 && ck >= k1 && ck <= k2;
-        // every lane calls slot(); lanes outside pass a window point
-        const int64_t sc = slot(in ? ci : i1, in ? cj : j1, in ? ck - k1 : 0);
-        if (in && sc >= 0) {
-          const int wi = a.windex[sc];
-          const float4 wn = a.wnode[sc];
-          if (wi > 0) {
-            dbest = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
-            mbest = wi;
-          }
-        }
-        float dmin = dbest;
+          if (s0 >= 0) rel = a.wrel_cnt[s0];
+          const int32_t* lists = rel > 0 ? a.wrel + a.wrel_off[s0] : nullptr;
+          for (int r0 = 0; r0 < rel; r0 += 32) {  // 32 lists at a time, in order
+            float d = 3.0e38f;
+            int t = -1;
+            if (r0 + lane < rel) wall_list_min(a, lists[r0 + lane], xp, yp, zp, d, t);
+            float dmin = d;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
-        const unsigned at = __ballot_sync(FULL, dbest == dmin && mbest > 0);
-        if (at) {
-          const int m = __shfl_sync(FULL, mbest, __ffs(at) - 1);
-          int unused = -1;
-          wall_list_min(a, m, xp, yp, zp, bound, unused);
+            for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
+            const unsigned at = __ballot_sync(FULL, d == dmin && t >= 0);
+            if (at && dmin < mindis) {
+              mindis = dmin;
+              triwall = __shfl_sync(FULL, t, __ffs(at) - 1);
+            }
+          }
         }
       }
-      float mindis = 1.5f;
-      int triwall = -1, last = 0, qn = 0;
-      auto flush = [&](int nb) {
-        __syncwarp();
-        float d = 3.0e38f;
-        int t = -1;
-        if (lane < nb) wall_list_min(a, queue[lane], xp, yp, zp, d, t);
-        float dmin = d;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
-        const unsigned at = __ballot_sync(FULL, d == dmin && t >= 0);
-        if (at && dmin < mindis) {
-          mindis = dmin;
-          triwall = __shfl_sync(FULL, t, __ffs(at) - 1);
-        }
-        const int rem = qn - nb;
-        const int tq = lane < rem ? queue[nb + lane] : 0;
-        __syncwarp();
-        if (lane < rem) queue[lane] = tq;
-        __syncwarp();
-        qn = rem;
-      };
-      {
-        int i = pi0, j = pj0, dk = pk0;
-        for (int p0 = 0; p0 < npts; p0 += 32) {
-          int wi = 0;
-          float4 wn = make_float4(0.f, 0.f, 0.f, -1.f);
-          const int64_t s = slot(i, j, dk);
-          if (p0 + lane < npts && s >= 0) {
-            wi = a.windex[s];
-            wn = a.wnode[s];
+      if (rel < 0) {
+        const int ni = i2 - i1 + 1, nj = j2 - j1 + 1, nk = k2 - k1 + 1;
+        const int k1w = wrapk(a, k1);
+        const int npts = ni * nj * nk;
+        // lane l starts at window point l and steps 32 points in mixed radix;
+        // (i, j, dk) with the wrapped z index kw = k1w + dk (minus nz past the end)
+        const int sk = 32 % nk, sj = (32 / nk) % nj, si = 32 / (nk * nj);
+        const int pi0 = i1 + lane / (nj * nk), pj0 = j1 + (lane / nk) % nj, pk0 = lane % nk;
+        auto step = [&](int& i, int& j, int& dk) {
+          dk += sk;
+          int cy = 0;
+          if (dk >= nk) {
+            dk -= nk;
+            cy = 1;
           }
-          step(i, j, dk);
-          int prev = __shfl_up_sync(FULL, wi, 1);
-          if (lane == 0) prev = last;
-          last = __shfl_sync(FULL, wi, 31);
-          bool want = false;
-          if (wi > 0 && wi != prev) {
-            const float dm = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
-            want = !(dm - wn.w > fminf(bound, mindis) + 1e-4f);
+          j += sj + cy;
+          cy = 0;
+          if (j > j2) {
+            j -= nj;
+            cy = 1;
           }
-          const unsigned bal = __ballot_sync(FULL, want);
-          if (want) queue[qn + __popc(bal & ((1u << lane) - 1u))] = wi;
-          qn += __popc(bal);
-          while (qn >= 32) flush(32);
+          i += si + cy;
+        };
+        // slot of window point (i, j, dk) in the IB view, -1 outside the wall tiles
+        auto slot = [&](int i, int j, int dk) -> int64_t {
+          int kw = k1w + dk;
+          if (kw >= a.nz) kw -= a.nz;
+          int lz = (kw >> 2) - tz + 1;
+          if (lz < 0) lz += a.ntz;
+          else if (lz > 2) lz -= a.ntz;
+          const int r = (lz * 3 + ((j >> 2) - ty + 1)) * 3 + ((i >> 2) - tx + 1);
+          const int t = __shfl_sync(FULL, rt, r);  // every lane calls slot()
+          return t < 0 ? (int64_t)-1 : (int64_t)t * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (kw & 3);
+        };
+        // bound: the first minimum of one list of the window bounds the window
+        // minimum from above (1.5 is the reference's starting value); take the
+        // nearest wall node among those of the 8 lattice points around the node
+        float bound = 1.5f;
+        {
+          float dbest = 3.0e38f;
+          int mbest = 0;
+          const int ci = (int)floor(((double)xp - a.X0) / a.DX) + (lane & 1);
+          const int cj = (int)floor(((double)yp - a.Y0) / a.DX) + ((lane >> 1) & 1);
+          const int ck = (int)floor(((double)zp - a.Z0) / a.DX) + ((lane >> 2) & 1);
+          const bool in = lane < 8 && ci >= i1 && ci <= i2 && cj >= j1 && cj <= j2 && ck >= k1 && ck <= k2;
+          // every lane calls slot(); lanes outside pass a window point
+          const int64_t sc = slot(in ? ci : i1, in ? cj : j1, in ? ck - k1 : 0);
+          if (in && sc >= 0) {
+            const int wi = a.windex[sc];
+            const float4 wn = a.wnode[sc];
+            if (wi > 0) {
+              dbest = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
+              mbest = wi;
+            }
+          }
+          float dmin = dbest;
+  #pragma unroll
+          for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
+          const unsigned at = __ballot_sync(FULL, dbest == dmin && mbest > 0);
+          if (at) {
+            const int m = __shfl_sync(FULL, mbest, __ffs(at) - 1);
+            int unused = -1;
+            wall_list_min(a, m, xp, yp, zp, bound, unused);
+          }
         }
-        while (qn > 0) flush(min(qn, 32));
-      }
+        int last = 0, qn = 0;
+        auto flush = [&](int nb) {
+          __syncwarp();
+          float d = 3.0e38f;
+          int t = -1;
+          if (lane < nb) wall_list_min(a, queue[lane], xp, yp, zp, d, t);
+          float dmin = d;
+  #pragma unroll
+          for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
+          const unsigned at = __ballot_sync(FULL, d == dmin && t >= 0);
+          if (at && dmin < mindis) {
+            mindis = dmin;
+            triwall = __shfl_sync(FULL, t, __ffs(at) - 1);
+          }
+          const int rem = qn - nb;
+          const int tq = lane < rem ? queue[nb + lane] : 0;
+          __syncwarp();
+          if (lane < rem) queue[lane] = tq;
+          __syncwarp();
+          qn = rem;
+        };
+        {
+          int i = pi0, j = pj0, dk = pk0;
+          for (int p0 = 0; p0 < npts; p0 += 32) {
+            int wi = 0;
+            float4 wn = make_float4(0.f, 0.f, 0.f, -1.f);
+            const int64_t s = slot(i, j, dk);
+            if (p0 + lane < npts && s >= 0) {
+              wi = a.windex[s];
+              wn = a.wnode[s];
+            }
+            step(i, j, dk);
+            int prev = __shfl_up_sync(FULL, wi, 1);
+            if (lane == 0) prev = last;
+            last = __shfl_sync(FULL, wi, 31);
+            bool want = false;
+            if (wi > 0 && wi != prev) {
+              const float dm = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
+              want = !(dm - wn.w > fminf(bound, mindis) + 1e-4f);
+            }
+            const unsigned bal = __ballot_sync(FULL, want);
+            if (want) queue[qn + __popc(bal & ((1u << lane) - 1u))] = wi;
+            qn += __popc(bal);
+            while (qn >= 32) flush(32);
+          }
+          while (qn > 0) flush(min(qn, 32));
+        }
+      }  // rel < 0
       if (triwall < 0 || lane != 0) continue;
       // signed distance to the plane of the wall triangle, repulsion, :9055-9077
       const int w1 = a.wtri[3 * triwall];
@@ -1759,18 +1908,6 @@ int wss_launch(zf_ctx* ctx, const float* d_normals, double pgauge, float* d_wss,
   return ZF_OK;
 }
 
-int wall_lb_launch(zf_ctx* ctx, float* d_wlb) {
-  const IbArgs& a = ctx->ib;
-  const int64_t ng = (int64_t)a.ntx * a.nty * a.ntz;
-  ZF_CUDA(cudaMemsetAsync(d_wlb, 0, (size_t)a.ns_all * sizeof(float), ctx->stream));  // 0: no skip
-  if (ng > 0 && a.nw > 0) {
-    k_wall_lb<<<(unsigned)ng, ZF_TC, 0, ctx->stream>>>(a, d_wlb);
-    ZF_CUDA(cudaGetLastError());
-    ctx->launches += 1;
-  }
-  return ZF_OK;
-}
-
 // Lists the patch's stencils (see k_wss_stencil_count); device buffers and
 // their sizes are appended to `bufs` (the caller frees them).
 int wss_patch_stencil(zf_ctx* ctx, const float* d_nrm, const int32_t* d_patch, int np, PatchStencil& ps,
@@ -1896,6 +2033,46 @@ void scan_launch(const int32_t* in, int64_t n, int32_t* out, int32_t* bsum, cuda
 
 }  // namespace
 
+// Builds the per-point lists of k_wall_rel into ctx->ib (wrel_cnt, wrel_off,
+// wrel); device buffers are appended to `own`.
+int wall_rel_build(zf_ctx* ctx, std::vector<void*>& own) {
+  IbArgs& a = ctx->ib;
+  a.wrel_cnt = a.wrel_off = a.wrel = nullptr;
+  const int64_t ng = (int64_t)a.ntx * a.nty * a.ntz;
+  if (ng == 0 || a.nw == 0 || a.ns_all == 0) return ZF_OK;
+  const int64_t n = a.ns_all;
+  const int64_t nb = (n + 1 + 1023) / 1024;
+  auto grab = [&](void** p, size_t b) -> int {
+    int r = dev_alloc(ctx, p, b);
+    if (!r) own.push_back(*p);
+    return r;
+  };
+  int32_t *cnt = nullptr, *off = nullptr, *tmp = nullptr, *list = nullptr;
+  int rc;
+  if ((rc = grab((void**)&cnt, (size_t)n * sizeof(int32_t))) ||
+      (rc = grab((void**)&off, (size_t)(n + 1) * sizeof(int32_t))))
+    return rc;
+  // scratch: clipped counts (n + 1, the last 0) and the scan's block sums
+  if ((rc = dev_alloc(ctx, (void**)&tmp, (size_t)(n + 1 + nb + 1) * sizeof(int32_t)))) return rc;
+  ZF_CUDA(cudaMemsetAsync(tmp, 0, (size_t)(n + 1) * sizeof(int32_t), ctx->stream));
+  k_wall_rel<false><<<(unsigned)ng, ZF_TC, 0, ctx->stream>>>(a, cnt, tmp, nullptr, nullptr);
+  ZF_CUDA(cudaGetLastError());
+  scan_launch(tmp, n + 1, off, tmp + n + 1, ctx->stream);
+  int32_t total = 0;
+  ZF_CUDA(cudaMemcpyAsync(&total, off + n, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  ZF_CUDA(cudaStreamSynchronize(ctx->stream));
+  cudaFree(tmp);
+  ctx->device_bytes -= (int64_t)((n + 1 + nb + 1) * sizeof(int32_t));
+  if ((rc = grab((void**)&list, (size_t)std::max<int32_t>(total, 1) * sizeof(int32_t)))) return rc;
+  k_wall_rel<true><<<(unsigned)ng, ZF_TC, 0, ctx->stream>>>(a, cnt, nullptr, off, list);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 5;
+  a.wrel_cnt = cnt;
+  a.wrel_off = off;
+  a.wrel = list;
+  return ZF_OK;
+}
+
 int ib_node_tiles_launch(zf_ctx* ctx) {
   const CellArgs& c = ctx->cells;
   IbArgs& a = ctx->ib;
@@ -1958,7 +2135,7 @@ int ib_bins_launch(zf_ctx* ctx) {
   k_bin_sort<<<(unsigned)((a.ns + 255) / 256), 256, 0, ctx->stream>>>(off, a.ns,
                                                                        const_cast<int32_t*>(a.bin_tri));
   k_bin_records<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(a, c, off + a.ns);
-  k_bin_cones<<<(unsigned)((a.ns + 255) / 256), 256, 0, ctx->stream>>>(a);
+  k_bin_headers<<<(unsigned)((a.ns + 255) / 256), 256, 0, ctx->stream>>>(a);
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 8;
   return ZF_OK;

@@ -130,17 +130,13 @@ int build_view(zf_ctx* c, const WallHost* W) {
     if ((rc = dalloc<float4>(c, own, const_cast<float4**>(&a.wcand), W->cand.size(), W->cand.data()))) return rc;
     if ((rc = dalloc<float>(c, own, const_cast<float**>(&a.wnnrm), W->nnrm.size(), W->nnrm.data())))
       return rc;
-    float* wlb = nullptr;
-    a.wlb = nullptr;
-    if ((rc = dalloc<float>(c, own, &wlb, (size_t)ns_all))) return rc;
-    if ((rc = wall_lb_launch(c, wlb))) return rc;
-    a.wlb = wlb;
+    if ((rc = wall_rel_build(c, own))) return rc;
   } else {
     a.nw = a.mt = a.wcap = 0;
     a.wxyz = a.wnrm = a.wcen = a.wrad = a.wnnrm = nullptr;
     a.wcand_off = nullptr;
     a.wcand = nullptr;
-    a.wlb = nullptr;
+    a.wrel_cnt = a.wrel_off = a.wrel = nullptr;
     a.wtri = a.wntri = nullptr;
   }
   ZF_CUDA(cudaStreamSynchronize(c->stream));
@@ -161,12 +157,12 @@ int ib_buffers(zf_ctx* c) {
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &buf, 2 * nscan + ntri + nb + 1))) return rc;
   a.bin_off = buf;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, const_cast<int32_t**>(&a.bin_tri), ntri))) return rc;
-  if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_c, ntri))) return rc;
-  if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_n, ntri))) return rc;
+  if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_rec, 2 * ntri))) return rc;
   if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_v, 3 * ntri))) return rc;
   if ((rc = dalloc<uint8_t>(c, c->ib_allocs, &a.bin_kk, ntri))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.bin_reach, nscan))) return rc;
-  if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_cone, nscan))) return rc;
+  if ((rc = dalloc<int4>(c, c->ib_allocs, &a.bin_hdr, nscan))) return rc;
+  if ((rc = dalloc<uint2>(c, c->ib_allocs, &a.bin_occ, (c->ns + ZF_TC - 1) / ZF_TC))) return rc;
   // node-tile lists
   const int64_t nnodes = (int64_t)cl.n_cells * (cl.nn + cl.nnn);
   a.ngrid = (int64_t)c->ntx * c->nty * c->ntz;

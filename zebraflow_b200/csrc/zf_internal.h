@@ -162,9 +162,12 @@ struct IbArgs {
   const float* wcen;            // [3][mt]
   const int32_t* wntri;         // [nw][wcap+1]
   const float* wrad;            // [nw] WallHost::rad
-  const float* wlb;             // [n_all*64] lower bound on the distance from a position whose
-                                // lattice index is this point to the wall candidates its
-                                // window lists (capped at 1.51 um), or nullptr
+  // per IB-view point: the wall nodes whose lists can hold the nearest wall
+  // triangle of a node with that lattice index (k_wall_rel), as CSR; count
+  // -1: too many, the node walks its window
+  const int32_t* wrel_cnt;      // [n_all*64]
+  const int32_t* wrel_off;      // [n_all*64 + 1]
+  const int32_t* wrel;          // 1-based wall node ids
   const int32_t* wcand_off;     // [nw+1] WallHost::cand_off
   const float4* wcand;          // WallHost::cand
   // cell list of triangle centroids over population slots (CSR).  Bin keys
@@ -172,14 +175,16 @@ struct IbArgs {
   // run of points along z are one contiguous range of entries.
   const int32_t* bin_off;       // [ns+1]
   const int32_t* bin_tri;       // [n_cells*nt] global triangle id = cell*nt + tri
-  float4* bin_c;                // [n_cells*nt] per entry: centroid xyz, bounding radius
-  float4* bin_n;                // [n_cells*nt] per entry: normal xyz, id (int bits)
+  float4* bin_rec;              // [n_cells*nt][2] per entry, adjacent: centroid xyz and bounding
+                                // radius (rec_pack); normal xyz and global triangle id (int bits)
   float4* bin_v;                // [3][n_cells*nt] per entry: vertex xyz (fp32), node id (int bits)
   uint8_t* bin_kk;              // [n_cells*nt] per entry: its key inside the tile (0..63)
   int32_t* bin_reach;           // [ns+1] float bits: farthest point of a bin's triangles
-  float4* bin_cone;             // [ns+1] normal cone of a non-empty bin: (c, r) with every
-                                // triangle normal n of the bin within |n - c| <= r
                                 // from the bin point (um, rounded up); [ns] the largest
+  int4* bin_hdr;                // [ns] per bin: first entry, entry count, reach (float bits),
+                                // normal cone (cone_pack) of its triangles
+  uint2* bin_occ;               // [ns/64] per population tile: bit 16x+4y+z set when that
+                                // bin holds a triangle (x: keys 0..31, y: keys 32..63)
   // membrane and nucleus nodes grouped by the lattice tile of their nearest
   // point (tile grid index over all ntx*nty*ntz tiles), rebuilt after positions change
   int64_t ngrid;                // ntx*nty*ntz
@@ -222,7 +227,7 @@ struct PatchStencil {
   const float* w = nullptr;        // [entries] Peskin weight
   const int32_t* uslot = nullptr;  // [nu] slot of each compact point
 };
-int wall_lb_launch(zf_ctx* c, float* d_wlb);
+int wall_rel_build(zf_ctx* c, std::vector<void*>& own);
 int wss_patch_stencil(zf_ctx* c, const float* d_nrm, const int32_t* d_patch, int np, PatchStencil& ps,
                       std::vector<std::pair<void*, size_t>>& bufs);
 int wss_patch_launch(zf_ctx* c, const PatchStencil& ps, const float* d_nrm, const float* d_U, double w,
