@@ -1298,28 +1298,91 @@ __global__ void k_wall_rel(IbArgs a, int32_t* __restrict__ cnt, int32_t* __restr
   }
 }
 
-// Nearest wall triangle and wall repulsion (as k_ib_wall).  A warp takes a
-// tile and then its nodes one by one.  Where the node's lattice point has its
-// wall-node lists (k_wall_rel), lane l scans the l-th of them and the lanes
-// fold as below; no list means no triangle.  Otherwise the warp walks the
-// node's window 32 points at a time in the reference scan order (i, j, k).
-// A first pass finds the
-// window's nearest wall node; the first minimum of its list bounds the window
-// minimum from above.  The second pass skips a point that repeats the
+__device__ __forceinline__ void wall_repel(const IbArgs& a, const CellArgs& c, int cell, int node, float xp,
+                                           float yp, float zp, int triwall) {
+  // signed distance to the plane of the wall triangle, repulsion, :9055-9077
+  const int nc = c.n_cells;
+  const int w1 = a.wtri[3 * triwall];
+  const float n0 = a.wnrm[triwall], n1 = a.wnrm[a.mt + triwall], n2 = a.wnrm[2 * a.mt + triwall];
+  const float ddx = xp - a.wxyz[w1], ddy = yp - a.wxyz[a.nw + w1], ddz = wrapd(zp - a.wxyz[2 * a.nw + w1], a.LZ);
+  const float dist = __fadd_rn(__fadd_rn(__fmul_rn(ddx, n0), __fmul_rn(ddy, n1)), __fmul_rn(ddz, n2));
+  if (dist < 0.25f && fabsf(dist) < 1.0f && node < c.nn) {
+    float repulf = (float)((0.25 - (double)dist) / 1.0);
+    if (dist < -0.75f) repulf = 1.f;
+    // nucleus nodes add to the membrane array at their own index, as the
+    // reference does (ZebraflowWT.c:9415-9430 write NODE_WALLREPUL[v][caps][node])
+    atomicAdd(&c.wrep[((size_t)0 * nc + cell) * c.nn + node], (float)((double)repulf * 1.e-04 * n0));
+    atomicAdd(&c.wrep[((size_t)1 * nc + cell) * c.nn + node], (float)((double)repulf * 1.e-04 * n1));
+    atomicAdd(&c.wrep[((size_t)2 * nc + cell) * c.nn + node], (float)((double)repulf * 1.e-04 * n2));
+  }
+}
+
+// Nearest wall triangle and wall repulsion (as k_ib_wall), first pass: one
+// thread per node.  Where the node's lattice point has its wall-node lists
+// (k_wall_rel), the thread scans them in order with the reference's running
+// minimum (strict <, starting at 1.5 um); no list means no triangle.  Nodes
+// whose point has no lists (too many, or outside the IB view) are queued for
+// k_wall_walk.
+__global__ void k_wall_nodes(IbArgs a, CellArgs c, int32_t* __restrict__ walk, int32_t* __restrict__ walk_n) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (int64_t)c.n_cells * (c.nn + c.nnn)) return;
+  bool nuc;
+  int cell, node;
+  if (!node_of(c, gid, nuc, cell, node)) return;
+  const int n = nuc ? c.nnn : c.nn;
+  float xp, yp, zp;
+  node_pos(nuc ? c.xn : c.x, c.n_cells, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
+  const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX), k0 = lat_index(zp, a.Z0, a.DX);
+  if (max(i0 - 4, 0) > min(i0 + 4, a.nx - 1) || max(j0 - 4, 0) > min(j0 + 4, a.ny - 1) ||
+      max(k0 - 4, a.kmin) > min(k0 + 4, a.kmax))
+    return;  // empty window
+  int rel = -1;
+  int64_t s0 = -1;
+  if (a.wrel_cnt && i0 >= 0 && i0 < a.nx && j0 >= 0 && j0 < a.ny) {
+    const int kw0 = wrapk(a, k0);
+    if (kw0 >= 0 && kw0 < a.nz) {
+      s0 = slot_of(a, i0, j0, kw0);
+      if (s0 >= 0) rel = a.wrel_cnt[s0];
+    }
+  }
+  if (rel < 0) {
+    walk[atomicAdd(walk_n, 1)] = (int32_t)gid;
+    return;
+  }
+  float mindis = 1.5f;
+  int triwall = -1;
+  const int32_t* lists = a.wrel + a.wrel_off[s0];
+  for (int r = 0; r < rel; ++r) wall_list_min(a, lists[r], xp, yp, zp, mindis, triwall);
+  if (triwall >= 0) wall_repel(a, c, cell, node, xp, yp, zp, triwall);
+}
+
+// Second pass for the queued nodes: a warp per node walks its window 32
+// points at a time in the reference scan order (i, j, k).  A first pass finds
+// the window's nearest wall node; the first minimum of its list bounds the
+// window minimum from above.  The second pass skips a point that repeats the
 // previous point's wall node or whose wall node cannot reach the bound, and
 // queues the other lists in scan order; they are scanned 32 at a time, one
 // per lane, and folded in queue order: the lowest lane holding the batch
 // minimum is the first candidate in scan order, and it replaces the running
 // minimum only when strictly smaller.
-__global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs c) {
+__global__ void __launch_bounds__(kTileThreads) k_wall_walk(IbArgs a, CellArgs c, const int32_t* __restrict__ walk,
+                                                           const int32_t* __restrict__ walk_n,
+                                                           int32_t* __restrict__ ctr) {
   __shared__ int s_q[kTileWarps][64];
   const unsigned FULL = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nc = c.n_cells;
-  const int nlist = a.tile_ctr[0];
+  const int nwalk = *walk_n;
   int* queue = s_q[warp];
-  for (int li = warp_next_tile(&a.tile_ctr[2], lane); li < nlist; li = warp_next_tile(&a.tile_ctr[2], lane)) {
-    const int gt = a.tile_list[li];
+  for (int li = warp_next_tile(ctr, lane); li < nwalk; li = warp_next_tile(ctr, lane)) {
+    const int64_t gid = walk[li];
+    bool nuc;
+    int cell, node;
+    if (!node_of(c, gid, nuc, cell, node)) continue;
+    const int n = nuc ? c.nnn : c.nn;
+    float xp, yp, zp;
+    node_pos(nuc ? c.xn : c.x, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
+    const int gt = node_grid_tile(a, xp, yp, zp);
     const int tx = gt % a.ntx, ty = (gt / a.ntx) % a.nty, tz = gt / (a.ntx * a.nty);
     // lane r < 27: tile id of neighbour r when it holds W_index points
     int rt = -1;
@@ -1329,177 +1392,125 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_tiles(IbArgs a, CellArgs 
       if (t >= 0 && a.tile_wall[t]) rt = t;
     }
     if (!__any_sync(FULL, rt >= 0)) continue;
-    const int n0 = a.node_off[gt], n1 = a.node_off[gt + 1];
-    for (int q = n0; q < n1; ++q) {
-      const int64_t gid = a.node_sorted[q];
-      bool nuc;
-      int cell, node;
-      if (!node_of(c, gid, nuc, cell, node)) continue;
-      const int n = nuc ? c.nnn : c.nn;
-      float xp, yp, zp;
-      node_pos(nuc ? c.xn : c.x, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
-      const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
-                k0 = lat_index(zp, a.Z0, a.DX);
-      const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
-      const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
-      const int k1 = max(k0 - 4, a.kmin), k2 = min(k0 + 4, a.kmax);
-      if (i1 > i2 || j1 > j2 || k1 > k2) continue;
-      float mindis = 1.5f;
-      int triwall = -1;
-      // the wall nodes listed for the node's lattice point (k_wall_rel): lane l
-      // scans the l-th list, and the ordered fold below keeps the first minimum
-      int rel = -1;  // -1: no lists here, walk the window
-      if (a.wrel_cnt && i0 >= 0 && i0 < a.nx && j0 >= 0 && j0 < a.ny) {
-        const int kw0 = wrapk(a, k0);
-        if (kw0 >= 0 && kw0 < a.nz) {
-          const int64_t s0 = slot_of(a, i0, j0, kw0);
-          if (s0 >= 0) rel = a.wrel_cnt[s0];
-          const int32_t* lists = rel > 0 ? a.wrel + a.wrel_off[s0] : nullptr;
-          for (int r0 = 0; r0 < rel; r0 += 32) {  // 32 lists at a time, in order
-            float d = 3.0e38f;
-            int t = -1;
-            if (r0 + lane < rel) wall_list_min(a, lists[r0 + lane], xp, yp, zp, d, t);
-            float dmin = d;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
-            const unsigned at = __ballot_sync(FULL, d == dmin && t >= 0);
-            if (at && dmin < mindis) {
-              mindis = dmin;
-              triwall = __shfl_sync(FULL, t, __ffs(at) - 1);
-            }
-          }
+    const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX), k0 = lat_index(zp, a.Z0, a.DX);
+    const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
+    const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
+    const int k1 = max(k0 - 4, a.kmin), k2 = min(k0 + 4, a.kmax);
+    if (i1 > i2 || j1 > j2 || k1 > k2) continue;
+    float mindis = 1.5f;
+    int triwall = -1;
+    const int ni = i2 - i1 + 1, nj = j2 - j1 + 1, nk = k2 - k1 + 1;
+    const int k1w = wrapk(a, k1);
+    const int npts = ni * nj * nk;
+    // lane l starts at window point l and steps 32 points in mixed radix;
+    // (i, j, dk) with the wrapped z index kw = k1w + dk (minus nz past the end)
+    const int sk = 32 % nk, sj = (32 / nk) % nj, si = 32 / (nk * nj);
+    const int pi0 = i1 + lane / (nj * nk), pj0 = j1 + (lane / nk) % nj, pk0 = lane % nk;
+    auto step = [&](int& i, int& j, int& dk) {
+      dk += sk;
+      int cy = 0;
+      if (dk >= nk) {
+        dk -= nk;
+        cy = 1;
+      }
+      j += sj + cy;
+      cy = 0;
+      if (j > j2) {
+        j -= nj;
+        cy = 1;
+      }
+      i += si + cy;
+    };
+    // slot of window point (i, j, dk) in the IB view, -1 outside the wall tiles
+    auto slot = [&](int i, int j, int dk) -> int64_t {
+      int kw = k1w + dk;
+      if (kw >= a.nz) kw -= a.nz;
+      int lz = (kw >> 2) - tz + 1;
+      if (lz < 0) lz += a.ntz;
+      else if (lz > 2) lz -= a.ntz;
+      const int r = (lz * 3 + ((j >> 2) - ty + 1)) * 3 + ((i >> 2) - tx + 1);
+      const int t = __shfl_sync(FULL, rt, r);  // every lane calls slot()
+      return t < 0 ? (int64_t)-1 : (int64_t)t * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (kw & 3);
+    };
+    // bound: the first minimum of one list of the window bounds the window
+    // minimum from above (1.5 is the reference's starting value); take the
+    // nearest wall node among those of the 8 lattice points around the node
+    float bound = 1.5f;
+    {
+      float dbest = 3.0e38f;
+      int mbest = 0;
+      const int ci = (int)floor(((double)xp - a.X0) / a.DX) + (lane & 1);
+      const int cj = (int)floor(((double)yp - a.Y0) / a.DX) + ((lane >> 1) & 1);
+      const int ck = (int)floor(((double)zp - a.Z0) / a.DX) + ((lane >> 2) & 1);
+      const bool in = lane < 8 && ci >= i1 && ci <= i2 && cj >= j1 && cj <= j2 && ck >= k1 && ck <= k2;
+      // every lane calls slot(); lanes outside pass a window point
+      const int64_t sc = slot(in ? ci : i1, in ? cj : j1, in ? ck - k1 : 0);
+      if (in && sc >= 0) {
+        const int wi = a.windex[sc];
+        const float4 wn = a.wnode[sc];
+        if (wi > 0) {
+          dbest = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
+          mbest = wi;
         }
       }
-      if (rel < 0) {
-        const int ni = i2 - i1 + 1, nj = j2 - j1 + 1, nk = k2 - k1 + 1;
-        const int k1w = wrapk(a, k1);
-        const int npts = ni * nj * nk;
-        // lane l starts at window point l and steps 32 points in mixed radix;
-        // (i, j, dk) with the wrapped z index kw = k1w + dk (minus nz past the end)
-        const int sk = 32 % nk, sj = (32 / nk) % nj, si = 32 / (nk * nj);
-        const int pi0 = i1 + lane / (nj * nk), pj0 = j1 + (lane / nk) % nj, pk0 = lane % nk;
-        auto step = [&](int& i, int& j, int& dk) {
-          dk += sk;
-          int cy = 0;
-          if (dk >= nk) {
-            dk -= nk;
-            cy = 1;
-          }
-          j += sj + cy;
-          cy = 0;
-          if (j > j2) {
-            j -= nj;
-            cy = 1;
-          }
-          i += si + cy;
-        };
-        // slot of window point (i, j, dk) in the IB view, -1 outside the wall tiles
-        auto slot = [&](int i, int j, int dk) -> int64_t {
-          int kw = k1w + dk;
-          if (kw >= a.nz) kw -= a.nz;
-          int lz = (kw >> 2) - tz + 1;
-          if (lz < 0) lz += a.ntz;
-          else if (lz > 2) lz -= a.ntz;
-          const int r = (lz * 3 + ((j >> 2) - ty + 1)) * 3 + ((i >> 2) - tx + 1);
-          const int t = __shfl_sync(FULL, rt, r);  // every lane calls slot()
-          return t < 0 ? (int64_t)-1 : (int64_t)t * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (kw & 3);
-        };
-        // bound: the first minimum of one list of the window bounds the window
-        // minimum from above (1.5 is the reference's starting value); take the
-        // nearest wall node among those of the 8 lattice points around the node
-        float bound = 1.5f;
-        {
-          float dbest = 3.0e38f;
-          int mbest = 0;
-          const int ci = (int)floor(((double)xp - a.X0) / a.DX) + (lane & 1);
-          const int cj = (int)floor(((double)yp - a.Y0) / a.DX) + ((lane >> 1) & 1);
-          const int ck = (int)floor(((double)zp - a.Z0) / a.DX) + ((lane >> 2) & 1);
-          const bool in = lane < 8 && ci >= i1 && ci <= i2 && cj >= j1 && cj <= j2 && ck >= k1 && ck <= k2;
-          // every lane calls slot(); lanes outside pass a window point
-          const int64_t sc = slot(in ? ci : i1, in ? cj : j1, in ? ck - k1 : 0);
-          if (in && sc >= 0) {
-            const int wi = a.windex[sc];
-            const float4 wn = a.wnode[sc];
-            if (wi > 0) {
-              dbest = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
-              mbest = wi;
-            }
-          }
-          float dmin = dbest;
-  #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
-          const unsigned at = __ballot_sync(FULL, dbest == dmin && mbest > 0);
-          if (at) {
-            const int m = __shfl_sync(FULL, mbest, __ffs(at) - 1);
-            int unused = -1;
-            wall_list_min(a, m, xp, yp, zp, bound, unused);
-          }
-        }
-        int last = 0, qn = 0;
-        auto flush = [&](int nb) {
-          __syncwarp();
-          float d = 3.0e38f;
-          int t = -1;
-          if (lane < nb) wall_list_min(a, queue[lane], xp, yp, zp, d, t);
-          float dmin = d;
-  #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
-          const unsigned at = __ballot_sync(FULL, d == dmin && t >= 0);
-          if (at && dmin < mindis) {
-            mindis = dmin;
-            triwall = __shfl_sync(FULL, t, __ffs(at) - 1);
-          }
-          const int rem = qn - nb;
-          const int tq = lane < rem ? queue[nb + lane] : 0;
-          __syncwarp();
-          if (lane < rem) queue[lane] = tq;
-          __syncwarp();
-          qn = rem;
-        };
-        {
-          int i = pi0, j = pj0, dk = pk0;
-          for (int p0 = 0; p0 < npts; p0 += 32) {
-            int wi = 0;
-            float4 wn = make_float4(0.f, 0.f, 0.f, -1.f);
-            const int64_t s = slot(i, j, dk);
-            if (p0 + lane < npts && s >= 0) {
-              wi = a.windex[s];
-              wn = a.wnode[s];
-            }
-            step(i, j, dk);
-            int prev = __shfl_up_sync(FULL, wi, 1);
-            if (lane == 0) prev = last;
-            last = __shfl_sync(FULL, wi, 31);
-            bool want = false;
-            if (wi > 0 && wi != prev) {
-              const float dm = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
-              want = !(dm - wn.w > fminf(bound, mindis) + 1e-4f);
-            }
-            const unsigned bal = __ballot_sync(FULL, want);
-            if (want) queue[qn + __popc(bal & ((1u << lane) - 1u))] = wi;
-            qn += __popc(bal);
-            while (qn >= 32) flush(32);
-          }
-          while (qn > 0) flush(min(qn, 32));
-        }
-      }  // rel < 0
-      if (triwall < 0 || lane != 0) continue;
-      // signed distance to the plane of the wall triangle, repulsion, :9055-9077
-      const int w1 = a.wtri[3 * triwall];
-      const float n0 = a.wnrm[triwall], n1 = a.wnrm[a.mt + triwall], n2 = a.wnrm[2 * a.mt + triwall];
-      const float ddx = xp - a.wxyz[w1], ddy = yp - a.wxyz[a.nw + w1],
-                  ddz = wrapd(zp - a.wxyz[2 * a.nw + w1], a.LZ);
-      const float dist = __fadd_rn(__fadd_rn(__fmul_rn(ddx, n0), __fmul_rn(ddy, n1)), __fmul_rn(ddz, n2));
-      if (dist < 0.25f && fabsf(dist) < 1.0f && node < c.nn) {
-        float repulf = (float)((0.25 - (double)dist) / 1.0);
-        if (dist < -0.75f) repulf = 1.f;
-        // nucleus nodes add to the membrane array at their own index, as the
-        // reference does (ZebraflowWT.c:9415-9430 write NODE_WALLREPUL[v][caps][node])
-        atomicAdd(&c.wrep[((size_t)0 * nc + cell) * c.nn + node], (float)((double)repulf * 1.e-04 * n0));
-        atomicAdd(&c.wrep[((size_t)1 * nc + cell) * c.nn + node], (float)((double)repulf * 1.e-04 * n1));
-        atomicAdd(&c.wrep[((size_t)2 * nc + cell) * c.nn + node], (float)((double)repulf * 1.e-04 * n2));
+      float dmin = dbest;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
+      const unsigned at = __ballot_sync(FULL, dbest == dmin && mbest > 0);
+      if (at) {
+        const int m = __shfl_sync(FULL, mbest, __ffs(at) - 1);
+        int unused = -1;
+        wall_list_min(a, m, xp, yp, zp, bound, unused);
       }
     }
+    int last = 0, qn = 0;
+    auto flush = [&](int nb) {
+      __syncwarp();
+      float d = 3.0e38f;
+      int t = -1;
+      if (lane < nb) wall_list_min(a, queue[lane], xp, yp, zp, d, t);
+      float dmin = d;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) dmin = fminf(dmin, __shfl_xor_sync(FULL, dmin, o));
+      const unsigned at = __ballot_sync(FULL, d == dmin && t >= 0);
+      if (at && dmin < mindis) {
+        mindis = dmin;
+        triwall = __shfl_sync(FULL, t, __ffs(at) - 1);
+      }
+      const int rem = qn - nb;
+      const int tq = lane < rem ? queue[nb + lane] : 0;
+      __syncwarp();
+      if (lane < rem) queue[lane] = tq;
+      __syncwarp();
+      qn = rem;
+    };
+    {
+      int i = pi0, j = pj0, dk = pk0;
+      for (int p0 = 0; p0 < npts; p0 += 32) {
+        int wi = 0;
+        float4 wn = make_float4(0.f, 0.f, 0.f, -1.f);
+        const int64_t s = slot(i, j, dk);
+        if (p0 + lane < npts && s >= 0) {
+          wi = a.windex[s];
+          wn = a.wnode[s];
+        }
+        step(i, j, dk);
+        int prev = __shfl_up_sync(FULL, wi, 1);
+        if (lane == 0) prev = last;
+        last = __shfl_sync(FULL, wi, 31);
+        bool want = false;
+        if (wi > 0 && wi != prev) {
+          const float dm = dist3(xp - wn.x, yp - wn.y, wrapd(zp - wn.z, a.LZ));
+          want = !(dm - wn.w > fminf(bound, mindis) + 1e-4f);
+        }
+        const unsigned bal = __ballot_sync(FULL, want);
+        if (want) queue[qn + __popc(bal & ((1u << lane) - 1u))] = wi;
+        qn += __popc(bal);
+        while (qn >= 32) flush(32);
+      }
+      while (qn > 0) flush(min(qn, 32));
+    }
+    if (triwall >= 0 && lane == 0) wall_repel(a, c, cell, node, xp, yp, zp, triwall);
   }
 }
 
@@ -2100,12 +2111,12 @@ int ib_interp_launch(zf_ctx* ctx) {
   ctx->launches += 1;
   if (a.nw > 0) {
     if (tiles_ok(a)) {
-      if (!ctx->node_tiles_valid) {
-        const int rc = ib_node_tiles_launch(ctx);
-        if (rc) return rc;
-      }
-      ZF_CUDA(cudaMemsetAsync(a.tile_ctr + 2, 0, sizeof(int32_t), ctx->stream));
-      k_wall_tiles<<<persistent_blocks(k_wall_tiles, kTileThreads), kTileThreads, 0, ctx->stream>>>(a, c);
+      // [0] queued nodes, [1] their work counter
+      ZF_CUDA(cudaMemsetAsync(a.wall_walk_ctr, 0, 2 * sizeof(int32_t), ctx->stream));
+      k_wall_nodes<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(a, c, a.wall_walk, a.wall_walk_ctr);
+      k_wall_walk<<<persistent_blocks(k_wall_walk, kTileThreads), kTileThreads, 0, ctx->stream>>>(
+          a, c, a.wall_walk, a.wall_walk_ctr, a.wall_walk_ctr + 1);
+      ctx->launches += 1;
     } else {
       k_ib_wall<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
           a, c);

@@ -168,6 +168,8 @@ struct IbArgs {
   const int32_t* wrel_cnt;      // [n_all*64]
   const int32_t* wrel_off;      // [n_all*64 + 1]
   const int32_t* wrel;          // 1-based wall node ids
+  int32_t* wall_walk;           // [n_cells*(nn+nnn)] nodes queued for the window walk
+  int32_t* wall_walk_ctr;       // [2] queued count, work counter
   const int32_t* wcand_off;     // [nw+1] WallHost::cand_off
   const float4* wcand;          // WallHost::cand
   // cell list of triangle centroids over population slots (CSR).  Bin keys
