@@ -180,7 +180,7 @@ class Case:
         if n_cells is None:
             n_cells = nc
         self.name, self.dims, self.g, self.seed = name, (nx, ny, nz), g, seed
-        self.b, _ = zf.gen_bifurcation(nx, ny, nz, Rp, Rd, ang)
+        self.b, self.layout = zf.gen_bifurcation(nx, ny, nz, Rp, Rd, ang)
         self.n_fluid = int((self.b > 0).sum())
         self.mesh = self.cells = self.wall = None
         self.n_cells = 0
@@ -444,6 +444,62 @@ def measure_adjoint(dev, stream, barrier, seed=2024, nsteps=500, t0=300, t1=500,
             "timing": "host wall clock around each call (one synchronisation at its end)"}
 
 
+def measure_c4(case, dev, stream, barrier, nsteps=2000, t0=1001, K=50, budget_gb=80.0):
+    """C4: the flux-split adjoint on the C1 workload (cells held at their
+    placed positions), forward in fp16 deviation storage, against the same
+    adjoint with fp32 deviation storage.  J = mean over steps t0..nsteps of
+    the share of the axial flux through the +x daughter's mid cross-section;
+    checkpoint interval K, whose memory (checkpoints + one segment of states)
+    must fit the budget.  Reports both costs and the fp16 gradient's error."""
+    import zebraflow_b200 as zf
+    nx = case.dims[0]
+    z2, z3 = case.layout[1], case.layout[2]
+    kp = int(round(0.5 * (z2 + z3)))
+    n = (0.0, 0.0, 1.0)
+    lst = np.argwhere(case.b >= 0) >> 2  # tiles holding listed points
+    n_tiles = int(np.unique((lst[:, 2] * 4096 + lst[:, 1]) * 4096 + lst[:, 0]).size)
+    res, grads = {}, {}
+    for name, st, esz in (("f32dev", zf.STORE_F32_DEV, 4), ("f16", zf.STORE_F16, 2)):
+        ctx = zf.Context(case.params(st), device=dev)
+        ctx.set_lattice(case.b)
+        if case.n_cells:
+            ctx.set_wall(*case.wall)
+            ctx.set_mesh(*case.mesh)
+            ctx.set_cells(*case.cells)
+        ctx.set_stream(stream.cuda_stream)
+        dom = ctx.domlist()
+        fluid = case.b[dom[:, 0], dom[:, 1], dom[:, 2]] > 0
+        plane = fluid & (dom[:, 2] == kp)
+        cx = 0.5 * (nx - 1)
+        p0 = np.nonzero(plane & (dom[:, 0] > cx))[0].astype(np.int32)
+        p1 = np.nonzero(plane & (dom[:, 0] < cx))[0].astype(np.int32)
+        ctx.flux_objective(20, 1, 20, p0, n, p1, n)  # warm-up
+        barrier()
+        t = time.perf_counter()
+        J = ctx.flux_objective(nsteps, t0, nsteps, p0, n, p1, n)
+        t_fwd = time.perf_counter() - t
+        barrier()
+        t = time.perf_counter()
+        Ja, g, gtau, gEs, gkb = ctx.flux_adjoint(nsteps, t0, nsteps, p0, n, p1, n, checkpoint=K)
+        t_adj = time.perf_counter() - t
+        ctx.set_stream(None)
+        ctx.close()
+        grads[name] = g.astype(np.float64)
+        # checkpoints and one segment of states, [tile][19][64] populations per state
+        states = -(-nsteps // K) + K + 1
+        res[name] = {"J": J, "forward_ms": round(1e3 * t_fwd, 2), "forward_and_adjoint_ms": round(1e3 * t_adj, 2),
+                     "gradient_cost_over_forward": round((t_adj - t_fwd) / t_fwd, 3), "dJ_dtau": gtau,
+                     "dJ_dEs": gEs, "dJ_dkb": gkb,
+                     "checkpoint_memory_gb": round(states * 19 * 64 * n_tiles * esz / 1e9, 2)}
+    g32, g16 = grads["f32dev"], grads["f16"]
+    return {"workload": case.name + "_flux_split", "steps": nsteps, "objective_window": [t0, nsteps],
+            "plane_k": kp, "checkpoint_interval": K, "memory_budget_gb": budget_gb,
+            "f32dev": res["f32dev"], "f16": res["f16"],
+            "f16_rel_l2_error_dJ_dfb": float(np.linalg.norm(g16 - g32) / np.linalg.norm(g32)),
+            "f16_rel_error_J": abs(res["f16"]["J"] - res["f32dev"]["J"]) / abs(res["f32dev"]["J"]),
+            "timing": "host wall clock around each call (one synchronisation at its end)"}
+
+
 def run_ours(args):
     world, rank, local = dist_setup()
     import torch
@@ -471,6 +527,8 @@ def run_ours(args):
 
     main_r = measure_storage(case, storage, args, dev, stream, barrier, sample_clocks=(rank == 0))
     adjoint = measure_adjoint(dev, stream, barrier) if args.adjoint else None
+    if adjoint is not None and case.n_cells:
+        adjoint = {"c3_wss": adjoint, "c4_flux_split_mixed_precision": measure_c4(case, dev, stream, barrier)}
     variants = {}
     for name in [v for v in args.variants.split(",") if v and v != args.storage]:
         variants[name] = (STORAGES[name], measure_storage(case, STORAGES[name], args, dev, stream,

@@ -342,8 +342,10 @@ int zf_wss(zf_ctx* ctx, const float* node_normals, double pgauge, float* wss, fl
  *   J = mean over steps t0..t1 (1 <= t0 <= t1 <= nsteps) of the mean over the
  *       patch's wall nodes of |WSS| (Pa) of the state after step t.
  * fb: [3][n_listed] per-node body-force field (DOMLIST order) or NULL (zero).
- * node_normals as in zf_wss.  Needs fp32 storage, halfway bounce-back and a
- * uniform tau.  Both calls leave the populations and BODYFORCE as they were.
+ * node_normals as in zf_wss.  Needs halfway bounce-back and a uniform tau;
+ * with fp16/bf16 population storage the forward runs in that storage and the
+ * adjoint (fp32) treats its rounding as the identity.  Both calls leave the
+ * populations and BODYFORCE as they were.
  * zf_wss_adjoint keeps the populations of every checkpoint_interval-th step,
  * recomputes each interval backwards from them, and returns J and
  * dJ/dfb ([3][n_listed], the same as dJ/dBODYFORCE), dJ/dtau, dJ/dEs and
@@ -354,6 +356,21 @@ int zf_wss_objective(zf_ctx* ctx, int nsteps, int t0, int t1, const int32_t* pat
 int zf_wss_adjoint(zf_ctx* ctx, int nsteps, int t0, int t1, const int32_t* patch, int n_patch,
                    const float* node_normals, const float* fb, int checkpoint_interval, double* J,
                    float* dJ_dfb, double* dJ_dtau, double* dJ_dEs, double* dJ_dkb);
+
+/* Flux-split objective and its adjoint (no counterpart in the reference): the
+ * same differentiated forward as zf_wss_objective, with
+ *   J = mean over steps t0..t1 of Q_0 / (Q_0 + Q_1),
+ *   Q_s = sum over the listed points pts_s (DOMLIST indices, 0-based, fluid
+ *         points, the two sets disjoint) of U . nrm_s,
+ * U the post-collision velocity (moments without force shift, as the
+ * reference's U, V, W, ZebraflowWT.c:6611-6614).  For two outlet
+ * cross-sections J is the share of the flow leaving through the first.
+ * Outputs as zf_wss_adjoint; the wall mesh is not needed. */
+int zf_flux_objective(zf_ctx* ctx, int nsteps, int t0, int t1, const int32_t* pts0, int n0, const float* nrm0,
+                      const int32_t* pts1, int n1, const float* nrm1, const float* fb, double* J);
+int zf_flux_adjoint(zf_ctx* ctx, int nsteps, int t0, int t1, const int32_t* pts0, int n0, const float* nrm0,
+                    const int32_t* pts1, int n1, const float* nrm1, const float* fb, int checkpoint_interval,
+                    double* J, float* dJ_dfb, double* dJ_dtau, double* dJ_dEs, double* dJ_dkb);
 
 /* nsteps iterations of the reference time loop (ZebraflowWT.c:5646-12190):
  * every iteration an LBM step; every `stagger`-th iteration also the

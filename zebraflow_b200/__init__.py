@@ -135,6 +135,11 @@ _SIGS = {
                                  C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p,
                                  C.POINTER(C.c_double), C.POINTER(C.c_double),
                                  C.POINTER(C.c_double)]),
+    "zf_flux_objective": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, _f32p, _i32p, C.c_int,
+                                    _f32p, C.c_void_p, C.POINTER(C.c_double)]),
+    "zf_flux_adjoint": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, _f32p, _i32p, C.c_int,
+                                  _f32p, C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p,
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "zf_gen_cells": (C.c_int, [_i32p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, C.c_int,
                                C.c_int, C.c_int, _f64p, C.c_int, _f64p, _f64p, C.c_double,
                                C.c_double, C.c_uint64, _f64p, _f64p, C.POINTER(C.c_int)]),
@@ -482,6 +487,28 @@ class Context:
         _check(lib().zf_wss_adjoint(self._h, nsteps, t0, t1, patch, patch.size, pn, pf, checkpoint,
                                     C.byref(J), g.ctypes.data_as(C.c_void_p), C.byref(gt),
                                     C.byref(ge), C.byref(gk)))
+        return J.value, g, gt.value, ge.value, gk.value
+
+    def flux_objective(self, nsteps, t0, t1, pts0, nrm0, pts1, nrm1, fb=None) -> float:
+        """J of zf_flux_objective (mean share of the flux through set 0)."""
+        p0, p1 = np.ascontiguousarray(pts0, np.int32), np.ascontiguousarray(pts1, np.int32)
+        n0, n1 = np.ascontiguousarray(nrm0, np.float32), np.ascontiguousarray(nrm1, np.float32)
+        _fb, pf = self._opt(fb, np.float32)
+        J = C.c_double()
+        _check(lib().zf_flux_objective(self._h, nsteps, t0, t1, p0, p0.size, n0, p1, p1.size, n1, pf,
+                                       C.byref(J)))
+        return J.value
+
+    def flux_adjoint(self, nsteps, t0, t1, pts0, nrm0, pts1, nrm1, fb=None, checkpoint=50):
+        """(J, dJ/dfb [3][n_listed], dJ/dtau, dJ/dEs, dJ/dkb) of zf_flux_adjoint."""
+        p0, p1 = np.ascontiguousarray(pts0, np.int32), np.ascontiguousarray(pts1, np.int32)
+        n0, n1 = np.ascontiguousarray(nrm0, np.float32), np.ascontiguousarray(nrm1, np.float32)
+        _fb, pf = self._opt(fb, np.float32)
+        g = np.zeros((3, self.n_listed), np.float32)
+        J, gt, ge, gk = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        _check(lib().zf_flux_adjoint(self._h, nsteps, t0, t1, p0, p0.size, n0, p1, p1.size, n1, pf, checkpoint,
+                                     C.byref(J), g.ctypes.data_as(C.c_void_p), C.byref(gt), C.byref(ge),
+                                     C.byref(gk)))
         return J.value, g, gt.value, ge.value, gk.value
 
     def wss(self, node_normals=None, pgauge=120.0):

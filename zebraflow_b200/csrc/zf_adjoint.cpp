@@ -1,5 +1,6 @@
-// Hand-written adjoint of the coupled step for a wall-shear-stress objective,
-// with checkpointing and recomputation (zf_wss_objective, zf_wss_adjoint).
+// Hand-written adjoint of the coupled step for a wall-shear-stress objective
+// or a flux-split objective, with checkpointing and recomputation
+// (zf_wss_objective / zf_wss_adjoint, zf_flux_objective / zf_flux_adjoint).
 //
 // The differentiated forward starts from the context's populations f_0 and
 // its cells, whose positions stay fixed over the window:
@@ -8,6 +9,8 @@
 //                                                        :5704-7535, plus a field)
 //   f_t = LBM(f_{t-1}; tau, BODYFORCE),   t = 1..N       (:6100-6145, bounce-back)
 //   J = 1/(t1-t0+1) sum_{t=t0..t1} 1/|P| sum_{m in P} |WSS_m(f_t)|   (W:319-369)
+//   or J = 1/(t1-t0+1) sum_{t=t0..t1} Q_0(f_t) / (Q_0(f_t) + Q_1(f_t)),
+//      Q_s = sum over the points of set s of U.n_s (outlet fluxes)
 // Gradients: dJ/dF_b (per listed point, the same as dJ/dBODYFORCE), dJ/dtau,
 // and dJ/dEs, dJ/dkb through the membrane forces: F_total = Es A(x) +
 // kb B(x) + C(x) at fixed positions (the springs' coefficients are
@@ -17,7 +20,11 @@
 //
 // Populations of every K-th step are kept; the backward pass recomputes each
 // segment of K steps from its checkpoint, keeps its states, and walks it
-// backwards with the adjoint kernel.
+// backwards with the adjoint kernel.  With 16-bit population storage the
+// forward and its recomputation round identically (step t always draws the
+// same stochastic-rounding bits), and the adjoint linearises the fp32
+// arithmetic around the stored states: the rounding itself is passed through
+// as the identity.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -45,13 +52,19 @@ struct DevBuf {
   }
 };
 
+enum Kind { kWss, kFlux };
+
 struct Setup {
   zf_ctx* c = nullptr;
+  Kind kind = kWss;
   size_t pop_bytes = 0;        // one population state
-  double weight = 0.0;         // 1 / (window length x patch size)
-  DevBuf nrm, patch, acc;      // normals [3][nw], patch ids, FP64 accumulator
-  DevBuf U;                    // velocities at the stencils' compact points [3][nu]
-  PatchStencil ps;             // the patch's WSS stencils
+  uint32_t step0 = 0;          // step number of the first forward step
+  double weight = 0.0;         // WSS: 1 / (window x patch size); flux: 1 / window
+  DevBuf nrm, patch, acc;      // WSS normals [3][nw], patch ids; FP64 accumulator
+  DevBuf U;                    // velocities at the compact points [3][nu]
+  DevBuf set, q;               // flux: set of each compact point, the two fluxes
+  float nrm6[6] = {};          // flux: the two sets' unit normals
+  PatchStencil ps;             // the objective's compact points (and WSS stencils)
   std::vector<std::pair<void*, size_t>> ps_bufs;
   std::vector<float> bf_save;  // BODYFORCE at entry (listed order)
   ~Setup() {
@@ -62,19 +75,27 @@ struct Setup {
   }
 };
 
-int check_args(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, int n_patch) {
-  if (!c || nsteps < 1 || t0 < 1 || t1 < t0 || t1 > nsteps || !patch || n_patch < 1) return ZF_ERR_ARG;
-  if (!c->lattice_set || c->wall_allocs.empty() || c->ib.nw == 0) {
-    set_error("WSS objective: lattice and wall must be set");
+// what both objectives need: the window, the flow model, a lattice
+int check_common(zf_ctx* c, int nsteps, int t0, int t1) {
+  if (!c || nsteps < 1 || t0 < 1 || t1 < t0 || t1 > nsteps) return ZF_ERR_ARG;
+  if (!c->lattice_set) {
+    set_error("adjoint: the lattice must be set");
     return ZF_ERR_STATE;
   }
-  if (c->p.storage != ZF_STORE_F32 && c->p.storage != ZF_STORE_F32_DEV) {
-    set_error("WSS adjoint: needs fp32 population storage");
+  if (c->p.wall_mode != ZF_WALL_HALFWAY_BB || c->p.tau_from_phase) {
+    set_error("adjoint: needs halfway bounce-back walls and a uniform tau");
     return ZF_ERR_ARG;
   }
-  if (c->p.wall_mode != ZF_WALL_HALFWAY_BB || c->p.tau_from_phase) {
-    set_error("WSS adjoint: needs halfway bounce-back walls and a uniform tau");
-    return ZF_ERR_ARG;
+  return ZF_OK;
+}
+
+int check_args(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, int n_patch) {
+  int rc = check_common(c, nsteps, t0, t1);
+  if (rc) return rc;
+  if (!patch || n_patch < 1) return ZF_ERR_ARG;
+  if (c->wall_allocs.empty() || c->ib.nw == 0) {
+    set_error("WSS objective: lattice and wall must be set");
+    return ZF_ERR_STATE;
   }
   for (int i = 0; i < n_patch; ++i)
     if (patch[i] < 0 || patch[i] >= c->ib.nw) {
@@ -84,24 +105,14 @@ int check_args(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, int 
   return ZF_OK;
 }
 
-// BODYFORCE := S F_total(x) + F_b; buffers for normals, patch, accumulator
-int setup(zf_ctx* c, int t0, int t1, const int32_t* patch, int n_patch, const float* normals,
-          const float* fb, Setup& S) {
+// BODYFORCE := S F_total(x) + F_b, saved first; the accumulator and velocities
+int setup_common(zf_ctx* c, const float* fb, Setup& S) {
   const size_t esz = c->p.storage == ZF_STORE_F32 || c->p.storage == ZF_STORE_F32_DEV ? 4 : 2;
-  S.c = c;
+  const size_t nl = (size_t)c->n_listed;
   S.pop_bytes = (size_t)ZF_Q * c->ns * esz;
-  S.weight = 1.0 / ((double)(t1 - t0 + 1) * n_patch);
-  const size_t nw = (size_t)c->ib.nw, nl = (size_t)c->n_listed;
+  S.step0 = (uint32_t)c->status.iter;
   int rc;
-  if ((rc = S.nrm.alloc(c, 3 * nw * sizeof(float)))) return rc;
-  if ((rc = S.patch.alloc(c, (size_t)n_patch * sizeof(int32_t)))) return rc;
   if ((rc = S.acc.alloc(c, sizeof(double)))) return rc;
-  ZF_CUDA(cudaMemcpyAsync(S.nrm.p, normals ? normals : c->ib.wnnrm, 3 * nw * sizeof(float),
-                          normals ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c->stream));
-  ZF_CUDA(cudaMemcpyAsync(S.patch.p, patch, (size_t)n_patch * sizeof(int32_t), cudaMemcpyHostToDevice,
-                          c->stream));
-  if ((rc = wss_patch_stencil(c, (const float*)S.nrm.p, (const int32_t*)S.patch.p, n_patch, S.ps, S.ps_bufs)))
-    return rc;
   if ((rc = S.U.alloc(c, 3 * (size_t)std::max(S.ps.nu, 1) * sizeof(float)))) return rc;
   S.bf_save.resize(3 * nl);
   if ((rc = lbm_gather_listed(c, c->d_force, 3, S.bf_save.data()))) return rc;
@@ -120,6 +131,89 @@ int setup(zf_ctx* c, int t0, int t1, const int32_t* patch, int n_patch, const fl
   return ZF_OK;
 }
 
+// WSS objective: normals, patch and its stencils
+int setup(zf_ctx* c, int t0, int t1, const int32_t* patch, int n_patch, const float* normals,
+          const float* fb, Setup& S) {
+  S.c = c;
+  S.kind = kWss;
+  S.weight = 1.0 / ((double)(t1 - t0 + 1) * n_patch);
+  const size_t nw = (size_t)c->ib.nw;
+  int rc;
+  if ((rc = S.nrm.alloc(c, 3 * nw * sizeof(float)))) return rc;
+  if ((rc = S.patch.alloc(c, (size_t)n_patch * sizeof(int32_t)))) return rc;
+  ZF_CUDA(cudaMemcpyAsync(S.nrm.p, normals ? normals : c->ib.wnnrm, 3 * nw * sizeof(float),
+                          normals ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c->stream));
+  ZF_CUDA(cudaMemcpyAsync(S.patch.p, patch, (size_t)n_patch * sizeof(int32_t), cudaMemcpyHostToDevice,
+                          c->stream));
+  if ((rc = wss_patch_stencil(c, (const float*)S.nrm.p, (const int32_t*)S.patch.p, n_patch, S.ps, S.ps_bufs)))
+    return rc;
+  return setup_common(c, fb, S);
+}
+
+// flux objective: the two point sets (listed ids, fluid points only, disjoint)
+// as compact points with their set, and the normals
+int setup_flux(zf_ctx* c, int t0, int t1, const int32_t* pts0, int n0, const float* nrm0, const int32_t* pts1,
+               int n1, const float* nrm1, const float* fb, Setup& S) {
+  S.c = c;
+  S.kind = kFlux;
+  S.weight = 1.0 / (double)(t1 - t0 + 1);
+  if (!pts0 || !pts1 || n0 < 1 || n1 < 1 || !nrm0 || !nrm1) return ZF_ERR_ARG;
+  for (int v = 0; v < 3; ++v) {
+    S.nrm6[v] = nrm0[v];
+    S.nrm6[3 + v] = nrm1[v];
+  }
+  const int64_t nl = c->n_listed;
+  std::vector<std::pair<int32_t, uint8_t>> pts;
+  pts.reserve((size_t)n0 + n1);
+  for (int s = 0; s < 2; ++s) {
+    const int32_t* p = s ? pts1 : pts0;
+    const int n = s ? n1 : n0;
+    for (int i = 0; i < n; ++i) {
+      const int32_t l = p[i];
+      if (l < 0 || l >= nl) {
+        set_error("flux objective: point %d out of range", l);
+        return ZF_ERR_ARG;
+      }
+      const int64_t d = ((int64_t)c->domlist[3 * l] * c->p.ny + c->domlist[3 * l + 1]) * c->p.nz +
+                        c->domlist[3 * l + 2];
+      const int32_t code = c->b_index[d];
+      if (code < 1 || code > 9) {
+        set_error("flux objective: point %d is not a fluid point", l);
+        return ZF_ERR_ARG;
+      }
+      pts.emplace_back(l, (uint8_t)s);
+    }
+  }
+  std::sort(pts.begin(), pts.end());
+  for (size_t i = 1; i < pts.size(); ++i)
+    if (pts[i].first == pts[i - 1].first) {
+      set_error("flux objective: point %d listed twice", pts[i].first);
+      return ZF_ERR_ARG;
+    }
+  // slots of the listed points, in the sorted order
+  std::vector<int32_t> dom(nl);
+  ZF_CUDA(cudaMemcpyAsync(dom.data(), c->d_dom_slot, nl * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  const int nu = (int)pts.size();
+  std::vector<int32_t> uslot(nu);
+  std::vector<uint8_t> set(nu);
+  for (int u = 0; u < nu; ++u) {
+    uslot[u] = dom[pts[u].first];
+    set[u] = pts[u].second;
+  }
+  int rc;
+  void* d_us = nullptr;
+  if ((rc = dev_alloc(c, &d_us, (size_t)nu * sizeof(int32_t)))) return rc;
+  S.ps_bufs.emplace_back(d_us, (size_t)nu * sizeof(int32_t));
+  if ((rc = S.set.alloc(c, (size_t)nu)) || (rc = S.q.alloc(c, 2 * sizeof(double)))) return rc;
+  ZF_CUDA(cudaMemcpyAsync(d_us, uslot.data(), (size_t)nu * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  ZF_CUDA(cudaMemcpyAsync(S.set.p, set.data(), (size_t)nu, cudaMemcpyHostToDevice, c->stream));
+  S.ps = PatchStencil{};
+  S.ps.nu = nu;
+  S.ps.uslot = (const int32_t*)d_us;
+  return setup_common(c, fb, S);
+}
+
 // BODYFORCE back as it was, and the moment planes of the context's populations
 int restore(zf_ctx* c, Setup& S) {
   int rc = lbm_scatter_listed(c, S.bf_save.data(), 3, c->d_force);
@@ -133,8 +227,46 @@ int restore(zf_ctx* c, Setup& S) {
 int objective_of(zf_ctx* c, const void* f, Setup& S) {
   int rc = lbm_moments_at(c, f, S.ps, (float*)S.U.p);
   if (rc) return rc;
+  if (S.kind == kFlux)
+    return flux_objective_launch(c, S.ps, (const uint8_t*)S.set.p, S.nrm6, (const float*)S.U.p, S.weight,
+                                 (double*)S.q.p, (double*)S.acc.p);
   return wss_patch_launch(c, S.ps, (const float*)S.nrm.p, (const float*)S.U.p, S.weight, (double*)S.acc.p);
 }
+
+// lam += dJ_t/df_t for the state f of a step in the window (gU: scratch of
+// 3 nu floats, zero on entry and on return)
+int objective_seed(zf_ctx* c, const void* f, Setup& S, float* gU, float* lam) {
+  int rc = lbm_moments_at(c, f, S.ps, (float*)S.U.p);
+  if (rc) return rc;
+  if (S.kind == kFlux)
+    rc = flux_adj_launch(c, S.ps, (const uint8_t*)S.set.p, S.nrm6, (const float*)S.U.p, S.weight, (double*)S.q.p,
+                         gU);
+  else
+    rc = wss_patch_adj_launch(c, S.ps, (const float*)S.nrm.p, (const float*)S.U.p, S.weight, gU);
+  if (rc) return rc;
+  return lbm_seed_at(c, f, S.ps, gU, lam);
+}
+
+// the forward from the context's populations: J over the window
+int run_objective(zf_ctx* c, int nsteps, int t0, int t1, Setup& S, double* J) {
+  int rc;
+  DevBuf a, b;
+  if ((rc = a.alloc(c, S.pop_bytes)) || (rc = b.alloc(c, S.pop_bytes))) return rc;
+  ZF_CUDA(cudaMemcpyAsync(a.p, c->d_f[c->cur], S.pop_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  ZF_CUDA(cudaMemsetAsync(S.acc.p, 0, sizeof(double), c->stream));
+  void* fin = a.p;
+  void* fout = b.p;
+  for (int t = 1; t <= nsteps; ++t) {
+    if ((rc = lbm_step_buffers(c, fin, fout, S.step0 + (uint32_t)(t - 1)))) return rc;
+    std::swap(fin, fout);
+    if (t >= t0 && t <= t1 && (rc = objective_of(c, fin, S))) return rc;
+  }
+  ZF_CUDA(cudaMemcpyAsync(J, S.acc.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return restore(c, S);
+}
+
+int run_adjoint(zf_ctx* c, int nsteps, int t0, int t1, int K, Setup& S, double* J, float* dJ_dfb,
+                double* dJ_dtau, double* dJ_dEs, double* dJ_dkb);
 
 }  // namespace
 
@@ -148,19 +280,7 @@ int zf_wss_objective(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch
   ZF_CUDA(cudaSetDevice(c->device));
   Setup S;
   if ((rc = setup(c, t0, t1, patch, n_patch, node_normals, fb, S))) return rc;
-  DevBuf a, b;
-  if ((rc = a.alloc(c, S.pop_bytes)) || (rc = b.alloc(c, S.pop_bytes))) return rc;
-  ZF_CUDA(cudaMemcpyAsync(a.p, c->d_f[c->cur], S.pop_bytes, cudaMemcpyDeviceToDevice, c->stream));
-  ZF_CUDA(cudaMemsetAsync(S.acc.p, 0, sizeof(double), c->stream));
-  void* fin = a.p;
-  void* fout = b.p;
-  for (int t = 1; t <= nsteps; ++t) {
-    if ((rc = lbm_step_buffers(c, fin, fout))) return rc;
-    std::swap(fin, fout);
-    if (t >= t0 && t <= t1 && (rc = objective_of(c, fin, S))) return rc;
-  }
-  ZF_CUDA(cudaMemcpyAsync(J, S.acc.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  return restore(c, S);
+  return run_objective(c, nsteps, t0, t1, S, J);
 }
 
 int zf_wss_adjoint(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, int n_patch,
@@ -168,11 +288,43 @@ int zf_wss_adjoint(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, 
                    float* dJ_dfb, double* dJ_dtau, double* dJ_dEs, double* dJ_dkb) {
   int rc = check_args(c, nsteps, t0, t1, patch, n_patch);
   if (rc) return rc;
-  const int K = checkpoint_interval;
-  if (K < 1) return ZF_ERR_ARG;
+  if (checkpoint_interval < 1) return ZF_ERR_ARG;
   ZF_CUDA(cudaSetDevice(c->device));
   Setup S;
   if ((rc = setup(c, t0, t1, patch, n_patch, node_normals, fb, S))) return rc;
+  return run_adjoint(c, nsteps, t0, t1, checkpoint_interval, S, J, dJ_dfb, dJ_dtau, dJ_dEs, dJ_dkb);
+}
+
+int zf_flux_objective(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* pts0, int n0, const float* nrm0,
+                      const int32_t* pts1, int n1, const float* nrm1, const float* fb, double* J) {
+  int rc = check_common(c, nsteps, t0, t1);
+  if (rc) return rc;
+  if (!J) return ZF_ERR_ARG;
+  ZF_CUDA(cudaSetDevice(c->device));
+  Setup S;
+  if ((rc = setup_flux(c, t0, t1, pts0, n0, nrm0, pts1, n1, nrm1, fb, S))) return rc;
+  return run_objective(c, nsteps, t0, t1, S, J);
+}
+
+int zf_flux_adjoint(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* pts0, int n0, const float* nrm0,
+                    const int32_t* pts1, int n1, const float* nrm1, const float* fb, int checkpoint_interval,
+                    double* J, float* dJ_dfb, double* dJ_dtau, double* dJ_dEs, double* dJ_dkb) {
+  int rc = check_common(c, nsteps, t0, t1);
+  if (rc) return rc;
+  if (checkpoint_interval < 1) return ZF_ERR_ARG;
+  ZF_CUDA(cudaSetDevice(c->device));
+  Setup S;
+  if ((rc = setup_flux(c, t0, t1, pts0, n0, nrm0, pts1, n1, nrm1, fb, S))) return rc;
+  return run_adjoint(c, nsteps, t0, t1, checkpoint_interval, S, J, dJ_dfb, dJ_dtau, dJ_dEs, dJ_dkb);
+}
+
+}  // extern "C"
+
+namespace {
+
+int run_adjoint(zf_ctx* c, int nsteps, int t0, int t1, int K, Setup& S, double* J, float* dJ_dfb,
+                double* dJ_dtau, double* dJ_dEs, double* dJ_dkb) {
+  int rc;
   const int nseg = (nsteps + K - 1) / K;
   const size_t PB = S.pop_bytes;
   // checkpoints f_0, f_K, ...; the states of one segment; adjoint fields
@@ -196,7 +348,7 @@ int zf_wss_adjoint(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, 
     void* fin = SG;
     void* fout = SG + PB;
     for (int t = 1; t <= nsteps; ++t) {
-      if ((rc = lbm_step_buffers(c, fin, fout))) return rc;
+      if ((rc = lbm_step_buffers(c, fin, fout, S.step0 + (uint32_t)(t - 1)))) return rc;
       std::swap(fin, fout);
       if (t >= t0 && t <= t1 && (rc = objective_of(c, fin, S))) return rc;
       if (t % K == 0 && t / K < nseg)
@@ -217,17 +369,13 @@ int zf_wss_adjoint(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, 
     // states f_base .. f_{base+len} of this segment
     ZF_CUDA(cudaMemcpyAsync(SG, CK + (size_t)s * PB, PB, cudaMemcpyDeviceToDevice, c->stream));
     for (int i = 1; i <= len; ++i)
-      if ((rc = lbm_step_buffers(c, SG + (size_t)(i - 1) * PB, SG + (size_t)i * PB))) return rc;
+      if ((rc = lbm_step_buffers(c, SG + (size_t)(i - 1) * PB, SG + (size_t)i * PB,
+                                 S.step0 + (uint32_t)(base + i - 1))))
+        return rc;
     for (int i = len; i >= 1; --i) {
       const int t = base + i;
       const char* ft = SG + (size_t)i * PB;
-      if (t >= t0 && t <= t1) {  // dJ_t/df_t
-        if ((rc = lbm_moments_at(c, ft, S.ps, (float*)S.U.p))) return rc;
-        if ((rc = wss_patch_adj_launch(c, S.ps, (const float*)S.nrm.p, (const float*)S.U.p, S.weight,
-                                       (float*)gU.p)))
-          return rc;
-        if ((rc = lbm_seed_at(c, ft, S.ps, (float*)gU.p, L))) return rc;
-      }
+      if (t >= t0 && t <= t1 && (rc = objective_seed(c, ft, S, (float*)gU.p, L))) return rc;  // dJ_t/df_t
       if ((rc = lbm_adj_launch(c, SG + (size_t)(i - 1) * PB, L, Lp, (float*)gF.p, (double*)gw.p)))
         return rc;
       std::swap(L, Lp);
@@ -303,4 +451,4 @@ int zf_wss_adjoint(zf_ctx* c, int nsteps, int t0, int t1, const int32_t* patch, 
   return restore(c, S);
 }
 
-}  // extern "C"
+}  // namespace

@@ -1842,6 +1842,61 @@ __global__ void k_wss_patch_adj(IbArgs a, PatchStencil ps, const float* __restri
   }
 }
 
+// ---- flux-split objective ---------------------------------------------------------
+//
+// For two sets of listed points (outlet cross-sections) with unit normals n_0,
+// n_1: Q_s = sum over set s of U.n_s, U the moments (no force shift) of the
+// populations, and J = c Q_0 / (Q_0 + Q_1) for one state; the compact points
+// of `ps` are the points of both sets, set[u] telling which.  This objective
+// has no counterpart in the reference.
+struct Nrm6 {
+  float v[6];
+};
+
+__global__ void k_flux_q(PatchStencil ps, const uint8_t* __restrict__ set, Nrm6 n, const float* __restrict__ U,
+                         double* q) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  double q0 = 0.0, q1 = 0.0;
+  if (u < ps.nu) {
+    const int st = set[u];
+    const float* nn = n.v + 3 * st;
+    const double f = (double)U[u] * nn[0] + (double)U[ps.nu + u] * nn[1] + (double)U[2 * ps.nu + u] * nn[2];
+    if (st) q1 = f;
+    else q0 = f;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    q0 += __shfl_down_sync(0xffffffffu, q0, o);
+    q1 += __shfl_down_sync(0xffffffffu, q1, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (q0 != 0.0) atomicAdd(&q[0], q0);
+    if (q1 != 0.0) atomicAdd(&q[1], q1);
+  }
+}
+
+__global__ void k_flux_j(const double* __restrict__ q, double c, double* acc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const double den = q[0] + q[1];
+    if (den != 0.0) *acc += c * q[0] / den;
+  }
+}
+
+// gU[3][nu] += c dJ/dU:  dJ/dQ_0 = Q_1/(Q_0+Q_1)^2, dJ/dQ_1 = -Q_0/(Q_0+Q_1)^2
+__global__ void k_flux_gu(PatchStencil ps, const uint8_t* __restrict__ set, Nrm6 n, const double* __restrict__ q,
+                          double c, float* __restrict__ gU) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= ps.nu) return;
+  const double den = q[0] + q[1];
+  if (den == 0.0) return;
+  const int st = set[u];
+  const double g = c * (st ? -q[0] : q[1]) / (den * den);
+  const float* nn = n.v + 3 * st;
+  gU[u] += (float)(g * nn[0]);
+  gU[ps.nu + u] += (float)(g * nn[1]);
+  gU[2 * ps.nu + u] += (float)(g * nn[2]);
+}
+
 // transpose of the spreading (k_ib_spread without the repulsion term): for
 // every node, g_v = force_scale sum_s w(s) G_v(s) over the spreading stencil
 __global__ void k_spread_adj(IbArgs a, CellArgs c, int spread_walls, const float* __restrict__ G,
@@ -1994,6 +2049,32 @@ int wss_patch_adj_launch(zf_ctx* ctx, const PatchStencil& ps, const float* d_nrm
   k_wss_patch_adj<<<(ps.np + 127) / 128, 128, 0, ctx->stream>>>(ctx->ib, ps, d_nrm, d_U, c, d_gU);
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 1;
+  return ZF_OK;
+}
+
+int flux_objective_launch(zf_ctx* ctx, const PatchStencil& ps, const uint8_t* d_set, const float* nrm6,
+                          const float* d_U, double c, double* d_q, double* d_acc) {
+  if (ps.nu <= 0) return ZF_OK;
+  Nrm6 n;
+  for (int i = 0; i < 6; ++i) n.v[i] = nrm6[i];
+  ZF_CUDA(cudaMemsetAsync(d_q, 0, 2 * sizeof(double), ctx->stream));
+  k_flux_q<<<(ps.nu + 255) / 256, 256, 0, ctx->stream>>>(ps, d_set, n, d_U, d_q);
+  k_flux_j<<<1, 32, 0, ctx->stream>>>(d_q, c, d_acc);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 2;
+  return ZF_OK;
+}
+
+int flux_adj_launch(zf_ctx* ctx, const PatchStencil& ps, const uint8_t* d_set, const float* nrm6, const float* d_U,
+                    double c, double* d_q, float* d_gU) {
+  if (ps.nu <= 0) return ZF_OK;
+  Nrm6 n;
+  for (int i = 0; i < 6; ++i) n.v[i] = nrm6[i];
+  ZF_CUDA(cudaMemsetAsync(d_q, 0, 2 * sizeof(double), ctx->stream));
+  k_flux_q<<<(ps.nu + 255) / 256, 256, 0, ctx->stream>>>(ps, d_set, n, d_U, d_q);
+  k_flux_gu<<<(ps.nu + 255) / 256, 256, 0, ctx->stream>>>(ps, d_set, n, d_q, c, d_gU);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 2;
   return ZF_OK;
 }
 

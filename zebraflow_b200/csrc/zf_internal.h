@@ -236,12 +236,19 @@ int wss_patch_launch(zf_ctx* c, const PatchStencil& ps, const float* d_nrm, cons
                      double* d_acc);
 int wss_patch_adj_launch(zf_ctx* c, const PatchStencil& ps, const float* d_nrm, const float* d_U, double w,
                          float* d_gU);
+// flux-split objective over compact points of two sets (set[u] = 0 or 1,
+// unit normals n[0..2], n[3..5]): q[0..1] := sum_u U.n_set, then
+// acc += w q0/(q0+q1); the adjoint writes gU = w d(q0/(q0+q1))/dU
+int flux_objective_launch(zf_ctx* c, const PatchStencil& ps, const uint8_t* d_set, const float* nrm6,
+                          const float* d_U, double w, double* d_q, double* d_acc);
+int flux_adj_launch(zf_ctx* c, const PatchStencil& ps, const uint8_t* d_set, const float* nrm6,
+                    const float* d_U, double w, double* d_q, float* d_gU);
 // velocities U[3][nu] of the populations f at the compact points
 int lbm_moments_at(zf_ctx* c, const void* f, const PatchStencil& ps, float* d_U);
 // lam += seed of gU[3][nu] at the compact points (f: the state the objective
 // read); clears gU
 int lbm_seed_at(zf_ctx* c, const void* f, const PatchStencil& ps, float* d_gU, float* lam);
-int lbm_step_buffers(zf_ctx* c, const void* fin, void* fout);
+int lbm_step_buffers(zf_ctx* c, const void* fin, void* fout, uint32_t step);
 int spread_adj_launch(zf_ctx* c, const float* d_G, float* d_gmem, float* d_gnuc);
 int scale_springs_launch(zf_ctx* c, float s);
 int wss_launch(zf_ctx* c, const float* d_normals, double pgauge, float* d_wss, float* d_press,

@@ -654,7 +654,7 @@ int lbm_moments_launch(zf_ctx* c) {
 //   dJ/dw   = sum_q lam_q (feq_q - f_q - S_q / (2 - w)).
 // gF accumulates dt dJ/dF (the sensitivity to BODYFORCE), gw per block dJ/dw.
 template <class C, typename I>
-__global__ void __launch_bounds__(kTilesPerBlock * ZF_TC, 3)
+__global__ void __launch_bounds__(kTilesPerBlock * ZF_TC, 4)
     k_lbm_adj(LbmArgs a, const float* __restrict__ lam, float* __restrict__ lam_prev,
               float* __restrict__ gF, double* __restrict__ gw_partial) {
   __shared__ double s_gw[kTilesPerBlock * ZF_TC / 32];
@@ -670,63 +670,80 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC, 3)
     const I ns = (I)a.ns;
     const typename C::T* __restrict__ fin = static_cast<const typename C::T*>(a.fin);
     const PullBases<I> pb(a.nbr, tile, cell);
-    float f[ZF_Q];
-#pragma unroll
-    for (int q = 0; q < ZF_Q; ++q) f[q] = WQ(q) * (a.rho_ref + C::dec(fin[pb.pull(q, link)], q, a));
-    const float Fx = a.gx + a.force_dt * a.force[self], Fy = a.gy + a.force_dt * a.force[ns + self],
-                Fz = a.gz + a.force_dt * a.force[2 * ns + self];
-    float rho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+    const float* __restrict__ lp = lam + pb.b0;
+    // every sum over q below is a polynomial of degree <= 2 in c_q weighted by
+    // lam_q w_q, so it is built from the moments of lam: L0 = sum lam w,
+    // L1_a = sum lam w c_a, L2_ab = sum lam w c_a c_b, and LD = sum lam w d
+    // with d = f/w - rho_ref the populations' deviations
+    float drho = 0.f, mx = 0.f, my = 0.f, mz = 0.f, LD = 0.f, L0 = 0.f, L1x = 0.f, L1y = 0.f, L1z = 0.f;
+    float Lxx = 0.f, Lyy = 0.f, Lzz = 0.f, Lxy = 0.f, Lxz = 0.f, Lyz = 0.f;
 #pragma unroll
     for (int q = 0; q < ZF_Q; ++q) {
-      rho += f[q];
-      if (EX(q)) mx += EX(q) * f[q];
-      if (EY(q)) my += EY(q) * f[q];
-      if (EZ(q)) mz += EZ(q) * f[q];
+      const float d = C::dec(fin[pb.pull(q, link)], q, a);
+      const float l = lp[q * ZF_TC];
+      const float wd = WQ(q) * d;
+      drho += wd;
+      if (EX(q)) mx += EX(q) * wd;
+      if (EY(q)) my += EY(q) * wd;
+      if (EZ(q)) mz += EZ(q) * wd;
+      const float lw = WQ(q) * l;
+      LD = fmaf(lw, d, LD);
+      L0 += lw;
+      if (EX(q)) {
+        L1x += EX(q) * lw;
+        Lxx += lw;
+      }
+      if (EY(q)) {
+        L1y += EY(q) * lw;
+        Lyy += lw;
+      }
+      if (EZ(q)) {
+        L1z += EZ(q) * lw;
+        Lzz += lw;
+      }
+      if (EX(q) && EY(q)) Lxy += EX(q) * EY(q) * lw;
+      if (EX(q) && EZ(q)) Lxz += EX(q) * EZ(q) * lw;
+      if (EY(q) && EZ(q)) Lyz += EY(q) * EZ(q) * lw;
     }
-    const float irho = 1.f / rho;
+    const float Fx = a.gx + a.force_dt * a.force[self], Fy = a.gy + a.force_dt * a.force[ns + self],
+                Fz = a.gz + a.force_dt * a.force[2 * ns + self];
+    const float rho = a.rho_ref + drho, irho = 1.f / rho;
     const float ux = (mx + 0.5f * Fx) * irho, uy = (my + 0.5f * Fy) * irho, uz = (mz + 0.5f * Fz) * irho;
     const float om = 1.f / a.tau, sfac = 1.f - 0.5f * om;
     const float usq = ux * ux + uy * uy + uz * uz, uF = ux * Fx + uy * Fy + uz * Fz;
-    float A = 0.f, Bx = 0.f, By = 0.f, Bz = 0.f, gFx = 0.f, gFy = 0.f, gFz = 0.f, gwp = 0.f;
-    const float* __restrict__ lp = lam + pb.b0;
-#pragma unroll
-    for (int q = 0; q < ZF_Q; ++q) {
-      const float l = lp[q * ZF_TC];
-      const float cu = EX(q) * ux + EY(q) * uy + EZ(q) * uz;
-      const float cF = EX(q) * Fx + EY(q) * Fy + EZ(q) * Fz;
-      const float poly = 1.f + 3.f * cu + 4.5f * cu * cu - 1.5f * usq;
-      const float feq = WQ(q) * rho * poly;
-      const float S = sfac * WQ(q) * (3.f * (cF - uF) + 9.f * cu * cF);
-      A += l * WQ(q) * poly;
-      const float e = om * WQ(q) * rho, sw = sfac * WQ(q);
-      // d feq/d u_a = w_q rho (3 c_a + 9 cu c_a - 3 u_a); d S/d u_a = sw (9 c_a cF - 3 F_a)
-      Bx += l * (e * (3.f * EX(q) + 9.f * cu * EX(q) - 3.f * ux) + sw * (9.f * EX(q) * cF - 3.f * Fx));
-      By += l * (e * (3.f * EY(q) + 9.f * cu * EY(q) - 3.f * uy) + sw * (9.f * EY(q) * cF - 3.f * Fy));
-      Bz += l * (e * (3.f * EZ(q) + 9.f * cu * EZ(q) - 3.f * uz) + sw * (9.f * EZ(q) * cF - 3.f * Fz));
-      // d S/d F_a at fixed u
-      gFx += l * sw * (3.f * (EX(q) - ux) + 9.f * cu * EX(q));
-      gFy += l * sw * (3.f * (EY(q) - uy) + 9.f * cu * EY(q));
-      gFz += l * sw * (3.f * (EZ(q) - uz) + 9.f * cu * EZ(q));
-      // d f'/d w = feq - f - S/(2 - w) ... written through sfac: dS/dw = -S/(2 sfac)
-      gwp += l * (feq - f[q] - 0.5f * WQ(q) * (3.f * (cF - uF) + 9.f * cu * cF));
-    }
-    gw = (double)gwp;
-    A *= om;
-    gFx += 0.5f * Bx * irho;
-    gFy += 0.5f * By * irho;
-    gFz += 0.5f * Bz * irho;
+    // L2 u and L2 F
+    const float U2x = Lxx * ux + Lxy * uy + Lxz * uz, U2y = Lxy * ux + Lyy * uy + Lyz * uz,
+                U2z = Lxz * ux + Lyz * uy + Lzz * uz;
+    const float F2x = Lxx * Fx + Lxy * Fy + Lxz * Fz, F2y = Lxy * Fx + Lyy * Fy + Lyz * Fz,
+                F2z = Lxz * Fx + Lyz * Fy + Lzz * Fz;
+    // sum_q lam_q w_q (1 + 3 c.u + 4.5 (c.u)^2 - 1.5 u.u) = L0 + Adev
+    const float Adev = -1.5f * usq * L0 + 3.f * (ux * L1x + uy * L1y + uz * L1z) +
+                       4.5f * (ux * U2x + uy * U2y + uz * U2z);
+    const float Araw = L0 + Adev;
+    // B_a = w rho (3 L1_a + 9 (L2 u)_a - 3 u_a L0) + sfac (9 (L2 F)_a - 3 F_a L0)
+    const float orho = om * rho;
+    const float Bx = orho * (3.f * L1x + 9.f * U2x - 3.f * ux * L0) + sfac * (9.f * F2x - 3.f * Fx * L0);
+    const float By = orho * (3.f * L1y + 9.f * U2y - 3.f * uy * L0) + sfac * (9.f * F2y - 3.f * Fy * L0);
+    const float Bz = orho * (3.f * L1z + 9.f * U2z - 3.f * uz * L0) + sfac * (9.f * F2z - 3.f * Fz * L0);
+    // dJ/dF_a = sfac (3 L1_a - 3 u_a L0 + 9 (L2 u)_a) + B_a / (2 rho)
+    const float gFx = sfac * (3.f * (L1x - ux * L0) + 9.f * U2x) + 0.5f * Bx * irho;
+    const float gFy = sfac * (3.f * (L1y - uy * L0) + 9.f * U2y) + 0.5f * By * irho;
+    const float gFz = sfac * (3.f * (L1z - uz * L0) + 9.f * U2z) + 0.5f * Bz * irho;
     gF[self] += a.force_dt * gFx;
     gF[ns + self] += a.force_dt * gFy;
     gF[2 * ns + self] += a.force_dt * gFz;
+    // dJ/dw = sum lam (feq - f) - 1/2 sum lam w (3 (c.F - u.F) + 9 (c.u)(c.F)), with
+    // sum lam (feq - f) = sum lam w (rho poly - rho_ref - d) = rho_ref Adev + drho Araw - LD:
+    // differences of O(u) terms, not of O(1) sums
+    gw = (double)(a.rho_ref * Adev + drho * Araw - LD -
+                  0.5f * (3.f * (Fx * L1x + Fy * L1y + Fz * L1z) - 3.f * uF * L0 + 9.f * (ux * F2x + uy * F2y + uz * F2z)));
+    // lam_in_q = (1 - w) lam_q + w Araw + B.(c_q - u)/rho; lam is read again
+    // (an L1/L2 hit) and the pull sources recomputed rather than held
     const float om1 = 1.f - om;
-    // lam is read again (an L1/L2 hit) and the pull sources recomputed, rather
-    // than both held in registers across the accumulation
+    const float bx = Bx * irho, by = By * irho, bz = Bz * irho;
+    const float A0 = om * Araw - (bx * ux + by * uy + bz * uz);
 #pragma unroll
-    for (int q = 0; q < ZF_Q; ++q) {
-      const float li =
-          om1 * lp[q * ZF_TC] + A + (Bx * (EX(q) - ux) + By * (EY(q) - uy) + Bz * (EZ(q) - uz)) * irho;
-      lam_prev[pb.pull(q, link)] = li;
-    }
+    for (int q = 0; q < ZF_Q; ++q) lam_prev[pb.pull(q, link)] = fmaf(om1, lp[q * ZF_TC], A0) + cdot(q, bx, by, bz);
   }
   // per-block sum of dJ/dw (uniform branch)
 #pragma unroll
@@ -853,11 +870,14 @@ int lbm_seed_at(zf_ctx* c, const void* f, const PatchStencil& ps, float* d_gU, f
 }
 
 // forward step from explicit population buffers (the body force and
-// parameters of the context; no moments, no force clearing)
-int lbm_step_buffers(zf_ctx* c, const void* fin, void* fout) {
+// parameters of the context; no moments, no force clearing); `step` seeds the
+// stochastic rounding of the 16-bit forms, so a step recomputed with the same
+// number reproduces its populations bit for bit
+int lbm_step_buffers(zf_ctx* c, const void* fin, void* fout, uint32_t step) {
   LbmArgs a = make_args(c);
   a.fin = fin;
   a.fout = fout;
+  a.step = step;
   dispatch_storage<StepBuffers>(c->p.storage, c, a);
   ZF_CUDA(cudaGetLastError());
   c->launches += (c->n_active > 0) + (c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0);
