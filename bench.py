@@ -424,14 +424,16 @@ def measure_adjoint(dev, stream, barrier, seed=2024, nsteps=500, t0=300, t1=500,
     ctx.set_cells(x, xn)
     ctx.set_stream(stream.cuda_stream)
     ctx.wss_objective(nsteps, t0, t1, patch)  # warm-up
-    barrier()
-    t = time.perf_counter()
-    J = ctx.wss_objective(nsteps, t0, t1, patch)
-    t_fwd = time.perf_counter() - t
-    barrier()
-    t = time.perf_counter()
-    Ja, gfb, gtau, gEs, gkb = ctx.wss_adjoint(nsteps, t0, t1, patch, checkpoint=K)
-    t_adj = time.perf_counter() - t
+    t_fwd = t_adj = float("inf")
+    for _ in range(3):  # fastest of three calls each (host wall clock)
+        barrier()
+        t = time.perf_counter()
+        J = ctx.wss_objective(nsteps, t0, t1, patch)
+        t_fwd = min(t_fwd, time.perf_counter() - t)
+        barrier()
+        t = time.perf_counter()
+        Ja, gfb, gtau, gEs, gkb = ctx.wss_adjoint(nsteps, t0, t1, patch, checkpoint=K)
+        t_adj = min(t_adj, time.perf_counter() - t)
     ctx.set_stream(None)
     ctx.close()
     return {"workload": "c3_tube_96x96x512_200rbc", "fluid_points": int((b > 0).sum()),
@@ -441,7 +443,7 @@ def measure_adjoint(dev, stream, barrier, seed=2024, nsteps=500, t0=300, t1=500,
             "gradient_cost_over_forward": round((t_adj - t_fwd) / t_fwd, 3),
             "J_pa": J, "dJ_dtau": gtau, "dJ_dEs": gEs, "dJ_dkb": gkb,
             "dJ_dfb_max": float(np.abs(gfb).max()),
-            "timing": "host wall clock around each call (one synchronisation at its end)"}
+            "timing": "host wall clock around each call (one synchronisation at its end), fastest of 3"}
 
 
 def measure_c4(case, dev, stream, barrier, nsteps=2000, t0=1001, K=50, budget_gb=80.0):
@@ -474,14 +476,16 @@ def measure_c4(case, dev, stream, barrier, nsteps=2000, t0=1001, K=50, budget_gb
         p0 = np.nonzero(plane & (dom[:, 0] > cx))[0].astype(np.int32)
         p1 = np.nonzero(plane & (dom[:, 0] < cx))[0].astype(np.int32)
         ctx.flux_objective(20, 1, 20, p0, n, p1, n)  # warm-up
-        barrier()
-        t = time.perf_counter()
-        J = ctx.flux_objective(nsteps, t0, nsteps, p0, n, p1, n)
-        t_fwd = time.perf_counter() - t
-        barrier()
-        t = time.perf_counter()
-        Ja, g, gtau, gEs, gkb = ctx.flux_adjoint(nsteps, t0, nsteps, p0, n, p1, n, checkpoint=K)
-        t_adj = time.perf_counter() - t
+        t_fwd = t_adj = float("inf")
+        for _ in range(2):  # faster of two calls each (host wall clock)
+            barrier()
+            t = time.perf_counter()
+            J = ctx.flux_objective(nsteps, t0, nsteps, p0, n, p1, n)
+            t_fwd = min(t_fwd, time.perf_counter() - t)
+            barrier()
+            t = time.perf_counter()
+            Ja, g, gtau, gEs, gkb = ctx.flux_adjoint(nsteps, t0, nsteps, p0, n, p1, n, checkpoint=K)
+            t_adj = min(t_adj, time.perf_counter() - t)
         ctx.set_stream(None)
         ctx.close()
         grads[name] = g.astype(np.float64)
@@ -497,7 +501,7 @@ def measure_c4(case, dev, stream, barrier, nsteps=2000, t0=1001, K=50, budget_gb
             "f32dev": res["f32dev"], "f16": res["f16"],
             "f16_rel_l2_error_dJ_dfb": float(np.linalg.norm(g16 - g32) / np.linalg.norm(g32)),
             "f16_rel_error_J": abs(res["f16"]["J"] - res["f32dev"]["J"]) / abs(res["f32dev"]["J"]),
-            "timing": "host wall clock around each call (one synchronisation at its end)"}
+            "timing": "host wall clock around each call (one synchronisation at its end), faster of 2"}
 
 
 def run_ours(args):
