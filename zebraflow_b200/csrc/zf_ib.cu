@@ -21,6 +21,7 @@
 // locals.  Sums of distances that pick a nearest triangle use non-contracted
 // fp32 operations so that ties resolve as on the CPU.
 #include <algorithm>
+#include <climits>
 
 #include "zf_internal.h"
 
@@ -1568,6 +1569,114 @@ __global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
   }
 }
 
+// k_ib_spread per lattice tile of nodes (node-tile lists): a block takes a
+// tile, adds its nodes' stencil contributions into shared memory over the
+// 12x12x12 points of the tile's 3x3x3 neighbourhood (a node's stencil stays
+// inside it), then adds each touched point to BODYFORCE once.  Neighbouring
+// nodes share most stencil points, so the global float atomics drop several
+// times.  The nodes' own updates (NODE_VEL += NODE_WALLREPUL, :10749-10754)
+// happen once per node in the first pass.  A contribution outside the
+// neighbourhood (not expected) goes straight to BODYFORCE.
+constexpr int kSpreadNodes = 256;  // nodes staged per pass
+__global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int spread_walls) {
+  __shared__ float acc[3][1728];
+  __shared__ float s_pos[3][kSpreadNodes], s_f[3][kSpreadNodes];
+  __shared__ int s_b[3][kSpreadNodes], s_c[3][kSpreadNodes];  // stencil corner, lat_index
+  __shared__ int s_li;
+  const int nc = c.n_cells;
+  const int nlist = a.tile_ctr[0];
+  const float h2 = 2.f * a.DX;
+  for (;;) {
+    if (threadIdx.x == 0) s_li = atomicAdd(&a.tile_ctr[3], 1);
+    __syncthreads();
+    const int li = s_li;
+    if (li >= nlist) break;
+    float* accf = &acc[0][0];
+    for (int e = threadIdx.x; e < 3 * 1728; e += blockDim.x) accf[e] = 0.f;
+    const int gt = a.tile_list[li];
+    const int tx = gt % a.ntx, ty = (gt / a.ntx) % a.nty, tz = gt / (a.ntx * a.nty);
+    const int ox = (tx - 1) * 4, oy = (ty - 1) * 4, oz = (tz - 1) * 4;
+    const int n0 = a.node_off[gt], n1 = a.node_off[gt + 1];
+    for (int c0 = n0; c0 < n1; c0 += kSpreadNodes) {
+      const int cnt = min(kSpreadNodes, n1 - c0);
+      __syncthreads();  // the previous chunk's items are done with the staged nodes
+      if ((int)threadIdx.x < cnt) {
+        const int t = threadIdx.x;
+        bool nuc;
+        int cell, node;
+        s_b[0][t] = INT_MIN;  // inactive node
+        if (node_of(c, a.node_sorted[c0 + t], nuc, cell, node)) {
+          const int n = nuc ? c.nnn : c.nn;
+          double* V = nuc ? c.vel_n : c.vel;
+          const float* R = nuc ? c.wrep_n : c.wrep;
+          const float* FT = nuc ? c.ftot_n : c.ftot;
+          for (int v = 0; v < 3; ++v) {  // :10749-10754
+            const size_t g = ((size_t)v * nc + cell) * n + node;
+            V[g] += (double)R[g];
+            s_f[v][t] = (float)((double)a.gamma_p * (double)R[g] + (double)FT[g]);
+          }
+          float xp, yp, zp;
+          node_pos(nuc ? c.xn : c.x, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
+          s_pos[0][t] = xp;
+          s_pos[1][t] = yp;
+          s_pos[2][t] = zp;
+          s_c[0][t] = lat_index(xp, a.X0, a.DX);
+          s_c[1][t] = lat_index(yp, a.Y0, a.DX);
+          s_c[2][t] = lat_index(zp, a.Z0, a.DX);
+          s_b[0][t] = (int)floor(((double)xp - a.X0) / a.DX) - 1;
+          s_b[1][t] = (int)floor(((double)yp - a.Y0) / a.DX) - 1;
+          s_b[2][t] = (int)floor(((double)zp - a.Z0) / a.DX) - 1;
+        }
+      }
+      __syncthreads();
+      for (int it = threadIdx.x; it < cnt * 64; it += blockDim.x) {
+        const int t = it >> 6, p = it & 63;
+        if (s_b[0][t] == INT_MIN) continue;
+        const int i = s_b[0][t] + (p >> 4), j = s_b[1][t] + ((p >> 2) & 3), k = s_b[2][t] + (p & 3);
+        const int i0 = s_c[0][t], j0 = s_c[1][t], k0 = s_c[2][t];
+        if (i < 0 || i >= a.nx || i < i0 - 4 || i > i0 + 4) continue;
+        if (j < 0 || j >= a.ny || j < j0 - 4 || j > j0 + 4) continue;
+        if (k < a.kmin || k > a.kmax || k < k0 - 4 || k > k0 + 4) continue;
+        const int kw = wrapk(a, k);
+        const int64_t sl = slot_of(a, i, j, kw);
+        if (sl < 0 || sl >= a.ns) continue;
+        const uint8_t cd = a.code[sl];
+        if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) continue;
+        const float xc = (float)((double)a.X0 + i * (double)a.DX);
+        const float yc = (float)((double)a.Y0 + j * (double)a.DX);
+        const float zc = (float)((double)a.Z0 + k * (double)a.DX);
+        const float dx = xc - s_pos[0][t], dy = yc - s_pos[1][t], dz = zc - s_pos[2][t];
+        if (!(dist3(dx, dy, dz) <= h2)) continue;
+        const float w = peskin(dx, dy, dz, h2);
+        const int di = i - ox, dj = j - oy;
+        int dk = k - oz;
+        if (a.per_z) dk = ((dk % a.nz) + a.nz) % a.nz;
+        const bool in = di >= 0 && di < 12 && dj >= 0 && dj < 12 && dk >= 0 && dk < 12;
+        for (int v = 0; v < 3; ++v) {
+          const float val = (float)((double)(w * s_f[v][t]) * (double)a.force_scale);
+          if (in) atomicAdd(&acc[v][(dk * 12 + dj) * 12 + di], val);
+          else atomicAdd(&a.force[v * a.ns + sl], val);
+        }
+      }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < 1728; r += blockDim.x) {
+      const float fx = acc[0][r], fy = acc[1][r], fz = acc[2][r];
+      if (fx == 0.f && fy == 0.f && fz == 0.f) continue;
+      const int i = ox + r % 12, j = oy + (r / 12) % 12;
+      int k = oz + r / 144;
+      if (a.per_z) k = ((k % a.nz) + a.nz) % a.nz;
+      if (i < 0 || i >= a.nx || j < 0 || j >= a.ny || k < 0 || k >= a.nz) continue;
+      const int64_t sl = slot_of(a, i, j, k);
+      if (sl < 0 || sl >= a.ns) continue;
+      atomicAdd(&a.force[sl], fx);
+      atomicAdd(&a.force[a.ns + sl], fy);
+      atomicAdd(&a.force[2 * a.ns + sl], fz);
+    }
+    __syncthreads();
+  }
+}
+
 // ---- position update ------------------------------------------------------------
 
 __global__ void k_update(IbArgs a, CellArgs c) {
@@ -2267,10 +2376,20 @@ int ib_rbc_rbc_launch(zf_ctx* ctx) {
 
 int ib_spread_launch(zf_ctx* ctx) {
   const CellArgs& c = ctx->cells;
+  IbArgs& a = ctx->ib;
   const int64_t n = (int64_t)c.n_cells * (c.nn + c.nnn);
   if (n == 0) return ZF_OK;
-  k_ib_spread<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
-      ctx->ib, c, ctx->p.wall_mode == ZF_WALL_REF_EQ);
+  if (tiles_ok(a) && !ctx->ib_allocs.empty()) {
+    if (!ctx->node_tiles_valid) {
+      const int rc = ib_node_tiles_launch(ctx);
+      if (rc) return rc;
+    }
+    ZF_CUDA(cudaMemsetAsync(a.tile_ctr + 3, 0, sizeof(int32_t), ctx->stream));
+    k_spread_tiles<<<persistent_blocks(k_spread_tiles, 256), 256, 0, ctx->stream>>>(
+        a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ);
+  } else {
+    k_ib_spread<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ);
+  }
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 1;
   return ZF_OK;
