@@ -609,6 +609,80 @@ def run_ours(args):
     return 0
 
 
+def wall_node_normals(wall):
+    """Area-weighted unit normals of the wall mesh's nodes ([3][nw])."""
+    xyz, tri1, nrm = wall
+    t = tri1 - 1
+    p = xyz.T.astype(np.float64)
+    area = 0.5 * np.linalg.norm(np.cross(p[t[1]] - p[t[0]], p[t[2]] - p[t[0]]), axis=1)
+    acc = np.zeros((xyz.shape[1], 3))
+    for v in range(3):
+        np.add.at(acc, t[v], area[:, None] * nrm.T)
+    acc /= np.linalg.norm(acc, axis=1, keepdims=True)
+    return np.ascontiguousarray(acc.T, np.float32)
+
+
+def run_c2(args):
+    """Precision report on the workload itself (not a throughput line): the
+    FP64 CPU oracle runs `--c2-steps` iterations of the reference loop; each
+    storage form runs the same iterations on the GPU; the relative L2 errors of
+    the fluid velocity, the density deviation, the wall shear stress and the
+    membrane-node displacement are printed as one JSON line."""
+    import zebraflow_b200 as zf
+    case = Case(args.workload, args.cells, args.seed)
+    n = args.c2_steps
+    nrm = wall_node_normals(case.wall)
+    t0 = time.perf_counter()
+    lbm, oc, w = case.oracle_world("f64")
+    w.step(n)
+    D, U, V, W = lbm.moments()
+    wss_ref, _, _ = w.wss(nrm)
+    oget = oc.get()
+    x_ref, live_ref = oget["x"], oget["status"] > 0
+    t_oracle = time.perf_counter() - t0
+    for o in (w, oc, lbm):
+        o.close()
+    dom = np.argwhere(case.b >= 0)
+    fl = case.b[dom[:, 0], dom[:, 1], dom[:, 2]] > 0
+    u_ref, rho_ref = np.stack([U, V, W])[:, fl], (D - 1.0)[fl]
+    x0 = case.cells[0]
+
+    def rel(a, b):
+        ok = np.isfinite(a) & np.isfinite(b)  # wall nodes without a valid probe give no WSS
+        return float(np.linalg.norm((a - b)[ok]) / np.linalg.norm(b[ok]))
+
+    out, fields = {}, {}
+    for name in ("f32", "f32dev", "f16", "bf16"):
+        ctx = zf.Context(case.params(STORAGES[name]))
+        ctx.set_lattice(case.b)
+        ctx.set_wall(*case.wall)
+        ctx.set_mesh(*case.mesh)
+        ctx.set_cells(*case.cells)
+        ctx.step(n)
+        wss, _, _ = ctx.wss(nrm)
+        Dg, Ug, Vg, Wg = ctx.download_moments()
+        x, _, status = ctx.cells()
+        live = (status > 0) & live_ref  # cells alive in both runs
+        u = np.stack([Ug, Vg, Wg])[:, fl]
+        fields[name] = (u, (Dg - 1.0)[fl], wss, x - x0, live)
+        out[name] = {"u": rel(u, u_ref), "rho_minus_1": rel((Dg - 1.0)[fl], rho_ref), "wss": rel(wss, wss_ref),
+                     "displacement": rel((x - x0)[:, live], (x_ref - x0)[:, live]),
+                     "cells_removed": int((status <= 0).sum())}
+        ctx.close()
+    # each storage form against the fp32 GPU run (the storage's own effect)
+    u32, r32, w32, d32, l32 = fields["f32"]
+    vs32 = {}
+    for name in ("f32dev", "f16", "bf16"):
+        u, r, wv, dsp, live = fields[name]
+        both = live & l32
+        vs32[name] = {"u": rel(u, u32), "wss": rel(wv, w32), "displacement": rel(dsp[:, both], d32[:, both])}
+    print(json.dumps({"report": "c2_precision_against_fp64_oracle", "workload": case.name,
+                      "iterations": n, "membrane_blocks": n // 50, "fp64_oracle_seconds": round(t_oracle, 1),
+                      "oracle_cells_removed": int((~live_ref).sum()),
+                      "relative_l2_vs_fp64_oracle": out, "relative_l2_vs_fp32_gpu": vs32}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -627,8 +701,13 @@ def main():
     ap.add_argument("--reference-seconds", type=float, default=90.0)
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the adjoint cost measurement on the C3 tube")
+    ap.add_argument("--c2-steps", type=int, default=0,
+                    help="instead of the bench line, a precision report of this many iterations "
+                         "against the FP64 oracle")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.c2_steps > 0:
+        return run_c2(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -748,12 +748,18 @@ __device__ __forceinline__ void rbc_entry(const IbArgs& a, const CellArgs& c, in
     const float cy = (tp[kSubA[v]][1] + tp[kSubB[v]][1] + tp[kSubC[v]][1]) * third;
     const float cz = (tp[kSubA[v]][2] + tp[kSubB[v]][2] + tp[kSubC[v]][2]) * third;
     const float dx = cx - xc, dy = cy - yc, dz = cz - zc;
-    const float d = dist3(dx, dy, dz);
-    if (d < 1.0f) {
-      const float s = -8.333e-07f * (1.f - d) / d;
-      tx += s * dx;
-      ty += s * dy;
-      tz += s * dz;
+    // dist3 without its square root unless the squared distance is below 1
+    // (the square root is correctly rounded, so d < 1 implies d2 < 1; the
+    // second test keeps the reference's d < 1 exactly)
+    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    if (d2 < 1.0f) {
+      const float d = sqrtf(d2);
+      if (d < 1.0f) {
+        const float s = -8.333e-07f * (1.f - d) / d;
+        tx += s * dx;
+        ty += s * dy;
+        tz += s * dz;
+      }
     }
   }
 }
