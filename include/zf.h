@@ -196,6 +196,21 @@ int zf_lbm_step_mass(zf_ctx* ctx, int store_moments, int zero_bodyforce, double*
  * calls that overlap on the GPU share the scratch and race. */
 int zf_lbm_step_mass_noalloc(zf_ctx* ctx, int store_moments, int zero_bodyforce, double* mass);
 
+/* Z-slab halo exchange (no counterpart in the reference, which runs on one
+ * node).  A lattice cut into z slabs, one per GPU, each with one 4-plane tile
+ * layer of halo on either side, stays exact if after every step the halo
+ * plane next to each face receives, from the rank owning it, the populations
+ * the interior pulls across that face: those of the 5 directions with
+ * e_z = dir (+1: pulled upwards, -1: downwards) of the listed points of one
+ * plane.  zf_plane_count gives the number of listed points of plane z = k of
+ * this context's lattice; zf_plane_pack copies their dir-populations of the
+ * current state, in (x, y) order, into dev_buf ([n][5] storage elements: 4
+ * bytes each for the fp32 forms, 2 for fp16/bf16; device memory, written on
+ * the context's stream); zf_plane_unpack writes such a buffer into plane k. */
+int zf_plane_count(zf_ctx* ctx, int k, int32_t* n);
+int zf_plane_pack(zf_ctx* ctx, int k, int dir, void* dev_buf);
+int zf_plane_unpack(zf_ctx* ctx, int k, int dir, const void* dev_buf);
+
 /* Sets the uniform effective body force g (lattice units) used from the next step. */
 int zf_set_uniform_force(zf_ctx* ctx, const float* g3);
 

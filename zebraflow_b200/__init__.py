@@ -135,6 +135,9 @@ _SIGS = {
                                  C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p,
                                  C.POINTER(C.c_double), C.POINTER(C.c_double),
                                  C.POINTER(C.c_double)]),
+    "zf_plane_count": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int32)]),
+    "zf_plane_pack": (C.c_int, [_P, C.c_int, C.c_int, C.c_void_p]),
+    "zf_plane_unpack": (C.c_int, [_P, C.c_int, C.c_int, C.c_void_p]),
     "zf_flux_objective": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, _f32p, _i32p, C.c_int,
                                     _f32p, C.c_void_p, C.POINTER(C.c_double)]),
     "zf_flux_adjoint": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, _f32p, _i32p, C.c_int,
@@ -488,6 +491,20 @@ class Context:
                                     C.byref(J), g.ctypes.data_as(C.c_void_p), C.byref(gt),
                                     C.byref(ge), C.byref(gk)))
         return J.value, g, gt.value, ge.value, gk.value
+
+    def plane_count(self, k) -> int:
+        """Listed points of lattice plane z = k (zf_plane_count)."""
+        n = C.c_int32()
+        _check(lib().zf_plane_count(self._h, int(k), C.byref(n)))
+        return n.value
+
+    def plane_pack(self, k, direction, dev_ptr):
+        """zf_plane_pack into device memory at dev_ptr (an int address)."""
+        _check(lib().zf_plane_pack(self._h, int(k), int(direction), C.c_void_p(dev_ptr)))
+
+    def plane_unpack(self, k, direction, dev_ptr):
+        """zf_plane_unpack from device memory at dev_ptr (an int address)."""
+        _check(lib().zf_plane_unpack(self._h, int(k), int(direction), C.c_void_p(dev_ptr)))
 
     def flux_objective(self, nsteps, t0, t1, pts0, nrm0, pts1, nrm1, fb=None) -> float:
         """J of zf_flux_objective (mean share of the flux through set 0)."""

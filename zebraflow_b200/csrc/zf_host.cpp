@@ -147,6 +147,8 @@ static void free_lattice(zf_ctx* c) {
                   c->d_red};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  for (auto& pl : c->planes) cudaFree(pl.d_slots);
+  c->planes.clear();
   c->d_tile_map = c->d_active = c->d_nbr = nullptr;
   c->d_link = nullptr;
   c->d_code = nullptr;
@@ -569,6 +571,31 @@ int zf_mass(zf_ctx* c, int include_walls, double* mass) {
   NEED_LATTICE("zf_mass");
   if (!mass) return ZF_ERR_ARG;
   return lbm_mass(c, include_walls, mass);
+}
+
+// ---- z-slab halo exchange (no counterpart in the reference, which runs on one
+// node): the populations that cross a z face are those of the 5 directions
+// with e_z = dir of the listed points of one lattice plane.
+int zf_plane_count(zf_ctx* c, int k, int32_t* n) {
+  NEED_LATTICE("zf_plane_count");
+  if (!n) return ZF_ERR_ARG;
+  zf_ctx::PlaneSlots pl{};
+  const int rc = lbm_plane_slots(c, k, &pl);
+  if (rc) return rc;
+  *n = pl.n;
+  return ZF_OK;
+}
+
+int zf_plane_pack(zf_ctx* c, int k, int dir, void* dev_buf) {
+  NEED_LATTICE("zf_plane_pack");
+  if (dir != 1 && dir != -1) return ZF_ERR_ARG;
+  return lbm_plane_copy(c, k, dir, dev_buf, true);
+}
+
+int zf_plane_unpack(zf_ctx* c, int k, int dir, const void* dev_buf) {
+  NEED_LATTICE("zf_plane_unpack");
+  if (dir != 1 && dir != -1) return ZF_ERR_ARG;
+  return lbm_plane_copy(c, k, dir, const_cast<void*>(dev_buf), false);
 }
 
 }  // extern "C"

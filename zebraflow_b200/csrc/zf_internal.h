@@ -295,6 +295,13 @@ struct zf_ctx {
   int n_wall = 0;
   double* d_red = nullptr;        // reduction scratch
   int red_cap = 0;
+  // listed points of single lattice planes z = k, in (x, y) order, for the
+  // z-slab halo exchange (zf_plane_pack / zf_plane_unpack)
+  struct PlaneSlots {
+    int k, n;
+    int32_t* d_slots;
+  };
+  std::vector<PlaneSlots> planes;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   zf_status status{};
@@ -332,6 +339,8 @@ int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out = 
 int ensure_red(zf_ctx* c, int n);
 int lbm_step_mass_noalloc(zf_ctx* c, int store_moments, int zero_force, double* mass_out);
 int lbm_upload_populations(zf_ctx* c, const float* f);
+int lbm_plane_slots(zf_ctx* c, int k, zf_ctx::PlaneSlots* out);
+int lbm_plane_copy(zf_ctx* c, int k, int dir, void* buf, bool pack);
 int lbm_download_populations(zf_ctx* c, float* f);
 int lbm_init_equilibrium(zf_ctx* c);
 int lbm_scatter_listed(zf_ctx* c, const float* h, int planes, float* d_dst);

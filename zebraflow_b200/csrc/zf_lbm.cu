@@ -24,6 +24,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <mutex>
 #include <type_traits>
 
@@ -969,6 +970,81 @@ int lbm_gather_listed(zf_ctx* c, const float* d_src, int planes, float* h) {
   ZF_CUDA(cudaMemcpyAsync(h, c->d_stage, (size_t)planes * n * sizeof(float),
                           cudaMemcpyDeviceToHost, c->stream));
   ZF_CUDA(cudaStreamSynchronize(c->stream));
+  return ZF_OK;
+}
+
+// z-slab halo exchange: the 5 populations with e_z = dir of the listed points
+// of plane k, [n][5] raw storage elements (ET: 4 or 2 bytes), in (x, y) order
+__host__ __device__ constexpr int zface_q(int dir, int d) {
+  return dir > 0 ? (d == 0 ? 4 : 8 + 2 * d) : (d == 0 ? 5 : 9 + 2 * d);  // {4,10,12,14,16} / {5,11,13,15,17}
+}
+template <typename ET>
+__global__ void k_plane_copy(ET* __restrict__ f, const int32_t* __restrict__ slots, int n, int dir,
+                             ET* __restrict__ buf, int pack) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n) return;
+  const int64_t s = slots[m];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    const int q = dir > 0 ? zface_q(1, d) : zface_q(-1, d);
+    if (pack) buf[m * 5 + d] = f[pop_at(q, s)];
+    else f[pop_at(q, s)] = buf[m * 5 + d];
+  }
+}
+
+int lbm_plane_slots(zf_ctx* c, int k, zf_ctx::PlaneSlots* out) {
+  if (k < 0 || k >= c->p.nz) {
+    set_error("plane %d outside the lattice (nz %d)", k, c->p.nz);
+    return ZF_ERR_ARG;
+  }
+  for (const auto& pl : c->planes)
+    if (pl.k == k) {
+      *out = pl;
+      return ZF_OK;
+    }
+  // listed points of the plane, ordered by (x, y)
+  std::vector<std::pair<int64_t, int32_t>> pts;
+  const int ntx = c->ntx, nty = c->nty;
+  for (int64_t l = 0; l < c->n_listed; ++l) {
+    const int i = c->domlist[3 * l], j = c->domlist[3 * l + 1], kk = c->domlist[3 * l + 2];
+    if (kk != k) continue;
+    const int64_t t = ((int64_t)(kk / ZF_TS) * nty + j / ZF_TS) * ntx + i / ZF_TS;
+    const int32_t id = c->h_tile_map[t];
+    if (id < 0) continue;
+    const int32_t slot = id * ZF_TC + (i % ZF_TS) + ZF_TS * (j % ZF_TS) + ZF_TS * ZF_TS * (kk % ZF_TS);
+    pts.emplace_back((int64_t)i * c->p.ny + j, slot);
+  }
+  std::sort(pts.begin(), pts.end());
+  std::vector<int32_t> slots(pts.size());
+  for (size_t m = 0; m < pts.size(); ++m) slots[m] = pts[m].second;
+  zf_ctx::PlaneSlots pl{k, (int)slots.size(), nullptr};
+  int rc = dev_alloc(c, (void**)&pl.d_slots, std::max<size_t>(slots.size(), 1) * sizeof(int32_t));
+  if (rc) return rc;
+  if (!slots.empty())
+    ZF_CUDA(cudaMemcpyAsync(pl.d_slots, slots.data(), slots.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                            c->stream));
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  c->planes.push_back(pl);
+  *out = pl;
+  return ZF_OK;
+}
+
+int lbm_plane_copy(zf_ctx* c, int k, int dir, void* buf, bool pack) {
+  zf_ctx::PlaneSlots pl{};
+  int rc = lbm_plane_slots(c, k, &pl);
+  if (rc) return rc;
+  if (pl.n == 0) return ZF_OK;
+  if (!buf) return ZF_ERR_ARG;
+  const bool half = c->p.storage == ZF_STORE_F16 || c->p.storage == ZF_STORE_BF16;
+  const unsigned grid = (unsigned)((pl.n + 255) / 256);
+  if (half)
+    k_plane_copy<uint16_t><<<grid, 256, 0, c->stream>>>(static_cast<uint16_t*>(c->d_f[c->cur]), pl.d_slots,
+                                                         pl.n, dir, static_cast<uint16_t*>(buf), pack);
+  else
+    k_plane_copy<uint32_t><<<grid, 256, 0, c->stream>>>(static_cast<uint32_t*>(c->d_f[c->cur]), pl.d_slots,
+                                                         pl.n, dir, static_cast<uint32_t*>(buf), pack);
+  ZF_CUDA(cudaGetLastError());
+  c->launches += 1;
   return ZF_OK;
 }
 

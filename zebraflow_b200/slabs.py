@@ -1,0 +1,145 @@
+"""Z-slab decomposition of the LBM step over ranks, one GPU each, with one
+halo exchange per step (no counterpart in the reference, which runs on one
+node with OpenMP).
+
+The lattice (periodic in z) is cut into equal slabs of whole 4x4x4 tile
+layers.  Each rank holds its slab with one tile layer of halo on either side
+(HALO planes).  A step of the interior pulls across a z face only the
+populations of the 5 directions with e_z pointing into the slab, from the
+halo plane next to the face; so after every step each rank sends the
+e_z = -1 populations of its first interior plane to the rank below (its top
+halo plane) and the e_z = +1 populations of its last interior plane to the
+rank above (its bottom halo plane), and the interior evolves exactly as in
+the unsplit lattice.  The halo planes' other populations and the rest of the
+halo layer are never read by the interior.  Body force, cells and the IB
+coupling are not split here: the slab path is the LBM step alone.
+"""
+import numpy as np
+
+from . import Context, default_params
+
+HALO = 4  # one tile layer
+
+
+def slab_bounds(nz, world, rank):
+    """Interior z planes [z0, z1) of `rank`: nz splits into `world` equal
+    slabs of whole tile layers."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad world/rank")
+    if nz % (4 * world):
+        raise ValueError(f"nz = {nz} does not split into {world} slabs of whole 4-plane tile layers")
+    n = nz // world
+    return rank * n, (rank + 1) * n
+
+
+def slab_lattice(b_index, world, rank):
+    """The rank's lattice: its interior planes with HALO planes on either
+    side, taken from the z-periodic lattice b_index [nx][ny][nz]."""
+    nz = b_index.shape[2]
+    z0, z1 = slab_bounds(nz, world, rank)
+    return np.ascontiguousarray(b_index[:, :, np.arange(z0 - HALO, z1 + HALO) % nz])
+
+
+def plane_counts(b_index):
+    """Listed points of every global z plane."""
+    return (b_index >= 0).sum(axis=(0, 1))
+
+
+def exchange_dist(send_dn, send_up, recv_dn, recv_up, rank, world, group=None):
+    """The halo exchange between ranks in a ring: send_dn goes to the rank
+    below (rank - 1), whose recv_up takes it; send_up to the rank above, whose
+    recv_dn takes it.  Tensors of any device the process group serves."""
+    import torch.distributed as dist
+    below, above = (rank - 1) % world, (rank + 1) % world
+    ops = [dist.P2POp(dist.isend, send_dn, below, group, tag=1),
+           dist.P2POp(dist.isend, send_up, above, group, tag=2),
+           dist.P2POp(dist.irecv, recv_up, above, group, tag=1),
+           dist.P2POp(dist.irecv, recv_dn, below, group, tag=2)]
+    for req in dist.batch_isend_irecv(ops):
+        req.wait()
+
+
+class SlabLBM:
+    """One rank's slab of a z-periodic lattice.
+
+    b_index: the whole lattice [nx][ny][nz] (reference codes); params: keyword
+    arguments of default_params for the whole lattice (nz and the z
+    periodicity are set here).  world == 1 exchanges with itself.  Several
+    slabs of one process (for instance on one GPU) are advanced together with
+    exchange_local."""
+
+    def __init__(self, b_index, world=1, rank=0, device=0, stream=None, group=None, **params):
+        import torch
+        nx, ny, nz = b_index.shape
+        self.world, self.rank, self.group = world, rank, group
+        self.z0, self.z1 = slab_bounds(nz, world, rank)
+        self.nzs = self.z1 - self.z0 + 2 * HALO
+        per = list(params.pop("periodic", (0, 0, 1)))
+        per[2] = 0
+        self.ctx = Context(default_params(nx=nx, ny=ny, nz=self.nzs, periodic=tuple(per), **params), device)
+        self.ctx.set_lattice(slab_lattice(b_index, world, rank))
+        self.stream = stream if stream is not None else torch.cuda.Stream(device=device)
+        self.ctx.set_stream(self.stream.cuda_stream)
+        # planes (local z): bottom halo / first interior / last interior / top halo
+        self.kb_halo, self.kb, self.kt, self.kt_halo = HALO - 1, HALO, self.nzs - HALO - 1, self.nzs - HALO
+        counts = plane_counts(b_index)
+        for k in (self.kb_halo, self.kb, self.kt, self.kt_halo):
+            if self.ctx.plane_count(k) != counts[(self.z0 - HALO + k) % nz]:
+                raise RuntimeError(f"slab plane {k}: listed points differ from the lattice's")
+        half = params.get("storage", 0) in (1, 2)
+        dt = torch.int16 if half else torch.int32
+        mk = lambda k: torch.empty(5 * self.ctx.plane_count(k), dtype=dt, device=f"cuda:{device}")
+        self.send_dn, self.send_up = mk(self.kb), mk(self.kt)
+        self.recv_up, self.recv_dn = mk(self.kt_halo), mk(self.kb_halo)
+
+    def pack(self):
+        self.ctx.plane_pack(self.kb, -1, self.send_dn.data_ptr())
+        self.ctx.plane_pack(self.kt, +1, self.send_up.data_ptr())
+
+    def unpack(self):
+        self.ctx.plane_unpack(self.kt_halo, -1, self.recv_up.data_ptr())
+        self.ctx.plane_unpack(self.kb_halo, +1, self.recv_dn.data_ptr())
+
+    def exchange(self):
+        """Halo exchange of this rank (all ranks call it together)."""
+        import torch
+        self.pack()
+        with torch.cuda.stream(self.stream):
+            if self.world == 1:
+                self.recv_up.copy_(self.send_dn)
+                self.recv_dn.copy_(self.send_up)
+            else:
+                exchange_dist(self.send_dn, self.send_up, self.recv_dn, self.recv_up, self.rank, self.world,
+                              self.group)
+        self.unpack()
+
+    def step(self, n=1):
+        """n LBM steps of the slab, each followed by the halo exchange."""
+        for _ in range(n):
+            self.ctx.lbm_step(store_moments=False, zero_bodyforce=False)
+            self.exchange()
+
+    def interior(self, dom=None):
+        """Mask of the slab's listed points that are interior, and their
+        global z plane."""
+        dom = self.ctx.domlist() if dom is None else dom
+        k = dom[:, 2]
+        return (k >= HALO) & (k < self.nzs - HALO), self.z0 + k - HALO
+
+    def close(self):
+        self.ctx.close()
+
+
+def exchange_local(slabs):
+    """The halo exchange among the slabs of one process, in ring order (slab
+    r's neighbours are r - 1 and r + 1); they must share one stream."""
+    import torch
+    n = len(slabs)
+    for s in slabs:
+        s.pack()
+    with torch.cuda.stream(slabs[0].stream):
+        for r, s in enumerate(slabs):
+            s.recv_up.copy_(slabs[(r + 1) % n].send_dn)
+            s.recv_dn.copy_(slabs[(r - 1) % n].send_up)
+    for s in slabs:
+        s.unpack()
