@@ -683,6 +683,52 @@ def run_c2(args):
     return 0
 
 
+def run_sharded(args):
+    """The LBM step of the workload's lattice (no cells) split into z slabs,
+    one per rank, with the halo exchange after every step (strong scaling:
+    the lattice is fixed, N ranks share it).  One JSON line, MLUPS of the
+    whole lattice from the slowest rank's device time."""
+    import torch
+    import torch.distributed as dist
+    import zebraflow_b200 as zf
+    from zebraflow_b200 import slabs
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    nx, ny, nz, Rp, Rd, ang, g, _ = WORKLOADS[args.workload]
+    b, _ = zf.gen_bifurcation(nx, ny, nz, Rp, Rd, ang)
+    n_fluid = int((b > 0).sum())
+    st = STORAGES[args.storage]
+    slab = slabs.SlabLBM(b, world=world, rank=rank, device=local, tau=0.9, tau_from_phase=0,
+                         wall_mode=zf.WALL_HALFWAY_BB, g=(0.0, 0.0, g), storage=st)
+    slab.step(args.warmup)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(local)
+    e0.record(slab.stream)
+    slab.step(args.steps)
+    e1.record(slab.stream)
+    torch.cuda.synchronize(local)
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        ms = max_over_ranks([ms], f"cuda:{local}")[0]
+    if rank == 0:
+        print(json.dumps({"metric": "MLUPS", "value": round(n_fluid * args.steps / (ms * 1e-3) / 1e6, 1),
+                          "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
+                          "scaling": "strong", "dtype": DTYPE_NAME[st], "data": "synthetic",
+                          "config": {"workload": args.workload + "_lbm_only", "fluid_points": n_fluid,
+                                     "parallelism": f"z slabs x{world}, halo exchange every step"}}),
+              flush=True)
+    slab.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -704,10 +750,15 @@ def main():
     ap.add_argument("--c2-steps", type=int, default=0,
                     help="instead of the bench line, a precision report of this many iterations "
                          "against the FP64 oracle")
+    ap.add_argument("--sharded", action="store_true",
+                    help="instead of the bench line, the LBM step of the lattice split into z slabs "
+                         "over the ranks (no cells)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.c2_steps > 0:
         return run_c2(args)
+    if args.sharded and args.impl == "ours":
+        return run_sharded(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
