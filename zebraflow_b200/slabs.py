@@ -90,7 +90,10 @@ class SlabLBM:
         dt = torch.int16 if half else torch.int32
         mk = lambda k: torch.empty(5 * self.ctx.plane_count(k), dtype=dt, device=f"cuda:{device}")
         self.send_dn, self.send_up = mk(self.kb), mk(self.kt)
-        self.recv_up, self.recv_dn = mk(self.kt_halo), mk(self.kb_halo)
+        if world == 1:  # the slab is its own neighbour: unpack straight from the packed planes
+            self.recv_up, self.recv_dn = self.send_dn, self.send_up
+        else:
+            self.recv_up, self.recv_dn = mk(self.kt_halo), mk(self.kb_halo)
 
     def pack(self):
         self.ctx.plane_pack(self.kb, -1, self.send_dn.data_ptr())
@@ -104,11 +107,8 @@ class SlabLBM:
         """Halo exchange of this rank (all ranks call it together)."""
         import torch
         self.pack()
-        with torch.cuda.stream(self.stream):
-            if self.world == 1:
-                self.recv_up.copy_(self.send_dn)
-                self.recv_dn.copy_(self.send_up)
-            else:
+        if self.world > 1:
+            with torch.cuda.stream(self.stream):
                 exchange_dist(self.send_dn, self.send_up, self.recv_dn, self.recv_up, self.rank, self.world,
                               self.group)
         self.unpack()
