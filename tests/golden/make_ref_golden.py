@@ -1,11 +1,19 @@
-"""Builds tests/golden/ref_setup.npz from the reference's own set-up code.
+"""Builds tests/golden/ref_setup.npz and tests/golden/ref_step.npz from the
+reference's own code.
 
 Runs oracle/ref/Makefile, which compiles the reference's ZebraflowWT.c where
-it lies (main renamed) with oracle/ref/harness_setup.c and runs its
-CGSM_ZFISHRBC_DATA_GEN / CGSM_FILAMENT_PARAMETERS / CGSM_EQUILIBRIUM_METRICS
-on the shipped RBC and nucleus meshes, and LBM_DOM_SETUP / LBM_BC_SETUP on a
-small synthetic lattice.  The fixture keeps the mesh inputs and the
-reference's outputs so that the pin runs where the reference tree is absent.
+it lies (main renamed) and runs two harnesses against it:
+ * oracle/ref/harness_setup.c: CGSM_ZFISHRBC_DATA_GEN /
+   CGSM_FILAMENT_PARAMETERS / CGSM_EQUILIBRIUM_METRICS on the shipped RBC and
+   nucleus meshes, and LBM_DOM_SETUP / LBM_BC_SETUP on a small synthetic
+   lattice -> ref_setup.npz;
+ * oracle/ref/harness_step.c: five LBM steps of the reference's own
+   stream-collide, wall and copy blocks of main() (ZebraflowWT.c:6101-6145,
+   :6292-6433, :6601-6626) on a small capped tube with a phase-5 ball ->
+   ref_step.npz (lattice, initial populations and body force, populations
+   after steps 1 and 5, moments and body force after step 5).
+The fixtures keep the inputs and the reference's outputs so that the pins run
+where the reference tree is absent.
 
 Usage: python tests/golden/make_ref_golden.py [reference_dir]
 """
@@ -53,6 +61,20 @@ def main():
                         nuc_edges=EN, edges=edges, epar=epar, epar_n=epar_n, domlist=domlist,
                         bclist=bc[:, :4], bcnlist=bc[:, 4:])
     print(f"edges {ne}, nucleus edges {nen}, listed points {dommax}, boundary points {bcmax}")
+
+    raw = open(os.path.join(ROOT, "oracle", "_ref", "ref_step.bin"), "rb").read()
+    a = np.frombuffer(raw, np.int32)
+    f = np.frombuffer(raw, np.float32)
+    n, steps = int(a[0]), int(a[1])
+    p = 2
+    listed = a[p:p + 4 * n].reshape(n, 4).copy(); p += 4 * n
+    out = {}
+    for key, k in (("f0", 19), ("bf0", 3), ("f1", 19), ("fN", 19), ("D", 1), ("U", 1), ("V", 1),
+                   ("W", 1), ("bfN", 3)):
+        out[key] = f[p:p + k * n].reshape(k, n).copy().squeeze(); p += k * n
+    assert p == a.size
+    np.savez_compressed(os.path.join(HERE, "ref_step.npz"), listed=listed, steps=steps, **out)
+    print(f"LBM step: {n} listed points, {steps} steps")
 
 
 if __name__ == "__main__":

@@ -6,15 +6,22 @@ oracle/ref/harness_setup.c and runs its set-up functions:
 CGSM_ZFISHRBC_DATA_GEN + CGSM_FILAMENT_PARAMETERS + CGSM_EQUILIBRIUM_METRICS on
 the shipped zebrafish RBC mesh (ZebraflowWT.c:1592-2223, :2336-2346) and
 LBM_DOM_SETUP + LBM_BC_SETUP on a synthetic tube lattice (:1481-1589).
+
+tests/golden/ref_step.npz comes from the same script and oracle/ref/harness_step.c:
+five LBM steps run by the reference's own stream-collide, wall and copy blocks
+of its main() (:6101-6145, :6292-6433, :6601-6626) on a capped tube with a
+phase-5 ball, from perturbed populations under a random body force.
 """
 import os
 
 import numpy as np
+import pytest
 
 import zebraflow_b200 as zf
 from oracle.bind import OracleCells, OracleLBM
 
 GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_setup.npz"))
+STEP = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_step.npz"))
 
 # the harness lattice: a tube of radius 6 around (i,j) = (20,30), fluid for
 # 7 < k < 38, wall points linked to it, all 1-based in the reference box; the
@@ -74,3 +81,65 @@ def test_lattice_setup_matches_reference():
     assert np.array_equal(dom[wall], ref_bc[:, :3] - np.array([I0, J0, K0]))
     assert np.all(ref_bc[:, 3] == 0)
     assert np.array_equal(dom[bcnb[wall]], ref_nb)
+
+
+def step_lattice():
+    """The step harness's lattice cropped to its listed points' bounding box
+    (listed order is unchanged by the crop), and the crop's origin."""
+    listed = STEP["listed"]
+    lo = listed[:, :3].min(0)
+    b = -np.ones(tuple(listed[:, :3].max(0) - lo + 1), np.int32)
+    b[tuple((listed[:, :3] - lo).T)] = listed[:, 3]
+    return b, lo
+
+
+def run_oracle_steps(precision, **kw):
+    b, lo = step_lattice()
+    args = dict(wall_mode=1, tau_from_phase=True, dt=0.5, precision=precision)
+    args.update(kw)
+    o = OracleLBM(b, **args)
+    dom, _ = o.dom()
+    assert np.array_equal(dom, STEP["listed"][:, :3] - lo)
+    o.set_f(STEP["f0"].astype(np.float64))
+    o.set_bodyforce(STEP["bf0"].astype(np.float64))
+    out = {}
+    steps = int(STEP["steps"])
+    for s in range(1, steps + 1):
+        o.step(rbc_flag=(s == steps))  # the harness's last step is a membrane step
+        if s == 1:
+            out["f1"] = o.get_f()
+    out["fN"] = o.get_f()
+    out["D"], out["U"], out["V"], out["W"] = o.moments()
+    out["bfN"] = o.get_bodyforce()
+    return out
+
+
+# The reference evaluates the step in float storage with double temporaries
+# (its equilibrium constants are double), the oracle in pure fp32 or fp64: the
+# populations agree to a few fp32 ulp (|f| <= 0.35, ulp 3e-8) per step.  The
+# body force moves them by ~4e-3 over the five steps, so an error in a
+# direction, a weight, the force term or a relaxation time shows up orders of
+# magnitude above these bounds (see test_lbm_step_pin_detects_a_wrong_tau).
+F_TOL = 3e-7
+D_TOL = 1e-6
+U_TOL = 1e-7
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_lbm_step_matches_reference(precision):
+    out = run_oracle_steps(precision)
+    assert np.max(np.abs(STEP["fN"] - STEP["f0"])) > 3e-3
+    assert np.max(np.abs(out["f1"] - STEP["f1"])) < F_TOL
+    assert np.max(np.abs(out["fN"] - STEP["fN"])) < F_TOL
+    assert np.max(np.abs(out["D"] - STEP["D"])) < D_TOL
+    for a in "UVW":
+        assert np.max(np.abs(out[a] - STEP[a])) < U_TOL
+    # the membrane step clears the body force at every listed point
+    assert np.all(STEP["bfN"] == 0) and np.all(out["bfN"] == 0)
+
+
+def test_lbm_step_pin_detects_a_wrong_tau():
+    """A mistake planted in the oracle: one relaxation time for every phase
+    (the 33 phase-5 points relax with tau = 1.22 instead of 4.1)."""
+    out = run_oracle_steps("f64", tau_from_phase=False, tau=1.22)
+    assert np.max(np.abs(out["fN"] - STEP["fN"])) > 100 * F_TOL
