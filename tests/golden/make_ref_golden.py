@@ -7,6 +7,11 @@ it lies (main renamed) and runs two harnesses against it:
    CGSM_FILAMENT_PARAMETERS / CGSM_EQUILIBRIUM_METRICS on the shipped RBC and
    nucleus meshes, and LBM_DOM_SETUP / LBM_BC_SETUP on a small synthetic
    lattice -> ref_setup.npz;
+ * oracle/ref/harness_cells.c: one membrane step of the reference's own
+   force blocks of main() (CGSM_NODAL_FORCE_ZERO, CGSM_AREA, centroid/area,
+   CGSM_LOCAL_FORCES, CGSM_VOLUME_CALC; ZebraflowWT.c:5706-7535) for two
+   deformed RBCs with nuclei -> ref_cells.npz (node coordinates, node forces,
+   triangle geometry, per-cell area/volume/centroid/global-area/volume terms);
  * oracle/ref/harness_step.c: five LBM steps of the reference's own
    stream-collide, wall and copy blocks of main() (ZebraflowWT.c:6101-6145,
    :6292-6433, :6601-6626) on a small capped tube with a phase-5 ball ->
@@ -75,6 +80,35 @@ def main():
     assert p == a.size
     np.savez_compressed(os.path.join(HERE, "ref_step.npz"), listed=listed, steps=steps, **out)
     print(f"LBM step: {n} listed points, {steps} steps")
+
+    raw = open(os.path.join(ROOT, "oracle", "_ref", "ref_cells.bin"), "rb").read()
+    pos = [0]
+
+    def rd(dt, k):
+        r = np.frombuffer(raw, dt, k, pos[0]).copy()
+        pos[0] += r.itemsize * k
+        return r
+    nc, nn, nnn, nt = rd(np.int32, 4)
+    area_eq = rd(np.float32, nt)
+    keys = (("x", np.float64, 3 * nn), ("xn", np.float64, 3 * nnn), ("ftot", np.float32, 3 * nn),
+            ("ftot_n", np.float32, 3 * nnn), ("tri_area", np.float32, nt),
+            ("tri_normal", np.float32, 3 * nt), ("tri_centroid", np.float32, 3 * nt),
+            ("node_normal", np.float32, 3 * nn), ("cell", np.float32, 7), ("status", np.int32, 2))
+    per = {k: [] for k, _, _ in keys}
+    for _ in range(nc):
+        for k, dt, m in keys:
+            per[k].append(rd(dt, m))
+    simfailure = int(rd(np.int32, 1)[0])
+    assert pos[0] == len(raw)
+    out = {}
+    for k, _, m in keys:
+        a = np.stack(per[k])                       # [cell][...]
+        if m % 3 == 0 and k not in ("tri_area",):  # [cell][3][n] -> [3][cell][n]
+            a = a.reshape(nc, 3, -1).transpose(1, 0, 2)
+        out[k] = a
+    np.savez_compressed(os.path.join(HERE, "ref_cells.npz"), tri_area_eq=area_eq,
+                        simfailure=simfailure, **out)
+    print(f"membrane step: {nc} cells, simfailure {simfailure}")
 
 
 if __name__ == "__main__":

@@ -11,6 +11,11 @@ tests/golden/ref_step.npz comes from the same script and oracle/ref/harness_step
 five LBM steps run by the reference's own stream-collide, wall and copy blocks
 of its main() (:6101-6145, :6292-6433, :6601-6626) on a capped tube with a
 phase-5 ball, from perturbed populations under a random body force.
+
+tests/golden/ref_cells.npz, from oracle/ref/harness_cells.c: one membrane step
+run by the reference's own force blocks of its main() (CGSM_NODAL_FORCE_ZERO,
+CGSM_AREA, cell centroid/area, CGSM_LOCAL_FORCES, CGSM_VOLUME_CALC;
+:5706-7535) on two deformed RBCs with nuclei built from the shipped meshes.
 """
 import os
 
@@ -22,6 +27,7 @@ from oracle.bind import OracleCells, OracleLBM
 
 GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_setup.npz"))
 STEP = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_step.npz"))
+CELLS = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_cells.npz"))
 
 # the harness lattice: a tube of radius 6 around (i,j) = (20,30), fluid for
 # 7 < k < 38, wall points linked to it, all 1-based in the reference box; the
@@ -143,3 +149,54 @@ def test_lbm_step_pin_detects_a_wrong_tau():
     (the 33 phase-5 points relax with tau = 1.22 instead of 4.1)."""
     out = run_oracle_steps("f64", tau_from_phase=False, tau=1.22)
     assert np.max(np.abs(out["fN"] - STEP["fN"])) > 100 * F_TOL
+
+
+def run_oracle_cells(precision, **params):
+    o = OracleCells(GOLD["mesh_x"], GOLD["mesh_tri"], GOLD["nuc_x"], GOLD["nuc_edges"],
+                    zf.default_params(**params), precision=precision)
+    ae = o.topology()[3]
+    o.set_cells(CELLS["x"], CELLS["xn"])
+    o.forces()
+    return o, ae, o.get(), o.geometry()
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b)) / np.max(np.abs(b))
+
+
+# Bounds, relative to the largest value of each array.  The reference keeps
+# coordinates in double and geometry and forces in float; the fp32 oracle
+# evaluates the same float expressions (triangle geometry and per-cell sums come
+# out identical here) and its node forces differ by summation order, a few
+# 1e-6 of the largest force.  The fp64 oracle carries none of the reference's
+# float rounding: its triangle areas differ by ~3e-5, node forces by ~1e-4.
+CELL_TOL = {"f32": dict(geo=1e-6, f=3e-5, fn=3e-6, cell=1e-6, glob=1e-5, vol=1e-4),
+            "f64": dict(geo=1e-4, f=5e-4, fn=1e-3, cell=1e-5, glob=3e-4, vol=3e-4)}
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_membrane_step_matches_reference(precision):
+    t = CELL_TOL[precision]
+    o, ae, g, (ta, tn, tc, nn) = run_oracle_cells(precision)
+    # the reference's shape constants are the defaults (RBC_SURF, MCV, moduli)
+    assert rel(ae, CELLS["tri_area_eq"]) < t["geo"]
+    assert rel(ta, CELLS["tri_area"]) < t["geo"]
+    assert np.max(np.abs(tn - CELLS["tri_normal"])) < t["geo"]
+    assert rel(tc, CELLS["tri_centroid"]) < t["geo"]
+    assert np.max(np.abs(nn - CELLS["node_normal"])) < 10 * t["geo"]
+    assert np.abs(CELLS["ftot"]).max() > 1e-13
+    assert rel(g["ftot"], CELLS["ftot"]) < t["f"]
+    assert rel(g["ftot_n"], CELLS["ftot_n"]) < t["fn"]
+    cf, rc = g["cell"], CELLS["cell"]
+    assert np.allclose(cf[:, :5], rc[:, :5], rtol=t["cell"], atol=0)  # area, volume, centroid
+    assert np.allclose(cf[:, 5], rc[:, 5], rtol=t["glob"], atol=0)     # F_AREA_GLOBAL
+    assert np.allclose(cf[:, 6], rc[:, 6], rtol=t["vol"], atol=0)      # F_VOLUME_SCALAR
+    # neither cell is removed and no failure is flagged, in either run
+    assert np.all(CELLS["status"][:, 0] == 1) and np.all(g["status"] == 1)
+    assert int(CELLS["simfailure"]) == 0 and g["counters"][0] == 0
+
+
+def test_membrane_pin_detects_a_wrong_modulus():
+    """A mistake planted in the oracle: the shear modulus 1 % too large."""
+    o, _, g, _ = run_oracle_cells("f32", Es=3.03e-6)
+    assert rel(g["ftot"], CELLS["ftot"]) > 30 * CELL_TOL["f32"]["f"]
