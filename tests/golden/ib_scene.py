@@ -1,0 +1,118 @@
+"""The IB-stage scene shared by tests/golden/make_ref_golden.py (which runs the
+reference's own IB blocks on it through oracle/ref/harness_ib.c) and
+tests/test_oracle_ref_pin.py (which runs the oracle on it).
+
+A straight tube (radius 9 um) in a 48 x 48 x 72 sub-box of the reference's
+lattice, at lattice offset (100, 100, 100) from the reference origin, with a
+wall layer 6 points thick, so that the +-4 point search windows of the
+reference around every cell node stay on listed points: fluid points carry a
+swirling Poiseuille flow, the wall mesh is a cylinder, and four
+zebrafish RBCs with nuclei (the shipped meshes) sit in it: cells 0 and 1
+0.3 um apart (RBC-RBC repulsion), cell 2 close to the wall (wall repulsion),
+cell 3 free; no nucleus touches its membrane (see place_cells).  Everything but the cell coordinates is regenerated from
+committed code (the lattice, wall and flow generators, the oracle's wall
+set-up); the fixture keeps the cell coordinates and checksums of the rest.
+"""
+import numpy as np
+
+import zebraflow_b200 as zf
+from oracle.bind import OracleCells, OracleLBM, OracleWorld
+
+NX, NY, NZ = 48, 48, 72
+CX = CY = 23.5          # lattice units
+R_LAT = 18.0            # tube radius, lattice units (9 um)
+OFFSET = (100, 100, 100)  # 0-based lattice offset of the sub-box in the reference box
+DX = 0.5
+REF_ORIGIN = (-1.0, 29.0, -27.0)  # X0, Y0, Z0 of the reference (ZebraflowWT.c:85-87)
+ORIGIN = tuple(o + DX * s for o, s in zip(REF_ORIGIN, OFFSET))
+ITER = 1000             # a membrane iteration that rebuilds the nucleus lists
+UMAX = 2e-3             # lattice units
+
+
+def lattice():
+    b = zf.gen_tube(NX, NY, NZ, CX, CY, R_LAT, True)
+    i, j = np.meshgrid(np.arange(NX) - CX, np.arange(NY) - CY, indexing="ij")
+    thick = (i * i + j * j < (R_LAT + 6.0) ** 2)[:, :, None] & (b < 0)
+    b[np.broadcast_to(thick, b.shape)] = 0
+    return b
+
+
+def wall():
+    return zf.gen_wall_tube(CX, CY, R_LAT, NZ, origin=ORIGIN, dx=DX)
+
+
+def populations(b):
+    """Equilibrium populations of a swirling Poiseuille flow at every listed
+    point (float64 arithmetic without transcendental functions, so every
+    machine builds the same values)."""
+    dom = np.argwhere(b >= 0).astype(np.float64)
+    dx_, dy_ = dom[:, 0] - CX, dom[:, 1] - CY
+    r2 = (dx_ * dx_ + dy_ * dy_) / (R_LAT * R_LAT)
+    w = UMAX * np.maximum(1.0 - r2, 0.0)
+    u = 0.2 * UMAX * dy_ / R_LAT
+    v = -0.2 * UMAX * dx_ / R_LAT
+    E = zf.E.astype(np.float64)
+    cu = E[:, 0:1] * u + E[:, 1:2] * v + E[:, 2:3] * w
+    usq = u * u + v * v + w * w
+    return zf.W[:, None] * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq)
+
+
+def place_cells(rest, rest_n, seed=2024):
+    """Four cells: deformed, rotated copies of the shipped meshes (about their
+    membrane centroid), positions in um.  Every membrane is stretched 2-3 %
+    along its long axis with 0.015 um node noise (so that the membrane forces
+    are not rounding noise).  The nuclei are shrunk to 85 % so that they stay
+    out of reach (0.2 um) of the nucleus-membrane repulsion: that block of the
+    reference reads and writes its sub-point array tp[16..19] past the 16 rows
+    it declares (ZebraflowWT.c:2307, :9690-9706), so its result there depends
+    on the compiler's stack layout and cannot serve as a pin."""
+    rng = np.random.default_rng(seed)
+    c0 = rest.mean(axis=0)
+    rest = rest - c0
+    rest_n = rest_n - c0
+    shape = [(1.0, 1.02, 1.0), (1.0, 1.02, 1.0), (1.0, 1.02, 1.0), (1.0, 1.03, 1.0)]
+
+    def rot(ax, deg):
+        a = np.deg2rad(deg)
+        c, s = np.cos(a), np.sin(a)
+        m = {"x": [[1, 0, 0], [0, c, -s], [0, s, c]], "y": [[c, 0, s], [0, 1, 0], [-s, 0, c]],
+             "z": [[c, -s, 0], [s, c, 0], [0, 0, 1]]}[ax]
+        return np.array(m)
+
+    def put(pts, Rm, t):
+        return (pts @ Rm.T + t).T
+
+    o = np.array(ORIGIN)
+    ctr = o + DX * np.array([CX, CY, 0.0])
+    # (rotation, centre offset from the tube axis at z) per cell; the long (y)
+    # axis of the mesh is laid along the tube
+    Rz = rot("x", 90.0)                       # mesh y -> z
+    # after Rz the mesh is 6 um wide in x, 2.4 um thick in y, 13 um long in z
+    cells = [(Rz, [0.0, -1.35, 10.0]),
+             (Rz, [0.0, 1.35, 10.0]),                  # 0.3 um from cell 0 in y
+             (Rz, [0.0, 9.0 - 1.2 - 0.15, 24.0]),      # 0.15 um from the wall at +y
+             (rot("z", 35.0) @ Rz, [1.0, -2.5, 24.0])]
+    X, XN = [], []
+    for (Rm, t), sc in zip(cells, shape):
+        t = ctr + np.array(t)
+        X.append(put(rest * np.array(sc) + 0.015 * rng.standard_normal(rest.shape), Rm, t))
+        XN.append(put(0.85 * rest_n + 0.01 * rng.standard_normal(rest_n.shape), Rm, t))
+    return np.stack(X, axis=1), np.stack(XN, axis=1)
+
+
+def oracle_world(mesh, x, xn, precision="f32", **overrides):
+    """(lattice, params, lbm, cells, world) oracle objects of the scene; x, xn
+    the cell coordinates [3][cell][node] in um; overrides: parameter changes."""
+    b = lattice()
+    kw = dict(nx=NX, ny=NY, nz=NZ, origin=ORIGIN, tau=1.22, tau_from_phase=0,
+              wall_mode=zf.WALL_REF_EQ, periodic=(0, 0, 0), stagger=50)
+    kw.update(overrides)
+    p = zf.default_params(**kw)
+    lbm = OracleLBM(b, wall_mode=1, periodic=(0, 0, 0), tau=1.22, dt=0.5, precision=precision)
+    lbm.set_f(populations(b))
+    lbm.moments_from_f()
+    oc = OracleCells(*mesh, p, precision=precision)
+    oc.set_cells(x, xn)
+    w = OracleWorld(lbm, oc, p)
+    w.set_wall(*wall())
+    return b, p, lbm, oc, w

@@ -12,6 +12,11 @@ it lies (main renamed) and runs two harnesses against it:
    CGSM_LOCAL_FORCES, CGSM_VOLUME_CALC; ZebraflowWT.c:5706-7535) for two
    deformed RBCs with nuclei -> ref_cells.npz (node coordinates, node forces,
    triangle geometry, per-cell area/volume/centroid/global-area/volume terms);
+ * oracle/ref/harness_ib.c: one membrane iteration of the reference's own
+   blocks of main() (forces, IB interpolation + wall repulsion, nucleus-
+   membrane and RBC-RBC repulsion, IB spreading, position update;
+   ZebraflowWT.c:5659-12189) on the scene of tests/golden/ib_scene.py ->
+   ref_ib.npz (cell coordinates, scene checksums, the state after each stage);
  * oracle/ref/harness_step.c: five LBM steps of the reference's own
    stream-collide, wall and copy blocks of main() (ZebraflowWT.c:6101-6145,
    :6292-6433, :6601-6626) on a small capped tube with a phase-5 ball ->
@@ -31,6 +36,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "tests")]  # the package, the oracle, tests/golden
 
 
 def read_mesh(ref):
@@ -109,6 +115,60 @@ def main():
     np.savez_compressed(os.path.join(HERE, "ref_cells.npz"), tri_area_eq=area_eq,
                         simfailure=simfailure, **out)
     print(f"membrane step: {nc} cells, simfailure {simfailure}")
+    ib_fixture()
+
+
+def ib_fixture():
+    from golden import ib_scene as S
+    G = np.load(os.path.join(HERE, "ref_setup.npz"))
+    mesh = (G["mesh_x"], G["mesh_tri"], G["nuc_x"], G["nuc_edges"])
+    x, xn = S.place_cells(G["mesh_x"], G["nuc_x"])
+    b, p, lbm, oc, w = S.oracle_world(mesh, x, xn, "f32")
+    _, U, V, W = lbm.moments()
+    vel = np.stack([U, V, W]).astype(np.float32)
+    wi, uv = w.wall_index(b.shape)
+    wxyz, wtri, wnrm = S.wall()
+    nc = x.shape[1]
+    hdr = np.array(list(S.OFFSET) + [S.NX, S.NY, S.NZ, wxyz.shape[1], wtri.shape[1], nc, S.ITER,
+                                     lbm.n, 0], np.int32)
+    scene = os.path.join(ROOT, "oracle", "_ref", "ib_scene.bin")
+    with open(scene, "wb") as f:
+        for a, dt in ((hdr, np.int32), (b, np.int32), (vel, np.float32), (wi, np.int32),
+                      (uv, np.float32), (wxyz, np.float32), (wtri, np.int32), (wnrm, np.float32),
+                      (x, np.float64), (xn, np.float64)):
+            f.write(np.ascontiguousarray(a, dt).tobytes())
+    out = os.path.join(ROOT, "oracle", "_ref", "ref_ib.bin")
+    if os.path.exists(out):
+        os.remove(out)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), "../_ref/ref_ib.bin"],
+                   check=True)
+    raw = open(out, "rb").read()
+    pos = [0]
+
+    def rd(dt, shape):
+        k = int(np.prod(shape))
+        r = np.frombuffer(raw, dt, k, pos[0]).copy().reshape(shape)
+        pos[0] += r.itemsize * k
+        return r
+    nn, nnn, n = x.shape[2], xn.shape[2], lbm.n
+    res = {}
+    res["ftot"], res["ftot_n"] = rd(np.float32, (3, nc, nn)), rd(np.float32, (3, nc, nnn))
+    res["vel_interp"], res["vel_n_interp"] = rd(np.float64, (3, nc, nn)), rd(np.float64, (3, nc, nnn))
+    res["rep_interp"], res["rep_n_interp"] = rd(np.float32, (3, nc, nn)), rd(np.float32, (3, nc, nnn))
+    res["rep_nuc"], res["rep_n_nuc"] = rd(np.float32, (3, nc, nn)), rd(np.float32, (3, nc, nnn))
+    res["rep_rbc"], res["rep_n_rbc"] = rd(np.float32, (3, nc, nn)), rd(np.float32, (3, nc, nnn))
+    bf = rd(np.float32, (3, n))
+    res["vel_spread"], res["vel_n_spread"] = rd(np.float64, (3, nc, nn)), rd(np.float64, (3, nc, nnn))
+    res["x_new"], res["xn_new"] = rd(np.float64, (3, nc, nn)), rd(np.float64, (3, nc, nnn))
+    res["status"] = rd(np.int32, (nc,))
+    res["simfailure"] = rd(np.int32, (1,))
+    assert pos[0] == len(raw)
+    nzr = np.flatnonzero(np.any(bf != 0, axis=0)).astype(np.int32)  # spread body force, sparse
+    np.savez_compressed(os.path.join(HERE, "ref_ib.npz"), x=x, xn=xn, bf_idx=nzr, bf_val=bf[:, nzr],
+                        sum_vel=vel.astype(np.float64).sum(axis=1), sum_windex=np.int64(wi.sum()),
+                        sum_uvoid=uv.astype(np.float64).sum(), n_listed=n, **res)
+    print(f"IB stages: {nc} cells, {n} listed points, {nzr.size} points with spread force, "
+          f"simfailure {int(res['simfailure'][0])}")
 
 
 if __name__ == "__main__":

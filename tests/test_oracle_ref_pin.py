@@ -12,6 +12,11 @@ five LBM steps run by the reference's own stream-collide, wall and copy blocks
 of its main() (:6101-6145, :6292-6433, :6601-6626) on a capped tube with a
 phase-5 ball, from perturbed populations under a random body force.
 
+tests/golden/ref_ib.npz, from oracle/ref/harness_ib.c: one membrane iteration
+of the reference's own blocks (forces, IB interpolation with wall repulsion,
+nucleus-membrane and RBC-RBC repulsion, IB spreading, position update;
+:5659-12189) on the scene of tests/golden/ib_scene.py, state after every stage.
+
 tests/golden/ref_cells.npz, from oracle/ref/harness_cells.c: one membrane step
 run by the reference's own force blocks of its main() (CGSM_NODAL_FORCE_ZERO,
 CGSM_AREA, cell centroid/area, CGSM_LOCAL_FORCES, CGSM_VOLUME_CALC;
@@ -28,6 +33,7 @@ from oracle.bind import OracleCells, OracleLBM
 GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_setup.npz"))
 STEP = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_step.npz"))
 CELLS = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_cells.npz"))
+IB = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_ib.npz"))
 
 # the harness lattice: a tube of radius 6 around (i,j) = (20,30), fluid for
 # 7 < k < 38, wall points linked to it, all 1-based in the reference box; the
@@ -200,3 +206,82 @@ def test_membrane_pin_detects_a_wrong_modulus():
     """A mistake planted in the oracle: the shear modulus 1 % too large."""
     o, _, g, _ = run_oracle_cells("f32", Es=3.03e-6)
     assert rel(g["ftot"], CELLS["ftot"]) > 30 * CELL_TOL["f32"]["f"]
+
+
+def run_oracle_ib(precision, **overrides):
+    from golden import ib_scene as S
+    mesh = (GOLD["mesh_x"], GOLD["mesh_tri"], GOLD["nuc_x"], GOLD["nuc_edges"])
+    b, p, lbm, oc, w = S.oracle_world(mesh, IB["x"], IB["xn"], precision, **overrides)
+    assert lbm.n == int(IB["n_listed"])
+    if precision == "f32" and not overrides:
+        # the scene regenerates as the fixture's script made it (fp32 oracle)
+        _, U, V, W = lbm.moments()
+        assert np.array_equal(np.stack([U, V, W]).astype(np.float32).astype(np.float64).sum(axis=1),
+                              IB["sum_vel"])
+        wi, uv = w.wall_index(b.shape)
+        assert int(wi.sum()) == int(IB["sum_windex"])
+        assert uv.astype(np.float64).sum() == float(IB["sum_uvoid"])
+    out = {}
+    oc.forces()
+    g = oc.get()
+    out["ftot"], out["ftot_n"] = g["ftot"], g["ftot_n"]
+    w.interp()
+    out["vel_interp"], out["vel_n_interp"], out["rep_interp"], out["rep_n_interp"] = w.kinematics()
+    w.nuc_memb(rebuild=True)
+    _, _, out["rep_nuc"], out["rep_n_nuc"] = w.kinematics()
+    w.rbc_rbc()
+    _, _, out["rep_rbc"], out["rep_n_rbc"] = w.kinematics()
+    w.spread()
+    out["vel_spread"], out["vel_n_spread"], _, _ = w.kinematics()
+    out["bf"] = lbm.get_bodyforce()
+    w.update()
+    g = oc.get()
+    out["x_new"], out["xn_new"], out["status"] = g["x"], g["xn"], g["status"]
+    return out
+
+
+# Bounds relative to the largest value of each array (positions: um).  The
+# fp32 oracle evaluates the reference's float expressions; its sums run in
+# another order (node forces ~2e-5, spread body force ~5e-6, velocities ~2e-7
+# here) while the wall and RBC-RBC repulsions come out identical.  The fp64
+# oracle carries none of the reference's float rounding.
+IB_TOL = {"f32": dict(f=1e-4, fn=1e-5, v=2e-6, rep=1e-6, bf=5e-5, x=1e-6),
+          "f64": dict(f=1e-3, fn=3e-4, v=1e-5, rep=1e-5, bf=3e-4, x=1e-6)}
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_ib_stages_match_reference(precision):
+    t = IB_TOL[precision]
+    o = run_oracle_ib(precision)
+    bf_ref = np.zeros_like(o["bf"])
+    bf_ref[:, IB["bf_idx"]] = IB["bf_val"]
+    assert rel(o["ftot"], IB["ftot"]) < t["f"] and rel(o["ftot_n"], IB["ftot_n"]) < t["fn"]
+    # interpolated node velocities, and the wall repulsion (it acts on cell 2)
+    assert rel(o["vel_interp"], IB["vel_interp"]) < t["v"]
+    assert rel(o["vel_n_interp"], IB["vel_n_interp"]) < t["v"]
+    assert np.abs(IB["rep_interp"]).max() > 0
+    assert rel(o["rep_interp"], IB["rep_interp"]) < t["rep"]
+    # the nuclei stay out of reach of their membranes in this scene
+    assert np.array_equal(IB["rep_nuc"], IB["rep_interp"])
+    assert np.array_equal(o["rep_nuc"], o["rep_interp"])
+    # RBC-RBC repulsion (cells 0 and 1), as an increment
+    d_ref = IB["rep_rbc"].astype(np.float64) - IB["rep_nuc"]
+    assert np.abs(d_ref).max() > 0
+    assert rel(o["rep_rbc"] - o["rep_nuc"], d_ref) < t["rep"] * 10
+    # IB spreading: body force on the lattice and the node velocities after it
+    assert np.abs(bf_ref).max() > 0
+    assert rel(o["bf"], bf_ref) < t["bf"]
+    assert rel(o["vel_spread"], IB["vel_spread"]) < t["v"]
+    assert rel(o["vel_n_spread"], IB["vel_n_spread"]) < t["v"]
+    # position update
+    assert np.abs(IB["x_new"] - IB["x"]).max() > 0.01
+    assert np.abs(o["x_new"] - IB["x_new"]).max() < t["x"]
+    assert np.abs(o["xn_new"] - IB["xn_new"]).max() < t["x"]
+    assert np.array_equal(o["status"], IB["status"]) and int(IB["simfailure"][0]) == 0
+
+
+def test_ib_pin_detects_a_wrong_velocity_scale():
+    """A mistake planted in the oracle: the lattice-to-physical velocity scale
+    1 % too large."""
+    o = run_oracle_ib("f32", vel_scale=zf.default_params().vel_scale * 1.01)
+    assert rel(o["vel_interp"], IB["vel_interp"]) > 100 * IB_TOL["f32"]["v"]
