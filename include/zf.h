@@ -154,7 +154,9 @@ int zf_get_domlist(zf_ctx* ctx, int32_t* ijk);
 
 /* ---- fluid fields (reference F, D/U/V/W, BODYFORCE; ZebraflowWT.c:176-183) -- */
 
-/* f: [19][n_listed] populations; NULL keeps them. */
+/* f: [19][n_listed] populations; NULL keeps them.  The stored moments
+ * D,U,V,W become those of the uploaded populations (the reference's restart
+ * loads both, ZebraflowWT.c:2649-2700). */
 int zf_upload_populations(zf_ctx* ctx, const float* f);
 int zf_download_populations(zf_ctx* ctx, float* f);
 /* bodyforce: [3][n_listed], reference BODYFORCE units (IB force density) */

@@ -155,3 +155,52 @@ def test_coupled_steps_match_oracle():
     assert np.max(np.abs(xg - go["x"])) < 2e-4
     assert np.max(np.abs(xng - go["xn"])) < 2e-4
     ctx.close()
+
+
+def test_ib_stages_match_reference_output():
+    """The CUDA IB coupling against the reference's own blocks:
+    tests/golden/ref_ib.npz holds the state after each stage of one membrane
+    iteration run by the reference's forces, IB interpolation with wall
+    repulsion, nucleus-membrane and RBC-RBC repulsion, IB spreading and position
+    update blocks of its main() (ZebraflowWT.c:5659-12189) on the scene of
+    tests/golden/ib_scene.py (fixture script: tests/golden/make_ref_golden.py).
+    Bounds as against the oracle: node velocities and repulsions 1e-5 of their
+    largest value, spread body force 1e-4, positions 1e-6 um."""
+    import os
+    from golden import ib_scene as S
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    G = np.load(os.path.join(here, "ref_setup.npz"))
+    R = np.load(os.path.join(here, "ref_ib.npz"))
+    b = S.lattice()
+    p = zf.default_params(nx=S.NX, ny=S.NY, nz=S.NZ, origin=S.ORIGIN, tau=1.22, tau_from_phase=0,
+                          wall_mode=zf.WALL_REF_EQ, periodic=(0, 0, 0), stagger=50)
+    ctx = zf.Context(p)
+    ctx.set_lattice(b)
+    ctx.set_wall(*S.wall())
+    ctx.set_mesh(G["mesh_x"], G["mesh_tri"], G["nuc_x"], G["nuc_edges"])
+    ctx.set_cells(R["x"], R["xn"])
+    ctx.upload_populations(S.populations(b).astype(np.float32))  # moments follow
+
+    ctx.cgsm_forces()
+    f, fn = ctx.cell_forces()
+    assert rel_close(f, R["ftot"], 1e-4) and rel_close(fn, R["ftot_n"], 1e-4)
+    ctx.ibm_interp()
+    vg, vng, wg, wng = ctx.cell_kinematics()
+    assert rel_close(vg, R["vel_interp"], 1e-5) and rel_close(vng, R["vel_n_interp"], 1e-5)
+    assert np.abs(R["rep_interp"]).max() > 0
+    assert rel_close(wg, R["rep_interp"], 1e-5)
+    ctx.nuc_memb_repulsion(rebuild=True)
+    ctx.rbc_rbc_repulsion()
+    _, _, wg, wng = ctx.cell_kinematics()
+    assert rel_close(wg, R["rep_rbc"], 1e-5) and rel_close(wng, R["rep_n_rbc"], 1e-5)
+    ctx.ibm_spread()
+    bf_ref = np.zeros((3, int(R["n_listed"])), np.float32)
+    bf_ref[:, R["bf_idx"]] = R["bf_val"]
+    assert rel_close(ctx.download_bodyforce(), bf_ref, 1e-4)
+    vg, vng, _, _ = ctx.cell_kinematics()
+    assert rel_close(vg, R["vel_spread"], 1e-5) and rel_close(vng, R["vel_n_spread"], 1e-5)
+    ctx.update_positions()
+    xg, xng, sg = ctx.cells()
+    assert np.array_equal(sg, R["status"])
+    assert np.max(np.abs(xg - R["x_new"])) < 1e-6 and np.max(np.abs(xng - R["xn_new"])) < 1e-6
+    ctx.close()

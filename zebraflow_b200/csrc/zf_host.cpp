@@ -468,7 +468,11 @@ int zf_get_domlist(zf_ctx* c, int32_t* ijk) {
 int zf_upload_populations(zf_ctx* c, const float* f) {
   NEED_LATTICE("zf_upload_populations");
   if (!f) return ZF_OK;
-  return lbm_upload_populations(c, f);
+  int rc = lbm_upload_populations(c, f);
+  if (rc) return rc;
+  // the stored moments follow the populations, as the reference's restart
+  // loads U, V, W, D with them (ZebraflowWT.c:2649-2700)
+  return lbm_moments_launch(c);
 }
 
 int zf_download_populations(zf_ctx* c, float* f) {
