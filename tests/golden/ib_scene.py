@@ -116,3 +116,23 @@ def oracle_world(mesh, x, xn, precision="f32", **overrides):
     w = OracleWorld(lbm, oc, p)
     w.set_wall(*wall())
     return b, p, lbm, oc, w
+
+
+def wss_populations(b):
+    """Equilibrium populations for the wall-shear-stress pin: the flow of
+    populations() at a density 1.05 + 0.01 r^2/R^2 (a gauge pressure above the
+    post-processor's 120 + 1 threshold, so every wall node near the lumen is
+    valid)."""
+    dom = np.argwhere(b >= 0).astype(np.float64)
+    dx_, dy_ = dom[:, 0] - CX, dom[:, 1] - CY
+    r2 = (dx_ * dx_ + dy_ * dy_) / (R_LAT * R_LAT)
+    return populations(b) * (1.05 + 0.01 * np.minimum(r2, 1.0))
+
+
+def wall_node_normals(xyz):
+    """Unit normals of the cylinder's nodes, pointing into the lumen."""
+    o = np.array(ORIGIN)
+    dx_ = xyz[0].astype(np.float64) - (o[0] + DX * CX)
+    dy_ = xyz[1].astype(np.float64) - (o[1] + DX * CY)
+    r = np.sqrt(dx_ * dx_ + dy_ * dy_)
+    return np.stack([-dx_ / r, -dy_ / r, np.zeros_like(r)]).astype(np.float32)

@@ -17,6 +17,11 @@ it lies (main renamed) and runs two harnesses against it:
    membrane and RBC-RBC repulsion, IB spreading, position update;
    ZebraflowWT.c:5659-12189) on the scene of tests/golden/ib_scene.py ->
    ref_ib.npz (cell coordinates, scene checksums, the state after each stage);
+ * the unmodified post-processor PostProWSSandPressure.c, run on input files
+   written here (the cylinder wall mesh and node normals of
+   tests/golden/ib_scene.py, and a FLUIDdomain csv of its lattice with a
+   pressurised swirling flow) -> ref_wss.npz (wall pressure, WSS and validity
+   of every wall node, as the post-processor prints them);
  * oracle/ref/harness_step.c: five LBM steps of the reference's own
    stream-collide, wall and copy blocks of main() (ZebraflowWT.c:6101-6145,
    :6292-6433, :6601-6626) on a small capped tube with a phase-5 ball ->
@@ -116,6 +121,67 @@ def main():
                         simfailure=simfailure, **out)
     print(f"membrane step: {nc} cells, simfailure {simfailure}")
     ib_fixture()
+    wss_fixture()
+
+
+def wss_fixture():
+    import shutil
+    from golden import ib_scene as S
+    from oracle.bind import OracleLBM
+    b = S.lattice()
+    lbm = OracleLBM(b, wall_mode=1, periodic=(0, 0, 0), tau=1.22, dt=0.5, precision="f32")
+    lbm.set_f(S.wss_populations(b))
+    lbm.moments_from_f()
+    D, U, V, W = [np.asarray(a, np.float32) for a in lbm.moments()]
+    xyz, tri, _ = S.wall()
+    nrm = S.wall_node_normals(xyz)
+    run = os.path.join(ROOT, "oracle", "_ref", "wss_run")
+    shutil.rmtree(run, ignore_errors=True)
+    for d in ("InputData", "SimulationOutputData", "PostProcessedData"):
+        os.makedirs(os.path.join(run, d))
+    inp = os.path.join(run, "InputData")
+    nw = xyz.shape[1]
+    # wall nodes beyond the mesh's own keep the post-processor's zero coordinates:
+    # their search windows hold no lattice point, so they come out invalid with zero WSS
+    with open(os.path.join(inp, "WallMeshNodeCoord.dat"), "w") as f:
+        f.write(f"{nw}\n")
+        for m in range(nw):
+            f.write("%.9e %.9e %.9e\n" % (xyz[0, m], xyz[1, m], xyz[2, m]))
+    with open(os.path.join(inp, "WallMeshNodeNormals.dat"), "w") as f:
+        f.write("normals\n\n")
+        for m in range(nw):
+            f.write("%.9e %.9e %.9e\n" % (nrm[0, m], nrm[1, m], nrm[2, m]))
+    with open(os.path.join(inp, "WallMeshCells.dat"), "w") as f:  # cells: only for the VTK output
+        f.write("cells\n")
+    with open(os.path.join(inp, "WallMeshCellNormals.aa"), "w") as f:
+        f.write("normals\n\n")
+    open(os.path.join(inp, "WallMeshCellNormals.ab"), "w").close()
+    dom = np.argwhere(b >= 0)
+    o = np.array(S.REF_ORIGIN)
+    with open(os.path.join(run, "SimulationOutputData", "FLUIDdomain-000000000.csv"), "w") as f:
+        f.write("X,Y,Z,Bindex,U,V,W,D,Bx,By,Bz,EulNeigh,Windex\n")
+        for l, (i, j, k) in enumerate(dom):
+            I, J, K = (np.array([i, j, k]) + np.array(S.OFFSET))  # 0-based reference indices
+            f.write("%f,%f,%f,%d,%.9e,%.9e,%.9e,%.9e,0,0,0,0,0\n" % (
+                o[0] + I * S.DX, o[1] + J * S.DX, o[2] + K * S.DX, b[i, j, k], U[l], V[l], W[l], D[l]))
+    # the post-processor stops with "Could not open file" at the next output iteration
+    subprocess.run([os.path.join(ROOT, "oracle", "_ref", "postpro_wss")], cwd=run, check=True,
+                   stdout=open(os.path.join(run, "postpro.log"), "w"))
+    txt = open(os.path.join(run, "PostProcessedData", "Wallpressure-000000000.vtk")).read()
+    txt = txt[txt.index("POINT_DATA"):]
+
+    def section(after, before, conv):
+        a = txt.index("\n", txt.index(after)) + 1
+        z = txt.index(before, a) if before else len(txt)
+        return np.array([conv(v) for v in txt[a:z].split()[:nw]])
+    press = section("LOOKUP_TABLE", "FIELD", float)
+    wss = np.stack([section("WSSx 1", "WSSy 1", float), section("WSSy 1", "WSSz 1", float),
+                    section("WSSz 1", "Valid 1", float)])
+    valid = section("Valid 1", None, int)
+    np.savez_compressed(os.path.join(HERE, "ref_wss.npz"), press=press.astype(np.float64),
+                        wss=wss.astype(np.float64), valid=valid.astype(np.int32),
+                        sum_vel=np.stack([U, V, W, D]).astype(np.float64).sum(axis=1))
+    print(f"WSS: {nw} wall nodes, {int(valid.sum())} valid, max |WSS| {np.abs(wss).max():.4g} Pa")
 
 
 def ib_fixture():

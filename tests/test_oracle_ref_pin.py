@@ -17,6 +17,11 @@ of the reference's own blocks (forces, IB interpolation with wall repulsion,
 nucleus-membrane and RBC-RBC repulsion, IB spreading, position update;
 :5659-12189) on the scene of tests/golden/ib_scene.py, state after every stage.
 
+tests/golden/ref_wss.npz: wall pressure, wall shear stress and validity of the
+cylinder's wall nodes, printed by the unmodified post-processor
+PostProWSSandPressure.c (:275-369) run on input files of the same scene with a
+pressurised swirling flow.
+
 tests/golden/ref_cells.npz, from oracle/ref/harness_cells.c: one membrane step
 run by the reference's own force blocks of its main() (CGSM_NODAL_FORCE_ZERO,
 CGSM_AREA, cell centroid/area, CGSM_LOCAL_FORCES, CGSM_VOLUME_CALC;
@@ -28,12 +33,13 @@ import numpy as np
 import pytest
 
 import zebraflow_b200 as zf
-from oracle.bind import OracleCells, OracleLBM
+from oracle.bind import OracleCells, OracleLBM, OracleWorld
 
 GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_setup.npz"))
 STEP = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_step.npz"))
 CELLS = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_cells.npz"))
 IB = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_ib.npz"))
+WSS = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_wss.npz"))
 
 # the harness lattice: a tube of radius 6 around (i,j) = (20,30), fluid for
 # 7 < k < 38, wall points linked to it, all 1-based in the reference box; the
@@ -285,3 +291,44 @@ def test_ib_pin_detects_a_wrong_velocity_scale():
     1 % too large."""
     o = run_oracle_ib("f32", vel_scale=zf.default_params().vel_scale * 1.01)
     assert rel(o["vel_interp"], IB["vel_interp"]) > 100 * IB_TOL["f32"]["v"]
+
+
+def run_oracle_wss(precision, origin_shift=0.0):
+    from golden import ib_scene as S
+    b = S.lattice()
+    lbm = OracleLBM(b, wall_mode=1, periodic=(0, 0, 0), tau=1.22, dt=0.5, precision=precision)
+    lbm.set_f(S.wss_populations(b))
+    lbm.moments_from_f()
+    if precision == "f32":
+        D, U, V, W = lbm.moments()
+        assert np.array_equal(np.stack([U, V, W, D]).astype(np.float32).astype(np.float64).sum(axis=1),
+                              WSS["sum_vel"])
+    origin = tuple(o + origin_shift for o in S.ORIGIN)
+    w = OracleWorld(lbm, None, zf.default_params(nx=S.NX, ny=S.NY, nz=S.NZ, origin=origin,
+                                                 periodic=(0, 0, 0)))
+    xyz, tri, nrm = S.wall()
+    w.set_wall(xyz, tri, nrm)
+    return w.wss(S.wall_node_normals(xyz), pgauge=120.0)
+
+
+# The post-processor prints pressure and WSS with six decimals (Pa): the fp32
+# oracle agrees to that rounding (5e-7); the fp64 oracle to the post-processor's
+# own float rounding (WSS ~5e-6 of its largest value, pressure ~6e-4 Pa from
+# (D - 1) * 10000 / 3 in float).
+WSS_TOL = {"f32": dict(wss=1e-6, press=1e-6), "f64": dict(wss=2e-5, press=2e-3)}
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_wss_matches_reference_postprocessor(precision):
+    wss, press, valid = run_oracle_wss(precision)
+    assert np.array_equal(valid, WSS["valid"]) and valid.sum() > 0.9 * valid.size
+    assert np.abs(WSS["wss"]).max() > 0.5
+    assert np.max(np.abs(wss - WSS["wss"])) < WSS_TOL[precision]["wss"]
+    assert np.max(np.abs(press - WSS["press"])) < WSS_TOL[precision]["press"]
+
+
+def test_wss_pin_detects_a_shifted_lattice():
+    """A mistake planted in the oracle: the lattice origin off by a quarter of
+    a lattice spacing."""
+    wss, _, _ = run_oracle_wss("f32", origin_shift=0.125)
+    assert np.max(np.abs(wss - WSS["wss"])) > 1000 * WSS_TOL["f32"]["wss"]

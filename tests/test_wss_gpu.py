@@ -84,3 +84,29 @@ def test_wss_poiseuille():
     assert abs(-mean_z - expected) <= 0.1 * expected
     assert np.abs(w[:2]).mean() <= 0.05 * expected
     ctx.close()
+
+
+def test_wss_matches_reference_postprocessor():
+    """k_wss against the reference's own post-processor: tests/golden/ref_wss.npz
+    holds the wall pressure, WSS and validity that the unmodified
+    PostProWSSandPressure.c (:275-369) printed (six decimals, Pa) for the
+    cylinder of tests/golden/ib_scene.py under a pressurised swirling flow
+    (fixture script: tests/golden/make_ref_golden.py).  Bound: 1e-5 of the
+    largest WSS plus the print rounding; pressure 2e-3 Pa (one fp32 ulp of the
+    density is 4e-4 Pa of (D - 1) * 10000 / 3)."""
+    import os
+    from golden import ib_scene as S
+    R = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_wss.npz"))
+    b = S.lattice()
+    p = zf.default_params(nx=S.NX, ny=S.NY, nz=S.NZ, origin=S.ORIGIN, tau=1.22, tau_from_phase=0,
+                          wall_mode=zf.WALL_REF_EQ, periodic=(0, 0, 0))
+    ctx = zf.Context(p)
+    ctx.set_lattice(b)
+    xyz, tri, nrm = S.wall()
+    ctx.set_wall(xyz, tri, nrm)
+    ctx.upload_populations(S.wss_populations(b).astype(np.float32))
+    wss, press, valid = ctx.wss(S.wall_node_normals(xyz), pgauge=120.0)
+    assert np.array_equal(valid, R["valid"])
+    assert np.max(np.abs(wss - R["wss"])) < 1e-5 * np.abs(R["wss"]).max() + 1e-6
+    assert np.max(np.abs(press - R["press"])) < 2e-3
+    ctx.close()
