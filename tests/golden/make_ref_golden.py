@@ -178,6 +178,7 @@ def wss_fixture():
     wss = np.stack([section("WSSx 1", "WSSy 1", float), section("WSSy 1", "WSSz 1", float),
                     section("WSSz 1", "Valid 1", float)])
     valid = section("Valid 1", None, int)
+    shutil.rmtree(run)  # ~120 MB of text files
     np.savez_compressed(os.path.join(HERE, "ref_wss.npz"), press=press.astype(np.float64),
                         wss=wss.astype(np.float64), valid=valid.astype(np.int32),
                         sum_vel=np.stack([U, V, W, D]).astype(np.float64).sum(axis=1))
