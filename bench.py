@@ -28,7 +28,10 @@ One JSON line on rank 0:
           OpenMP, reference pass structure) on the host cores, one bounded
           block of 50 steps
 
-``--impl reference`` times that CPU restatement alone, as the reference arm.
+``--impl reference`` times that CPU restatement alone, as the reference arm,
+and beside it (``reference_code_lbm``) the reference's own LBM blocks, compiled
+from its source by oracle/ref/Makefile, on the part of the lattice that fits
+the reference's compile-time box.
 Input data are synthetic (seeded geometry and cells); there is no dataset.
 """
 from __future__ import annotations
@@ -269,6 +272,46 @@ def time_oracle(case, max_seconds, max_steps, stagger=50):
     return steps, mem, spent
 
 
+# the reference's compile-time lattice box (ZebraflowWT.c:81-83): IM, JM, KM
+REF_BOX = (249, 547, 723)
+
+
+def time_reference_code(case, max_seconds, max_steps):
+    """Times the reference's own LBM step (its stream-collide, wall and copy
+    blocks of main(), run by oracle/_ref/ref_time; oracle/ref/Makefile builds
+    it from ZebraflowWT.c) on the part of the workload's lattice that fits the
+    reference's compile-time box, the cut planes closed by walls.  Returns a
+    dict for the JSON line, or None when the program was not built."""
+    import tempfile
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_time")
+    if not os.path.exists(exe):
+        return None
+    nx, ny, nz = case.b.shape
+    s = np.array(case.b[:min(nx, REF_BOX[0] - 1), :min(ny, REF_BOX[1] - 1), :min(nz, REF_BOX[2] - 3)],
+                 np.int32)
+    for sl in ((slice(None), slice(None), 0), (slice(None), slice(None), -1),
+               (0, slice(None), slice(None)), (-1, slice(None), slice(None)),
+               (slice(None), 0, slice(None)), (slice(None), -1, slice(None))):
+        pl = s[sl]
+        pl[pl > 0] = 0
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "lattice.bin")
+        with open(path, "wb") as fh:
+            fh.write(np.array(s.shape, np.int32).tobytes())
+            fh.write(s.tobytes())
+        out = subprocess.run([exe, path, str(max_steps), str(max_seconds)], capture_output=True,
+                             text=True, timeout=max_seconds + 600)
+    if out.returncode != 0:
+        return {"unavailable": f"ref_time exited {out.returncode}: {out.stderr.strip()[-200:]}"}
+    fluid, steps, t, threads = out.stdout.strip().split("\n")[-1].split()
+    fluid, steps, t, threads = int(fluid), int(steps), float(t), int(threads)
+    return {"value": round(fluid * steps / t / 1e6, 3), "unit": "MLUPS", "cores": threads,
+            "kind": "reference",
+            "sample": f"{steps} LBM steps of the reference's own code on the first "
+                      f"{'x'.join(map(str, s.shape))} points of the lattice ({fluid} fluid points; "
+                      f"the reference box holds no more), after 3 warm-up steps; LBM step only"}
+
+
 def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
@@ -292,6 +335,10 @@ def run_reference(args):
         "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    ref = time_reference_code(case, args.reference_seconds, max(args.steps, 10))
+    if ref is not None:
+        # the compiled reference's own LBM blocks beside the restatement's coupled step
+        line["reference_code_lbm"] = ref
     print(json.dumps(line), flush=True)
     return 0
 
