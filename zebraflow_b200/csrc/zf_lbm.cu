@@ -627,6 +627,7 @@ struct Moments {
 };
 
 int lbm_moments_launch(zf_ctx* c) {
+  if (c->ns == 0) return ZF_OK;
   const LbmArgs a = make_args(c);  // a.fin: the current populations
   dispatch_storage<Moments>(c->p.storage, c, a);
   ZF_CUDA(cudaGetLastError());
@@ -894,6 +895,7 @@ struct Fill {
 };
 
 int lbm_init_equilibrium(zf_ctx* c) {
+  if (c->ns == 0) return ZF_OK;  // a lattice without listed points
   LbmArgs a = make_args(c);
   for (int b = 0; b < 2; ++b) {
     dispatch_storage<Fill>(c->p.storage, c, a, b);
