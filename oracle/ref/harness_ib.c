@@ -29,9 +29,15 @@
  *   zf_ref_omp_L11923  position update (region-of-interest)   :11923-12189
  * The LBM regions between them are left out (the fluid velocity is the
  * scene's) and so are the parent-domain regions (no parent cells).  Cells are
- * region-of-interest cells 345.. with CellStatus 1.  Every region runs on one
- * thread, so that the float sums it accumulates into shared arrays (spreading,
- * pairwise repulsion) come out the same on every run.
+ * region-of-interest cells 345.. with CellStatus 1.  Every cell region runs on
+ * one thread, so that the float sums it accumulates into shared arrays
+ * (spreading, pairwise repulsion) come out the same on every run.
+ *
+ * With a step count in the scene header the harness runs that many iterations
+ * of main()'s time loop instead, from the scene's populations: every iteration
+ * the LBM blocks (:6101-6145, :6292-6433, :6601-6626, after LBM_BC_SETUP), every
+ * 50th also the cell blocks above around them in main()'s order, and writes the
+ * final populations, body force and node positions.
  */
 #include <stdint.h>
 #include <stdio.h>
@@ -57,6 +63,8 @@ extern float X[IM_ + 1][JM_ + 1][KM_ + 1], Y[IM_ + 1][JM_ + 1][KM_ + 1], Z[IM_ +
 extern float Uvoid[IM_ + 1][JM_ + 1][KM_ + 1], Vvoid[IM_ + 1][JM_ + 1][KM_ + 1],
     Wvoid[IM_ + 1][JM_ + 1][KM_ + 1];
 extern float U[NL], V[NL], W[NL], D[NL], BODYFORCE[3][NL];
+extern float F[20][NL], F_OLD[20][NL];
+extern float Xlattice[3][20], UC[20], VC[20], WC[20], Wcoeff[20];
 extern float WALLNODECOORD[3][NODEW + 1], WALLCELLNORMALS[3][CELLW + 1], WALL_CENTROID[3][CELLW + 1];
 extern int WALLCELLNODE[3][CELLW + 1], WALLNODETOCELLNEIGHBORLIST[12 + 1][NODEW + 1];
 extern double NODECOORD[3][CAPSM + 1][NODEM + 1], NODECOORD_N[3][CAPSM + 1][NODEM_N + 1];
@@ -71,10 +79,14 @@ void CGSM_ZFISHRBC_DATA_GEN(void);
 void CGSM_FILAMENT_PARAMETERS(void);
 void CGSM_EQUILIBRIUM_METRICS(void);
 void LBM_DOM_SETUP(void);
+void LBM_BC_SETUP(void);
 void GOMP_parallel(void (*fn)(void*), void* data, unsigned num_threads, unsigned flags);
 void zf_ref_omp_L5659(void*);
 void zf_ref_omp_L5706(void*);
 void zf_ref_omp_L5749(void*);
+void zf_ref_omp_L6101(void*);
+void zf_ref_omp_L6292(void*);
+void zf_ref_omp_L6601(void*);
 void zf_ref_omp_L6718(void*);
 void zf_ref_omp_L6801(void*);
 void zf_ref_omp_L7513(void*);
@@ -134,7 +146,7 @@ int main(int argc, char** argv) {
   int hdr[12];
   get(fs, hdr, sizeof hdr);
   const int I0 = hdr[0], J0 = hdr[1], K0 = hdr[2], nx = hdr[3], ny = hdr[4], nz = hdr[5];
-  const int nw = hdr[6], mt = hdr[7], n_listed = hdr[10];
+  const int nw = hdr[6], mt = hdr[7], n_listed = hdr[10], n_steps = hdr[11];
   nc = hdr[8];
   const size_t npts = (size_t)nx * ny * nz;
   int32_t* b = malloc(npts * 4);
@@ -153,6 +165,11 @@ int main(int argc, char** argv) {
   get(fs, wnrm, 3 * (size_t)mt * 4);
   get(fs, cx, 3 * (size_t)nc * NODEM * 8);
   get(fs, cxn, 3 * (size_t)nc * NODEM_N * 8);
+  float* f0 = NULL;
+  if (n_steps > 0) {
+    f0 = malloc(19 * (size_t)n_listed * 4);
+    get(fs, f0, 19 * (size_t)n_listed * 4);
+  }
   fclose(fs);
   if (nc < 1 || C0 + nc - 1 > CAPSM || nw > NODEW || mt > CELLW) return 4;
 
@@ -261,6 +278,57 @@ int main(int argc, char** argv) {
 
   fo = fopen(argv[2], "wb");
   if (!fo) return 1;
+  if (n_steps > 0) {
+    /* lattice constants as main() sets them (:2471-2503), boundary list,
+       the scene's populations, no body force */
+    static const int E[19][3] = {{1, 0, 0},  {-1, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0, 0, 1},
+                                 {0, 0, -1}, {1, 1, 0},  {-1, -1, 0}, {-1, 1, 0}, {1, -1, 0},
+                                 {1, 0, 1},  {-1, 0, -1}, {-1, 0, 1}, {1, 0, -1}, {0, 1, 1},
+                                 {0, -1, -1}, {0, -1, 1}, {0, 1, -1}, {0, 0, 0}};
+    for (int c = 1; c <= 19; ++c) {
+      for (int a = 0; a < 3; ++a) Xlattice[a][c] = (float)E[c - 1][a];
+      UC[c] = Xlattice[0][c];
+      VC[c] = Xlattice[1][c];
+      WC[c] = Xlattice[2][c];
+      Wcoeff[c] = c <= 6 ? 1.f / 18.f : (c <= 18 ? 1.f / 36.f : 1.f / 3.f);
+    }
+    LBM_BC_SETUP();
+    for (int l = 1; l <= DOMMAX; ++l)
+      for (int c = 1; c <= 19; ++c) F[c][l] = F_OLD[c][l] = f0[(size_t)(c - 1) * n_listed + l - 1];
+    int i_shared = 0;
+    struct { int* i; } d4 = {&i_shared};
+    struct { int node; } d19 = {0};
+    for (int s = 1; s <= n_steps; ++s) {
+      iter = s;
+      RBCSOLVERFLAG = s % 50 == 0;
+      if (RBCSOLVERFLAG) {
+        GOMP_parallel(zf_ref_omp_L5659, NULL, 1, 0);
+        GOMP_parallel(zf_ref_omp_L5706, &d4, 1, 0);
+        GOMP_parallel(zf_ref_omp_L5749, NULL, 1, 0);
+      }
+      GOMP_parallel(zf_ref_omp_L6101, NULL, 0, 0);
+      GOMP_parallel(zf_ref_omp_L6292, NULL, 0, 0);
+      GOMP_parallel(zf_ref_omp_L6601, NULL, 0, 0);
+      if (RBCSOLVERFLAG) {
+        GOMP_parallel(zf_ref_omp_L6718, NULL, 1, 0);
+        GOMP_parallel(zf_ref_omp_L6801, &d19, 1, 0);
+        GOMP_parallel(zf_ref_omp_L7513, NULL, 1, 0);
+        GOMP_parallel(zf_ref_omp_L8694, NULL, 1, 0);
+        GOMP_parallel(zf_ref_omp_L9520, NULL, 1, 0);
+        GOMP_parallel(zf_ref_omp_L9915, NULL, 1, 0);
+        GOMP_parallel(zf_ref_omp_L10740, NULL, 1, 0);
+        GOMP_parallel(zf_ref_omp_L11923, NULL, 1, 0);
+      }
+    }
+    for (int c = 1; c <= 19; ++c) put(&F_OLD[c][1], 4 * (size_t)DOMMAX);
+    for (int a = 0; a < 3; ++a) put(&BODYFORCE[a][1], 4 * (size_t)DOMMAX);
+    put_nodes_d(NODECOORD);
+    put_nuc_d(NODECOORD_N);
+    for (int c = 0; c < nc; ++c) put(&CellStatus[C0 + c], 4);
+    put(&simfailure, 4);
+    fclose(fo);
+    return 0;
+  }
   forces(0);
   put_nodes_f(F_Total);
   put_nuc_f(F_Total_N);

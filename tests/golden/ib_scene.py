@@ -29,11 +29,17 @@ ITER = 1000             # a membrane iteration that rebuilds the nucleus lists
 UMAX = 2e-3             # lattice units
 
 
-def lattice():
+def lattice(capped=False):
+    """The tube's lattice codes; capped: the first and last z planes walls, so
+    that no fluid point pulls from outside the lattice (for LBM steps)."""
     b = zf.gen_tube(NX, NY, NZ, CX, CY, R_LAT, True)
     i, j = np.meshgrid(np.arange(NX) - CX, np.arange(NY) - CY, indexing="ij")
     thick = (i * i + j * j < (R_LAT + 6.0) ** 2)[:, :, None] & (b < 0)
     b[np.broadcast_to(thick, b.shape)] = 0
+    if capped:
+        for k in (0, NZ - 1):
+            pl = b[:, :, k]
+            pl[pl > 0] = 0
     return b
 
 
@@ -100,15 +106,16 @@ def place_cells(rest, rest_n, seed=2024):
     return np.stack(X, axis=1), np.stack(XN, axis=1)
 
 
-def oracle_world(mesh, x, xn, precision="f32", **overrides):
+def oracle_world(mesh, x, xn, precision="f32", capped=False, **overrides):
     """(lattice, params, lbm, cells, world) oracle objects of the scene; x, xn
     the cell coordinates [3][cell][node] in um; overrides: parameter changes."""
-    b = lattice()
+    b = lattice(capped)
     kw = dict(nx=NX, ny=NY, nz=NZ, origin=ORIGIN, tau=1.22, tau_from_phase=0,
               wall_mode=zf.WALL_REF_EQ, periodic=(0, 0, 0), stagger=50)
     kw.update(overrides)
     p = zf.default_params(**kw)
-    lbm = OracleLBM(b, wall_mode=1, periodic=(0, 0, 0), tau=1.22, dt=0.5, precision=precision)
+    lbm = OracleLBM(b, wall_mode=1, periodic=(0, 0, 0), tau=1.22, tau_from_phase=True, dt=0.5,
+                    precision=precision)
     lbm.set_f(populations(b))
     lbm.moments_from_f()
     oc = OracleCells(*mesh, p, precision=precision)

@@ -121,6 +121,7 @@ def main():
                         simfailure=simfailure, **out)
     print(f"membrane step: {nc} cells, simfailure {simfailure}")
     ib_fixture()
+    loop_fixture()
     wss_fixture()
 
 
@@ -183,6 +184,67 @@ def wss_fixture():
                         wss=wss.astype(np.float64), valid=valid.astype(np.int32),
                         sum_vel=np.stack([U, V, W, D]).astype(np.float64).sum(axis=1))
     print(f"WSS: {nw} wall nodes, {int(valid.sum())} valid, max |WSS| {np.abs(wss).max():.4g} Pa")
+
+
+LOOP_STEPS = 100
+
+
+def loop_fixture():
+    """100 iterations of the reference's time loop (LBM every step, cell blocks
+    at 50 and 100) on the capped IB scene, by oracle/ref/harness_ib.c."""
+    from golden import ib_scene as S
+    G = np.load(os.path.join(HERE, "ref_setup.npz"))
+    R = np.load(os.path.join(HERE, "ref_ib.npz"))
+    x, xn = R["x"], R["xn"]
+    b = S.lattice(capped=True)
+    f0 = S.populations(b).astype(np.float32)
+    n = f0.shape[1]
+    wxyz, wtri, wnrm = S.wall()
+    from oracle.bind import OracleLBM, OracleWorld
+    lbm = OracleLBM(b, wall_mode=1, periodic=(0, 0, 0), precision="f32")
+    w = OracleWorld(lbm, None, zf_params(S))
+    w.set_wall(wxyz, wtri, wnrm)
+    wi, uv = w.wall_index(b.shape)
+    nc = x.shape[1]
+    hdr = np.array(list(S.OFFSET) + [S.NX, S.NY, S.NZ, wxyz.shape[1], wtri.shape[1], nc, 0, n,
+                                     LOOP_STEPS], np.int32)
+    scene = os.path.join(ROOT, "oracle", "_ref", "loop_scene.bin")
+    with open(scene, "wb") as f:
+        for a, dt in ((hdr, np.int32), (b, np.int32), (np.zeros((3, n)), np.float32), (wi, np.int32),
+                      (uv, np.float32), (wxyz, np.float32), (wtri, np.int32), (wnrm, np.float32),
+                      (x, np.float64), (xn, np.float64), (f0, np.float32)):
+            f.write(np.ascontiguousarray(a, dt).tobytes())
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), "../_ref/ref_ib"], check=True)
+    out = os.path.join(ROOT, "oracle", "_ref", "ref_loop.bin")
+    run = os.path.join(ROOT, "oracle", "_ref", "run")
+    subprocess.run([os.path.join(ROOT, "oracle", "_ref", "ref_ib"), scene, out], cwd=run, check=True,
+                   stdout=open(os.path.join(ROOT, "oracle", "_ref", "ref_loop.log"), "w"))
+    raw = open(out, "rb").read()
+    pos = [0]
+
+    def rd(dt, shape):
+        k = int(np.prod(shape))
+        r = np.frombuffer(raw, dt, k, pos[0]).copy().reshape(shape)
+        pos[0] += r.itemsize * k
+        return r
+    f = rd(np.float32, (19, n))
+    bf = rd(np.float32, (3, n))
+    x_new, xn_new = rd(np.float64, (3, nc, x.shape[2])), rd(np.float64, (3, nc, xn.shape[2]))
+    status, simf = rd(np.int32, (nc,)), rd(np.int32, (1,))
+    assert pos[0] == len(raw)
+    sample = np.arange(0, n, 97, dtype=np.int32)
+    nzr = np.flatnonzero(np.any(bf != 0, axis=0)).astype(np.int32)
+    np.savez_compressed(os.path.join(HERE, "ref_loop.npz"), steps=LOOP_STEPS, sample=sample,
+                        f_sample=f[:, sample], f_sum=f.astype(np.float64).sum(axis=1),
+                        bf_idx=nzr, bf_val=bf[:, nzr], x_new=x_new, xn_new=xn_new, status=status,
+                        simfailure=simf)
+    print(f"time loop: {LOOP_STEPS} steps, {n} listed points, moved up to "
+          f"{np.abs(x_new - x).max():.3f} um, simfailure {int(simf[0])}")
+
+
+def zf_params(S):
+    import zebraflow_b200 as zf
+    return zf.default_params(nx=S.NX, ny=S.NY, nz=S.NZ, origin=S.ORIGIN, periodic=(0, 0, 0))
 
 
 def ib_fixture():

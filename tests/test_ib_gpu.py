@@ -204,3 +204,38 @@ def test_ib_stages_match_reference_output():
     assert np.array_equal(sg, R["status"])
     assert np.max(np.abs(xg - R["x_new"])) < 1e-6 and np.max(np.abs(xng - R["xn_new"])) < 1e-6
     ctx.close()
+
+
+def test_time_loop_matches_reference_output():
+    """The CUDA time loop against the reference's own: tests/golden/ref_loop.npz
+    holds populations (a sample), body force and node positions after 100
+    iterations of the reference's loop (LBM blocks every step, its cell blocks at
+    50 and 100; ZebraflowWT.c:5646-12189) on the capped scene of
+    tests/golden/ib_scene.py.  Bounds: populations 2e-6 (they move by ~6e-4),
+    body force 1e-3 of its largest value (float atomics in the spreading),
+    positions 1e-5 um."""
+    import os
+    from golden import ib_scene as S
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    G = np.load(os.path.join(here, "ref_setup.npz"))
+    R = np.load(os.path.join(here, "ref_ib.npz"))
+    L = np.load(os.path.join(here, "ref_loop.npz"))
+    b = S.lattice(capped=True)
+    p = zf.default_params(nx=S.NX, ny=S.NY, nz=S.NZ, origin=S.ORIGIN, tau=1.22, tau_from_phase=1,
+                          wall_mode=zf.WALL_REF_EQ, periodic=(0, 0, 0), stagger=50)
+    ctx = zf.Context(p)
+    ctx.set_lattice(b)
+    ctx.set_wall(*S.wall())
+    ctx.set_mesh(G["mesh_x"], G["mesh_tri"], G["nuc_x"], G["nuc_edges"])
+    ctx.set_cells(R["x"], R["xn"])
+    ctx.upload_populations(S.populations(b).astype(np.float32))
+    ctx.step(int(L["steps"]))
+    f = ctx.download_populations()
+    assert np.max(np.abs(f[:, L["sample"]] - L["f_sample"])) < 2e-6
+    bf_ref = np.zeros((3, f.shape[1]), np.float32)
+    bf_ref[:, L["bf_idx"]] = L["bf_val"]
+    assert rel_close(ctx.download_bodyforce(), bf_ref, 1e-3)
+    xg, xng, sg = ctx.cells()
+    assert np.array_equal(sg, L["status"])
+    assert np.max(np.abs(xg - L["x_new"])) < 1e-5 and np.max(np.abs(xng - L["xn_new"])) < 1e-5
+    ctx.close()

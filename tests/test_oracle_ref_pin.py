@@ -17,6 +17,10 @@ of the reference's own blocks (forces, IB interpolation with wall repulsion,
 nucleus-membrane and RBC-RBC repulsion, IB spreading, position update;
 :5659-12189) on the scene of tests/golden/ib_scene.py, state after every stage.
 
+tests/golden/ref_loop.npz, from the same harness: 100 iterations of the
+reference's time loop (LBM blocks every step, the cell blocks at 50 and 100)
+on that scene with its z ends capped, from its flow at rest force.
+
 tests/golden/ref_wss.npz: wall pressure, wall shear stress and validity of the
 cylinder's wall nodes, printed by the unmodified post-processor
 PostProWSSandPressure.c (:275-369) run on input files of the same scene with a
@@ -40,6 +44,7 @@ STEP = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_step.npz")
 CELLS = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_cells.npz"))
 IB = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_ib.npz"))
 WSS = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_wss.npz"))
+LOOP = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_loop.npz"))
 
 # the harness lattice: a tube of radius 6 around (i,j) = (20,30), fluid for
 # 7 < k < 38, wall points linked to it, all 1-based in the reference box; the
@@ -332,3 +337,35 @@ def test_wss_pin_detects_a_shifted_lattice():
     a lattice spacing."""
     wss, _, _ = run_oracle_wss("f32", origin_shift=0.125)
     assert np.max(np.abs(wss - WSS["wss"])) > 1000 * WSS_TOL["f32"]["wss"]
+
+
+# 100 coupled iterations: populations change by ~6e-4 and agree to ~3e-7
+# (fp32 and fp64 oracles alike: the reference's own float rounding), spread
+# body force to ~3e-5 of its largest value, positions to ~2e-6 um.
+LOOP_TOL = {"f32": dict(f=1e-6, bf=2e-4, x=1e-5), "f64": dict(f=2e-6, bf=3e-4, x=1e-5)}
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_time_loop_matches_reference(precision):
+    from golden import ib_scene as S
+    t = LOOP_TOL[precision]
+    mesh = (GOLD["mesh_x"], GOLD["mesh_tri"], GOLD["nuc_x"], GOLD["nuc_edges"])
+    b, p, lbm, oc, w = S.oracle_world(mesh, IB["x"], IB["xn"], precision, capped=True)
+    f0 = S.populations(b)
+    lbm.set_f(f0)
+    w.step(int(LOOP["steps"]))
+    f = lbm.get_f()
+    smp = LOOP["sample"]
+    assert np.abs(LOOP["f_sample"] - f0[:, smp]).max() > 1e-4
+    assert np.max(np.abs(f[:, smp] - LOOP["f_sample"])) < t["f"]
+    assert np.allclose(f.sum(axis=1), LOOP["f_sum"], rtol=1e-5, atol=0)
+    bf = lbm.get_bodyforce()
+    bf_ref = np.zeros_like(bf)
+    bf_ref[:, LOOP["bf_idx"]] = LOOP["bf_val"]
+    assert np.abs(bf_ref).max() > 0
+    assert rel(bf, bf_ref) < t["bf"]
+    g = oc.get()
+    assert np.abs(LOOP["x_new"] - IB["x"]).max() > 0.01
+    assert np.max(np.abs(g["x"] - LOOP["x_new"])) < t["x"]
+    assert np.max(np.abs(g["xn"] - LOOP["xn_new"])) < t["x"]
+    assert np.array_equal(g["status"], LOOP["status"]) and int(LOOP["simfailure"][0]) == 0

@@ -376,7 +376,22 @@ __global__ void k_lbm_wall(LbmArgs a, const int32_t* __restrict__ wall_slot,
   if (w >= n_wall) return;
   const int64_t slot = wall_slot[w];
   const int nb = wall_nbr[w];
-  const float rho_m = nb >= 0 ? a.rho_pre[nb] : a.rho_ref;
+  // D_bc = D[m] of the designated neighbour (ZebraflowWT.c:6306-6311): a fluid
+  // neighbour's density is this step's (k_lbm wrote it); a wall neighbour's is
+  // what the reference's copy pass left in D, the density of its populations
+  // of the previous step, read back from fin
+  float rho_m = a.rho_ref;
+  if (nb >= 0) {
+    if (a.code[nb] == ZF_CODE_WALL) {
+      const T* __restrict__ fin = static_cast<const T*>(a.fin);
+      float r = 0.f;
+#pragma unroll
+      for (int q = 0; q < ZF_Q; ++q) r += WQ(q) * C::dec(fin[pop_at(q, (int64_t)nb)], q, a);
+      rho_m = a.rho_ref + r;
+    } else {
+      rho_m = a.rho_pre[nb];
+    }
+  }
   T* __restrict__ fout = static_cast<T*>(a.fout);
   float r2 = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
 #pragma unroll
