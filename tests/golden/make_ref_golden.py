@@ -30,7 +30,9 @@ it lies (main renamed) and runs two harnesses against it:
 The fixtures keep the inputs and the reference's outputs so that the pins run
 where the reference tree is absent.
 
-Usage: python tests/golden/make_ref_golden.py [reference_dir]
+Usage: python tests/golden/make_ref_golden.py [reference_dir [output_dir]]
+(output_dir defaults to tests/golden; tests/test_oracle_ref_pin.py regenerates
+the fixtures into a scratch folder and compares them with the committed ones)
 """
 import gzip
 import os
@@ -41,6 +43,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
+OUT = HERE  # where the fixtures go (second argument)
 sys.path[:0] = [ROOT, os.path.join(ROOT, "tests")]  # the package, the oracle, tests/golden
 
 
@@ -56,7 +59,10 @@ def read_mesh(ref):
 
 
 def main():
+    global OUT
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) > 2:
+        OUT = sys.argv[2]
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), f"REF={ref}"], check=True)
     raw = open(os.path.join(ROOT, "oracle", "_ref", "ref_setup.bin"), "rb").read()
     a = np.frombuffer(raw, np.int32)
@@ -73,7 +79,7 @@ def main():
     bc = a[p:p + 7 * bcmax].reshape(bcmax, 7).copy(); p += 7 * bcmax
     assert p == a.size
     X, T, XN, EN = read_mesh(ref)
-    np.savez_compressed(os.path.join(HERE, "ref_setup.npz"), mesh_x=X, mesh_tri=T, nuc_x=XN,
+    np.savez_compressed(os.path.join(OUT, "ref_setup.npz"), mesh_x=X, mesh_tri=T, nuc_x=XN,
                         nuc_edges=EN, edges=edges, epar=epar, epar_n=epar_n, domlist=domlist,
                         bclist=bc[:, :4], bcnlist=bc[:, 4:])
     print(f"edges {ne}, nucleus edges {nen}, listed points {dommax}, boundary points {bcmax}")
@@ -89,7 +95,7 @@ def main():
                    ("W", 1), ("bfN", 3)):
         out[key] = f[p:p + k * n].reshape(k, n).copy().squeeze(); p += k * n
     assert p == a.size
-    np.savez_compressed(os.path.join(HERE, "ref_step.npz"), listed=listed, steps=steps, **out)
+    np.savez_compressed(os.path.join(OUT, "ref_step.npz"), listed=listed, steps=steps, **out)
     print(f"LBM step: {n} listed points, {steps} steps")
 
     raw = open(os.path.join(ROOT, "oracle", "_ref", "ref_cells.bin"), "rb").read()
@@ -117,7 +123,7 @@ def main():
         if m % 3 == 0 and k not in ("tri_area",):  # [cell][3][n] -> [3][cell][n]
             a = a.reshape(nc, 3, -1).transpose(1, 0, 2)
         out[k] = a
-    np.savez_compressed(os.path.join(HERE, "ref_cells.npz"), tri_area_eq=area_eq,
+    np.savez_compressed(os.path.join(OUT, "ref_cells.npz"), tri_area_eq=area_eq,
                         simfailure=simfailure, **out)
     print(f"membrane step: {nc} cells, simfailure {simfailure}")
     ib_fixture()
@@ -180,7 +186,7 @@ def wss_fixture():
                     section("WSSz 1", "Valid 1", float)])
     valid = section("Valid 1", None, int)
     shutil.rmtree(run)  # ~120 MB of text files
-    np.savez_compressed(os.path.join(HERE, "ref_wss.npz"), press=press.astype(np.float64),
+    np.savez_compressed(os.path.join(OUT, "ref_wss.npz"), press=press.astype(np.float64),
                         wss=wss.astype(np.float64), valid=valid.astype(np.int32),
                         sum_vel=np.stack([U, V, W, D]).astype(np.float64).sum(axis=1))
     print(f"WSS: {nw} wall nodes, {int(valid.sum())} valid, max |WSS| {np.abs(wss).max():.4g} Pa")
@@ -193,8 +199,8 @@ def loop_fixture():
     """100 iterations of the reference's time loop (LBM every step, cell blocks
     at 50 and 100) on the capped IB scene, by oracle/ref/harness_ib.c."""
     from golden import ib_scene as S
-    G = np.load(os.path.join(HERE, "ref_setup.npz"))
-    R = np.load(os.path.join(HERE, "ref_ib.npz"))
+    G = np.load(os.path.join(OUT, "ref_setup.npz"))
+    R = np.load(os.path.join(OUT, "ref_ib.npz"))
     x, xn = R["x"], R["xn"]
     b = S.lattice(capped=True)
     f0 = S.populations(b).astype(np.float32)
@@ -234,7 +240,7 @@ def loop_fixture():
     assert pos[0] == len(raw)
     sample = np.arange(0, n, 97, dtype=np.int32)
     nzr = np.flatnonzero(np.any(bf != 0, axis=0)).astype(np.int32)
-    np.savez_compressed(os.path.join(HERE, "ref_loop.npz"), steps=LOOP_STEPS, sample=sample,
+    np.savez_compressed(os.path.join(OUT, "ref_loop.npz"), steps=LOOP_STEPS, sample=sample,
                         f_sample=f[:, sample], f_sum=f.astype(np.float64).sum(axis=1),
                         bf_idx=nzr, bf_val=bf[:, nzr], x_new=x_new, xn_new=xn_new, status=status,
                         simfailure=simf)
@@ -249,7 +255,7 @@ def zf_params(S):
 
 def ib_fixture():
     from golden import ib_scene as S
-    G = np.load(os.path.join(HERE, "ref_setup.npz"))
+    G = np.load(os.path.join(OUT, "ref_setup.npz"))
     mesh = (G["mesh_x"], G["mesh_tri"], G["nuc_x"], G["nuc_edges"])
     x, xn = S.place_cells(G["mesh_x"], G["nuc_x"])
     b, p, lbm, oc, w = S.oracle_world(mesh, x, xn, "f32")
@@ -293,7 +299,7 @@ def ib_fixture():
     res["simfailure"] = rd(np.int32, (1,))
     assert pos[0] == len(raw)
     nzr = np.flatnonzero(np.any(bf != 0, axis=0)).astype(np.int32)  # spread body force, sparse
-    np.savez_compressed(os.path.join(HERE, "ref_ib.npz"), x=x, xn=xn, bf_idx=nzr, bf_val=bf[:, nzr],
+    np.savez_compressed(os.path.join(OUT, "ref_ib.npz"), x=x, xn=xn, bf_idx=nzr, bf_val=bf[:, nzr],
                         sum_vel=vel.astype(np.float64).sum(axis=1), sum_windex=np.int64(wi.sum()),
                         sum_uvoid=uv.astype(np.float64).sum(), n_listed=n, **res)
     print(f"IB stages: {nc} cells, {n} listed points, {nzr.size} points with spread force, "

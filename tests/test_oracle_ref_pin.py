@@ -369,3 +369,21 @@ def test_time_loop_matches_reference(precision):
     assert np.max(np.abs(g["x"] - LOOP["x_new"])) < t["x"]
     assert np.max(np.abs(g["xn"] - LOOP["xn_new"])) < t["x"]
     assert np.array_equal(g["status"], LOOP["status"]) and int(LOOP["simfailure"][0]) == 0
+
+
+@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="reference tree not present")
+def test_fixtures_regenerate_from_the_reference(tmp_path):
+    """The committed fixtures are what tests/golden/make_ref_golden.py makes
+    from the reference tree: regenerated into a scratch folder, every array is
+    identical."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    subprocess.run([sys.executable, os.path.join(root, "tests", "golden", "make_ref_golden.py"),
+                    "/root/reference", str(tmp_path)], check=True, capture_output=True)
+    for name in ("ref_setup", "ref_step", "ref_cells", "ref_ib", "ref_loop", "ref_wss"):
+        a = np.load(os.path.join(root, "tests", "golden", name + ".npz"))
+        b = np.load(os.path.join(str(tmp_path), name + ".npz"))
+        assert sorted(a.files) == sorted(b.files), name
+        for k in a.files:
+            assert np.array_equal(a[k], b[k]), (name, k)
