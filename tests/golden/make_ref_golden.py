@@ -127,6 +127,7 @@ def main():
                         simfailure=simfailure, **out)
     print(f"membrane step: {nc} cells, simfailure {simfailure}")
     ib_fixture()
+    ib_fixture(nucleus=True)
     loop_fixture()
     wss_fixture()
 
@@ -253,11 +254,17 @@ def zf_params(S):
     return zf.default_params(nx=S.NX, ny=S.NY, nz=S.NZ, origin=S.ORIGIN, periodic=(0, 0, 0))
 
 
-def ib_fixture():
+def ib_fixture(nucleus=False):
+    """The stage-by-stage IB fixture (ref_ib.npz); nucleus: the variant whose
+    nuclei reach their membranes, run on the reference build with a 20-row tp
+    array (ref_nuc.npz, nucleus-membrane stage only)."""
     from golden import ib_scene as S
     G = np.load(os.path.join(OUT, "ref_setup.npz"))
     mesh = (G["mesh_x"], G["mesh_tri"], G["nuc_x"], G["nuc_edges"])
-    x, xn = S.place_cells(G["mesh_x"], G["nuc_x"])
+    if nucleus:
+        x, xn = S.place_cells(G["mesh_x"], G["nuc_x"], nucleus_scale=1.0, flatten3=0.92)
+    else:
+        x, xn = S.place_cells(G["mesh_x"], G["nuc_x"])
     b, p, lbm, oc, w = S.oracle_world(mesh, x, xn, "f32")
     _, U, V, W = lbm.moments()
     vel = np.stack([U, V, W]).astype(np.float32)
@@ -272,11 +279,18 @@ def ib_fixture():
                       (uv, np.float32), (wxyz, np.float32), (wtri, np.int32), (wnrm, np.float32),
                       (x, np.float64), (xn, np.float64)):
             f.write(np.ascontiguousarray(a, dt).tobytes())
-    out = os.path.join(ROOT, "oracle", "_ref", "ref_ib.bin")
+    out = os.path.join(ROOT, "oracle", "_ref", "ref_nuc.bin" if nucleus else "ref_ib.bin")
     if os.path.exists(out):
         os.remove(out)
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), "../_ref/ref_ib.bin"],
-                   check=True)
+    if nucleus:
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), "../_ref/ref_ib_tp20"],
+                       check=True)
+        subprocess.run([os.path.join(ROOT, "oracle", "_ref", "ref_ib_tp20"), scene, out],
+                       cwd=os.path.join(ROOT, "oracle", "_ref", "run"), check=True,
+                       stdout=open(os.path.join(ROOT, "oracle", "_ref", "ref_nuc.log"), "w"))
+    else:
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), "../_ref/ref_ib.bin"],
+                       check=True)
     raw = open(out, "rb").read()
     pos = [0]
 
@@ -298,6 +312,13 @@ def ib_fixture():
     res["status"] = rd(np.int32, (nc,))
     res["simfailure"] = rd(np.int32, (1,))
     assert pos[0] == len(raw)
+    if nucleus:
+        np.savez_compressed(os.path.join(OUT, "ref_nuc.npz"), x=x, xn=xn,
+                            rep_interp=res["rep_interp"], rep_n_interp=res["rep_n_interp"],
+                            rep_nuc=res["rep_nuc"], rep_n_nuc=res["rep_n_nuc"])
+        touched = int(np.any(res["rep_nuc"] != res["rep_interp"], axis=0).sum())
+        print(f"nucleus-membrane stage: {touched} membrane nodes repelled")
+        return
     nzr = np.flatnonzero(np.any(bf != 0, axis=0)).astype(np.int32)  # spread body force, sparse
     np.savez_compressed(os.path.join(OUT, "ref_ib.npz"), x=x, xn=xn, bf_idx=nzr, bf_val=bf[:, nzr],
                         sum_vel=vel.astype(np.float64).sum(axis=1), sum_windex=np.int64(wi.sum()),

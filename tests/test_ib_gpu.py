@@ -239,3 +239,34 @@ def test_time_loop_matches_reference_output():
     assert np.array_equal(sg, L["status"])
     assert np.max(np.abs(xg - L["x_new"])) < 1e-5 and np.max(np.abs(xng - L["xn_new"])) < 1e-5
     ctx.close()
+
+
+def test_nucleus_membrane_stage_matches_reference_output():
+    """k_nuc_memb against the reference's nucleus-membrane block, built with its
+    sub-point array tp widened to the 20 rows its loops use (the shipped
+    declaration holds 16, ZebraflowWT.c:2307): tests/golden/ref_nuc.npz holds
+    the repulsion increments on the scene variant of tests/golden/ib_scene.py
+    whose nuclei reach their membranes.  Bound: 1e-5 of the largest increment."""
+    import os
+    from golden import ib_scene as S
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    G = np.load(os.path.join(here, "ref_setup.npz"))
+    N = np.load(os.path.join(here, "ref_nuc.npz"))
+    b = S.lattice()
+    p = zf.default_params(nx=S.NX, ny=S.NY, nz=S.NZ, origin=S.ORIGIN, tau=1.22, tau_from_phase=0,
+                          wall_mode=zf.WALL_REF_EQ, periodic=(0, 0, 0), stagger=50)
+    ctx = zf.Context(p)
+    ctx.set_lattice(b)
+    ctx.set_wall(*S.wall())
+    ctx.set_mesh(G["mesh_x"], G["mesh_tri"], G["nuc_x"], G["nuc_edges"])
+    ctx.set_cells(N["x"], N["xn"])
+    ctx.upload_populations(S.populations(b).astype(np.float32))
+    ctx.cgsm_forces()
+    ctx.ibm_interp()
+    _, _, w0, _ = ctx.cell_kinematics()
+    ctx.nuc_memb_repulsion(rebuild=True)
+    _, _, w1, _ = ctx.cell_kinematics()
+    d_ref = N["rep_nuc"].astype(np.float64) - N["rep_interp"]
+    assert np.abs(d_ref).max() > 0
+    assert rel_close(w1.astype(np.float64) - w0, d_ref, 1e-5)
+    ctx.close()

@@ -17,6 +17,11 @@ of the reference's own blocks (forces, IB interpolation with wall repulsion,
 nucleus-membrane and RBC-RBC repulsion, IB spreading, position update;
 :5659-12189) on the scene of tests/golden/ib_scene.py, state after every stage.
 
+tests/golden/ref_nuc.npz, from the same harness linked against a build of the
+reference whose nucleus-membrane sub-point array tp holds the 20 rows its loops
+use (declared with 16, ZebraflowWT.c:2307): the nucleus-membrane stage on the
+scene's variant whose nuclei reach their membranes.
+
 tests/golden/ref_loop.npz, from the same harness: 100 iterations of the
 reference's time loop (LBM blocks every step, the cell blocks at 50 and 100)
 on that scene with its z ends capped, from its flow at rest force.
@@ -45,6 +50,7 @@ CELLS = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_cells.npz
 IB = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_ib.npz"))
 WSS = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_wss.npz"))
 LOOP = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_loop.npz"))
+NUC = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_nuc.npz"))
 
 # the harness lattice: a tube of radius 6 around (i,j) = (20,30), fluid for
 # 7 < k < 38, wall points linked to it, all 1-based in the reference box; the
@@ -291,6 +297,25 @@ def test_ib_stages_match_reference(precision):
     assert np.array_equal(o["status"], IB["status"]) and int(IB["simfailure"][0]) == 0
 
 
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_nucleus_membrane_stage_matches_reference(precision):
+    from golden import ib_scene as S
+    mesh = (GOLD["mesh_x"], GOLD["mesh_tri"], GOLD["nuc_x"], GOLD["nuc_edges"])
+    b, p, lbm, oc, w = S.oracle_world(mesh, NUC["x"], NUC["xn"], precision)
+    oc.forces()
+    w.interp()
+    _, _, r0, rn0 = w.kinematics()
+    w.nuc_memb(rebuild=True)
+    _, _, r1, rn1 = w.kinematics()
+    d_ref = NUC["rep_nuc"].astype(np.float64) - NUC["rep_interp"]
+    touched = np.any(d_ref != 0, axis=0)
+    assert touched.sum() > 20
+    assert np.array_equal(np.any(r1 - r0 != 0, axis=0), touched)
+    # fp32: the same float expressions (6e-9 of the largest increment here); fp64: 3e-6
+    assert rel(r1 - r0, d_ref) < (1e-6 if precision == "f32" else 3e-5)
+    assert np.array_equal(rn1, rn0) and np.array_equal(NUC["rep_n_nuc"], NUC["rep_n_interp"])
+
+
 def test_ib_pin_detects_a_wrong_velocity_scale():
     """A mistake planted in the oracle: the lattice-to-physical velocity scale
     1 % too large."""
@@ -381,7 +406,7 @@ def test_fixtures_regenerate_from_the_reference(tmp_path):
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     subprocess.run([sys.executable, os.path.join(root, "tests", "golden", "make_ref_golden.py"),
                     "/root/reference", str(tmp_path)], check=True, capture_output=True)
-    for name in ("ref_setup", "ref_step", "ref_cells", "ref_ib", "ref_loop", "ref_wss"):
+    for name in ("ref_setup", "ref_step", "ref_cells", "ref_ib", "ref_nuc", "ref_loop", "ref_wss"):
         a = np.load(os.path.join(root, "tests", "golden", name + ".npz"))
         b = np.load(os.path.join(str(tmp_path), name + ".npz"))
         assert sorted(a.files) == sorted(b.files), name
