@@ -62,8 +62,8 @@ void zf_ref_omp_L6718(void*);
 void zf_ref_omp_L6801(void*);
 void zf_ref_omp_L7513(void*);
 
-#define NCELL 2
-static const int CELL[NCELL] = {345, 346};
+#define NCELL 4
+static const int CELL[NCELL] = {345, 346, 347, 348};
 
 static uint64_t rng = 0x2545F4914F6CDD1Dull;
 static double u01(void) {
@@ -89,7 +89,8 @@ static void membrane_step(int geometry_only) {
   GOMP_parallel(zf_ref_omp_L5749, NULL, 0, 0);
   if (geometry_only) return;
   GOMP_parallel(zf_ref_omp_L6718, NULL, 0, 0);
-  GOMP_parallel(zf_ref_omp_L6801, &d19, 0, 0);
+  /* one thread: the block counts screened forces into the shared simfailure */
+  GOMP_parallel(zf_ref_omp_L6801, &d19, 1, 0);
   GOMP_parallel(zf_ref_omp_L7513, NULL, 0, 0);
 }
 
@@ -129,20 +130,31 @@ int main(int argc, char** argv) {
   for (int t = 1; t <= TRIM; ++t) TRI_AREA_eq[t] = TRI_AREA[c0][t];
   for (int n = 1; n <= NODEM; ++n) NODE_AREA0[n] = NODE_AREA[c0][n];
 
-  /* two deformed cells: rest mesh stretched (1.06, 0.97, 1.0) and (0.98,
-     1.03, 1.05), moved into the box, node noise 0.03 um (nucleus 0.02 um) */
-  const double stretch[NCELL][3] = {{1.06, 0.97, 1.0}, {0.98, 1.03, 1.05}};
-  const double shift[NCELL][3] = {{60.0, 150.0, 150.0}, {75.0, 160.0, 170.0}};
+  /* four deformed cells: rest mesh stretched, moved into the box, with node
+     noise 0.03 um (nucleus 0.02 um); the last two with noise large enough
+     that force screening acts (0.3 um) and that the cell is removed (1 um) */
+  const double stretch[NCELL][3] = {{1.06, 0.97, 1.0}, {0.98, 1.03, 1.05}, {1.0, 1.0, 1.0},
+                                    {1.0, 1.0, 1.0}};
+  const double shift[NCELL][3] = {{60.0, 150.0, 150.0}, {75.0, 160.0, 170.0},
+                                  {90.0, 150.0, 150.0}, {105.0, 160.0, 170.0}};
+  const double noise[NCELL] = {0.03, 0.03, 0.3, 1.0};
   for (int s = 0; s < NCELL; ++s) {
     const int c = CELL[s];
     for (int n = 1; n <= NODEM; ++n)
       for (int a = 0; a < 3; ++a)
-        NODECOORD[a][c][n] = NODECOORD[a][1][n] * stretch[s][a] + shift[s][a] + 0.03 * nrm();
+        NODECOORD[a][c][n] = NODECOORD[a][1][n] * stretch[s][a] + shift[s][a] + noise[s] * nrm();
     for (int n = 1; n <= NODEM_N; ++n)
       for (int a = 0; a < 3; ++a)
         NODECOORD_N[a][c][n] = NODECOORD_N[a][1][n] * stretch[s][a] + shift[s][a] + 0.02 * nrm();
     CellStatus[c] = 1;
   }
+  /* the input coordinates (a removed cell's are overwritten by the step) */
+  static double x_in[NCELL][3][NODEM + 1], xn_in[NCELL][3][NODEM_N + 1];
+  for (int s = 0; s < NCELL; ++s)
+    for (int a = 0; a < 3; ++a) {
+      for (int n = 1; n <= NODEM; ++n) x_in[s][a][n] = NODECOORD[a][CELL[s]][n];
+      for (int n = 1; n <= NODEM_N; ++n) xn_in[s][a][n] = NODECOORD_N[a][CELL[s]][n];
+    }
   simfailure = 0;
   printf("membrane step of the deformed cells\n");
   fflush(stdout);
@@ -155,8 +167,8 @@ int main(int argc, char** argv) {
   put(f, &TRI_AREA_eq[1], 4 * TRIM);
   for (int s = 0; s < NCELL; ++s) {
     const int c = CELL[s];
-    for (int a = 0; a < 3; ++a) put(f, &NODECOORD[a][c][1], 8 * NODEM);
-    for (int a = 0; a < 3; ++a) put(f, &NODECOORD_N[a][c][1], 8 * NODEM_N);
+    for (int a = 0; a < 3; ++a) put(f, &x_in[s][a][1], 8 * NODEM);
+    for (int a = 0; a < 3; ++a) put(f, &xn_in[s][a][1], 8 * NODEM_N);
     for (int a = 0; a < 3; ++a) put(f, &F_Total[a][c][1], 4 * NODEM);
     for (int a = 0; a < 3; ++a) put(f, &F_Total_N[a][c][1], 4 * NODEM_N);
     put(f, &TRI_AREA[c][1], 4 * TRIM);

@@ -54,13 +54,14 @@ def test_mesh_topology_and_calibration_match_oracle():
 
 def test_membrane_forces_match_reference_output():
     """k_membrane against the reference's own membrane step:
-    tests/golden/ref_cells.npz holds the node forces, triangle geometry and
-    per-cell terms that the reference's force blocks of its main()
-    (ZebraflowWT.c:5706-7535) computed for two deformed RBCs with nuclei built
-    from the shipped meshes (fixture script: tests/golden/make_ref_golden.py).
-    Default parameters are the reference's constants (moduli, RBC_SURF, MCV).
-    Bounds as for the oracle comparison: node forces within 1e-4 of the largest
-    force, geometry 2e-5."""
+    tests/golden/ref_cells.npz holds the node forces, triangle geometry,
+    per-cell terms, screening counts and removals that the reference's force
+    blocks of its main() (ZebraflowWT.c:5706-7535) computed for four deformed
+    RBCs with nuclei built from the shipped meshes (the third with one screened
+    force component, the fourth removed; fixture script:
+    tests/golden/make_ref_golden.py).  Default parameters are the reference's
+    constants (moduli, RBC_SURF, MCV).  Bounds as for the oracle comparison:
+    node forces within 1e-4 of the largest force, geometry 2e-5; statuses exact."""
     import os
     here = os.path.join(os.path.dirname(__file__), "golden")
     G = np.load(os.path.join(here, "ref_setup.npz"))
@@ -71,17 +72,20 @@ def test_membrane_forces_match_reference_output():
     ctx.set_mesh(G["mesh_x"], G["mesh_tri"], G["nuc_x"], G["nuc_edges"])
     ctx.set_cells(C["x"], C["xn"])
     ctx.cgsm_forces()
+    _, _, status = ctx.cells()
+    assert np.array_equal(status, C["status"][:, 0])
     f, fn = ctx.cell_forces()
     assert np.max(np.abs(f - C["ftot"])) < 1e-4 * np.abs(C["ftot"]).max()
     assert np.max(np.abs(fn - C["ftot_n"])) < 1e-4 * np.abs(C["ftot_n"]).max()
     ta, tn, tc, nrm, cf = ctx.cell_geometry()
-    assert np.allclose(ta, C["tri_area"], rtol=2e-5)
-    assert np.max(np.abs(tn - C["tri_normal"])) < 2e-5
-    assert np.max(np.abs(tc - C["tri_centroid"])) < 2e-5 * np.abs(C["tri_centroid"]).max()
-    assert np.max(np.abs(nrm - C["node_normal"])) < 2e-5
-    assert np.allclose(cf[:, :2], C["cell"][:, :2], rtol=2e-5)      # area, volume
-    assert np.allclose(cf[:, 2:5], C["cell"][:, 2:5], rtol=2e-6)    # centroid
-    assert np.allclose(cf[:, 5:7], C["cell"][:, 5:7], rtol=2e-3, atol=1e-9)
+    live = C["status"][:, 0] == 1
+    assert np.allclose(ta[live], C["tri_area"][live], rtol=2e-5)
+    assert np.max(np.abs(tn[:, live] - C["tri_normal"][:, live])) < 2e-5
+    assert np.max(np.abs(tc[:, live] - C["tri_centroid"][:, live])) < 2e-5 * np.abs(C["tri_centroid"]).max()
+    assert np.max(np.abs(nrm[:, live] - C["node_normal"][:, live])) < 2e-5
+    assert np.allclose(cf[live, :2], C["cell"][live, :2], rtol=2e-5)      # area, volume
+    assert np.allclose(cf[live, 2:5], C["cell"][live, 2:5], rtol=2e-6)    # centroid
+    assert np.allclose(cf[live, 5:7], C["cell"][live, 5:7], rtol=2e-3, atol=1e-9)
     ctx.close()
 
 
