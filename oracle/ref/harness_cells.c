@@ -1,6 +1,6 @@
 /*
  * ORACLE — test infrastructure only.  Runs the reference's own membrane step
- * (forces of two deformed RBCs with nuclei) and writes inputs and outputs to a
+ * (forces of four deformed RBCs with nuclei, one screened, one removed) and writes inputs and outputs to a
  * binary file that the oracle tests compare with the CPU restatement.
  *
  * Linked against ZebraflowWT.c compiled where it lies (`main` renamed) and
