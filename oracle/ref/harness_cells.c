@@ -1,7 +1,8 @@
 /*
  * ORACLE — test infrastructure only.  Runs the reference's own membrane step
- * (forces of four deformed RBCs with nuclei, one screened, one removed) and writes inputs and outputs to a
- * binary file that the oracle tests compare with the CPU restatement.
+ * (forces of four deformed RBCs with nuclei, one screened, one removed) and
+ * writes inputs and outputs to a binary file that the oracle tests compare
+ * with the CPU restatement.
  *
  * Linked against ZebraflowWT.c compiled where it lies (`main` renamed) and
  * passed through oracle/ref/expose_omp.py (OpenMP regions of main() callable as
@@ -89,7 +90,8 @@ static void membrane_step(int geometry_only) {
   GOMP_parallel(zf_ref_omp_L5749, NULL, 0, 0);
   if (geometry_only) return;
   GOMP_parallel(zf_ref_omp_L6718, NULL, 0, 0);
-  /* one thread: the block counts screened forces into the shared simfailure */
+  /* one thread: the block counts screened forces into the shared simfailure
+     without atomics */
   GOMP_parallel(zf_ref_omp_L6801, &d19, 1, 0);
   GOMP_parallel(zf_ref_omp_L7513, NULL, 0, 0);
 }
