@@ -335,7 +335,7 @@ def run_reference(args):
         "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
-    ref = time_reference_code(case, args.reference_seconds, max(args.steps, 10))
+    ref = time_reference_code(case, min(30.0, args.reference_seconds), max(args.steps, 10))
     if ref is not None:
         # the compiled reference's own LBM blocks beside the restatement's coupled step
         line["reference_code_lbm"] = ref
