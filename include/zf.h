@@ -192,10 +192,15 @@ int zf_lbm_step_mass(zf_ctx* ctx, int store_moments, int zero_bodyforce, double*
  * device array of 65,536 + 1 doubles (512 KB, held on every GPU that loads the
  * library until exit), so it serves lattices of at most 65,536 blocks of four
  * 4x4x4 tiles with fluid (262,144 tiles); larger ones get ZF_ERR_ARG with a
- * message.  The first call on a device looks the array's address up
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * message.  The first call on a device does the set-up: it looks the array's
+ * address up (cudaGetSymbolAddress) and, with lazy module loading, may load the
+ * library's device code, which is when the array's 512 KB are reserved; make
+ * that first call once, as a warm-up, before the caller's allocator takes the
+ * GPU and before any stream capture.  The address is cached per device for the
+ * primary context: do not call this again on a device after cudaDeviceReset.
  * Every call overwrites the scratch, so nothing carries over between calls;
- * calls that overlap on the GPU share the scratch and race. */
+ * calls that overlap on the GPU (other streams or contexts of the same device)
+ * share the scratch and race. */
 int zf_lbm_step_mass_noalloc(zf_ctx* ctx, int store_moments, int zero_bodyforce, double* mass);
 
 /* Z-slab halo exchange (no counterpart in the reference, which runs on one
@@ -413,6 +418,13 @@ int zf_launch_count(zf_ctx* ctx, int64_t* n);
 int zf_profile(zf_ctx* ctx, int enable, int capacity);
 int zf_profile_read(zf_ctx* ctx, float* lbm_ms, int* lbm_count, float* membrane_ms,
                     int* membrane_count);
+
+/* Per-stage device time (ms) of the membrane iterations profiled since
+ * zf_profile(ctx, 1, ...), summed over `*blocks` iterations: stage_ms[8] =
+ * {membrane forces, LBM step, IB interpolation + wall repulsion,
+ *  nucleus-membrane repulsion, cell-list build, RBC-RBC repulsion,
+ *  IB spreading, position update}. */
+int zf_profile_stages(zf_ctx* ctx, float* stage_ms, int* blocks);
 
 /* Completed iterations (the reference's iter). */
 int zf_iteration(zf_ctx* ctx, int64_t* iter);

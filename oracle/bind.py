@@ -84,6 +84,24 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+_inputs = None
+
+
+def inputs():
+    """The workload generators and reference parameter defaults compiled into
+    this library (orc_gen.cpp), with the interface of zebraflow_b200.inputs():
+    a CPU run builds the same inputs as the GPU library without loading it."""
+    global _inputs
+    if _inputs is None:
+        import sys
+        root = os.path.dirname(_HERE)
+        if root not in sys.path:
+            sys.path.insert(0, root)
+        from zebraflow_b200 import Inputs  # the ctypes binding class only; libzf.so is not loaded
+        _inputs = Inputs(lib(), "orc_")
+    return _inputs
+
+
 class OracleCells:
     """Reference membrane set-up and membrane step (ZebraflowWT.c:1592-2460,
     :5704-7535) restated in C; see oracle/orc_cells.inc."""

@@ -60,7 +60,8 @@ def read_mesh(ref):
 
 def main():
     global OUT
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    from oracle.refsrc import reference_dir
+    ref = sys.argv[1] if len(sys.argv) > 1 else reference_dir()
     if len(sys.argv) > 2:
         OUT = sys.argv[2]
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), f"REF={ref}"], check=True)

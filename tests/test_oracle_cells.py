@@ -11,8 +11,9 @@ import pytest
 
 import zebraflow_b200 as zf
 from oracle.bind import OracleCells
+from oracle.refsrc import reference_dir
 
-REF = "/root/reference"
+REF = reference_dir()
 
 
 def ellipsoid_meshes():

@@ -45,6 +45,7 @@ import pytest
 
 import zebraflow_b200 as zf
 from oracle.bind import OracleCells, OracleLBM, OracleWorld
+from oracle.refsrc import have_reference, reference_dir
 
 GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_setup.npz"))
 STEP = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_step.npz"))
@@ -405,7 +406,7 @@ def test_time_loop_matches_reference(precision):
     assert np.array_equal(g["status"], LOOP["status"]) and int(LOOP["simfailure"][0]) == 0
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="reference tree not present")
+@pytest.mark.skipif(not have_reference(), reason="reference tree not present")
 def test_fixtures_regenerate_from_the_reference(tmp_path):
     """The committed fixtures are what tests/golden/make_ref_golden.py makes
     from the reference tree: regenerated into a scratch folder, every array is
@@ -414,7 +415,7 @@ def test_fixtures_regenerate_from_the_reference(tmp_path):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     subprocess.run([sys.executable, os.path.join(root, "tests", "golden", "make_ref_golden.py"),
-                    "/root/reference", str(tmp_path)], check=True, capture_output=True)
+                    reference_dir(), str(tmp_path)], check=True, capture_output=True)
     for name in ("ref_setup", "ref_step", "ref_cells", "ref_ib", "ref_nuc", "ref_loop", "ref_wss"):
         a = np.load(os.path.join(root, "tests", "golden", name + ".npz"))
         b = np.load(os.path.join(str(tmp_path), name + ".npz"))

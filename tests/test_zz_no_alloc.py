@@ -6,10 +6,14 @@ already reserved the GPU, and time loops that must not take cudaMalloc's
 implicit device synchronisation or an out-of-memory failure mid-run.  Its
 reduction scratch is a file-scope device array instead of cudaMalloc'd memory.
 
-Checked here through the C ABI: two calls in a row give the same mass and the
-same populations as the allocating entry point on an identical context, and a
-lattice larger than the fixed scratch is refused with a clear error.  This file
-sorts last so that a run stopping at the first failure has run everything else.
+Checked here through the C ABI, for every population storage form and with
+and without the moments written: two calls in a row give the same mass,
+populations and moments as the allocating entry point on an identical
+context; the mass equals an FP64 sum of the densities of the populations
+downloaded before each call; neither the context's device memory nor the
+GPU's free memory changes across the calls; and a lattice larger than the
+fixed scratch is refused with a clear error.  This file sorts last so that a
+run stopping at the first failure has run everything else.
 """
 import ctypes
 
@@ -20,11 +24,14 @@ import zebraflow_b200 as zf
 
 pytestmark = pytest.mark.gpu
 
+STORAGES = {"f32": zf.STORE_F32, "f16": zf.STORE_F16, "bf16": zf.STORE_BF16, "f32dev": zf.STORE_F32_DEV}
 
-def make_context(b, rng_seed):
+
+def make_context(b, rng_seed, storage):
     nx, ny, nz = b.shape
     p = zf.default_params(nx=nx, ny=ny, nz=nz, tau=0.85, tau_from_phase=0,
-                          wall_mode=zf.WALL_HALFWAY_BB, periodic=(0, 0, 1), g=(0, 0, 1e-5))
+                          wall_mode=zf.WALL_HALFWAY_BB, periodic=(0, 0, 1), g=(0, 0, 1e-5),
+                          storage=storage)
     ctx = zf.Context(p)
     ctx.set_lattice(b)
     rng = np.random.default_rng(rng_seed)
@@ -35,21 +42,55 @@ def make_context(b, rng_seed):
     return ctx
 
 
-def test_noalloc_matches_allocating_step_twice():
+@pytest.mark.parametrize("store_moments", [0, 1])
+@pytest.mark.parametrize("storage", sorted(STORAGES))
+def test_noalloc_matches_allocating_step_twice(storage, store_moments):
+    import torch
     b = zf.gen_tube(32, 30, 48, 15.2, 14.7, 13.0, True)
-    ref = make_context(b, 21)
-    new = make_context(b, 21)
+    ref = make_context(b, 21, STORAGES[storage])
+    new = make_context(b, 21, STORAGES[storage])
+    dom = new.domlist()
+    fluid = b[dom[:, 0], dom[:, 1], dom[:, 2]] > 0
+    L = zf.lib()
+    # the allocating entry sizes its scratch on its first call: make that call
+    # on both contexts before memory is compared
+    m_ref, m_new = ctypes.c_double(), ctypes.c_double()
+    zf._check(L.zf_lbm_step_mass(ref._h, store_moments, 0, ctypes.byref(m_ref)))
+    zf._check(L.zf_lbm_step_mass_noalloc(new._h, store_moments, 0, ctypes.byref(m_new)))
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    ctx_bytes0 = new.device_bytes()
     for call in range(2):
-        m_ref, m_new = ctypes.c_double(), ctypes.c_double()
-        zf._check(zf.lib().zf_lbm_step_mass(ref._h, 0, 0, ctypes.byref(m_ref)))
-        zf._check(zf.lib().zf_lbm_step_mass_noalloc(new._h, 0, 0, ctypes.byref(m_new)))
+        f_before = new.download_populations().astype(np.float64)
+        zf._check(L.zf_lbm_step_mass(ref._h, store_moments, 0, ctypes.byref(m_ref)))
+        zf._check(L.zf_lbm_step_mass_noalloc(new._h, store_moments, 0, ctypes.byref(m_new)))
         # the same step kernel on the same inputs: the sums agree to fp64 rounding
         assert abs(m_new.value - m_ref.value) <= 1e-12 * abs(m_ref.value), call
-        assert m_new.value > 0
-        # and the populations the step wrote agree within the fp32 parity bound
+        # and the sum is the FP64 total of the pre-step densities (each formed
+        # in fp32 inside the kernel, hence the fp32-rounding tolerance)
+        direct = float(f_before[:, fluid].sum())
+        assert abs(m_new.value - direct) <= 1e-6 * direct, (call, m_new.value, direct)
+        # the populations (and moments) the step wrote agree within the fp32 parity bound
         assert np.max(np.abs(new.download_populations() - ref.download_populations())) < 2e-6
+        if store_moments:
+            for a, r in zip(new.download_moments(), ref.download_moments()):
+                assert np.max(np.abs(a[fluid] - r[fluid])) < 2e-6
+    torch.cuda.synchronize()
+    assert new.device_bytes() == ctx_bytes0
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
     ref.close()
     new.close()
+
+
+def test_noalloc_counts_its_launches():
+    b = zf.gen_tube(24, 24, 16, 11.5, 11.5, 9.0, True)
+    ctx = make_context(b, 5, zf.STORE_F32)
+    n0 = ctx.launch_count()
+    m = ctypes.c_double()
+    zf._check(zf.lib().zf_lbm_step_mass_noalloc(ctx._h, 0, 0, ctypes.byref(m)))
+    assert ctx.launch_count() - n0 == 2  # the step kernel and the sum (no wall pass in bounce-back mode)
+    ctx.close()
 
 
 def test_noalloc_refuses_lattice_beyond_its_scratch():

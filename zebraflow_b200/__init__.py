@@ -65,7 +65,6 @@ _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 
 # name -> (restype, argtypes)
 _SIGS = {
-    "zf_params_default": (None, [C.POINTER(Params)]),
     "zf_params_size": (C.c_size_t, []),
     "zf_create": (_P, [C.POINTER(Params), C.c_int]),
     "zf_destroy": (None, [_P]),
@@ -89,11 +88,6 @@ _SIGS = {
     "zf_mass": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double)]),
     "zf_lbm_steps_timed": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float)]),
     "zf_device_bytes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
-    "zf_gen_tube": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
-                              C.c_int, _i32p]),
-    "zf_gen_bifurcation": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
-                                     C.c_double, _i32p, C.c_void_p]),
-    "zf_gen_icosphere": (C.c_int, [C.c_int, _f64p, _i32p]),
     "zf_set_mesh": (C.c_int, [_P, C.c_int, C.c_int, _i32p, _f64p, C.c_int, C.c_int, _i32p, _f64p]),
     "zf_mesh_info": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_double),
                                C.POINTER(C.c_double)]),
@@ -121,13 +115,7 @@ _SIGS = {
     "zf_profile": (C.c_int, [_P, C.c_int, C.c_int]),
     "zf_profile_read": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int),
                                   C.POINTER(C.c_float), C.POINTER(C.c_int)]),
-    "zf_gen_wall_tube": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
-                                   _f64p, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int),
-                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
-    "zf_gen_wall_bifurcation": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
-                                          C.c_double, _f64p, C.c_double, C.POINTER(C.c_int),
-                                          C.POINTER(C.c_int), C.c_void_p, C.c_void_p, C.c_void_p,
-                                          C.c_int, C.c_int]),
+    "zf_profile_stages": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "zf_wss": (C.c_int, [_P, C.c_void_p, C.c_double, _f32p, C.c_void_p, C.c_void_p]),
     "zf_wss_objective": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, C.c_void_p,
                                    C.c_void_p, C.POINTER(C.c_double)]),
@@ -143,9 +131,6 @@ _SIGS = {
     "zf_flux_adjoint": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, _f32p, _i32p, C.c_int,
                                   _f32p, C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p,
                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
-    "zf_gen_cells": (C.c_int, [_i32p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, C.c_int,
-                               C.c_int, C.c_int, _f64p, C.c_int, _f64p, _f64p, C.c_double,
-                               C.c_double, C.c_uint64, _f64p, _f64p, C.POINTER(C.c_int)]),
 }
 
 
@@ -178,88 +163,161 @@ def _check(rc: int) -> None:
         raise ZfError(rc, lib().zf_last_error().decode(errors="replace"))
 
 
+_GEN_SIGS = {
+    "params_default": (None, [C.POINTER(Params)]),
+    "gen_tube": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _i32p]),
+    "gen_bifurcation": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _i32p,
+                                  C.c_void_p]),
+    "gen_icosphere": (C.c_int, [C.c_int, _f64p, _i32p]),
+    "gen_wall_tube": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, _f64p,
+                                C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_int, C.c_int]),
+    "gen_wall_bifurcation": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _f64p,
+                                       C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "gen_cells": (C.c_int, [_i32p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, C.c_int, C.c_int, C.c_int,
+                            _f64p, C.c_int, _f64p, _f64p, C.c_double, C.c_double, C.c_uint64, _f64p, _f64p,
+                            C.POINTER(C.c_int)]),
+}
+
+
+class Inputs:
+    """Reference parameter defaults and the workload generators of
+    zebraflow_b200/csrc/zf_gen.cpp, bound to a library that exports them under
+    `prefix`: libzf.so ("zf_"), or the CPU arm's oracle/liboracle.so ("orc_"),
+    which compiles the same source, so that a CPU run builds the same inputs
+    without loading the GPU library."""
+
+    def __init__(self, L: C.CDLL, prefix: str):
+        self._L, self._pre = L, prefix
+        for name, (res, args) in _GEN_SIGS.items():
+            fn = getattr(L, prefix + name)
+            fn.restype = res
+            fn.argtypes = args
+
+    def _fn(self, name):
+        return getattr(self._L, self._pre + name)
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != ZF_OK:
+            raise ZfError(rc, f"{self._pre}{what} failed")
+
+    def default_params(self, **kw) -> Params:
+        p = Params()
+        self._fn("params_default")(C.byref(p))
+        for k, v in kw.items():
+            if k in ("origin", "g", "periodic"):
+                arr = getattr(p, k)
+                for i, x in enumerate(v):
+                    arr[i] = x
+            else:
+                setattr(p, k, v)
+        return p
+
+    def gen_tube(self, nx, ny, nz, cx, cy, R, periodic_z=True) -> np.ndarray:
+        b = np.empty(nx * ny * nz, np.int32)
+        self._check(self._fn("gen_tube")(nx, ny, nz, cx, cy, R, int(periodic_z), b), "gen_tube")
+        return b.reshape(nx, ny, nz)
+
+    def gen_bifurcation(self, nx, ny, nz, Rp, Rd, half_angle_deg=20.0):
+        b = np.empty(nx * ny * nz, np.int32)
+        layout = (C.c_double * 6)()
+        self._check(self._fn("gen_bifurcation")(nx, ny, nz, Rp, Rd, half_angle_deg, b,
+                                                C.cast(layout, C.c_void_p)), "gen_bifurcation")
+        return b.reshape(nx, ny, nz), list(layout)
+
+    def gen_icosphere(self, level: int):
+        """Unit icosphere: (xyz [n][3] float64, tri [m][3] int32 1-based)."""
+        n, m = 10 * 4 ** level + 2, 20 * 4 ** level
+        xyz = np.empty(3 * n)
+        tri = np.empty(3 * m, np.int32)
+        self._check(self._fn("gen_icosphere")(level, xyz, tri), "gen_icosphere")
+        return xyz.reshape(n, 3), tri.reshape(m, 3)
+
+    def _wall_out(self, name, *args):
+        fn = self._fn(name)
+        nn_, nt_ = C.c_int(), C.c_int()
+        self._check(fn(*args, C.byref(nn_), C.byref(nt_), None, None, None, 0, 0), name)
+        xyz = np.empty(3 * nn_.value, np.float32)
+        tri = np.empty(3 * nt_.value, np.int32)
+        nrm = np.empty(3 * nt_.value, np.float32)
+        self._check(fn(*args, C.byref(nn_), C.byref(nt_), _ptr(xyz), _ptr(tri), _ptr(nrm), nn_.value,
+                       nt_.value), name)
+        return xyz.reshape(3, -1), tri.reshape(3, -1), nrm.reshape(3, -1)
+
+    def gen_wall_tube(self, cx, cy, R, nz, origin=(0.0, 0.0, 0.0), dx=0.5, h=1.0, nseg=None):
+        """Cylinder wall mesh in um: (xyz [3][n], tri [3][m] 1-based, normals [3][m])."""
+        if nseg is None:
+            nseg = max(12, int(round(2 * np.pi * R / h)))
+        return self._wall_out("gen_wall_tube", cx, cy, R, nz, h, nseg, np.asarray(origin, np.float64), dx)
+
+    def gen_wall_bifurcation(self, nx, ny, nz, Rp, Rd, half_angle_deg=20.0, origin=(0.0, 0.0, 0.0), dx=0.5):
+        return self._wall_out("gen_wall_bifurcation", nx, ny, nz, Rp, Rd, half_angle_deg,
+                              np.asarray(origin, np.float64), dx)
+
+    def gen_cells(self, b, n_cells, rest, rest_n, axes, seed=1234, origin=(0.0, 0.0, 0.0), dx=0.5,
+                  periodic_z=True, margin=0.25, wall_clear=0.0):
+        """Seeded placement; returns (x [3][placed][n_node], xn [3][placed][n_node_n]).
+        margin (um) inflates each cell's ellipsoid against the others; wall_clear
+        (um) is the least lattice (Chebyshev) distance of every membrane node
+        from a non-fluid point, at least one lattice unit."""
+        b = np.ascontiguousarray(b, np.int32)
+        nx, ny, nz = b.shape
+        rest = np.ascontiguousarray(rest, np.float64)
+        rest_n = np.ascontiguousarray(rest_n, np.float64)
+        nn_, nnn = rest.shape[0], rest_n.shape[0]
+        x = np.zeros(3 * n_cells * nn_)
+        xn = np.zeros(max(3 * n_cells * nnn, 1))
+        placed = C.c_int()
+        self._check(self._fn("gen_cells")(b.ravel(), nx, ny, nz, np.asarray(origin, np.float64), dx,
+                                          int(periodic_z), n_cells, nn_, rest.ravel(), nnn, rest_n.ravel(),
+                                          np.asarray(axes, np.float64), margin, wall_clear, seed, x, xn,
+                                          C.byref(placed)), "gen_cells")
+        k = placed.value
+        x = x.reshape(3, n_cells, nn_)[:, :k, :].copy()
+        xn = xn[:3 * n_cells * nnn].reshape(3, n_cells, nnn)[:, :k, :].copy()
+        return x, xn
+
+
+_inputs = None
+
+
+def inputs() -> Inputs:
+    """The generators and parameter defaults of libzf.so."""
+    global _inputs
+    if _inputs is None:
+        _inputs = Inputs(lib(), "zf_")
+    return _inputs
+
+
 def default_params(**kw) -> Params:
-    p = Params()
-    lib().zf_params_default(C.byref(p))
-    for k, v in kw.items():
-        if k in ("origin", "g", "periodic"):
-            arr = getattr(p, k)
-            for i, x in enumerate(v):
-                arr[i] = x
-        else:
-            setattr(p, k, v)
-    return p
+    return inputs().default_params(**kw)
 
 
 def gen_tube(nx, ny, nz, cx, cy, R, periodic_z=True) -> np.ndarray:
-    b = np.empty(nx * ny * nz, np.int32)
-    _check(lib().zf_gen_tube(nx, ny, nz, cx, cy, R, int(periodic_z), b))
-    return b.reshape(nx, ny, nz)
+    return inputs().gen_tube(nx, ny, nz, cx, cy, R, periodic_z)
 
 
 def gen_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg=20.0):
-    b = np.empty(nx * ny * nz, np.int32)
-    layout = (C.c_double * 6)()
-    _check(lib().zf_gen_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg, b,
-                                    C.cast(layout, C.c_void_p)))
-    return b.reshape(nx, ny, nz), list(layout)
+    return inputs().gen_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg)
 
 
 def gen_icosphere(level: int):
-    """Unit icosphere: (xyz [n][3] float64, tri [m][3] int32 1-based)."""
-    n, m = 10 * 4 ** level + 2, 20 * 4 ** level
-    xyz = np.empty(3 * n)
-    tri = np.empty(3 * m, np.int32)
-    _check(lib().zf_gen_icosphere(level, xyz, tri))
-    return xyz.reshape(n, 3), tri.reshape(m, 3)
-
-
-def _wall_out(fn, *args):
-    nn_, nt_ = C.c_int(), C.c_int()
-    _check(fn(*args, C.byref(nn_), C.byref(nt_), None, None, None, 0, 0))
-    xyz = np.empty(3 * nn_.value, np.float32)
-    tri = np.empty(3 * nt_.value, np.int32)
-    nrm = np.empty(3 * nt_.value, np.float32)
-    _check(fn(*args, C.byref(nn_), C.byref(nt_), _ptr(xyz), _ptr(tri), _ptr(nrm), nn_.value,
-              nt_.value))
-    return xyz.reshape(3, -1), tri.reshape(3, -1), nrm.reshape(3, -1)
+    return inputs().gen_icosphere(level)
 
 
 def gen_wall_tube(cx, cy, R, nz, origin=(0.0, 0.0, 0.0), dx=0.5, h=1.0, nseg=None):
-    """Cylinder wall mesh in um: (xyz [3][n], tri [3][m] 1-based, normals [3][m])."""
-    if nseg is None:
-        nseg = max(12, int(round(2 * np.pi * R / h)))
-    return _wall_out(lib().zf_gen_wall_tube, cx, cy, R, nz, h, nseg,
-                     np.asarray(origin, np.float64), dx)
+    return inputs().gen_wall_tube(cx, cy, R, nz, origin, dx, h, nseg)
 
 
 def gen_wall_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg=20.0, origin=(0.0, 0.0, 0.0), dx=0.5):
-    return _wall_out(lib().zf_gen_wall_bifurcation, nx, ny, nz, Rp, Rd, half_angle_deg,
-                     np.asarray(origin, np.float64), dx)
+    return inputs().gen_wall_bifurcation(nx, ny, nz, Rp, Rd, half_angle_deg, origin, dx)
 
 
 def gen_cells(b, n_cells, rest, rest_n, axes, seed=1234, origin=(0.0, 0.0, 0.0), dx=0.5,
               periodic_z=True, margin=0.25, wall_clear=0.0):
-    """Seeded placement; returns (x [3][placed][n_node], xn [3][placed][n_node_n]).
-    margin (um) inflates each cell's ellipsoid against the others; wall_clear
-    (um) is the least lattice (Chebyshev) distance of every membrane node
-    from a non-fluid point, at least one lattice unit."""
-    b = np.ascontiguousarray(b, np.int32)
-    nx, ny, nz = b.shape
-    rest = np.ascontiguousarray(rest, np.float64)
-    rest_n = np.ascontiguousarray(rest_n, np.float64)
-    nn_, nnn = rest.shape[0], rest_n.shape[0]
-    x = np.zeros(3 * n_cells * nn_)
-    xn = np.zeros(max(3 * n_cells * nnn, 1))
-    placed = C.c_int()
-    _check(lib().zf_gen_cells(b.ravel(), nx, ny, nz, np.asarray(origin, np.float64), dx,
-                              int(periodic_z), n_cells, nn_, rest.ravel(), nnn, rest_n.ravel(),
-                              np.asarray(axes, np.float64), margin, wall_clear, seed, x, xn,
-                              C.byref(placed)))
-    k = placed.value
-    x = x.reshape(3, n_cells, nn_)[:, :k, :].copy()
-    xn = xn[:3 * n_cells * nnn].reshape(3, n_cells, nnn)[:, :k, :].copy()
-    return x, xn
+    return inputs().gen_cells(b, n_cells, rest, rest_n, axes, seed, origin, dx, periodic_z, margin,
+                              wall_clear)
 
 
 def mesh_edges(tri1: np.ndarray) -> np.ndarray:
@@ -568,6 +626,16 @@ class Context:
         lm, lc, mm, mc = C.c_float(), C.c_int(), C.c_float(), C.c_int()
         _check(lib().zf_profile_read(self._h, C.byref(lm), C.byref(lc), C.byref(mm), C.byref(mc)))
         return lm.value, lc.value, mm.value, mc.value
+
+    PROFILE_STAGES = ("membrane_forces", "lbm", "ib_interp", "nuc_memb", "cell_list", "rbc_rbc",
+                      "ib_spread", "update")
+
+    def profile_stages(self):
+        """({stage: summed ms} over the profiled membrane iterations, blocks)."""
+        st = (C.c_float * 8)()
+        nb = C.c_int()
+        _check(lib().zf_profile_stages(self._h, st, C.byref(nb)))
+        return dict(zip(self.PROFILE_STAGES, list(st))), nb.value
 
     def set_stream(self, stream_handle):
         """Queue the context's work on a CUDA stream (a cudaStream_t as int);

@@ -53,49 +53,6 @@ const char* zf_last_error(void) { return g_last_error.c_str(); }
 
 size_t zf_params_size(void) { return sizeof(zf_params); }
 
-void zf_params_default(zf_params* p) {
-  std::memset(p, 0, sizeof *p);
-  // ZebraflowWT.c:81-87 (ROI box) and :40-41 (DX, DT)
-  p->nx = 249;
-  p->ny = 547;
-  p->nz = 723;
-  p->origin[0] = -1.0;
-  p->origin[1] = 29.0;
-  p->origin[2] = -27.0;
-  p->dx = 0.5;
-  p->dt = 0.5;
-  // TauPlasma = 0.5 + MU_SCALE*MU = 1.22 (ZebraflowWT.c:62); phase-dependent (ZebraflowWT.c:6110)
-  p->tau = 1.22f;
-  p->tau_from_phase = 1;
-  p->wall_mode = ZF_WALL_REF_EQ;
-  p->storage = ZF_STORE_F32;
-  p->rho_ref = 1.0f;
-  p->stagger = 50;                 // SOLVERSTAGGER, ZebraflowWT.c:151
-  p->Es = 3.e-06;                  // ZebraflowWT.c:130
-  p->Es_nucleus_ratio = 0.1;       // ZebraflowWT.c:2039
-  p->kbend = 1.3856406e-19;        // ZebraflowWT.c:129
-  p->kd = 3.6e-05;                 // ZebraflowWT.c:131
-  p->ka = 7.7e-05;                 // ZebraflowWT.c:132
-  p->kv = 55.;                     // ZebraflowWT.c:133
-  p->area0 = 144.916e-012;         // RBC_SURF, ZebraflowWT.c:127
-  p->volume0 = 97.5671e-018;       // MCV, ZebraflowWT.c:126
-  p->kT = 300 * 1.3806488e-023;    // TEMPERATURE*BOLTZ, ZebraflowWT.c:36-37
-  p->e_ratio_eq = 0.3154574132;    // ZebraflowWT.c:134
-  p->calib_passes = 51;            // iterrelax loop, ZebraflowWT.c:2339-2346
-  p->gamma_p = 1.e-07;             // ZebraflowWT.c:125
-  p->unit_mass = 0.5e-6 * 0.5e-6 * 0.5e-6 * 10. * 1000.;  // UNITMASS, ZebraflowWT.c:50-51
-  p->bforce_scale = 1. / 3. * 0.5e-6 / (0.5e-6 * 0.5e-6);  // LBM_BFORCE_SCALE, ZebraflowWT.c:65
-  p->vel_scale = 1.0;              // VEL_SCALE, ZebraflowWT.c:67
-  p->vmax_remove = 5.e-3;          // ZebraflowWT.c:11976
-  p->remove_count = 500;           // ZebraflowWT.c:7473
-  p->nuc_list_period = 1000;       // ZebraflowWT.c:9527
-  p->nuc_list_max = 1004;          // NucMembMAX, ZebraflowWT.c:158
-  p->stochastic_round = 1;
-  // WALLNODETOCELLNEIGHBORLIST holds 12 entries but its overflow check fires
-  // above 24 (ZebraflowWT.c:221, :3911-3934); 24 is the capacity here
-  p->wall_list_max = 24;
-}
-
 zf_ctx* zf_create(const zf_params* p, int device) {
   if (!p) {
     set_error("zf_create: params is NULL");

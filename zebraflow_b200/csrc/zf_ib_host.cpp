@@ -360,10 +360,17 @@ static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
     const bool last = s == nsteps - 1;
     int rc;
     if (membrane && (rc = close_run())) return rc;
+    // on profiled membrane iterations an event precedes each stage and one
+    // follows the last: [forces][LBM][interp][nucleus][bins][RBC-RBC][spread][update]
     const bool pm = c->profiling && membrane && c->prof_mem < c->prof_cap;
-    if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (c->prof_cap + c->prof_mem)], c->stream));
+    auto mark = [&](int k) -> int {
+      if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (size_t)c->prof_cap + ZF_PROF_MARKS * (size_t)c->prof_mem + k],
+                                      c->stream));
+      return ZF_OK;
+    };
+    if ((rc = mark(0))) return rc;
     if (membrane && (rc = cells_membrane_launch(c))) return rc;
-    if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (c->prof_cap + c->prof_mem) + 1], c->stream));
+    if ((rc = mark(1))) return rc;
     if (!membrane && c->profiling && !c->prof_open && c->prof_lbm < c->prof_cap) {
       ZF_CUDA(cudaEventRecord(c->prof_ev[2 * c->prof_lbm], c->stream));
       c->prof_open = true;
@@ -373,19 +380,16 @@ static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
       return rc;
     if (c->prof_open) c->prof_open_n++;
     if (membrane) {
-      if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (2 * c->prof_cap + c->prof_mem)], c->stream));
       const bool rebuild = !c->nuc_lists_valid || (iter % c->p.nuc_list_period == 0);
-      if ((rc = ib_interp_launch(c))) return rc;
-      if ((rc = ib_nuc_memb_launch(c, rebuild))) return rc;
+      if ((rc = mark(2)) || (rc = ib_interp_launch(c))) return rc;
+      if ((rc = mark(3)) || (rc = ib_nuc_memb_launch(c, rebuild))) return rc;
       c->nuc_lists_valid = true;
-      if ((rc = ib_bins_launch(c))) return rc;
-      if ((rc = ib_rbc_rbc_launch(c))) return rc;
-      if ((rc = ib_spread_launch(c))) return rc;
-      if ((rc = ib_update_launch(c))) return rc;
-      if (pm) {
-        ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (2 * c->prof_cap + c->prof_mem) + 1], c->stream));
-        c->prof_mem++;
-      }
+      if ((rc = mark(4)) || (rc = ib_bins_launch(c))) return rc;
+      if ((rc = mark(5)) || (rc = ib_rbc_rbc_launch(c))) return rc;
+      if ((rc = mark(6)) || (rc = ib_spread_launch(c))) return rc;
+      if ((rc = mark(7)) || (rc = ib_update_launch(c))) return rc;
+      if ((rc = mark(8))) return rc;
+      if (pm) c->prof_mem++;
     }
     c->status.iter = iter;
   }
@@ -417,16 +421,30 @@ int zf_profile(zf_ctx* c, int enable, int capacity) {
   c->profiling = enable != 0;
   if (!enable) return ZF_OK;
   c->prof_cap = capacity > 0 ? capacity : 4096;
-  // [LBM pairs][membrane-force pairs][IB-block pairs]
-  c->prof_ev.resize(6 * (size_t)c->prof_cap);
+  // [LBM run pairs: 2 per run][membrane iterations: ZF_PROF_MARKS per block]
+  c->prof_ev.resize((2 + ZF_PROF_MARKS) * (size_t)c->prof_cap);
   for (auto& e : c->prof_ev) ZF_CUDA(cudaEventCreate(&e));
+  return ZF_OK;
+}
+
+// Summed device time (ms) of each stage of the profiled membrane iterations.
+static int stage_times(zf_ctx* c, float* st) {
+  for (int k = 0; k < ZF_PROF_STAGES; ++k) st[k] = 0.f;
+  for (int i = 0; i < c->prof_mem; ++i) {
+    const size_t b = 2 * (size_t)c->prof_cap + ZF_PROF_MARKS * (size_t)i;
+    for (int k = 0; k < ZF_PROF_STAGES; ++k) {
+      float ms = 0.f;
+      ZF_CUDA(cudaEventElapsedTime(&ms, c->prof_ev[b + k], c->prof_ev[b + k + 1]));
+      st[k] += ms;
+    }
+  }
   return ZF_OK;
 }
 
 int zf_profile_read(zf_ctx* c, float* lbm_ms, int* lbm_count, float* membrane_ms, int* membrane_count) {
   if (!c) return ZF_ERR_ARG;
   ZF_CUDA(cudaStreamSynchronize(c->stream));
-  float tl = 0.f, tm = 0.f;
+  float tl = 0.f;
   int runs_n = 0;
   for (int i = 0; i < c->prof_lbm; ++i) {
     runs_n += c->prof_run_n[i];
@@ -434,17 +452,25 @@ int zf_profile_read(zf_ctx* c, float* lbm_ms, int* lbm_count, float* membrane_ms
     ZF_CUDA(cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]));
     tl += ms;
   }
-  for (int i = 0; i < c->prof_mem; ++i) {
-    float a = 0.f, b = 0.f;
-    ZF_CUDA(cudaEventElapsedTime(&a, c->prof_ev[2 * (c->prof_cap + i)], c->prof_ev[2 * (c->prof_cap + i) + 1]));
-    ZF_CUDA(cudaEventElapsedTime(&b, c->prof_ev[2 * (2 * c->prof_cap + i)],
-                                 c->prof_ev[2 * (2 * c->prof_cap + i) + 1]));
-    tm += a + b;
-  }
+  float st[ZF_PROF_STAGES];
+  int rc = stage_times(c, st);
+  if (rc) return rc;
+  float tm = 0.f;
+  for (int k = 0; k < ZF_PROF_STAGES; ++k)
+    if (k != 1) tm += st[k];  // the membrane iteration's own LBM launch is not part of the block
   if (lbm_ms) *lbm_ms = tl;
   if (lbm_count) *lbm_count = runs_n;
   if (membrane_ms) *membrane_ms = tm;
   if (membrane_count) *membrane_count = c->prof_mem;
+  return ZF_OK;
+}
+
+int zf_profile_stages(zf_ctx* c, float* stage_ms, int* blocks) {
+  if (!c || !stage_ms) return ZF_ERR_ARG;
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  int rc = stage_times(c, stage_ms);
+  if (rc) return rc;
+  if (blocks) *blocks = c->prof_mem;
   return ZF_OK;
 }
 

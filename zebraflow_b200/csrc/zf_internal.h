@@ -30,6 +30,10 @@ enum : uint8_t {
 
 namespace zf {
 
+// membrane-iteration stages timed by zf_profile (see zf_profile_stages)
+constexpr int ZF_PROF_STAGES = 8;
+constexpr int ZF_PROF_MARKS = ZF_PROF_STAGES + 1;
+
 void set_error(const char* fmt, ...);
 
 #define ZF_CUDA(call)                                                          \
@@ -327,7 +331,7 @@ struct zf_ctx {
   // kernel and the membrane block of zf_step
   int64_t launches = 0;
   bool profiling = false;
-  std::vector<cudaEvent_t> prof_ev;  // [2*cap]: LBM pairs then membrane pairs
+  std::vector<cudaEvent_t> prof_ev;  // [2*cap] LBM run pairs, then ZF_PROF_MARKS per membrane block
   int prof_cap = 0, prof_lbm = 0, prof_mem = 0;  // event pairs: LBM runs, membrane blocks
   bool prof_open = false;                          // an LBM run is being timed
   int prof_open_n = 0;                             // its launches so far

@@ -1106,7 +1106,10 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxBlocks + 1]
 
 // Device address of g_noalloc_scratch on `device`, looked up once per device
 // with that device current.  In host code the array's name is only a host-side
-// stand-in; kernels must be given this address instead.
+// stand-in; kernels must be given this address instead.  The cached address
+// belongs to the device's primary context: after cudaDeviceReset on that
+// device it is stale, so a process that resets a device must not call the
+// allocation-free entry on it again.
 static int noalloc_scratch(int device, double** out) {
   static std::mutex mu;
   static double* addr[256] = {};
@@ -1149,6 +1152,8 @@ int lbm_step_mass_noalloc(zf_ctx* c, int store_moments, int zero_force, double* 
   c->cur ^= 1;
   k_sum_partials<<<1, 256, 0, c->stream>>>(scratch, grid, scratch + grid);
   ZF_CUDA(cudaGetLastError());
+  // the step kernel, the wall pass where it runs, and the sum
+  c->launches += (c->n_active > 0) + (c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0) + 1;
   ZF_CUDA(cudaMemcpyAsync(mass_out, scratch + grid, sizeof(double), cudaMemcpyDeviceToHost,
                           c->stream));
   ZF_CUDA(cudaStreamSynchronize(c->stream));

@@ -1,6 +1,5 @@
 // Membrane mesh set-up on the host: topology, spring calibration and rest
-// metrics shared by every cell, plus the icosphere and cell-placement
-// generators used by the synthetic workloads.
+// metrics shared by every cell.
 //
 // Reference behaviour restated here (ZebraflowWT.c):
 //  - edge list and 4-node rhombus (n1,n2 edge; n3,n4 opposite vertices;
@@ -195,56 +194,6 @@ int mesh_build(MeshHost& m, const zf_params& P) {
 }
 
 }  // namespace zf
-
-extern "C" {
-
-// Icosphere: the unit icosahedron subdivided `level` times (each triangle
-// into four, midpoints projected to the sphere).  10*4^L+2 nodes and
-// 20*4^L triangles, wound counter-clockwise seen from outside (outward
-// normals, like the reference mesh).  xyz [n_node][3]; tri [n_tri][3] 1-based.
-int zf_gen_icosphere(int level, double* xyz, int32_t* tri) {
-  if (level < 0 || level > 6 || !xyz || !tri) return ZF_ERR_ARG;
-  const double t = (1.0 + std::sqrt(5.0)) / 2.0;
-  std::vector<double> V = {-1, t, 0, 1, t, 0, -1, -t, 0, 1, -t, 0, 0, -1, t, 0, 1, t,
-                           0, -1, -t, 0, 1, -t, t, 0, -1, t, 0, 1, -t, 0, -1, -t, 0, 1};
-  std::vector<int> F = {0, 11, 5, 0, 5,  1,  0, 1, 7, 0, 7,  10, 0, 10, 11, 1, 5, 9, 5, 11,
-                        4, 11, 10, 2, 10, 7, 6, 7, 1, 8, 3, 9,  4,  3,  4,  2, 3, 2, 6, 3,
-                        6, 8,  3, 8, 9,  4, 9, 5, 2, 4, 11, 6,  2,  10, 8,  6, 7, 9, 8, 1};
-  auto norm = [&](int i) {
-    double* p = &V[3 * i];
-    const double r = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
-    p[0] /= r;
-    p[1] /= r;
-    p[2] /= r;
-  };
-  for (int i = 0; i < 12; ++i) norm(i);
-  for (int L = 0; L < level; ++L) {
-    std::unordered_map<uint64_t, int> mid;
-    std::vector<int> G;
-    auto midpoint = [&](int a, int b) {
-      const uint64_t k = zf::pair_key(a, b);
-      auto it = mid.find(k);
-      if (it != mid.end()) return it->second;
-      const int id = (int)(V.size() / 3);
-      for (int s = 0; s < 3; ++s) V.push_back(0.5 * (V[3 * a + s] + V[3 * b + s]));
-      norm(id);
-      mid[k] = id;
-      return id;
-    };
-    for (size_t f = 0; f < F.size(); f += 3) {
-      const int a = F[f], b = F[f + 1], c = F[f + 2];
-      const int ab = midpoint(a, b), bc = midpoint(b, c), ca = midpoint(c, a);
-      const int g[12] = {a, ab, ca, b, bc, ab, c, ca, bc, ab, bc, ca};
-      G.insert(G.end(), g, g + 12);
-    }
-    F.swap(G);
-  }
-  std::memcpy(xyz, V.data(), V.size() * sizeof(double));
-  for (size_t f = 0; f < F.size(); ++f) tri[f] = F[f] + 1;
-  return ZF_OK;
-}
-
-}  // extern "C"
 
 // ---- C ABI: mesh and cells -------------------------------------------------
 
@@ -506,172 +455,6 @@ int zf_cgsm_forces(zf_ctx* c) {
   NEED(c->cells_set, "zf_cgsm_forces", "cells not set");
   ZF_CUDA(cudaSetDevice(c->device));
   return cells_membrane_launch(c);
-}
-
-// Seeded placement of n_cells cells in a vessel (B_index codes, lattice
-// units): centres uniform over fluid points, orientations uniform (random
-// unit quaternion), rejecting a candidate whose ellipsoid (semi-axes
-// `axes` um plus `margin` um) overlaps an accepted one on the lattice, or
-// any of whose membrane nodes has a non-fluid lattice point within the cube
-// of half-width r = max(1, ceil(wall_clear / dx)) around its nearest lattice
-// point.  Outputs x [3][n_cells][n_node], xn [3][n_cells][n_node_n] in um.
-// Returns the number placed in *placed (fewer than asked when the attempts
-// run out).
-int zf_gen_cells(const int32_t* b, int nx, int ny, int nz, const double* origin, double dx,
-                 int periodic_z, int n_cells, int n_node, const double* rest, int n_node_n,
-                 const double* rest_n, const double* axes, double margin, double wall_clear,
-                 uint64_t seed, double* x, double* xn, int* placed) {
-  if (!b || !origin || !rest || !axes || !x || !placed || n_cells < 0 || dx <= 0) return ZF_ERR_ARG;
-  uint64_t st = seed;
-  auto next = [&]() {  // splitmix64
-    uint64_t z = (st += 0x9E3779B97F4A7C15ull);
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-  };
-  auto uni = [&]() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); };
-  std::vector<int64_t> fluid;
-  for (int64_t p = 0; p < (int64_t)nx * ny * nz; ++p)
-    if (b[p] > 0) fluid.push_back(p);
-  if (fluid.empty()) return ZF_ERR_ARG;
-  std::vector<uint8_t> occ((size_t)nx * ny * nz, 0);
-  // clear[p] = 1 when every point of the cube of half-width r around p is
-  // fluid: the fluid mask eroded by a cube, one axis at a time (a point
-  // outside the box counts as non-fluid, except across a periodic z face)
-  const int r_clear = std::max(1, (int)std::ceil(wall_clear / dx - 1e-9));
-  std::vector<uint8_t> clear((size_t)nx * ny * nz);
-  for (int64_t p = 0; p < (int64_t)nx * ny * nz; ++p) clear[p] = b[p] > 0;
-  {
-    const int64_t stride[3] = {(int64_t)ny * nz, nz, 1};
-    const int len[3] = {nx, ny, nz};
-    for (int ax = 0; ax < 3; ++ax) {
-      const int L = len[ax];
-      const bool wrap = ax == 2 && periodic_z;
-      const int64_t nlines = (int64_t)nx * ny * nz / L;
-#pragma omp parallel
-      {
-        std::vector<int> bad((size_t)L + 1);
-        std::vector<uint8_t> line((size_t)L);
-#pragma omp for schedule(static)
-        for (int64_t l = 0; l < nlines; ++l) {
-          // base point of line l: the index with the axis coordinate zero
-          int64_t base;
-          if (ax == 0) base = l;                                    // l = j*nz + k
-          else if (ax == 1) base = (l / nz) * (int64_t)ny * nz + l % nz;  // l = i*nz + k
-          else base = l * nz;                                       // l = i*ny + j
-          for (int t = 0; t < L; ++t) line[t] = clear[base + t * stride[ax]];
-          bad[0] = 0;  // prefix counts of non-fluid points
-          for (int t = 0; t < L; ++t) bad[t + 1] = bad[t] + (line[t] ? 0 : 1);
-          const int total = bad[L];
-          for (int t = 0; t < L; ++t) {
-            int lo = t - r_clear, hi = t + r_clear, cnt;
-            if (wrap) {
-              if (2 * r_clear + 1 >= L) cnt = total;
-              else if (lo < 0) cnt = bad[hi + 1] + (total - bad[L + lo]);
-              else if (hi >= L) cnt = (total - bad[lo]) + bad[hi - L + 1];
-              else cnt = bad[hi + 1] - bad[lo];
-            } else {
-              cnt = (lo < 0 || hi >= L) ? 1 : bad[hi + 1] - bad[lo];
-            }
-            clear[base + t * stride[ax]] = cnt == 0;
-          }
-        }
-      }
-    }
-  }
-  auto at = [&](int i, int j, int k) -> int64_t {
-    if (i < 0 || i >= nx || j < 0 || j >= ny) return -1;
-    if (k < 0 || k >= nz) {
-      if (!periodic_z) return -1;
-      k = ((k % nz) + nz) % nz;
-    }
-    return ((int64_t)i * ny + j) * nz + k;
-  };
-  const double A[3] = {axes[0] + margin, axes[1] + margin, axes[2] + margin};
-  const int reach = (int)std::ceil(std::max(A[0], std::max(A[1], A[2])) / dx) + 1;
-  struct Cand {
-    double c[3];
-    double R[3][3];
-  };
-  // the whole candidate stream comes from the seed; a candidate is accepted
-  // when it fits against the cells accepted before it, so evaluating a batch
-  // in parallel against the occupancy at the start of the batch and then
-  // re-checking the survivors in order gives the sequential result
-  auto fits = [&](const Cand& cd, std::vector<int64_t>* mark) -> bool {
-    const double ci = cd.c[0], cj = cd.c[1], ck = cd.c[2];
-    const int64_t s0 = at((int)std::lround(ci), (int)std::lround(cj), (int)std::lround(ck));
-    if (s0 < 0 || occ[s0]) return false;
-    // every membrane node at least r lattice units (Chebyshev) from the wall
-    for (int n = 0; n < n_node; ++n) {
-      double pos[3];
-      for (int a = 0; a < 3; ++a)
-        pos[a] = cd.R[a][0] * rest[3 * n] + cd.R[a][1] * rest[3 * n + 1] + cd.R[a][2] * rest[3 * n + 2];
-      const int64_t s = at((int)std::lround(ci + pos[0] / dx), (int)std::lround(cj + pos[1] / dx),
-                           (int)std::lround(ck + pos[2] / dx));
-      if (s < 0 || !clear[s]) return false;
-    }
-    // lattice points inside the inflated ellipsoid: free?
-    for (int di = -reach; di <= reach; ++di)
-      for (int dj = -reach; dj <= reach; ++dj)
-        for (int dk = -reach; dk <= reach; ++dk) {
-          const int i = (int)std::floor(ci) + di, j = (int)std::floor(cj) + dj, k = (int)std::floor(ck) + dk;
-          const double v[3] = {(i - ci) * dx, (j - cj) * dx, (k - ck) * dx};
-          double q[3];
-          for (int a = 0; a < 3; ++a) q[a] = cd.R[0][a] * v[0] + cd.R[1][a] * v[1] + cd.R[2][a] * v[2];
-          const double e = q[0] * q[0] / (A[0] * A[0]) + q[1] * q[1] / (A[1] * A[1]) + q[2] * q[2] / (A[2] * A[2]);
-          if (e > 1.0) continue;
-          const int64_t s = at(i, j, k);
-          if (s < 0 || occ[s]) return false;
-          if (mark) mark->push_back(s);
-        }
-    return true;
-  };
-  int n_ok = 0;
-  const int64_t max_tries = 12000LL * n_cells + 1000;
-  const int64_t batch = 4096;
-  std::vector<Cand> cand((size_t)batch);
-  std::vector<uint8_t> pass((size_t)batch);
-  std::vector<int64_t> mark;
-  for (int64_t tries = 0; n_ok < n_cells && tries < max_tries; tries += batch) {
-    const int64_t nb = std::min(batch, max_tries - tries);
-    for (int64_t t = 0; t < nb; ++t) {
-      Cand& cd = cand[(size_t)t];
-      const int64_t p = fluid[(size_t)(uni() * fluid.size()) % fluid.size()];
-      cd.c[0] = (double)(p / ((int64_t)ny * nz)) + uni() - 0.5;
-      cd.c[1] = (double)((p / nz) % ny) + uni() - 0.5;
-      cd.c[2] = (double)(p % nz) + uni() - 0.5;
-      // uniform rotation (Shoemake)
-      const double u1 = uni(), u2 = uni(), u3 = uni();
-      const double qw = std::sqrt(1 - u1) * std::sin(2 * M_PI * u2), qx = std::sqrt(1 - u1) * std::cos(2 * M_PI * u2),
-                   qy = std::sqrt(u1) * std::sin(2 * M_PI * u3), qz = std::sqrt(u1) * std::cos(2 * M_PI * u3);
-      const double R[3][3] = {{1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qz * qw), 2 * (qx * qz + qy * qw)},
-                              {2 * (qx * qy + qz * qw), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qx * qw)},
-                              {2 * (qx * qz - qy * qw), 2 * (qy * qz + qx * qw), 1 - 2 * (qx * qx + qy * qy)}};
-      std::memcpy(cd.R, R, sizeof(R));
-    }
-#pragma omp parallel for schedule(dynamic, 16)
-    for (int64_t t = 0; t < nb; ++t) pass[(size_t)t] = fits(cand[(size_t)t], nullptr);
-    for (int64_t t = 0; t < nb && n_ok < n_cells; ++t) {
-      if (!pass[(size_t)t]) continue;
-      const Cand& cd = cand[(size_t)t];
-      mark.clear();
-      if (!fits(cd, &mark)) continue;
-      for (int64_t s : mark) occ[s] = 1;
-      const double c0[3] = {origin[0] + cd.c[0] * dx, origin[1] + cd.c[1] * dx, origin[2] + cd.c[2] * dx};
-      for (int n = 0; n < n_node; ++n)
-        for (int a = 0; a < 3; ++a)
-          x[((size_t)a * n_cells + n_ok) * n_node + n] =
-              c0[a] + cd.R[a][0] * rest[3 * n] + cd.R[a][1] * rest[3 * n + 1] + cd.R[a][2] * rest[3 * n + 2];
-      if (xn && rest_n)
-        for (int n = 0; n < n_node_n; ++n)
-          for (int a = 0; a < 3; ++a)
-            xn[((size_t)a * n_cells + n_ok) * n_node_n + n] =
-                c0[a] + cd.R[a][0] * rest_n[3 * n] + cd.R[a][1] * rest_n[3 * n + 1] + cd.R[a][2] * rest_n[3 * n + 2];
-      ++n_ok;
-    }
-  }
-  *placed = n_ok;
-  return ZF_OK;
 }
 
 }  // extern "C"

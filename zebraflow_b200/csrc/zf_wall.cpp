@@ -1,5 +1,4 @@
-// Vessel wall meshes: generators for the synthetic vessels and the host
-// set-up of the wall data the IB kernels read.
+// Vessel wall meshes: the host set-up of the wall data the IB kernels read.
 //
 // Reference behaviour restated in zf_set_wall (ZebraflowWT.c):
 //  - W_index: for every wall-mesh node in order, the lattice points of its
@@ -206,221 +205,3 @@ int wall_build(zf_ctx* c, int nw, const float* xyz, int mt, const int32_t* tri1,
 }
 
 }  // namespace zf
-
-// ---- generators ---------------------------------------------------------------
-
-namespace {
-
-struct MeshOut {
-  std::vector<float> x, y, z;
-  std::vector<int32_t> tri;  // 0-based
-  std::vector<float> n;      // per triangle, 3 each
-};
-
-void orient_and_normals(MeshOut& M, const std::vector<float>& gx, const std::vector<float>& gy,
-                        const std::vector<float>& gz) {
-  // make each triangle's geometric normal point along the given inward direction
-  const size_t mt = M.tri.size() / 3;
-  M.n.resize(3 * mt);
-  for (size_t t = 0; t < mt; ++t) {
-    int* v = &M.tri[3 * t];
-    const float ax = M.x[v[1]] - M.x[v[0]], ay = M.y[v[1]] - M.y[v[0]], az = M.z[v[1]] - M.z[v[0]];
-    const float bx = M.x[v[2]] - M.x[v[0]], by = M.y[v[2]] - M.y[v[0]], bz = M.z[v[2]] - M.z[v[0]];
-    float nx = ay * bz - az * by, ny = az * bx - ax * bz, nz = ax * by - ay * bx;
-    if (nx * gx[t] + ny * gy[t] + nz * gz[t] < 0) {
-      std::swap(v[1], v[2]);
-      nx = -nx;
-      ny = -ny;
-      nz = -nz;
-    }
-    const float r = sqrtf(nx * nx + ny * ny + nz * nz);
-    M.n[3 * t] = nx / r;
-    M.n[3 * t + 1] = ny / r;
-    M.n[3 * t + 2] = nz / r;
-  }
-}
-
-int emit(const MeshOut& M, int* n_node, int* n_tri, float* xyz, int32_t* tri, float* nrm, int cap_node,
-         int cap_tri) {
-  const int nw = (int)M.x.size(), mt = (int)(M.tri.size() / 3);
-  *n_node = nw;
-  *n_tri = mt;
-  if (!xyz || !tri || !nrm) return ZF_OK;  // size query
-  if (nw > cap_node || mt > cap_tri) return ZF_ERR_OVERFLOW;
-  for (int i = 0; i < nw; ++i) {
-    xyz[i] = M.x[i];
-    xyz[nw + i] = M.y[i];
-    xyz[2 * nw + i] = M.z[i];
-  }
-  for (int t = 0; t < mt; ++t)
-    for (int a = 0; a < 3; ++a) {
-      tri[(size_t)a * mt + t] = M.tri[3 * t + a] + 1;
-      nrm[(size_t)a * mt + t] = M.n[3 * t + a];
-    }
-  return ZF_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-// Cylinder wall of radius R (lattice units) around the lattice axis (cx, cy),
-// along z over nz lattice spacings, in um with the lattice origin/spacing;
-// rings every `h` lattice units, `nseg` segments around; inward normals.
-// The band that would close the periodic seam is left open.  With NULL
-// outputs only the sizes are returned.
-int zf_gen_wall_tube(double cx, double cy, double R, int nz, double h, int nseg,
-                     const double* origin, double dx, int* n_node, int* n_tri, float* xyz,
-                     int32_t* tri, float* nrm, int cap_node, int cap_tri) {
-  if (R <= 0 || nz <= 0 || h <= 0 || nseg < 3 || !origin || dx <= 0) return ZF_ERR_ARG;
-  MeshOut M;
-  const int nring = (int)std::floor(nz / h);
-  for (int r = 0; r < nring; ++r)
-    for (int s = 0; s < nseg; ++s) {
-      const double th = 2 * M_PI * (s + 0.5 * (r & 1)) / nseg;
-      M.x.push_back((float)(origin[0] + (cx + R * std::cos(th)) * dx));
-      M.y.push_back((float)(origin[1] + (cy + R * std::sin(th)) * dx));
-      M.z.push_back((float)(origin[2] + r * h * dx));
-    }
-  std::vector<float> gx, gy, gz;
-  for (int r = 0; r + 1 < nring; ++r)
-    for (int s = 0; s < nseg; ++s) {
-      const int a = r * nseg + s, b = r * nseg + (s + 1) % nseg;
-      const int c2 = (r + 1) * nseg + s, d = (r + 1) * nseg + (s + 1) % nseg;
-      const int tris[2][3] = {{a, b, c2}, {b, d, c2}};
-      for (auto& t : tris) {
-        M.tri.insert(M.tri.end(), t, t + 3);
-        const float mx = (M.x[t[0]] + M.x[t[1]] + M.x[t[2]]) / 3.f - (float)(origin[0] + cx * dx);
-        const float my = (M.y[t[0]] + M.y[t[1]] + M.y[t[2]]) / 3.f - (float)(origin[1] + cy * dx);
-        gx.push_back(-mx);
-        gy.push_back(-my);
-        gz.push_back(0.f);
-      }
-    }
-  orient_and_normals(M, gx, gy, gz);
-  return emit(M, n_node, n_tri, xyz, tri, nrm, cap_node, cap_tri);
-}
-
-// Wall of the periodic Y-bifurcation of zf_gen_bifurcation (same arguments):
-// the zero set of the signed distance to the vessel (union of capsules),
-// extracted by marching tetrahedra on the lattice, vertices shared between
-// neighbouring cubes, inward normals.  The periodic seam cubes are skipped.
-int zf_gen_wall_bifurcation(int nx, int ny, int nz, double Rp, double Rd, double half_angle_deg,
-                            const double* origin, double dx, int* n_node, int* n_tri, float* xyz,
-                            int32_t* tri, float* nrm, int cap_node, int cap_tri) {
-  if (!origin || dx <= 0 || nx <= 1 || ny <= 1 || nz <= 1) return ZF_ERR_ARG;
-  const double cxa = 0.5 * (nx - 1), cya = 0.5 * (ny - 1);
-  const double ta = std::tan(half_angle_deg * M_PI / 180.0);
-  double D = 0.8 * (0.5 * (nx - 1) - Rd - 2.0), Ldiv = D / ta;
-  const double Lpar = 0.1 * nz;
-  if (2 * Lpar + 2 * Ldiv > 0.9 * nz) {
-    Ldiv = 0.5 * (0.9 * nz - 2 * Lpar);
-    D = Ldiv * ta;
-  }
-  const double z1 = Lpar, z2 = z1 + Ldiv, z4 = nz - Lpar, z3 = z4 - Ldiv;
-  struct Seg {
-    double a[3], b[3], r;
-  };
-  std::vector<Seg> segs = {{{cxa, cya, z4 - nz}, {cxa, cya, z1}, Rp},
-                           {{cxa, cya, z4}, {cxa, cya, z1 + nz}, Rp}};
-  for (int s = -1; s <= 1; s += 2) {
-    segs.push_back({{cxa, cya, z1}, {cxa + s * D, cya, z2}, Rd});
-    segs.push_back({{cxa + s * D, cya, z2}, {cxa + s * D, cya, z3}, Rd});
-    segs.push_back({{cxa + s * D, cya, z3}, {cxa, cya, z4}, Rd});
-  }
-  auto sdf = [&](double x, double y, double z) {  // < 0 inside the lumen
-    double best = 1e30;
-    for (const Seg& g : segs) {
-      double d[3] = {g.b[0] - g.a[0], g.b[1] - g.a[1], g.b[2] - g.a[2]};
-      double w[3] = {x - g.a[0], y - g.a[1], z - g.a[2]};
-      double dd = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-      double t = dd > 0 ? (w[0] * d[0] + w[1] * d[1] + w[2] * d[2]) / dd : 0.0;
-      t = t < 0 ? 0 : (t > 1 ? 1 : t);
-      double r[3] = {w[0] - t * d[0], w[1] - t * d[1], w[2] - t * d[2]};
-      best = std::min(best, std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]) - g.r);
-    }
-    return best;
-  };
-  // signed distance at lattice points
-  std::vector<float> phi((size_t)nx * ny * nz);
-#pragma omp parallel for collapse(2) schedule(static)
-  for (int i = 0; i < nx; ++i)
-    for (int j = 0; j < ny; ++j)
-      for (int k = 0; k < nz; ++k) phi[((size_t)i * ny + j) * nz + k] = (float)sdf(i, j, k);
-  auto P = [&](int i, int j, int k) { return phi[((size_t)i * ny + j) * nz + k]; };
-  MeshOut M;
-  std::unordered_map<uint64_t, int> vid;  // lattice edge (min point, max point) -> vertex
-  auto vertex = [&](const int* p, const int* q) -> int {
-    uint64_t a = ((uint64_t)p[0] * ny + p[1]) * nz + p[2], b = ((uint64_t)q[0] * ny + q[1]) * nz + q[2];
-    if (a > b) std::swap(a, b);
-    const uint64_t key = a * 0x9E3779B97F4A7C15ull ^ (b + 0x632BE59BD9B4E019ull + (a << 6) + (a >> 2));
-    auto it = vid.find(key);
-    if (it != vid.end()) return it->second;
-    const double fp = P(p[0], p[1], p[2]), fq = P(q[0], q[1], q[2]);
-    const double t = fp / (fp - fq);
-    const int id = (int)M.x.size();
-    M.x.push_back((float)(origin[0] + (p[0] + t * (q[0] - p[0])) * dx));
-    M.y.push_back((float)(origin[1] + (p[1] + t * (q[1] - p[1])) * dx));
-    M.z.push_back((float)(origin[2] + (p[2] + t * (q[2] - p[2])) * dx));
-    vid[key] = id;
-    return id;
-  };
-  std::vector<float> gx, gy, gz;
-  // Kuhn split of a cube into 6 tetrahedra along the main diagonal 0-7
-  static const int corner[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0},
-                                   {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
-  static const int tets[6][4] = {{0, 1, 3, 7}, {0, 3, 2, 7}, {0, 2, 6, 7},
-                                 {0, 6, 4, 7}, {0, 4, 5, 7}, {0, 5, 1, 7}};
-  for (int i = 0; i + 1 < nx; ++i)
-    for (int j = 0; j + 1 < ny; ++j)
-      for (int k = 0; k + 1 < nz; ++k) {
-        float f[8];
-        bool neg = false, pos = false;
-        for (int v = 0; v < 8; ++v) {
-          f[v] = P(i + corner[v][0], j + corner[v][1], k + corner[v][2]);
-          (f[v] < 0 ? neg : pos) = true;
-        }
-        if (!neg || !pos) continue;
-        for (const auto& T : tets) {
-          int in[4], out[4], ni = 0, no = 0;
-          for (int v = 0; v < 4; ++v) (f[T[v]] < 0 ? in[ni++] : out[no++]) = T[v];
-          if (ni == 0 || no == 0) continue;
-          auto pt = [&](int v, int* o3) {
-            o3[0] = i + corner[v][0];
-            o3[1] = j + corner[v][1];
-            o3[2] = k + corner[v][2];
-          };
-          auto V = [&](int a, int b) {
-            int pa[3], pb[3];
-            pt(a, pa);
-            pt(b, pb);
-            return vertex(pa, pb);
-          };
-          std::vector<std::array<int, 3>> ts;
-          if (ni == 1) ts.push_back({V(in[0], out[0]), V(in[0], out[1]), V(in[0], out[2])});
-          else if (ni == 3) ts.push_back({V(out[0], in[0]), V(out[0], in[1]), V(out[0], in[2])});
-          else {
-            const int a = V(in[0], out[0]), b = V(in[0], out[1]), c2 = V(in[1], out[1]),
-                      d = V(in[1], out[0]);
-            ts.push_back({a, b, c2});
-            ts.push_back({a, c2, d});
-          }
-          for (auto& t : ts) {
-            if (t[0] == t[1] || t[1] == t[2] || t[0] == t[2]) continue;
-            M.tri.insert(M.tri.end(), t.begin(), t.end());
-            // inward = -grad(phi) at the triangle centroid (central differences)
-            const double mx = ((M.x[t[0]] + M.x[t[1]] + M.x[t[2]]) / 3.0 - origin[0]) / dx;
-            const double my = ((M.y[t[0]] + M.y[t[1]] + M.y[t[2]]) / 3.0 - origin[1]) / dx;
-            const double mz = ((M.z[t[0]] + M.z[t[1]] + M.z[t[2]]) / 3.0 - origin[2]) / dx;
-            const double e = 0.25;
-            gx.push_back((float)-(sdf(mx + e, my, mz) - sdf(mx - e, my, mz)));
-            gy.push_back((float)-(sdf(mx, my + e, mz) - sdf(mx, my - e, mz)));
-            gz.push_back((float)-(sdf(mx, my, mz + e) - sdf(mx, my, mz - e)));
-          }
-        }
-      }
-  orient_and_normals(M, gx, gy, gz);
-  return emit(M, n_node, n_tri, xyz, tri, nrm, cap_node, cap_tri);
-}
-
-}  // extern "C"
