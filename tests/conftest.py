@@ -1,7 +1,8 @@
 """Shared test set-up: the `gpu` marker and the two libraries under test.
 
-`libzf.so` (the product, include/zf.h) and `oracle/liboracle.so` (the CPU
-restatement of the reference used as the checker) are built on first use.
+`libzf.so` (the product, include/zf.h) with its C host driver `zf_run`, and
+`oracle/liboracle.so` (the CPU restatement of the reference used as the
+checker) are built on first use.
 """
 import os
 import subprocess
@@ -19,7 +20,7 @@ def pytest_configure(config):
 
 
 def _ensure_built():
-    if not os.path.exists(os.path.join(ROOT, "zebraflow_b200", "libzf.so")):
+    if not all(os.path.exists(os.path.join(ROOT, "zebraflow_b200", f)) for f in ("libzf.so", "zf_run")):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "zebraflow_b200", "csrc")],
                        check=True)
     if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):

@@ -1,0 +1,95 @@
+"""The plain FP32 GPU path against the FP32 oracle on a bifurcation at the
+scale of the benchmark's cell interactions: a periodic Y-bifurcation of
+128x128x256 lattice points (parent radius 18, daughters 13, half-angle 20
+degrees, 269,356 fluid points), halfway bounce-back, tau 0.9, Guo force 2e-6
+along the parent axis, 152 nucleated RBCs placed from seed 2024 (icosphere
+642/1280 scaled to 7, 4.5, 2 lattice units, nucleus 162 nodes scaled to 2.5,
+1.8, 1.2), the vessel's marching-tetrahedra wall mesh, membrane/IB block
+every 50 iterations.  Both run the reference loop from rest; after 50, 100
+and 200 iterations the fluid velocity, density deviation, wall shear stress
+and node displacement are compared (relative L2).  The two sides differ only
+in the order of float sums (atomics in the GPU spreading, the oracle's
+OpenMP reductions), so the differences start at fp32 rounding and grow with
+the cells' interactions; the bounds are written per checkpoint.
+"""
+import numpy as np
+import pytest
+
+import zebraflow_b200 as zf
+from oracle.bind import OracleCells, OracleLBM, OracleWorld
+
+pytestmark = pytest.mark.gpu
+
+DIMS, RP, RD, ANGLE, G = (128, 128, 256), 18.0, 13.0, 20.0, 2e-6
+N_CELLS, SEED = 160, 2024
+CHECKS = (50, 100, 200)
+# relative L2 bounds per checkpoint: u, rho - 1, WSS, displacement
+BOUNDS = {50: (1e-4, 1e-3, 1e-4, 1e-4), 100: (2e-4, 2e-3, 2e-4, 2e-4), 200: (5e-4, 5e-3, 5e-4, 5e-4)}
+
+
+def rel(a, b):
+    ok = np.isfinite(a) & np.isfinite(b)
+    return float(np.linalg.norm((a - b)[ok]) / np.linalg.norm(b[ok]))
+
+
+def node_normals(wall):
+    xyz, tri1, nrm = wall
+    t = tri1 - 1
+    p = xyz.T.astype(np.float64)
+    area = 0.5 * np.linalg.norm(np.cross(p[t[1]] - p[t[0]], p[t[2]] - p[t[0]]), axis=1)
+    acc = np.zeros((xyz.shape[1], 3))
+    for v in range(3):
+        np.add.at(acc, t[v], area[:, None] * nrm.T)
+    acc /= np.linalg.norm(acc, axis=1, keepdims=True)
+    return np.ascontiguousarray(acc.T, np.float32)
+
+
+def test_bifurcation_with_cells_against_fp32_oracle():
+    nx, ny, nz = DIMS
+    b, _ = zf.gen_bifurcation(nx, ny, nz, RP, RD, ANGLE)
+    wall = zf.gen_wall_bifurcation(nx, ny, nz, RP, RD, ANGLE, dx=0.5)
+    xyz, tri = zf.gen_icosphere(3)
+    xyzn, trin = zf.gen_icosphere(2)
+    rest, rest_n = xyz * np.array([3.5, 2.25, 1.0]), xyzn * np.array([1.25, 0.9, 0.6])
+    mesh = (rest, tri, rest_n, zf.mesh_edges(trin))
+    cells = zf.gen_cells(b, N_CELLS, rest, rest_n, (3.5, 2.25, 1.0), seed=SEED, dx=0.5, margin=0.4)
+    assert cells[0].shape[1] >= 150
+    p = zf.default_params(nx=nx, ny=ny, nz=nz, tau=0.9, tau_from_phase=0, wall_mode=zf.WALL_HALFWAY_BB,
+                          periodic=(0, 0, 1), g=(0.0, 0.0, G), origin=(0.0, 0.0, 0.0), dx=0.5,
+                          area0=0.0, volume0=0.0)
+    nrm = node_normals(wall)
+    lbm = OracleLBM(b, wall_mode=0, periodic=(0, 0, 1), tau=0.9, g=(0.0, 0.0, G), precision="f32")
+    oc = OracleCells(*mesh, p, precision="f32")
+    oc.set_cells(*cells)
+    w = OracleWorld(lbm, oc, p)
+    w.set_wall(*wall)
+    dom = np.argwhere(b >= 0)
+    fl = b[dom[:, 0], dom[:, 1], dom[:, 2]] > 0
+    x0 = cells[0]
+    with zf.Context(p) as ctx:
+        ctx.set_lattice(b)
+        ctx.set_wall(*wall)
+        ctx.set_mesh(*mesh)
+        ctx.set_cells(*cells)
+        done = 0
+        for it in CHECKS:
+            ctx.step(it - done)
+            w.step(it - done)
+            done = it
+            wss_g, _, _ = ctx.wss(nrm)  # leaves the moments of the current populations
+            Dg, Ug, Vg, Wg = ctx.download_moments()
+            xg, _, sg = ctx.cells()
+            D, U, V, W = lbm.moments()
+            wss_o, _, _ = w.wss(nrm)
+            go = oc.get()
+            assert np.array_equal(sg, go["status"])
+            live = go["status"] > 0
+            err = (rel(np.stack([Ug, Vg, Wg])[:, fl], np.stack([U, V, W])[:, fl]),
+                   rel((Dg - 1.0)[fl], (D - 1.0)[fl]),
+                   rel(wss_g, wss_o),
+                   rel((xg - x0)[:, live], (go["x"] - x0)[:, live]))
+            print(f"iteration {it}: u {err[0]:.2e}  rho-1 {err[1]:.2e}  WSS {err[2]:.2e}  disp {err[3]:.2e}")
+            for e, bound in zip(err, BOUNDS[it]):
+                assert e <= bound, (it, err)
+    for o in (w, oc, lbm):
+        o.close()

@@ -29,7 +29,6 @@ namespace zf {
 
 namespace {
 
-constexpr float kPI = 3.14159265358979f;
 // warps per block of the queue-based search kernels
 constexpr int kRepWarps = 4;
 
@@ -60,13 +59,77 @@ __device__ __forceinline__ int64_t slot_of(const IbArgs& a, int i, int j, int k)
   return (int64_t)t * ZF_TC + (i & 3) + 4 * (j & 3) + 16 * (k & 3);
 }
 
-// Peskin cosine weight of a lattice point at offsets (dx,dy,dz) from the node,
-// ZebraflowWT.c:8971-8973 (support radius 2 DX = StencilWidth*DX)
-__device__ __forceinline__ float peskin(float dx, float dy, float dz, float h2) {
-  const float cx = cosf((float)((double)kPI * fabsf(dx) / (double)h2));
-  const float cy = cosf((float)((double)kPI * fabsf(dy) / (double)h2));
-  const float cz = cosf((float)((double)kPI * fabsf(dz) / (double)h2));
-  return (1.f + cx) * (1.f + cy) * (1.f + cz) / 64.f;
+// The Peskin stencil of a node (ZebraflowWT.c:8963-8996 interpolation,
+// :10806-10866 spreading): of the reference's +-4 window only the 4 lattice
+// points b..b+3 per axis around the node can lie within the support radius
+// 2 DX (StencilWidth*DX).  The cosine delta is a product of one factor per
+// axis, so the factors are formed once per axis point -- 12 cosines per node
+// instead of 3 per stencil point -- each as the reference forms it: the
+// offset d = x_lattice - x_node in float, the cosine of PI |d| / (2 DX) with
+// its argument in double (PI is a double literal there), and the product
+// (1 + cx)(1 + cy)(1 + cz) / 64 in double.  The distance test keeps the
+// reference's float sqrtf of the summed float squares.
+constexpr double kPId = 3.14159265358979;  // PI, ZebraflowWT.c:34
+
+struct StencilAxis {
+  int b;        // first lattice index along the axis
+  unsigned ok;  // bit m: point b + m lies in the box and in the node's +-4 window
+  float s[4];   // d^2
+  float c[4];   // cosf(PI |d| / (2 DX))
+};
+
+// lo, hi: the box's index range along the axis; i0: the node's lattice index
+__device__ __forceinline__ void stencil_axis(StencilAxis& ax, float xp, double x0, double dx, int lo, int hi,
+                                             int i0) {
+  ax.b = (int)floor(((double)xp - x0) / dx) - 1;
+  ax.ok = 0u;
+  const double h2 = 2.0 * dx;
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const int i = ax.b + m;
+    if (i >= lo && i <= hi && i >= i0 - 4 && i <= i0 + 4) ax.ok |= 1u << m;
+    const float d = (float)(x0 + i * dx) - xp;
+    ax.s[m] = __fmul_rn(d, d);
+    ax.c[m] = cosf((float)(kPId * (double)fabsf(d) / h2));
+  }
+}
+
+// entry m of a 4-array held in registers (m not a compile-time constant)
+__device__ __forceinline__ float sel4(const float (&v)[4], int m) {
+  return m < 2 ? (m == 0 ? v[0] : v[1]) : (m == 2 ? v[2] : v[3]);
+}
+
+// Walks the stencil points of a node in the reference's i, j, k order and
+// calls fn(i, j, k, w) for those within the support radius, w > 0 in double:
+// (1 + cx)(1 + cy)(1 + cz) / 64, the three factors multiplied left to right.
+template <class Fn>
+__device__ __forceinline__ void stencil_walk(const StencilAxis& X, const StencilAxis& Y, const StencilAxis& Z,
+                                             float h2, Fn&& fn) {
+  for (int mi = 0; mi < 4; ++mi) {
+    if (!((X.ok >> mi) & 1u)) continue;
+    const float sx = sel4(X.s, mi);
+    const double fx = 1.0 + (double)sel4(X.c, mi);
+    for (int mj = 0; mj < 4; ++mj) {
+      if (!((Y.ok >> mj) & 1u)) continue;
+      const float sxy = __fadd_rn(sx, sel4(Y.s, mj));
+      const double fxy = fx * (1.0 + (double)sel4(Y.c, mj));
+#pragma unroll
+      for (int mk = 0; mk < 4; ++mk) {
+        if (!((Z.ok >> mk) & 1u)) continue;
+        if (!(sqrtf(__fadd_rn(sxy, Z.s[mk])) <= h2)) continue;
+        const double w = fxy * (1.0 + (double)Z.c[mk]) / 64.0;
+        if (w > 0.0) fn(X.b + mi, Y.b + mj, Z.b + mk, w);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void node_stencil(const IbArgs& a, float xp, float yp, float zp, StencilAxis& X,
+                                             StencilAxis& Y, StencilAxis& Z) {
+  const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX), k0 = lat_index(zp, a.Z0, a.DX);
+  stencil_axis(X, xp, a.X0, a.DX, 0, a.nx - 1, i0);
+  stencil_axis(Y, yp, a.Y0, a.DX, 0, a.ny - 1, j0);
+  stencil_axis(Z, zp, a.Z0, a.DX, a.kmin, a.kmax, k0);
 }
 
 struct NodeRef {
@@ -99,54 +162,34 @@ __global__ void k_ib_interp(IbArgs a, CellArgs c) {
   const double* X = nuc ? c.xn : c.x;
   float xp, yp, zp;
   node_pos(X, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
-  const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
-            k0 = lat_index(zp, a.Z0, a.DX);
   const float h2 = 2.f * a.DX;
+  StencilAxis SX, SY, SZ;
+  node_stencil(a, xp, yp, zp, SX, SY, SZ);
 
-  // velocity interpolation over the points that can lie within 2 DX
+  // velocity interpolation over the 4x4x4 stencil points, in the reference's
+  // i, j, k order; fluid points give U, V, W, non-fluid points with a wall
+  // index the void velocity
   double vx = 0.0, vy = 0.0, vz = 0.0;
-  {
-    // candidates: the 4 points per axis around the node (the others of the
-    // reference's +-4 window lie beyond 2 DX or weigh 0)
-    const int ib = (int)floor(((double)xp - a.X0) / a.DX) - 1;
-    const int jb = (int)floor(((double)yp - a.Y0) / a.DX) - 1;
-    const int kb = (int)floor(((double)zp - a.Z0) / a.DX) - 1;
-    for (int i = ib; i <= ib + 3; ++i) {
-      if (i < 0 || i >= a.nx || i < i0 - 4 || i > i0 + 4) continue;
-      for (int j = jb; j <= jb + 3; ++j) {
-        if (j < 0 || j >= a.ny || j < j0 - 4 || j > j0 + 4) continue;
-        for (int k = kb; k <= kb + 3; ++k) {
-          if (k < a.kmin || k > a.kmax || k < k0 - 4 || k > k0 + 4) continue;
-          const int kw = wrapk(a, k);
-          const float xc = (float)(a.X0 + i * a.DX);
-          const float yc = (float)(a.Y0 + j * a.DX);
-          const float zc = (float)(a.Z0 + k * a.DX);
-          const float dx = xc - xp, dy = yc - yp, dz = zc - zp;
-          const int64_t s = slot_of(a, i, j, kw);
-          if (s < 0) continue;
-          const uint8_t cd = a.code[s];
-          const bool fluid = cd >= 1 && cd <= 9;
-          if (!fluid && a.windex[s] <= 0) continue;
-          const float d = dist3(dx, dy, dz);
-          if (!(d <= h2)) continue;
-          const float w = peskin(dx, dy, dz, h2);
-          float u, v, ww;
-          if (fluid) {
-            u = a.mom[a.ns + s];
-            v = a.mom[2 * a.ns + s];
-            ww = a.mom[3 * a.ns + s];
-          } else {
-            u = a.uvoid[s];
-            v = a.uvoid[a.ns_all + s];
-            ww = a.uvoid[2 * a.ns_all + s];
-          }
-          vx += (double)w * (double)(a.vel_scale * u);
-          vy += (double)w * (double)(a.vel_scale * v);
-          vz += (double)w * (double)(a.vel_scale * ww);
-        }
-      }
+  stencil_walk(SX, SY, SZ, h2, [&](int i, int j, int k, double w) {
+    const int64_t s = slot_of(a, i, j, wrapk(a, k));
+    if (s < 0) return;
+    const uint8_t cd = a.code[s];
+    const bool fluid = cd >= 1 && cd <= 9;
+    if (!fluid && a.windex[s] <= 0) return;
+    float u, v, ww;
+    if (fluid) {
+      u = a.mom[a.ns + s];
+      v = a.mom[2 * a.ns + s];
+      ww = a.mom[3 * a.ns + s];
+    } else {
+      u = a.uvoid[s];
+      v = a.uvoid[a.ns_all + s];
+      ww = a.uvoid[2 * a.ns_all + s];
     }
-  }
+    vx += w * (double)(a.vel_scale * u);
+    vy += w * (double)(a.vel_scale * v);
+    vz += w * (double)(a.vel_scale * ww);
+  });
   double* V = nuc ? c.vel_n : c.vel;
   V[((size_t)0 * nc + cell) * n + node] += vx;
   V[((size_t)1 * nc + cell) * n + node] += vy;
@@ -1196,6 +1239,307 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
   }
 }
 
+// RBC-RBC repulsion (ZebraflowWT.c:9911-10053), one block per lattice tile of
+// nodes.  The block stages up to kRgNodes membrane nodes of the tile, takes
+// their bounding box, and walks the bin entries of the 27 tiles around it (the
+// +-4 window of any node of the tile lies inside them) in their stored order,
+// keeping in shared memory the triangles that some node of the box could
+// reach: a sub-centroid lies within 3/4 of the bounding radius of the
+// centroid, so a triangle whose centroid is farther than 1 um + 3/4 of that
+// radius from the box (plus a margin for rounding) contributes to none of
+// them.  Each warp then takes nodes one at a time and its lanes test the kept
+// triangles against the node with the reference's conditions (bin inside the
+// node's window, centroid within 2 um, facing normals, not one of the node's
+// own triangles) and the disk bound of k_rbc_tiles; survivors queue up and are
+// evaluated 32 at a time, one per lane (the 16 sub-centroids).  Each node's
+// contributions are met in the same order whatever else the block holds, and
+// lane sums meet in a fixed butterfly.
+constexpr int kRgThreads = 256;
+constexpr int kRgWarps = kRgThreads / 32;
+constexpr int kRgNodes = 256;   // nodes staged per chunk (one per thread)
+constexpr int kRgCand = 1024;   // candidate triangles held per pass
+
+struct RgShared {
+  float4 cand_c[kRgCand];   // centroid, then the squared reach bound (1 um + 3/4 radius, with margin)
+  float4 cand_n[kRgCand];   // normal, global triangle id (int bits)
+  int cand_w[kRgCand];      // the record's w word (in-tile key, bounding radius)
+  int cand_e[kRgCand];      // bin entry (vertices in bin_v)
+  int cand_xy[kRgCand];     // one-hot bin column: bit x, bit 12 + y (x, y relative to the 12^3 block)
+  int cand_z[kRgCand];      // one-hot bin z: bit z
+  float4 node_p[kRgNodes];  // position (z wrapped into the box), node normal |e| in w
+  float4 node_n[kRgNodes];  // normal; cell id in w (int bits, -1: inactive)
+  int node_wxy[kRgNodes];   // window columns: x bits 0..11, y bits 12..23
+  int node_wz[kRgNodes];    // window z bits
+  int node_id[kRgNodes];    // node index in its cell
+  float acc[kRgNodes][3];
+  int q[kRgWarps][64];
+  int rng[28];              // prefix of entry counts over the 27 tiles
+  int rst[27];              // first entry of each tile
+  int rrel[27];             // tile offset in the 12^3 block: x | y << 8 | z << 16 (in units of 4 points)
+  float bb[6];              // node box: min x, y, z, max x, y, z
+  int wsum[kRgWarps];
+  int li, ncand, nn;
+};
+
+__device__ __forceinline__ int onehot_range(int lo, int hi) {  // bits lo..hi of 12, clamped
+  lo = max(lo, 0);
+  hi = min(hi, 11);
+  return lo > hi ? 0 : (int)(((2u << hi) - 1u) & ~((1u << lo) - 1u));
+}
+
+__global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs c) {
+  extern __shared__ __align__(16) unsigned char rg_raw[];
+  RgShared& S = *reinterpret_cast<RgShared*>(rg_raw);
+  const unsigned FULL = 0xffffffffu;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nc = c.n_cells;
+  const int64_t nmem = (int64_t)nc * c.nn;
+  const int64_t n_pop_tiles = a.ns / ZF_TC;
+  const int nlist = a.tile_ctr[0];
+  for (;;) {
+    if (tid == 0) S.li = atomicAdd(&a.tile_ctr[1], 1);
+    __syncthreads();
+    const int li = S.li;
+    if (li >= nlist) break;
+    const int gt = a.tile_list[li];
+    const int tx = gt % a.ntx, ty = (gt / a.ntx) % a.nty, tz = gt / (a.ntx * a.nty);
+    const int ox = (tx - 1) * 4, oy = (ty - 1) * 4, oz = (tz - 1) * 4;
+    if (tid < 27) {
+      int X, Y, Z;
+      const int t = neighbour_tile(a, tx, ty, tz, tid, X, Y, Z);
+      int e0 = 0, len = 0;
+      if (t >= 0 && t < n_pop_tiles) {
+        e0 = a.bin_off[(int64_t)t * ZF_TC];
+        len = a.bin_off[(int64_t)t * ZF_TC + ZF_TC] - e0;
+      }
+      S.rst[tid] = e0;
+      S.rng[tid + 1] = len;  // counts, scanned below
+      S.rrel[tid] = (tid % 3) | (((tid / 3) % 3) << 8) | ((tid / 9) << 16);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      S.rng[0] = 0;
+      for (int r = 0; r < 27; ++r) S.rng[r + 1] += S.rng[r];
+    }
+    const int n0 = a.node_off[gt], n1 = a.node_off[gt + 1];
+    for (int c0 = n0; c0 < n1; c0 += kRgNodes) {
+      const int cnt = min(kRgNodes, n1 - c0);
+      __syncthreads();
+      // stage the chunk's membrane nodes and their box
+      float px = 0.f, py = 0.f, pz = 0.f;
+      bool live = false;
+      if (tid < cnt) {
+        const int64_t gid = a.node_sorted[c0 + tid];
+        int cell = -1, node = 0;
+        if (gid < nmem) {
+          cell = (int)(gid / c.nn);
+          node = (int)(gid % c.nn);
+          if (c.status[cell] <= 0) cell = -1;
+        }
+        int wxy = 0, wz = 0;
+        float ex = 0.f, ey = 0.f, ez = 0.f;
+        if (cell >= 0) {
+          node_pos(c.x, nc, c.nn, cell, node, a.LZ, a.Z0, px, py, pz);
+          ex = c.node_normal[((size_t)0 * nc + cell) * c.nn + node];
+          ey = c.node_normal[((size_t)1 * nc + cell) * c.nn + node];
+          ez = c.node_normal[((size_t)2 * nc + cell) * c.nn + node];
+          const int i0 = lat_index(px, a.X0, a.DX), j0 = lat_index(py, a.Y0, a.DX), k0 = lat_index(pz, a.Z0, a.DX);
+          const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
+          const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
+          // z unwrapped around the node's tile: window k and the block share one frame
+          const int kw = a.per_z ? ((k0 % a.nz) + a.nz) % a.nz : k0;
+          const int k1 = a.per_z ? kw - 4 : max(k0 - 4, 2), k2 = a.per_z ? kw + 4 : min(k0 + 4, a.nz - 4);
+          wxy = onehot_range(i1 - ox, i2 - ox) | (onehot_range(j1 - oy, j2 - oy) << 12);
+          wz = onehot_range(k1 - oz, k2 - oz);
+          live = (wxy & 0xfff) && (wxy >> 12) && wz;
+          if (!live) cell = -1;
+        }
+        S.node_p[tid] = make_float4(px, py, pz, sqrtf(ex * ex + ey * ey + ez * ez));
+        S.node_n[tid] = make_float4(ex, ey, ez, __int_as_float(cell));
+        S.node_wxy[tid] = wxy;
+        S.node_wz[tid] = wz;
+        S.node_id[tid] = node;
+        S.acc[tid][0] = S.acc[tid][1] = S.acc[tid][2] = 0.f;
+      }
+      // box of the live nodes (warp reductions, then one warp over the warps)
+      float mn[3] = {live ? px : 3e38f, live ? py : 3e38f, live ? pz : 3e38f};
+      float mx[3] = {live ? px : -3e38f, live ? py : -3e38f, live ? pz : -3e38f};
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          mn[d] = fminf(mn[d], __shfl_xor_sync(FULL, mn[d], o));
+          mx[d] = fmaxf(mx[d], __shfl_xor_sync(FULL, mx[d], o));
+        }
+      const int nlive = __popc(__ballot_sync(FULL, live));
+      __shared__ float s_wb[kRgWarps][6];
+      if (lane == 0) {
+        for (int d = 0; d < 3; ++d) {
+          s_wb[warp][d] = mn[d];
+          s_wb[warp][3 + d] = mx[d];
+        }
+        S.wsum[warp] = nlive;
+      }
+      __syncthreads();
+      if (tid < 6) {
+        float v = s_wb[0][tid];
+        for (int w = 1; w < kRgWarps; ++w) v = tid < 3 ? fminf(v, s_wb[w][tid]) : fmaxf(v, s_wb[w][tid]);
+        S.bb[tid] = v;
+      }
+      if (tid == 0) {
+        int t = 0;
+        for (int w = 0; w < kRgWarps; ++w) t += S.wsum[w];
+        S.nn = t;
+        S.ncand = 0;
+      }
+      __syncthreads();
+      if (S.nn == 0) continue;
+      const float hx = 0.5f * (S.bb[3] - S.bb[0]), hy = 0.5f * (S.bb[4] - S.bb[1]), hz = 0.5f * (S.bb[5] - S.bb[2]);
+      const float mxc = S.bb[0] + hx, myc = S.bb[1] + hy, mzc = S.bb[2] + hz;
+      const int total = S.rng[27];
+
+      // the kept triangles, tested against the staged nodes
+      auto process = [&]() {
+        __syncthreads();
+        const int ncand = S.ncand;
+        int* queue = S.q[warp];
+        for (int t = warp; t < cnt; t += kRgWarps) {
+          const float4 np = S.node_p[t], nn4 = S.node_n[t];
+          const int cell = __float_as_int(nn4.w);
+          if (cell < 0) continue;
+          const float xc = np.x, yc = np.y, zc = np.z;
+          const float e1x = nn4.x, e1y = nn4.y, e1z = nn4.z;
+          const int wxy = S.node_wxy[t], wz = S.node_wz[t], node = S.node_id[t];
+          const int g_own = cell * c.nt;
+          float rx = 0.f, ry = 0.f, rz = 0.f;
+          int qn = 0;
+          auto flush = [&](int nb) {
+            __syncwarp();
+            if (lane < nb) {
+              const int e = queue[lane];
+              float tx2, ty2, tz2;
+              rbc_entry(a, c, e, a.bin_rec[2 * e], xc, yc, zc, tx2, ty2, tz2);
+              rx += tx2;
+              ry += ty2;
+              rz += tz2;
+            }
+            const int rem = qn - nb;
+            const int tq = lane < rem ? queue[nb + lane] : 0;
+            __syncwarp();
+            if (lane < rem) queue[lane] = tq;
+            __syncwarp();
+            qn = rem;
+          };
+          for (int k0 = 0; k0 < ncand; k0 += 32) {
+            const int k = k0 + lane;
+            bool pass = false;
+            int e = 0;
+            if (k < ncand) {
+              const float4 cc = S.cand_c[k];
+              const float dzc = wrapd(cc.z - zc, a.LZ);
+              const float ddx = xc - cc.x, ddy = yc - cc.y;
+              if (ddx * ddx + ddy * ddy + dzc * dzc <= cc.w) {
+                const int cxy = S.cand_xy[k];
+                if ((cxy & wxy) == cxy && (S.cand_z[k] & wz)) {
+                  const float rw = __int_as_float(S.cand_w[k]);
+                  const float dcen = dist3(ddx, ddy, -dzc);
+                  const float4 nr = S.cand_n[k];
+                  if (dcen < 2.f && !(dcen - rec_rb(rw) > 1.f) && e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
+                    const float pd = (cc.x - xc) * nr.x + (cc.y - yc) * nr.y + dzc * nr.z;
+                    const float qd = fmaxf(sqrtf(fmaxf(dcen * dcen - pd * pd, 0.f)) - 0.75f * rec_rb(rw), 0.f);
+                    const int tri = __float_as_int(nr.w) - g_own;  // not the node's own triangle
+                    pass = pd * pd + qd * qd <= 1.004f &&
+                           !((unsigned)tri < (unsigned)c.nt &&
+                             (c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node));
+                    e = S.cand_e[k];
+                  }
+                }
+              }
+            }
+            const unsigned bal = __ballot_sync(FULL, pass);
+            if (pass) queue[qn + __popc(bal & ((1u << lane) - 1u))] = e;
+            qn += __popc(bal);
+            if (qn >= 32) flush(32);
+          }
+          while (qn > 0) flush(min(qn, 32));
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            rx += __shfl_xor_sync(FULL, rx, o);
+            ry += __shfl_xor_sync(FULL, ry, o);
+            rz += __shfl_xor_sync(FULL, rz, o);
+          }
+          if (lane == 0) {
+            S.acc[t][0] += rx;
+            S.acc[t][1] += ry;
+            S.acc[t][2] += rz;
+          }
+        }
+        __syncthreads();
+        if (tid == 0) S.ncand = 0;
+        __syncthreads();
+      };
+
+      for (int f0 = 0; f0 < total; f0 += kRgThreads) {
+        if (S.ncand + kRgThreads > kRgCand) process();
+        const int f = f0 + tid;
+        bool keep = false;
+        float4 cr = make_float4(0.f, 0.f, 0.f, 0.f);
+        int e = 0, r = 0;
+        if (f < total) {
+#pragma unroll
+          for (int stp = 16; stp > 0; stp >>= 1)
+            if (r + stp < 27 && f >= S.rng[r + stp]) r += stp;
+          e = S.rst[r] + (f - S.rng[r]);
+          cr = a.bin_rec[2 * e];
+          const float rb = rec_rb(cr.w);
+          const float dx = fmaxf(fabsf(cr.x - mxc) - hx, 0.f), dy = fmaxf(fabsf(cr.y - myc) - hy, 0.f);
+          const float dz = fmaxf(fabsf(wrapd(cr.z - mzc, a.LZ)) - hz, 0.f);
+          const float lim = 1.0021f + 0.75f * rb;
+          keep = dx * dx + dy * dy + dz * dz <= lim * lim * 1.0001f;
+        }
+        const unsigned bal = __ballot_sync(FULL, keep);
+        if (lane == 0) S.wsum[warp] = __popc(bal);
+        __syncthreads();
+        int base = S.ncand;
+        for (int w = 0; w < warp; ++w) base += S.wsum[w];
+        if (keep) {
+          const int pos = base + __popc(bal & ((1u << lane) - 1u));
+          const float rb = rec_rb(cr.w);
+          const float lim = 1.0021f + 0.75f * rb;
+          S.cand_c[pos] = make_float4(cr.x, cr.y, cr.z, lim * lim * 1.0001f);
+          S.cand_n[pos] = a.bin_rec[2 * e + 1];
+          S.cand_w[pos] = __float_as_int(cr.w);
+          S.cand_e[pos] = e;
+          const int kk = rec_kk(cr.w), rel = S.rrel[r];
+          const int bi = (rel & 0xff) * 4 + (kk >> 4), bj = ((rel >> 8) & 0xff) * 4 + ((kk >> 2) & 3),
+                    bk = (rel >> 16) * 4 + (kk & 3);
+          S.cand_xy[pos] = (1 << bi) | (1 << (12 + bj));
+          S.cand_z[pos] = 1 << bk;
+        }
+        __syncthreads();
+        if (tid == 0) {
+          int t = S.ncand;
+          for (int w = 0; w < kRgWarps; ++w) t += S.wsum[w];
+          S.ncand = t;
+        }
+        __syncthreads();
+      }
+      if (S.ncand > 0) process();
+      // the chunk's sums into NODE_WALLREPUL (one writer per node)
+      if (tid < cnt) {
+        const int cell = __float_as_int(S.node_n[tid].w);
+        if (cell >= 0) {
+          const int node = S.node_id[tid];
+          c.wrep[((size_t)0 * nc + cell) * c.nn + node] += S.acc[tid][0];
+          c.wrep[((size_t)1 * nc + cell) * c.nn + node] += S.acc[tid][1];
+          c.wrep[((size_t)2 * nc + cell) * c.nn + node] += S.acc[tid][2];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Wall nodes that can hold a node's nearest wall triangle, per lattice point
 // p of a tile near the wall (ZebraflowWT.c:8998-9077).  A node whose lattice
 // index is p lies in the box B = [p - 0.01, p + 0.99] DX per axis (as
@@ -1545,34 +1889,16 @@ __global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
   }
   float xp, yp, zp;
   node_pos(X, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
-  const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
-            k0 = lat_index(zp, a.Z0, a.DX);
   const float h2 = 2.f * a.DX;
-  const int ib = (int)floor(((double)xp - a.X0) / a.DX) - 1;
-  const int jb = (int)floor(((double)yp - a.Y0) / a.DX) - 1;
-  const int kb = (int)floor(((double)zp - a.Z0) / a.DX) - 1;
-  for (int i = ib; i <= ib + 3; ++i) {
-    if (i < 0 || i >= a.nx || i < i0 - 4 || i > i0 + 4) continue;
-    for (int j = jb; j <= jb + 3; ++j) {
-      if (j < 0 || j >= a.ny || j < j0 - 4 || j > j0 + 4) continue;
-      for (int k = kb; k <= kb + 3; ++k) {
-        if (k < a.kmin || k > a.kmax || k < k0 - 4 || k > k0 + 4) continue;
-        const int kw = wrapk(a, k);
-        const int64_t s = slot_of(a, i, j, kw);
-        if (s < 0 || s >= a.ns) continue;
-        const uint8_t cd = a.code[s];
-        if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) continue;
-        const float xc = (float)((double)a.X0 + i * (double)a.DX);
-        const float yc = (float)((double)a.Y0 + j * (double)a.DX);
-        const float zc = (float)((double)a.Z0 + k * (double)a.DX);
-        const float dx = xc - xp, dy = yc - yp, dz = zc - zp;
-        if (!(dist3(dx, dy, dz) <= h2)) continue;
-        const float w = peskin(dx, dy, dz, h2);
-        for (int v = 0; v < 3; ++v)
-          atomicAdd(&a.force[v * a.ns + s], (float)((double)(w * Ff[v]) * (double)a.force_scale));
-      }
-    }
-  }
+  StencilAxis SX, SY, SZ;
+  node_stencil(a, xp, yp, zp, SX, SY, SZ);
+  stencil_walk(SX, SY, SZ, h2, [&](int i, int j, int k, double w) {
+    const int64_t s = slot_of(a, i, j, wrapk(a, k));
+    if (s < 0 || s >= a.ns) return;
+    const uint8_t cd = a.code[s];
+    if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) return;
+    for (int v = 0; v < 3; ++v) atomicAdd(&a.force[v * a.ns + s], (float)(w * (double)Ff[v] * a.force_scale));
+  });
 }
 
 // k_ib_spread per lattice tile of nodes (node-tile lists): a block takes a
@@ -1583,11 +1909,11 @@ __global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
 // times.  The nodes' own updates (NODE_VEL += NODE_WALLREPUL, :10749-10754)
 // happen once per node in the first pass.  A contribution outside the
 // neighbourhood (not expected) goes straight to BODYFORCE.
-constexpr int kSpreadNodes = 256;  // nodes staged per pass
+constexpr int kSpreadNodes = 128;  // nodes staged per pass
 __global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int spread_walls) {
   __shared__ float acc[3][1728];
-  __shared__ float s_pos[3][kSpreadNodes], s_f[3][kSpreadNodes];
-  __shared__ int s_b[3][kSpreadNodes], s_c[3][kSpreadNodes];  // stencil corner, lat_index
+  __shared__ float s_f[3][kSpreadNodes];
+  __shared__ StencilAxis s_ax[3][kSpreadNodes];  // per staged node: its stencil along x, y, z
   __shared__ int s_li;
   const int nc = c.n_cells;
   const int nlist = a.tile_ctr[0];
@@ -1610,7 +1936,7 @@ __global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int 
         const int t = threadIdx.x;
         bool nuc;
         int cell, node;
-        s_b[0][t] = INT_MIN;  // inactive node
+        s_ax[0][t].ok = 0u;  // inactive node: no stencil point
         if (node_of(c, a.node_sorted[c0 + t], nuc, cell, node)) {
           const int n = nuc ? c.nnn : c.nn;
           double* V = nuc ? c.vel_n : c.vel;
@@ -1623,45 +1949,51 @@ __global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int 
           }
           float xp, yp, zp;
           node_pos(nuc ? c.xn : c.x, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
-          s_pos[0][t] = xp;
-          s_pos[1][t] = yp;
-          s_pos[2][t] = zp;
-          s_c[0][t] = lat_index(xp, a.X0, a.DX);
-          s_c[1][t] = lat_index(yp, a.Y0, a.DX);
-          s_c[2][t] = lat_index(zp, a.Z0, a.DX);
-          s_b[0][t] = (int)floor(((double)xp - a.X0) / a.DX) - 1;
-          s_b[1][t] = (int)floor(((double)yp - a.Y0) / a.DX) - 1;
-          s_b[2][t] = (int)floor(((double)zp - a.Z0) / a.DX) - 1;
+          StencilAxis X, Y, Z;
+          node_stencil(a, xp, yp, zp, X, Y, Z);
+          s_ax[0][t] = X;
+          s_ax[1][t] = Y;
+          s_ax[2][t] = Z;
         }
       }
       __syncthreads();
-      for (int it = threadIdx.x; it < cnt * 64; it += blockDim.x) {
-        const int t = it >> 6, p = it & 63;
-        if (s_b[0][t] == INT_MIN) continue;
-        const int i = s_b[0][t] + (p >> 4), j = s_b[1][t] + ((p >> 2) & 3), k = s_b[2][t] + (p & 3);
-        const int i0 = s_c[0][t], j0 = s_c[1][t], k0 = s_c[2][t];
-        if (i < 0 || i >= a.nx || i < i0 - 4 || i > i0 + 4) continue;
-        if (j < 0 || j >= a.ny || j < j0 - 4 || j > j0 + 4) continue;
-        if (k < a.kmin || k > a.kmax || k < k0 - 4 || k > k0 + 4) continue;
-        const int kw = wrapk(a, k);
-        const int64_t sl = slot_of(a, i, j, kw);
-        if (sl < 0 || sl >= a.ns) continue;
-        const uint8_t cd = a.code[sl];
-        if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) continue;
-        const float xc = (float)((double)a.X0 + i * (double)a.DX);
-        const float yc = (float)((double)a.Y0 + j * (double)a.DX);
-        const float zc = (float)((double)a.Z0 + k * (double)a.DX);
-        const float dx = xc - s_pos[0][t], dy = yc - s_pos[1][t], dz = zc - s_pos[2][t];
-        if (!(dist3(dx, dy, dz) <= h2)) continue;
-        const float w = peskin(dx, dy, dz, h2);
-        const int di = i - ox, dj = j - oy;
-        int dk = k - oz;
-        if (a.per_z) dk = ((dk % a.nz) + a.nz) % a.nz;
-        const bool in = di >= 0 && di < 12 && dj >= 0 && dj < 12 && dk >= 0 && dk < 12;
-        for (int v = 0; v < 3; ++v) {
-          const float val = (float)((double)(w * s_f[v][t]) * (double)a.force_scale);
-          if (in) atomicAdd(&acc[v][(dk * 12 + dj) * 12 + di], val);
-          else atomicAdd(&a.force[v * a.ns + sl], val);
+      // one item per (node, x, y) column of its stencil, walking z
+      for (int it = threadIdx.x; it < cnt * 16; it += blockDim.x) {
+        const int t = it >> 4, mi = (it >> 2) & 3, mj = it & 3;
+        const StencilAxis& X = s_ax[0][t];
+        const StencilAxis& Y = s_ax[1][t];
+        const StencilAxis& Z = s_ax[2][t];
+        if (!((X.ok >> mi) & (Y.ok >> mj) & 1u)) continue;
+        const int i = X.b + mi, j = Y.b + mj;
+        const float sxy = __fadd_rn(X.s[mi], Y.s[mj]);
+        const double fxy = (1.0 + (double)X.c[mi]) * (1.0 + (double)Y.c[mj]);
+        const float f0 = s_f[0][t], f1 = s_f[1][t], f2 = s_f[2][t];
+        for (int mk = 0; mk < 4; ++mk) {
+          if (!((Z.ok >> mk) & 1u)) continue;
+          if (!(sqrtf(__fadd_rn(sxy, Z.s[mk])) <= h2)) continue;
+          const double w = fxy * (1.0 + (double)Z.c[mk]) / 64.0;
+          if (!(w > 0.0)) continue;
+          const int k = Z.b + mk;
+          const int64_t sl = slot_of(a, i, j, wrapk(a, k));
+          if (sl < 0 || sl >= a.ns) continue;
+          const uint8_t cd = a.code[sl];
+          if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) continue;
+          const int di = i - ox, dj = j - oy;
+          int dk = k - oz;
+          if (a.per_z) dk = ((dk % a.nz) + a.nz) % a.nz;
+          const bool in = di >= 0 && di < 12 && dj >= 0 && dj < 12 && dk >= 0 && dk < 12;
+          const float v0 = (float)(w * (double)f0 * a.force_scale), v1 = (float)(w * (double)f1 * a.force_scale),
+                      v2 = (float)(w * (double)f2 * a.force_scale);
+          if (in) {
+            const int r = (dk * 12 + dj) * 12 + di;
+            atomicAdd(&acc[0][r], v0);
+            atomicAdd(&acc[1][r], v1);
+            atomicAdd(&acc[2][r], v2);
+          } else {
+            atomicAdd(&a.force[sl], v0);
+            atomicAdd(&a.force[a.ns + sl], v1);
+            atomicAdd(&a.force[2 * a.ns + sl], v2);
+          }
         }
       }
     }
@@ -1784,9 +2116,9 @@ __device__ __forceinline__ void wss_stencil(const IbArgs& a, float xm, float ym,
         const uint8_t cd = a.code[s];
         if (!(cd >= 1 && cd <= 9)) continue;  // 0.11 < B_index < 4997
         const float w =
-            (float)((1. + cosf((float)((double)kPI * fabsf(dx) / 2 / a.DX))) *
-                    (1. + cosf((float)((double)kPI * fabsf(dy) / 2 / a.DX))) *
-                    (1. + cosf((float)((double)kPI * fabsf(dz) / 2 / a.DX))) / 64.);
+            (float)((1. + cosf((float)(kPId * fabsf(dx) / 2 / a.DX))) *
+                    (1. + cosf((float)(kPId * fabsf(dy) / 2 / a.DX))) *
+                    (1. + cosf((float)(kPId * fabsf(dz) / 2 / a.DX))) / 64.);
         fn(s, w);
       }
 }
@@ -2029,31 +2361,16 @@ __global__ void k_spread_adj(IbArgs a, CellArgs c, int spread_walls, const float
   if (c.status[cell] > 0) {
     float xp, yp, zp;
     node_pos(nuc ? c.xn : c.x, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
-    const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX),
-              k0 = lat_index(zp, a.Z0, a.DX);
     const float h2 = 2.f * a.DX;
-    const int ib = (int)floor(((double)xp - a.X0) / a.DX) - 1;
-    const int jb = (int)floor(((double)yp - a.Y0) / a.DX) - 1;
-    const int kb = (int)floor(((double)zp - a.Z0) / a.DX) - 1;
-    for (int i = ib; i <= ib + 3; ++i) {
-      if (i < 0 || i >= a.nx || i < i0 - 4 || i > i0 + 4) continue;
-      for (int j = jb; j <= jb + 3; ++j) {
-        if (j < 0 || j >= a.ny || j < j0 - 4 || j > j0 + 4) continue;
-        for (int k = kb; k <= kb + 3; ++k) {
-          if (k < a.kmin || k > a.kmax || k < k0 - 4 || k > k0 + 4) continue;
-          const int64_t s = slot_of(a, i, j, wrapk(a, k));
-          if (s < 0 || s >= a.ns) continue;
-          const uint8_t cd = a.code[s];
-          if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) continue;
-          const float dx = (float)((double)a.X0 + i * (double)a.DX) - xp;
-          const float dy = (float)((double)a.Y0 + j * (double)a.DX) - yp;
-          const float dz = (float)((double)a.Z0 + k * (double)a.DX) - zp;
-          if (!(dist3(dx, dy, dz) <= h2)) continue;
-          const float w = peskin(dx, dy, dz, h2);
-          for (int v = 0; v < 3; ++v) acc[v] += (double)w * G[v * a.ns + s];
-        }
-      }
-    }
+    StencilAxis SX, SY, SZ;
+    node_stencil(a, xp, yp, zp, SX, SY, SZ);
+    stencil_walk(SX, SY, SZ, h2, [&](int i, int j, int k, double w) {
+      const int64_t s = slot_of(a, i, j, wrapk(a, k));
+      if (s < 0 || s >= a.ns) return;
+      const uint8_t cd = a.code[s];
+      if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) return;
+      for (int v = 0; v < 3; ++v) acc[v] += w * G[v * a.ns + s];
+    });
   }
   for (int v = 0; v < 3; ++v) out[((size_t)v * nc + cell) * n + node] = (float)(acc[v] * a.force_scale);
 }
@@ -2370,7 +2687,17 @@ int ib_rbc_rbc_launch(zf_ctx* ctx) {
       if (rc) return rc;
     }
     ZF_CUDA(cudaMemsetAsync(a.tile_ctr + 1, 0, sizeof(int32_t), ctx->stream));
-    k_rbc_tiles<<<persistent_blocks(k_rbc_tiles, kTileThreads), kTileThreads, 0, ctx->stream>>>(a, c);
+    static bool smem_set[256] = {};
+    const size_t smem = sizeof(RgShared);
+    if (!smem_set[ctx->device & 255]) {
+      ZF_CUDA(cudaFuncSetAttribute(k_rbc_group, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      smem_set[ctx->device & 255] = true;
+    }
+    int dev = 0, sms = 0, per_sm = 0;
+    ZF_CUDA(cudaGetDevice(&dev));
+    ZF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    ZF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rbc_group, kRgThreads, smem));
+    k_rbc_group<<<sms * (per_sm > 0 ? per_sm : 1), kRgThreads, smem, ctx->stream>>>(a, c);
   } else {
     k_rbc_rbc<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
         a, c);
