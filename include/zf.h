@@ -476,6 +476,96 @@ int zf_gen_cells(const int32_t* b, int nx, int ny, int nz, const double* origin,
                  const double* rest_n, const double* axes, double margin, double wall_clear,
                  uint64_t seed, double* x, double* xn, int* placed);
 
+/* ---- the reference's file formats (host only, no device needed) -----------
+ * Readers of the reference's input files and writers of the snapshots its
+ * OUTPUT() (ZebraflowWT.c:282-509) and post-processor write, on caller-owned
+ * host arrays in the layouts above.  Writers print with the reference's
+ * formats, so a file written from the same values is the reference's file
+ * byte for byte.  Coordinates map to lattice points as the reference does:
+ * 0-based i = (int)((x - origin)/dx + 1.01) - 1. */
+
+/* FLUIDdomainBindex.csv (read at ZebraflowWT.c:2574-2619): a header line, then
+ * "B_index,X,Y,Z" per row.  b_index [nx][ny][nz] is set to -1 (:2516) and then
+ * to each row's code; a row outside the box is an error. */
+int zf_read_bindex_csv(const char* path, int nx, int ny, int nz, const double* origin, double dx,
+                       int32_t* b_index, int64_t* n_rows);
+
+/* Fluid snapshot "X,Y,Z,Bindex,U,V,W,D,Bx,By,Bz,EulNeigh,Windex" (OUTPUT(),
+ * ZebraflowWT.c:356-370): one row per listed point in DOMLIST order.  D..W,
+ * eulneigh [n_listed] and bodyforce [3][n_listed] are in DOMLIST order;
+ * windex is [nx][ny][nz]; eulneigh / windex NULL print 0. */
+int zf_write_fluid_csv(const char* path, int nx, int ny, int nz, const double* origin, double dx,
+                       const int32_t* b_index, const float* D, const float* U, const float* V, const float* W,
+                       const float* bodyforce, const int32_t* eulneigh, const int32_t* windex);
+
+/* Reads a fluid snapshot back (the reference's restart, :2649-2700): for each
+ * row of a listed point of b_index, D, U, V, W, BODYFORCE and EulNeigh of
+ * that point (DOMLIST order) and W_index ([nx][ny][nz]).  NULL outputs skip. */
+int zf_read_fluid_csv(const char* path, int nx, int ny, int nz, const double* origin, double dx,
+                      const int32_t* b_index, float* D, float* U, float* V, float* W, float* bodyforce,
+                      int32_t* eulneigh, int32_t* windex, int64_t* n_rows);
+
+/* Populations f [19][n] = feq(D, (U, V, W)), as the reference initialises F
+ * from the restored moments (ZebraflowWT.c:2561-2570, :5253-5295); upload
+ * them with zf_upload_populations. */
+int zf_equilibrium_populations(int64_t n, const float* D, const float* U, const float* V, const float* W,
+                               float* f);
+
+/* Membrane snapshot, 21 columns (OUTPUT(), ZebraflowWT.c:429-442): rows of
+ * every cell with status > -5000.  cell_id [n_cells] (the reference's 1-based
+ * cell slot; NULL: c + 1), status [n_cells], x / vel [3][n_cells][n_node]
+ * fp64, wall_tri / area_ratio / out_flag [n_cells][n_node], wrep / ftot /
+ * fvol [3][n_cells][n_node], regress [n_cells].  NULL arrays print 0. */
+int zf_write_membrane_csv(const char* path, int n_cells, int n_node, const int32_t* cell_id,
+                          const int32_t* status, const double* x, const double* vel, const int32_t* wall_tri,
+                          const float* wrep, const int32_t* regress, const float* area_ratio, const float* ftot,
+                          const float* fvol, const int32_t* out_flag);
+
+/* Nucleus snapshot, 13 columns (OUTPUT(), ZebraflowWT.c:446-459); layouts as
+ * the membrane's with n_node_n nodes; neigh / neigh_flag [n_cells][n_node_n]. */
+int zf_write_nucleus_csv(const char* path, int n_cells, int n_node_n, const int32_t* cell_id,
+                         const int32_t* status, const double* xn, const double* vel_n, const float* ftot_n,
+                         const int32_t* neigh, const int32_t* neigh_flag);
+
+/* Nucleus spring snapshot "X,Y,Z,Cell,LX,LY,LZ,Stretch" (ZebraflowWT.c:461-504):
+ * per nucleus edge its midpoint, n1 - n2 and |n1 - n2| 1e-6 / LMAX_N.
+ * edge_n [n_edge_n][2] 1-based, lmax_n [n_edge_n] (zf_get_edge_params). */
+int zf_write_nucleus_edges_csv(const char* path, int n_cells, int n_node_n, int n_edge_n, const int32_t* cell_id,
+                               const int32_t* status, const double* xn, const int32_t* edge_n, const float* lmax_n);
+
+/* Appends the cells' rows to VolumeAreaHistory.dat (ZebraflowWT.c:345-350;
+ * the header is written when iter is 0).  cell_f [n_cells][8] as
+ * zf_get_cell_geometry returns it (area, volume, centroid). */
+int zf_append_volume_area(const char* path, int64_t iter, int n_cells, const int32_t* cell_id,
+                          const int32_t* status, const float* cell_f, const int32_t* regress);
+
+/* Reads a membrane (nucleus = 0, 21 columns) or nucleus (nucleus = 1, 13
+ * columns) snapshot: the reference's cell restart (ZebraflowWT.c:5323-5420,
+ * :5549-5574), n_node rows per cell.  With x NULL only *n_cells is returned;
+ * otherwise cell_id, status [cap_cells] and x, vel, ftot [3][n_cells][n_node]
+ * (NULL skips) are filled. */
+int zf_read_cells_csv(const char* path, int nucleus, int n_node, int cap_cells, int* n_cells, int32_t* cell_id,
+                      int32_t* status, double* x, double* vel, float* ftot);
+
+/* Mesh files as the reference ships them (read at ZebraflowWT.c:1601-1922):
+ * kind 0 "POINTS n ..." then n x 3 coordinates, kind 1 "CELLS n m" then n x 3
+ * node ids (as stored, 1-based), kind 2 "LINES n m" then n x 2 node ids.
+ * With values NULL only *n is returned. */
+int zf_read_mesh_dat(const char* path, int kind, int* n, double* values, int cap);
+
+/* Wall mesh files (read at ZebraflowWT.c:3724-3897): "POINTS n float" with the
+ * coordinates, "POLYGONS n 4n" with "3 a b c" 0-based rows, and "CELL_DATA n"
+ * / "NORMALS ..." with one normal per triangle.  Outputs as zf_set_wall takes
+ * them: xyz [3][n], tri [3][m] 1-based (+1 as the reference adds), normals
+ * [3][m].  With NULL outputs only the sizes are returned. */
+int zf_read_wall_mesh(const char* nodes_path, const char* cells_path, const char* normals_path, int* n_node_w,
+                      int* n_tri_w, float* xyz, int32_t* tri, float* normals, int cap_node, int cap_tri);
+
+/* Legacy-VTK wall file of the post-processor (PostProWSSandPressure.c:375-433):
+ * points, triangles, PRESSURE, WSSx/y/z and Valid per wall node (zf_wss). */
+int zf_write_wall_vtk(const char* path, int n_node_w, const float* xyz, int n_tri_w, const int32_t* tri,
+                      const float* pressure, const float* wss, const int32_t* valid);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,5 +1,4 @@
-"""Builds tests/golden/ref_setup.npz and tests/golden/ref_step.npz from the
-reference's own code.
+"""Builds the fixtures tests/golden/ref_*.npz from the reference's own code.
 
 Runs oracle/ref/Makefile, which compiles the reference's ZebraflowWT.c where
 it lies (main renamed) and runs two harnesses against it:
@@ -22,6 +21,10 @@ it lies (main renamed) and runs two harnesses against it:
    tests/golden/ib_scene.py, and a FLUIDdomain csv of its lattice with a
    pressurised swirling flow) -> ref_wss.npz (wall pressure, WSS and validity
    of every wall node, as the post-processor prints them);
+ * oracle/ref/harness_output.c: the reference's OUTPUT() writer on a small
+   lattice and two cells with seeded values -> ref_output.npz (the inputs and
+   the bytes of the fluid, membrane, nucleus, nucleus-edge and volume/area
+   files it writes);
  * oracle/ref/harness_step.c: five LBM steps of the reference's own
    stream-collide, wall and copy blocks of main() (ZebraflowWT.c:6101-6145,
    :6292-6433, :6601-6626) on a small capped tube with a phase-5 ball ->
@@ -131,6 +134,64 @@ def main():
     ib_fixture(nucleus=True)
     loop_fixture()
     wss_fixture()
+    output_fixture()
+
+
+OUTPUT_FILES = ("FLUIDdomain", "AllCellMemb", "AllCellNucleus", "AllNucEdgeMesh")
+
+
+def output_fixture():
+    """The reference's own OUTPUT() (oracle/ref/harness_output.c) on a small
+    lattice and two cells: its inputs and the bytes of the files it writes."""
+    import shutil
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), "../_ref/ref_output"], check=True)
+    run = os.path.join(ROOT, "oracle", "_ref", "output_run")
+    shutil.rmtree(run, ignore_errors=True)
+    os.makedirs(run)
+    subprocess.run([os.path.join(ROOT, "oracle", "_ref", "ref_output"), "inputs.bin"], cwd=run, check=True,
+                   stdout=open(os.path.join(run, "output.log"), "w"))
+    raw = open(os.path.join(run, "inputs.bin"), "rb").read()
+    pos = [0]
+
+    def rd(dt, k):
+        r = np.frombuffer(raw, dt, k, pos[0]).copy()
+        pos[0] += r.itemsize * k
+        return r
+    n, nx, ny, nz, i0, j0, k0 = rd(np.int32, 7)
+    rec = rd(np.int32, 6 * n).reshape(n, 6)
+    fl = {k: rd(np.float32, n) for k in ("D", "U", "V", "W")}
+    bf = rd(np.float32, 3 * n).reshape(3, n)
+    area0 = rd(np.float32, 504)
+    edge_n = rd(np.int32, 2 * 544).reshape(544, 2)
+    lmax_n = rd(np.float32, 544)
+    cells = {k: [] for k in ("head", "cellf", "x", "vel", "walltri", "wrep", "area", "ftot", "fvol", "outflag",
+                             "xn", "veln", "ftotn", "nneigh", "nflag")}
+    for _ in range(2):
+        cells["head"].append(rd(np.int32, 3))
+        cells["cellf"].append(rd(np.float32, 5))
+        for k, dt, m in (("x", np.float64, 3 * 504), ("vel", np.float64, 3 * 504), ("walltri", np.int32, 504),
+                         ("wrep", np.float32, 3 * 504), ("area", np.float32, 504), ("ftot", np.float32, 3 * 504),
+                         ("fvol", np.float32, 3 * 504), ("outflag", np.int32, 504), ("xn", np.float64, 3 * 121),
+                         ("veln", np.float64, 3 * 121), ("ftotn", np.float32, 3 * 121), ("nneigh", np.int32, 121),
+                         ("nflag", np.int32, 121)):
+            cells[k].append(rd(dt, m))
+    assert pos[0] == len(raw)
+    out = {"n_listed": n, "box": np.array([nx, ny, nz, i0, j0, k0], np.int32), "listed": rec, "bodyforce": bf,
+           "area0": area0, "edge_n": edge_n, "lmax_n": lmax_n, **fl}
+    for k, v in cells.items():
+        a = np.stack(v)
+        if a.shape[1] in (3 * 504, 3 * 121):  # [cell][3][n] -> [3][cell][n]
+            a = a.reshape(2, 3, -1).transpose(1, 0, 2)
+        out["cell_" + k] = a
+    sdir = os.path.join(run, "SimulationOutputData")
+    for name in OUTPUT_FILES:
+        out["file_" + name] = np.frombuffer(open(os.path.join(sdir, name + "-000000000.csv"), "rb").read(), np.uint8)
+    out["file_VolumeAreaHistory"] = np.frombuffer(open(os.path.join(sdir, "VolumeAreaHistory.dat"), "rb").read(),
+                                                  np.uint8)
+    shutil.rmtree(run)
+    np.savez_compressed(os.path.join(OUT, "ref_output.npz"), **out)
+    print(f"OUTPUT(): {n} listed points, 2 cells, files " +
+          ", ".join(f"{k[5:]} {out[k].size} B" for k in out if k.startswith("file_")))
 
 
 def wss_fixture():

@@ -115,6 +115,28 @@ _SIGS = {
     "zf_profile": (C.c_int, [_P, C.c_int, C.c_int]),
     "zf_profile_read": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int),
                                   C.POINTER(C.c_float), C.POINTER(C.c_int)]),
+    "zf_read_bindex_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, _i32p,
+                                     C.POINTER(C.c_int64)]),
+    "zf_write_fluid_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, _i32p, _f32p, _f32p,
+                                     _f32p, _f32p, _f32p, C.c_void_p, C.c_void_p]),
+    "zf_read_fluid_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, _i32p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.POINTER(C.c_int64)]),
+    "zf_equilibrium_populations": (C.c_int, [C.c_int64, _f32p, _f32p, _f32p, _f32p, _f32p]),
+    "zf_write_membrane_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_void_p, _i32p, _f64p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
+    "zf_write_nucleus_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_void_p, _i32p, _f64p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+    "zf_write_nucleus_edges_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p, _i32p, _f64p,
+                                             _i32p, _f32p]),
+    "zf_append_volume_area": (C.c_int, [C.c_char_p, C.c_int64, C.c_int, C.c_void_p, _i32p, _f32p, C.c_void_p]),
+    "zf_read_cells_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "zf_read_mesh_dat": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_int), C.c_void_p, C.c_int]),
+    "zf_read_wall_mesh": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "zf_write_wall_vtk": (C.c_int, [C.c_char_p, C.c_int, _f32p, C.c_int, _i32p, _f32p, _f32p, _i32p]),
     "zf_profile_stages": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "zf_wss": (C.c_int, [_P, C.c_void_p, C.c_double, _f32p, C.c_void_p, C.c_void_p]),
     "zf_wss_objective": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, C.c_void_p,
@@ -327,6 +349,143 @@ def mesh_edges(tri1: np.ndarray) -> np.ndarray:
     e = np.sort(e, axis=1)
     e = np.unique(e, axis=0)
     return (e + 1).astype(np.int32)
+
+
+# ---- the reference's file formats (zf_io.cpp; host only) -------------------
+
+def _path(p) -> bytes:
+    return os.fsencode(p)
+
+
+def _opt(a, dtype):
+    return None if a is None else np.ascontiguousarray(a, dtype)
+
+
+def read_bindex_csv(path, dims, origin=(0.0, 0.0, 0.0), dx=0.5):
+    nx, ny, nz = dims
+    b = np.empty(nx * ny * nz, np.int32)
+    rows = C.c_int64()
+    _check(lib().zf_read_bindex_csv(_path(path), nx, ny, nz, np.asarray(origin, np.float64), dx, b,
+                                    C.byref(rows)))
+    return b.reshape(nx, ny, nz), rows.value
+
+
+def write_fluid_csv(path, b_index, D, U, V, W, bodyforce, eulneigh=None, windex=None, origin=(0.0, 0.0, 0.0),
+                    dx=0.5):
+    b = np.ascontiguousarray(b_index, np.int32)
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)  # noqa: E731
+    en, wi = _opt(eulneigh, np.int32), _opt(windex, np.int32)
+    _check(lib().zf_write_fluid_csv(_path(path), *b.shape, np.asarray(origin, np.float64), dx, b.ravel(), f32(D),
+                                    f32(U), f32(V), f32(W), f32(bodyforce).ravel(), _ptr(en), _ptr(wi)))
+
+
+def read_fluid_csv(path, b_index, origin=(0.0, 0.0, 0.0), dx=0.5):
+    """(D, U, V, W [n], bodyforce [3][n], eulneigh [n] in DOMLIST order,
+    windex [nx][ny][nz], rows)."""
+    b = np.ascontiguousarray(b_index, np.int32)
+    n = int((b >= 0).sum())
+    D, U, V, W = (np.zeros(n, np.float32) for _ in range(4))
+    bf = np.zeros((3, n), np.float32)
+    en = np.zeros(n, np.int32)
+    wi = np.zeros(b.shape, np.int32)
+    rows = C.c_int64()
+    _check(lib().zf_read_fluid_csv(_path(path), *b.shape, np.asarray(origin, np.float64), dx, b.ravel(), _ptr(D),
+                                   _ptr(U), _ptr(V), _ptr(W), _ptr(bf), _ptr(en), _ptr(wi), C.byref(rows)))
+    return D, U, V, W, bf, en, wi, rows.value
+
+
+def equilibrium_populations(D, U, V, W):
+    D, U, V, W = (np.ascontiguousarray(a, np.float32) for a in (D, U, V, W))
+    f = np.empty((19, D.size), np.float32)
+    _check(lib().zf_equilibrium_populations(D.size, D, U, V, W, f.ravel()))
+    return f
+
+
+def write_membrane_csv(path, status, x, vel=None, wall_tri=None, wrep=None, regress=None, area_ratio=None,
+                       ftot=None, fvol=None, out_flag=None, cell_id=None):
+    x = np.ascontiguousarray(x, np.float64)
+    nc, nn = x.shape[1], x.shape[2]
+    args = [_opt(cell_id, np.int32), np.ascontiguousarray(status, np.int32), x.ravel(), _opt(vel, np.float64),
+            _opt(wall_tri, np.int32), _opt(wrep, np.float32), _opt(regress, np.int32),
+            _opt(area_ratio, np.float32), _opt(ftot, np.float32), _opt(fvol, np.float32), _opt(out_flag, np.int32)]
+    _check(lib().zf_write_membrane_csv(_path(path), nc, nn, _ptr(args[0]), args[1], args[2],
+                                       *[_ptr(a) for a in args[3:]]))
+
+
+def write_nucleus_csv(path, status, xn, vel_n=None, ftot_n=None, neigh=None, neigh_flag=None, cell_id=None):
+    xn = np.ascontiguousarray(xn, np.float64)
+    nc, nn = xn.shape[1], xn.shape[2]
+    opt = [_opt(vel_n, np.float64), _opt(ftot_n, np.float32), _opt(neigh, np.int32), _opt(neigh_flag, np.int32)]
+    cid = _opt(cell_id, np.int32)
+    _check(lib().zf_write_nucleus_csv(_path(path), nc, nn, _ptr(cid), np.ascontiguousarray(status, np.int32),
+                                      xn.ravel(), *[_ptr(a) for a in opt]))
+
+
+def write_nucleus_edges_csv(path, status, xn, edge_n, lmax_n, cell_id=None):
+    xn = np.ascontiguousarray(xn, np.float64)
+    e = np.ascontiguousarray(edge_n, np.int32)
+    cid = _opt(cell_id, np.int32)
+    _check(lib().zf_write_nucleus_edges_csv(_path(path), xn.shape[1], xn.shape[2], e.shape[0], _ptr(cid),
+                                            np.ascontiguousarray(status, np.int32), xn.ravel(), e.ravel(),
+                                            np.ascontiguousarray(lmax_n, np.float32)))
+
+
+def append_volume_area(path, it, status, cell_f, regress=None, cell_id=None):
+    st = np.ascontiguousarray(status, np.int32)
+    cid, rg = _opt(cell_id, np.int32), _opt(regress, np.int32)
+    _check(lib().zf_append_volume_area(_path(path), it, st.size, _ptr(cid), st,
+                                       np.ascontiguousarray(cell_f, np.float32).ravel(), _ptr(rg)))
+
+
+def read_cells_csv(path, n_node, nucleus=False):
+    """(cell_id [nc], status [nc], x, vel [3][nc][n_node] fp64, ftot [3][nc][n_node] fp32)."""
+    nc = C.c_int()
+    L = lib()
+    _check(L.zf_read_cells_csv(_path(path), int(nucleus), n_node, 0, C.byref(nc), None, None, None, None, None))
+    k = nc.value
+    cid, st = np.empty(k, np.int32), np.empty(k, np.int32)
+    x, vel = np.empty((3, k, n_node)), np.empty((3, k, n_node))
+    ft = np.empty((3, k, n_node), np.float32)
+    _check(L.zf_read_cells_csv(_path(path), int(nucleus), n_node, k, C.byref(nc), _ptr(cid), _ptr(st), _ptr(x),
+                               _ptr(vel), _ptr(ft)))
+    return cid, st, x, vel, ft
+
+
+MESH_POINTS, MESH_CELLS, MESH_LINES = 0, 1, 2
+
+
+def read_mesh_dat(path, kind):
+    n = C.c_int()
+    L = lib()
+    _check(L.zf_read_mesh_dat(_path(path), kind, C.byref(n), None, 0))
+    per = 2 if kind == MESH_LINES else 3
+    v = np.empty(n.value * per)
+    _check(L.zf_read_mesh_dat(_path(path), kind, C.byref(n), _ptr(v), n.value))
+    v = v.reshape(n.value, per)
+    return v if kind == MESH_POINTS else v.astype(np.int32)
+
+
+def read_wall_mesh(nodes_path, cells_path, normals_path):
+    """(xyz [3][n], tri [3][m] 1-based, normals [3][m]) as zf_set_wall takes them."""
+    nn_, nt_ = C.c_int(), C.c_int()
+    L = lib()
+    paths = (_path(nodes_path), _path(cells_path), _path(normals_path))
+    _check(L.zf_read_wall_mesh(*paths, C.byref(nn_), C.byref(nt_), None, None, None, 0, 0))
+    xyz = np.empty((3, nn_.value), np.float32)
+    tri = np.empty((3, nt_.value), np.int32)
+    nrm = np.empty((3, nt_.value), np.float32)
+    _check(L.zf_read_wall_mesh(*paths, C.byref(nn_), C.byref(nt_), _ptr(xyz), _ptr(tri), _ptr(nrm), nn_.value,
+                               nt_.value))
+    return xyz, tri, nrm
+
+
+def write_wall_vtk(path, xyz, tri, pressure, wss, valid):
+    xyz = np.ascontiguousarray(xyz, np.float32)
+    tri = np.ascontiguousarray(tri, np.int32)
+    _check(lib().zf_write_wall_vtk(_path(path), xyz.shape[1], xyz.ravel(), tri.shape[1], tri.ravel(),
+                                   np.ascontiguousarray(pressure, np.float32),
+                                   np.ascontiguousarray(wss, np.float32).ravel(),
+                                   np.ascontiguousarray(valid, np.int32)))
 
 
 class Context:
