@@ -166,6 +166,11 @@ int zf_download_bodyforce(zf_ctx* ctx, float* bodyforce);
  * (post-collision moments without force shift, ZebraflowWT.c:6599-6616). */
 int zf_download_moments(zf_ctx* ctx, float* D, float* U, float* V, float* W);
 
+/* Recomputes the stored D,U,V,W from the current populations (the moments
+ * of the reference's LBM_FLUID pass, ZebraflowWT.c:6603-6616), so that a
+ * snapshot can be taken after any step. */
+int zf_lbm_moments(zf_ctx* ctx);
+
 /* ---- LBM step ------------------------------------------------------------ */
 
 /* One LBM time step: pull stream + BGK/Guo collision (ZebraflowWT.c:6100-6145),
@@ -319,6 +324,11 @@ int zf_get_wall_index(zf_ctx* ctx, int32_t* windex, float* uvoid);
  * :9149-9430).  Adds to NODE_VEL / NODE_VEL_N and NODE_WALLREPUL. */
 int zf_ibm_interp(zf_ctx* ctx);
 
+/* Number of triangle centroids the cell list of the last membrane step holds
+ * at each listed point, DOMLIST order (the reference's EulNeigh[0][o], filled
+ * by CGSM_AREA, ZebraflowWT.c:5857-5900); 0 before any membrane step. */
+int zf_get_cell_list_counts(zf_ctx* ctx, int32_t* counts);
+
 /* Nucleus-membrane repulsion (ZebraflowWT.c:9516-9730); rebuild_lists=1
  * rebuilds every nucleus node's triangle list (the reference does so every
  * 1000 iterations, :9527).  Adds to NODE_WALLREPUL. */
@@ -428,6 +438,18 @@ int zf_profile_stages(zf_ctx* ctx, float* stage_ms, int* blocks);
 
 /* Completed iterations (the reference's iter). */
 int zf_iteration(zf_ctx* ctx, int64_t* iter);
+
+/* Exact checkpoints (the reference restarts from its CSV snapshots, rebuilding
+ * the populations as feq(D, u), ZebraflowWT.c:2649-2700, :5253-5295, which
+ * leaves the trajectory).  zf_save_state writes what the next step reads: the
+ * current populations in their storage form, BODYFORCE, the stored moments,
+ * the cells' fp64 positions and velocities, forces, repulsion increments,
+ * statuses and counters, the nucleus-membrane lists and the iteration count.
+ * zf_load_state restores it into a context set up with the same lattice,
+ * storage form, mesh and cell count (else ZF_ERR_ARG), after which zf_step
+ * continues the saved run.  Both wait for the context's queued work. */
+int zf_save_state(zf_ctx* ctx, const char* path);
+int zf_load_state(zf_ctx* ctx, const char* path);
 
 /* ---- input generators (synthetic stand-ins for the reference's input files,
  *      FLUIDdomainBindex.csv read at ZebraflowWT.c:2574-2619) ---------------- */

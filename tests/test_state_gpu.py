@@ -1,0 +1,78 @@
+"""Exact checkpoints (zf_save_state / zf_load_state).  A run of the coupled
+step saved at iteration 120 and continued in a fresh context is the run that
+wrote it: populations, moments, body force and node positions agree after 130
+more iterations (three membrane blocks) within the run-to-run spread of the
+spreading's float atomics, for plain fp32 and for fp16 storage with
+stochastic rounding (whose bits are seeded by the restored iteration count).
+A context with another lattice refuses the file."""
+import numpy as np
+import pytest
+
+import zebraflow_b200 as zf
+
+pytestmark = pytest.mark.gpu
+
+NX, NY, NZ, R, C = 40, 40, 48, 16.0, 19.5
+
+
+def setup(storage):
+    b = zf.gen_tube(NX, NY, NZ, C, C, R, True)
+    p = zf.default_params(nx=NX, ny=NY, nz=NZ, tau=0.9, tau_from_phase=0, wall_mode=zf.WALL_HALFWAY_BB,
+                          periodic=(0, 0, 1), g=(0, 0, 2e-5), origin=(0.0, 0.0, 0.0), area0=0.0, volume0=0.0,
+                          storage=storage)
+    xyz, tri = zf.gen_icosphere(3)
+    xyzn, trin = zf.gen_icosphere(2)
+    rest, rest_n = xyz * np.array([3.5, 2.25, 1.0]), xyzn * np.array([1.25, 0.9, 0.6])
+    cells = zf.gen_cells(b, 4, rest, rest_n, (3.5, 2.25, 1.0), seed=11, margin=0.4)
+    ctx = zf.Context(p)
+    ctx.set_lattice(b)
+    ctx.set_wall(*zf.gen_wall_tube(C, C, R, NZ))
+    ctx.set_mesh(rest, tri, rest_n, zf.mesh_edges(trin))
+    ctx.set_cells(*cells)
+    return ctx, cells
+
+
+def state(ctx):
+    x, xn, st = ctx.cells()
+    return dict(f=ctx.download_populations(), bf=ctx.download_bodyforce(), mom=np.stack(ctx.download_moments()),
+                x=x, xn=xn, st=st, it=ctx.iteration())
+
+
+@pytest.mark.parametrize("storage", [zf.STORE_F32, zf.STORE_F16])
+def test_continued_run_is_the_saved_run(storage, tmp_path):
+    path = str(tmp_path / "state.bin")
+    a, cells = setup(storage)
+    a.step(120)
+    a.save_state(path)
+    a.step(130)
+    A = state(a)
+    a.close()
+    b, _ = setup(storage)
+    b.load_state(path)
+    assert b.iteration() == 120
+    b.step(130)
+    B = state(b)
+    b.close()
+    assert A["it"] == B["it"] == 250
+    assert np.array_equal(A["st"], B["st"])
+    assert np.abs(A["x"] - cells[0]).max() > 1e-3  # the cells moved
+    assert np.abs(A["x"] - B["x"]).max() < 1e-7 and np.abs(A["xn"] - B["xn"]).max() < 1e-7
+    assert np.abs(A["f"] - B["f"]).max() < 1e-6
+    assert np.abs(A["mom"] - B["mom"]).max() < 1e-6
+    assert np.abs(A["bf"] - B["bf"]).max() <= 1e-5 * max(np.abs(A["bf"]).max(), 1e-30)
+
+
+def test_other_lattice_refuses_the_file(tmp_path):
+    path = str(tmp_path / "state.bin")
+    a, _ = setup(zf.STORE_F32)
+    a.step(10)
+    a.save_state(path)
+    a.close()
+    b = zf.gen_tube(NX, NY, NZ + 4, C, C, R, True)
+    p = zf.default_params(nx=NX, ny=NY, nz=NZ + 4, tau=0.9, tau_from_phase=0, wall_mode=zf.WALL_HALFWAY_BB,
+                          periodic=(0, 0, 1))
+    with zf.Context(p) as ctx:
+        ctx.set_lattice(b)
+        with pytest.raises(zf.ZfError) as e:
+            ctx.load_state(path)
+        assert "another lattice" in str(e.value)

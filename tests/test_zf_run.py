@@ -85,3 +85,45 @@ def test_driver_matches_the_python_path(tmp_path):
     assert np.array_equal(d["status"], st)
     assert np.abs(d["wss"] - wss).max() <= 1e-5 * np.abs(wss).max()
     assert np.abs(d["mom"] - mom).max() < 1e-6
+
+
+@pytest.mark.gpu
+def test_driver_writes_reference_files_and_restarts_exactly(tmp_path):
+    out_dir = tmp_path / "SimulationOutputData"
+    out_dir.mkdir()
+    full, half, cont = (str(tmp_path / n) for n in ("full.bin", "half.bin", "cont.bin"))
+    state = str(tmp_path / "state.bin")
+    r = subprocess.run([EXE, "--steps", "100", "--output-every", "50", "--output-dir", str(out_dir), "--out", half,
+                        "--save-state", state], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    names = sorted(os.listdir(out_dir))
+    for it in (0, 50, 100):
+        for stem, ext in (("FLUIDdomain", "csv"), ("AllCellMemb", "csv"), ("AllCellNucleus", "csv"),
+                          ("AllNucEdgeMesh", "csv"), ("Wallpressure", "vtk")):
+            assert f"{stem}-{it:09d}.{ext}" in names
+    assert "VolumeAreaHistory.dat" in names
+    d = read_dump(half)
+    # the last snapshot holds the dumped state, to its printed digits
+    b = zf.gen_tube(48, 48, 128, 23.5, 23.5, 20.0, True)
+    D, U, V, W, bf, en, wi, rows = zf.read_fluid_csv(str(out_dir / "FLUIDdomain-000000100.csv"), b)
+    assert rows == int((b >= 0).sum())
+    # (the snapshot's moments are recomputed from the populations; velocities
+    # carry the fp32 rounding of momentum sums of O(0.05) populations)
+    assert np.all(np.abs(D - d["mom"][0]) <= 3e-7 * np.abs(d["mom"][0]))
+    for a, ref in ((U, d["mom"][1]), (V, d["mom"][2]), (W, d["mom"][3])):
+        assert np.all(np.abs(a - ref) <= 1.2e-7 * np.abs(ref) + 5e-8)
+    assert en.sum() > 0 and (wi > 0).sum() > 0  # cell-list counts and wall indices are filled
+    cid, st, x, vel, ft = zf.read_cells_csv(str(out_dir / "AllCellMemb-000000100.csv"), 642)
+    assert np.array_equal(cid, np.arange(1, 9)) and np.abs(x - d["x"]).max() < 5e-6
+    hist = open(out_dir / "VolumeAreaHistory.dat").read().splitlines()
+    assert hist[0].startswith("Iteration#") and len(hist) == 1 + 3 * 8
+    # continuing from the checkpoint is the uninterrupted run
+    r = subprocess.run([EXE, "--steps", "100", "--load-state", state, "--out", cont], capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([EXE, "--steps", "200", "--out", full], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    a, c = read_dump(full), read_dump(cont)
+    assert a["iter"] == c["iter"] == 200
+    assert np.abs(a["x"] - c["x"]).max() < 1e-7 and np.array_equal(a["status"], c["status"])
+    assert np.abs(a["mom"] - c["mom"]).max() < 1e-6

@@ -138,6 +138,8 @@ _SIGS = {
                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
     "zf_write_wall_vtk": (C.c_int, [C.c_char_p, C.c_int, _f32p, C.c_int, _i32p, _f32p, _f32p, _i32p]),
     "zf_profile_stages": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
+    "zf_save_state": (C.c_int, [_P, C.c_char_p]),
+    "zf_load_state": (C.c_int, [_P, C.c_char_p]),
     "zf_wss": (C.c_int, [_P, C.c_void_p, C.c_double, _f32p, C.c_void_p, C.c_void_p]),
     "zf_wss_objective": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, C.c_void_p,
                                    C.c_void_p, C.POINTER(C.c_double)]),
@@ -772,6 +774,15 @@ class Context:
         m = C.c_double()
         _check(lib().zf_step_mass(self._h, C.byref(m)))
         return m.value
+
+    def save_state(self, path):
+        """Exact checkpoint of the time-stepping state (zf_save_state)."""
+        _check(lib().zf_save_state(self._h, os.fsencode(path)))
+
+    def load_state(self, path):
+        """Restores a checkpoint into this context (same lattice, storage,
+        mesh and cell count)."""
+        _check(lib().zf_load_state(self._h, os.fsencode(path)))
 
     def launch_count(self) -> int:
         n = C.c_int64()

@@ -461,6 +461,12 @@ int zf_download_moments(zf_ctx* c, float* D, float* U, float* V, float* W) {
   return ZF_OK;
 }
 
+int zf_lbm_moments(zf_ctx* c) {
+  NEED_LATTICE("zf_lbm_moments");
+  ZF_CUDA(cudaSetDevice(c->device));
+  return lbm_moments_launch(c);
+}
+
 int zf_lbm_step(zf_ctx* c, int store_moments, int zero_bodyforce) {
   NEED_LATTICE("zf_lbm_step");
   int rc = lbm_launch(c, store_moments, zero_bodyforce);

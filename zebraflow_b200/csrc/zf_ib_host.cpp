@@ -301,6 +301,29 @@ int zf_wss(zf_ctx* c, const float* node_normals, double pgauge, float* wss, floa
   return rc;
 }
 
+int zf_get_cell_list_counts(zf_ctx* c, int32_t* counts) {
+  if (!c || !counts) return ZF_ERR_ARG;
+  if (!c->lattice_set) {
+    set_error("zf_get_cell_list_counts: lattice not set");
+    return ZF_ERR_STATE;
+  }
+  ZF_CUDA(cudaSetDevice(c->device));
+  const int64_t n = c->n_listed;
+  for (int64_t l = 0; l < n; ++l) counts[l] = 0;
+  if (!c->cells_set || c->ib_allocs.empty() || !c->ib.bin_off) return ZF_OK;
+  std::vector<int32_t> off((size_t)c->ns + 1), slot((size_t)n);
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  ZF_CUDA(cudaMemcpy(off.data(), c->ib.bin_off, off.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  ZF_CUDA(cudaMemcpy(slot.data(), c->d_dom_slot, slot.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  for (int64_t l = 0; l < n; ++l) {
+    const int64_t s = slot[(size_t)l], cc = s & 63;
+    // the cell list is keyed with z fastest inside a tile (k_bin_assign)
+    const int64_t key = (s & ~(int64_t)63) | (((cc >> 4) & 3) + 4 * ((cc >> 2) & 3) + 16 * (cc & 3));
+    counts[l] = off[(size_t)key + 1] - off[(size_t)key];
+  }
+  return ZF_OK;
+}
+
 int zf_ibm_interp(zf_ctx* c) {
   NEED_IB("zf_ibm_interp");
   return ib_interp_launch(c);

@@ -10,12 +10,19 @@
  * icosphere membranes and nuclei placed from a seed), runs the loop through
  * zf_step in whole cycles of SOLVERSTAGGER iterations, reports throughput
  * from CUDA events, and writes the final state (node positions, cell status,
- * wall shear stress, fluid moments) as a binary dump (--out).
+ * wall shear stress, fluid moments) as a binary dump (--out).  With
+ * --output-every N it writes, at iteration 0 and every N iterations, the
+ * files the reference's OUTPUT() writes (FLUIDdomain, AllCellMemb,
+ * AllCellNucleus, AllNucEdgeMesh, VolumeAreaHistory; ZebraflowWT.c:282-509)
+ * and the post-processor's Wallpressure VTK file (PostProWSSandPressure.c:
+ * 375-433) into --output-dir.  --save-state / --load-state write and read an
+ * exact checkpoint (zf_save_state) at the end / start of the run.
  *
  * usage: zf_run [--tube NX NY NZ R | --bifurcation NX NY NZ RP RD HALF_ANGLE]
  *               [--cells N] [--seed S] [--steps N] [--stagger S] [--tau T]
  *               [--g G] [--storage f32|f16|bf16|f32dev] [--device D]
- *               [--out FILE]
+ *               [--out FILE] [--output-every N] [--output-dir DIR]
+ *               [--save-state FILE] [--load-state FILE]
  * Defaults: the 48x48x128 tube of radius 20 with 8 cells, 1000 iterations.
  */
 #include <math.h>
@@ -90,18 +97,24 @@ typedef struct {
   float tau, g;
   int storage, device;
   const char* out;
+  int output_every;
+  const char* output_dir;
+  const char* save_state;
+  const char* load_state;
 } opts;
 
 static void usage(void) {
   fprintf(stderr,
           "usage: zf_run [--tube NX NY NZ R | --bifurcation NX NY NZ RP RD HALF_ANGLE] [--cells N]\n"
           "              [--seed S] [--steps N] [--stagger S] [--tau T] [--g G]\n"
-          "              [--storage f32|f16|bf16|f32dev] [--device D] [--out FILE]\n");
+          "              [--storage f32|f16|bf16|f32dev] [--device D] [--out FILE]\n"
+          "              [--output-every N] [--output-dir DIR] [--save-state FILE] [--load-state FILE]\n");
   exit(2);
 }
 
 static opts parse(int argc, char** argv) {
-  opts o = {0, 48, 48, 128, 20.0, 0, 0, 20.0, 8, 1234, 1000, 50, 0.9f, 1e-6f, ZF_STORE_F32, 0, NULL};
+  opts o = {0,    48,   48, 128, 20.0, 0, 0, 20.0, 8, 1234, 1000, 50, 0.9f, 1e-6f, ZF_STORE_F32, 0, NULL, 0,
+            "SimulationOutputData", NULL, NULL};
   for (int i = 1; i < argc; ++i) {
     const char* a = argv[i];
 #define NEED(k) \
@@ -154,12 +167,25 @@ static opts parse(int argc, char** argv) {
     } else if (!strcmp(a, "--out")) {
       NEED(1);
       o.out = argv[++i];
+    } else if (!strcmp(a, "--output-every")) {
+      NEED(1);
+      o.output_every = atoi(argv[++i]);
+    } else if (!strcmp(a, "--output-dir")) {
+      NEED(1);
+      o.output_dir = argv[++i];
+    } else if (!strcmp(a, "--save-state")) {
+      NEED(1);
+      o.save_state = argv[++i];
+    } else if (!strcmp(a, "--load-state")) {
+      NEED(1);
+      o.load_state = argv[++i];
     } else {
       usage();
     }
 #undef NEED
   }
-  if (o.nx <= 0 || o.ny <= 0 || o.nz <= 0 || o.cells < 0 || o.steps < 0 || o.stagger <= 0) usage();
+  if (o.nx <= 0 || o.ny <= 0 || o.nz <= 0 || o.cells < 0 || o.steps < 0 || o.stagger <= 0 || o.output_every < 0)
+    usage();
   return o;
 }
 
@@ -187,6 +213,87 @@ static void wall_mesh(const opts* o, const double* origin, int* nw, int* mt, flo
       *nrm = (float*)xmalloc(sizeof(float) * 3 * (size_t)*mt);
     }
   }
+}
+
+/* the reference's output file name: DIR/NAME-<iteration, 9 digits>.EXT (:304-337) */
+static const char* out_name(char* buf, size_t n, const char* dir, const char* name, long long it, const char* ext) {
+  snprintf(buf, n, "%s/%s-%09lld.%s", dir, name, it, ext);
+  return buf;
+}
+
+typedef struct {
+  const opts* o;
+  zf_ctx* ctx;
+  const int32_t* b;
+  int placed, nn, nnn, nw, mt, n_edge_n;
+  const float* wxyz;
+  const int32_t* wtri;
+  const int32_t* edge_n;
+} run_t;
+
+/* OUTPUT() of the reference (ZebraflowWT.c:282-509) and the post-processor's
+ * wall file, for the current state */
+static void write_outputs(const run_t* r) {
+  const opts* o = r->o;
+  zf_ctx* ctx = r->ctx;
+  char path[4096];
+  int64_t it = 0, n = 0, nf = 0;
+  check(zf_iteration(ctx, &it), "zf_iteration");
+  check(zf_num_listed(ctx, &n, &nf), "zf_num_listed");
+  const size_t npts = (size_t)o->nx * o->ny * o->nz;
+  float* mom = (float*)xmalloc(sizeof(float) * 4 * (size_t)n);
+  float* bf = (float*)xmalloc(sizeof(float) * 3 * (size_t)n);
+  int32_t* en = (int32_t*)xmalloc(sizeof(int32_t) * (size_t)n);
+  int32_t* wi = (int32_t*)xmalloc(sizeof(int32_t) * npts);
+  check(zf_lbm_moments(ctx), "zf_lbm_moments");
+  check(zf_download_moments(ctx, mom, mom + n, mom + 2 * n, mom + 3 * n), "zf_download_moments");
+  check(zf_download_bodyforce(ctx, bf), "zf_download_bodyforce");
+  check(zf_get_cell_list_counts(ctx, en), "zf_get_cell_list_counts");
+  check(zf_get_wall_index(ctx, wi, NULL), "zf_get_wall_index");
+  const double origin[3] = {0.0, 0.0, 0.0};
+  check(zf_write_fluid_csv(out_name(path, sizeof path, o->output_dir, "FLUIDdomain", it, "csv"), o->nx, o->ny,
+                           o->nz, origin, DX_UM, r->b, mom, mom + n, mom + 2 * n, mom + 3 * n, bf, en, wi),
+        "zf_write_fluid_csv");
+  if (r->placed > 0) {
+    const size_t nc = (size_t)r->placed, m = 3 * nc * r->nn, mn = 3 * nc * r->nnn;
+    double *x = (double*)xmalloc(sizeof(double) * m), *xn = (double*)xmalloc(sizeof(double) * mn);
+    double *v = (double*)xmalloc(sizeof(double) * m), *vn = (double*)xmalloc(sizeof(double) * mn);
+    float *wr = (float*)xmalloc(sizeof(float) * m), *wrn = (float*)xmalloc(sizeof(float) * mn);
+    float *ft = (float*)xmalloc(sizeof(float) * m), *ftn = (float*)xmalloc(sizeof(float) * mn);
+    float* cf = (float*)xmalloc(sizeof(float) * 8 * nc);
+    int32_t* st = (int32_t*)xmalloc(sizeof(int32_t) * nc);
+    int32_t ne = 0;
+    double a0 = 0, v0 = 0;
+    check(zf_mesh_info(ctx, &ne, &a0, &v0), "zf_mesh_info");
+    float* epar = (float*)xmalloc(sizeof(float) * 5 * (size_t)ne);
+    float* epar_n = (float*)xmalloc(sizeof(float) * 3 * (size_t)r->n_edge_n);
+    check(zf_get_cells(ctx, x, xn, st), "zf_get_cells");
+    check(zf_get_cell_kinematics(ctx, v, vn, wr, wrn), "zf_get_cell_kinematics");
+    check(zf_get_cell_forces(ctx, ft, ftn), "zf_get_cell_forces");
+    check(zf_get_cell_geometry(ctx, NULL, NULL, NULL, NULL, cf), "zf_get_cell_geometry");
+    check(zf_get_edge_params(ctx, epar, epar_n, NULL), "zf_get_edge_params");
+    check(zf_write_membrane_csv(out_name(path, sizeof path, o->output_dir, "AllCellMemb", it, "csv"), r->placed,
+                                r->nn, NULL, st, x, v, NULL, wr, NULL, NULL, ft, NULL, NULL),
+          "zf_write_membrane_csv");
+    check(zf_write_nucleus_csv(out_name(path, sizeof path, o->output_dir, "AllCellNucleus", it, "csv"), r->placed,
+                               r->nnn, NULL, st, xn, vn, ftn, NULL, NULL),
+          "zf_write_nucleus_csv");
+    check(zf_write_nucleus_edges_csv(out_name(path, sizeof path, o->output_dir, "AllNucEdgeMesh", it, "csv"),
+                                     r->placed, r->nnn, r->n_edge_n, NULL, st, xn, r->edge_n, epar_n),
+          "zf_write_nucleus_edges_csv");
+    snprintf(path, sizeof path, "%s/VolumeAreaHistory.dat", o->output_dir);
+    check(zf_append_volume_area(path, it, r->placed, NULL, st, cf, NULL), "zf_append_volume_area");
+    free(x), free(xn), free(v), free(vn), free(wr), free(wrn), free(ft), free(ftn), free(cf), free(st);
+    free(epar), free(epar_n);
+  }
+  float* wss = (float*)xmalloc(sizeof(float) * 3 * (size_t)r->nw);
+  float* press = (float*)xmalloc(sizeof(float) * (size_t)r->nw);
+  int32_t* valid = (int32_t*)xmalloc(sizeof(int32_t) * (size_t)r->nw);
+  check(zf_wss(ctx, NULL, 120.0, wss, press, valid), "zf_wss");
+  check(zf_write_wall_vtk(out_name(path, sizeof path, o->output_dir, "Wallpressure", it, "vtk"), r->nw, r->wxyz,
+                          r->mt, r->wtri, press, wss, valid),
+        "zf_write_wall_vtk");
+  free(mom), free(bf), free(en), free(wi), free(wss), free(press), free(valid);
 }
 
 int main(int argc, char** argv) {
@@ -269,18 +376,33 @@ int main(int argc, char** argv) {
     if (placed > 0) check(zf_set_cells(ctx, placed, x, xn), "zf_set_cells");
   }
 
-  /* the time loop: whole cycles of `stagger` iterations, then the rest */
+  if (o.load_state) check(zf_load_state(ctx, o.load_state), "zf_load_state");
+  const run_t run = {&o, ctx, b, placed, nn, nnn, nw, mt, n_edge_n, wxyz, wtri, edge_n};
+  int64_t it0 = 0;
+  check(zf_iteration(ctx, &it0), "zf_iteration");
+  if (o.output_every > 0 && it0 % o.output_every == 0) write_outputs(&run);
+
+  /* the time loop in whole cycles of `stagger` iterations (and up to each
+     output iteration); outputs are written outside the timed steps */
   float ms = 0.f, part = 0.f;
   int done = 0;
   while (done < o.steps) {
-    const int n = o.steps - done < o.stagger ? o.steps - done : o.stagger;
+    const int64_t it = it0 + done;
+    int n = o.stagger - (int)(it % o.stagger);
+    if (o.output_every > 0) {
+      const int to_out = o.output_every - (int)(it % o.output_every);
+      if (to_out < n) n = to_out;
+    }
+    if (n > o.steps - done) n = o.steps - done;
     check(zf_step_timed(ctx, n, &part), "zf_step_timed");
     ms += part;
     done += n;
+    if (o.output_every > 0 && (it0 + done) % o.output_every == 0) write_outputs(&run);
   }
+  if (o.save_state) check(zf_save_state(ctx, o.save_state), "zf_save_state");
   zf_status st;
   check(zf_get_status(ctx, &st), "zf_get_status");
-  const int64_t blocks = placed > 0 ? st.iter / o.stagger : 0;
+  const int64_t blocks = placed > 0 ? st.iter / o.stagger - it0 / o.stagger : 0;
   const double s = ms * 1e-3;
   printf("zf_run: %d iterations, %lld fluid points, %d cells (%lld removed), %lld membrane blocks, "
          "%.3f ms device time, %.1f MLUPS, %.4g membrane-node updates/s\n",
