@@ -139,6 +139,8 @@ _SIGS = {
     "zf_write_wall_vtk": (C.c_int, [C.c_char_p, C.c_int, _f32p, C.c_int, _i32p, _f32p, _f32p, _i32p]),
     "zf_profile_stages": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "zf_save_state": (C.c_int, [_P, C.c_char_p]),
+    "zf_lbm_moments": (C.c_int, [_P]),
+    "zf_get_cell_list_counts": (C.c_int, [_P, _i32p]),
     "zf_load_state": (C.c_int, [_P, C.c_char_p]),
     "zf_wss": (C.c_int, [_P, C.c_void_p, C.c_double, _f32p, C.c_void_p, C.c_void_p]),
     "zf_wss_objective": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, C.c_void_p,
@@ -774,6 +776,16 @@ class Context:
         m = C.c_double()
         _check(lib().zf_step_mass(self._h, C.byref(m)))
         return m.value
+
+    def refresh_moments(self):
+        """Recomputes the stored D, U, V, W from the current populations."""
+        _check(lib().zf_lbm_moments(self._h))
+
+    def cell_list_counts(self):
+        """Triangle centroids per listed point in the last cell list (EulNeigh)."""
+        n = np.empty(self.n_listed, np.int32)
+        _check(lib().zf_get_cell_list_counts(self._h, n))
+        return n
 
     def save_state(self, path):
         """Exact checkpoint of the time-stepping state (zf_save_state)."""
