@@ -139,8 +139,11 @@ int zf_get_status(zf_ctx* ctx, zf_status* out);
 /* ---- lattice ------------------------------------------------------------- */
 
 /* Sets the lattice from reference B_index codes ([nx][ny][nz], k fastest):
- * <0 solid, 0 wall point, 1..9 fluid of that phase.  Codes >= 10 (pressure
- * inlets >= 1000, the deprecated 4998) are rejected with ZF_ERR_ARG.
+ * <0 solid, 0 wall point, 1..9 fluid of that phase, 1001..1009 pressure
+ * inlet/outlet points of the reference's waveforms (ZebraflowWT.c:6316-6426;
+ * reference wall mode only: they take feq(P(t)/LBM_PRESSURE_SCALE + 1, u) of
+ * their designated neighbour every step).  Other codes (the deprecated 4998)
+ * are rejected with ZF_ERR_ARG.
  * Builds the listed-node order (LBM_DOM_SETUP, ZebraflowWT.c:1481-1502), the
  * designated neighbour of every wall point (LBM_BC_SETUP, ZebraflowWT.c:1506-1589)
  * and the device tile index; initialises f = feq(rho_ref, 0) (ZebraflowWT.c:5253-5295). */
@@ -438,6 +441,12 @@ int zf_profile_stages(zf_ctx* ctx, float* stage_ms, int* blocks);
 
 /* Completed iterations (the reference's iter). */
 int zf_iteration(zf_ctx* ctx, int64_t* iter);
+
+/* Sets the count of completed iterations, as a run restarted at iteration
+ * `iter` has it: the next step is iteration iter + 1, which fixes the
+ * membrane cadence, the pressure waveforms' time and the stochastic-rounding
+ * seed. */
+int zf_set_iteration(zf_ctx* ctx, int64_t iter);
 
 /* Exact checkpoints (the reference restarts from its CSV snapshots, rebuilding
  * the populations as feq(D, u), ZebraflowWT.c:2649-2700, :5253-5295, which

@@ -76,6 +76,7 @@ def lib() -> C.CDLL:
             g("orc_world_wss").argtypes = [C.c_void_p, _f32p, C.c_double, _f64p, C.c_void_p,
                                            C.c_void_p]
             g("orc_lbm_moments_from_f").argtypes = [C.c_void_p]
+            g("orc_lbm_set_iter").argtypes = [C.c_void_p, C.c_int64]
         _lib = L
     return _lib
 
@@ -220,6 +221,10 @@ class OracleLBM:
     def moments_from_f(self):
         """Recomputes D, U, V, W from the current populations."""
         self._fn("orc_lbm_moments_from_f")(self._h)
+
+    def set_iter(self, it):
+        """Completed steps; the next step is iteration it + 1 (pressure inlets' time)."""
+        self._fn("orc_lbm_set_iter")(self._h, int(it))
 
     def moments(self):
         outs = [np.empty(self.n) for _ in range(4)]

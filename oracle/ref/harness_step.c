@@ -20,6 +20,7 @@
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include <string.h>
 
 #define IM_ 249
 #define JM_ 547
@@ -48,7 +49,11 @@ static const int E[19][3] = {{1, 0, 0},  {-1, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0,
 
 /* the lattice: a tube of radius 4 along k (centre i = 20, j = 30), fluid for
    6 < k < 20, with a ball of phase 5 (tau from the phase) inside it and wall
-   points (code 0) at every point linked to the fluid; all else unlisted */
+   points (code 0) at every point linked to the fluid; all else unlisted.
+   With argv[2] = "pressure" the tube's end layers k = 6 and k = 20 are
+   pressure inlets/outlets of codes argv[3] and argv[4] (1001-1009, the
+   reference's waveforms, ZebraflowWT.c:6316-6426) and the steps are
+   iterations argv[5] + 1 ... of its time loop. */
 #define CI 20
 #define CJ 30
 #define TUBE_R2 16
@@ -74,6 +79,9 @@ static void put_pops(FILE* f, float (*a)[NL]) {
 
 int main(int argc, char** argv) {
   const char* out = argc > 1 ? argv[1] : "ref_step.bin";
+  const int pressure = argc > 5 && !strcmp(argv[2], "pressure");
+  const int code_lo = pressure ? atoi(argv[3]) : 0, code_hi = pressure ? atoi(argv[4]) : 0;
+  const int iter0 = pressure ? atoi(argv[5]) : 0;
   FILE* f = fopen(out, "wb");
   if (!f) return 1;
 
@@ -95,6 +103,8 @@ int main(int argc, char** argv) {
         const int r2 = (i - CI) * (i - CI) + (j - CJ) * (j - CJ);
         const int b2 = r2 + (k - 13) * (k - 13);
         if (r2 < TUBE_R2 && k > K_LO && k < K_HI) B_index[i][j][k] = b2 < 5 ? 5 : 1;
+        if (pressure && r2 < TUBE_R2 && k == K_LO) B_index[i][j][k] = code_lo;
+        if (pressure && r2 < TUBE_R2 && k == K_HI) B_index[i][j][k] = code_hi;
       }
   for (int i = CI - 6; i <= CI + 6; ++i)
     for (int j = CJ - 6; j <= CJ + 6; ++j)
@@ -106,7 +116,7 @@ int main(int argc, char** argv) {
             break;
           }
       }
-  iter = 0;
+  iter = iter0;
   LBM_DOM_SETUP();
   LBM_BC_SETUP();
 
@@ -122,6 +132,7 @@ int main(int argc, char** argv) {
   int n = DOMMAX, steps = N_STEPS;
   put(f, &n, 4);
   put(f, &steps, 4);
+  if (pressure) put(f, &iter0, 4);
   for (int l = 1; l <= DOMMAX; ++l) {
     put(f, &DOMLIST[l][0], 12);
     put(f, &B_index[DOMLIST[l][0]][DOMLIST[l][1]][DOMLIST[l][2]], 4);
@@ -132,7 +143,7 @@ int main(int argc, char** argv) {
   /* N_STEPS steps; the last one is a membrane step (RBCSOLVERFLAG = 1), which
      also clears the body force in LBM_FLUID & LBM_COPY */
   for (int s = 1; s <= N_STEPS; ++s) {
-    iter = s;
+    iter = iter0 + s;
     RBCSOLVERFLAG = s == N_STEPS;
     GOMP_parallel(zf_ref_omp_L6101, NULL, 0, 0);
     GOMP_parallel(zf_ref_omp_L6292, NULL, 0, 0);

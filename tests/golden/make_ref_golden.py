@@ -25,6 +25,9 @@ it lies (main renamed) and runs two harnesses against it:
    lattice and two cells with seeded values -> ref_output.npz (the inputs and
    the bytes of the fluid, membrane, nucleus, nucleus-edge and volume/area
    files it writes);
+ * oracle/ref/harness_step.c in its pressure mode: the same blocks with
+   pressure inlet/outlet layers of the reference's waveform codes at both
+   ends of the tube (tests/golden/pressure_scene.py) -> ref_pressure.npz;
  * oracle/ref/harness_step.c: five LBM steps of the reference's own
    stream-collide, wall and copy blocks of main() (ZebraflowWT.c:6101-6145,
    :6292-6433, :6601-6626) on a small capped tube with a phase-5 ball ->
@@ -135,6 +138,47 @@ def main():
     loop_fixture()
     wss_fixture()
     output_fixture()
+    pressure_fixture()
+
+
+def pressure_fixture():
+    """The reference's own LBM blocks (oracle/ref/harness_step.c, pressure
+    mode) with pressure inlet/outlet layers at both ends of the tube, for the
+    runs of tests/golden/pressure_scene.py: the lattice and initial state are
+    rebuilt from the scene (checked here against what the harness used), so
+    the fixture keeps the reference's moments after the last step and the
+    populations of the boundary points (walls and inlets)."""
+    from golden import pressure_scene as PS
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_step")
+    out = {"runs": np.array(PS.RUNS, np.int64)}
+    for r, (lo, hi, it0) in enumerate(PS.RUNS):
+        path = os.path.join(ROOT, "oracle", "_ref", "ref_pressure.bin")
+        subprocess.run([exe, path, "pressure", str(lo), str(hi), str(it0)], check=True, stdout=subprocess.DEVNULL)
+        raw = open(path, "rb").read()
+        a = np.frombuffer(raw, np.int32)
+        f = np.frombuffer(raw, np.float32)
+        n, steps, it = int(a[0]), int(a[1]), int(a[2])
+        assert steps == PS.STEPS and it == it0
+        p = 3
+        listed = a[p:p + 4 * n].reshape(n, 4).copy(); p += 4 * n
+        arr = {}
+        for key, k in (("f0", 19), ("bf0", 3), ("f1", 19), ("fN", 19), ("D", 1), ("U", 1), ("V", 1), ("W", 1),
+                       ("bfN", 3)):
+            arr[key] = f[p:p + k * n].reshape(k, n).copy().squeeze(); p += k * n
+        assert p == a.size
+        b = PS.lattice(lo, hi)
+        dom = np.argwhere(b >= 0)
+        assert np.array_equal(listed[:, :3] - np.array(PS.BOX_LO), dom)
+        assert np.array_equal(listed[:, 3], b[tuple(dom.T)])
+        f0, bf0 = PS.initial_state(n)
+        assert np.array_equal(f0, arr["f0"]) and np.array_equal(bf0, arr["bf0"])
+        bc = np.flatnonzero((listed[:, 3] == 0) | (listed[:, 3] >= 1000)).astype(np.int32)
+        out[f"run{r}_mom"] = np.stack([arr["D"], arr["U"], arr["V"], arr["W"]])
+        out[f"run{r}_bc"] = bc
+        out[f"run{r}_fN_bc"] = arr["fN"][:, bc]
+        os.remove(path)
+    np.savez_compressed(os.path.join(OUT, "ref_pressure.npz"), **out)
+    print(f"pressure inlets: {len(PS.RUNS)} runs of {PS.STEPS} steps, {n} listed points")
 
 
 OUTPUT_FILES = ("FLUIDdomain", "AllCellMemb", "AllCellNucleus", "AllNucEdgeMesh")

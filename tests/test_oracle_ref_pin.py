@@ -177,6 +177,49 @@ def test_lbm_step_pin_detects_a_wrong_tau():
     assert np.max(np.abs(out["fN"] - STEP["fN"])) > 100 * F_TOL
 
 
+PRESSURE = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_pressure.npz"))
+
+
+def run_oracle_pressure(precision, run, shift=0):
+    """The fixture's pressure-inlet run `run` through the oracle (shift moves
+    the waveform's time by that many iterations)."""
+    from golden import pressure_scene as PS
+    lo, hi, it0 = (int(v) for v in PRESSURE["runs"][run])
+    b = PS.lattice(lo, hi)
+    o = OracleLBM(b, wall_mode=1, tau_from_phase=True, dt=0.5, precision=precision)
+    f0, bf0 = PS.initial_state(o.n)
+    o.set_f(f0.astype(np.float64))
+    o.set_bodyforce(bf0.astype(np.float64))
+    o.set_iter(it0 + shift)
+    for s in range(1, PS.STEPS + 1):
+        o.step(rbc_flag=(s == PS.STEPS))
+    return o.get_f(), np.stack(o.moments())
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_pressure_inlets_match_reference(precision):
+    """Pressure inlet/outlet points (codes 1001-1009, ZebraflowWT.c:6316-6426)
+    against the reference's own blocks on five runs covering the waveforms:
+    moments of every listed point and the populations of the boundary points
+    after five steps."""
+    for run in range(len(PRESSURE["runs"])):
+        f, mom = run_oracle_pressure(precision, run)
+        ref = PRESSURE[f"run{run}_mom"]
+        bc = PRESSURE[f"run{run}_bc"]
+        assert np.max(np.abs(f[:, bc] - PRESSURE[f"run{run}_fN_bc"])) < F_TOL, run
+        assert np.max(np.abs(mom[0] - ref[0])) < D_TOL, run
+        assert np.max(np.abs(mom[1:] - ref[1:])) < U_TOL, run
+        # the inlet layers are driven: their density is the waveform's, not 1
+        codes = PRESSURE["runs"][run][:2]
+        assert np.abs(ref[0, bc] - 1).max() > 0.03, codes
+
+
+def test_pressure_pin_detects_a_wrong_waveform_time():
+    """A mistake planted in the oracle: the waveforms read a time 0.18 s late."""
+    f, mom = run_oracle_pressure("f64", 0, shift=360000)
+    assert np.max(np.abs(mom[0] - PRESSURE["run0_mom"][0])) > 100 * D_TOL
+
+
 def run_oracle_cells(precision, **params):
     o = OracleCells(GOLD["mesh_x"], GOLD["mesh_tri"], GOLD["nuc_x"], GOLD["nuc_edges"],
                     zf.default_params(**params), precision=precision)
@@ -416,7 +459,8 @@ def test_fixtures_regenerate_from_the_reference(tmp_path):
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     subprocess.run([sys.executable, os.path.join(root, "tests", "golden", "make_ref_golden.py"),
                     reference_dir(), str(tmp_path)], check=True, capture_output=True)
-    for name in ("ref_setup", "ref_step", "ref_cells", "ref_ib", "ref_nuc", "ref_loop", "ref_wss"):
+    for name in ("ref_setup", "ref_step", "ref_cells", "ref_ib", "ref_nuc", "ref_loop", "ref_wss", "ref_output",
+                 "ref_pressure"):
         a = np.load(os.path.join(root, "tests", "golden", name + ".npz"))
         b = np.load(os.path.join(str(tmp_path), name + ".npz"))
         assert sorted(a.files) == sorted(b.files), name

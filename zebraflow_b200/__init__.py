@@ -140,6 +140,7 @@ _SIGS = {
     "zf_profile_stages": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "zf_save_state": (C.c_int, [_P, C.c_char_p]),
     "zf_lbm_moments": (C.c_int, [_P]),
+    "zf_set_iteration": (C.c_int, [_P, C.c_int64]),
     "zf_get_cell_list_counts": (C.c_int, [_P, _i32p]),
     "zf_load_state": (C.c_int, [_P, C.c_char_p]),
     "zf_wss": (C.c_int, [_P, C.c_void_p, C.c_double, _f32p, C.c_void_p, C.c_void_p]),
@@ -776,6 +777,10 @@ class Context:
         m = C.c_double()
         _check(lib().zf_step_mass(self._h, C.byref(m)))
         return m.value
+
+    def set_iteration(self, it):
+        """Completed iterations; the next step is iteration it + 1."""
+        _check(lib().zf_set_iteration(self._h, int(it)))
 
     def refresh_moments(self):
         """Recomputes the stored D, U, V, W from the current populations."""

@@ -101,7 +101,7 @@ static void free_lattice(zf_ctx* c) {
   void* ptrs[] = {c->d_tile_map, c->d_active, c->d_nbr, c->d_link,
                   c->d_code,     c->d_f[0],   c->d_f[1],  c->d_force,    c->d_mom,
                   c->d_rho_pre,  c->d_dom_slot, c->d_stage, c->d_wall_slot, c->d_wall_nbr,
-                  c->d_red};
+                  c->d_red,      c->d_u_pre};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (auto& pl : c->planes) cudaFree(pl.d_slots);
@@ -110,7 +110,8 @@ static void free_lattice(zf_ctx* c) {
   c->d_link = nullptr;
   c->d_code = nullptr;
   c->d_f[0] = c->d_f[1] = nullptr;
-  c->d_force = c->d_mom = c->d_rho_pre = c->d_stage = nullptr;
+  c->d_force = c->d_mom = c->d_rho_pre = c->d_stage = c->d_u_pre = nullptr;
+  c->n_pressure = 0;
   c->d_dom_slot = c->d_wall_slot = c->d_wall_nbr = nullptr;
   c->d_red = nullptr;
   c->red_cap = 0;
@@ -164,13 +165,21 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
   const zf_params& P = c->p;
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const int64_t npts = (int64_t)nx * ny * nz;
+  int64_t n_pressure = 0;
   for (int64_t n = 0; n < npts; ++n) {
-    if (b[n] >= 10) {
-      set_error("zf_set_lattice: B_index %d at linear index %lld is not supported "
-                "(pressure inlets >= 1000 and the deprecated 4998 are out of scope)",
+    const bool pressure = b[n] >= 1001 && b[n] <= 1009;
+    if (pressure && P.wall_mode != ZF_WALL_REF_EQ) {
+      set_error("zf_set_lattice: pressure inlet/outlet code %d at linear index %lld needs the "
+                "reference wall mode (ZF_WALL_REF_EQ)", b[n], (long long)n);
+      return ZF_ERR_ARG;
+    }
+    if (b[n] >= 10 && !pressure) {
+      set_error("zf_set_lattice: B_index %d at linear index %lld is not supported (codes are <0 "
+                "solid, 0 wall, 1..9 fluid phases, 1001..1009 pressure inlets/outlets)",
                 b[n], (long long)n);
       return ZF_ERR_ARG;
     }
+    n_pressure += pressure;
   }
   ZF_CUDA(cudaStreamSynchronize(c->stream));
   ib_free(c);  // the wall and IB views belong to the previous lattice
@@ -188,7 +197,7 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
           c->domlist.push_back(i);
           c->domlist.push_back(j);
           c->domlist.push_back(k);
-          if (v > 0) c->n_fluid++;
+          if (v > 0 && v < 10) c->n_fluid++;
         }
       }
   c->n_listed = (int64_t)c->domlist.size() / 3;
@@ -205,7 +214,8 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
     int i = c->domlist[3 * l], j = c->domlist[3 * l + 1], k = c->domlist[3 * l + 2];
     int64_t t = ((int64_t)(k / ZF_TS) * nty + j / ZF_TS) * ntx + i / ZF_TS;
     has_listed[t] = 1;
-    if (b[((int64_t)i * ny + j) * nz + k] > 0) has_fluid[t] = 1;
+    const int32_t v = b[((int64_t)i * ny + j) * nz + k];
+    if (v > 0 && v < 10) has_fluid[t] = 1;
   }
   c->h_tile_map.assign(ntiles_box, -1);
   c->h_tile_origin.clear();
@@ -247,7 +257,7 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
     int32_t v = b[((int64_t)i * ny + j) * nz + k];
     int64_t s = slot_of(i, j, k);
     dom_slot[l] = (int32_t)s;
-    code[s] = v > 0 ? (uint8_t)v : (uint8_t)ZF_CODE_WALL;
+    code[s] = v >= 1000 ? (uint8_t)(ZF_CODE_PRESSURE0 + (v - 1000)) : v > 0 ? (uint8_t)v : (uint8_t)ZF_CODE_WALL;
   }
   // Link word of every fluid point: bit 31 marks the point live, bit q that the
   // pull along q bounces back because its upstream point x - e_q is not a
@@ -257,7 +267,8 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
   const bool ref_eq = P.wall_mode == ZF_WALL_REF_EQ;
   for (int64_t l = 0; l < c->n_listed; ++l) {
     int i = c->domlist[3 * l], j = c->domlist[3 * l + 1], k = c->domlist[3 * l + 2];
-    if (b[((int64_t)i * ny + j) * nz + k] <= 0) continue;
+    const int32_t v0 = b[((int64_t)i * ny + j) * nz + k];
+    if (!(v0 > 0 && v0 < 10)) continue;  // collided points only, ZebraflowWT.c:6109
     uint32_t w = 1u << 31;
     for (int q = 0; q < ZF_Q - 1; ++q) {
       int p3[3] = {i - kE[q][0], j - kE[q][1], k - kE[q][2]}, lim[3] = {nx, ny, nz};
@@ -296,8 +307,9 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
         }
   }
 
-  // Designated neighbour of each wall point, reference search order
-  // (fluid first over c=1..18, then wall), ZebraflowWT.c:1534-1578.
+  // Designated neighbour of each wall and pressure point, reference search
+  // order over c=1..18 (a fluid point, else an inlet/outlet point, else a
+  // wall), ZebraflowWT.c:1530-1578.
   std::vector<int32_t> wall_slot, wall_nbr;
   c->status.bc_no_neighbour = 0;
   if (P.wall_mode == ZF_WALL_REF_EQ) {
@@ -316,14 +328,15 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
     };
     for (int64_t l = 0; l < c->n_listed; ++l) {
       int i = c->domlist[3 * l], j = c->domlist[3 * l + 1], k = c->domlist[3 * l + 2];
-      if (b[((int64_t)i * ny + j) * nz + k] != 0) continue;
+      const int32_t self = b[((int64_t)i * ny + j) * nz + k];
+      if (self != 0 && self < 1000) continue;
       int64_t found = -1;
-      for (int pass = 0; pass < 2 && found < 0; ++pass) {
+      for (int pass = 0; pass < 3 && found < 0; ++pass) {
         for (int q = 0; q < ZF_Q - 1; ++q) {
           int ii, jj, kk;
           int32_t v = code_at(i + kE[q][0], j + kE[q][1], k + kE[q][2], &ii, &jj, &kk);
           if (v == INT32_MIN) continue;
-          bool ok = pass == 0 ? (v > 0 && v < 1000) : (v == 0);
+          bool ok = pass == 0 ? (v > 0 && v < 1000) : (pass == 1 ? v > 1000 : v == 0);
           if (ok) {
             found = slot_of(ii, jj, kk);
             break;
@@ -355,6 +368,8 @@ int zf_set_lattice(zf_ctx* c, const int32_t* b) {
   ALLOC(c->d_f[1], (size_t)ZF_Q * ns * esz);
   ALLOC(c->d_force, 3 * ns * sizeof(float));
   ALLOC(c->d_mom, 4 * ns * sizeof(float));
+  c->n_pressure = n_pressure;
+  if (n_pressure > 0) ALLOC(c->d_u_pre, 3 * ns * sizeof(float));
   if (P.wall_mode == ZF_WALL_REF_EQ) {
     ALLOC(c->d_rho_pre, ns * sizeof(float));
     ALLOC(c->d_wall_slot, std::max(c->n_wall, 1) * sizeof(int32_t));

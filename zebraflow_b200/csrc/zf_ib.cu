@@ -174,7 +174,7 @@ __global__ void k_ib_interp(IbArgs a, CellArgs c) {
     const int64_t s = slot_of(a, i, j, wrapk(a, k));
     if (s < 0) return;
     const uint8_t cd = a.code[s];
-    const bool fluid = cd >= 1 && cd <= 9;
+    const bool fluid = zf_code_fluid(cd) || zf_code_pressure(cd);  // 0 < B_index < 4998
     if (!fluid && a.windex[s] <= 0) return;
     float u, v, ww;
     if (fluid) {
@@ -1896,7 +1896,7 @@ __global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
     const int64_t s = slot_of(a, i, j, wrapk(a, k));
     if (s < 0 || s >= a.ns) return;
     const uint8_t cd = a.code[s];
-    if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) return;
+    if (!(zf_code_fluid(cd) || (spread_walls && (cd == ZF_CODE_WALL || zf_code_pressure(cd))))) return;
     for (int v = 0; v < 3; ++v) atomicAdd(&a.force[v * a.ns + s], (float)(w * (double)Ff[v] * a.force_scale));
   });
 }
@@ -1977,7 +1977,7 @@ __global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int 
           const int64_t sl = slot_of(a, i, j, wrapk(a, k));
           if (sl < 0 || sl >= a.ns) continue;
           const uint8_t cd = a.code[sl];
-          if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) continue;
+          if (!(zf_code_fluid(cd) || (spread_walls && (cd == ZF_CODE_WALL || zf_code_pressure(cd))))) continue;
           const int di = i - ox, dj = j - oy;
           int dk = k - oz;
           if (a.per_z) dk = ((dk % a.nz) + a.nz) % a.nz;
@@ -2114,7 +2114,7 @@ __device__ __forceinline__ void wss_stencil(const IbArgs& a, float xm, float ym,
         const int64_t s = slot_of(a, i, j, kk);
         if (s < 0 || s >= a.ns) continue;
         const uint8_t cd = a.code[s];
-        if (!(cd >= 1 && cd <= 9)) continue;  // 0.11 < B_index < 4997
+        if (!(zf_code_fluid(cd) || zf_code_pressure(cd))) continue;  // 0.11 < B_index < 4997
         const float w =
             (float)((1. + cosf((float)(kPId * fabsf(dx) / 2 / a.DX))) *
                     (1. + cosf((float)(kPId * fabsf(dy) / 2 / a.DX))) *
@@ -2368,7 +2368,7 @@ __global__ void k_spread_adj(IbArgs a, CellArgs c, int spread_walls, const float
       const int64_t s = slot_of(a, i, j, wrapk(a, k));
       if (s < 0 || s >= a.ns) return;
       const uint8_t cd = a.code[s];
-      if (!((cd >= 1 && cd <= 9) || (spread_walls && cd == ZF_CODE_WALL))) return;
+      if (!(zf_code_fluid(cd) || (spread_walls && (cd == ZF_CODE_WALL || zf_code_pressure(cd))))) return;
       for (int v = 0; v < 3; ++v) acc[v] += w * G[v * a.ns + s];
     });
   }

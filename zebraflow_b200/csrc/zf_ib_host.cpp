@@ -514,4 +514,10 @@ int zf_iteration(zf_ctx* c, int64_t* iter) {
   return ZF_OK;
 }
 
+int zf_set_iteration(zf_ctx* c, int64_t iter) {
+  if (!c || iter < 0) return ZF_ERR_ARG;
+  c->status.iter = iter;
+  return ZF_OK;
+}
+
 }  // extern "C"

@@ -23,10 +23,17 @@ __host__ __device__ __forceinline__ int64_t pop_at(int q, int64_t s) {
 
 // Cell codes stored per tile slot (uint8).
 enum : uint8_t {
-  ZF_CODE_SOLID = 0,   // not listed (reference B_index < 0)
+  ZF_CODE_SOLID = 0,      // not listed (reference B_index < 0)
   // 1..9: fluid of that phase (reference B_index 1..9)
-  ZF_CODE_WALL = 10    // listed wall point (reference B_index == 0)
+  ZF_CODE_WALL = 10,      // listed wall point (reference B_index == 0)
+  ZF_CODE_PRESSURE0 = 100 // 101..109: pressure inlet/outlet of reference code 1001..1009
 };
+// fluid points (collided), and the points the IB coupling treats as fluid
+// (reference 0 < B_index < 4998: fluid and pressure inlets/outlets)
+__host__ __device__ __forceinline__ bool zf_code_fluid(uint8_t cd) { return cd >= 1 && cd <= 9; }
+__host__ __device__ __forceinline__ bool zf_code_pressure(uint8_t cd) {
+  return cd > ZF_CODE_PRESSURE0 && cd < ZF_CODE_PRESSURE0 + 10;
+}
 
 namespace zf {
 
@@ -67,6 +74,9 @@ struct LbmArgs {
   float* force;               // [3][ns] BODYFORCE (reference units)
   float* mom;                 // [4][ns] D,U,V,W
   float* rho_pre;             // [ns] pre-collision density (wall-equilibrium mode)
+  float* u_pre;               // [3][ns] pre-collision velocity (lattices with pressure points)
+  int64_t iter_now;           // the iteration this step computes (pressure waveforms)
+  double dt_us;               // time step, us (the reference's DT; T_SCALE = DT 1e-6 s)
   int64_t ns;
   float tau;
   float force_dt;             // multiplier of BODYFORCE in the Guo step (reference DT)
@@ -74,7 +84,7 @@ struct LbmArgs {
   float rho_ref, scale, inv_scale;
   double* mass_partial;       // per-block FP64 density sums, or nullptr
   uint32_t step;              // step counter (seeds the stochastic rounding)
-  int store_moments, zero_force, tau_from_phase, write_rho_pre, stochastic;
+  int store_moments, zero_force, tau_from_phase, write_rho_pre, write_u_pre, stochastic;
 };
 
 // Device view of the cells (membrane + nucleus meshes shared by every cell).
@@ -292,6 +302,8 @@ struct zf_ctx {
   float* d_force = nullptr;
   float* d_mom = nullptr;
   float* d_rho_pre = nullptr;
+  float* d_u_pre = nullptr;       // [3][ns], only with pressure points
+  int64_t n_pressure = 0;         // pressure inlet/outlet points (codes 1001..1009)
   int32_t* d_dom_slot = nullptr;  // [n_listed] slot of listed node l
   float* d_stage = nullptr;       // [19*n_listed] upload/download staging
   int32_t* d_wall_slot = nullptr; // REF mode wall points

@@ -348,6 +348,11 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC, 6) k_lbm(LbmArgs a) {
       a.mom[3 * ns + self] = m2z / D;
     }
     if (a.write_rho_pre) a.rho_pre[self] = rho;
+    if (a.write_u_pre) {  // U, V, W of the collision pass, ZebraflowWT.c:6133-6135
+      a.u_pre[self] = ux;
+      a.u_pre[ns + self] = uy;
+      a.u_pre[2 * ns + self] = uz;
+    }
   }
 
   if (a.mass_partial) {  // FP64 block sum of the fluid density (uniform branch)
@@ -365,9 +370,39 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC, 6) k_lbm(LbmArgs a) {
   }
 }
 
-// Reference wall points: F[c][n] = feq(D[m], u=0) with m the designated
-// neighbour (ZebraflowWT.c:6303-6315, :6429-6432), then the moments pass for
-// those points (ZebraflowWT.c:6603-6616).
+// Inlet/outlet pressure (Pa) of reference code 1001..1009 at iteration iter:
+// the reference's cardiac waveforms (ZebraflowWT.c:6318-6418) with its float
+// locals (simtime, cycletime, taucycle, pressure; :2283) and double constants.
+__device__ float inlet_pressure(int code, int64_t iter, double dt_us) {
+  const float simtime = (float)((double)iter * (dt_us * 1.e-06));  // iter*T_SCALE
+  const double T = 0.36;
+  const double lag = code == 1001 ? 0.0 : (code == 1002 ? 0.06 * 0.36 : 0.2 * 0.36);
+  float cycletime = (float)fmod((double)simtime - lag, T);
+  if (code != 1001 && cycletime < 0) cycletime = (float)(cycletime + T);
+  const float taucycle = (float)(cycletime / T);
+  if (code == 1003 || code == 1004 || code == 1005) {
+    const double base = code == 1003 ? 11. : (code == 1004 ? 18. : 23.);
+    const double amp = code == 1003 ? 23. : 27.;
+    if (taucycle <= 0.3) return (float)(120. + base + amp * sinf((float)(3.14159265359 * taucycle / 0.6)));
+    return (float)(120. + base +
+                   amp * (1. + sinf((float)(2 * 3.14159265359 * (taucycle + 0.4) / 1.4 - 3.14159265359 / 2.))) / 2.);
+  }
+  double base = 28.5, amp = 60.;  // 1007, 1009
+  if (code == 1001) base = 54., amp = 82.;
+  else if (code == 1002) base = 48., amp = 68.;
+  else if (code == 1006 || code == 1008) base = 29., amp = 66.;
+  if (taucycle <= 0.23) {
+    const float s1 = sinf((float)(3.14159265359 * taucycle / 0.46));
+    return (float)(120. + base + amp * s1 * s1);
+  }
+  return (float)(120. + base +
+                 amp * (1. + sinf((float)(2 * 3.14159265359 * (taucycle + 0.54) / 1.54 - 3.14159265359 / 2.))) / 2.);
+}
+
+// Reference boundary points (ZebraflowWT.c:6292-6433): a wall point takes
+// F[c][n] = feq(D[m], u=0) and a pressure inlet/outlet feq(P(t)/
+// LBM_PRESSURE_SCALE + 1, u[m]) (LBM_PRESSURE_SCALE = 1e4/3 Pa), m its
+// designated neighbour; then the moments pass for those points (:6603-6616).
 template <class C>
 __global__ void k_lbm_wall(LbmArgs a, const int32_t* __restrict__ wall_slot,
                            const int32_t* __restrict__ wall_nbr, int n_wall) {
@@ -376,27 +411,59 @@ __global__ void k_lbm_wall(LbmArgs a, const int32_t* __restrict__ wall_slot,
   if (w >= n_wall) return;
   const int64_t slot = wall_slot[w];
   const int nb = wall_nbr[w];
-  // D_bc = D[m] of the designated neighbour (ZebraflowWT.c:6306-6311): a fluid
-  // neighbour's density is this step's (k_lbm wrote it); a wall neighbour's is
-  // what the reference's copy pass left in D, the density of its populations
-  // of the previous step, read back from fin
-  float rho_m = a.rho_ref;
-  if (nb >= 0) {
-    if (a.code[nb] == ZF_CODE_WALL) {
-      const T* __restrict__ fin = static_cast<const T*>(a.fin);
-      float r = 0.f;
+  const uint8_t self_code = a.code[slot];
+  const T* __restrict__ fin = static_cast<const T*>(a.fin);
+  // density and momentum of a boundary neighbour as the reference's copy pass
+  // left them in D, U, V, W: the moments of its previous populations
+  auto bc_moments = [&](float& r, float& mx, float& my, float& mz) {
+    r = mx = my = mz = 0.f;
 #pragma unroll
-      for (int q = 0; q < ZF_Q; ++q) r += WQ(q) * C::dec(fin[pop_at(q, (int64_t)nb)], q, a);
-      rho_m = a.rho_ref + r;
-    } else {
+    for (int q = 0; q < ZF_Q; ++q) {
+      const float d = C::dec(fin[pop_at(q, (int64_t)nb)], q, a);
+      r += WQ(q) * d;
+      if (EX(q)) mx += EX(q) * WQ(q) * d;
+      if (EY(q)) my += EY(q) * WQ(q) * d;
+      if (EZ(q)) mz += EZ(q) * WQ(q) * d;
+    }
+    r += a.rho_ref;  // sum w = 1, sum w c = 0
+  };
+  float rho_m = a.rho_ref, ux = 0.f, uy = 0.f, uz = 0.f;
+  if (zf_code_pressure(self_code)) {
+    const float P = inlet_pressure(1000 + (self_code - ZF_CODE_PRESSURE0), a.iter_now, a.dt_us);
+    rho_m = (float)(P / (1. / 3. * 10. * 1000.) + 1.);  // D_bc, ZebraflowWT.c:6421
+    if (nb >= 0) {
+      if (zf_code_fluid(a.code[nb])) {  // U, V, W of this step's collision pass
+        ux = a.u_pre[nb];
+        uy = a.u_pre[a.ns + nb];
+        uz = a.u_pre[2 * a.ns + nb];
+      } else {
+        float r, mx, my, mz;
+        bc_moments(r, mx, my, mz);
+        ux = mx / r;
+        uy = my / r;
+        uz = mz / r;
+      }
+    }
+  } else if (nb >= 0) {
+    // D_bc = D[m] (ZebraflowWT.c:6306-6311): a fluid neighbour's density is this
+    // step's (k_lbm wrote it); a boundary neighbour's is what the reference's
+    // copy pass left in D, the density of its populations of the previous step
+    if (zf_code_fluid(a.code[nb])) {
       rho_m = a.rho_pre[nb];
+    } else {
+      float r, mx, my, mz;
+      bc_moments(r, mx, my, mz);
+      rho_m = r;
     }
   }
   T* __restrict__ fout = static_cast<T*>(a.fout);
+  const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
   float r2 = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
 #pragma unroll
   for (int q = 0; q < ZF_Q; ++q) {
-    const T v = C::enc(rho_m - a.rho_ref, q, a);  // feq(rho, 0)/w - rho_ref
+    const float cu = cdot(q, ux, uy, uz);
+    // feq(rho, u)/w - rho_ref (ZebraflowWT.c:6430)
+    const T v = C::enc(rho_m * (1.f + 3.f * cu + 4.5f * cu * cu - usq15) - a.rho_ref, q, a);
     fout[pop_at(q, slot)] = v;
     const float ds = C::dec(v, q, a);
     r2 += WQ(q) * ds;
@@ -473,7 +540,7 @@ __global__ void k_mass_partial(const typename C::T* __restrict__ f, int64_t ns,
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < ns;
        s += (int64_t)gridDim.x * blockDim.x) {
     const uint8_t cd = code[s];
-    const bool take = (cd >= 1 && cd <= 9) || (include_walls && cd == ZF_CODE_WALL);
+    const bool take = zf_code_fluid(cd) || (include_walls && (cd == ZF_CODE_WALL || zf_code_pressure(cd)));
     if (!take) continue;
     double r = a.rho_ref;
 #pragma unroll
@@ -516,6 +583,10 @@ static LbmArgs make_args(zf_ctx* c) {
   a.force = c->d_force;
   a.mom = c->d_mom;
   a.rho_pre = c->d_rho_pre;
+  a.u_pre = c->d_u_pre;
+  a.write_u_pre = c->n_pressure > 0;
+  a.iter_now = c->status.iter + 1;
+  a.dt_us = P.dt;
   a.ns = c->ns;
   a.tau = P.tau;
   a.force_dt = (float)P.dt;
