@@ -344,7 +344,8 @@ int main(int argc, char** argv) {
   check(zf_set_wall(ctx, nw, wxyz, mt, wtri, wnrm), "zf_set_wall");
 
   /* membrane and nucleus meshes (the reference reads them at :1601-1922) */
-  const int nn = 10 * 256 + 2, nt = 20 * 256, nnn = 10 * 64 + 2, ntn = 20 * 64;
+  /* icosphere levels 3 (membrane) and 2 (nucleus): 10 4^L + 2 nodes, 20 4^L triangles */
+  const int nn = 10 * 64 + 2, nt = 20 * 64, nnn = 10 * 16 + 2, ntn = 20 * 16;
   double* rest = (double*)xmalloc(sizeof(double) * 3 * nn);
   double* rest_n = (double*)xmalloc(sizeof(double) * 3 * nnn);
   int32_t* tri = (int32_t*)xmalloc(sizeof(int32_t) * 3 * nt);
