@@ -31,9 +31,16 @@ pytestmark = pytest.mark.gpu
 DIMS, RP, RD, ANGLE, G = (128, 128, 256), 18.0, 13.0, 20.0, 2e-6
 N_CELLS, SEED = 160, 2024
 CHECKS = (50, 100, 200)
-# relative L2 bounds per checkpoint: u, WSS, displacement
-BOUNDS_DEV = {50: (1e-4, 1e-4, 1e-4), 100: (1e-3, 1e-3, 1e-3), 200: (1e-2, 1e-2, 1e-2)}
-BOUNDS_F32 = {50: (1e-2, 1e-2, 1e-2), 100: (1e-2, 1e-2, 1e-2), 200: (2e-2, 2e-2, 2e-2)}
+# relative L2 bounds per checkpoint: u, WSS, displacement.  Measured on a
+# B200: fp32 deviations against FP64, 8.0e-7 / 7.0e-7 / 1.9e-6 after the
+# first membrane block (iteration 50), 6.5e-5 / 6.3e-5 / 9.3e-5 at 100 and
+# 2.4e-3 / 2.4e-3 / 1.6e-3 at 200; plain fp32 against the fp32 oracle
+# 2.7e-3 / 2.8e-3 / 2.6e-3, 2.9e-4 / 4.2e-4 / 5.1e-4 and 2.7e-3 / 3.0e-3 /
+# 1.6e-3.  The bounds are twice the measured values after the first block,
+# where the two sides differ only in rounding, and three times them later,
+# where the amplification of those differences varies from run to run.
+BOUNDS_DEV = {50: (2e-6, 2e-6, 4e-6), 100: (2e-4, 2e-4, 3e-4), 200: (7e-3, 7e-3, 5e-3)}
+BOUNDS_F32 = {50: (6e-3, 6e-3, 6e-3), 100: (1e-3, 1.3e-3, 1.5e-3), 200: (8e-3, 9e-3, 5e-3)}
 
 
 def rel(a, b):
