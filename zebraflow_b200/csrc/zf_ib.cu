@@ -1287,7 +1287,7 @@ __device__ __forceinline__ int onehot_range(int lo, int hi) {  // bits lo..hi of
   return lo > hi ? 0 : (int)(((2u << hi) - 1u) & ~((1u << lo) - 1u));
 }
 
-__global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs c) {
+__global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs c, float* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char rg_raw[];
   RgShared& S = *reinterpret_cast<RgShared*>(rg_raw);
   const unsigned FULL = 0xffffffffu;
@@ -1530,9 +1530,9 @@ __global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs 
         const int cell = __float_as_int(S.node_n[tid].w);
         if (cell >= 0) {
           const int node = S.node_id[tid];
-          c.wrep[((size_t)0 * nc + cell) * c.nn + node] += S.acc[tid][0];
-          c.wrep[((size_t)1 * nc + cell) * c.nn + node] += S.acc[tid][1];
-          c.wrep[((size_t)2 * nc + cell) * c.nn + node] += S.acc[tid][2];
+          out[((size_t)0 * nc + cell) * c.nn + node] += S.acc[tid][0];
+          out[((size_t)1 * nc + cell) * c.nn + node] += S.acc[tid][1];
+          out[((size_t)2 * nc + cell) * c.nn + node] += S.acc[tid][2];
         }
       }
     }
@@ -1867,7 +1867,7 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_walk(IbArgs a, CellArgs c
 
 // ---- spreading ----------------------------------------------------------------
 
-__global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
+__global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls, int fold) {
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = c.n_cells;
   const int64_t nmem = (int64_t)nc * c.nn;
@@ -1884,8 +1884,14 @@ __global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
   float Ff[3];
   for (int v = 0; v < 3; ++v) {  // :10749-10754
     const size_t g = ((size_t)v * nc + cell) * n + node;
-    V[g] += (double)R[g];
-    Ff[v] = (float)((double)a.gamma_p * (double)R[g] + (double)FT[g]);
+    float r = R[g];
+    if (fold && !nuc) {  // the RBC-RBC increments of an overlapped step, added last
+      r += c.wrep_rr[g];
+      c.wrep[g] = r;
+      c.wrep_rr[g] = 0.f;
+    }
+    V[g] += (double)r;
+    Ff[v] = (float)((double)a.gamma_p * (double)r + (double)FT[g]);
   }
   float xp, yp, zp;
   node_pos(X, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
@@ -1910,7 +1916,7 @@ __global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
 // happen once per node in the first pass.  A contribution outside the
 // neighbourhood (not expected) goes straight to BODYFORCE.
 constexpr int kSpreadNodes = 128;  // nodes staged per pass
-__global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int spread_walls) {
+__global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int spread_walls, int fold) {
   __shared__ float acc[3][1728];
   __shared__ float s_f[3][kSpreadNodes];
   __shared__ StencilAxis s_ax[3][kSpreadNodes];  // per staged node: its stencil along x, y, z
@@ -1944,8 +1950,14 @@ __global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int 
           const float* FT = nuc ? c.ftot_n : c.ftot;
           for (int v = 0; v < 3; ++v) {  // :10749-10754
             const size_t g = ((size_t)v * nc + cell) * n + node;
-            V[g] += (double)R[g];
-            s_f[v][t] = (float)((double)a.gamma_p * (double)R[g] + (double)FT[g]);
+            float r = R[g];
+            if (fold && !nuc) {  // the RBC-RBC increments of an overlapped step, added last
+              r += c.wrep_rr[g];
+              c.wrep[g] = r;
+              c.wrep_rr[g] = 0.f;
+            }
+            V[g] += (double)r;
+            s_f[v][t] = (float)((double)a.gamma_p * (double)r + (double)FT[g]);
           }
           float xp, yp, zp;
           node_pos(nuc ? c.xn : c.x, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
@@ -2531,12 +2543,12 @@ int scale_springs_launch(zf_ctx* ctx, float s) {
   return ZF_OK;
 }
 
-namespace {
-
 // the tile kernels need the 3x3x3 tile neighbourhood of a tile to hold every
 // window point: along a periodic z axis the tiles must wrap with the lattice
 // (nz a multiple of the tile edge) and be at least three
 bool tiles_ok(const IbArgs& a) { return !a.per_z || (a.nz % ZF_TS == 0 && a.ntz >= 3); }
+
+namespace {
 
 template <typename K>
 int persistent_blocks(K kernel, int threads) {
@@ -2676,7 +2688,7 @@ int ib_nuc_memb_launch(zf_ctx* ctx, int rebuild) {
   return ZF_OK;
 }
 
-int ib_rbc_rbc_launch(zf_ctx* ctx) {
+int ib_rbc_rbc_launch(zf_ctx* ctx, float* out, int max_per_sm) {
   const CellArgs& c = ctx->cells;
   IbArgs& a = ctx->ib;
   const int64_t n = (int64_t)c.n_cells * c.nn;
@@ -2697,7 +2709,9 @@ int ib_rbc_rbc_launch(zf_ctx* ctx) {
     ZF_CUDA(cudaGetDevice(&dev));
     ZF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     ZF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rbc_group, kRgThreads, smem));
-    k_rbc_group<<<sms * (per_sm > 0 ? per_sm : 1), kRgThreads, smem, ctx->stream>>>(a, c);
+    if (per_sm < 1) per_sm = 1;
+    if (max_per_sm > 0 && per_sm > max_per_sm) per_sm = max_per_sm;
+    k_rbc_group<<<sms * per_sm, kRgThreads, smem, ctx->stream>>>(a, c, out ? out : c.wrep);
   } else {
     k_rbc_rbc<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
         a, c);
@@ -2707,7 +2721,7 @@ int ib_rbc_rbc_launch(zf_ctx* ctx) {
   return ZF_OK;
 }
 
-int ib_spread_launch(zf_ctx* ctx) {
+int ib_spread_launch(zf_ctx* ctx, int fold) {
   const CellArgs& c = ctx->cells;
   IbArgs& a = ctx->ib;
   const int64_t n = (int64_t)c.n_cells * (c.nn + c.nnn);
@@ -2719,9 +2733,10 @@ int ib_spread_launch(zf_ctx* ctx) {
     }
     ZF_CUDA(cudaMemsetAsync(a.tile_ctr + 3, 0, sizeof(int32_t), ctx->stream));
     k_spread_tiles<<<persistent_blocks(k_spread_tiles, 256), 256, 0, ctx->stream>>>(
-        a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ);
+        a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ, fold);
   } else {
-    k_ib_spread<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ);
+    k_ib_spread<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ,
+                                                                     fold);
   }
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 1;
