@@ -773,10 +773,24 @@ def run_c2(args):
     import zebraflow_b200 as zf
     case = Case(args.workload, args.cells, args.seed)
     n = args.c2_steps
+    every = args.c2_avg_every
+    first = n - every * ((n // 2) // every)  # the time average covers about the second half of the run
     nrm = wall_node_normals(case.wall)
+
+    def sampled(step, wss_now):
+        """Step n iterations; the mean of the WSS taken at iteration `first`
+        and every `every` iterations after it (one sample per output of the
+        post-processor's loop over output iterations)."""
+        step(first)
+        acc, k = wss_now(), 1
+        for _ in range((n - first) // every):
+            step(every)
+            acc, k = acc + wss_now(), k + 1
+        return acc / k, k
+
     t0 = time.perf_counter()
     lbm, oc, w = case.oracle_world("f64")
-    w.step(n)
+    wss_avg_ref, n_samples = sampled(w.step, lambda: w.wss(nrm)[0].astype(np.float64))
     D, U, V, W = lbm.moments()
     wss_ref, _, _ = w.wss(nrm)
     oget = oc.get()
@@ -800,7 +814,7 @@ def run_c2(args):
         ctx.set_wall(*case.wall)
         ctx.set_mesh(*case.mesh)
         ctx.set_cells(*case.cells)
-        ctx.step(n)
+        wss_avg, _ = sampled(ctx.step, lambda: ctx.wss(nrm)[0].astype(np.float64))
         wss, _, _ = ctx.wss(nrm)
         Dg, Ug, Vg, Wg = ctx.download_moments()
         x, _, status = ctx.cells()
@@ -808,6 +822,7 @@ def run_c2(args):
         u = np.stack([Ug, Vg, Wg])[:, fl]
         fields[name] = (u, (Dg - 1.0)[fl], wss, x - x0, live)
         out[name] = {"u": rel(u, u_ref), "rho_minus_1": rel((Dg - 1.0)[fl], rho_ref), "wss": rel(wss, wss_ref),
+                     "wss_time_averaged": rel(wss_avg, wss_avg_ref),
                      "displacement": rel((x - x0)[:, live], (x_ref - x0)[:, live]),
                      "cells_removed": int((status <= 0).sum())}
         ctx.close()
@@ -820,6 +835,7 @@ def run_c2(args):
         vs32[name] = {"u": rel(u, u32), "wss": rel(wv, w32), "displacement": rel(dsp[:, both], d32[:, both])}
     print(json.dumps({"report": "c2_precision_against_fp64_oracle", "workload": case.name,
                       "iterations": n, "membrane_blocks": n // 50, "fp64_oracle_seconds": round(t_oracle, 1),
+                      "wss_time_average": {"first_iteration": first, "every": every, "samples": n_samples},
                       "oracle_cells_removed": int((~live_ref).sum()),
                       "relative_l2_vs_fp64_oracle": out, "relative_l2_vs_fp32_gpu": vs32}), flush=True)
     return 0
@@ -894,6 +910,8 @@ def main():
     ap.add_argument("--c2-steps", type=int, default=0,
                     help="instead of the bench line, a precision report of this many iterations "
                          "against the FP64 oracle")
+    ap.add_argument("--c2-avg-every", type=int, default=50,
+                    help="iterations between the WSS samples of the report's time average")
     ap.add_argument("--sharded", action="store_true",
                     help="instead of the bench line, the LBM step of the lattice split into z slabs "
                          "over the ranks (no cells)")

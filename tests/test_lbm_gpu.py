@@ -174,16 +174,18 @@ def poiseuille_run(storage, steps=3000, stochastic=1):
 
 # (storage, stochastic rounding, bound on the relative L2 velocity error after
 # 3000 steps of Poiseuille flow driven by g = 2e-6, against the fp64 oracle).
-# Bounds follow the CPU emulation of each storage rounding on the fp64 oracle
-# (raw fp32 3.3e-4, fp32 deviation 3.3e-7, fp16 deviation 2.5e-3 with
-# round-to-nearest and 1.3e-4 with stochastic rounding, bf16 deviation 5.7e-2
-# with round-to-nearest), with margin for the fp32 arithmetic of the kernel.
+# The run has no atomics, so it repeats exactly; the bounds are twice what a
+# B200 measured: raw fp32 1.0e-4, fp32 deviation 9.6e-7, fp16 deviation
+# 3.7e-4 with stochastic rounding and 2.7e-3 with round-to-nearest, bf16
+# deviation 1.7e-3 with stochastic rounding.  (The CPU emulation of each
+# storage rounding on the fp64 oracle gives raw fp32 3.3e-4, fp32 deviation
+# 3.3e-7, fp16 1.3e-4 / 2.5e-3, bf16 with round-to-nearest 5.7e-2.)
 STORAGE_BOUNDS = [
-    (zf.STORE_F32, 1, 1e-3),
-    (zf.STORE_F32_DEV, 1, 1e-5),
-    (zf.STORE_F16, 1, 1e-3),
-    (zf.STORE_F16, 0, 5e-3),
-    (zf.STORE_BF16, 1, 5e-2),
+    (zf.STORE_F32, 1, 2.1e-4),
+    (zf.STORE_F32_DEV, 1, 2e-6),
+    (zf.STORE_F16, 1, 7.4e-4),
+    (zf.STORE_F16, 0, 5.4e-3),
+    (zf.STORE_BF16, 1, 3.4e-3),
 ]
 
 

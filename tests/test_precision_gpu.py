@@ -6,23 +6,32 @@ tube's wall mesh, 1000 steps of the reference loop from rest (membrane/IB
 block every 50 steps).  The FP64 CPU oracle (oracle/orc_*.inc) runs the same
 loop; the relative L2 errors of velocity, density (deviation from 1), wall
 shear stress and membrane-node displacement are bounded per storage form.
-BOUNDS holds about 10x what was measured on a B200 (float atomics in the
-spreading make runs differ slightly):
+BOUNDS holds twice the largest value measured on a B200 over repeated runs
+(float atomics in the spreading make runs differ slightly, and with the
+16-bit forms that changes which way some stochastic roundings go):
 
-  storage            u        rho-1    WSS      displacement   (measured)
-  fp32 (plain)       3.2e-4   1.6      4.0e-4   3.5e-4
-  fp32 deviation     8.1e-4   1.1e-2   4.1e-4   5.4e-4
-  fp16 dev. + SR     5.0e-4   9.9e-3   3.6e-4   5.9e-4
-  bf16 dev. + SR     2.1e-3   5.1e-2   1.1e-3   1.1e-3
+  storage            u        rho-1    WSS      displacement  WSS, time-averaged
+  fp32 (plain)       1.2e-3   1.5e-2   6.2e-4   1.3e-3        4.0e-4
+  fp32 deviation     8.1e-4   1.1e-2   4.1e-4   5.4e-4        1.8e-4
+  fp16 dev. + SR     1.7e-3   2.9e-2   9.1e-4   1.4e-3        4.4e-4
+  bf16 dev. + SR     1.7e-3   4.9e-2   8.6e-4   1.2e-3        5.4e-4
+
+The time average is the mean of the WSS at iterations 500, 550, ..., 1000
+(the post-processor's WSS per output file, PostProWSSandPressure.c:319-369,
+averaged over the outputs); fp16 storage must keep it within 1e-3 of the FP64
+oracle's.
 
 At this force the flow is slow (u_max ~ 7.5e-4) and the cells' forcing is a
 comparable signal, so the fp32 arithmetic of the membrane and IB path, not
 the population storage, sets the error of every form; the storage effect
 alone is measured on Poiseuille flow in test_lbm_gpu.py.
 
-Plain fp32 populations cannot resolve the density deviation of this flow
-(rho - 1 is close to the fp32 spacing of populations of ~0.05); the deviation
-forms store f/w - rho_ref and keep it.
+Plain fp32 populations keep the density deviation only to the rounding of
+populations of ~0.05; they are read back as (f - w rho_ref)/w, which adds no
+offset of its own (reading them as f/w - rho_ref adds about 3e-8 per
+population per step, since the weights have no exact fp32 value, and that
+lost rho - 1 altogether: relative error 1.6).  The deviation forms store
+f/w - rho_ref itself.
 """
 import numpy as np
 import pytest
@@ -35,8 +44,11 @@ pytestmark = pytest.mark.gpu
 NX, NY, NZ, R = 48, 48, 128, 20.0
 CX = CY = 23.5
 NSTEPS, STAGGER = 1000, 50
-BOUNDS = {zf.STORE_F32: (3e-3, 5.0, 4e-3, 3.5e-3), zf.STORE_F32_DEV: (8e-3, 0.11, 4e-3, 5e-3),
-          zf.STORE_F16: (5e-3, 0.1, 3.6e-3, 6e-3), zf.STORE_BF16: (2e-2, 0.5, 1.1e-2, 1.1e-2)}
+AVG_FROM, AVG_EVERY = 500, 50  # time average of the WSS over iterations 500, 550, ..., 1000
+BOUNDS = {zf.STORE_F32: (2.4e-3, 3e-2, 1.3e-3, 2.6e-3, 8e-4),
+          zf.STORE_F32_DEV: (1.7e-3, 2.3e-2, 8.1e-4, 1.1e-3, 3.7e-4),
+          zf.STORE_F16: (3.5e-3, 5.9e-2, 1.9e-3, 2.9e-3, 9e-4),
+          zf.STORE_BF16: (3.4e-3, 9.8e-2, 1.8e-3, 2.5e-3, 1.1e-3)}
 
 
 def case():
@@ -62,27 +74,35 @@ def rel(a, b):
     return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
 
 
+def run_sampled(step, wss_now):
+    """Step to NSTEPS, taking the wall shear stress at AVG_FROM and every
+    AVG_EVERY iterations after it; returns the time-averaged WSS."""
+    step(AVG_FROM)
+    acc, n = wss_now(), 1
+    for _ in range((NSTEPS - AVG_FROM) // AVG_EVERY):
+        step(AVG_EVERY)
+        acc = acc + wss_now()
+        n += 1
+    return acc / n
+
+
 @pytest.fixture(scope="module")
 def reference():
     b, mesh, cells, wall = case()
     p = params(zf.STORE_F32)
+    nrm = _node_normals(wall)
     lbm = OracleLBM(b, wall_mode=0, periodic=(0, 0, 1), tau=0.9, g=tuple(p.g), precision="f64")
     oc = OracleCells(*mesh, p, precision="f64")
     oc.set_cells(*cells)
     w = OracleWorld(lbm, oc, p)
     w.set_wall(*wall)
-    w.step(NSTEPS)
-    ctx = zf.Context(p)
-    ctx.set_lattice(b)
-    ctx.set_wall(*wall)
-    nrm = None
+    wss_avg = run_sampled(w.step, lambda: w.wss(nrm)[0].astype(np.float64))
     D, U, V, W = lbm.moments()
-    wss, _, _ = w.wss(_node_normals(wall))
+    wss, _, _ = w.wss(nrm)
     x = oc.get()["x"]
-    ctx.close()
     for o in (w, oc, lbm):
         o.close()
-    return dict(case=(b, mesh, cells, wall), u=np.stack([U, V, W]), rho=D - 1.0, wss=wss,
+    return dict(case=(b, mesh, cells, wall), u=np.stack([U, V, W]), rho=D - 1.0, wss=wss, wss_avg=wss_avg,
                 disp=x - cells[0], nrm=nrm)
 
 
@@ -101,13 +121,14 @@ def _node_normals(wall):
 @pytest.mark.parametrize("storage", [zf.STORE_F32, zf.STORE_F32_DEV, zf.STORE_F16, zf.STORE_BF16])
 def test_coupled_run_against_fp64_oracle(reference, storage):
     b, mesh, cells, wall = reference["case"]
+    nrm = reference["nrm"]
     ctx = zf.Context(params(storage))
     ctx.set_lattice(b)
     ctx.set_wall(*wall)
     ctx.set_mesh(*mesh)
     ctx.set_cells(*cells)
-    ctx.step(NSTEPS)
-    wss, _, _ = ctx.wss(_node_normals(wall))  # also leaves the moments of the final state
+    wss_avg = run_sampled(ctx.step, lambda: ctx.wss(nrm)[0].astype(np.float64))
+    wss, _, _ = ctx.wss(nrm)  # also leaves the moments of the final state
     D, U, V, W = ctx.download_moments()
     x, _, status = ctx.cells()
     assert np.all(status > 0)
@@ -116,8 +137,12 @@ def test_coupled_run_against_fp64_oracle(reference, storage):
     err = (rel(np.stack([U, V, W])[:, fl], reference["u"][:, fl]),
            rel((D - 1.0)[fl], reference["rho"][fl]),
            rel(wss, reference["wss"]),
-           rel(x - cells[0], reference["disp"]))
-    print(f"storage {storage}: u {err[0]:.2e}  rho-1 {err[1]:.2e}  WSS {err[2]:.2e}  disp {err[3]:.2e}")
+           rel(x - cells[0], reference["disp"]),
+           rel(wss_avg, reference["wss_avg"]))
+    print(f"storage {storage}: u {err[0]:.2e}  rho-1 {err[1]:.2e}  WSS {err[2]:.2e}  disp {err[3]:.2e}  "
+          f"time-averaged WSS {err[4]:.2e}")
+    ctx.close()
     for e, bound in zip(err, BOUNDS[storage]):
         assert e <= bound, (storage, err)
-    ctx.close()
+    if storage == zf.STORE_F16:
+        assert err[4] <= 1e-3, err

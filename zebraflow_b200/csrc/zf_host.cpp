@@ -129,12 +129,6 @@ void zf_destroy(zf_ctx* c) {
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
-  if (c->side_stream) {
-    cudaStreamSynchronize(c->side_stream);
-    cudaStreamDestroy(c->side_stream);
-  }
-  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
-  if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }

@@ -400,19 +400,12 @@ __device__ __forceinline__ int64_t bin_key(int64_t s) {
 // within 2 lattice units per axis can lie within 1 um (2 DX), and the first
 // minimum of the reference scan is the first minimum of any sub-scan in the
 // same order that holds every point within 1 um, so the scan covers +-2.
-//
-// Each bin also records its reach: the largest, over its triangles, of the
-// centroid's distance from the bin point plus the triangle's bounding radius
-// (as in k_bin_records), rounded up; reach[ns] holds the largest of all.  No
-// point of a triangle in a bin lies farther than the reach from the bin point.
 __global__ void k_bin_assign(IbArgs a, CellArgs c, int32_t* tri_bin, int32_t* counts) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = c.n_cells;
-  const unsigned live = __ballot_sync(0xffffffffu, g < (int64_t)nc * c.nt);
   if (g >= (int64_t)nc * c.nt) return;
   const int cell = (int)(g / c.nt), t = (int)(g % c.nt);
   tri_bin[g] = -1;
-  unsigned reach_bits = 0;
   if (c.status[cell] > 0) {
     const float xp = c.tri_c[((size_t)0 * nc + cell) * c.nt + t];
     const float yp = c.tri_c[((size_t)1 * nc + cell) * c.nt + t];
@@ -464,22 +457,8 @@ __global__ void k_bin_assign(IbArgs a, CellArgs c, int32_t* tri_bin, int32_t* co
       const int64_t key = bin_key(best);
       tri_bin[g] = (int32_t)key;
       atomicAdd(&counts[key], 1);
-      float r2 = 0.f;
-      for (int v = 0; v < 3; ++v) {
-        const int n = c.tri[3 * t + v];
-        const float dx = (float)c.x[((size_t)0 * nc + cell) * c.nn + n] - xp;
-        const float dy = (float)c.x[((size_t)1 * nc + cell) * c.nn + n] - yp;
-        const float dz = (float)c.x[((size_t)2 * nc + cell) * c.nn + n] - zraw;
-        r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
-      }
-      const float reach = (mindis + sqrtf(r2) * 1.0001f + 1e-3f) * 1.0001f + 1e-3f;
-      reach_bits = __float_as_uint(reach);
-      atomicMax(reinterpret_cast<unsigned*>(&a.bin_reach[key]), reach_bits);
     }
   }
-  const unsigned wmax = __reduce_max_sync(live, reach_bits);
-  if ((threadIdx.x & 31) == __ffs(live) - 1 && wmax)
-    atomicMax(reinterpret_cast<unsigned*>(&a.bin_reach[a.ns]), wmax);
 }
 
 // exclusive scan of counts[0..n) into off[0..n], three passes
@@ -583,69 +562,6 @@ __global__ void k_bin_records(IbArgs a, CellArgs c, const int32_t* total) {
   a.bin_rec[2 * e + 1] = make_float4(c.tri_nrm[((size_t)0 * nc + m) * c.nt + tri],
                            c.tri_nrm[((size_t)1 * nc + m) * c.nt + tri],
                            c.tri_nrm[((size_t)2 * nc + m) * c.nt + tri], __int_as_float(g));
-}
-
-// Normal cone of a bin packed in 32 bits: c = the mean of its triangles'
-// normals quantised to 8 signed bits per component (c' = q/127), and r' >= the
-// largest |n - c'| in units of 1/127 (8 bits, rounded up, the quantisation
-// error of c' included).  A node with normal e1 for which e1.c' > r' |e1| sees
-// e1.n > 0 for every triangle of the bin, so none passes the reference's
-// facing test (e1.n < 0, ZebraflowWT.c:9911-10053).
-__device__ __forceinline__ int cone_pack(float cx, float cy, float cz, float r) {
-  const int qx = __float2int_rn(fminf(fmaxf(cx, -1.f), 1.f) * 127.f);
-  const int qy = __float2int_rn(fminf(fmaxf(cy, -1.f), 1.f) * 127.f);
-  const int qz = __float2int_rn(fminf(fmaxf(cz, -1.f), 1.f) * 127.f);
-  // |c - c'| <= |c - clamp(c)| + sqrt(3) 0.5/127 (clamping moves c towards c')
-  const float dq = sqrtf((cx - qx / 127.f) * (cx - qx / 127.f) + (cy - qy / 127.f) * (cy - qy / 127.f) +
-                         (cz - qz / 127.f) * (cz - qz / 127.f));
-  const int qr = min((int)ceilf((r + dq) * 1.0001f * 127.f + 1e-3f), 255);
-  return (int)((unsigned)(qx & 0xff) | ((unsigned)(qy & 0xff) << 8) | ((unsigned)(qz & 0xff) << 16) |
-               ((unsigned)qr << 24));
-}
-// true when no triangle of the bin can face a node of normal e (|e| = en)
-__device__ __forceinline__ bool cone_excludes(int w, float ex, float ey, float ez, float en) {
-  const float cx = (float)(signed char)(w & 0xff), cy = (float)(signed char)((w >> 8) & 0xff),
-              cz = (float)(signed char)((w >> 16) & 0xff);
-  const float r = (float)((unsigned)w >> 24);
-  // in units of 1/127; the margin covers the rounding of the dot products
-  return ex * cx + ey * cy + ez * cz > (r + 0.0127f) * en;
-}
-
-// One header per bin: first entry, entry count, reach, and the normal cone of
-// its triangles (mean normal c and r = the largest |n - c|, rounded up).
-__global__ void k_bin_headers(IbArgs a) {
-  const int64_t key = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (key >= a.ns) return;
-  const int e0 = a.bin_off[key], e1 = a.bin_off[key + 1];
-  int cone = 0;
-  if (e1 > e0) {
-    float cx = 0.f, cy = 0.f, cz = 0.f;
-    for (int e = e0; e < e1; ++e) {
-      const float4 n = a.bin_rec[2 * e + 1];
-      cx += n.x;
-      cy += n.y;
-      cz += n.z;
-    }
-    const float inv = 1.f / (float)(e1 - e0);
-    cx *= inv;
-    cy *= inv;
-    cz *= inv;
-    float r2 = 0.f;
-    for (int e = e0; e < e1; ++e) {
-      const float4 n = a.bin_rec[2 * e + 1];
-      const float dx = n.x - cx, dy = n.y - cy, dz = n.z - cz;
-      r2 = fmaxf(r2, dx * dx + dy * dy + dz * dz);
-    }
-    cone = cone_pack(cx, cy, cz, sqrtf(r2) * 1.0001f + 1e-6f);
-  }
-  a.bin_hdr[key] = make_int4(e0, e1 - e0, a.bin_reach[key], cone);
-  // occupancy of the tile's 64 bins, bit = key within the tile (ns is a
-  // multiple of 64, so a warp is either wholly inside or wholly past the end)
-  const unsigned occ = __ballot_sync(0xffffffffu, e1 > e0);
-  if ((threadIdx.x & 31) == 0) {
-    unsigned* o = reinterpret_cast<unsigned*>(a.bin_occ);
-    o[key >> 5] = occ;
-  }
 }
 
 // ---- nucleus-membrane repulsion --------------------------------------------
@@ -1026,219 +942,6 @@ __device__ __forceinline__ int neighbour_tile(const IbArgs& a, int tx, int ty, i
   return a.tile_map[((int64_t)Z * a.nty + Y) * a.ntx + X];
 }
 
-// bits lo..hi (clamped to 0..3) of a 4-bit mask
-__device__ __forceinline__ unsigned axis_mask4(int lo, int hi) {
-  lo = max(lo, 0);
-  hi = min(hi, 3);
-  return lo > hi ? 0u : ((2u << hi) - 1u) & ~((1u << lo) - 1u);
-}
-// position of the n-th (0-based) set bit of m (n < popc(m))
-__device__ __forceinline__ int select_bit(unsigned m, int n) {
-  int pos = 0;
-#pragma unroll
-  for (int w = 16; w >= 1; w >>= 1) {
-    const unsigned low = m & ((1u << w) - 1u);
-    const int cnt = __popc(low);
-    if (n >= cnt) {
-      n -= cnt;
-      m >>= w;
-      pos += w;
-    } else {
-      m = low;
-    }
-  }
-  return pos;
-}
-
-// RBC-RBC repulsion (ZebraflowWT.c:9911-10053).  For each node the warp lists
-// the bins of its window that hold triangles (the tiles' occupancy masks cut
-// to the window) and takes them 32 at a time.  Only triangles with a
-// sub-centroid within 1 um of the node contribute, so a bin point farther
-// than 1 um plus its reach (plus a rounding margin) holds none, and a bin
-// whose normal cone lies in the node normal's half-space holds no facing
-// triangle: both are skipped.  The triangles of the remaining bins pass the
-// reference's tests (centroid within 2 um, facing normals, not the node's own
-// triangle) and one whose plane is within 1 um queues up; queued triangles
-// are evaluated 32 at a time, one per lane.  The sum over a node's triangles
-// does not depend on the order they are met in (up to rounding); lane sums
-// meet in a fixed butterfly, so the result is deterministic.
-__global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArgs c) {
-  __shared__ int s_q[kTileWarps][64];
-  const unsigned FULL = 0xffffffffu;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nc = c.n_cells;
-  const int64_t nmem = (int64_t)nc * c.nn;
-  const int64_t n_pop_tiles = a.ns / ZF_TC;
-  const int nlist = a.tile_ctr[0];
-  int* queue = s_q[warp];
-  for (int li = warp_next_tile(&a.tile_ctr[1], lane); li < nlist; li = warp_next_tile(&a.tile_ctr[1], lane)) {
-    const int gt = a.tile_list[li];
-    const int tx = gt % a.ntx, ty = (gt / a.ntx) % a.nty, tz = gt / (a.ntx * a.nty);
-    // lane r < 27: population tile of neighbour r, or -1
-    int rt = -1;
-    if (lane < 27) {
-      int X, Y, Z;
-      const int t = neighbour_tile(a, tx, ty, tz, lane, X, Y, Z);
-      if (t >= 0 && t < n_pop_tiles) rt = t;
-    }
-    if (!__any_sync(FULL, rt >= 0)) continue;
-    const int n0 = a.node_off[gt], n1 = a.node_off[gt + 1];
-    for (int q = n0; q < n1; ++q) {
-      const int64_t gid = a.node_sorted[q];
-      if (gid >= nmem) continue;  // nucleus node: no RBC-RBC term
-      const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
-      if (c.status[cell] <= 0) continue;
-      float xc, yc, zc;
-      node_pos(c.x, nc, c.nn, cell, node, a.LZ, a.Z0, xc, yc, zc);
-      const float e1x = c.node_normal[((size_t)0 * nc + cell) * c.nn + node];
-      const float e1y = c.node_normal[((size_t)1 * nc + cell) * c.nn + node];
-      const float e1z = c.node_normal[((size_t)2 * nc + cell) * c.nn + node];
-      // a bin whose normal cone lies in the node normal's half-space holds no
-      // facing triangle (margin for the rounding of the dot products)
-      const float e1n = sqrtf(e1x * e1x + e1y * e1y + e1z * e1z);
-      const int i0 = lat_index(xc, a.X0, a.DX), j0 = lat_index(yc, a.Y0, a.DX),
-                k0 = lat_index(zc, a.Z0, a.DX);
-      const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
-      const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
-      const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
-      if (i1 > i2 || j1 > j2 || k1 > k2) continue;
-      const int g_own = cell * c.nt;
-      // the window's bins that hold triangles: lane r < 27 intersects the
-      // window with tile r and its occupancy mask (bit 16 x + 4 y + z).  z is
-      // unwrapped around the node: window k and tile origins share one frame.
-      const int kshift = a.per_z ? (((k0 % a.nz) + a.nz) % a.nz) - k0 : 0;
-      unsigned mlo = 0, mhi = 0;
-      if (rt >= 0) {
-        const int ox = (tx + lane % 3 - 1) * 4, oy = (ty + (lane / 3) % 3 - 1) * 4, oz = (tz + lane / 9 - 1) * 4;
-        const unsigned xm = axis_mask4(i1 - ox, i2 - ox), ym = axis_mask4(j1 - oy, j2 - oy),
-                       zm = axis_mask4(k1 + kshift - oz, k2 + kshift - oz);
-        unsigned long long w = 0ull;
-#pragma unroll
-        for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-          for (int jj = 0; jj < 4; ++jj)
-            if (((xm >> ii) & 1u) && ((ym >> jj) & 1u)) w |= (unsigned long long)zm << (16 * ii + 4 * jj);
-        const uint2 occ = a.bin_occ[rt];
-        mlo = occ.x & (unsigned)w;
-        mhi = occ.y & (unsigned)(w >> 32);
-      }
-      const int nbin = __popc(mlo) + __popc(mhi);
-      int bincl = nbin;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(FULL, bincl, o);
-        if (lane >= o) bincl += v;
-      }
-      const int nbins = __shfl_sync(FULL, bincl, 31);
-      const int bbase = bincl - nbin;  // this tile lane's first candidate
-      float rx = 0.f, ry = 0.f, rz = 0.f;
-      int qn = 0;
-      auto flush = [&](int nb) {
-        __syncwarp();
-        if (lane < nb) {
-          const int e = queue[lane];
-          float tx2, ty2, tz2;
-          rbc_entry(a, c, e, a.bin_rec[2 * e], xc, yc, zc, tx2, ty2, tz2);
-          rx += tx2;
-          ry += ty2;
-          rz += tz2;
-        }
-        const int rem = qn - nb;
-        const int tq = lane < rem ? queue[nb + lane] : 0;
-        __syncwarp();
-        if (lane < rem) queue[lane] = tq;
-        __syncwarp();
-        qn = rem;
-      };
-      const float X0f = (float)a.X0, Y0f = (float)a.Y0, Z0f = (float)a.Z0, DXf = (float)a.DX;
-      for (int p0 = 0; p0 < nbins; p0 += 32) {
-        // candidate p0 + lane: its tile lane r and the bin's bit in that tile
-        const int gb = p0 + lane;
-        int r = 0;
-#pragma unroll
-        for (int stp = 16; stp > 0; stp >>= 1) {
-          const int v = __shfl_sync(FULL, bbase, r + stp);
-          if (r + stp < 27 && gb >= v) r += stp;
-        }
-        const unsigned lo = __shfl_sync(FULL, mlo, r), hi = __shfl_sync(FULL, mhi, r);
-        const int t = __shfl_sync(FULL, rt, r);
-        const int nth = gb - __shfl_sync(FULL, bbase, r);
-        int e0 = 0, len = 0;
-        if (gb < nbins) {
-          const int nlo = __popc(lo);
-          const int b = nth < nlo ? select_bit(lo, nth) : 32 + select_bit(hi, nth - nlo);
-          const int ii = b >> 4, jj = (b >> 2) & 3, kk = b & 3;
-          const int i = (tx + r % 3 - 1) * 4 + ii, j = (ty + (r / 3) % 3 - 1) * 4 + jj,
-                    k = (tz + r / 9 - 1) * 4 + kk - kshift;  // unwrapped around the node
-          const float ddx = (X0f + i * DXf) - xc, ddy = (Y0f + j * DXf) - yc, ddz = (Z0f + k * DXf) - zc;
-          const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-          const int4 h = a.bin_hdr[(int64_t)t * ZF_TC + b];
-          const float rr = __int_as_float(h.z) + 1.f + 1e-3f;
-          if (d2 <= rr * rr && !cone_excludes(h.w, e1x, e1y, e1z, e1n)) {
-            e0 = h.x;
-            len = h.y;
-          }
-        }
-        // the triangles of the remaining bins as one sequence over the lanes
-        int incl = len;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int v = __shfl_up_sync(FULL, incl, o);
-          if (lane >= o) incl += v;
-        }
-        const int total = __shfl_sync(FULL, incl, 31);
-        const int base = incl - len;  // this lane's first position
-        for (int g0 = 0; g0 < total; g0 += 32) {
-          const int gpos = g0 + lane;
-          // source lane: the last lane whose first position is <= gpos
-          int src = 0;
-#pragma unroll
-          for (int stp = 16; stp > 0; stp >>= 1) {
-            const int v = __shfl_sync(FULL, base, src + stp);
-            if (src + stp < 32 && gpos >= v && v < total) src += stp;
-          }
-          const int e = __shfl_sync(FULL, e0, src) + (gpos - __shfl_sync(FULL, base, src));
-          bool pass = false;
-          if (gpos < total) {
-            const float4 cr = a.bin_rec[2 * e], nr = a.bin_rec[2 * e + 1];
-            const float dzc = wrapd(cr.z - zc, a.LZ);
-            const float dcen = dist3(xc - cr.x, yc - cr.y, -dzc);
-            if (dcen < 2.f && !(dcen - rec_rb(cr.w) > 1.f) && e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f) {
-              // the 16 sub-centroids lie in the triangle's plane, within 3/4 of
-              // the bounding radius of the centroid (the farthest, at
-              // barycentric (10,1,1)/12, is half a median away): none is within
-              // 1 um unless the node's distance to that disk is (margin for the
-              // float rounding of the sub-centroids)
-              const float pd = (cr.x - xc) * nr.x + (cr.y - yc) * nr.y + dzc * nr.z;
-              const float qd = fmaxf(sqrtf(fmaxf(dcen * dcen - pd * pd, 0.f)) - 0.75f * rec_rb(cr.w), 0.f);
-              const int tri = __float_as_int(nr.w) - g_own;  // not the node's own triangle
-              pass = pd * pd + qd * qd <= 1.004f &&
-                     !((unsigned)tri < (unsigned)c.nt &&
-                       (c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node));
-            }
-          }
-          const unsigned bal = __ballot_sync(FULL, pass);
-          if (pass) queue[qn + __popc(bal & ((1u << lane) - 1u))] = e;
-          qn += __popc(bal);
-          if (qn >= 32) flush(32);
-        }
-      }
-      while (qn > 0) flush(min(qn, 32));
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        rx += __shfl_xor_sync(FULL, rx, o);
-        ry += __shfl_xor_sync(FULL, ry, o);
-        rz += __shfl_xor_sync(FULL, rz, o);
-      }
-      if (lane == 0) {
-        c.wrep[((size_t)0 * nc + cell) * c.nn + node] += rx;
-        c.wrep[((size_t)1 * nc + cell) * c.nn + node] += ry;
-        c.wrep[((size_t)2 * nc + cell) * c.nn + node] += rz;
-      }
-    }
-  }
-}
-
 // RBC-RBC repulsion (ZebraflowWT.c:9911-10053), one block per lattice tile of
 // nodes.  The block stages up to kRgNodes membrane nodes of the tile, takes
 // their bounding box, and walks the bin entries of the 27 tiles around it (the
@@ -1250,7 +953,8 @@ __global__ void __launch_bounds__(kTileThreads, 5) k_rbc_tiles(IbArgs a, CellArg
 // them.  Each warp then takes nodes one at a time and its lanes test the kept
 // triangles against the node with the reference's conditions (bin inside the
 // node's window, centroid within 2 um, facing normals, not one of the node's
-// own triangles) and the disk bound of k_rbc_tiles; survivors queue up and are
+// own triangles) and a disk bound (the 16 sub-centroids lie within 3/4 of the bounding radius
+// of the centroid, in the triangle's plane); survivors queue up and are
 // evaluated 32 at a time, one per lane (the 16 sub-centroids).  Each node's
 // contributions are met in the same order whatever else the block holds, and
 // lane sums meet in a fixed butterfly.
@@ -1278,7 +982,7 @@ struct RgShared {
   int rrel[27];             // tile offset in the 12^3 block: x | y << 8 | z << 16 (in units of 4 points)
   float bb[6];              // node box: min x, y, z, max x, y, z
   int wsum[kRgWarps];
-  int li, ncand, nn;
+  int li, ncand, nn, node_next;
 };
 
 __device__ __forceinline__ int onehot_range(int lo, int hi) {  // bits lo..hi of 12, clamped
@@ -1287,7 +991,7 @@ __device__ __forceinline__ int onehot_range(int lo, int hi) {  // bits lo..hi of
   return lo > hi ? 0 : (int)(((2u << hi) - 1u) & ~((1u << lo) - 1u));
 }
 
-__global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs c, float* __restrict__ out) {
+__global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs c) {
   extern __shared__ __align__(16) unsigned char rg_raw[];
   RgShared& S = *reinterpret_cast<RgShared*>(rg_raw);
   const unsigned FULL = 0xffffffffu;
@@ -1400,10 +1104,16 @@ __global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs 
 
       // the kept triangles, tested against the staged nodes
       auto process = [&]() {
+        if (tid == 0) S.node_next = 0;
         __syncthreads();
         const int ncand = S.ncand;
         int* queue = S.q[warp];
-        for (int t = warp; t < cnt; t += kRgWarps) {
+        // nodes go to the warps as they free up (their costs differ widely)
+        for (;;) {
+          int t = 0;
+          if (lane == 0) t = atomicAdd(&S.node_next, 1);
+          t = __shfl_sync(FULL, t, 0);
+          if (t >= cnt) break;
           const float4 np = S.node_p[t], nn4 = S.node_n[t];
           const int cell = __float_as_int(nn4.w);
           if (cell < 0) continue;
@@ -1530,9 +1240,9 @@ __global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs 
         const int cell = __float_as_int(S.node_n[tid].w);
         if (cell >= 0) {
           const int node = S.node_id[tid];
-          out[((size_t)0 * nc + cell) * c.nn + node] += S.acc[tid][0];
-          out[((size_t)1 * nc + cell) * c.nn + node] += S.acc[tid][1];
-          out[((size_t)2 * nc + cell) * c.nn + node] += S.acc[tid][2];
+          c.wrep[((size_t)0 * nc + cell) * c.nn + node] += S.acc[tid][0];
+          c.wrep[((size_t)1 * nc + cell) * c.nn + node] += S.acc[tid][1];
+          c.wrep[((size_t)2 * nc + cell) * c.nn + node] += S.acc[tid][2];
         }
       }
     }
@@ -1669,14 +1379,15 @@ __device__ __forceinline__ void wall_repel(const IbArgs& a, const CellArgs& c, i
 }
 
 // Nearest wall triangle and wall repulsion (as k_ib_wall), first pass: one
-// thread per node.  Where the node's lattice point has its wall-node lists
-// (k_wall_rel), the thread scans them in order with the reference's running
-// minimum (strict <, starting at 1.5 um); no list means no triangle.  Nodes
-// whose point has no lists (too many, or outside the IB view) are queued for
-// k_wall_walk.
-__global__ void k_wall_nodes(IbArgs a, CellArgs c, int32_t* __restrict__ walk, int32_t* __restrict__ walk_n) {
+// thread per node.  A node whose lattice point has wall-node lists
+// (k_wall_rel) is queued at the back of `walk` for k_wall_lists; no list means
+// no triangle.  Nodes whose point has no lists (too many, or outside the IB
+// view) are queued at the front for k_wall_walk.  ctr: [0] front count,
+// [2] back count.
+__global__ void k_wall_nodes(IbArgs a, CellArgs c, int32_t* __restrict__ walk, int32_t* __restrict__ ctr) {
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= (int64_t)c.n_cells * (c.nn + c.nnn)) return;
+  const int64_t ntot = (int64_t)c.n_cells * (c.nn + c.nnn);
+  if (gid >= ntot) return;
   bool nuc;
   int cell, node;
   if (!node_of(c, gid, nuc, cell, node)) return;
@@ -1696,15 +1407,62 @@ __global__ void k_wall_nodes(IbArgs a, CellArgs c, int32_t* __restrict__ walk, i
       if (s0 >= 0) rel = a.wrel_cnt[s0];
     }
   }
-  if (rel < 0) {
-    walk[atomicAdd(walk_n, 1)] = (int32_t)gid;
-    return;
+  if (rel < 0) walk[atomicAdd(&ctr[0], 1)] = (int32_t)gid;
+  else if (rel > 0) walk[ntot - 1 - atomicAdd(&ctr[2], 1)] = (int32_t)gid;
+}
+
+// The queued nodes with wall-node lists, a warp per node: the lanes take each
+// list's candidates 32 at a time in list order, each lane keeping its first
+// strict minimum below 1.5 um and that candidate's position in the node's
+// scan; the warp then takes the smallest distance, ties to the earliest
+// position -- the first candidate in scan order that reaches the minimum,
+// which is what the reference's running minimum (strict <) ends on.
+__global__ void __launch_bounds__(kTileThreads) k_wall_lists(IbArgs a, CellArgs c, const int32_t* __restrict__ walk,
+                                                            const int32_t* __restrict__ ctr, int32_t* __restrict__ work) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t ntot = (int64_t)c.n_cells * (c.nn + c.nnn);
+  const int nq = ctr[2];
+  for (int li = warp_next_tile(work, lane); li < nq; li = warp_next_tile(work, lane)) {
+    const int64_t gid = walk[ntot - 1 - li];
+    bool nuc;
+    int cell, node;
+    node_of(c, gid, nuc, cell, node);
+    const int n = nuc ? c.nnn : c.nn;
+    float xp, yp, zp;
+    node_pos(nuc ? c.xn : c.x, c.n_cells, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
+    const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX), k0 = lat_index(zp, a.Z0, a.DX);
+    const int64_t s0 = slot_of(a, i0, j0, wrapk(a, k0));
+    const int rel = a.wrel_cnt[s0];
+    const int32_t* lists = a.wrel + a.wrel_off[s0];
+    float best = 1.5f;
+    int bpos = INT_MAX, tbest = -1, pos = 0;
+    for (int r = 0; r < rel; ++r) {
+      const int m = lists[r];
+      const int32_t c0 = a.wcand_off[m - 1], c1 = a.wcand_off[m];
+      for (int i = c0 + lane; i < c1; i += 32) {
+        const float4 p = a.wcand[i];
+        const float d = dist3(xp - p.x, yp - p.y, wrapd(zp - p.z, a.LZ));
+        if (d < best) {
+          best = d;
+          bpos = pos + (i - c0);
+          tbest = __float_as_int(p.w);
+        }
+      }
+      pos += c1 - c0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ob = __shfl_xor_sync(FULL, best, o);
+      const int op = __shfl_xor_sync(FULL, bpos, o), ot = __shfl_xor_sync(FULL, tbest, o);
+      if (ob < best || (ob == best && op < bpos)) {
+        best = ob;
+        bpos = op;
+        tbest = ot;
+      }
+    }
+    if (lane == 0 && tbest >= 0) wall_repel(a, c, cell, node, xp, yp, zp, tbest);
   }
-  float mindis = 1.5f;
-  int triwall = -1;
-  const int32_t* lists = a.wrel + a.wrel_off[s0];
-  for (int r = 0; r < rel; ++r) wall_list_min(a, lists[r], xp, yp, zp, mindis, triwall);
-  if (triwall >= 0) wall_repel(a, c, cell, node, xp, yp, zp, triwall);
 }
 
 // Second pass for the queued nodes: a warp per node walks its window 32
@@ -1867,7 +1625,7 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_walk(IbArgs a, CellArgs c
 
 // ---- spreading ----------------------------------------------------------------
 
-__global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls, int fold) {
+__global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int nc = c.n_cells;
   const int64_t nmem = (int64_t)nc * c.nn;
@@ -1884,14 +1642,8 @@ __global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls, int fold) {
   float Ff[3];
   for (int v = 0; v < 3; ++v) {  // :10749-10754
     const size_t g = ((size_t)v * nc + cell) * n + node;
-    float r = R[g];
-    if (fold && !nuc) {  // the RBC-RBC increments of an overlapped step, added last
-      r += c.wrep_rr[g];
-      c.wrep[g] = r;
-      c.wrep_rr[g] = 0.f;
-    }
-    V[g] += (double)r;
-    Ff[v] = (float)((double)a.gamma_p * (double)r + (double)FT[g]);
+    V[g] += (double)R[g];
+    Ff[v] = (float)((double)a.gamma_p * (double)R[g] + (double)FT[g]);
   }
   float xp, yp, zp;
   node_pos(X, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
@@ -1916,7 +1668,7 @@ __global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls, int fold) {
 // happen once per node in the first pass.  A contribution outside the
 // neighbourhood (not expected) goes straight to BODYFORCE.
 constexpr int kSpreadNodes = 128;  // nodes staged per pass
-__global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int spread_walls, int fold) {
+__global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int spread_walls) {
   __shared__ float acc[3][1728];
   __shared__ float s_f[3][kSpreadNodes];
   __shared__ StencilAxis s_ax[3][kSpreadNodes];  // per staged node: its stencil along x, y, z
@@ -1950,14 +1702,8 @@ __global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int 
           const float* FT = nuc ? c.ftot_n : c.ftot;
           for (int v = 0; v < 3; ++v) {  // :10749-10754
             const size_t g = ((size_t)v * nc + cell) * n + node;
-            float r = R[g];
-            if (fold && !nuc) {  // the RBC-RBC increments of an overlapped step, added last
-              r += c.wrep_rr[g];
-              c.wrep[g] = r;
-              c.wrep_rr[g] = 0.f;
-            }
-            V[g] += (double)r;
-            s_f[v][t] = (float)((double)a.gamma_p * (double)r + (double)FT[g]);
+            V[g] += (double)R[g];
+            s_f[v][t] = (float)((double)a.gamma_p * (double)R[g] + (double)FT[g]);
           }
           float xp, yp, zp;
           node_pos(nuc ? c.xn : c.x, nc, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
@@ -2543,12 +2289,12 @@ int scale_springs_launch(zf_ctx* ctx, float s) {
   return ZF_OK;
 }
 
+namespace {
+
 // the tile kernels need the 3x3x3 tile neighbourhood of a tile to hold every
 // window point: along a periodic z axis the tiles must wrap with the lattice
 // (nz a multiple of the tile edge) and be at least three
 bool tiles_ok(const IbArgs& a) { return !a.per_z || (a.nz % ZF_TS == 0 && a.ntz >= 3); }
-
-namespace {
 
 template <typename K>
 int persistent_blocks(K kernel, int threads) {
@@ -2637,11 +2383,13 @@ int ib_interp_launch(zf_ctx* ctx) {
   if (a.nw > 0) {
     if (tiles_ok(a)) {
       // [0] queued nodes, [1] their work counter
-      ZF_CUDA(cudaMemsetAsync(a.wall_walk_ctr, 0, 2 * sizeof(int32_t), ctx->stream));
+      ZF_CUDA(cudaMemsetAsync(a.wall_walk_ctr, 0, 4 * sizeof(int32_t), ctx->stream));
       k_wall_nodes<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(a, c, a.wall_walk, a.wall_walk_ctr);
+      k_wall_lists<<<persistent_blocks(k_wall_lists, kTileThreads), kTileThreads, 0, ctx->stream>>>(
+          a, c, a.wall_walk, a.wall_walk_ctr, a.wall_walk_ctr + 3);
       k_wall_walk<<<persistent_blocks(k_wall_walk, kTileThreads), kTileThreads, 0, ctx->stream>>>(
           a, c, a.wall_walk, a.wall_walk_ctr, a.wall_walk_ctr + 1);
-      ctx->launches += 1;
+      ctx->launches += 2;
     } else {
       k_ib_wall<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
           a, c);
@@ -2662,7 +2410,6 @@ int ib_bins_launch(zf_ctx* ctx) {
   int32_t* bsum = tri_bin + ntri;
   int32_t* off = const_cast<int32_t*>(a.bin_off);
   ZF_CUDA(cudaMemsetAsync(counts, 0, (a.ns + 1) * sizeof(int32_t), ctx->stream));
-  ZF_CUDA(cudaMemsetAsync(a.bin_reach, 0, (a.ns + 1) * sizeof(int32_t), ctx->stream));
   k_bin_assign<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(a, c, tri_bin, counts);
   scan_launch(counts, a.ns + 1, off, bsum, ctx->stream);
   ZF_CUDA(cudaMemsetAsync(counts, 0, (a.ns + 1) * sizeof(int32_t), ctx->stream));
@@ -2671,9 +2418,8 @@ int ib_bins_launch(zf_ctx* ctx) {
   k_bin_sort<<<(unsigned)((a.ns + 255) / 256), 256, 0, ctx->stream>>>(off, a.ns,
                                                                        const_cast<int32_t*>(a.bin_tri));
   k_bin_records<<<(unsigned)((ntri + 255) / 256), 256, 0, ctx->stream>>>(a, c, off + a.ns);
-  k_bin_headers<<<(unsigned)((a.ns + 255) / 256), 256, 0, ctx->stream>>>(a);
   ZF_CUDA(cudaGetLastError());
-  ctx->launches += 8;
+  ctx->launches += 7;
   return ZF_OK;
 }
 
@@ -2688,7 +2434,7 @@ int ib_nuc_memb_launch(zf_ctx* ctx, int rebuild) {
   return ZF_OK;
 }
 
-int ib_rbc_rbc_launch(zf_ctx* ctx, float* out, int max_per_sm) {
+int ib_rbc_rbc_launch(zf_ctx* ctx) {
   const CellArgs& c = ctx->cells;
   IbArgs& a = ctx->ib;
   const int64_t n = (int64_t)c.n_cells * c.nn;
@@ -2709,9 +2455,7 @@ int ib_rbc_rbc_launch(zf_ctx* ctx, float* out, int max_per_sm) {
     ZF_CUDA(cudaGetDevice(&dev));
     ZF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     ZF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rbc_group, kRgThreads, smem));
-    if (per_sm < 1) per_sm = 1;
-    if (max_per_sm > 0 && per_sm > max_per_sm) per_sm = max_per_sm;
-    k_rbc_group<<<sms * per_sm, kRgThreads, smem, ctx->stream>>>(a, c, out ? out : c.wrep);
+    k_rbc_group<<<sms * (per_sm > 0 ? per_sm : 1), kRgThreads, smem, ctx->stream>>>(a, c);
   } else {
     k_rbc_rbc<<<(unsigned)((n + kRepWarps * 32 - 1) / (kRepWarps * 32)), kRepWarps * 32, 0, ctx->stream>>>(
         a, c);
@@ -2721,7 +2465,7 @@ int ib_rbc_rbc_launch(zf_ctx* ctx, float* out, int max_per_sm) {
   return ZF_OK;
 }
 
-int ib_spread_launch(zf_ctx* ctx, int fold) {
+int ib_spread_launch(zf_ctx* ctx) {
   const CellArgs& c = ctx->cells;
   IbArgs& a = ctx->ib;
   const int64_t n = (int64_t)c.n_cells * (c.nn + c.nnn);
@@ -2733,10 +2477,9 @@ int ib_spread_launch(zf_ctx* ctx, int fold) {
     }
     ZF_CUDA(cudaMemsetAsync(a.tile_ctr + 3, 0, sizeof(int32_t), ctx->stream));
     k_spread_tiles<<<persistent_blocks(k_spread_tiles, 256), 256, 0, ctx->stream>>>(
-        a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ, fold);
+        a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ);
   } else {
-    k_ib_spread<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ,
-                                                                     fold);
+    k_ib_spread<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ);
   }
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 1;

@@ -160,9 +160,6 @@ int ib_buffers(zf_ctx* c) {
   if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_rec, 2 * ntri))) return rc;
   if ((rc = dalloc<float4>(c, c->ib_allocs, &a.bin_v, 3 * ntri))) return rc;
   if ((rc = dalloc<uint8_t>(c, c->ib_allocs, &a.bin_kk, ntri))) return rc;
-  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.bin_reach, nscan))) return rc;
-  if ((rc = dalloc<int4>(c, c->ib_allocs, &a.bin_hdr, nscan))) return rc;
-  if ((rc = dalloc<uint2>(c, c->ib_allocs, &a.bin_occ, (c->ns + ZF_TC - 1) / ZF_TC))) return rc;
   // node-tile lists
   const int64_t nnodes = (int64_t)cl.n_cells * (cl.nn + cl.nnn);
   a.ngrid = (int64_t)c->ntx * c->nty * c->ntz;
@@ -172,7 +169,7 @@ int ib_buffers(zf_ctx* c) {
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.node_off, ng1))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.node_sorted, nnodes))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.wall_walk, nnodes))) return rc;
-  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.wall_walk_ctr, 2))) return rc;
+  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.wall_walk_ctr, 4))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.tile_list, std::min(a.ngrid, nnodes)))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.tile_ctr, 4))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.node_bsum, (ng1 + 1023) / 1024 + 1))) return rc;
@@ -383,10 +380,8 @@ static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
     const bool last = s == nsteps - 1;
     int rc;
     if (membrane && (rc = close_run())) return rc;
-    // on profiled membrane iterations events bracket the stages: 0 forces 1
-    // LBM 2 interpolation 3 nucleus 4 (join) 6 spreading 7 update 8 on the
-    // context's stream, and 9 cell list 10 RBC-RBC 11 on whichever stream
-    // runs those two
+    // on profiled membrane iterations an event precedes each stage and one
+    // follows the last: [forces][LBM][interp][nucleus][bins][RBC-RBC][spread][update]
     const bool pm = c->profiling && membrane && c->prof_mem < c->prof_cap;
     auto mark = [&](int k) -> int {
       if (pm) ZF_CUDA(cudaEventRecord(c->prof_ev[2 * (size_t)c->prof_cap + ZF_PROF_MARKS * (size_t)c->prof_mem + k],
@@ -394,40 +389,7 @@ static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
       return ZF_OK;
     };
     if ((rc = mark(0))) return rc;
-    // The cell list and the RBC-RBC search need only the geometry of the
-    // membrane-force stage, so they run on a second stream beside the LBM
-    // step, the IB interpolation with wall repulsion and the nucleus-membrane
-    // repulsion; their increments go to wrep_rr, which the spreading adds to
-    // NODE_WALLREPUL last, as the reference's order (:9911-10053 after
-    // :8694-9730) does.
-    bool overlap = false;
-    if (membrane) {
-      if ((rc = cells_membrane_launch(c))) return rc;
-      overlap = tiles_ok(c->ib) && !c->ib_allocs.empty();
-      if (overlap) {
-        if (!c->node_tiles_valid && (rc = ib_node_tiles_launch(c))) return rc;
-        if (!c->side_stream) {
-          ZF_CUDA(cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
-          ZF_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
-          ZF_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
-        }
-        ZF_CUDA(cudaEventRecord(c->ev_fork, c->stream));
-        ZF_CUDA(cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
-        const cudaStream_t main_stream = c->stream;
-        c->stream = c->side_stream;
-        auto side = [&]() -> int {
-          int r;
-          if ((r = mark(9)) || (r = ib_bins_launch(c)) || (r = mark(10))) return r;
-          // two resident blocks per SM leave room for the other stream's kernels
-          if ((r = ib_rbc_rbc_launch(c, c->cells.wrep_rr, 2)) || (r = mark(11))) return r;
-          ZF_CUDA(cudaEventRecord(c->ev_join, c->stream));
-          return ZF_OK;
-        };
-        rc = side();
-        c->stream = main_stream;
-        if (rc) return rc;
-      }
-    }
+    if (membrane && (rc = cells_membrane_launch(c))) return rc;
     if ((rc = mark(1))) return rc;
     if (!membrane && c->profiling && !c->prof_open && c->prof_lbm < c->prof_cap) {
       ZF_CUDA(cudaEventRecord(c->prof_ev[2 * c->prof_lbm], c->stream));
@@ -442,14 +404,9 @@ static int step_impl(zf_ctx* c, int nsteps, double* mass_last) {
       if ((rc = mark(2)) || (rc = ib_interp_launch(c))) return rc;
       if ((rc = mark(3)) || (rc = ib_nuc_memb_launch(c, rebuild))) return rc;
       c->nuc_lists_valid = true;
-      if ((rc = mark(4))) return rc;
-      if (overlap) {
-        ZF_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
-      } else {
-        if ((rc = mark(9)) || (rc = ib_bins_launch(c))) return rc;
-        if ((rc = mark(10)) || (rc = ib_rbc_rbc_launch(c)) || (rc = mark(11))) return rc;
-      }
-      if ((rc = mark(6)) || (rc = ib_spread_launch(c, overlap))) return rc;
+      if ((rc = mark(4)) || (rc = ib_bins_launch(c))) return rc;
+      if ((rc = mark(5)) || (rc = ib_rbc_rbc_launch(c))) return rc;
+      if ((rc = mark(6)) || (rc = ib_spread_launch(c))) return rc;
       if ((rc = mark(7)) || (rc = ib_update_launch(c))) return rc;
       if ((rc = mark(8))) return rc;
       if (pm) c->prof_mem++;
@@ -490,25 +447,16 @@ int zf_profile(zf_ctx* c, int enable, int capacity) {
   return ZF_OK;
 }
 
-// Summed device time (ms) of each stage of the profiled membrane iterations
-// (the cell list and RBC-RBC search may overlap the stages after the
-// forces), and of the whole membrane iterations.
-static int stage_times(zf_ctx* c, float* st, float* span) {
+// Summed device time (ms) of each stage of the profiled membrane iterations.
+static int stage_times(zf_ctx* c, float* st) {
   for (int k = 0; k < ZF_PROF_STAGES; ++k) st[k] = 0.f;
-  *span = 0.f;
   for (int i = 0; i < c->prof_mem; ++i) {
     const size_t b = 2 * (size_t)c->prof_cap + ZF_PROF_MARKS * (size_t)i;
-    auto el = [&](int from, int to, float& acc) -> int {
+    for (int k = 0; k < ZF_PROF_STAGES; ++k) {
       float ms = 0.f;
-      ZF_CUDA(cudaEventElapsedTime(&ms, c->prof_ev[b + from], c->prof_ev[b + to]));
-      acc += ms;
-      return ZF_OK;
-    };
-    static const int pairs[ZF_PROF_STAGES][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {9, 10}, {10, 11}, {6, 7}, {7, 8}};
-    int rc;
-    for (int k = 0; k < ZF_PROF_STAGES; ++k)
-      if ((rc = el(pairs[k][0], pairs[k][1], st[k]))) return rc;
-    if ((rc = el(0, 8, *span))) return rc;
+      ZF_CUDA(cudaEventElapsedTime(&ms, c->prof_ev[b + k], c->prof_ev[b + k + 1]));
+      st[k] += ms;
+    }
   }
   return ZF_OK;
 }
@@ -524,13 +472,15 @@ int zf_profile_read(zf_ctx* c, float* lbm_ms, int* lbm_count, float* membrane_ms
     ZF_CUDA(cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]));
     tl += ms;
   }
-  float st[ZF_PROF_STAGES], span = 0.f;
-  int rc = stage_times(c, st, &span);
+  float st[ZF_PROF_STAGES];
+  int rc = stage_times(c, st);
   if (rc) return rc;
+  float tm = 0.f;
+  for (int k = 0; k < ZF_PROF_STAGES; ++k)
+    if (k != 1) tm += st[k];  // the membrane iteration's own LBM launch is not part of the block
   if (lbm_ms) *lbm_ms = tl;
   if (lbm_count) *lbm_count = runs_n;
-  // the membrane iterations without their own LBM launch
-  if (membrane_ms) *membrane_ms = span - st[1];
+  if (membrane_ms) *membrane_ms = tm;
   if (membrane_count) *membrane_count = c->prof_mem;
   return ZF_OK;
 }
@@ -538,8 +488,7 @@ int zf_profile_read(zf_ctx* c, float* lbm_ms, int* lbm_count, float* membrane_ms
 int zf_profile_stages(zf_ctx* c, float* stage_ms, int* blocks) {
   if (!c || !stage_ms) return ZF_ERR_ARG;
   ZF_CUDA(cudaStreamSynchronize(c->stream));
-  float span = 0.f;
-  int rc = stage_times(c, stage_ms, &span);
+  int rc = stage_times(c, stage_ms);
   if (rc) return rc;
   if (blocks) *blocks = c->prof_mem;
   return ZF_OK;

@@ -37,11 +37,9 @@ __host__ __device__ __forceinline__ bool zf_code_pressure(uint8_t cd) {
 
 namespace zf {
 
-// membrane-iteration stages timed by zf_profile (see zf_profile_stages):
-// events 0..8 on the context's stream, 9..11 around the cell list and the
-// RBC-RBC search (on the second stream when they overlap the IB stages)
+// membrane-iteration stages timed by zf_profile (see zf_profile_stages)
 constexpr int ZF_PROF_STAGES = 8;
-constexpr int ZF_PROF_MARKS = 12;
+constexpr int ZF_PROF_MARKS = ZF_PROF_STAGES + 1;
 
 void set_error(const char* fmt, ...);
 
@@ -109,9 +107,6 @@ struct CellArgs {
   float* ftot_n;             // [3][nc][nnn]
   float* wrep;               // [3][nc][nn] velocity increments (NODE_WALLREPUL)
   float* wrep_n;             // [3][nc][nnn]
-  float* wrep_rr;            // [3][nc][nn] RBC-RBC increments of a membrane step whose cell-cell
-                             // search ran beside the IB interpolation; the spreading folds them
-                             // into wrep (and clears them)
   float* node_normal;        // [3][nc][nn]
   float* tri_c;              // [3][nc][nt] um
   float* tri_nrm;            // [3][nc][nt]
@@ -187,8 +182,9 @@ struct IbArgs {
   const int32_t* wrel_cnt;      // [n_all*64]
   const int32_t* wrel_off;      // [n_all*64 + 1]
   const int32_t* wrel;          // 1-based wall node ids
-  int32_t* wall_walk;           // [n_cells*(nn+nnn)] nodes queued for the window walk
-  int32_t* wall_walk_ctr;       // [2] queued count, work counter
+  int32_t* wall_walk;           // [n_cells*(nn+nnn)] nodes queued for the window walk (from the
+                                // front) and for the warp scan of their wall-node lists (from the back)
+  int32_t* wall_walk_ctr;       // [4] walk: queued count, work counter; lists: queued count, work counter
   const int32_t* wcand_off;     // [nw+1] WallHost::cand_off
   const float4* wcand;          // WallHost::cand
   // cell list of triangle centroids over population slots (CSR).  Bin keys
@@ -200,12 +196,6 @@ struct IbArgs {
                                 // radius (rec_pack); normal xyz and global triangle id (int bits)
   float4* bin_v;                // [3][n_cells*nt] per entry: vertex xyz (fp32), node id (int bits)
   uint8_t* bin_kk;              // [n_cells*nt] per entry: its key inside the tile (0..63)
-  int32_t* bin_reach;           // [ns+1] float bits: farthest point of a bin's triangles
-                                // from the bin point (um, rounded up); [ns] the largest
-  int4* bin_hdr;                // [ns] per bin: first entry, entry count, reach (float bits),
-                                // normal cone (cone_pack) of its triangles
-  uint2* bin_occ;               // [ns/64] per population tile: bit 16x+4y+z set when that
-                                // bin holds a triangle (x: keys 0..31, y: keys 32..63)
   // membrane and nucleus nodes grouped by the lattice tile of their nearest
   // point (tile grid index over all ntx*nty*ntz tiles), rebuilt after positions change
   int64_t ngrid;                // ntx*nty*ntz
@@ -230,13 +220,8 @@ int ib_prepare(zf_ctx* c);
 void ib_free(zf_ctx* c);
 int ib_interp_launch(zf_ctx* c);
 int ib_bins_launch(zf_ctx* c);
-// the tile-cooperative IB kernels apply (z tiles wrap with a periodic lattice)
-bool tiles_ok(const IbArgs& a);
 int ib_nuc_memb_launch(zf_ctx* c, int rebuild);
-// out: where the RBC-RBC increments go (nullptr: NODE_WALLREPUL itself);
-// max_per_sm > 0 caps the resident blocks per SM of the persistent search so
-// that kernels of another stream can run beside it
-int ib_rbc_rbc_launch(zf_ctx* c, float* out = nullptr, int max_per_sm = 0);
+int ib_rbc_rbc_launch(zf_ctx* c);
 int ib_node_tiles_launch(zf_ctx* c);
 int lbm_moments_launch(zf_ctx* c);
 // adjoint building blocks
@@ -277,8 +262,7 @@ int spread_adj_launch(zf_ctx* c, const float* d_G, float* d_gmem, float* d_gnuc)
 int scale_springs_launch(zf_ctx* c, float s);
 int wss_launch(zf_ctx* c, const float* d_normals, double pgauge, float* d_wss, float* d_press,
                int32_t* d_valid);
-// fold = 1: first add the RBC-RBC increments of wrep_rr into wrep (and clear them)
-int ib_spread_launch(zf_ctx* c, int fold = 0);
+int ib_spread_launch(zf_ctx* c);
 int ib_update_launch(zf_ctx* c);
 
 }  // namespace zf
@@ -353,10 +337,6 @@ struct zf_ctx {
   // instrumentation: kernel launches, and optional event pairs around the LBM
   // kernel and the membrane block of zf_step
   int64_t launches = 0;
-  // second stream of the membrane step: the cell list and RBC-RBC search run
-  // on it while the context's stream runs the LBM step and the IB stages
-  cudaStream_t side_stream = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;  // [2*cap] LBM run pairs, then ZF_PROF_MARKS per membrane block
   int prof_cap = 0, prof_lbm = 0, prof_mem = 0;  // event pairs: LBM runs, membrane blocks

@@ -67,10 +67,18 @@ __device__ __forceinline__ float cdot(int q, float x, float y, float z) {
 }
 
 // ---- storage codecs: decode to / encode from the deviation d = f/w - rho_ref
-struct RawF32 {  // plain populations, as the reference keeps F
+// Plain populations, as the reference keeps F.  f = w (rho_ref + d) is
+// formed with one rounding, fma(w, d, w rho_ref), and read back as
+// (f - w rho_ref) / w: the subtraction is exact (f lies within a factor 2 of
+// w rho_ref), so the only error left is the storage rounding itself.  (The
+// form f/w - rho_ref would add (w_fp32/w - 1)(rho_ref + d), a fixed offset
+// of about 3e-8 per population per step, since 1/18, 1/36, 1/3 have no exact
+// fp32 value.)
+struct RawF32 {
   using T = float;
-  __device__ static float dec(T v, int q, const LbmArgs& a) { return v * IWQ(q) - a.rho_ref; }
-  __device__ static T enc(float d, int q, const LbmArgs& a) { return WQ(q) * (a.rho_ref + d); }
+  __device__ static float wr(int q, const LbmArgs& a) { return __fmul_rn(WQ(q), a.rho_ref); }
+  __device__ static float dec(T v, int q, const LbmArgs& a) { return __fmul_rn(__fsub_rn(v, wr(q, a)), IWQ(q)); }
+  __device__ static T enc(float d, int q, const LbmArgs& a) { return __fmaf_rn(WQ(q), d, wr(q, a)); }
 };
 struct DevF32 {
   using T = float;
@@ -485,6 +493,18 @@ __global__ void k_lbm_wall(LbmArgs a, const int32_t* __restrict__ wall_slot,
   }
 }
 
+// populations f at the boundary <-> stored values (plain fp32 stores f itself)
+template <class C>
+__device__ __forceinline__ typename C::T from_f(float f, int q, const LbmArgs& a) {
+  if constexpr (std::is_same<C, RawF32>::value) return f;
+  else return C::enc(__fmul_rn(__fsub_rn(f, RawF32::wr(q, a)), IWQ(q)), q, a);
+}
+template <class C>
+__device__ __forceinline__ float to_f(typename C::T v, int q, const LbmArgs& a) {
+  if constexpr (std::is_same<C, RawF32>::value) return v;
+  else return __fmaf_rn(WQ(q), C::dec(v, q, a), RawF32::wr(q, a));
+}
+
 template <class C>
 __global__ void k_fill_equilibrium(typename C::T* f, int64_t ns, LbmArgs a) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -501,7 +521,7 @@ __global__ void k_scatter_pop(typename C::T* f, int64_t ns, const float* __restr
   const int64_t s = dom_slot[l];
 #pragma unroll
   for (int q = 0; q < ZF_Q; ++q)
-    f[pop_at(q, s)] = C::enc(stage[q * n + l] * IWQ(q) - a.rho_ref, q, a);
+    f[pop_at(q, s)] = from_f<C>(stage[q * n + l], q, a);
 }
 
 template <class C>
@@ -511,7 +531,7 @@ __global__ void k_gather_pop(const typename C::T* f, int64_t ns, float* __restri
   if (l >= n) return;
   const int64_t s = dom_slot[l];
 #pragma unroll
-  for (int q = 0; q < ZF_Q; ++q) stage[q * n + l] = WQ(q) * (a.rho_ref + C::dec(f[pop_at(q, s)], q, a));
+  for (int q = 0; q < ZF_Q; ++q) stage[q * n + l] = to_f<C>(f[pop_at(q, s)], q, a);
 }
 
 __global__ void k_scatter_planes(float* dst, int64_t ns, const float* __restrict__ stage,
@@ -884,7 +904,7 @@ __global__ void k_seed_at(LbmArgs a, const int32_t* __restrict__ uslot, int nu, 
   float fq[ZF_Q], rho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
 #pragma unroll
   for (int q = 0; q < ZF_Q; ++q) {
-    fq[q] = WQ(q) * (a.rho_ref + C::dec(f[pop_at(q, s)], q, a));
+    fq[q] = to_f<C>(f[pop_at(q, s)], q, a);
     rho += fq[q];
     mx += EX(q) * fq[q];
     my += EY(q) * fq[q];

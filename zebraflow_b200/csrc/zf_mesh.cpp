@@ -376,7 +376,6 @@ int zf_set_cells(zf_ctx* c, int n_cells, const double* x, const double* xn) {
   if ((rc = upload<float>(c, own, &a.ftot_n, nullptr, 3 * nc * nnn))) return rc;
   if ((rc = upload<float>(c, own, &a.wrep, nullptr, 3 * nc * nn))) return rc;
   if ((rc = upload<float>(c, own, &a.wrep_n, nullptr, 3 * nc * nnn))) return rc;
-  if ((rc = upload<float>(c, own, &a.wrep_rr, nullptr, 3 * nc * nn))) return rc;
   if ((rc = upload<float>(c, own, &a.node_normal, nullptr, 3 * nc * nn))) return rc;
   if ((rc = upload<float>(c, own, &a.tri_c, nullptr, 3 * nc * nt))) return rc;
   if ((rc = upload<float>(c, own, &a.tri_nrm, nullptr, 3 * nc * nt))) return rc;
