@@ -477,16 +477,40 @@ __global__ void k_scan_blocks(const int32_t* in, int64_t n, int32_t* out, int32_
   if (i < n) out[i] = sh[threadIdx.x] - v;
   if (threadIdx.x == 1023) bsum[blockIdx.x] = sh[1023];
 }
-__global__ void k_scan_sums(int32_t* bsum, int nb, int32_t* total) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    int32_t run = 0;
-    for (int b = 0; b < nb; ++b) {
-      const int32_t v = bsum[b];
-      bsum[b] = run;
-      run += v;
+// exclusive scan of the nb block sums in place, *total their sum: one block
+// of 1024 threads, 1024 sums per round (warp scans, then a scan of the 32
+// warp totals), the running total carried between rounds
+__global__ void __launch_bounds__(1024) k_scan_sums(int32_t* bsum, int nb, int32_t* total) {
+  __shared__ int32_t s_w[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int32_t carry = 0;
+  for (int base = 0; base < nb; base += 1024) {
+    const int i = base + (int)threadIdx.x;
+    const int32_t v = i < nb ? bsum[i] : 0;
+    int32_t x = v;  // inclusive scan within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
     }
-    *total = run;
+    if (lane == 31) s_w[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      int32_t t = s_w[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += y;
+      }
+      s_w[lane] = t;  // inclusive over warps
+    }
+    __syncthreads();
+    const int32_t before = carry + (w > 0 ? s_w[w - 1] : 0) + x - v;
+    if (i < nb) bsum[i] = before;
+    carry += s_w[31];
+    __syncthreads();  // s_w is rewritten by the next round
   }
+  if (threadIdx.x == 0) *total = carry;
 }
 __global__ void k_scan_add(int32_t* out, int64_t n, const int32_t* bsum) {
   const int64_t i = (int64_t)blockIdx.x * 1024 + threadIdx.x;
@@ -982,7 +1006,8 @@ struct RgShared {
   int rrel[27];             // tile offset in the 12^3 block: x | y << 8 | z << 16 (in units of 4 points)
   float bb[6];              // node box: min x, y, z, max x, y, z
   int wsum[kRgWarps];
-  int li, ncand, nn, node_next;
+  int wsum2[2][kRgWarps];   // per warp: kept records of a staging round (two rounds alternate)
+  int li, nn, node_next;
 };
 
 __device__ __forceinline__ int onehot_range(int lo, int hi) {  // bits lo..hi of 12, clamped
@@ -1094,19 +1119,19 @@ __global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs 
         int t = 0;
         for (int w = 0; w < kRgWarps; ++w) t += S.wsum[w];
         S.nn = t;
-        S.ncand = 0;
       }
       __syncthreads();
       if (S.nn == 0) continue;
       const float hx = 0.5f * (S.bb[3] - S.bb[0]), hy = 0.5f * (S.bb[4] - S.bb[1]), hz = 0.5f * (S.bb[5] - S.bb[2]);
       const float mxc = S.bb[0] + hx, myc = S.bb[1] + hy, mzc = S.bb[2] + hz;
       const int total = S.rng[27];
+      int ncl = 0;  // kept records held (the same in every thread)
 
       // the kept triangles, tested against the staged nodes
       auto process = [&]() {
         if (tid == 0) S.node_next = 0;
         __syncthreads();
-        const int ncand = S.ncand;
+        const int ncand = ncl;
         int* queue = S.q[warp];
         // nodes go to the warps as they free up (their costs differ widely)
         for (;;) {
@@ -1184,57 +1209,72 @@ __global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs 
             S.acc[t][2] += rz;
           }
         }
-        __syncthreads();
-        if (tid == 0) S.ncand = 0;
-        __syncthreads();
+        __syncthreads();  // the list is free for the next records
+        ncl = 0;
       };
 
-      for (int f0 = 0; f0 < total; f0 += kRgThreads) {
-        if (S.ncand + kRgThreads > kRgCand) process();
-        const int f = f0 + tid;
-        bool keep = false;
-        float4 cr = make_float4(0.f, 0.f, 0.f, 0.f);
-        int e = 0, r = 0;
+      // one barrier per round: each warp's count goes to one of two arrays in
+      // turn, and every thread sums them itself, so records keep their order.
+      // A thread's record of the next round (centroid and normal words, one
+      // 32-byte sector) is loaded while the current round is filtered.
+      auto fetch = [&](int f, int& e, int& r, float4& cr, float4& nr) {
+        e = 0;
+        r = 0;
+        cr = nr = make_float4(0.f, 0.f, 0.f, 0.f);
         if (f < total) {
 #pragma unroll
           for (int stp = 16; stp > 0; stp >>= 1)
             if (r + stp < 27 && f >= S.rng[r + stp]) r += stp;
           e = S.rst[r] + (f - S.rng[r]);
           cr = a.bin_rec[2 * e];
-          const float rb = rec_rb(cr.w);
-          const float dx = fmaxf(fabsf(cr.x - mxc) - hx, 0.f), dy = fmaxf(fabsf(cr.y - myc) - hy, 0.f);
-          const float dz = fmaxf(fabsf(wrapd(cr.z - mzc, a.LZ)) - hz, 0.f);
-          const float lim = 1.0021f + 0.75f * rb;
-          keep = dx * dx + dy * dy + dz * dz <= lim * lim * 1.0001f;
+          nr = a.bin_rec[2 * e + 1];
         }
-        const unsigned bal = __ballot_sync(FULL, keep);
-        if (lane == 0) S.wsum[warp] = __popc(bal);
-        __syncthreads();
-        int base = S.ncand;
-        for (int w = 0; w < warp; ++w) base += S.wsum[w];
-        if (keep) {
-          const int pos = base + __popc(bal & ((1u << lane) - 1u));
-          const float rb = rec_rb(cr.w);
-          const float lim = 1.0021f + 0.75f * rb;
-          S.cand_c[pos] = make_float4(cr.x, cr.y, cr.z, lim * lim * 1.0001f);
-          S.cand_n[pos] = a.bin_rec[2 * e + 1];
-          S.cand_w[pos] = __float_as_int(cr.w);
-          S.cand_e[pos] = e;
-          const int kk = rec_kk(cr.w), rel = S.rrel[r];
-          const int bi = (rel & 0xff) * 4 + (kk >> 4), bj = ((rel >> 8) & 0xff) * 4 + ((kk >> 2) & 3),
-                    bk = (rel >> 16) * 4 + (kk & 3);
-          S.cand_xy[pos] = (1 << bi) | (1 << (12 + bj));
-          S.cand_z[pos] = 1 << bk;
+      };
+      int f0 = 0, par = 0;
+      while (f0 < total) {
+        if (ncl + kRgThreads > kRgCand) process();  // outside the rounds: no prefetch is live
+        int e_nx, r_nx;
+        float4 cr_nx, nr_nx;
+        fetch(f0 + tid, e_nx, r_nx, cr_nx, nr_nx);
+        for (; f0 < total && ncl + kRgThreads <= kRgCand; f0 += kRgThreads, par ^= 1) {
+          const int f = f0 + tid, e = e_nx, r = r_nx;
+          const float4 cr = cr_nx, nr = nr_nx;
+          fetch(f + kRgThreads, e_nx, r_nx, cr_nx, nr_nx);
+          bool keep = false;
+          if (f < total) {
+            const float rb = rec_rb(cr.w);
+            const float dx = fmaxf(fabsf(cr.x - mxc) - hx, 0.f), dy = fmaxf(fabsf(cr.y - myc) - hy, 0.f);
+            const float dz = fmaxf(fabsf(wrapd(cr.z - mzc, a.LZ)) - hz, 0.f);
+            const float lim = 1.0021f + 0.75f * rb;
+            keep = dx * dx + dy * dy + dz * dz <= lim * lim * 1.0001f;
+          }
+          const unsigned bal = __ballot_sync(FULL, keep);
+          if (lane == 0) S.wsum2[par][warp] = __popc(bal);
+          __syncthreads();
+          int base = ncl, kept = 0;
+          for (int w = 0; w < kRgWarps; ++w) {
+            const int n = S.wsum2[par][w];
+            if (w < warp) base += n;
+            kept += n;
+          }
+          if (keep) {
+            const int pos = base + __popc(bal & ((1u << lane) - 1u));
+            const float rb = rec_rb(cr.w);
+            const float lim = 1.0021f + 0.75f * rb;
+            S.cand_c[pos] = make_float4(cr.x, cr.y, cr.z, lim * lim * 1.0001f);
+            S.cand_n[pos] = nr;
+            S.cand_w[pos] = __float_as_int(cr.w);
+            S.cand_e[pos] = e;
+            const int kk = rec_kk(cr.w), rel = S.rrel[r];
+            const int bi = (rel & 0xff) * 4 + (kk >> 4), bj = ((rel >> 8) & 0xff) * 4 + ((kk >> 2) & 3),
+                      bk = (rel >> 16) * 4 + (kk & 3);
+            S.cand_xy[pos] = (1 << bi) | (1 << (12 + bj));
+            S.cand_z[pos] = 1 << bk;
+          }
+          ncl += kept;
         }
-        __syncthreads();
-        if (tid == 0) {
-          int t = S.ncand;
-          for (int w = 0; w < kRgWarps; ++w) t += S.wsum[w];
-          S.ncand = t;
-        }
-        __syncthreads();
       }
-      if (S.ncand > 0) process();
+      if (ncl > 0) process();
       // the chunk's sums into NODE_WALLREPUL (one writer per node)
       if (tid < cnt) {
         const int cell = __float_as_int(S.node_n[tid].w);
@@ -1264,7 +1304,7 @@ __global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs 
 // min(U, 1.5) + 1e-3 of B: at most kWallRel of them (more: -1, and the node
 // walks its window instead).  One thread per point, one block of 64 per grid
 // tile; the count pass writes counts, the fill pass the lists.
-constexpr int kWallRel = 96;
+constexpr int kWallRel = 192;
 template <bool kFill>
 __global__ void k_wall_rel(IbArgs a, int32_t* __restrict__ cnt, int32_t* __restrict__ clipped,
                            const int32_t* __restrict__ off, int32_t* __restrict__ out) {
@@ -2309,7 +2349,7 @@ int persistent_blocks(K kernel, int threads) {
 void scan_launch(const int32_t* in, int64_t n, int32_t* out, int32_t* bsum, cudaStream_t st) {
   const int nb = (int)((n + 1023) / 1024);
   k_scan_blocks<<<nb, 1024, 0, st>>>(in, n, out, bsum);
-  k_scan_sums<<<1, 32, 0, st>>>(bsum, nb, bsum + nb);
+  k_scan_sums<<<1, 1024, 0, st>>>(bsum, nb, bsum + nb);
   k_scan_add<<<nb, 1024, 0, st>>>(out, n, bsum);
 }
 
