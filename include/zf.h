@@ -521,6 +521,15 @@ int zf_gen_cells(const int32_t* b, int nx, int ny, int nz, const double* origin,
 int zf_read_bindex_csv(const char* path, int nx, int ny, int nz, const double* origin, double dx,
                        int32_t* b_index, int64_t* n_rows);
 
+/* Boundary CSV of a parent segment, "Bindex","D","U","V","W","Points:0",
+ * "Points:1","Points:2" (DAparentBoundary.csv and PCVparent*Boundary.csv, read
+ * at ZebraflowWT.c:557-588): b_index [nx][ny][nz] is set to -1 and then to each
+ * row's Bindex at its point; D, U, V, W are read and not kept, as the
+ * reference does.  (The reference then marks and extrudes the parent segment,
+ * :583-600, which is not part of this library.) */
+int zf_read_boundary_csv(const char* path, int nx, int ny, int nz, const double* origin, double dx,
+                         int32_t* b_index, int64_t* n_rows);
+
 /* Fluid snapshot "X,Y,Z,Bindex,U,V,W,D,Bx,By,Bz,EulNeigh,Windex" (OUTPUT(),
  * ZebraflowWT.c:356-370): one row per listed point in DOMLIST order.  D..W,
  * eulneigh [n_listed] and bodyforce [3][n_listed] are in DOMLIST order;

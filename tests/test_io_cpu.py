@@ -140,6 +140,27 @@ def test_bindex_file(tmp_path):
         zf.read_bindex_csv(p, dims, origin=origin)
 
 
+def test_parent_boundary_file(tmp_path):
+    rng = np.random.default_rng(4)
+    dims, origin = (5, 6, 4), (69.0, 218.5, -27.5)
+    b = rng.integers(-1, 3, dims).astype(np.int32)
+    p = str(tmp_path / "DAparentBoundary.csv")
+    with open(p, "w") as f:  # quoted header, then Bindex, D, U, V, W and the point (ZebraflowWT.c:557-580)
+        f.write('"Bindex","D","U","V","W","Points:0","Points:1","Points:2"\n')
+        for i, j, k in np.argwhere(b >= 0):
+            f.write(f"{b[i, j, k]},1,0,0,0,{origin[0] + 0.5 * i:g},{origin[1] + 0.5 * j:g},{origin[2] + 0.5 * k:g}\n")
+    got, rows = zf.read_boundary_csv(p, dims, origin=origin)
+    assert rows == int((b >= 0).sum()) and np.array_equal(got, b)
+    if have_reference():  # the shipped file: 3008 rows inside its parent segment's box
+        q = str(tmp_path / "shipped.csv")
+        open(q, "wb").write(gzip.open(os.path.join(reference_dir(), "DAparentBoundary.csv.gz")).read())
+        pts = np.loadtxt(q, delimiter=",", skiprows=1)
+        lo = pts[:, 5:8].min(axis=0)
+        ext = np.rint((pts[:, 5:8].max(axis=0) - lo) / 0.5).astype(int) + 1
+        got, rows = zf.read_boundary_csv(q, tuple(ext), origin=tuple(lo))
+        assert rows == 3008 and int((got >= 0).sum()) == len(np.unique(pts[:, 5:8], axis=0))
+
+
 def test_mesh_files(tmp_path):
     s = np.load(os.path.join(GOLD, "ref_setup.npz"))
     X, T, XN, EN = s["mesh_x"], s["mesh_tri"], s["nuc_x"], s["nuc_edges"]

@@ -117,6 +117,8 @@ _SIGS = {
                                   C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "zf_read_bindex_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, _i32p,
                                      C.POINTER(C.c_int64)]),
+    "zf_read_boundary_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, _i32p,
+                                       C.POINTER(C.c_int64)]),
     "zf_write_fluid_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, _i32p, _f32p, _f32p,
                                      _f32p, _f32p, _f32p, C.c_void_p, C.c_void_p]),
     "zf_read_fluid_csv": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _f64p, C.c_double, _i32p, C.c_void_p,
@@ -372,6 +374,17 @@ def read_bindex_csv(path, dims, origin=(0.0, 0.0, 0.0), dx=0.5):
     rows = C.c_int64()
     _check(lib().zf_read_bindex_csv(_path(path), nx, ny, nz, np.asarray(origin, np.float64), dx, b,
                                     C.byref(rows)))
+    return b.reshape(nx, ny, nz), rows.value
+
+
+def read_boundary_csv(path, dims, origin=(0.0, 0.0, 0.0), dx=0.5):
+    """A parent segment's boundary CSV ("Bindex","D","U","V","W","Points:0..2"):
+    the B_index array it describes (-1 elsewhere) and the row count."""
+    nx, ny, nz = dims
+    b = np.empty(nx * ny * nz, np.int32)
+    rows = C.c_int64()
+    _check(lib().zf_read_boundary_csv(_path(path), nx, ny, nz, np.asarray(origin, np.float64), dx, b,
+                                      C.byref(rows)))
     return b.reshape(nx, ny, nz), rows.value
 
 

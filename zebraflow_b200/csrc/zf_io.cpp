@@ -146,6 +146,30 @@ int zf_read_bindex_csv(const char* path, int nx, int ny, int nz, const double* o
   return ZF_OK;
 }
 
+int zf_read_boundary_csv(const char* path, int nx, int ny, int nz, const double* origin, double dx,
+                         int32_t* b_index, int64_t* n_rows) {
+  static const char* fn = "zf_read_boundary_csv";
+  if (!b_index || !origin || nx <= 0 || ny <= 0 || nz <= 0 || dx <= 0) return ZF_ERR_ARG;
+  Reader r;
+  if (!r.load(path)) return fail_open(fn, path);
+  for (size_t p = 0; p < (size_t)nx * ny * nz; ++p) b_index[p] = -1;  // ZebraflowWT.c:546-555
+  r.line();                                                            // header
+  long long row = 0;
+  while (!r.eof()) {
+    int32_t b;
+    float d, u, v, w, x, y, z;  // D, U, V, W are read and not kept, as at :563-570
+    if (!r.i32(b) || !r.f32(d) || !r.f32(u) || !r.f32(v) || !r.f32(w) || !r.f32(x) || !r.f32(y) || !r.f32(z))
+      return fail_parse(fn, path, "expected Bindex,D,U,V,W,Points:0,Points:1,Points:2", row + 1);
+    const int i = lat0(x, origin[0], dx), j = lat0(y, origin[1], dx), k = lat0(z, origin[2], dx);
+    if (i < 0 || i >= nx || j < 0 || j >= ny || k < 0 || k >= nz)
+      return fail_parse(fn, path, "point outside the lattice box", row + 1);
+    b_index[((size_t)i * ny + j) * nz + k] = b;
+    ++row;
+  }
+  if (n_rows) *n_rows = row;
+  return ZF_OK;
+}
+
 int zf_write_fluid_csv(const char* path, int nx, int ny, int nz, const double* origin, double dx,
                        const int32_t* b_index, const float* D, const float* U, const float* V, const float* W,
                        const float* bodyforce, const int32_t* eulneigh, const int32_t* windex) {
