@@ -230,13 +230,28 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC, 6) k_lbm(LbmArgs a) {
     // moments with the half-force shift, ZebraflowWT.c:6125-6135:
     // rho = rho_ref + sum w d,  m = sum w c d  (sum w c = 0)
     float drho = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+    if constexpr (kHalf) {
+      // from the sums and differences of the opposite pairs (q, q + 1), q even
+      // (fewer instructions; the fp32 forms keep the per-direction order)
+      float S[9], Dd[9];
 #pragma unroll
-    for (int q = 0; q < ZF_Q; ++q) {
-      const float wd = WQ(q) * d[q];
-      drho += wd;
-      if (EX(q)) mx += EX(q) * wd;
-      if (EY(q)) my += EY(q) * wd;
-      if (EZ(q)) mz += EZ(q) * wd;
+      for (int p = 0; p < 9; ++p) {
+        S[p] = d[2 * p] + d[2 * p + 1];
+        Dd[p] = d[2 * p] - d[2 * p + 1];
+      }
+      drho = fmaf(WQ(18), d[18], fmaf(WQ(0), S[0] + S[1] + S[2], WQ(6) * ((S[3] + S[4]) + (S[5] + S[6]) + (S[7] + S[8]))));
+      mx = fmaf(WQ(0), Dd[0], WQ(6) * ((Dd[3] - Dd[4]) + (Dd[5] - Dd[6])));  // c_x of q = 6, 8, 10, 12: +, -, +, -
+      my = fmaf(WQ(0), Dd[1], WQ(6) * ((Dd[3] + Dd[4]) + (Dd[7] - Dd[8])));  // c_y of q = 6, 8, 14, 16: +, +, +, -
+      mz = fmaf(WQ(0), Dd[2], WQ(6) * ((Dd[5] + Dd[6]) + (Dd[7] + Dd[8])));  // c_z of q = 10, 12, 14, 16: all +
+    } else {
+#pragma unroll
+      for (int q = 0; q < ZF_Q; ++q) {
+        const float wd = WQ(q) * d[q];
+        drho += wd;
+        if (EX(q)) mx += EX(q) * wd;
+        if (EY(q)) my += EY(q) * wd;
+        if (EZ(q)) mz += EZ(q) * wd;
+      }
     }
     if constexpr (kHalf) {
       drho *= a.inv_scale;
@@ -270,7 +285,7 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC, 6) k_lbm(LbmArgs a) {
     float r2 = 0.f, m2x = 0.f, m2y = 0.f, m2z = 0.f;
     uint32_t rseed = 0;
     if (kHalf) rseed = mix32((uint32_t)self * 0x9E3779B1u + a.step * 0x85EBCA77u);
-    float dn_prev = 0.f;
+    float dn_prev = 0.f, dn_odd = 0.f;
     T* __restrict__ fo = fout + pb.b0;
 #pragma unroll
     for (int q = 0; q < ZF_Q; ++q) {
@@ -282,12 +297,17 @@ __global__ void __launch_bounds__(kTilesPerBlock * ZF_TC, 6) k_lbm(LbmArgs a) {
         const float src = sfac * (3.f * (cF - uF) + 9.f * cu * cF);
         dn = d[q] + omega * (deq - d[q]) + src;
       } else if constexpr (kHalf) {
+        // E(q) = Aw + K1w cu + K2w cu^2 + K4s cF + K3s cu cF; the opposite
+        // direction q + 1 has -cu, -cF: E = S +- T with S, T shared
         if (q == 18) {
           dn = fmaf(omc, d[q], Aw);
-        } else {
+        } else if ((q & 1) == 0) {
           const float cu = cdot(q, ux, uy, uz), cF = cdot(q, Fx, Fy, Fz);
-          const float E = fmaf(cF, fmaf(K3s, cu, K4s), fmaf(cu, fmaf(K2w, cu, K1w), Aw));
-          dn = fmaf(omc, d[q], E);
+          const float Sq = fmaf(cu, fmaf(K2w, cu, K3s * cF), Aw), Tq = fmaf(K1w, cu, K4s * cF);
+          dn = fmaf(omc, d[q], Sq + Tq);
+          dn_odd = fmaf(omc, d[q + 1], Sq - Tq);
+        } else {
+          dn = dn_odd;
         }
       } else if (q == 18) {
         dn = fmaf(omega, A - d[q], d[q]) - K5;
