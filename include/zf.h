@@ -283,6 +283,17 @@ int zf_set_cells(zf_ctx* ctx, int n_cells, const double* x, const double* xn);
  * -5000 removed).  NULL skips. */
 int zf_get_cells(zf_ctx* ctx, double* x, double* xn, int32_t* status);
 
+/* No counterpart in the reference.  zf_get_cells without waiting: the copies
+ * of the positions and statuses as they stand after the work queued so far
+ * run on a second stream while the caller queues more steps; the next kernel
+ * that changes positions or statuses (the membrane forces and the position
+ * update of the next membrane iteration, zf_set_cells, zf_load_state) waits
+ * for them, so the LBM iterations in between overlap the copy.  The host
+ * buffers must be pinned (cudaHostAlloc / cudaHostRegister) for the copy to
+ * run asynchronously, and hold their values once zf_wait_cells returns. */
+int zf_get_cells_async(zf_ctx* ctx, double* x, double* xn, int32_t* status);
+int zf_wait_cells(zf_ctx* ctx);
+
 /* F_Total [3][n_cells][n_node] and F_Total_N [3][n_cells][n_node_n] in N. */
 int zf_get_cell_forces(zf_ctx* ctx, float* ftot, float* ftot_n);
 

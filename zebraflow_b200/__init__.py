@@ -95,6 +95,8 @@ _SIGS = {
     "zf_get_edge_params": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
     "zf_set_cells": (C.c_int, [_P, C.c_int, _f64p, C.c_void_p]),
     "zf_get_cells": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "zf_get_cells_async": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "zf_wait_cells": (C.c_int, [_P]),
     "zf_get_cell_forces": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "zf_get_cell_kinematics": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "zf_get_cell_geometry": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -636,6 +638,15 @@ class Context:
         st = np.empty(self.nc, np.int32)
         _check(lib().zf_get_cells(self._h, _ptr(x), _ptr(xn), _ptr(st)))
         return x, xn, st
+
+    def cells_async(self, x, xn, status):
+        """Queue the copies of zf_get_cells into x [3][nc][nn], xn and status
+        (pinned host arrays, or None) without waiting; they hold the values
+        once wait_cells() returns."""
+        _check(lib().zf_get_cells_async(self._h, _ptr(x), _ptr(xn), _ptr(status)))
+
+    def wait_cells(self):
+        _check(lib().zf_wait_cells(self._h))
 
     def cell_forces(self):
         f = np.empty((3, self.nc, self.nn), np.float32)

@@ -373,6 +373,8 @@ size_t membrane_smem_bytes(const CellArgs& a) {
 int cells_membrane_launch(zf_ctx* c) {
   const CellArgs& a = c->cells;
   if (a.n_cells == 0) return ZF_OK;
+  int rc0 = cells_write_fence(c);  // k_membrane may remove cells (status)
+  if (rc0) return rc0;
   const size_t smem = membrane_smem_bytes(a);
   ZF_CUDA(cudaFuncSetAttribute(k_membrane, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_membrane<<<a.n_cells, 256, smem, c->stream>>>(a);

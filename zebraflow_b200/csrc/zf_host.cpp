@@ -123,12 +123,16 @@ void zf_destroy(zf_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   ib_free(c);
   free_lattice(c);
   cells_free(c);
   for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->ev_ready) cudaEventDestroy(c->ev_ready);
+  if (c->ev_copied) cudaEventDestroy(c->ev_copied);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }

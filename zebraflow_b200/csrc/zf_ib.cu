@@ -2529,6 +2529,8 @@ int ib_spread_launch(zf_ctx* ctx) {
 int ib_update_launch(zf_ctx* ctx) {
   const CellArgs& c = ctx->cells;
   if (c.n_cells == 0) return ZF_OK;
+  const int rc = cells_write_fence(ctx);  // positions and statuses change
+  if (rc) return rc;
   k_update<<<c.n_cells, 256, 0, ctx->stream>>>(ctx->ib, c);
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 1;

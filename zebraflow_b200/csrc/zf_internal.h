@@ -264,6 +264,11 @@ int wss_launch(zf_ctx* c, const float* d_normals, double pgauge, float* d_wss, f
                int32_t* d_valid);
 int ib_spread_launch(zf_ctx* c);
 int ib_update_launch(zf_ctx* c);
+// before a kernel that writes cell positions or statuses: the context's stream
+// waits for a pending zf_get_cells_async copy; cells_copy_wait_host waits on
+// the host (before cell buffers are freed or replaced)
+int cells_write_fence(zf_ctx* c);
+int cells_copy_wait_host(zf_ctx* c);
 
 }  // namespace zf
 
@@ -272,6 +277,12 @@ struct zf_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;      // stream the context's work is queued on
   cudaStream_t own_stream = nullptr;  // created by zf_create
+  // zf_get_cells_async: the copies run on copy_stream after ev_ready (the
+  // context's stream); ev_copied marks their end, which the next kernel that
+  // writes positions or statuses waits for (cells_write_fence)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_ready = nullptr, ev_copied = nullptr;
+  bool copy_pending = false;
   bool lattice_set = false;
 
   // listed nodes (reference DOMLIST order)

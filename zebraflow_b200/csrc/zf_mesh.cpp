@@ -237,6 +237,24 @@ void cells_free(zf_ctx* c) {
     return ZF_ERR_STATE;               \
   }
 
+namespace zf {
+
+int cells_write_fence(zf_ctx* c) {
+  if (c->copy_pending) {
+    ZF_CUDA(cudaStreamWaitEvent(c->stream, c->ev_copied, 0));
+    c->copy_pending = false;
+  }
+  return ZF_OK;
+}
+
+int cells_copy_wait_host(zf_ctx* c) {
+  if (c->copy_stream) ZF_CUDA(cudaStreamSynchronize(c->copy_stream));
+  c->copy_pending = false;
+  return ZF_OK;
+}
+
+}  // namespace zf
+
 extern "C" {
 
 int zf_set_mesh(zf_ctx* c, int n_node, int n_tri, const int32_t* tri, const double* rest,
@@ -362,6 +380,8 @@ int zf_set_cells(zf_ctx* c, int n_cells, const double* x, const double* xn) {
   NEED(c->mesh_set, "zf_set_cells", "mesh not set");
   ZF_CUDA(cudaSetDevice(c->device));
   ZF_CUDA(cudaStreamSynchronize(c->stream));
+  int rc0 = cells_copy_wait_host(c);  // a zf_get_cells_async copy may still read the old buffers
+  if (rc0) return rc0;
   free_owned(c->cell_allocs);
   CellArgs& a = c->cells;
   a.n_cells = n_cells;
@@ -400,6 +420,34 @@ int zf_get_cells(zf_ctx* c, double* x, double* xn, int32_t* status) {
     ZF_CUDA(cudaMemcpyAsync(xn, a.xn, 3 * nc * a.nnn * 8, cudaMemcpyDeviceToHost, c->stream));
   if (status) ZF_CUDA(cudaMemcpyAsync(status, a.status, nc * 4, cudaMemcpyDeviceToHost, c->stream));
   ZF_CUDA(cudaStreamSynchronize(c->stream));
+  return ZF_OK;
+}
+
+
+int zf_get_cells_async(zf_ctx* c, double* x, double* xn, int32_t* status) {
+  if (!c) return ZF_ERR_ARG;
+  NEED(c->cells_set, "zf_get_cells_async", "cells not set");
+  if (!c->copy_stream) {
+    ZF_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    ZF_CUDA(cudaEventCreateWithFlags(&c->ev_ready, cudaEventDisableTiming));
+    ZF_CUDA(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
+  }
+  const CellArgs& a = c->cells;
+  const size_t nc = a.n_cells;
+  ZF_CUDA(cudaEventRecord(c->ev_ready, c->stream));
+  ZF_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_ready, 0));
+  if (x) ZF_CUDA(cudaMemcpyAsync(x, a.x, 3 * nc * a.nn * 8, cudaMemcpyDeviceToHost, c->copy_stream));
+  if (xn && a.nnn)
+    ZF_CUDA(cudaMemcpyAsync(xn, a.xn, 3 * nc * a.nnn * 8, cudaMemcpyDeviceToHost, c->copy_stream));
+  if (status) ZF_CUDA(cudaMemcpyAsync(status, a.status, nc * 4, cudaMemcpyDeviceToHost, c->copy_stream));
+  ZF_CUDA(cudaEventRecord(c->ev_copied, c->copy_stream));
+  c->copy_pending = true;
+  return ZF_OK;
+}
+
+int zf_wait_cells(zf_ctx* c) {
+  if (!c) return ZF_ERR_ARG;
+  if (c->copy_stream) ZF_CUDA(cudaEventSynchronize(c->ev_copied));
   return ZF_OK;
 }
 

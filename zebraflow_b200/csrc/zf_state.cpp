@@ -140,6 +140,10 @@ int zf_load_state(zf_ctx* c, const char* path) {
     const int rc = ib_prepare(c);
     if (rc) return rc;
   }
+  {
+    const int rc = cells_copy_wait_host(c);  // the cell buffers are about to be overwritten
+    if (rc) return rc;
+  }
   FILE* f = std::fopen(path, "rb");
   if (!f) {
     set_error("zf_load_state: cannot open %s", path);
