@@ -63,7 +63,9 @@ __device__ double block_sum(double v, double* red) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(256) k_membrane(CellArgs a) {
+// three blocks per SM (80 registers; the shared memory of a 642-node cell,
+// about 71 KB, also allows three)
+__global__ void __launch_bounds__(256, 3) k_membrane(CellArgs a) {
   const int cell = blockIdx.x;
   if (a.status[cell] <= -5000) return;
   const int nn = a.nn, nt = a.nt, ne = a.ne, nnn = a.nnn, nen = a.nen, nc = a.n_cells;

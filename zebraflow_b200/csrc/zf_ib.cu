@@ -1708,7 +1708,9 @@ __global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
 // happen once per node in the first pass.  A contribution outside the
 // neighbourhood (not expected) goes straight to BODYFORCE.
 constexpr int kSpreadNodes = 128;  // nodes staged per pass
-__global__ void __launch_bounds__(256) k_spread_tiles(IbArgs a, CellArgs c, int spread_walls) {
+// five blocks per SM (48 registers): the block waits on its shared-memory
+// atomics and barriers, and more resident blocks hide that
+__global__ void __launch_bounds__(256, 5) k_spread_tiles(IbArgs a, CellArgs c, int spread_walls) {
   __shared__ float acc[3][1728];
   __shared__ float s_f[3][kSpreadNodes];
   __shared__ StencilAxis s_ax[3][kSpreadNodes];  // per staged node: its stencil along x, y, z
