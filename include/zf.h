@@ -222,6 +222,18 @@ int zf_lbm_step_mass_noalloc(zf_ctx* ctx, int store_moments, int zero_bodyforce,
  * current state, in (x, y) order, into dev_buf ([n][5] storage elements: 4
  * bytes each for the fp32 forms, 2 for fp16/bf16; device memory, written on
  * the context's stream); zf_plane_unpack writes such a buffer into plane k. */
+/* No counterpart in the reference.  Slab stepping: a context holding a z slab
+ * with one tile layer (4 planes) of halo on either side declares its interior
+ * planes [k_lo, k_hi) (multiples of 4); its active tiles then split into the
+ * inner tile layers and the two face layers next to the halo, and the halo
+ * layers are not stepped.  zf_lbm_step_part(ctx, 0, 0) steps the inner layers,
+ * which read no halo plane, so it can run while the halo exchange of the
+ * previous step is in flight; zf_lbm_step_part(ctx, 1, 1) steps the face
+ * layers once the halo planes are unpacked and completes the step (wall pass,
+ * buffer swap, iteration count).  Neither stores moments or clears BODYFORCE. */
+int zf_set_slab(zf_ctx* ctx, int k_lo, int k_hi);
+int zf_lbm_step_part(zf_ctx* ctx, int part, int finish);
+
 int zf_plane_count(zf_ctx* ctx, int k, int32_t* n);
 int zf_plane_pack(zf_ctx* ctx, int k, int dir, void* dev_buf);
 int zf_plane_unpack(zf_ctx* ctx, int k, int dir, const void* dev_buf);

@@ -96,6 +96,8 @@ _SIGS = {
     "zf_set_cells": (C.c_int, [_P, C.c_int, _f64p, C.c_void_p]),
     "zf_get_cells": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
     "zf_get_cells_async": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "zf_set_slab": (C.c_int, [_P, C.c_int, C.c_int]),
+    "zf_lbm_step_part": (C.c_int, [_P, C.c_int, C.c_int]),
     "zf_wait_cells": (C.c_int, [_P]),
     "zf_get_cell_forces": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "zf_get_cell_kinematics": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -574,6 +576,12 @@ class Context:
     # steps -----------------------------------------------------------------
     def lbm_step(self, store_moments=True, zero_bodyforce=False):
         _check(lib().zf_lbm_step(self._h, int(store_moments), int(zero_bodyforce)))
+
+    def set_slab(self, k_lo: int, k_hi: int):
+        _check(lib().zf_set_slab(self._h, k_lo, k_hi))
+
+    def lbm_step_part(self, part: int, finish: bool):
+        _check(lib().zf_lbm_step_part(self._h, part, int(finish)))
 
     def lbm_steps(self, n: int):
         _check(lib().zf_lbm_steps(self._h, n))

@@ -104,6 +104,12 @@ static void free_lattice(zf_ctx* c) {
                   c->d_red,      c->d_u_pre};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  for (int part = 0; part < 2; ++part) {
+    if (c->d_active_part[part]) cudaFree(c->d_active_part[part]);
+    c->d_active_part[part] = nullptr;
+    c->n_active_part[part] = 0;
+  }
+  c->slab_set = false;
   for (auto& pl : c->planes) cudaFree(pl.d_slots);
   c->planes.clear();
   c->d_tile_map = c->d_active = c->d_nbr = nullptr;
@@ -490,6 +496,49 @@ int zf_lbm_step(zf_ctx* c, int store_moments, int zero_bodyforce) {
   NEED_LATTICE("zf_lbm_step");
   int rc = lbm_launch(c, store_moments, zero_bodyforce);
   if (rc == ZF_OK) c->status.iter++;
+  return rc;
+}
+
+int zf_set_slab(zf_ctx* c, int k_lo, int k_hi) {
+  NEED_LATTICE("zf_set_slab");
+  if (k_lo < ZF_TS || k_hi > c->p.nz - ZF_TS || k_lo % ZF_TS || k_hi % ZF_TS || k_hi - k_lo < ZF_TS) {
+    set_error("zf_set_slab: interior planes [%d, %d) must be whole 4-plane tile layers with at least one "
+              "layer of halo on either side (nz %d)", k_lo, k_hi, c->p.nz);
+    return ZF_ERR_ARG;
+  }
+  ZF_CUDA(cudaSetDevice(c->device));
+  std::vector<int32_t> active(c->n_active);
+  if (c->n_active)
+    ZF_CUDA(cudaMemcpy(active.data(), c->d_active, active.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  const int tz_lo = k_lo / ZF_TS, tz_hi = k_hi / ZF_TS - 1;
+  std::vector<int32_t> part[2];
+  for (int32_t t : active) {
+    const int tz = c->h_tile_origin[3 * (size_t)t + 2] / ZF_TS;
+    if (tz > tz_lo && tz < tz_hi) part[0].push_back(t);
+    else if (tz == tz_lo || tz == tz_hi) part[1].push_back(t);
+  }
+  for (int p = 0; p < 2; ++p) {
+    if (c->d_active_part[p]) cudaFree(c->d_active_part[p]);
+    c->d_active_part[p] = nullptr;
+    int rc = dev_alloc(c, (void**)&c->d_active_part[p], std::max<size_t>(part[p].size(), 1) * sizeof(int32_t));
+    if (rc) return rc;
+    if (!part[p].empty())
+      ZF_CUDA(cudaMemcpy(c->d_active_part[p], part[p].data(), part[p].size() * sizeof(int32_t),
+                         cudaMemcpyHostToDevice));
+    c->n_active_part[p] = (int)part[p].size();
+  }
+  c->slab_set = true;
+  return ZF_OK;
+}
+
+int zf_lbm_step_part(zf_ctx* c, int part, int finish) {
+  NEED_LATTICE("zf_lbm_step_part");
+  if (!c->slab_set || part < 0 || part > 1) {
+    set_error("zf_lbm_step_part: %s", c->slab_set ? "part is 0 (inner) or 1 (faces)" : "zf_set_slab first");
+    return ZF_ERR_ARG;
+  }
+  int rc = lbm_launch_part(c, part, finish);
+  if (rc == ZF_OK && finish) c->status.iter++;
   return rc;
 }
 

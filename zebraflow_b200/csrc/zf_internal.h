@@ -300,6 +300,12 @@ struct zf_ctx {
 
   int32_t* d_tile_map = nullptr;
   int32_t* d_active = nullptr;
+  // z-slab stepping (zf_set_slab): the active tiles of the inner tile layers
+  // [0] and of the two face layers next to the halo [1]; halo layers are not
+  // stepped
+  int32_t* d_active_part[2] = {nullptr, nullptr};
+  int n_active_part[2] = {0, 0};
+  bool slab_set = false;
   int32_t* d_nbr = nullptr;
   uint32_t* d_link = nullptr;
   uint8_t* d_code = nullptr;
@@ -358,6 +364,7 @@ struct zf_ctx {
 
 namespace zf {
 int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out = nullptr);
+int lbm_launch_part(zf_ctx* c, int part, int finish);
 int ensure_red(zf_ctx* c, int n);
 int lbm_step_mass_noalloc(zf_ctx* c, int store_moments, int zero_force, double* mass_out);
 int lbm_upload_populations(zf_ctx* c, const float* f);

@@ -671,15 +671,17 @@ struct LaunchStep {
     if (a.store_moments) k_lbm<C, I, true, false><<<grid, nt, 0, c->stream>>>(a);
     else k_lbm<C, I, false, false><<<grid, nt, 0, c->stream>>>(a);
   }
-  static void run(zf_ctx* c, const LbmArgs& a) {
-    if (c->n_active > 0) {
-      const int grid = (c->n_active + kTilesPerBlock - 1) / kTilesPerBlock;
+  // a.active / a.n_active: the tiles to step (all active tiles, or a part of
+  // them); walls: also run the reference wall pass
+  static void run(zf_ctx* c, const LbmArgs& a, bool walls = true) {
+    if (a.n_active > 0) {
+      const int grid = (a.n_active + kTilesPerBlock - 1) / kTilesPerBlock;
       if ((int64_t)ZF_Q * c->ns < (int64_t)INT32_MAX)
         launch_lbm<int32_t>(c, a, grid);
       else
         launch_lbm<int64_t>(c, a, grid);
     }
-    if (c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0)
+    if (walls && c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0)
       k_lbm_wall<C><<<(c->n_wall + 255) / 256, 256, 0, c->stream>>>(a, c->d_wall_slot,
                                                                     c->d_wall_nbr, c->n_wall);
   }
@@ -718,6 +720,22 @@ int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out) {
                             c->stream));
     ZF_CUDA(cudaStreamSynchronize(c->stream));
   }
+  return ZF_OK;
+}
+
+// One part of a slab step (zf_set_slab): the inner tile layers (part 0) or
+// the two face layers next to the halo (part 1); finish: the step is complete
+// (wall pass, swap of the population buffers).
+int lbm_launch_part(zf_ctx* c, int part, int finish) {
+  LbmArgs a = make_args(c);
+  a.active = c->d_active_part[part];
+  a.n_active = c->n_active_part[part];
+  a.store_moments = 0;
+  a.zero_force = 0;
+  dispatch_storage<LaunchStep>(c->p.storage, c, a, finish != 0);
+  ZF_CUDA(cudaGetLastError());
+  c->launches += (a.n_active > 0) + (finish && c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0);
+  if (finish) c->cur ^= 1;
   return ZF_OK;
 }
 

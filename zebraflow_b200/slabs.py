@@ -78,7 +78,11 @@ class SlabLBM:
         per[2] = 0
         self.ctx = Context(default_params(nx=nx, ny=ny, nz=self.nzs, periodic=tuple(per), **params), device)
         self.ctx.set_lattice(slab_lattice(b_index, world, rank))
+        # inner tile layers and the two face layers are stepped apart; the
+        # halo layers are not stepped
+        self.ctx.set_slab(HALO, self.nzs - HALO)
         self.stream = stream if stream is not None else torch.cuda.Stream(device=device)
+        self.comm = torch.cuda.Stream(device=device) if world > 1 else None
         self.ctx.set_stream(self.stream.cuda_stream)
         # planes (local z): bottom halo / first interior / last interior / top halo
         self.kb_halo, self.kb, self.kt, self.kt_halo = HALO - 1, HALO, self.nzs - HALO - 1, self.nzs - HALO
@@ -114,10 +118,23 @@ class SlabLBM:
         self.unpack()
 
     def step(self, n=1):
-        """n LBM steps of the slab, each followed by the halo exchange."""
+        """n LBM steps of the slab.  Each step packs the faces of the current
+        state and exchanges them while the inner tile layers are stepped (they
+        read no halo plane), then unpacks the halos and steps the two face
+        layers.  The halos of the final state are not filled."""
+        import torch
         for _ in range(n):
-            self.ctx.lbm_step(store_moments=False, zero_bodyforce=False)
-            self.exchange()
+            self.pack()
+            if self.world > 1:
+                self.comm.wait_stream(self.stream)
+                with torch.cuda.stream(self.comm):
+                    exchange_dist(self.send_dn, self.send_up, self.recv_dn, self.recv_up, self.rank,
+                                  self.world, self.group)
+            self.ctx.lbm_step_part(0, False)
+            if self.world > 1:
+                self.stream.wait_stream(self.comm)
+            self.unpack()
+            self.ctx.lbm_step_part(1, True)
 
     def interior(self, dom=None):
         """Mask of the slab's listed points that are interior, and their
