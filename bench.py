@@ -63,6 +63,9 @@ import numpy as np  # noqa: E402
 WORKLOADS = {
     # name: (nx, ny, nz, Rp, Rd, half_angle_deg, g, cells)
     "c1_bifurcation_256x256x1024_2000rbc": (256, 256, 1024, 30.0, 22.0, 20.0, 2e-6, 2000),
+    # the same box with radii doubled: the ~12 M fluid nodes the workload's
+    # description states (12,047,196), and 8000 cells for about its 20 % hematocrit
+    "c1x2_bifurcation_256x256x1024_r60_8000rbc": (256, 256, 1024, 60.0, 44.0, 20.0, 2e-6, 8000),
     "bifurcation_small_128x96x256_60rbc": (128, 96, 256, 15.0, 11.0, 20.0, 2e-6, 60),
 }
 DX_UM = 0.5
