@@ -1451,12 +1451,12 @@ __global__ void k_wall_nodes(IbArgs a, CellArgs c, int32_t* __restrict__ walk, i
   else if (rel > 0) walk[ntot - 1 - atomicAdd(&ctr[2], 1)] = (int32_t)gid;
 }
 
-// The queued nodes with wall-node lists, a warp per node: the lanes take each
-// list's candidates 32 at a time in list order, each lane keeping its first
-// strict minimum below 1.5 um and that candidate's position in the node's
-// scan; the warp then takes the smallest distance, ties to the earliest
-// position -- the first candidate in scan order that reaches the minimum,
-// which is what the reference's running minimum (strict <) ends on.
+// The queued nodes with wall-node lists, a warp per node: each lane scans
+// whole lists (lane l takes list l of every 32), keeping its first strict
+// minimum below 1.5 um and that candidate's position in the node's scan; the
+// warp then takes the smallest distance, ties to the earliest position -- the
+// first candidate in scan order that reaches the minimum, which is what the
+// reference's running minimum (strict <) ends on.
 __global__ void __launch_bounds__(kTileThreads) k_wall_lists(IbArgs a, CellArgs c, const int32_t* __restrict__ walk,
                                                             const int32_t* __restrict__ ctr, int32_t* __restrict__ work) {
   const unsigned FULL = 0xffffffffu;
@@ -1475,21 +1475,36 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_lists(IbArgs a, CellArgs 
     const int64_t s0 = slot_of(a, i0, j0, wrapk(a, k0));
     const int rel = a.wrel_cnt[s0];
     const int32_t* lists = a.wrel + a.wrel_off[s0];
+    // lane l scans list r0 + l of each chunk of 32 lists, in order; a
+    // candidate's position in the node's scan is the lists' running count
+    // before its list (a warp scan) plus its place in the list
     float best = 1.5f;
-    int bpos = INT_MAX, tbest = -1, pos = 0;
-    for (int r = 0; r < rel; ++r) {
-      const int m = lists[r];
-      const int32_t c0 = a.wcand_off[m - 1], c1 = a.wcand_off[m];
-      for (int i = c0 + lane; i < c1; i += 32) {
-        const float4 p = a.wcand[i];
+    int bpos = INT_MAX, tbest = -1, pos0 = 0;
+    for (int r0 = 0; r0 < rel; r0 += 32) {
+      int32_t c0 = 0, len = 0;
+      if (r0 + lane < rel) {
+        const int m = lists[r0 + lane];
+        c0 = a.wcand_off[m - 1];
+        len = a.wcand_off[m] - c0;
+      }
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int before = pos0 + incl - len;
+#pragma unroll 4
+      for (int i = 0; i < len; ++i) {
+        const float4 p = a.wcand[c0 + i];
         const float d = dist3(xp - p.x, yp - p.y, wrapd(zp - p.z, a.LZ));
         if (d < best) {
           best = d;
-          bpos = pos + (i - c0);
+          bpos = before + i;
           tbest = __float_as_int(p.w);
         }
       }
-      pos += c1 - c0;
+      pos0 += __shfl_sync(FULL, incl, 31);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
