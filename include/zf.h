@@ -430,6 +430,34 @@ int zf_flux_adjoint(zf_ctx* ctx, int nsteps, int t0, int t1, const int32_t* pts0
                     const int32_t* pts1, int n1, const float* nrm1, const float* fb, int checkpoint_interval,
                     double* J, float* dJ_dfb, double* dJ_dtau, double* dJ_dEs, double* dJ_dkb);
 
+/* The forward the four calls above differentiate.  move = 0 (the default):
+ * the cells stay at their positions over the window.  move = 1: the cells
+ * move -- the window is the reference time loop (zf_step, ZebraflowWT.c:
+ * 5646-12190) from the context's iteration, with BF_0 = S(x_0) F(x_0) + fb
+ * in effect until the first membrane iteration and fb added to every spread
+ * field; the adjoint carries the positions' adjoint through the position
+ * update (:11965-11997), interpolation (:8963-8996), spreading (:10745-10870)
+ * and the membrane and nucleus forces (:5749-7535), and holds the repulsion
+ * velocities (wall, nucleus-membrane, RBC-RBC) fixed: their dependence on the
+ * positions is not differentiated.  Memory: positions, spread forces and the
+ * spread field of every membrane iteration in the window are kept.  The calls
+ * leave the cells' positions, statuses, counters and nucleus-membrane lists
+ * as they were. */
+int zf_adjoint_move_cells(zf_ctx* ctx, int move);
+
+/* dJ/dx_0 and dJ/dxn_0 ([3][cells][nodes], um^-1 per unit of J) of the last
+ * adjoint run with moving cells, with respect to the positions the window
+ * started from. */
+int zf_adjoint_position_gradient(zf_ctx* ctx, float* dJ_dx, float* dJ_dxn);
+
+/* Vector-Jacobian product of the membrane and nucleus forces at the current
+ * positions (ZebraflowWT.c:5749-7535): given lam ([3][cells][nn], the weights
+ * of the membrane node forces) and lam_n ([3][cells][nnn] or NULL), returns
+ * dx = lam^T dF/dx, dxn = lam_n^T dF/dxn, and lam^T dF/dEs, lam^T dF/dkb.
+ * Any output may be NULL. */
+int zf_membrane_vjp(zf_ctx* ctx, const float* lam, const float* lam_n, float* dx, float* dxn, double* dEs,
+                    double* dkb);
+
 /* nsteps iterations of the reference time loop (ZebraflowWT.c:5646-12190):
  * every iteration an LBM step; every `stagger`-th iteration also the
  * membrane forces, IB interpolation, repulsions, spreading and position

@@ -70,6 +70,7 @@ def lib() -> C.CDLL:
                       "orc_world_update", "orc_world_destroy"):
                 g(n).argtypes = [C.c_void_p]
             g("orc_world_nuc_memb").argtypes = [C.c_void_p, C.c_int]
+            g("orc_world_set_exact").argtypes = [C.c_void_p, C.c_int]
             g("orc_world_step").argtypes = [C.c_void_p, C.c_int]
             g("orc_world_kinematics").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                   C.c_void_p]
@@ -283,6 +284,13 @@ class OracleWorld:
         uv = np.empty(3 * n, np.float32)
         self._fn("orc_world_get_wall")(self._h, _p(wi), _p(uv))
         return wi.reshape(shape), uv.reshape((3,) + tuple(shape))
+
+    def set_exact(self, on=True):
+        """Interpolation and spreading weights from the fp64 positions instead of
+        the reference's fp32 ones: the forward becomes smooth in the positions
+        below fp32 resolution, as finite-difference checks of position
+        derivatives need."""
+        self._fn("orc_world_set_exact")(self._h, int(bool(on)))
 
     def interp(self):
         self._fn("orc_world_interp")(self._h)

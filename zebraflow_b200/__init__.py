@@ -164,6 +164,10 @@ _SIGS = {
     "zf_flux_adjoint": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _i32p, C.c_int, _f32p, _i32p, C.c_int,
                                   _f32p, C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_void_p,
                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "zf_adjoint_move_cells": (C.c_int, [_P, C.c_int]),
+    "zf_adjoint_position_gradient": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "zf_membrane_vjp": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 
 
@@ -781,6 +785,30 @@ class Context:
                                      C.byref(J), g.ctypes.data_as(C.c_void_p), C.byref(gt), C.byref(ge),
                                      C.byref(gk)))
         return J.value, g, gt.value, ge.value, gk.value
+
+    def adjoint_move_cells(self, move=True):
+        """zf_adjoint_move_cells: the adjoint calls' forward moves the cells."""
+        _check(lib().zf_adjoint_move_cells(self._h, int(bool(move))))
+
+    def adjoint_position_gradient(self):
+        """(dJ/dx_0 [3][nc][nn], dJ/dxn_0 [3][nc][nnn]) of the last adjoint with
+        moving cells."""
+        g = np.empty((3, self.nc, self.nn), np.float32)
+        gn = np.empty((3, self.nc, self.nnn), np.float32) if self.nnn else None
+        _check(lib().zf_adjoint_position_gradient(self._h, _ptr(g), _ptr(gn)))
+        return g, gn
+
+    def membrane_vjp(self, lam, lam_n=None):
+        """(lam^T dF/dx, lam_n^T dF/dxn, lam^T dF/dEs, lam^T dF/dkb) of the
+        membrane and nucleus forces at the current positions (zf_membrane_vjp)."""
+        lam = np.ascontiguousarray(lam, np.float32)
+        ln = None if lam_n is None else np.ascontiguousarray(lam_n, np.float32)
+        g = np.empty((3, self.nc, self.nn), np.float32)
+        gn = np.empty((3, self.nc, self.nnn), np.float32) if self.nnn else None
+        ge, gk = C.c_double(), C.c_double()
+        _check(lib().zf_membrane_vjp(self._h, _ptr(lam), _ptr(ln), _ptr(g), _ptr(gn), C.byref(ge),
+                                     C.byref(gk)))
+        return g, gn, ge.value, gk.value
 
     def wss(self, node_normals=None, pgauge=120.0):
         """WSS [3][nw] (Pa), wall pressure [nw] (Pa), valid [nw] from the current

@@ -258,6 +258,21 @@ int lbm_moments_at(zf_ctx* c, const void* f, const PatchStencil& ps, float* d_U)
 // read); clears gU
 int lbm_seed_at(zf_ctx* c, const void* f, const PatchStencil& ps, float* d_gU, float* lam);
 int lbm_step_buffers(zf_ctx* c, const void* fin, void* fout, uint32_t step);
+// moments D, U, V, W of the populations f into the context's moment planes
+int lbm_moments_of(zf_ctx* c, const void* f);
+// the adjoint kernels of the cells (zf_adjoint_cells.cu):
+// gx += lam^T dF/dx, gxn += lam_n^T dF/dxn, gpar[0..1] += lam^T dF/d(Es, kb)
+// for the membrane and nucleus forces at the context's positions
+int membrane_vjp_launch(zf_ctx* c, const float* lam, const float* lam_n, float* gx, float* gxn, double* gpar);
+// transposed spreading of G (dJ/dBODYFORCE, or null), interpolation and
+// position update (lam_x: adjoint of the updated positions, or null) at the
+// context's positions: gF/gFn := adjoint of the spread node forces, gx/gxn +=
+// position terms, GU[3][ns] += dJ/dU; ftot..wrep_n: the forces the forward spread
+int ib_vjp_launch(zf_ctx* c, const float* G, const float* lam_x, const float* lam_xn, float* gx, float* gxn,
+                  float* gF, float* gFn, float* GU, const float* ftot, const float* ftot_n, const float* wrep,
+                  const float* wrep_n);
+// y[0..n) += x[0..n)
+int add_launch(zf_ctx* c, float* y, const float* x, int64_t n);
 int spread_adj_launch(zf_ctx* c, const float* d_G, float* d_gmem, float* d_gnuc);
 int scale_springs_launch(zf_ctx* c, float s);
 int wss_launch(zf_ctx* c, const float* d_normals, double pgauge, float* d_wss, float* d_press,
@@ -350,6 +365,11 @@ struct zf_ctx {
   bool nuc_lists_valid = false;    // nucleus-membrane lists built since the cells were set
   bool node_tiles_valid = false;   // node-tile lists match the current positions
   int tile_blocks = 0;             // persistent grid of the tile kernels
+
+  // adjoint: whether its forward moves the cells (zf_adjoint_cells), and the
+  // gradient of the last such adjoint with respect to the starting positions
+  bool adj_move_cells = false;
+  std::vector<float> adj_gx, adj_gxn;  // [3][nc][nn], [3][nc][nnn]
 
   // instrumentation: kernel launches, and optional event pairs around the LBM
   // kernel and the membrane block of zf_step

@@ -995,6 +995,16 @@ int lbm_adj_launch(zf_ctx* c, const void* f_pre, const float* lam, float* lam_pr
   return ZF_OK;
 }
 
+int lbm_moments_of(zf_ctx* c, const void* f) {
+  if (c->ns == 0) return ZF_OK;
+  LbmArgs a = make_args(c);
+  a.fin = f;
+  dispatch_storage<Moments>(c->p.storage, c, a);
+  ZF_CUDA(cudaGetLastError());
+  c->launches += 1;
+  return ZF_OK;
+}
+
 int lbm_moments_at(zf_ctx* c, const void* f, const PatchStencil& ps, float* d_U) {
   if (ps.nu <= 0) return ZF_OK;
   LbmArgs a = make_args(c);

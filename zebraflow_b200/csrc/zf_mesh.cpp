@@ -383,6 +383,8 @@ int zf_set_cells(zf_ctx* c, int n_cells, const double* x, const double* xn) {
   int rc0 = cells_copy_wait_host(c);  // a zf_get_cells_async copy may still read the old buffers
   if (rc0) return rc0;
   free_owned(c->cell_allocs);
+  c->adj_gx.clear();  // a position gradient belongs to the cells it was taken for
+  c->adj_gxn.clear();
   CellArgs& a = c->cells;
   a.n_cells = n_cells;
   const size_t nc = n_cells, nn = a.nn, nnn = a.nnn, nt = a.nt;
