@@ -583,7 +583,7 @@ def measure_adjoint(dev, stream, barrier, seed=2024, nsteps=500, t0=300, t1=500,
               "gradient_cost_over_forward": round((m_adj - m_fwd) / m_fwd, 3), "membrane_iterations": nsteps // 50,
               "J_pa": Jm, "dJ_dtau": mtau, "dJ_dEs": mEs, "dJ_dkb": mkb, "dJ_dfb_max": float(np.abs(mfb).max()),
               "dJ_dx0_max": float(np.abs(gx).max()),
-              "repulsions": "held (their position dependence is not differentiated)"}
+              "repulsions": "differentiated (wall, nucleus-membrane, RBC-RBC)"}
     ctx.set_stream(None)
     ctx.close()
     return {"workload": "c3_tube_96x96x512_200rbc", "fluid_points": int((b > 0).sum()),

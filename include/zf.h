@@ -438,8 +438,10 @@ int zf_flux_adjoint(zf_ctx* ctx, int nsteps, int t0, int t1, const int32_t* pts0
  * field; the adjoint carries the positions' adjoint through the position
  * update (:11965-11997), interpolation (:8963-8996), spreading (:10745-10870)
  * and the membrane and nucleus forces (:5749-7535), and holds the repulsion
- * velocities (wall, nucleus-membrane, RBC-RBC) fixed: their dependence on the
- * positions is not differentiated.  Memory: positions, spread forces and the
+ * velocities through the wall, nucleus-membrane and RBC-RBC repulsions
+ * (:9055-9077, :9516-9730, :9919-10053; their choices of wall triangle, list
+ * entries and facing triangles are held, as the derivative of the branch the
+ * forward took).  Memory: positions, spread forces and the
  * spread field of every membrane iteration in the window are kept.  The calls
  * leave the cells' positions, statuses, counters and nucleus-membrane lists
  * as they were. */
@@ -457,6 +459,17 @@ int zf_adjoint_position_gradient(zf_ctx* ctx, float* dJ_dx, float* dJ_dxn);
  * Any output may be NULL. */
 int zf_membrane_vjp(zf_ctx* ctx, const float* lam, const float* lam_n, float* dx, float* dxn, double* dEs,
                     double* dkb);
+
+/* Vector-Jacobian product of the repulsion velocities (NODE_WALLREPUL) of a
+ * membrane iteration at the current positions: the wall repulsion
+ * (ZebraflowWT.c:9055-9077, with the nucleus nodes' share, :9415-9430), the
+ * nucleus-membrane repulsion (:9516-9730, lists rebuilt at the current
+ * positions) and the RBC-RBC repulsion (:9919-10053): given lam_w
+ * ([3][cells][nn], the weights of the membrane nodes' repulsion velocities),
+ * returns dx = lam_w^T dwrep/dx and dxn = lam_w^T dwrep/dxn.  Overwrites the
+ * cells' forces, velocities and repulsion velocities, as a membrane iteration
+ * would. */
+int zf_repulsion_vjp(zf_ctx* ctx, const float* lam_w, float* dx, float* dxn);
 
 /* nsteps iterations of the reference time loop (ZebraflowWT.c:5646-12190):
  * every iteration an LBM step; every `stagger`-th iteration also the

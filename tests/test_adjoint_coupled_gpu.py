@@ -5,12 +5,14 @@ FP64 CPU oracle (oracle/orc_*.inc) running the same forward.
 
 1. The membrane and nucleus forces' vector-Jacobian product at deformed
    cells: lam^T dF/dx along a random direction, lam^T dF/dEs and dF/dkb.
-2. The coupled forward: a bounce-back tube from rest with two deformed cells
+2. The repulsion velocities' vector-Jacobian product (wall, nucleus-membrane,
+   RBC-RBC).
+3. The coupled forward: a bounce-back tube from rest with two deformed cells
    and the IB coupling every 10 iterations (the cells are interpolated,
    spread and moved 4 times in the window), J = mean |WSS| over a wall patch
    and steps 20..40.  Gradients with respect to tau, Es, kb, the body-force
    field (along a random direction) and the cells' starting positions (along
-   a random direction).
+   a random direction); once with the repulsions off, then with each on.
 
 The GPU adjoint runs in fp32 against the FP64 differences (measured: forces
 x 2e-6, xn 5e-6, Es 3e-6, kb 4e-6; coupled tau 3e-5, Es 1e-6, kb 9e-5,
@@ -166,8 +168,104 @@ def oracle_J(b, mesh, cells, wall, patch, nrm, fb, f0, **kw):
 TOL_COUPLED = 3e-4
 
 
-def test_coupled_adjoint_matches_fp64_finite_differences():
-    b, mesh, cells, wall, patch = case()
+def rep_case():
+    """Thick cells stacked 0.6 um apart along z, 0.15 um from the wall, with a
+    nucleus 0.15 um inside each membrane: the wall, nucleus-membrane and
+    RBC-RBC repulsions are all on, and their forward stays smooth under small
+    steps (facing surfaces, no rims in reach)."""
+    b = zf.gen_tube(NX, NY, NZ, CX, CY, R, True)
+    xyz, tri = zf.gen_icosphere(3)
+    xyzn, trin = zf.gen_icosphere(2)
+    rest = xyz * np.array([3.5, 2.25, 2.0])
+    rest_n = xyzn * np.array([1.25, 0.9, 1.85])
+    mesh = (rest, tri, rest_n, zf.mesh_edges(trin))
+    rng = np.random.default_rng(9)
+    cen = np.array([[14.1, 9.75, 6.0], [14.1, 9.75, 10.6]])
+    x = np.stack([(rest + c).T for c in cen], axis=1) + 0.02 * rng.standard_normal((3, 2, rest.shape[0]))
+    xn = np.stack([(rest_n + c).T for c in cen], axis=1)
+    wall = zf.gen_wall_tube(CX, CY, R, NZ)
+    z = wall[0][2]
+    patch = np.nonzero((z > 6.0) & (z < 16.0))[0].astype(np.int32)
+    return b, mesh, (x, xn), wall, patch
+
+
+def one_repulsion_case(kind):
+    """Thick cells with one repulsion on: "wall" (a cell 0.15 um from the
+    wall), "nuc" (nucleus 0.15 um inside its membrane), "rbc" (two cells
+    stacked 0.6 um apart)."""
+    b = zf.gen_tube(NX, NY, NZ, CX, CY, R, True)
+    xyz, tri = zf.gen_icosphere(3)
+    xyzn, trin = zf.gen_icosphere(2)
+    rest = xyz * np.array([3.5, 2.25, 2.0])
+    rest_n = xyzn * np.array([1.25, 0.9, 1.85 if kind == "nuc" else 1.2])
+    mesh = (rest, tri, rest_n, zf.mesh_edges(trin))
+    rng = np.random.default_rng(9)
+    cen = {"wall": [[14.1, 9.75, 6.0], [9.75, 9.75, 16.0]], "nuc": [[9.75, 9.75, 6.0], [9.75, 9.75, 16.0]],
+           "rbc": [[9.75, 9.75, 6.0], [9.75, 9.75, 10.6]]}[kind]
+    x = np.stack([(rest + np.array(c)).T for c in cen], axis=1) + 0.02 * rng.standard_normal((3, 2, rest.shape[0]))
+    xn = np.stack([(rest_n + np.array(c)).T for c in cen], axis=1)
+    wall = zf.gen_wall_tube(CX, CY, R, NZ)
+    z = wall[0][2]
+    patch = np.nonzero((z > 6.0) & (z < 16.0))[0].astype(np.int32)
+    return b, mesh, (x, xn), wall, patch
+
+
+def oracle_wrep(b, mesh, cells, base, wall):
+    """Repulsion velocities of one membrane iteration on the FP64 oracle from
+    the fp64 positions (nucleus-membrane lists built at `base`)."""
+    p = params()
+    lbm = OracleLBM(b, wall_mode=0, periodic=(0, 0, 1), tau=p.tau, g=tuple(p.g), precision="f64")
+    oc = OracleCells(*mesh, p, precision="f64")
+    w = OracleWorld(lbm, oc, p)
+    w.set_wall(*wall)
+    w.set_exact(True)
+    oc.set_cells(*base)
+    oc.forces()
+    w.nuc_memb(rebuild=True)
+    oc.set_cells(*cells)
+    oc.forces()
+    w.interp()
+    w.nuc_memb(rebuild=False)
+    w.rbc_rbc()
+    k = w.kinematics()[2]
+    for o in (w, oc, lbm):
+        o.close()
+    return k
+
+
+def test_repulsion_vjp_matches_fp64_finite_differences():
+    """zf_repulsion_vjp: the wall, nucleus-membrane and RBC-RBC repulsion
+    velocities' vector-Jacobian product (measured 2e-6 and 1e-6 relative)."""
+    b, mesh, cells, wall, _ = rep_case()
+    x, xn = cells
+    ctx = gpu_ctx(b, mesh, cells, wall)
+    rng = np.random.default_rng(7)
+    lam = rng.standard_normal(x.shape).astype(np.float32)
+    gx, gxn = ctx.repulsion_vjp(lam)
+    ctx.close()
+    parts = oracle_wrep(b, mesh, cells, cells, wall)
+    assert (np.abs(parts) > 0).any(axis=0).sum() > 50  # the repulsions are on
+    v = rng.standard_normal(x.shape)
+    vn = rng.standard_normal(xn.shape)
+    h = 1e-8
+    lf = lambda xx, xxn: float(np.sum(lam * oracle_wrep(b, mesh, (xx, xxn), cells, wall)))  # noqa: E731
+    fd = {"x.v": (lf(x + h * v, xn) - lf(x - h * v, xn)) / (2 * h),
+          "xn.vn": (lf(x, xn + h * vn) - lf(x, xn - h * vn)) / (2 * h)}
+    ad = {"x.v": float(np.sum(gx * v)), "xn.vn": float(np.sum(gxn * vn))}
+    print({k: (ad[k], fd[k], abs(ad[k] - fd[k]) / abs(fd[k])) for k in fd})
+    for k in fd:
+        assert fd[k] != 0.0
+        assert abs(ad[k] - fd[k]) <= TOL * abs(fd[k]), (k, ad[k], fd[k])
+
+
+@pytest.mark.parametrize("scene", ["clear", "wall", "nuc", "rbc"])
+def test_coupled_adjoint_matches_fp64_finite_differences(scene):
+    """clear: the repulsions stay off in the window; wall, nuc, rbc: that
+    repulsion acts on every membrane iteration (measured x_0 1e-6, 1e-5,
+    7e-6).  One scene per repulsion: in the scene with all three on
+    (rep_case) their position gradients cancel to a sixth of each, and the
+    agreement measured there was 9e-4."""
+    b, mesh, cells, wall, patch = case() if scene == "clear" else one_repulsion_case(scene)
     nrm = node_normals(*wall)
     ctx = gpu_ctx(b, mesh, cells, wall)
     ctx.adjoint_move_cells(True)
@@ -183,10 +281,9 @@ def test_coupled_adjoint_matches_fp64_finite_differences():
     ctx.close()
 
     Jo, kin = oracle_J(b, mesh, cells, wall, patch, nrm, fb, f0)
-    # the repulsions are held by the adjoint: in this window they stay off
-    print("repulsion velocities", np.abs(kin[2]).max(), np.abs(kin[3]).max(),
-          np.argwhere(np.abs(kin[2]) > 0)[:5])
-    assert np.abs(kin[2]).max() == 0.0 and np.abs(kin[3]).max() == 0.0
+    active = int((np.abs(kin[2]) > 0).any(axis=0).sum())
+    print("nodes with repulsion", active)
+    assert (active == 0) if scene == "clear" else (active > 5)
     assert J == pytest.approx(Jo, rel=1e-4)
     x, xn = cells
     P = params()

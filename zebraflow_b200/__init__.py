@@ -166,6 +166,7 @@ _SIGS = {
                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "zf_adjoint_move_cells": (C.c_int, [_P, C.c_int]),
     "zf_adjoint_position_gradient": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "zf_repulsion_vjp": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
     "zf_membrane_vjp": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
@@ -796,6 +797,15 @@ class Context:
         g = np.empty((3, self.nc, self.nn), np.float32)
         gn = np.empty((3, self.nc, self.nnn), np.float32) if self.nnn else None
         _check(lib().zf_adjoint_position_gradient(self._h, _ptr(g), _ptr(gn)))
+        return g, gn
+
+    def repulsion_vjp(self, lam_w):
+        """(lam_w^T dwrep/dx, lam_w^T dwrep/dxn) of the repulsion velocities of a
+        membrane iteration at the current positions (zf_repulsion_vjp)."""
+        lam_w = np.ascontiguousarray(lam_w, np.float32)
+        g = np.empty((3, self.nc, self.nn), np.float32)
+        gn = np.empty((3, self.nc, self.nnn), np.float32) if self.nnn else None
+        _check(lib().zf_repulsion_vjp(self._h, _ptr(lam_w), _ptr(g), _ptr(gn)))
         return g, gn
 
     def membrane_vjp(self, lam, lam_n=None):

@@ -484,10 +484,13 @@ int run_adjoint(zf_ctx* c, int nsteps, int t0, int t1, int K, Setup& S, double* 
 // transposed update, spreading and interpolation (k_ib_vjp) and the membrane
 // forces' vector-Jacobian product (k_membrane_vjp) carry the adjoint of the
 // positions, the spread field's dJ/dBF turns into dJ/dF, and the interpolation
-// seeds dJ/dU into the populations' adjoint.  The repulsion velocities (wall,
-// nucleus-membrane, RBC-RBC) are held: their position dependence is not
-// differentiated.  Positions, spread forces and the spread field of every
-// membrane iteration are kept (M + 1 snapshots for M membrane iterations).
+// seeds dJ/dU into the populations' adjoint, and the repulsion velocities'
+// adjoint goes through the transposed wall, nucleus-membrane and RBC-RBC
+// repulsions (k_wall_vjp, k_nuc_vjp, k_rbc_vjp) at the iteration's positions:
+// the backward re-forms the iteration's geometry, cell list, wall triangles
+// and nucleus-membrane lists there.  Positions, spread forces and the spread
+// field of every membrane iteration are kept (M + 1 snapshots for M membrane
+// iterations).
 
 namespace {
 
@@ -501,6 +504,7 @@ struct Coupled {
   size_t nxm = 0, nxn = 0;     // doubles of the membrane and nucleus positions
   size_t bf_bytes = 0, snap_bytes = 0;
   std::vector<Event> ev;
+  std::vector<char> rebuilt;   // the forward rebuilt the nucleus-membrane lists at event k
   DevBuf snaps;                // per event: x, xn (double), ftot, ftot_n, wrep, wrep_n (float), BF
   DevBuf fbdev;                // F_b in slot layout [3][ns]
   DevBuf save_x;               // positions at entry
@@ -530,6 +534,7 @@ int coupled_setup(zf_ctx* c, int nsteps, const float* fb, bool keep, Coupled& P)
   for (int t = 1; t <= nsteps; ++t)
     if ((iter0 + t) % c->p.stagger == 0) P.ev.push_back(Event{t, 0});
   for (size_t k = 0; k < P.ev.size(); ++k) P.ev[k].off = k * P.snap_bytes;
+  P.rebuilt.assign(P.ev.size(), 0);
   int rc;
   if (keep && (rc = P.snaps.alloc(c, P.ev.size() * P.snap_bytes))) return rc;
   if ((rc = P.fbdev.alloc(c, P.bf_bytes))) return rc;
@@ -626,6 +631,7 @@ int coupled_forward(zf_ctx* c, int nsteps, int t0, int t1, int K, Setup& S, Coup
     if (membrane) {
       const int64_t iter = iter0 + t;
       const bool rebuild = !c->nuc_lists_valid || (iter % c->p.nuc_list_period == 0);
+      P.rebuilt[k] = rebuild;
       ZF_CUDA(cudaMemsetAsync(c->d_force, 0, P.bf_bytes, c->stream));
       if ((rc = lbm_moments_of(c, fin)) || (rc = ib_interp_launch(c)) || (rc = ib_nuc_memb_launch(c, rebuild)))
         return rc;
@@ -665,7 +671,7 @@ int run_adjoint_coupled(zf_ctx* c, int nsteps, int t0, int t1, int K, const floa
   const size_t PB = S.pop_bytes;
   const size_t fl = (size_t)ZF_Q * c->ns * sizeof(float);
   const size_t nx = P.nxm + P.nxn;
-  DevBuf ck, seg, lam, lam2, gFc, gFb, gU, gw, lx, gFn, GU, gpar, allslots;
+  DevBuf ck, seg, lam, lam2, gFc, gFb, gU, gw, lx, gFn, GU, gpar, allslots, lw;
   if ((rc = ck.alloc(c, (size_t)nseg * PB)) || (rc = seg.alloc(c, (size_t)(K + 1) * PB))) return rc;
   if ((rc = lam.alloc(c, fl)) || (rc = lam2.alloc(c, fl))) return rc;
   if ((rc = gFc.alloc(c, P.bf_bytes)) || (rc = gFb.alloc(c, P.bf_bytes)) || (rc = GU.alloc(c, P.bf_bytes)))
@@ -674,7 +680,7 @@ int run_adjoint_coupled(zf_ctx* c, int nsteps, int t0, int t1, int K, const floa
   const int nb = lbm_adj_blocks(c);
   if ((rc = gw.alloc(c, (size_t)std::max(nb, 1) * sizeof(double)))) return rc;
   if ((rc = lx.alloc(c, nx * sizeof(float))) || (rc = gFn.alloc(c, nx * sizeof(float)))) return rc;
-  if ((rc = gpar.alloc(c, 2 * sizeof(double)))) return rc;
+  if ((rc = gpar.alloc(c, 2 * sizeof(double))) || (rc = lw.alloc(c, P.nxm * sizeof(float)))) return rc;
   // the seed of dJ/dU at every slot: a stencil of all slots
   PatchStencil all;
   {
@@ -721,17 +727,50 @@ int run_adjoint_coupled(zf_ctx* c, int nsteps, int t0, int t1, int K, const floa
   };
   // transposed membrane iteration k (spreading, forces; with interp: also
   // interpolation and update) at its positions
+  // nucleus-membrane lists as the forward used them at event k: built at the
+  // last rebuild event r <= k (at its positions), else the lists at entry
+  int lists_of = -2;  // event whose lists are loaded (-1: the entry lists)
+  auto load_lists = [&](int k) -> int {
+    int r = -1;
+    for (int i = k; i >= 1; --i)
+      if (P.rebuilt[i]) {
+        r = i;
+        break;
+      }
+    if (r == lists_of) return ZF_OK;
+    int e;
+    if (r < 0) {
+      if (P.save_lists.p) {
+        ZF_CUDA(cudaMemcpyAsync(c->ib.nuc_list, P.save_lists.p, P.list_bytes, cudaMemcpyDeviceToDevice,
+                                c->stream));
+        ZF_CUDA(cudaMemcpyAsync(c->ib.nuc_cnt, (char*)P.save_lists.p + P.list_bytes, P.cnt_bytes,
+                                cudaMemcpyDeviceToDevice, c->stream));
+      }
+    } else {
+      if ((e = put_positions(c, P, P.X(r))) || (e = cells_membrane_launch(c)) || (e = ib_nuc_memb_launch(c, 1)))
+        return e;
+    }
+    lists_of = r;
+    return ZF_OK;
+  };
   auto event_adj = [&](int k, const void* ft) -> int {
     int r;
-    if ((r = put_positions(c, P, P.X(k)))) return r;
     const float* F = P.F(k);
     const bool interp = k > 0;
-    if (interp && (r = lbm_moments_of(c, ft))) return r;
+    if (interp) {
+      // the iteration's geometry, wall triangles and cell list at its positions
+      if ((r = load_lists(k)) || (r = put_positions(c, P, P.X(k))) || (r = cells_membrane_launch(c)) ||
+          (r = lbm_moments_of(c, ft)) || (r = ib_interp_launch(c)) || (r = ib_bins_launch(c)))
+        return r;
+    } else if ((r = put_positions(c, P, P.X(k)))) {
+      return r;
+    }
     if ((r = ib_vjp_launch(c, (const float*)gFc.p, interp ? LX : nullptr, interp ? LXn : nullptr, LX, LXn, GFm,
-                           GFn, interp ? (float*)GU.p : nullptr, F, F + P.nxm, F + P.nxm + P.nxn,
-                           F + 2 * P.nxm + P.nxn)))
+                           GFn, interp ? (float*)GU.p : nullptr, interp ? (float*)lw.p : nullptr, F, F + P.nxm,
+                           F + P.nxm + P.nxn, F + 2 * P.nxm + P.nxn)))
       return r;
     if ((r = membrane_vjp_launch(c, GFm, GFn, LX, LXn, (double*)gpar.p))) return r;
+    if (interp && (r = repulsion_vjp_launch(c, (const float*)lw.p, LX, LXn))) return r;
     if ((r = add_launch(c, (float*)gFb.p, (const float*)gFc.p, 3 * c->ns))) return r;
     ZF_CUDA(cudaMemsetAsync(gFc.p, 0, P.bf_bytes, c->stream));
     if (interp && (r = lbm_seed_at(c, ft, all, (float*)GU.p, L))) return r;
@@ -804,6 +843,38 @@ int zf_adjoint_position_gradient(zf_ctx* c, float* dJ_dx, float* dJ_dxn) {
   }
   if (dJ_dx) std::copy(c->adj_gx.begin(), c->adj_gx.end(), dJ_dx);
   if (dJ_dxn) std::copy(c->adj_gxn.begin(), c->adj_gxn.end(), dJ_dxn);
+  return ZF_OK;
+}
+
+int zf_repulsion_vjp(zf_ctx* c, const float* lam_w, float* dx, float* dxn) {
+  if (!c || !lam_w) return ZF_ERR_ARG;
+  if (!c->cells_set || !c->lattice_set) {
+    set_error("zf_repulsion_vjp: lattice and cells must be set");
+    return ZF_ERR_STATE;
+  }
+  ZF_CUDA(cudaSetDevice(c->device));
+  const CellArgs& cl = c->cells;
+  const size_t nm = 3 * (size_t)cl.n_cells * cl.nn, nn_ = 3 * (size_t)cl.n_cells * cl.nnn;
+  int rc;
+  if (c->ib_allocs.empty() && (rc = ib_prepare(c))) return rc;
+  DevBuf b;
+  const size_t bytes = (2 * nm + nn_) * sizeof(float);
+  if ((rc = b.alloc(c, bytes))) return rc;
+  float* dl = (float*)b.p;
+  float* g = dl + nm;
+  float* gn = g + nm;
+  ZF_CUDA(cudaMemsetAsync(b.p, 0, bytes, c->stream));
+  ZF_CUDA(cudaMemcpyAsync(dl, lam_w, nm * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  // the membrane iteration's geometry, wall triangles, lists and cell list at
+  // the current positions (forces, velocities and repulsions are overwritten)
+  if ((rc = cells_membrane_launch(c)) || (rc = lbm_moments_launch(c)) || (rc = ib_interp_launch(c)) ||
+      (rc = ib_nuc_memb_launch(c, 1)) || (rc = ib_bins_launch(c)))
+    return rc;
+  c->nuc_lists_valid = true;
+  if ((rc = repulsion_vjp_launch(c, dl, g, gn))) return rc;
+  if (dx) ZF_CUDA(cudaMemcpyAsync(dx, g, nm * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  if (dxn && nn_) ZF_CUDA(cudaMemcpyAsync(dxn, gn, nn_ * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
   return ZF_OK;
 }
 

@@ -584,6 +584,7 @@ struct IbVjpArgs {
   float* gF;             // [3][nc][nn]  := adjoint of the spread node forces
   float* gFn;            // [3][nc][nnn]
   float* GU;             // [3][ns] += dJ/dU (fluid points), with lam_x
+  float* lam_w;          // [3][nc][nn] := adjoint of the membrane nodes' repulsion velocities, or null
   const float* ftot;     // the spread forces: gamma_p wrep + ftot, as the forward formed them
   const float* ftot_n;
   const float* wrep;
@@ -606,7 +607,10 @@ __global__ void k_ib_vjp(IbArgs a, CellArgs c, IbVjpArgs v) {
   auto at = [&](int q) { return ((size_t)q * nc + cell) * n + node; };
   float* gF = nuc ? v.gFn : v.gF;
   if (c.status[cell] <= 0) {
-    for (int q = 0; q < 3; ++q) gF[at(q)] = 0.f;
+    for (int q = 0; q < 3; ++q) {
+      gF[at(q)] = 0.f;
+      if (v.lam_w && !nuc) v.lam_w[at(q)] = 0.f;
+    }
     return;
   }
   const double* X = nuc ? c.xn : c.x;
@@ -674,22 +678,275 @@ __global__ void k_ib_vjp(IbArgs a, CellArgs c, IbVjpArgs v) {
   }
   float* GX = nuc ? v.gxn : v.gx;
   for (int q = 0; q < 3; ++q) {
-    gF[at(q)] = (float)(gf[q] * fs);
+    const float g = (float)(gf[q] * fs);
+    gF[at(q)] = g;
     GX[at(q)] += (float)gp[q];
+    // the repulsion velocity wrep moves the node (update) and is spread as
+    // gamma_p wrep (:10749-10754)
+    if (v.lam_w && !nuc) v.lam_w[at(q)] = lu[q] + a.gamma_p * g;
   }
 }
 
 int ib_vjp_launch(zf_ctx* ctx, const float* G, const float* lam_x, const float* lam_xn, float* gx, float* gxn,
-                  float* gF, float* gFn, float* GU, const float* ftot, const float* ftot_n, const float* wrep,
-                  const float* wrep_n) {
+                  float* gF, float* gFn, float* GU, float* lam_w, const float* ftot, const float* ftot_n,
+                  const float* wrep, const float* wrep_n) {
   const CellArgs& c = ctx->cells;
   const int64_t n = (int64_t)c.n_cells * (c.nn + c.nnn);
   if (n == 0) return ZF_OK;
-  IbVjpArgs v{G, lam_x, lam_xn, gx, gxn, gF, gFn, GU, ftot, ftot_n, wrep, wrep_n,
+  IbVjpArgs v{G, lam_x, lam_xn, gx, gxn, gF, gFn, GU, lam_w, ftot, ftot_n, wrep, wrep_n,
               ctx->p.wall_mode == ZF_WALL_REF_EQ};
   k_ib_vjp<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c, v);
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 1;
+  return ZF_OK;
+}
+
+// ---- repulsions --------------------------------------------------------------------
+
+namespace {
+
+__device__ __forceinline__ float wrapd_(float d, float L) {
+  if (L > 0.f) {
+    if (d > 0.5f * L) d -= L;
+    else if (d < -0.5f * L) d += L;
+  }
+  return d;
+}
+__device__ __forceinline__ float d3_(float dx, float dy, float dz) {
+  return sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
+}
+__device__ __forceinline__ float rec_rb_(float w) { return (float)(__float_as_uint(w) >> 8) * (1.f / 1048576.f); }
+__device__ __forceinline__ void npos(const IbArgs& a, const double* X, int nc, int n, int cell, int node, float& xp,
+                                     float& yp, float& zp) {
+  xp = (float)X[((size_t)0 * nc + cell) * n + node];
+  yp = (float)X[((size_t)1 * nc + cell) * n + node];
+  double z = X[((size_t)2 * nc + cell) * n + node];
+  if (a.LZ > 0.f) z -= (double)a.LZ * floor((z - a.Z0) / (double)a.LZ);
+  zp = (float)z;
+}
+
+// barycentric weights of the 15 points of the subdivided triangle (1-based,
+// ZebraflowWT.c:9981-10027, as k_rbc_rbc's rbc_entry forms them)
+__device__ __forceinline__ void sub_points(float (&b)[16][3]) {
+  for (int k = 0; k < 16; ++k) b[k][0] = b[k][1] = b[k][2] = 0.f;
+  b[1][0] = b[2][1] = b[3][2] = 1.f;
+  const int pa[12] = {1, 2, 1, 1, 2, 2, 5, 3, 6, 4, 4, 5}, pb[12] = {2, 3, 3, 4, 4, 5, 3, 6, 1, 6, 5, 6};
+  for (int k = 0; k < 12; ++k)
+    for (int q = 0; q < 3; ++q) b[4 + k][q] = 0.5f * (b[pa[k]][q] + b[pb[k]][q]);
+}
+
+}  // namespace
+
+// RBC-RBC repulsion (ZebraflowWT.c:9919-10053; k_rbc_rbc's search, one thread
+// per membrane node): wrep += f(r) = -K (1 - d)/d r, r = c_sub - x, d = |r| < 1,
+// over the facing triangles near the node.  With J = df/dr = -K ((1-d)/d I -
+// r r^T / d^3) (symmetric): gx(node) -= J lam, gx(vertex i) += alpha_i J lam,
+// alpha the sub-centroid's barycentric weights.
+__global__ void k_rbc_vjp(IbArgs a, CellArgs c, const float* __restrict__ lam_w, float* gx) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  if (gid >= (int64_t)nc * c.nn) return;
+  const int cell = (int)(gid / c.nn), node = (int)(gid % c.nn);
+  if (c.status[cell] <= 0) return;
+  auto at = [&](int q, int m, int i) { return ((size_t)q * nc + m) * c.nn + i; };
+  const float lx = lam_w[at(0, cell, node)], ly = lam_w[at(1, cell, node)], lz = lam_w[at(2, cell, node)];
+  if (lx == 0.f && ly == 0.f && lz == 0.f) return;
+  float xc, yc, zc;
+  npos(a, c.x, nc, c.nn, cell, node, xc, yc, zc);
+  const float e1x = c.node_normal[at(0, cell, node)], e1y = c.node_normal[at(1, cell, node)],
+              e1z = c.node_normal[at(2, cell, node)];
+  const int i0 = (int)floor(((double)xc - a.X0) / a.DX + 1.01) - 1;
+  const int j0 = (int)floor(((double)yc - a.Y0) / a.DX + 1.01) - 1;
+  const int k0 = (int)floor(((double)zc - a.Z0) / a.DX + 1.01) - 1;
+  const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1), j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
+  const int k1 = a.per_z ? k0 - 4 : max(k0 - 4, 2), k2 = a.per_z ? k0 + 4 : min(k0 + 4, a.nz - 4);
+  if (i1 > i2 || j1 > j2 || k1 > k2) return;
+  float bw[16][3];
+  sub_points(bw);
+  constexpr int kA[16] = {1, 7, 7, 4, 4, 8, 8, 12, 13, 13, 14, 14, 6, 15, 15, 11};
+  constexpr int kB[16] = {7, 13, 4, 14, 8, 9, 2, 13, 15, 14, 5, 9, 15, 10, 5, 10};
+  constexpr int kC[16] = {12, 12, 13, 13, 14, 14, 9, 6, 6, 15, 15, 5, 11, 11, 10, 3};
+  const int64_t stride = (int64_t)nc * c.nt, n_pop_tiles = a.ns / ZF_TC;
+  const float K = 8.333e-07f;
+  float gn[3] = {0.f, 0.f, 0.f};
+  for (int ci = i1; ci <= i2; ++ci)
+    for (int cj = j1; cj <= j2; ++cj)
+      for (int ck = k1; ck <= k2; ++ck) {
+        const int kw = a.per_z ? ((ck % a.nz) + a.nz) % a.nz : ck;
+        const int t = a.tile_map[((kw >> 2) * a.nty + (cj >> 2)) * a.ntx + (ci >> 2)];
+        if (t < 0 || t >= n_pop_tiles) continue;
+        const int64_t key = (int64_t)t * ZF_TC + 16 * (ci & 3) + 4 * (cj & 3) + (kw & 3);
+        for (int e = a.bin_off[key]; e < a.bin_off[key + 1]; ++e) {
+          const float4 cr = a.bin_rec[2 * e];
+          const float dzc = wrapd_(cr.z - zc, a.LZ);
+          const float dcen = d3_(xc - cr.x, yc - cr.y, -dzc);
+          if (!(dcen < 2.f) || dcen - rec_rb_(cr.w) > 1.f) continue;
+          const float4 nr = a.bin_rec[2 * e + 1];
+          if (!(e1x * nr.x + e1y * nr.y + e1z * nr.z < 0.f)) continue;
+          const int g = __float_as_int(nr.w);
+          const int m = g / c.nt, tri = g - m * c.nt;
+          if (m == cell && (c.tri[3 * tri] == node || c.tri[3 * tri + 1] == node || c.tri[3 * tri + 2] == node))
+            continue;
+          const float4 v1 = a.bin_v[e], v2 = a.bin_v[stride + e], v3 = a.bin_v[2 * stride + e];
+          const float shift = (cr.z - zc) - dzc;
+          const float P[3][3] = {{v1.x, v1.y, v1.z - shift}, {v2.x, v2.y, v2.z - shift}, {v3.x, v3.y, v3.z - shift}};
+          const int vid[3] = {__float_as_int(v1.w), __float_as_int(v2.w), __float_as_int(v3.w)};
+          float gv[3][3] = {};
+          for (int v = 0; v < 16; ++v) {
+            float al[3], r[3];
+            for (int q = 0; q < 3; ++q) al[q] = (bw[kA[v]][q] + bw[kB[v]][q] + bw[kC[v]][q]) * (1.f / 3.f);
+            for (int q = 0; q < 3; ++q) r[q] = al[0] * P[0][q] + al[1] * P[1][q] + al[2] * P[2][q];
+            r[0] -= xc;
+            r[1] -= yc;
+            r[2] -= zc;
+            const float d2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+            if (!(d2 < 1.f)) continue;
+            const float d = sqrtf(d2);
+            if (!(d < 1.f) || !(d > 0.f)) continue;
+            const float aI = -K * (1.f - d) / d, bR = K / (d2 * d);
+            const float rl = r[0] * lx + r[1] * ly + r[2] * lz;
+            const float Jl[3] = {aI * lx + bR * r[0] * rl, aI * ly + bR * r[1] * rl, aI * lz + bR * r[2] * rl};
+            for (int q = 0; q < 3; ++q) {
+              gn[q] -= Jl[q];
+              for (int i = 0; i < 3; ++i) gv[i][q] += al[i] * Jl[q];
+            }
+          }
+          for (int i = 0; i < 3; ++i)
+            for (int q = 0; q < 3; ++q)
+              if (gv[i][q] != 0.f) atomicAdd(&gx[at(q, m, vid[i])], gv[i][q]);
+        }
+      }
+  for (int q = 0; q < 3; ++q)
+    if (gn[q] != 0.f) atomicAdd(&gx[at(q, cell, node)], gn[q]);
+}
+
+// wall repulsion (ZebraflowWT.c:9055-9077): wrep += (0.25 - dist) 1e-4 n for
+// -0.75 <= dist < 0.25, dist = (x - w1) . n the signed distance to the plane of
+// the node's wall triangle (constant 1e-4 n below -0.75): gx -= 1e-4 (n . lam) n.
+// Nucleus nodes add to the membrane node of their own index (as the forward).
+__global__ void k_wall_vjp(IbArgs a, CellArgs c, const float* __restrict__ lam_w, float* gx, float* gxn) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  const int64_t nmem = (int64_t)nc * c.nn;
+  const bool nuc = gid >= nmem;
+  if (gid >= nmem + (int64_t)nc * c.nnn) return;
+  const int n = nuc ? c.nnn : c.nn;
+  const int64_t lid = nuc ? gid - nmem : gid;
+  const int cell = (int)(lid / n), node = (int)(lid % n);
+  if (c.status[cell] <= 0 || node >= c.nn) return;
+  const int tw = a.wall_tri[gid];
+  if (tw < 0) return;
+  float xp, yp, zp;
+  npos(a, nuc ? c.xn : c.x, nc, n, cell, node, xp, yp, zp);
+  const int w1 = a.wtri[3 * tw];
+  const float n0 = a.wnrm[tw], n1 = a.wnrm[a.mt + tw], n2 = a.wnrm[2 * a.mt + tw];
+  const float ddx = xp - a.wxyz[w1], ddy = yp - a.wxyz[a.nw + w1], ddz = wrapd_(zp - a.wxyz[2 * a.nw + w1], a.LZ);
+  const float dist = __fadd_rn(__fadd_rn(__fmul_rn(ddx, n0), __fmul_rn(ddy, n1)), __fmul_rn(ddz, n2));
+  if (!(dist < 0.25f && fabsf(dist) < 1.0f) || dist < -0.75f) return;
+  const size_t m = (size_t)cell * c.nn + node;
+  const float nl = n0 * lam_w[m] + n1 * lam_w[nmem + m] + n2 * lam_w[2 * nmem + m];
+  float* G = nuc ? gxn : gx;
+  const int64_t stride = nuc ? (int64_t)nc * c.nnn : nmem;
+  G[lid] -= 1.e-4f * nl * n0;
+  G[stride + lid] -= 1.e-4f * nl * n1;
+  G[2 * stride + lid] -= 1.e-4f * nl * n2;
+}
+
+// nucleus-membrane repulsion (ZebraflowWT.c:9516-9730; k_nuc_memb, one thread
+// per nucleus node, over its current list): for each listed triangle within
+// 1 um and each of its 19 sample points tp within d <= 0.2 of the nucleus node
+// xc, the triangle's three nodes get wrep += repulf n / 3, repulf = (0.2 - d)/0.2
+// 4.1666667e-7, n the triangle's unit normal.  Differentiated in 12-tangent
+// duals (the three vertices, xc).
+__global__ void k_nuc_vjp(IbArgs a, CellArgs c, const float* __restrict__ lam_w, float* gx, float* gxn) {
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.n_cells;
+  if (gid >= (int64_t)nc * c.nnn) return;
+  const int cell = (int)(gid / c.nnn), node = (int)(gid % c.nnn);
+  if (c.status[cell] <= 0) return;
+  using D = Dl<12>;
+  using V = V3d<12>;
+  auto atm = [&](int q, int i) { return ((size_t)q * nc + cell) * c.nn + i; };
+  auto atn = [&](int q) { return ((size_t)q * nc + cell) * c.nnn + node; };
+  const float xcf = (float)c.xn[atn(0)], ycf = (float)c.xn[atn(1)], zcf = (float)c.xn[atn(2)];
+  const V xc = {var<12>(xcf, 9), var<12>(ycf, 10), var<12>(zcf, 11)};
+  const uint16_t* list = a.nuc_list + (size_t)gid * a.nuc_cap;
+  const int cnt = a.nuc_cnt[gid];
+  float gnode[3] = {0.f, 0.f, 0.f};
+  for (int l = 0; l < cnt; ++l) {
+    const int tri = list[l];
+    const int nd[3] = {c.tri[3 * tri], c.tri[3 * tri + 1], c.tri[3 * tri + 2]};
+    float L[3] = {0.f, 0.f, 0.f};
+    for (int k = 0; k < 3; ++k)
+      for (int q = 0; q < 3; ++q) L[q] += lam_w[atm(q, nd[k])];
+    if (L[0] == 0.f && L[1] == 0.f && L[2] == 0.f) continue;
+    V p[3];
+    for (int k = 0; k < 3; ++k)
+      p[k] = {var<12>((float)c.x[atm(0, nd[k])], 3 * k), var<12>((float)c.x[atm(1, nd[k])], 3 * k + 1),
+              var<12>((float)c.x[atm(2, nd[k])], 3 * k + 2)};
+    D ar;
+    V nrm, cen;
+    tri_geom(p[0], p[1], p[2], ar, nrm, cen);
+    if (!(d3_(xcf - cen.x.v, ycf - cen.y.v, zcf - cen.z.v) < 1.f)) continue;
+    // 19 sample points as k_nuc_memb forms them: vertices' midpoints ep, then tp
+    V ep[10], tp[20];
+    ep[1] = vmul(0.5f, vadd(p[0], p[1]));
+    ep[2] = vmul(0.5f, vadd(p[1], p[2]));
+    ep[3] = vmul(0.5f, vadd(p[2], p[0]));
+    ep[4] = vmul(0.5f, vadd(p[0], ep[1]));
+    ep[5] = vmul(0.5f, vadd(ep[1], p[1]));
+    ep[6] = vmul(0.5f, vadd(p[1], ep[2]));
+    ep[7] = vmul(0.5f, vadd(ep[2], p[2]));
+    ep[8] = vmul(0.5f, vadd(p[2], ep[3]));
+    ep[9] = vmul(0.5f, vadd(ep[3], p[0]));
+    const float third = 1.f / 3.f;
+    tp[1] = vmul(third, vadd(vadd(p[0], p[1]), p[2]));
+    tp[2] = vmul(third, vadd(vadd(ep[3], p[0]), ep[1]));
+    tp[3] = vmul(third, vadd(vadd(ep[1], p[1]), ep[2]));
+    tp[4] = vmul(third, vadd(vadd(ep[2], p[2]), ep[3]));
+    tp[5] = vmul(0.5f, vadd(ep[1], ep[3]));
+    tp[6] = vmul(0.5f, vadd(ep[1], ep[2]));
+    tp[7] = vmul(0.5f, vadd(ep[2], ep[3]));
+    tp[8] = vmul(0.5f, vadd(p[0], tp[2]));
+    tp[9] = vmul(0.5f, vadd(ep[1], tp[2]));
+    tp[10] = vmul(0.5f, vadd(ep[3], tp[2]));
+    tp[11] = vmul(0.5f, vadd(ep[1], tp[3]));
+    tp[12] = vmul(0.5f, vadd(p[1], tp[3]));
+    tp[13] = vmul(0.5f, vadd(ep[2], tp[3]));
+    tp[14] = vmul(0.5f, vadd(ep[3], tp[4]));
+    tp[15] = vmul(0.5f, vadd(ep[2], tp[4]));
+    tp[16] = vmul(0.5f, vadd(p[2], tp[4]));
+    tp[17] = vmul(0.5f, vadd(ep[1], tp[1]));
+    tp[18] = vmul(0.5f, vadd(ep[2], tp[1]));
+    tp[19] = vmul(0.5f, vadd(ep[3], tp[1]));
+    float acc[12];
+    for (int k = 0; k < 12; ++k) acc[k] = 0.f;
+    for (int v = 1; v <= 19; ++v) {
+      const V r = vsub(tp[v], xc);
+      const D d = dsqrt(vdot(r, r));
+      if (!(d.v <= 0.2f)) continue;
+      const D rf = (4.1666667e-07f / 0.2f) * (cst<12>(0.2f) - d);
+      vjp_acc(acc, vmul(third, vmul(rf, nrm)), L[0], L[1], L[2]);
+    }
+    for (int k = 0; k < 3; ++k)
+      for (int q = 0; q < 3; ++q)
+        if (acc[3 * k + q] != 0.f) atomicAdd(&gx[atm(q, nd[k])], acc[3 * k + q]);
+    for (int q = 0; q < 3; ++q) gnode[q] += acc[9 + q];
+  }
+  for (int q = 0; q < 3; ++q)
+    if (gnode[q] != 0.f) atomicAdd(&gxn[atn(q)], gnode[q]);
+}
+
+int repulsion_vjp_launch(zf_ctx* ctx, const float* lam_w, float* gx, float* gxn) {
+  const CellArgs& c = ctx->cells;
+  const int64_t nm = (int64_t)c.n_cells * c.nn, nn_ = (int64_t)c.n_cells * c.nnn;
+  if (nm == 0) return ZF_OK;
+  k_rbc_vjp<<<(unsigned)((nm + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c, lam_w, gx);
+  if (ctx->ib.nw > 0 && ctx->ib.wall_tri)
+    k_wall_vjp<<<(unsigned)((nm + nn_ + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c, lam_w, gx, gxn);
+  if (nn_ > 0) k_nuc_vjp<<<(unsigned)((nn_ + 127) / 128), 128, 0, ctx->stream>>>(ctx->ib, c, lam_w, gx, gxn);
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 3;
   return ZF_OK;
 }
 

@@ -158,6 +158,7 @@ __global__ void k_ib_interp(IbArgs a, CellArgs c) {
   const int n = nuc ? c.nnn : c.nn;
   const int64_t lid = nuc ? gid - nmem : gid;
   const int cell = (int)(lid / n), node = (int)(lid % n);
+  if (a.wall_tri) a.wall_tri[gid] = -1;  // the wall search that follows sets it
   if (c.status[cell] <= 0) return;
   const double* X = nuc ? c.xn : c.x;
   float xp, yp, zp;
@@ -366,6 +367,7 @@ __global__ void __launch_bounds__(kRepWarps * 32) k_ib_wall(IbArgs a, CellArgs c
   if (qn > 0) batch(qn);
   if (!active) return;
   if (triwall < 0) return;
+  if (a.wall_tri) a.wall_tri[gid] = triwall;  // for the adjoint
   // signed distance to the plane of the wall triangle, repulsion, :9055-9077
   const int w1 = a.wtri[3 * triwall];
   const float n0 = a.wnrm[triwall], n1 = a.wnrm[a.mt + triwall], n2 = a.wnrm[2 * a.mt + triwall];
@@ -1399,9 +1401,10 @@ __global__ void k_wall_rel(IbArgs a, int32_t* __restrict__ cnt, int32_t* __restr
   }
 }
 
-__device__ __forceinline__ void wall_repel(const IbArgs& a, const CellArgs& c, int cell, int node, float xp,
-                                           float yp, float zp, int triwall) {
+__device__ __forceinline__ void wall_repel(const IbArgs& a, const CellArgs& c, int64_t gid, int cell, int node,
+                                           float xp, float yp, float zp, int triwall) {
   // signed distance to the plane of the wall triangle, repulsion, :9055-9077
+  if (a.wall_tri) a.wall_tri[gid] = triwall;  // for the adjoint
   const int nc = c.n_cells;
   const int w1 = a.wtri[3 * triwall];
   const float n0 = a.wnrm[triwall], n1 = a.wnrm[a.mt + triwall], n2 = a.wnrm[2 * a.mt + triwall];
@@ -1516,7 +1519,7 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_lists(IbArgs a, CellArgs 
         tbest = ot;
       }
     }
-    if (lane == 0 && tbest >= 0) wall_repel(a, c, cell, node, xp, yp, zp, tbest);
+    if (lane == 0 && tbest >= 0) wall_repel(a, c, gid, cell, node, xp, yp, zp, tbest);
   }
 }
 
@@ -1674,7 +1677,7 @@ __global__ void __launch_bounds__(kTileThreads) k_wall_walk(IbArgs a, CellArgs c
       }
       while (qn > 0) flush(min(qn, 32));
     }
-    if (triwall >= 0 && lane == 0) wall_repel(a, c, cell, node, xp, yp, zp, triwall);
+    if (triwall >= 0 && lane == 0) wall_repel(a, c, gid, cell, node, xp, yp, zp, triwall);
   }
 }
 

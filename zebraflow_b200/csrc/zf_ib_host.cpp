@@ -170,6 +170,7 @@ int ib_buffers(zf_ctx* c) {
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.node_sorted, nnodes))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.wall_walk, nnodes))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.wall_walk_ctr, 4))) return rc;
+  if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.wall_tri, nnodes))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.tile_list, std::min(a.ngrid, nnodes)))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.tile_ctr, 4))) return rc;
   if ((rc = dalloc<int32_t>(c, c->ib_allocs, &a.node_bsum, (ng1 + 1023) / 1024 + 1))) return rc;

@@ -185,6 +185,7 @@ struct IbArgs {
   int32_t* wall_walk;           // [n_cells*(nn+nnn)] nodes queued for the window walk (from the
                                 // front) and for the warp scan of their wall-node lists (from the back)
   int32_t* wall_walk_ctr;       // [4] walk: queued count, work counter; lists: queued count, work counter
+  int32_t* wall_tri;            // [n_cells*(nn+nnn)] the wall triangle of each node's repulsion, -1 none
   const int32_t* wcand_off;     // [nw+1] WallHost::cand_off
   const float4* wcand;          // WallHost::cand
   // cell list of triangle centroids over population slots (CSR).  Bin keys
@@ -269,8 +270,13 @@ int membrane_vjp_launch(zf_ctx* c, const float* lam, const float* lam_n, float* 
 // context's positions: gF/gFn := adjoint of the spread node forces, gx/gxn +=
 // position terms, GU[3][ns] += dJ/dU; ftot..wrep_n: the forces the forward spread
 int ib_vjp_launch(zf_ctx* c, const float* G, const float* lam_x, const float* lam_xn, float* gx, float* gxn,
-                  float* gF, float* gFn, float* GU, const float* ftot, const float* ftot_n, const float* wrep,
-                  const float* wrep_n);
+                  float* gF, float* gFn, float* GU, float* lam_w, const float* ftot, const float* ftot_n,
+                  const float* wrep, const float* wrep_n);
+// transposed repulsions at the context's positions: gx/gxn += lam_w^T
+// d(wrep)/d(x, xn) of the wall (the triangles the last interpolation chose),
+// nucleus-membrane (the current lists) and RBC-RBC repulsions (the current
+// cell list); lam_w [3][nc][nn]: the adjoint of the membrane repulsion velocities
+int repulsion_vjp_launch(zf_ctx* c, const float* lam_w, float* gx, float* gxn);
 // y[0..n) += x[0..n)
 int add_launch(zf_ctx* c, float* y, const float* x, int64_t n);
 int spread_adj_launch(zf_ctx* c, const float* d_G, float* d_gmem, float* d_gnuc);
