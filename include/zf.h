@@ -471,6 +471,27 @@ int zf_membrane_vjp(zf_ctx* ctx, const float* lam, const float* lam_n, float* dx
  * would. */
 int zf_repulsion_vjp(zf_ctx* ctx, const float* lam_w, float* dx, float* dxn);
 
+/* The coupled step on a lattice split into z slabs (one context per slab, no
+ * counterpart in the reference).  The context's lattice is its slab with
+ * halo planes, not periodic in z; every context holds all cells (positions in
+ * the global frame), the wall mesh with its z folded into the frame
+ * [origin z, origin z + lz), and:
+ *   zf_set_ib_slab: the planes [k_lo, k_hi) this slab owns (at least 8 halo
+ *     planes on either side) and the period lz (um) of the whole lattice along
+ *     z.  Interpolation then sums over owned planes only, spreading writes
+ *     owned planes only, and the wall, nucleus-membrane and RBC-RBC repulsions
+ *     run for the nodes whose lattice index lies in the owned planes.
+ *   zf_cells_reduce_size / zf_cells_reduce_buffer: the node velocities and
+ *     repulsion velocities as one fp64 device buffer of n values (dir 0:
+ *     copied into it, 1: back).  Summed over the slabs after the repulsions
+ *     and before spreading, it gives every slab the unsplit values.
+ *   zf_lbm_step_part_mf: zf_lbm_step_part with the moment store and body-force
+ *     clearing of a membrane iteration. */
+int zf_set_ib_slab(zf_ctx* ctx, int k_lo, int k_hi, double lz);
+int zf_cells_reduce_size(zf_ctx* ctx, int64_t* n);
+int zf_cells_reduce_buffer(zf_ctx* ctx, int dir, void* dev_buf);
+int zf_lbm_step_part_mf(zf_ctx* ctx, int part, int finish, int store_moments, int zero_bodyforce);
+
 /* nsteps iterations of the reference time loop (ZebraflowWT.c:5646-12190):
  * every iteration an LBM step; every `stagger`-th iteration also the
  * membrane forces, IB interpolation, repulsions, spreading and position

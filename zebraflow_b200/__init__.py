@@ -167,6 +167,10 @@ _SIGS = {
     "zf_adjoint_move_cells": (C.c_int, [_P, C.c_int]),
     "zf_adjoint_position_gradient": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "zf_repulsion_vjp": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "zf_set_ib_slab": (C.c_int, [_P, C.c_int, C.c_int, C.c_double]),
+    "zf_cells_reduce_size": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "zf_cells_reduce_buffer": (C.c_int, [_P, C.c_int, C.c_void_p]),
+    "zf_lbm_step_part_mf": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
     "zf_membrane_vjp": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
@@ -585,8 +589,21 @@ class Context:
     def set_slab(self, k_lo: int, k_hi: int):
         _check(lib().zf_set_slab(self._h, k_lo, k_hi))
 
-    def lbm_step_part(self, part: int, finish: bool):
-        _check(lib().zf_lbm_step_part(self._h, part, int(finish)))
+    def lbm_step_part(self, part: int, finish: bool, store_moments=False, zero_bodyforce=False):
+        _check(lib().zf_lbm_step_part_mf(self._h, part, int(finish), int(store_moments), int(zero_bodyforce)))
+
+    def set_ib_slab(self, k_lo: int, k_hi: int, lz: float):
+        """zf_set_ib_slab: owned planes [k_lo, k_hi) of this slab, z period lz (um)."""
+        _check(lib().zf_set_ib_slab(self._h, k_lo, k_hi, float(lz)))
+
+    def cells_reduce_size(self) -> int:
+        n = C.c_int64()
+        _check(lib().zf_cells_reduce_size(self._h, C.byref(n)))
+        return n.value
+
+    def cells_reduce_buffer(self, direction: int, dev_ptr):
+        """zf_cells_reduce_buffer with a device buffer of fp64 at dev_ptr."""
+        _check(lib().zf_cells_reduce_buffer(self._h, int(direction), C.c_void_p(dev_ptr)))
 
     def lbm_steps(self, n: int):
         _check(lib().zf_lbm_steps(self._h, n))

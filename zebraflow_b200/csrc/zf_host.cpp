@@ -531,13 +531,15 @@ int zf_set_slab(zf_ctx* c, int k_lo, int k_hi) {
   return ZF_OK;
 }
 
-int zf_lbm_step_part(zf_ctx* c, int part, int finish) {
+int zf_lbm_step_part(zf_ctx* c, int part, int finish) { return zf_lbm_step_part_mf(c, part, finish, 0, 0); }
+
+int zf_lbm_step_part_mf(zf_ctx* c, int part, int finish, int store_moments, int zero_bodyforce) {
   NEED_LATTICE("zf_lbm_step_part");
   if (!c->slab_set || part < 0 || part > 1) {
     set_error("zf_lbm_step_part: %s", c->slab_set ? "part is 0 (inner) or 1 (faces)" : "zf_set_slab first");
     return ZF_ERR_ARG;
   }
-  int rc = lbm_launch_part(c, part, finish);
+  int rc = lbm_launch_part(c, part, finish, store_moments, zero_bodyforce);
   if (rc == ZF_OK && finish) c->status.iter++;
   return rc;
 }

@@ -166,12 +166,15 @@ __global__ void k_ib_interp(IbArgs a, CellArgs c) {
   const float h2 = 2.f * a.DX;
   StencilAxis SX, SY, SZ;
   node_stencil(a, xp, yp, zp, SX, SY, SZ);
+  if (SZ.b + 3 < a.own_k0 || SZ.b >= a.own_k1) return;  // no owned plane in reach
 
   // velocity interpolation over the 4x4x4 stencil points, in the reference's
   // i, j, k order; fluid points give U, V, W, non-fluid points with a wall
-  // index the void velocity
+  // index the void velocity (on a slab of a split lattice: the owned planes
+  // only, the other slabs add the rest)
   double vx = 0.0, vy = 0.0, vz = 0.0;
   stencil_walk(SX, SY, SZ, h2, [&](int i, int j, int k, double w) {
+    if (k < a.own_k0 || k >= a.own_k1) return;
     const int64_t s = slot_of(a, i, j, wrapk(a, k));
     if (s < 0) return;
     const uint8_t cd = a.code[s];
@@ -250,6 +253,7 @@ __global__ void __launch_bounds__(kRepWarps * 32) k_ib_wall(IbArgs a, CellArgs c
     i0 = lat_index(xp, a.X0, a.DX);
     j0 = lat_index(yp, a.Y0, a.DX);
     k0 = lat_index(zp, a.Z0, a.DX);
+    if (k0 < a.own_k0 || k0 >= a.own_k1) active = false;  // another slab's node
     i1 = max(i0 - 4, 0);
     i2 = min(i0 + 4, a.nx - 1);
     j1 = max(j0 - 4, 0);
@@ -616,6 +620,12 @@ __global__ void k_nuc_memb(IbArgs a, CellArgs c, int rebuild, unsigned long long
     }
     a.nuc_cnt[gid] = l;
   }
+  if (a.own_k0 > -(1 << 30)) {  // a slab of a split lattice: the slab of the node's lattice point pushes
+    float px, py, pz;
+    node_pos(c.xn, nc, c.nnn, cell, node, a.LZ, a.Z0, px, py, pz);
+    const int k0 = lat_index(pz, a.Z0, a.DX);
+    if (k0 < a.own_k0 || k0 >= a.own_k1) return;
+  }
   const int cnt = a.nuc_cnt[gid];
   for (int l = 0; l < cnt; ++l) {
     const int tri = list[l];
@@ -773,6 +783,7 @@ __global__ void __launch_bounds__(kRepWarps * 32) k_rbc_rbc(IbArgs a, CellArgs c
     e1z = c.node_normal[((size_t)2 * nc + cell) * c.nn + node];
     const int i0 = lat_index(xc, a.X0, a.DX), j0 = lat_index(yc, a.Y0, a.DX),
               k0 = lat_index(zc, a.Z0, a.DX);
+    if (k0 < a.own_k0 || k0 >= a.own_k1) active = false;  // another slab's node
     i1 = max(i0 - 4, 0);
     i2 = min(i0 + 4, a.nx - 1);
     j1 = max(j0 - 4, 0);
@@ -1077,12 +1088,13 @@ __global__ void __launch_bounds__(kRgThreads, 3) k_rbc_group(IbArgs a, CellArgs 
           const int i0 = lat_index(px, a.X0, a.DX), j0 = lat_index(py, a.Y0, a.DX), k0 = lat_index(pz, a.Z0, a.DX);
           const int i1 = max(i0 - 4, 0), i2 = min(i0 + 4, a.nx - 1);
           const int j1 = max(j0 - 4, 0), j2 = min(j0 + 4, a.ny - 1);
+          if (k0 < a.own_k0 || k0 >= a.own_k1) cell = -1;  // another slab's node
           // z unwrapped around the node's tile: window k and the block share one frame
           const int kw = a.per_z ? ((k0 % a.nz) + a.nz) % a.nz : k0;
           const int k1 = a.per_z ? kw - 4 : max(k0 - 4, 2), k2 = a.per_z ? kw + 4 : min(k0 + 4, a.nz - 4);
           wxy = onehot_range(i1 - ox, i2 - ox) | (onehot_range(j1 - oy, j2 - oy) << 12);
           wz = onehot_range(k1 - oz, k2 - oz);
-          live = (wxy & 0xfff) && (wxy >> 12) && wz;
+          live = cell >= 0 && (wxy & 0xfff) && (wxy >> 12) && wz;
           if (!live) cell = -1;
         }
         S.node_p[tid] = make_float4(px, py, pz, sqrtf(ex * ex + ey * ey + ez * ez));
@@ -1438,6 +1450,7 @@ __global__ void k_wall_nodes(IbArgs a, CellArgs c, int32_t* __restrict__ walk, i
   float xp, yp, zp;
   node_pos(nuc ? c.xn : c.x, c.n_cells, n, cell, node, a.LZ, a.Z0, xp, yp, zp);
   const int i0 = lat_index(xp, a.X0, a.DX), j0 = lat_index(yp, a.Y0, a.DX), k0 = lat_index(zp, a.Z0, a.DX);
+  if (k0 < a.own_k0 || k0 >= a.own_k1) return;  // another slab's node
   if (max(i0 - 4, 0) > min(i0 + 4, a.nx - 1) || max(j0 - 4, 0) > min(j0 + 4, a.ny - 1) ||
       max(k0 - 4, a.kmin) > min(k0 + 4, a.kmax))
     return;  // empty window
@@ -1709,6 +1722,7 @@ __global__ void k_ib_spread(IbArgs a, CellArgs c, int spread_walls) {
   StencilAxis SX, SY, SZ;
   node_stencil(a, xp, yp, zp, SX, SY, SZ);
   stencil_walk(SX, SY, SZ, h2, [&](int i, int j, int k, double w) {
+    if (k < a.own_k0 || k >= a.own_k1) return;  // another slab's plane
     const int64_t s = slot_of(a, i, j, wrapk(a, k));
     if (s < 0 || s >= a.ns) return;
     const uint8_t cd = a.code[s];
@@ -1792,6 +1806,7 @@ __global__ void __launch_bounds__(256, 5) k_spread_tiles(IbArgs a, CellArgs c, i
           const double w = fxy * (1.0 + (double)Z.c[mk]) / 64.0;
           if (!(w > 0.0)) continue;
           const int k = Z.b + mk;
+          if (k < a.own_k0 || k >= a.own_k1) continue;  // another slab's plane
           const int64_t sl = slot_of(a, i, j, wrapk(a, k));
           if (sl < 0 || sl >= a.ns) continue;
           const uint8_t cd = a.code[sl];
@@ -2541,6 +2556,34 @@ int ib_spread_launch(zf_ctx* ctx) {
   } else {
     k_ib_spread<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(a, c, ctx->p.wall_mode == ZF_WALL_REF_EQ);
   }
+  ZF_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  return ZF_OK;
+}
+
+// node velocities and repulsion velocities <-> one fp64 buffer
+// [vel: 3 nc nn][vel_n: 3 nc nnn][wrep: 3 nc nn] (dir 0: into the buffer, 1: back)
+__global__ void k_kin_buffer(CellArgs c, double* buf, int dir) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nm = 3 * (int64_t)c.n_cells * c.nn, nn_ = 3 * (int64_t)c.n_cells * c.nnn;
+  if (i >= 2 * nm + nn_) return;
+  if (i < nm) {
+    if (dir == 0) buf[i] = c.vel[i];
+    else c.vel[i] = buf[i];
+  } else if (i < nm + nn_) {
+    if (dir == 0) buf[i] = c.vel_n[i - nm];
+    else c.vel_n[i - nm] = buf[i];
+  } else {
+    if (dir == 0) buf[i] = (double)c.wrep[i - nm - nn_];
+    else c.wrep[i - nm - nn_] = (float)buf[i];
+  }
+}
+
+int ib_kin_buffer_launch(zf_ctx* ctx, double* buf, int dir) {
+  const CellArgs& c = ctx->cells;
+  const int64_t n = 3 * (int64_t)c.n_cells * (2 * c.nn + c.nnn);
+  if (n == 0) return ZF_OK;
+  k_kin_buffer<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(c, buf, dir);
   ZF_CUDA(cudaGetLastError());
   ctx->launches += 1;
   return ZF_OK;

@@ -48,6 +48,15 @@ int build_view(zf_ctx* c, const WallHost* W) {
   a.Z0 = P.origin[2];
   a.DX = P.dx;
   a.LZ = P.periodic[2] ? (float)(P.nz * P.dx) : 0.f;
+  a.own_k0 = -(1 << 30);
+  a.own_k1 = 1 << 30;
+  if (c->ib_slab) {  // one slab of a split lattice: see zf_set_ib_slab
+    a.own_k0 = c->ib_k0;
+    a.own_k1 = c->ib_k1;
+    a.kmin = 0;
+    a.kmax = P.nz - 1;
+    a.LZ = (float)c->ib_lz;
+  }
   a.mom = c->d_mom;
   a.force = c->d_force;
   a.ns = c->ns;
@@ -320,6 +329,50 @@ int zf_get_cell_list_counts(zf_ctx* c, int32_t* counts) {
     counts[l] = off[(size_t)key + 1] - off[(size_t)key];
   }
   return ZF_OK;
+}
+
+int zf_set_ib_slab(zf_ctx* c, int k_lo, int k_hi, double lz) {
+  if (!c) return ZF_ERR_ARG;
+  if (!c->lattice_set) {
+    set_error("zf_set_ib_slab: lattice not set");
+    return ZF_ERR_STATE;
+  }
+  if (c->p.periodic[2] || k_lo < 8 || k_hi > c->p.nz - 8 || k_hi <= k_lo || lz < 0.0) {
+    set_error("zf_set_ib_slab: needs a lattice not periodic in z, owned planes [%d, %d) with 8 planes of halo "
+              "on either side (nz %d), lz >= 0",
+              k_lo, k_hi, c->p.nz);
+    return ZF_ERR_ARG;
+  }
+  ZF_CUDA(cudaSetDevice(c->device));
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  c->ib_slab = true;
+  c->ib_k0 = k_lo;
+  c->ib_k1 = k_hi;
+  c->ib_lz = lz;
+  IbArgs& a = c->ib;
+  a.own_k0 = k_lo;
+  a.own_k1 = k_hi;
+  a.kmin = 0;
+  a.kmax = c->p.nz - 1;
+  a.LZ = (float)lz;
+  c->node_tiles_valid = false;
+  return ZF_OK;
+}
+
+int zf_cells_reduce_size(zf_ctx* c, int64_t* n) {
+  if (!c || !n) return ZF_ERR_ARG;
+  *n = c->cells_set ? 3 * (int64_t)c->cells.n_cells * (2 * c->cells.nn + c->cells.nnn) : 0;
+  return ZF_OK;
+}
+
+int zf_cells_reduce_buffer(zf_ctx* c, int dir, void* dev_buf) {
+  if (!c || (dir != 0 && dir != 1) || !dev_buf) return ZF_ERR_ARG;
+  if (!c->cells_set) {
+    set_error("zf_cells_reduce_buffer: cells not set");
+    return ZF_ERR_STATE;
+  }
+  ZF_CUDA(cudaSetDevice(c->device));
+  return ib_kin_buffer_launch(c, (double*)dev_buf, dir);
 }
 
 int zf_ibm_interp(zf_ctx* c) {

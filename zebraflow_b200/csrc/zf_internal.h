@@ -152,6 +152,10 @@ int wall_build(zf_ctx* c, int nw, const float* xyz, int mt, const int32_t* tri1,
 struct IbArgs {
   int nx, ny, nz, ntx, nty, ntz;
   int per_z;
+  int own_k0, own_k1;           // z planes [own_k0, own_k1) this context owns when the lattice is
+                                // one slab of a split one (zf_set_ib_slab): interpolation and
+                                // spreading use only those planes, the repulsions run only for
+                                // nodes whose lattice index lies there; unbounded otherwise
   int kmin, kmax;               // z range of lattice points the coupling sees: the
                                 // reference keeps 3 <= k <= KM-3 (1-based) in its region
                                 // of interest; a periodic axis has no limit
@@ -224,6 +228,7 @@ int ib_bins_launch(zf_ctx* c);
 int ib_nuc_memb_launch(zf_ctx* c, int rebuild);
 int ib_rbc_rbc_launch(zf_ctx* c);
 int ib_node_tiles_launch(zf_ctx* c);
+int ib_kin_buffer_launch(zf_ctx* c, double* buf, int dir);
 int lbm_moments_launch(zf_ctx* c);
 // adjoint building blocks
 int lbm_adj_blocks(zf_ctx* c);
@@ -375,6 +380,12 @@ struct zf_ctx {
   // adjoint: whether its forward moves the cells (zf_adjoint_cells), and the
   // gradient of the last such adjoint with respect to the starting positions
   bool adj_move_cells = false;
+
+  // the IB slab of a split lattice (zf_set_ib_slab): owned planes, and the
+  // period of z positions (0: none)
+  bool ib_slab = false;
+  int ib_k0 = 0, ib_k1 = 0;
+  double ib_lz = 0.0;
   std::vector<float> adj_gx, adj_gxn;  // [3][nc][nn], [3][nc][nnn]
 
   // instrumentation: kernel launches, and optional event pairs around the LBM
@@ -390,7 +401,7 @@ struct zf_ctx {
 
 namespace zf {
 int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out = nullptr);
-int lbm_launch_part(zf_ctx* c, int part, int finish);
+int lbm_launch_part(zf_ctx* c, int part, int finish, int store_moments = 0, int zero_force = 0);
 int ensure_red(zf_ctx* c, int n);
 int lbm_step_mass_noalloc(zf_ctx* c, int store_moments, int zero_force, double* mass_out);
 int lbm_upload_populations(zf_ctx* c, const float* f);

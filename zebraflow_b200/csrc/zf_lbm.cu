@@ -726,12 +726,12 @@ int lbm_launch(zf_ctx* c, int store_moments, int zero_force, double* mass_out) {
 // One part of a slab step (zf_set_slab): the inner tile layers (part 0) or
 // the two face layers next to the halo (part 1); finish: the step is complete
 // (wall pass, swap of the population buffers).
-int lbm_launch_part(zf_ctx* c, int part, int finish) {
+int lbm_launch_part(zf_ctx* c, int part, int finish, int store_moments, int zero_force) {
   LbmArgs a = make_args(c);
   a.active = c->d_active_part[part];
   a.n_active = c->n_active_part[part];
-  a.store_moments = 0;
-  a.zero_force = 0;
+  a.store_moments = store_moments;
+  a.zero_force = zero_force;
   dispatch_storage<LaunchStep>(c->p.storage, c, a, finish != 0);
   ZF_CUDA(cudaGetLastError());
   c->launches += (a.n_active > 0) + (finish && c->p.wall_mode == ZF_WALL_REF_EQ && c->n_wall > 0);

@@ -11,8 +11,8 @@ e_z = -1 populations of its first interior plane to the rank below (its top
 halo plane) and the e_z = +1 populations of its last interior plane to the
 rank above (its bottom halo plane), and the interior evolves exactly as in
 the unsplit lattice.  The halo planes' other populations and the rest of the
-halo layer are never read by the interior.  Body force, cells and the IB
-coupling are not split here: the slab path is the LBM step alone.
+halo layer are never read by the interior.  SlabLBM is the LBM step alone;
+SlabCoupled (below) splits the whole coupled step.
 """
 import numpy as np
 
@@ -32,12 +32,12 @@ def slab_bounds(nz, world, rank):
     return rank * n, (rank + 1) * n
 
 
-def slab_lattice(b_index, world, rank):
-    """The rank's lattice: its interior planes with HALO planes on either
+def slab_lattice(b_index, world, rank, halo=HALO):
+    """The rank's lattice: its interior planes with `halo` planes on either
     side, taken from the z-periodic lattice b_index [nx][ny][nz]."""
     nz = b_index.shape[2]
     z0, z1 = slab_bounds(nz, world, rank)
-    return np.ascontiguousarray(b_index[:, :, np.arange(z0 - HALO, z1 + HALO) % nz])
+    return np.ascontiguousarray(b_index[:, :, np.arange(z0 - halo, z1 + halo) % nz])
 
 
 def plane_counts(b_index):
@@ -68,27 +68,29 @@ class SlabLBM:
     slabs of one process (for instance on one GPU) are advanced together with
     exchange_local."""
 
-    def __init__(self, b_index, world=1, rank=0, device=0, stream=None, group=None, **params):
+    def __init__(self, b_index, world=1, rank=0, device=0, stream=None, group=None, halo=HALO, **params):
         import torch
         nx, ny, nz = b_index.shape
-        self.world, self.rank, self.group = world, rank, group
+        if halo < HALO or halo % HALO:
+            raise ValueError("the halo is whole tile layers")
+        self.world, self.rank, self.group, self.halo = world, rank, group, halo
         self.z0, self.z1 = slab_bounds(nz, world, rank)
-        self.nzs = self.z1 - self.z0 + 2 * HALO
+        self.nzs = self.z1 - self.z0 + 2 * halo
         per = list(params.pop("periodic", (0, 0, 1)))
         per[2] = 0
         self.ctx = Context(default_params(nx=nx, ny=ny, nz=self.nzs, periodic=tuple(per), **params), device)
-        self.ctx.set_lattice(slab_lattice(b_index, world, rank))
+        self.ctx.set_lattice(slab_lattice(b_index, world, rank, halo))
         # inner tile layers and the two face layers are stepped apart; the
         # halo layers are not stepped
-        self.ctx.set_slab(HALO, self.nzs - HALO)
+        self.ctx.set_slab(halo, self.nzs - halo)
         self.stream = stream if stream is not None else torch.cuda.Stream(device=device)
         self.comm = torch.cuda.Stream(device=device) if world > 1 else None
         self.ctx.set_stream(self.stream.cuda_stream)
         # planes (local z): bottom halo / first interior / last interior / top halo
-        self.kb_halo, self.kb, self.kt, self.kt_halo = HALO - 1, HALO, self.nzs - HALO - 1, self.nzs - HALO
+        self.kb_halo, self.kb, self.kt, self.kt_halo = halo - 1, halo, self.nzs - halo - 1, self.nzs - halo
         counts = plane_counts(b_index)
         for k in (self.kb_halo, self.kb, self.kt, self.kt_halo):
-            if self.ctx.plane_count(k) != counts[(self.z0 - HALO + k) % nz]:
+            if self.ctx.plane_count(k) != counts[(self.z0 - halo + k) % nz]:
                 raise RuntimeError(f"slab plane {k}: listed points differ from the lattice's")
         half = params.get("storage", 0) in (1, 2)
         dt = torch.int16 if half else torch.int32
@@ -122,26 +124,29 @@ class SlabLBM:
         state and exchanges them while the inner tile layers are stepped (they
         read no halo plane), then unpacks the halos and steps the two face
         layers.  The halos of the final state are not filled."""
-        import torch
         for _ in range(n):
-            self.pack()
-            if self.world > 1:
-                self.comm.wait_stream(self.stream)
-                with torch.cuda.stream(self.comm):
-                    exchange_dist(self.send_dn, self.send_up, self.recv_dn, self.recv_up, self.rank,
-                                  self.world, self.group)
-            self.ctx.lbm_step_part(0, False)
-            if self.world > 1:
-                self.stream.wait_stream(self.comm)
-            self.unpack()
-            self.ctx.lbm_step_part(1, True)
+            self._lbm_step(False)
+
+    def _lbm_step(self, membrane):
+        import torch
+        self.pack()
+        if self.world > 1:
+            self.comm.wait_stream(self.stream)
+            with torch.cuda.stream(self.comm):
+                exchange_dist(self.send_dn, self.send_up, self.recv_dn, self.recv_up, self.rank,
+                              self.world, self.group)
+        self.ctx.lbm_step_part(0, False, membrane, membrane)
+        if self.world > 1:
+            self.stream.wait_stream(self.comm)
+        self.unpack()
+        self.ctx.lbm_step_part(1, True, membrane, membrane)
 
     def interior(self, dom=None):
         """Mask of the slab's listed points that are interior, and their
         global z plane."""
         dom = self.ctx.domlist() if dom is None else dom
         k = dom[:, 2]
-        return (k >= HALO) & (k < self.nzs - HALO), self.z0 + k - HALO
+        return (k >= self.halo) & (k < self.nzs - self.halo), self.z0 + k - self.halo
 
     def close(self):
         self.ctx.close()
@@ -160,3 +165,121 @@ def exchange_local(slabs):
             s.recv_dn.copy_(slabs[(r - 1) % n].send_up)
     for s in slabs:
         s.unpack()
+
+
+# ---- the coupled step over slabs -------------------------------------------------
+#
+# Fluid sharded, cells replicated.  Every rank holds all cells (their state is
+# small beside the fluid's: 2000 cells of 804 nodes are 39 MB of fp64 positions
+# against 0.56 GB of populations on the C1 workload) and runs the membrane forces
+# for all of them, so cell ownership, migration and ghost cells do not arise.
+# The IB coupling is split by lattice plane (zf_set_ib_slab): a rank
+# interpolates over its own planes only, pushes (wall, nucleus-membrane,
+# RBC-RBC) only the nodes whose lattice point it owns, and spreads only into its
+# own planes.  One all-reduce of the node and repulsion velocities per membrane
+# iteration (2 x 3 x nodes + 3 x nucleus nodes fp64 values) then gives every
+# rank the unsplit velocities, and every rank moves all cells identically.
+# IB_HALO planes of halo (two tile layers) keep the +-4 point windows of the
+# repulsion searches of owned nodes inside the slab's lattice.
+
+IB_HALO = 8
+
+
+class SlabCoupled(SlabLBM):
+    """One rank's slab of the coupled step (zf_step split over z slabs).
+
+    wall = (xyz [3][nw], tri1 [3][mt], nrm [3][mt]) in the global frame; mesh =
+    the zf_set_mesh arguments; cells = (x, xn) of all cells in the global frame;
+    params: default_params keywords for the whole lattice (z periodic)."""
+
+    def __init__(self, b_index, wall, mesh, cells, world=1, rank=0, device=0, stream=None, group=None,
+                 **params):
+        import torch
+        nz = b_index.shape[2]
+        base = default_params()
+        dx = params.get("dx", base.dx)
+        origin = tuple(params.pop("origin", tuple(base.origin)))
+        z0, _ = slab_bounds(nz, world, rank)
+        oz = origin[2] + (z0 - IB_HALO) * dx  # z of the slab lattice's plane 0
+        super().__init__(b_index, world, rank, device, stream, group, halo=IB_HALO,
+                         origin=(origin[0], origin[1], oz), **params)
+        self.lz = nz * dx
+        self.stagger = params.get("stagger", base.stagger)
+        self.nuc_period = params.get("nuc_list_period", base.nuc_list_period)
+        self.ctx.set_ib_slab(IB_HALO, self.nzs - IB_HALO, self.lz)
+        xyz, tri, nrm = wall
+        xyz = np.array(xyz, np.float32)
+        xyz[2] = oz + np.mod(xyz[2] - oz, self.lz)  # folded into the slab's frame
+        self.ctx.set_wall(xyz, tri, nrm)
+        self.ctx.set_mesh(*mesh)
+        self.ctx.set_cells(*cells)
+        self.kin = torch.empty(self.ctx.cells_reduce_size(), dtype=torch.float64, device=f"cuda:{device}")
+
+    def membrane_before_reduce(self):
+        """The membrane iteration up to the velocities' reduction: forces, the
+        LBM step (moments, body force cleared), interpolation and repulsions of
+        this slab; the partial velocities are left in self.kin."""
+        it = self.ctx.iteration() + 1
+        self.ctx.cgsm_forces()
+        self._lbm_step(True)
+        self.ctx.ibm_interp()
+        self.ctx.nuc_memb_repulsion(it % self.nuc_period == 0)
+        self.ctx.rbc_rbc_repulsion()
+        self.ctx.cells_reduce_buffer(0, self.kin.data_ptr())
+
+    def membrane_after_reduce(self):
+        """Back from the reduction: spreading into this slab's planes, update."""
+        self.ctx.cells_reduce_buffer(1, self.kin.data_ptr())
+        self.ctx.ibm_spread()
+        self.ctx.update_positions()
+
+    def step(self, n=1):
+        """n iterations of the reference loop (all ranks call it together)."""
+        import torch
+        import torch.distributed as dist
+        for _ in range(n):
+            if (self.ctx.iteration() + 1) % self.stagger:
+                self._lbm_step(False)
+                continue
+            self.membrane_before_reduce()
+            if self.world > 1:
+                with torch.cuda.stream(self.stream):
+                    dist.all_reduce(self.kin, group=self.group)
+            self.membrane_after_reduce()
+
+
+def coupled_step_local(slabs, n=1):
+    """n iterations of the coupled step over the slabs of one process (one
+    stream): the halo exchange of exchange_local and the velocities' sum in
+    place of the collectives."""
+    import torch
+    for _ in range(n):
+        membrane = (slabs[0].ctx.iteration() + 1) % slabs[0].stagger == 0
+        it = slabs[0].ctx.iteration() + 1
+        if membrane:
+            for s in slabs:
+                s.ctx.cgsm_forces()
+        for s in slabs:
+            s.pack()
+        with torch.cuda.stream(slabs[0].stream):
+            m = len(slabs)
+            for r, s in enumerate(slabs):
+                s.recv_up.copy_(slabs[(r + 1) % m].send_dn)
+                s.recv_dn.copy_(slabs[(r - 1) % m].send_up)
+        for s in slabs:
+            s.unpack()
+            s.ctx.lbm_step_part(0, False, membrane, membrane)
+            s.ctx.lbm_step_part(1, True, membrane, membrane)
+        if not membrane:
+            continue
+        for s in slabs:
+            s.ctx.ibm_interp()
+            s.ctx.nuc_memb_repulsion(it % s.nuc_period == 0)
+            s.ctx.rbc_rbc_repulsion()
+            s.ctx.cells_reduce_buffer(0, s.kin.data_ptr())
+        with torch.cuda.stream(slabs[0].stream):
+            total = torch.stack([s.kin for s in slabs]).sum(dim=0)
+            for s in slabs:
+                s.kin.copy_(total)
+        for s in slabs:
+            s.membrane_after_reduce()
