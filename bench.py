@@ -921,6 +921,58 @@ def run_sharded(args):
     return 0
 
 
+def run_split(args):
+    """The coupled step (the workload's cells included) split into z slabs,
+    one per rank (zebraflow_b200.slabs.SlabCoupled: the fluid sharded, the
+    cells replicated, the IB coupling by owned planes with one all-reduce of
+    the node velocities per membrane iteration).  Strong scaling: the workload
+    is fixed, N ranks share it.  One JSON line, MLUPS of the coupled step from
+    the slowest rank's device time (a step is one 50-iteration cycle)."""
+    import torch
+    import torch.distributed as dist
+    from zebraflow_b200 import slabs
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    case = Case(args.workload, args.cells, args.seed)
+    st = STORAGES[args.storage]
+    p = case.params(st)
+    kw = dict(tau=p.tau, tau_from_phase=0, wall_mode=WALL_HALFWAY_BB, g=tuple(p.g), storage=st,
+              origin=(0.0, 0.0, 0.0), dx=DX_UM, area0=0.0, volume0=0.0)
+    slab = slabs.SlabCoupled(case.b, case.wall, case.mesh, case.cells, world=world, rank=rank, device=local,
+                             **kw)
+    cycle = slab.stagger
+    slab.step(args.warmup * cycle)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(local)
+    e0.record(slab.stream)
+    slab.step(args.steps * cycle)
+    e1.record(slab.stream)
+    torch.cuda.synchronize(local)
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        ms = max_over_ranks([ms], f"cuda:{local}")[0]
+    if rank == 0:
+        print(json.dumps({"metric": "MLUPS", "value": round(case.n_fluid * cycle * args.steps / (ms * 1e-3) / 1e6, 1),
+                          "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+                          "scaling": "strong", "dtype": DTYPE_NAME[st], "data": "synthetic",
+                          "config": {"workload": args.workload, "fluid_points": case.n_fluid,
+                                     "cells": case.n_cells, "iterations_per_step": cycle,
+                                     "parallelism": f"z slabs x{world}: fluid sharded, cells replicated, "
+                                                    "IB by owned planes, velocity all-reduce per membrane "
+                                                    "iteration"}}),
+              flush=True)
+    slab.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -949,12 +1001,17 @@ def main():
     ap.add_argument("--sharded", action="store_true",
                     help="instead of the bench line, the LBM step of the lattice split into z slabs "
                          "over the ranks (no cells)")
+    ap.add_argument("--split", action="store_true",
+                    help="instead of the bench line, the coupled step split into z slabs over the ranks "
+                         "(fluid sharded, cells replicated)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.c2_steps > 0:
         return run_c2(args)
     if args.sharded and args.impl == "ours":
         return run_sharded(args)
+    if args.split and args.impl == "ours":
+        return run_split(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -27,8 +27,10 @@
 //               lam_x += vs sum_s grad_x w (U(s) . lam_u)
 // with w = prod_a (1 + cos(pi |d_a| / (2 DX))) / 64, d_a = x_lat,a - x_a, so
 // dw/dx_a = (pi / (2 DX)) sin(pi |d_a| / (2 DX)) sign(d_a) prod_{b != a}(...) / 64.
-// The repulsion terms (wall, nucleus-membrane, RBC-RBC) enter as held values:
-// their dependence on the positions is not differentiated.
+// It also forms lam_w = lam_u + gamma_p lam_F, the adjoint of the repulsion
+// velocities wrep, which k_rbc_vjp, k_wall_vjp and k_nuc_vjp (below) carry
+// through the RBC-RBC (:9919-10053), wall (:9055-9077) and nucleus-membrane
+// (:9516-9730) repulsions to the positions.
 #include "zf_internal.h"
 
 namespace zf {
