@@ -84,3 +84,55 @@ def test_two_slabs_match_the_whole_coupled_step():
     assert moved > 1e-3
     assert dx_split <= max(10 * dx_runs, 1e-9 * moved)
     assert df_split <= max(10 * df_runs, 1e-7)
+
+
+def _free_port():
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _gloo_rank(rank, world, port, out_dir):
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=120))
+    b, mesh, cells, wall, kw = setup()
+    s = slabs.SlabCoupled(b, wall, mesh, cells, world=world, rank=rank, device=0, **kw)
+    s.step(NSTEPS)
+    torch.cuda.synchronize()
+    sdom = s.ctx.domlist()
+    inner, gz = s.interior(sdom)
+    np.savez(f"{out_dir}/rank{rank}.npz", x=s.ctx.cells()[0], ij=sdom[inner, :2], gz=gz[inner],
+             f=s.ctx.download_populations()[:, inner])
+    s.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_match_the_whole_coupled_step(tmp_path):
+    """SlabCoupled.step itself at world 2: two processes, one slab each, on the
+    one GPU, with the halo ring and the velocities' all-reduce through
+    torch.distributed (gloo, staged through host memory; no kernel waits on
+    another rank's)."""
+    import torch.multiprocessing as mp
+    mp.start_processes(_gloo_rank, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    b, mesh, cells, wall, kw = setup()
+    f1, xa, dom = unsplit(b, mesh, cells, wall, kw)
+    f2, xb, _ = unsplit(b, mesh, cells, wall, kw)
+    index = {tuple(p): l for l, p in enumerate(dom.tolist())}
+    r = [np.load(tmp_path / f"rank{k}.npz") for k in range(2)]
+    assert np.array_equal(r[0]["x"], r[1]["x"])
+    dx_runs = np.abs(xb - xa).max()
+    dx_split = np.abs(r[0]["x"] - xa).max()
+    df_runs = np.abs(f2 - f1).max()
+    df_split = 0.0
+    for q in r:
+        gl = np.array([index[(i, j, k % NZ)] for (i, j), k in zip(q["ij"].tolist(), q["gz"].tolist())])
+        df_split = max(df_split, np.abs(q["f"] - f1[:, gl]).max())
+    print(f"positions: split {dx_split:.3e}, between runs {dx_runs:.3e}; "
+          f"populations: split {df_split:.3e}, between runs {df_runs:.3e}")
+    assert np.abs(xa - cells[0]).max() > 1e-3
+    assert dx_split <= max(10 * dx_runs, 1e-9)
+    assert df_split <= max(10 * df_runs, 1e-7)

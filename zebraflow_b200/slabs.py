@@ -45,11 +45,25 @@ def plane_counts(b_index):
     return (b_index >= 0).sum(axis=(0, 1))
 
 
+def _staged(t, group):
+    """Whether a device tensor goes through host memory for this group's
+    backend (gloo moves host tensors)."""
+    import torch.distributed as dist
+    return t.is_cuda and dist.get_backend(group) == "gloo"
+
+
 def exchange_dist(send_dn, send_up, recv_dn, recv_up, rank, world, group=None):
     """The halo exchange between ranks in a ring: send_dn goes to the rank
     below (rank - 1), whose recv_up takes it; send_up to the rank above, whose
-    recv_dn takes it.  Tensors of any device the process group serves."""
+    recv_dn takes it.  Device tensors with NCCL; with gloo they are staged
+    through host memory."""
     import torch.distributed as dist
+    if _staged(send_dn, group):
+        h = [t.cpu() for t in (send_dn, send_up)] + [torch_empty_host(t) for t in (recv_dn, recv_up)]
+        exchange_dist(h[0], h[1], h[2], h[3], rank, world, group)
+        recv_dn.copy_(h[2])
+        recv_up.copy_(h[3])
+        return
     below, above = (rank - 1) % world, (rank + 1) % world
     ops = [dist.P2POp(dist.isend, send_dn, below, group, tag=1),
            dist.P2POp(dist.isend, send_up, above, group, tag=2),
@@ -57,6 +71,23 @@ def exchange_dist(send_dn, send_up, recv_dn, recv_up, rank, world, group=None):
            dist.P2POp(dist.irecv, recv_dn, below, group, tag=2)]
     for req in dist.batch_isend_irecv(ops):
         req.wait()
+
+
+def torch_empty_host(t):
+    import torch
+    return torch.empty(t.shape, dtype=t.dtype, device="cpu")
+
+
+def all_reduce_sum(t, group=None):
+    """Sum of t over the group's ranks, in place (staged through host memory
+    for gloo)."""
+    import torch.distributed as dist
+    if _staged(t, group):
+        h = t.cpu()
+        dist.all_reduce(h, group=group)
+        t.copy_(h)
+    else:
+        dist.all_reduce(t, group=group)
 
 
 class SlabLBM:
@@ -236,7 +267,6 @@ class SlabCoupled(SlabLBM):
     def step(self, n=1):
         """n iterations of the reference loop (all ranks call it together)."""
         import torch
-        import torch.distributed as dist
         for _ in range(n):
             if (self.ctx.iteration() + 1) % self.stagger:
                 self._lbm_step(False)
@@ -244,7 +274,7 @@ class SlabCoupled(SlabLBM):
             self.membrane_before_reduce()
             if self.world > 1:
                 with torch.cuda.stream(self.stream):
-                    dist.all_reduce(self.kin, group=self.group)
+                    all_reduce_sum(self.kin, self.group)
             self.membrane_after_reduce()
 
 
