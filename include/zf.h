@@ -492,6 +492,45 @@ int zf_cells_reduce_size(zf_ctx* ctx, int64_t* n);
 int zf_cells_reduce_buffer(zf_ctx* ctx, int dir, void* dev_buf);
 int zf_lbm_step_part_mf(zf_ctx* ctx, int part, int finish, int store_moments, int zero_bodyforce);
 
+/* Periodic parent segments and cell cloning (the reference's inflow,
+ * ZebraflowWT.c:11926-11960, :12193-12403), as host steps on host arrays
+ * between membrane iterations; zebraflow_b200/inflow.py drives them around a
+ * parent-segment context and a region context.  A segment is periodic over
+ * [z0, z1) (um); direction +1: the flow leaves it at z1, -1: at z0; dx is the
+ * lattice spacing (um).  Statuses as the reference's (:256-263): parents 2
+ * (interior) or 4 (cloned, not yet re-armed); region slots -(p + 1) (clone
+ * slaved to parent p), 1 (independent), -5000 (free).
+ *   zf_inflow_slaves: after the region's update, the nodes of slaved clones
+ *     that were not yet 5 dx past the exit plane move with their parent's
+ *     node velocity (vp, vnp) instead of their own (vr, vnr; x += (vp - vr)
+ *     dt_stagger); a clone whose nodes all passed the plane becomes 1.
+ *   zf_inflow_parents: after the segment's update, the parents' z folded into
+ *     [z0, z1); clone[p] = 1 for a status-2 parent that crossed the exit plane
+ *     and has not regressed; status-4 parents are re-armed inside the window.
+ *   zf_inflow_clone: every parent with clone[p] copied, in order, into the
+ *     first free slot (z made contiguous across the exit plane), the slot
+ *     -(p + 1), the parent 4; cloned_into[p] the slot or -1 (may be NULL). */
+typedef struct {
+  double z0, z1;
+  int32_t direction;
+  double dx;
+} zf_inflow_segment;
+int zf_inflow_slaves(const zf_inflow_segment* seg, double dt_stagger, int n_slots, int nn, int nnn, double* xr,
+                     double* xnr, const double* vr, const double* vnr, int32_t* status_r, int n_parents,
+                     const double* vp, const double* vnp);
+int zf_inflow_parents(const zf_inflow_segment* seg, int n_parents, int nn, int nnn, double* x, double* xn,
+                      int32_t* status, int32_t* regress, int32_t* clone);
+int zf_inflow_clone(const zf_inflow_segment* seg, int n_parents, int nn, int nnn, const double* xp,
+                    const double* xnp, int32_t* status_p, int32_t* regress_p, int32_t* clone, int n_slots,
+                    double* xr, double* xnr, int32_t* status_r, int32_t* cloned_into);
+
+/* The cells' positions and statuses overwritten from host arrays of the
+ * context's cell count (zf_set_cells keeps the cell count and buffers but
+ * makes every cell active; these keep everything else): x [3][cells][nn],
+ * xn [3][cells][nnn] (or NULL), status [cells] (or NULL; -5000 a free slot,
+ * skipped by every kernel, > 0 active). */
+int zf_put_cells(zf_ctx* ctx, const double* x, const double* xn, const int32_t* status);
+
 /* nsteps iterations of the reference time loop (ZebraflowWT.c:5646-12190):
  * every iteration an LBM step; every `stagger`-th iteration also the
  * membrane forces, IB interpolation, repulsions, spreading and position

@@ -78,6 +78,13 @@ def lib() -> C.CDLL:
                                            C.c_void_p]
             g("orc_lbm_moments_from_f").argtypes = [C.c_void_p]
             g("orc_lbm_set_iter").argtypes = [C.c_void_p, C.c_int64]
+        # the inflow steps (one precision: fp64 positions, as the reference's)
+        L.orc_inflow_roi_update.argtypes = [C.c_double, C.c_double, C.c_int, C.c_double, C.c_double, C.c_int,
+                                            C.c_int, C.c_int] + [C.c_void_p] * 5 + [C.c_int] + [C.c_void_p] * 2
+        L.orc_inflow_parent_update.argtypes = [C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int,
+                                               C.c_int] + [C.c_void_p] * 7
+        L.orc_inflow_clone.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int] + \
+            [C.c_void_p] * 5 + [C.c_int] + [C.c_void_p] * 3
         _lib = L
     return _lib
 

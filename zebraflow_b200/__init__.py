@@ -168,6 +168,14 @@ _SIGS = {
     "zf_adjoint_position_gradient": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "zf_repulsion_vjp": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
     "zf_set_ib_slab": (C.c_int, [_P, C.c_int, C.c_int, C.c_double]),
+    "zf_put_cells": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "zf_inflow_slaves": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "zf_inflow_parents": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]),
+    "zf_inflow_clone": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p]),
     "zf_cells_reduce_size": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "zf_cells_reduce_buffer": (C.c_int, [_P, C.c_int, C.c_void_p]),
     "zf_lbm_step_part_mf": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -668,6 +676,13 @@ class Context:
         st = np.empty(self.nc, np.int32)
         _check(lib().zf_get_cells(self._h, _ptr(x), _ptr(xn), _ptr(st)))
         return x, xn, st
+
+    def put_cells(self, x=None, xn=None, status=None):
+        """zf_put_cells: overwrite positions and/or statuses of all cells."""
+        x_ = None if x is None else np.ascontiguousarray(x, np.float64)
+        xn_ = None if xn is None else np.ascontiguousarray(xn, np.float64)
+        st = None if status is None else np.ascontiguousarray(status, np.int32)
+        _check(lib().zf_put_cells(self._h, _ptr(x_), _ptr(xn_), _ptr(st)))
 
     def cells_async(self, x, xn, status):
         """Queue the copies of zf_get_cells into x [3][nc][nn], xn and status

@@ -412,6 +412,23 @@ int zf_set_cells(zf_ctx* c, int n_cells, const double* x, const double* xn) {
   return ib_prepare(c);  // cell list and nucleus lists sized for these cells
 }
 
+int zf_put_cells(zf_ctx* c, const double* x, const double* xn, const int32_t* status) {
+  if (!c) return ZF_ERR_ARG;
+  NEED(c->cells_set, "zf_put_cells", "cells not set");
+  ZF_CUDA(cudaSetDevice(c->device));
+  int rc = cells_write_fence(c);  // a pending asynchronous copy still reads the positions
+  if (rc) return rc;
+  const CellArgs& a = c->cells;
+  const size_t nc = a.n_cells;
+  if (x) ZF_CUDA(cudaMemcpyAsync(a.x, x, 3 * nc * a.nn * 8, cudaMemcpyHostToDevice, c->stream));
+  if (xn && a.nnn) ZF_CUDA(cudaMemcpyAsync(a.xn, xn, 3 * nc * a.nnn * 8, cudaMemcpyHostToDevice, c->stream));
+  if (status) ZF_CUDA(cudaMemcpyAsync(a.status, status, nc * 4, cudaMemcpyHostToDevice, c->stream));
+  ZF_CUDA(cudaStreamSynchronize(c->stream));
+  c->node_tiles_valid = false;  // positions changed
+  c->nuc_lists_valid = false;
+  return ZF_OK;
+}
+
 int zf_get_cells(zf_ctx* c, double* x, double* xn, int32_t* status) {
   if (!c) return ZF_ERR_ARG;
   NEED(c->cells_set, "zf_get_cells", "cells not set");
