@@ -27,7 +27,7 @@ def _rank(rank, world, port, out):
 
 def test_two_ranks_report_the_slowest():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # a forked manager could inherit held locks
         out = m.dict()
         mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
         res = dict(out)

@@ -56,7 +56,7 @@ def _rank(rank, world, port, out):
 
 @pytest.mark.parametrize("world", [2, 3])
 def test_ring_exchange_between_gloo_ranks(world):
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # a forked manager could inherit held locks
         out = m.dict()
         mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
         res = dict(out)
@@ -128,7 +128,7 @@ def test_two_gloo_ranks_step_the_split_lattice_exactly():
     rf = ref.get_f()
     ref.close()
     where = {tuple(p): i for i, p in enumerate(rdom)}
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # a forked manager could inherit held locks
         out = m.dict()
         mp.spawn(_slab_rank, args=(world, _free_port(), b, steps, out), nprocs=world, join=True)
         res = dict(out)
