@@ -57,6 +57,11 @@ def test_noalloc_matches_allocating_step_twice(storage, store_moments):
     m_ref, m_new = ctypes.c_double(), ctypes.c_double()
     zf._check(L.zf_lbm_step_mass(ref._h, store_moments, 0, ctypes.byref(m_ref)))
     zf._check(L.zf_lbm_step_mass_noalloc(new._h, store_moments, 0, ctypes.byref(m_new)))
+    # the download kernels' first launches too, so that the driver loading
+    # their code cannot fall between the two free-memory readings
+    for ctx in (ref, new):
+        ctx.download_populations()
+        ctx.download_moments()
     torch.cuda.synchronize()
     free0, _ = torch.cuda.mem_get_info(0)
     ctx_bytes0 = new.device_bytes()
