@@ -1,8 +1,8 @@
 """Shared test set-up: the `gpu` marker and the two libraries under test.
 
 `libzf.so` (the product, include/zf.h) with its C host driver `zf_run`, and
-`oracle/liboracle.so` (the CPU restatement of the reference used as the
-checker) are built on first use.
+`oracle/liboracle.so` (the CPU restatement of the reference that the
+parity tests compare against) are built on first use.
 """
 import os
 import subprocess
