@@ -1,6 +1,7 @@
 """ORACLE — test infrastructure only.
 
-CPU restatement of the reference (SweSoe/Zebraflow) hot path, that the parity
-tests compare against, in tests/, by ``__graft_entry__.smoke()`` and by the CPU
-baseline leg of ``bench.py``.  The product library never imports or links it.
+CPU restatement of the reference (SweSoe/Zebraflow) hot path.  The parity
+tests in tests/ and ``__graft_entry__.smoke()`` compare the GPU path against
+it, and the CPU baseline leg of ``bench.py`` times it.  The product library
+never imports or links it.
 """
